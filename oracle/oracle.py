@@ -1,0 +1,211 @@
+"""ctypes loader for the CPU FP64 oracle -- TEST INFRASTRUCTURE, NOT THE PRODUCT.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs import
+this module.  It wraps oracle/libthp_oracle.so (built by oracle/Makefile), the
+C++ restatement of the Tinker-HP v1.2 polarization path.  Parity status:
+unpinned by the reference (no golden vectors exist for this path); pinned by
+self-consistency tests in tests/test_oracle.py.
+"""
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libthp_oracle.so")
+
+CONN_NAMES = ("i12", "i13", "i14", "i15", "ip11", "ip12", "ip13", "ip14")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class OrSystem(C.Structure):
+    _fields_ = [
+        ("n", C.c_int),
+        ("xbox", C.c_double), ("ybox", C.c_double), ("zbox", C.c_double),
+        ("x", _dp), ("y", _dp), ("z", _dp),
+        ("rpole", _dp), ("polarity", _dp), ("thole", _dp), ("pdamp", _dp),
+        ("conn_off", _ip * 8), ("conn_idx", _ip * 8),
+        ("p_scale", C.c_double * 4), ("pi_scale", C.c_double * 4),
+        ("d_scale", C.c_double * 4), ("u_scale", C.c_double * 4),
+        ("aewald", C.c_double), ("ewaldcut", C.c_double), ("lbuffer", C.c_double),
+        ("vdwcut", C.c_double),
+        ("nfft1", C.c_int), ("nfft2", C.c_int), ("nfft3", C.c_int), ("bsorder", C.c_int),
+        ("politer", C.c_int), ("poleps", C.c_double), ("nthreads", C.c_int),
+    ]
+
+
+class OrSolveInfo(C.Structure):
+    _fields_ = [("niter", C.c_int), ("converged", C.c_int), ("resnrm", C.c_double),
+                ("ene", C.c_double * 2)]
+
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.or_create.restype = C.c_void_p
+        L.or_create.argtypes = [C.POINTER(OrSystem)]
+        L.or_destroy.argtypes = [C.c_void_p]
+        L.or_mlistcell.argtypes = [C.c_void_p, C.c_int, _ip, _ip]
+        L.or_efld0_direct.argtypes = [C.c_void_p, _dp]
+        L.or_tmatxb_pme.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp]
+        L.or_efld0_recip.argtypes = [C.c_void_p, _dp]
+        L.or_tmatxbrecip.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+        L.or_newinduce_pme2.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.POINTER(OrSolveInfo)]
+        L.or_epolar.restype = C.c_double
+        L.or_epolar.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+        L.or_rotpole.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _dp]
+        L.or_ewaldcof.restype = C.c_double
+        L.or_ewaldcof.argtypes = [C.c_double]
+        L.or_erfc.restype = C.c_double
+        L.or_erfc.argtypes = [C.c_double]
+        L.or_fft3d.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_int]
+        _lib = L
+    return _lib
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def rotpole(ws):
+    """Global-frame multipoles [n,13] for a water.WaterSystem (rotpole.f:17)."""
+    n = ws.n
+    rp = np.zeros((n, 13))
+    pole = np.ascontiguousarray(ws.pole, dtype=np.float64)
+    lib().or_rotpole(n, _p(ws.x), _p(ws.y), _p(ws.z), _p(pole), _p(ws.zaxis, _ip), _p(ws.xaxis, _ip),
+                     _p(ws.axt, _ip), _p(rp))
+    return rp
+
+
+def fft3d(grid, sign):
+    """In-place unnormalised complex FFT of a [n3,n2,n1] complex128 array."""
+    g = np.ascontiguousarray(grid, dtype=np.complex128).copy()
+    n3, n2, n1 = g.shape
+    lib().or_fft3d(g.ctypes.data_as(_dp), n1, n2, n3, sign)
+    return g
+
+
+class Oracle:
+    """One system on the CPU oracle. Vectors use the reference's (3,nrhs,n)
+    interleave: shape [n, nrhs, 3]."""
+
+    MAXELST = 1200  # MOD_sizes.f:58
+
+    def __init__(self, ws, rpole=None, politer=500, poleps=1e-6, nthreads=1, vdwcut=9.0):
+        self.ws = ws
+        self.rpole = np.ascontiguousarray(rotpole(ws) if rpole is None else rpole, dtype=np.float64)
+        self._keep = []
+        s = OrSystem()
+        s.n = ws.n
+        s.xbox, s.ybox, s.zbox = ws.box
+        self._x = np.ascontiguousarray(ws.x, dtype=np.float64)
+        self._y = np.ascontiguousarray(ws.y, dtype=np.float64)
+        self._z = np.ascontiguousarray(ws.z, dtype=np.float64)
+        self._pol = np.ascontiguousarray(ws.polarity, dtype=np.float64)
+        self._thl = np.ascontiguousarray(ws.thole, dtype=np.float64)
+        self._pd = np.ascontiguousarray(ws.pdamp, dtype=np.float64)
+        s.x, s.y, s.z = _p(self._x), _p(self._y), _p(self._z)
+        s.rpole = _p(self.rpole)
+        s.polarity, s.thole, s.pdamp = _p(self._pol), _p(self._thl), _p(self._pd)
+        for q, name in enumerate(CONN_NAMES):
+            off, idx = ws.conn[name]
+            off = np.ascontiguousarray(off, dtype=np.int32)
+            idx = np.ascontiguousarray(idx if len(idx) else np.zeros(1, np.int32), dtype=np.int32)
+            self._keep += [off, idx]
+            s.conn_off[q] = _p(off, _ip)
+            s.conn_idx[q] = _p(idx, _ip)
+        for key in ("p_scale", "pi_scale", "d_scale", "u_scale"):
+            arr = getattr(s, key)
+            for q in range(4):
+                arr[q] = ws.scales[key][q]
+        s.aewald, s.ewaldcut, s.lbuffer, s.vdwcut = ws.aewald, ws.ewaldcut, ws.lbuffer, vdwcut
+        s.nfft1, s.nfft2, s.nfft3 = ws.nfft
+        s.bsorder = ws.bsorder
+        s.politer, s.poleps, s.nthreads = politer, poleps, nthreads
+        self.sys = s
+        self.ctx = lib().or_create(C.byref(s))
+        self.nelst = None
+        self.elst = None
+
+    def close(self):
+        if self.ctx:
+            lib().or_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def mlistcell(self, maxelst=None):
+        maxelst = maxelst or self.MAXELST
+        n = self.ws.n
+        nelst = np.zeros(n, np.int32)
+        elst = np.zeros(n * maxelst, np.int32)
+        st = lib().or_mlistcell(self.ctx, maxelst, _p(nelst, _ip), _p(elst, _ip))
+        self.nelst, self.elst = nelst, elst.reshape(n, maxelst)
+        return st, nelst, self.elst
+
+    def pairs(self):
+        """Sorted (i, k) half-list pairs as an [P,2] int array."""
+        rows = np.repeat(np.arange(self.ws.n), self.nelst)
+        mask = np.arange(self.elst.shape[1])[None, :] < self.nelst[:, None]
+        cols = self.elst[mask]
+        p = np.stack([rows, cols], axis=1)
+        return p[np.lexsort((p[:, 1], p[:, 0]))]
+
+    def efld0_direct(self):
+        ef = np.zeros((self.ws.n, 2, 3))
+        lib().or_efld0_direct(self.ctx, _p(ef))
+        return ef
+
+    def tmatxb(self, mu, dodiag=True):
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        efi = np.zeros_like(mu)
+        lib().or_tmatxb_pme(self.ctx, mu.shape[1], int(dodiag), _p(mu), _p(efi))
+        return efi
+
+    def efld0_recip(self):
+        cphi = np.zeros((self.ws.n, 10))
+        lib().or_efld0_recip(self.ctx, _p(cphi))
+        return cphi
+
+    def tmatxbrecip(self, mu):
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        out = np.zeros_like(mu)
+        lib().or_tmatxbrecip(self.ctx, mu.shape[1], _p(mu), _p(out))
+        return out
+
+    def solve(self, mu_guess=None):
+        n = self.ws.n
+        uind = np.zeros((n, 3))
+        uinp = np.zeros((n, 3))
+        ef = np.zeros((n, 2, 3))
+        info = OrSolveInfo()
+        g = None if mu_guess is None else np.ascontiguousarray(mu_guess, dtype=np.float64)
+        st = lib().or_newinduce_pme2(self.ctx, _p(g), _p(uind), _p(uinp), _p(ef), C.byref(info))
+        if st != 0:
+            raise RuntimeError(f"oracle solve failed with status {st}")
+        return {"uind": uind, "uinp": uinp, "ef": ef, "niter": info.niter,
+                "converged": bool(info.converged), "resnrm": info.resnrm, "ene": tuple(info.ene)}
+
+    def epolar(self, uind):
+        uind = np.ascontiguousarray(uind, dtype=np.float64)
+        er, ek, es = C.c_double(), C.c_double(), C.c_double()
+        e = lib().or_epolar(self.ctx, _p(uind), C.byref(er), C.byref(ek), C.byref(es))
+        return e, {"real": er.value, "recip": ek.value, "self": es.value}

@@ -1,0 +1,1430 @@
+// thp_oracle.cpp -- TEST INFRASTRUCTURE, NOT THE PRODUCT.
+//
+// CPU FP64 restatement of the Tinker-HP v1.2 induced-dipole polarization path.
+// Each routine cites the reference routine it restates (paths are relative to
+// the Tinker-HP repository).  Only tests/, __graft_entry__.smoke() and the CPU
+// baseline legs of bench.py load this code; the CUDA library never does.
+//
+// Parity status: unpinned by the reference (no Fortran toolchain here, no
+// golden vectors for this path); pinned by self-consistency tests.
+//
+// Build: oracle/Makefile (-O2 -ffp-contract=off so that r^2 tests round like
+// the reference's unfused Fortran arithmetic).
+
+#include "thp_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr double kPi = 3.141592653589793238;
+constexpr double kSqrtPi = 1.772453850905516027;
+constexpr double kElectric = 332.063714;  // MOD_units.f:81 (coulomb)
+constexpr double kTinyPol = (double)1e-5f; // MOD_polar.f:36 (single-precision literal)
+
+int nthreads_of(const OrSystem* s) { return s->nthreads > 0 ? s->nthreads : 1; }
+
+// ---------------------------------------------------------------------------
+// image.f:113-138, orthogonal branch
+struct Cell {
+  double xcell, ycell, zcell, xcell2, ycell2, zcell2;
+};
+
+inline void image1(double& r, double cell, double cell2) {
+  if (std::fabs(r) > cell2) {
+    double cel = std::copysign(cell, r);
+    r = r - cel * std::floor(std::fabs(r) / cell);
+    if (std::fabs(r) > cell2) r = r - std::copysign(cell, r);
+  }
+}
+inline void image(const Cell& c, double& xr, double& yr, double& zr) {
+  image1(xr, c.xcell, c.xcell2);
+  image1(yr, c.ycell, c.ycell2);
+  image1(zr, c.zcell, c.zcell2);
+}
+
+// ---------------------------------------------------------------------------
+// erf.f:44-200 (erfcore, mode 1): W. J. Cody, "Rational Chebyshev
+// Approximations for the Error Function", Math. Comp. 23, 631-638 (1969).
+double erfc_cody(double arg) {
+  static const double a[5] = {3.16112374387056560e0, 1.13864154151050156e2, 3.77485237685302021e2,
+                              3.20937758913846947e3, 1.85777706184603153e-1};
+  static const double b[4] = {2.36012909523441209e1, 2.44024637934444173e2, 1.28261652607737228e3,
+                              2.84423683343917062e3};
+  static const double c[9] = {5.64188496988670089e-1, 8.88314979438837594e0, 6.61191906371416295e1,
+                              2.98635138197400131e2,  8.81952221241769090e2, 1.71204761263407058e3,
+                              2.05107837782607147e3,  1.23033935479799725e3, 2.15311535474403846e-8};
+  static const double d[8] = {1.57449261107098347e1, 1.17693950891312499e2, 5.37181101862009858e2,
+                              1.62138957456669019e3, 3.29079923573345963e3, 4.36261909014324716e3,
+                              3.43936767414372164e3, 1.23033935480374942e3};
+  static const double p[6] = {3.05326634961232344e-1, 3.60344899949804439e-1, 1.25781726111229246e-1,
+                              1.60837851487422766e-2, 6.58749161529837803e-4, 1.63153871373020978e-2};
+  static const double q[5] = {2.56852019228982242e0, 1.87295284992346047e0, 5.27905102951428412e-1,
+                              6.05183413124413191e-2, 2.33520497626869185e-3};
+  const double sqrpi = 5.6418958354775628695e-1;
+  const double xtiny = 1.11e-16, xbig = 26.543;
+  double x = arg, y = std::fabs(x), result;
+  if (y <= 0.46875) {
+    double ysq = 0.0;
+    if (y > xtiny) ysq = y * y;
+    double xnum = a[4] * ysq, xden = ysq;
+    for (int i = 0; i < 3; ++i) {
+      xnum = (xnum + a[i]) * ysq;
+      xden = (xden + b[i]) * ysq;
+    }
+    result = x * (xnum + a[3]) / (xden + b[3]);
+    result = 1.0 - result;
+  } else if (y <= 4.0) {
+    double xnum = c[8] * y, xden = y;
+    for (int i = 0; i < 7; ++i) {
+      xnum = (xnum + c[i]) * y;
+      xden = (xden + d[i]) * y;
+    }
+    result = (xnum + c[7]) / (xden + d[7]);
+    double ysq = std::trunc(16.0 * y) / 16.0;
+    double del = (y - ysq) * (y + ysq);
+    result = std::exp(-ysq * ysq - del) * result;
+    if (x < 0.0) result = 2.0 - result;
+  } else {
+    result = 0.0;
+    if (y < xbig) {
+      double ysq = 1.0 / (y * y);
+      double xnum = p[5] * ysq, xden = ysq;
+      for (int i = 0; i < 4; ++i) {
+        xnum = (xnum + p[i]) * ysq;
+        xden = (xden + q[i]) * ysq;
+      }
+      result = ysq * (xnum + p[4]) / (xden + q[4]);
+      result = (sqrpi - result) / y;
+      ysq = std::trunc(16.0 * y) / 16.0;
+      double del = (y - ysq) * (y + ysq);
+      result = std::exp(-ysq * ysq - del) * result;
+    }
+    if (x < 0.0) result = 2.0 - result;
+  }
+  return result;
+}
+
+// damping.f:17-55 (dampewald)
+inline void dampewald(int rorder, double r, double r2, double scale, double aewald, double* dmpe) {
+  for (int i = 1; i <= rorder; ++i) dmpe[i] = scale;
+  double ra = aewald * r;
+  double bn[6];
+  bn[0] = erfc_cody(ra) / r;
+  dmpe[1] = scale * bn[0];
+  double expterm = std::exp(-ra * ra);
+  double aesq2 = 2.0 * aewald * aewald;
+  double afac = 0.0;
+  if (aewald > 0.0) afac = 1.0 / (kSqrtPi * aewald);
+  int niter = (rorder - 1) / 2;
+  for (int i = 1; i <= niter; ++i) {
+    double bfac = (double)(2 * i - 1);
+    afac = aesq2 * afac;
+    bn[i] = (bfac * bn[i - 1] + afac * expterm) / r2;
+    dmpe[2 * i + 1] = scale * bn[i];
+  }
+}
+
+// damping.f:74-124 (dampthole) == damping.f:142-216 (damptholed, AMOEBA branch)
+inline void dampthole(double pdi, double pdk, double thi, double thk, int rorder, double r,
+                      double* dmpik) {
+  for (int j = 1; j <= rorder; ++j) dmpik[j] = 1.0;
+  double damp = pdi * pdk;
+  // kpolar.f:281-290 pair rule: min, or max when the min is zero
+  double pgamma = std::min(thi, thk);
+  if (pgamma == 0.0) pgamma = std::max(thi, thk);
+  if (damp != 0.0 && pgamma != 0.0) {
+    double t = r / damp;
+    damp = pgamma * (t * t * t);
+    if (damp < 50.0) {
+      double expdamp = std::exp(-damp);
+      dmpik[3] = 1.0 - expdamp;
+      dmpik[5] = 1.0 - expdamp * (1.0 + damp);
+      if (rorder >= 7) {
+        double damp2 = damp * damp;
+        dmpik[7] = 1.0 - expdamp * (1.0 + damp + 0.6 * damp2);
+        if (rorder >= 9) {
+          double damp3 = damp * damp2;
+          dmpik[9] = 1.0 - expdamp * (1.0 + damp + (18.0 / 35.0) * damp2 + (9.0 / 35.0) * damp3);
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-radix complex FFT (factors 2, 3, 5 and any other prime by direct DFT),
+// unnormalised, used in place of 2DECOMP's generic engine (fft_mpi.f90:65,115).
+using cd = std::complex<double>;
+
+void factorize(int n, std::vector<int>& f) {
+  f.clear();
+  for (int p : {4, 2, 3, 5}) {
+    while (n % p == 0) {
+      f.push_back(p);
+      n /= p;
+    }
+  }
+  for (int p = 7; n > 1; p += 2)
+    while (n % p == 0) {
+      f.push_back(p);
+      n /= p;
+    }
+}
+
+void fft_rec(const cd* in, cd* out, int n, int stride, int sign, const int* fac, const cd* tw,
+             int twn, cd* scratch) {
+  if (n == 1) {
+    out[0] = in[0];
+    return;
+  }
+  int p = fac[0], m = n / p;
+  for (int q = 0; q < p; ++q) fft_rec(in + q * stride, out + q * m, m, stride * p, sign, fac + 1, tw, twn, scratch);
+  // butterfly: X[k + m*s] = sum_q W_n^{q(k+m s)} Y_q[k]
+  int step = twn / n;
+  for (int k = 0; k < m; ++k) {
+    for (int q = 0; q < p; ++q) scratch[q] = out[q * m + k];
+    for (int s = 0; s < p; ++s) {
+      cd acc = 0.0;
+      int idx = k + m * s;
+      for (int q = 0; q < p; ++q) {
+        long e = ((long)q * idx) % n;
+        cd w = tw[e * step];
+        if (sign > 0) w = std::conj(w);
+        acc += w * scratch[q];
+      }
+      out[idx] = acc;
+    }
+  }
+}
+
+struct Fft1d {
+  int n = 0;
+  std::vector<int> fac;
+  std::vector<cd> tw;  // exp(-2 pi i k / n)
+  void init(int n_) {
+    n = n_;
+    factorize(n, fac);
+    fac.push_back(1);
+    tw.resize(n);
+    for (int k = 0; k < n; ++k) tw[k] = cd(std::cos(2.0 * kPi * k / n), -std::sin(2.0 * kPi * k / n));
+  }
+  void run(cd* line, int sign, cd* tmp, cd* scratch) const {
+    std::memcpy(tmp, line, sizeof(cd) * n);
+    fft_rec(tmp, line, n, 1, sign, fac.data(), tw.data(), n, scratch);
+  }
+};
+
+void fft3d_impl(cd* g, int n1, int n2, int n3, int sign, int nthr) {
+  Fft1d f1, f2, f3;
+  f1.init(n1);
+  f2.init(n2);
+  f3.init(n3);
+  int nmax = std::max(n1, std::max(n2, n3));
+  // axis 1 (contiguous)
+#pragma omp parallel num_threads(nthr)
+  {
+    std::vector<cd> line(nmax), tmp(nmax), scr(nmax);
+#pragma omp for schedule(static)
+    for (int l = 0; l < n2 * n3; ++l) f1.run(g + (size_t)l * n1, sign, tmp.data(), scr.data());
+#pragma omp for schedule(static)
+    for (int l = 0; l < n1 * n3; ++l) {
+      int i = l % n1, k = l / n1;
+      for (int j = 0; j < n2; ++j) line[j] = g[((size_t)k * n2 + j) * n1 + i];
+      f2.run(line.data(), sign, tmp.data(), scr.data());
+      for (int j = 0; j < n2; ++j) g[((size_t)k * n2 + j) * n1 + i] = line[j];
+    }
+#pragma omp for schedule(static)
+    for (int l = 0; l < n1 * n2; ++l) {
+      for (int k = 0; k < n3; ++k) line[k] = g[(size_t)k * n1 * n2 + l];
+      f3.run(line.data(), sign, tmp.data(), scr.data());
+      for (int k = 0; k < n3; ++k) g[(size_t)k * n1 * n2 + l] = line[k];
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct OrCtx {
+  OrSystem s;
+  Cell cell;
+  double recip[3][3];  // recip[i][j] == reference recip(i+1,j+1)
+  double volbox;
+  // neighbor list (half, k>i)
+  int maxelst = 0;
+  std::vector<int> nelst, elst;
+  bool have_list = false;
+  // PME state
+  int bsorder = 5, grdoff = 0, nlpts = 0, nrpts = 0;
+  std::vector<double> bsmod1, bsmod2, bsmod3;
+  std::vector<double> qfac;          // [n3][n2][n1]
+  std::vector<double> theta1, theta2, theta3;  // [n][5][4]: (level j, point m) -> [(i*bs + m)*4 + j]
+  std::vector<int> igrid;            // [n][3]
+  std::vector<double> fphirec;       // [n][20]
+  std::vector<cd> grid;              // [n3][n2][n1]
+  bool have_bspline = false;
+};
+
+namespace {
+
+// lattice.f:20-126 for orthogonal boxes
+void setup_box(OrCtx* c) {
+  const OrSystem& s = c->s;
+  c->cell.xcell = s.xbox;
+  c->cell.ycell = s.ybox;
+  c->cell.zcell = s.zbox;
+  c->cell.xcell2 = 0.5 * s.xbox;
+  c->cell.ycell2 = 0.5 * s.ybox;
+  c->cell.zcell2 = 0.5 * s.zbox;
+  double ar1 = s.xbox, ar2 = 0.0, ar3 = 0.0;
+  double br1 = s.ybox * 0.0, br2 = s.ybox * 1.0, br3 = 0.0;
+  double cr1 = s.zbox * 0.0, cr2 = s.zbox * 0.0, cr3 = s.zbox * 1.0;
+  c->volbox = s.xbox * s.ybox * s.zbox;
+  double v = c->volbox;
+  c->recip[0][0] = (br2 * cr3 - cr2 * br3) / v;
+  c->recip[1][0] = (br3 * cr1 - cr3 * br1) / v;
+  c->recip[2][0] = (br1 * cr2 - cr1 * br2) / v;
+  c->recip[0][1] = (cr2 * ar3 - ar2 * cr3) / v;
+  c->recip[1][1] = (cr3 * ar1 - ar3 * cr1) / v;
+  c->recip[2][1] = (cr1 * ar2 - ar1 * cr2) / v;
+  c->recip[0][2] = (ar2 * br3 - br2 * ar3) / v;
+  c->recip[1][2] = (ar3 * br1 - br3 * ar1) / v;
+  c->recip[2][2] = (ar1 * br2 - br1 * ar2) / v;
+}
+
+// kewald.f:693-717 (bspline)
+void bspline_coef(double x, int n, double* cc /*1-based*/) {
+  cc[1] = 1.0 - x;
+  cc[2] = x;
+  for (int k = 3; k <= n; ++k) {
+    double denom = 1.0 / (double)(k - 1);
+    cc[k] = x * cc[k - 1] * denom;
+    for (int i = 1; i <= k - 2; ++i) cc[k - i] = ((x + (double)i) * cc[k - i - 1] + ((double)(k - i) - x) * cc[k - i]) * denom;
+    cc[1] = (1.0 - x) * cc[1] * denom;
+  }
+}
+
+// kewald.f:747-812 (dftmod)
+void dftmod(std::vector<double>& bsmod, const std::vector<double>& bsarray, int nfft, int order) {
+  bsmod.assign(nfft + 1, 0.0);  // 1-based
+  double factor = 2.0 * kPi / (double)nfft;
+  for (int i = 1; i <= nfft; ++i) {
+    double sum1 = 0.0, sum2 = 0.0;
+    for (int j = 1; j <= nfft; ++j) {
+      double arg = factor * (double)((i - 1) * (j - 1));
+      sum1 = sum1 + bsarray[j] * std::cos(arg);
+      sum2 = sum2 + bsarray[j] * std::sin(arg);
+    }
+    bsmod[i] = sum1 * sum1 + sum2 * sum2;
+  }
+  double eps = 1.0e-7;
+  if (bsmod[1] < eps) bsmod[1] = 0.5 * bsmod[2];
+  for (int i = 2; i <= nfft - 1; ++i)
+    if (bsmod[i] < eps) bsmod[i] = 0.5 * (bsmod[i - 1] + bsmod[i + 1]);
+  if (bsmod[nfft] < eps) bsmod[nfft] = 0.5 * bsmod[nfft - 1];
+  int jcut = 50;
+  int order2 = 2 * order;
+  for (int i = 1; i <= nfft; ++i) {
+    int k = i - 1;
+    if (i > nfft / 2) k = k - nfft;
+    double zeta;
+    if (k == 0) {
+      zeta = 1.0;
+    } else {
+      double sum1 = 1.0, sum2 = 1.0;
+      double fac = kPi * (double)k / (double)nfft;
+      for (int j = 1; j <= jcut; ++j) {
+        double arg = fac / (fac + kPi * (double)j);
+        sum1 = sum1 + std::pow(arg, order);
+        sum2 = sum2 + std::pow(arg, order2);
+      }
+      for (int j = 1; j <= jcut; ++j) {
+        double arg = fac / (fac - kPi * (double)j);
+        sum1 = sum1 + std::pow(arg, order);
+        sum2 = sum2 + std::pow(arg, order2);
+      }
+      zeta = sum2 / sum1;
+    }
+    bsmod[i] = bsmod[i] * zeta * zeta;
+  }
+}
+
+// kewald.f:672-690 (moduli) and newinduce_pme.f:1802-1854 (qfac)
+void setup_pme(OrCtx* c) {
+  const OrSystem& s = c->s;
+  c->bsorder = s.bsorder;
+  c->nlpts = (c->bsorder - 1) / 2;
+  c->nrpts = c->bsorder - c->nlpts - 1;
+  c->grdoff = (c->bsorder + 1) / 2 + 1;
+  int maxfft = std::max(s.nfft1, std::max(s.nfft2, s.nfft3));
+  std::vector<double> arr(c->bsorder + 2, 0.0), bsarray(maxfft + 2, 0.0);
+  bspline_coef(0.0, c->bsorder, arr.data());
+  for (int i = 2; i <= c->bsorder + 1; ++i) bsarray[i] = arr[i - 1];
+  dftmod(c->bsmod1, bsarray, s.nfft1, c->bsorder);
+  dftmod(c->bsmod2, bsarray, s.nfft2, c->bsorder);
+  dftmod(c->bsmod3, bsarray, s.nfft3, c->bsorder);
+  size_t ng = (size_t)s.nfft1 * s.nfft2 * s.nfft3;
+  c->qfac.assign(ng, 0.0);
+  c->grid.assign(ng, cd(0.0, 0.0));
+  double pterm = (kPi / s.aewald) * (kPi / s.aewald);
+  double volterm = kPi * c->volbox;
+  int nf1 = (s.nfft1 + 1) / 2, nf2 = (s.nfft2 + 1) / 2, nf3 = (s.nfft3 + 1) / 2;
+  for (int k3 = 1; k3 <= s.nfft3; ++k3)
+    for (int k2 = 1; k2 <= s.nfft2; ++k2)
+      for (int k1 = 1; k1 <= s.nfft1; ++k1) {
+        int m1 = k1 - 1, m2 = k2 - 1, m3 = k3 - 1;
+        if (k1 > nf1) m1 -= s.nfft1;
+        if (k2 > nf2) m2 -= s.nfft2;
+        if (k3 > nf3) m3 -= s.nfft3;
+        size_t idx = ((size_t)(k3 - 1) * s.nfft2 + (k2 - 1)) * s.nfft1 + (k1 - 1);
+        if (m1 == 0 && m2 == 0 && m3 == 0) continue;
+        double r1 = m1, r2 = m2, r3 = m3;
+        double h1 = c->recip[0][0] * r1 + c->recip[0][1] * r2 + c->recip[0][2] * r3;
+        double h2 = c->recip[1][0] * r1 + c->recip[1][1] * r2 + c->recip[1][2] * r3;
+        double h3 = c->recip[2][0] * r1 + c->recip[2][1] * r2 + c->recip[2][2] * r3;
+        double hsq = h1 * h1 + h2 * h2 + h3 * h3;
+        double term = -pterm * hsq;
+        if (term > -50.0) {
+          double denom = volterm * hsq * c->bsmod1[k1] * c->bsmod2[k2] * c->bsmod3[k3];
+          c->qfac[idx] = std::exp(term) / denom;
+        }
+      }
+}
+
+// pmestuff.f:64-157 (bsplgen), level 4 (use_polar)
+void bsplgen(double w, int bsorder, double* thetai /*[bsorder][4]*/) {
+  const int level = 4;
+  double temp[12][12];  // 1-based (maxorder <= 10)
+  temp[2][2] = w;
+  temp[2][1] = 1.0 - w;
+  temp[3][3] = 0.5 * w * temp[2][2];
+  temp[3][2] = 0.5 * ((1.0 + w) * temp[2][1] + (2.0 - w) * temp[2][2]);
+  temp[3][1] = 0.5 * (1.0 - w) * temp[2][1];
+  for (int i = 4; i <= bsorder; ++i) {
+    int k = i - 1;
+    double denom = 1.0 / (double)k;
+    temp[i][i] = denom * w * temp[k][k];
+    for (int j = 1; j <= i - 2; ++j)
+      temp[i][i - j] = denom * ((w + (double)j) * temp[k][i - j - 1] + ((double)(i - j) - w) * temp[k][i - j]);
+    temp[i][1] = denom * (1.0 - w) * temp[k][1];
+  }
+  int k = bsorder - 1;
+  temp[k][bsorder] = temp[k][bsorder - 1];
+  for (int i = bsorder - 1; i >= 2; --i) temp[k][i] = temp[k][i - 1] - temp[k][i];
+  temp[k][1] = -temp[k][1];
+  // second derivative
+  k = bsorder - 2;
+  temp[k][bsorder - 1] = temp[k][bsorder - 2];
+  for (int i = bsorder - 2; i >= 2; --i) temp[k][i] = temp[k][i - 1] - temp[k][i];
+  temp[k][1] = -temp[k][1];
+  temp[k][bsorder] = temp[k][bsorder - 1];
+  for (int i = bsorder - 1; i >= 2; --i) temp[k][i] = temp[k][i - 1] - temp[k][i];
+  temp[k][1] = -temp[k][1];
+  // third derivative
+  k = bsorder - 3;
+  temp[k][bsorder - 2] = temp[k][bsorder - 3];
+  for (int i = bsorder - 3; i >= 2; --i) temp[k][i] = temp[k][i - 1] - temp[k][i];
+  temp[k][1] = -temp[k][1];
+  temp[k][bsorder - 1] = temp[k][bsorder - 2];
+  for (int i = bsorder - 2; i >= 2; --i) temp[k][i] = temp[k][i - 1] - temp[k][i];
+  temp[k][1] = -temp[k][1];
+  temp[k][bsorder] = temp[k][bsorder - 1];
+  for (int i = bsorder - 1; i >= 2; --i) temp[k][i] = temp[k][i - 1] - temp[k][i];
+  temp[k][1] = -temp[k][1];
+  for (int i = 1; i <= bsorder; ++i)
+    for (int j = 1; j <= level; ++j) thetai[(i - 1) * 4 + (j - 1)] = temp[bsorder - j + 1][i];
+}
+
+// pmestuff.f:13-51 (bspline_fill_site) for every site
+void bspline_fill(OrCtx* c) {
+  const OrSystem& s = c->s;
+  int n = s.n, bs = c->bsorder;
+  c->theta1.resize((size_t)n * bs * 4);
+  c->theta2.resize((size_t)n * bs * 4);
+  c->theta3.resize((size_t)n * bs * 4);
+  c->igrid.resize((size_t)n * 3);
+  const double eps = 1.0e-8;
+  int nf[3] = {s.nfft1, s.nfft2, s.nfft3};
+  double* th[3] = {c->theta1.data(), c->theta2.data(), c->theta3.data()};
+  for (int i = 0; i < n; ++i) {
+    double xi = s.x[i], yi = s.y[i], zi = s.z[i];
+    for (int d = 0; d < 3; ++d) {
+      double w = xi * c->recip[0][d] + yi * c->recip[1][d] + zi * c->recip[2][d];
+      double fr = (double)nf[d] * (w - std::round(w) + 0.5);
+      int ifr = (int)(fr - eps);
+      w = fr - (double)ifr;
+      c->igrid[i * 3 + d] = ifr - bs;
+      bsplgen(w, bs, th[d] + (size_t)i * bs * 4);
+    }
+  }
+  c->have_bspline = true;
+}
+
+inline int wrap0(int v, int n) { return v < 0 ? v + n : v; }
+
+// 0-based grid index of stencil point t (0..bsorder-1) along one axis
+// (grid_*_site with adjust: kk = igrid+grdoff-nlpts+t, 1-based, wrapped once)
+inline int stencil_index(const OrCtx* c, int ig, int t, int nfft) {
+  int kk = ig + c->grdoff - c->nlpts + t;  // 1-based
+  if (kk < 1) kk += nfft;
+  return kk - 1;
+}
+
+// cart_to_frac (pmestuff.f:1131-1185)
+void cart_to_frac(const OrCtx* c, double ctf[10][10]) {
+  const OrSystem& s = c->s;
+  double a[3][3];
+  int nf[3] = {s.nfft1, s.nfft2, s.nfft3};
+  for (int i = 0; i < 3; ++i)
+    for (int d = 0; d < 3; ++d) a[d][i] = (double)nf[d] * c->recip[i][d];
+  for (int i = 0; i < 10; ++i)
+    for (int j = 0; j < 10; ++j) ctf[j][i] = 0.0;
+  ctf[0][0] = 1.0;
+  for (int i = 1; i < 4; ++i)
+    for (int j = 1; j < 4; ++j) ctf[i][j] = a[i - 1][j - 1];
+  const int qi1[6] = {0, 1, 2, 0, 0, 1}, qi2[6] = {0, 1, 2, 1, 2, 2};
+  for (int i1 = 0; i1 < 3; ++i1) {
+    int k = qi1[i1];
+    for (int i2 = 0; i2 < 6; ++i2) {
+      int i = qi1[i2], j = qi2[i2];
+      ctf[i1 + 4][i2 + 4] = a[k][i] * a[k][j];
+    }
+  }
+  for (int i1 = 3; i1 < 6; ++i1) {
+    int k = qi1[i1], m = qi2[i1];
+    for (int i2 = 0; i2 < 6; ++i2) {
+      int i = qi1[i2], j = qi2[i2];
+      ctf[i1 + 4][i2 + 4] = a[k][i] * a[m][j] + a[k][j] * a[m][i];
+    }
+  }
+}
+
+// frac_to_cart (pmestuff.f:1237-1290)
+void frac_to_cart(const OrCtx* c, double ftc[10][10]) {
+  const OrSystem& s = c->s;
+  double a[3][3];
+  int nf[3] = {s.nfft1, s.nfft2, s.nfft3};
+  for (int i = 0; i < 3; ++i)
+    for (int d = 0; d < 3; ++d) a[i][d] = (double)nf[d] * c->recip[i][d];
+  for (int i = 0; i < 10; ++i)
+    for (int j = 0; j < 10; ++j) ftc[j][i] = 0.0;
+  ftc[0][0] = 1.0;
+  for (int i = 1; i < 4; ++i)
+    for (int j = 1; j < 4; ++j) ftc[i][j] = a[i - 1][j - 1];
+  const int qi1[6] = {0, 1, 2, 0, 0, 1}, qi2[6] = {0, 1, 2, 1, 2, 2};
+  for (int i1 = 0; i1 < 3; ++i1) {
+    int k = qi1[i1];
+    for (int i2 = 0; i2 < 3; ++i2) {
+      int i = qi1[i2];
+      ftc[i1 + 4][i2 + 4] = a[k][i] * a[k][i];
+    }
+    for (int i2 = 3; i2 < 6; ++i2) {
+      int i = qi1[i2], j = qi2[i2];
+      ftc[i1 + 4][i2 + 4] = 2.0 * a[k][i] * a[k][j];
+    }
+  }
+  for (int i1 = 3; i1 < 6; ++i1) {
+    int k = qi1[i1], m = qi2[i1];
+    for (int i2 = 0; i2 < 3; ++i2) {
+      int i = qi1[i2];
+      ftc[i1 + 4][i2 + 4] = a[k][i] * a[m][i];
+    }
+    for (int i2 = 3; i2 < 6; ++i2) {
+      int i = qi1[i2], j = qi2[i2];
+      ftc[i1 + 4][i2 + 4] = a[k][i] * a[m][j] + a[m][i] * a[k][j];
+    }
+  }
+}
+
+// Grid spread, parallel over z-plane slabs so that every grid point is
+// written by one thread (the same sums as the reference's serial loop,
+// accumulated per point in atom order).
+template <class F>
+void spread_sites(OrCtx* c, F&& site_terms) {
+  const OrSystem& s = c->s;
+  int n = s.n, bs = c->bsorder;
+  int n1 = s.nfft1, n2 = s.nfft2, n3 = s.nfft3;
+  std::fill(c->grid.begin(), c->grid.end(), cd(0.0, 0.0));
+  int nthr = nthreads_of(&s);
+#pragma omp parallel num_threads(nthr)
+  {
+    int tid = 0, nt = 1;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+    nt = omp_get_num_threads();
+#endif
+    int z0 = (int)((long)n3 * tid / nt), z1 = (int)((long)n3 * (tid + 1) / nt);
+    for (int i = 0; i < n; ++i) {
+      const double* t1 = &c->theta1[(size_t)i * bs * 4];
+      const double* t2 = &c->theta2[(size_t)i * bs * 4];
+      const double* t3 = &c->theta3[(size_t)i * bs * 4];
+      const int* ig = &c->igrid[i * 3];
+      for (int it3 = 0; it3 < bs; ++it3) {
+        int k = stencil_index(c, ig[2], it3, n3);
+        if (k < z0 || k >= z1) continue;
+        for (int it2 = 0; it2 < bs; ++it2) {
+          int j = stencil_index(c, ig[1], it2, n2);
+          for (int it1 = 0; it1 < bs; ++it1) {
+            int ii = stencil_index(c, ig[0], it1, n1);
+            cd add = site_terms(i, t1 + it1 * 4, t2 + it2 * 4, t3 + it3 * 4);
+            c->grid[((size_t)k * n2 + j) * n1 + ii] += add;
+          }
+        }
+      }
+    }
+  }
+}
+
+void convolve(OrCtx* c) {
+  const OrSystem& s = c->s;
+  int nthr = nthreads_of(&s);
+  fft3d_impl(c->grid.data(), s.nfft1, s.nfft2, s.nfft3, -1, nthr);
+  size_t ng = c->grid.size();
+#pragma omp parallel for num_threads(nthr) schedule(static)
+  for (long q = 0; q < (long)ng; ++q) c->grid[q] *= c->qfac[q];
+  fft3d_impl(c->grid.data(), s.nfft1, s.nfft2, s.nfft3, +1, nthr);
+}
+
+// grid value at stencil point, 0-based index per fphi_*_site:
+// i0 = igrid + it (it=1..bs), i = i0 mod nfft
+inline int gather_index(int ig, int it1based, int nfft) {
+  int i0 = ig + it1based;
+  return i0 >= 0 ? i0 : i0 + nfft;
+}
+
+// fphi_mpole_site (pmestuff.f:453-600): 20 potential derivatives per site
+void fphi_mpole(OrCtx* c) {
+  const OrSystem& s = c->s;
+  int n = s.n, bs = c->bsorder;
+  c->fphirec.assign((size_t)n * 20, 0.0);
+  int nthr = nthreads_of(&s);
+#pragma omp parallel for num_threads(nthr) schedule(static)
+  for (int i = 0; i < n; ++i) {
+    const double* th1 = &c->theta1[(size_t)i * bs * 4];
+    const double* th2 = &c->theta2[(size_t)i * bs * 4];
+    const double* th3 = &c->theta3[(size_t)i * bs * 4];
+    const int* ig = &c->igrid[i * 3];
+    double tuv000 = 0, tuv100 = 0, tuv010 = 0, tuv001 = 0, tuv200 = 0, tuv020 = 0, tuv002 = 0, tuv110 = 0,
+           tuv101 = 0, tuv011 = 0, tuv300 = 0, tuv030 = 0, tuv003 = 0, tuv210 = 0, tuv201 = 0, tuv120 = 0,
+           tuv021 = 0, tuv102 = 0, tuv012 = 0, tuv111 = 0;
+    for (int it3 = 1; it3 <= bs; ++it3) {
+      int k = gather_index(ig[2], it3, s.nfft3);
+      double v0 = th3[(it3 - 1) * 4 + 0], v1 = th3[(it3 - 1) * 4 + 1], v2 = th3[(it3 - 1) * 4 + 2],
+             v3 = th3[(it3 - 1) * 4 + 3];
+      double tu00 = 0, tu10 = 0, tu01 = 0, tu20 = 0, tu11 = 0, tu02 = 0, tu30 = 0, tu21 = 0, tu12 = 0, tu03 = 0;
+      for (int it2 = 1; it2 <= bs; ++it2) {
+        int j = gather_index(ig[1], it2, s.nfft2);
+        double u0 = th2[(it2 - 1) * 4 + 0], u1 = th2[(it2 - 1) * 4 + 1], u2 = th2[(it2 - 1) * 4 + 2],
+               u3 = th2[(it2 - 1) * 4 + 3];
+        double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+        for (int it1 = 1; it1 <= bs; ++it1) {
+          int ii = gather_index(ig[0], it1, s.nfft1);
+          double tq = c->grid[((size_t)k * s.nfft2 + j) * s.nfft1 + ii].real();
+          t0 = t0 + tq * th1[(it1 - 1) * 4 + 0];
+          t1 = t1 + tq * th1[(it1 - 1) * 4 + 1];
+          t2 = t2 + tq * th1[(it1 - 1) * 4 + 2];
+          t3 = t3 + tq * th1[(it1 - 1) * 4 + 3];
+        }
+        tu00 = tu00 + t0 * u0;
+        tu10 = tu10 + t1 * u0;
+        tu01 = tu01 + t0 * u1;
+        tu20 = tu20 + t2 * u0;
+        tu11 = tu11 + t1 * u1;
+        tu02 = tu02 + t0 * u2;
+        tu30 = tu30 + t3 * u0;
+        tu21 = tu21 + t2 * u1;
+        tu12 = tu12 + t1 * u2;
+        tu03 = tu03 + t0 * u3;
+      }
+      tuv000 = tuv000 + tu00 * v0;
+      tuv100 = tuv100 + tu10 * v0;
+      tuv010 = tuv010 + tu01 * v0;
+      tuv001 = tuv001 + tu00 * v1;
+      tuv200 = tuv200 + tu20 * v0;
+      tuv020 = tuv020 + tu02 * v0;
+      tuv002 = tuv002 + tu00 * v2;
+      tuv110 = tuv110 + tu11 * v0;
+      tuv101 = tuv101 + tu10 * v1;
+      tuv011 = tuv011 + tu01 * v1;
+      tuv300 = tuv300 + tu30 * v0;
+      tuv030 = tuv030 + tu03 * v0;
+      tuv003 = tuv003 + tu00 * v3;
+      tuv210 = tuv210 + tu21 * v0;
+      tuv201 = tuv201 + tu20 * v1;
+      tuv120 = tuv120 + tu12 * v0;
+      tuv021 = tuv021 + tu02 * v1;
+      tuv102 = tuv102 + tu10 * v2;
+      tuv012 = tuv012 + tu01 * v2;
+      tuv111 = tuv111 + tu11 * v1;
+    }
+    double* f = &c->fphirec[(size_t)i * 20];
+    f[0] = tuv000; f[1] = tuv100; f[2] = tuv010; f[3] = tuv001; f[4] = tuv200;
+    f[5] = tuv020; f[6] = tuv002; f[7] = tuv110; f[8] = tuv101; f[9] = tuv011;
+    f[10] = tuv300; f[11] = tuv030; f[12] = tuv003; f[13] = tuv210; f[14] = tuv201;
+    f[15] = tuv120; f[16] = tuv021; f[17] = tuv102; f[18] = tuv012; f[19] = tuv111;
+  }
+}
+
+// scale-factor workspace, reset after each i exactly as the reference does
+struct ScaleWs {
+  std::vector<double> d, p, u;
+  void init(int n) {
+    d.assign(n, 1.0);
+    p.assign(n, 1.0);
+    u.assign(n, 1.0);
+  }
+};
+
+inline bool in_list(const OrSystem& s, int slot, int i, int k) {
+  if (!s.conn_off[slot]) return false;
+  for (int q = s.conn_off[slot][i]; q < s.conn_off[slot][i + 1]; ++q)
+    if (s.conn_idx[slot][q] == k) return true;
+  return false;
+}
+
+template <class F>
+inline void for_conn(const OrSystem& s, int slot, int i, F&& f) {
+  if (!s.conn_off[slot]) return;
+  for (int q = s.conn_off[slot][i]; q < s.conn_off[slot][i + 1]; ++q) f(s.conn_idx[slot][q]);
+}
+
+// newinduce_pme.f:1062-1136 (dpequal false branch)
+void set_dp_scales(const OrSystem& s, int i, ScaleWs& w) {
+  const int islot[4] = {OR_I12, OR_I13, OR_I14, OR_I15};
+  for (int b = 0; b < 4; ++b)
+    for_conn(s, islot[b], i, [&](int k) {
+      w.p[k] = s.p_scale[b];
+      if (in_list(s, OR_IP11, i, k)) w.p[k] = s.pi_scale[b];
+    });
+  const int pslot[4] = {OR_IP11, OR_IP12, OR_IP13, OR_IP14};
+  for (int b = 0; b < 4; ++b) for_conn(s, pslot[b], i, [&](int k) { w.d[k] = s.d_scale[b]; });
+}
+void reset_dp_scales(const OrSystem& s, int i, ScaleWs& w) {
+  const int islot[4] = {OR_I12, OR_I13, OR_I14, OR_I15};
+  for (int b = 0; b < 4; ++b) for_conn(s, islot[b], i, [&](int k) { w.p[k] = 1.0; });
+  const int pslot[4] = {OR_IP11, OR_IP12, OR_IP13, OR_IP14};
+  for (int b = 0; b < 4; ++b) for_conn(s, pslot[b], i, [&](int k) { w.d[k] = 1.0; });
+}
+// newinduce_pme.f:1495-1518 (uscale part)
+void set_u_scales(const OrSystem& s, int i, ScaleWs& w, bool reset) {
+  const int pslot[4] = {OR_IP11, OR_IP12, OR_IP13, OR_IP14};
+  for (int b = 0; b < 4; ++b) for_conn(s, pslot[b], i, [&](int k) { w.u[k] = reset ? 1.0 : s.u_scale[b]; });
+}
+// epolar.f:300-330 (pscale only)
+void set_p_scales(const OrSystem& s, int i, ScaleWs& w, bool reset) {
+  const int islot[4] = {OR_I12, OR_I13, OR_I14, OR_I15};
+  for (int b = 0; b < 4; ++b)
+    for_conn(s, islot[b], i, [&](int k) {
+      if (reset) {
+        w.p[k] = 1.0;
+      } else {
+        w.p[k] = s.p_scale[b];
+        if (in_list(s, OR_IP11, i, k)) w.p[k] = s.pi_scale[b];
+      }
+    });
+}
+
+// Per-thread accumulation for Newton's-3rd-law pair loops over the half list.
+template <class F>
+void pair_loop(OrCtx* c, int ncomp, double* out, F&& body) {
+  const OrSystem& s = c->s;
+  int n = s.n, nthr = nthreads_of(&s);
+  std::vector<std::vector<double>> acc(nthr);
+#pragma omp parallel num_threads(nthr)
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    acc[tid].assign((size_t)n * ncomp, 0.0);
+    ScaleWs w;
+    w.init(n);
+#pragma omp for schedule(dynamic, 64)
+    for (int i = 0; i < n; ++i) body(i, w, acc[tid].data());
+  }
+  for (int t = 0; t < nthr; ++t)
+    for (size_t q = 0; q < (size_t)n * ncomp; ++q) out[q] += acc[t][q];
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+double or_erfc(double x) { return erfc_cody(x); }
+
+// kewald.f:575-620 (ewaldcof)
+double or_ewaldcof(double cutoff) {
+  double eps = 1.0e-8;
+  double ratio = eps + 1.0, x = 0.5;
+  int i = 0;
+  while (ratio >= eps) {
+    i++;
+    x = 2.0 * x;
+    ratio = erfc_cody(x * cutoff) / cutoff;
+  }
+  int k = i + 60;
+  double xlo = 0.0, xhi = x;
+  for (int it = 1; it <= k; ++it) {
+    x = (xlo + xhi) / 2.0;
+    ratio = erfc_cody(x * cutoff) / cutoff;
+    if (ratio >= eps)
+      xlo = x;
+    else
+      xhi = x;
+  }
+  return x;
+}
+
+void or_fft3d(double* data, int n1, int n2, int n3, int sign) {
+  fft3d_impl(reinterpret_cast<cd*>(data), n1, n2, n3, sign, 1);
+}
+
+OrCtx* or_create(const OrSystem* sys) {
+  OrCtx* c = new OrCtx();
+  c->s = *sys;
+  setup_box(c);
+  setup_pme(c);
+  return c;
+}
+
+void or_destroy(OrCtx* c) { delete c; }
+
+// nblist.f:117-247 (mlistcell) with build_cell_list (nblist.f:607-866) at nproc=1
+int or_mlistcell(OrCtx* c, int maxelst, int* nelst, int* elst) {
+  const OrSystem& s = c->s;
+  int n = s.n;
+  double mbuf2 = (s.ewaldcut + s.lbuffer) * (s.ewaldcut + s.lbuffer);
+  double vbuf2 = (s.vdwcut + s.lbuffer) * (s.vdwcut + s.lbuffer);
+  double boxedge2 = std::min(c->cell.xcell2, std::min(c->cell.ycell2, c->cell.zcell2));
+  if (mbuf2 > boxedge2 * boxedge2) return OR_E_BOX_TOO_SMALL;
+  // build_cell_list
+  double eps1 = 1.0e-10, eps2 = 1.0e-8;
+  double mbuf = std::sqrt(mbuf2);
+  double vbuf = std::sqrt(vbuf2) + 2.0;
+  double bigbuf = ((mbuf + s.lbuffer) > vbuf) ? (mbuf + s.lbuffer) / 3 : vbuf / 3;
+  double xmin = -c->cell.xcell2, xmax = c->cell.xcell2;
+  double ymin = -c->cell.ycell2, ymax = c->cell.ycell2;
+  double zmin = -c->cell.zcell2, zmax = c->cell.zcell2;
+  double lenx = std::fabs(xmax - xmin), leny = std::fabs(ymax - ymin), lenz = std::fabs(zmax - zmin);
+  int nx = std::max(1, (int)(lenx / bigbuf)), ny = std::max(1, (int)(leny / bigbuf)),
+      nz = std::max(1, (int)(lenz / bigbuf));
+  double lxc = lenx / nx, lyc = leny / ny, lzc = lenz / nz;
+  std::vector<double> xb(nx), xe(nx), yb(ny), ye(ny), zb(nz), ze(nz);
+  for (int i = 0; i < nx; ++i) { xb[i] = xmin + i * lxc; xe[i] = xmin + (i + 1) * lxc; }
+  for (int i = 0; i < ny; ++i) { yb[i] = ymin + i * lyc; ye[i] = ymin + (i + 1) * lyc; }
+  for (int i = 0; i < nz; ++i) { zb[i] = zmin + i * lzc; ze[i] = zmin + (i + 1) * lzc; }
+  int ncell = nx * ny * nz;
+  // neighbor cells: p (x) outer, q (y), r (z) inner, first occurrence kept
+  std::vector<std::vector<int>> neig(ncell);
+  std::vector<int> filled(ncell);
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        int icell = (k * ny + j) * nx + i;
+        std::fill(filled.begin(), filled.end(), 0);
+        filled[icell] = 1;
+        for (int p = -3; p <= 3; ++p)
+          for (int q = -3; q <= 3; ++q)
+            for (int r = -3; r <= 3; ++r) {
+              if (p == 0 && q == 0 && r == 0) continue;
+              int tx = ((i + p) % nx + nx) % nx, ty = ((j + q) % ny + ny) % ny, tz = ((k + r) % nz + nz) % nz;
+              int t = (tz * ny + ty) * nx + tx;
+              if (filled[t]) continue;
+              filled[t] = 1;
+              neig[icell].push_back(t);
+            }
+      }
+  auto find_cell = [](double v, const std::vector<double>& b, const std::vector<double>& e) {
+    int nc = (int)b.size();
+    for (int q = 0; q < nc; ++q)
+      if (v >= b[q] && v < e[q]) return q;
+    return -1;
+  };
+  std::vector<int> repart(n), cell_len(ncell, 0);
+  std::vector<std::vector<int>> cell_atoms(ncell);
+  for (int i = 0; i < n; ++i) {
+    double xr = s.x[i], yr = s.y[i], zr = s.z[i];
+    image(c->cell, xr, yr, zr);
+    if (std::fabs(xr - xmax) < eps1) xr = xr - eps2;
+    if (std::fabs(yr - ymax) < eps1) yr = yr - eps2;
+    if (std::fabs(zr - zmax) < eps1) zr = zr - eps2;
+    int ci = find_cell(xr, xb, xe), cj = find_cell(yr, yb, ye), ck = find_cell(zr, zb, ze);
+    if (ci < 0 || cj < 0 || ck < 0) return OR_E_BOX_TOO_SMALL;  // not reachable for imaged inputs
+    int icell = (ck * ny + cj) * nx + ci;
+    repart[i] = icell;
+    cell_atoms[icell].push_back(i);
+  }
+  // mlistcell
+  int status = OR_OK;
+  for (int i = 0; i < n; ++i) {
+    int icell = repart[i];
+    double xi = s.x[i], yi = s.y[i], zi = s.z[i];
+    int j = 0;
+    auto visit = [&](int k) {
+      if (k <= i) return;
+      double px = xi - s.x[k], py = yi - s.y[k], pz = zi - s.z[k];
+      image(c->cell, px, py, pz);  // midpointimage (domdecstuff.f:1773) always accepts at nproc=1
+      double r2 = px * px + py * py + pz * pz;
+      if (r2 <= mbuf2) {
+        if (j < maxelst) elst[(size_t)i * maxelst + j] = k;
+        j++;
+      }
+    };
+    for (int k : cell_atoms[icell]) visit(k);
+    for (int kc : neig[icell])
+      for (int k : cell_atoms[kc]) visit(k);
+    nelst[i] = std::min(j, maxelst);
+    if (j >= maxelst) status = OR_E_LIST_OVERFLOW;
+  }
+  c->maxelst = maxelst;
+  c->nelst.assign(nelst, nelst + n);
+  c->elst.assign(elst, elst + (size_t)n * maxelst);
+  c->have_list = (status == OR_OK);
+  return status;
+}
+
+// newinduce_pme.f:948-1389 (efld0_direct), Thole branch
+void or_efld0_direct(OrCtx* c, double* ef) {
+  const OrSystem& s = c->s;
+  const double cutoff2 = s.ewaldcut * s.ewaldcut;
+  const int maxelst = c->maxelst;
+  pair_loop(c, 6, ef, [&](int i, ScaleWs& w, double* acc) {
+    const double* ri = &s.rpole[(size_t)i * 13];
+    double ci = ri[0], dix = ri[1], diy = ri[2], diz = ri[3];
+    double qixx = ri[4], qixy = ri[5], qixz = ri[6], qiyy = ri[8], qiyz = ri[9], qizz = ri[12];
+    set_dp_scales(s, i, w);
+    for (int kkk = 0; kkk < c->nelst[i]; ++kkk) {
+      int k = c->elst[(size_t)i * maxelst + kkk];
+      double xr = s.x[k] - s.x[i], yr = s.y[k] - s.y[i], zr = s.z[k] - s.z[i];
+      image(c->cell, xr, yr, zr);
+      double r2 = xr * xr + yr * yr + zr * zr;
+      if (r2 > cutoff2) continue;
+      double r = std::sqrt(r2);
+      double rr1 = 1.0 / r, rr2 = rr1 * rr1, rr3 = rr2 * rr1;
+      double rr5 = 3.0 * rr2 * rr3, rr7 = 5.0 * rr2 * rr5;
+      const double* rk = &s.rpole[(size_t)k * 13];
+      double ck = rk[0], dkx = rk[1], dky = rk[2], dkz = rk[3];
+      double qkxx = rk[4], qkxy = rk[5], qkxz = rk[6], qkyy = rk[8], qkyz = rk[9], qkzz = rk[12];
+      double dir = dix * xr + diy * yr + diz * zr;
+      double qix = qixx * xr + qixy * yr + qixz * zr;
+      double qiy = qixy * xr + qiyy * yr + qiyz * zr;
+      double qiz = qixz * xr + qiyz * yr + qizz * zr;
+      double qir = qix * xr + qiy * yr + qiz * zr;
+      double dkr = dkx * xr + dky * yr + dkz * zr;
+      double qkx = qkxx * xr + qkxy * yr + qkxz * zr;
+      double qky = qkxy * xr + qkyy * yr + qkyz * zr;
+      double qkz = qkxz * xr + qkyz * yr + qkzz * zr;
+      double qkr = qkx * xr + qky * yr + qkz * zr;
+      double dmpe[8], dmpik[8];
+      dampewald(7, r, r2, 1.0, s.aewald, dmpe);
+      dampthole(s.pdamp[i], s.pdamp[k], s.thole[i], s.thole[k], 7, r, dmpik);
+      double fid[3], fkd[3], fip[3], fkp[3];
+      double scalek = w.d[k];
+      double dmp3 = dmpe[3] - (1.0 - scalek * dmpik[3]) * rr3;
+      double dmp5 = dmpe[5] - (1.0 - scalek * dmpik[5]) * rr5;
+      double dmp7 = dmpe[7] - (1.0 - scalek * dmpik[7]) * rr7;
+      fid[0] = -xr * (dmp3 * ck - dmp5 * dkr + dmp7 * qkr) - dmp3 * dkx + 2.0 * dmp5 * qkx;
+      fid[1] = -yr * (dmp3 * ck - dmp5 * dkr + dmp7 * qkr) - dmp3 * dky + 2.0 * dmp5 * qky;
+      fid[2] = -zr * (dmp3 * ck - dmp5 * dkr + dmp7 * qkr) - dmp3 * dkz + 2.0 * dmp5 * qkz;
+      fkd[0] = xr * (dmp3 * ci + dmp5 * dir + dmp7 * qir) - dmp3 * dix - 2.0 * dmp5 * qix;
+      fkd[1] = yr * (dmp3 * ci + dmp5 * dir + dmp7 * qir) - dmp3 * diy - 2.0 * dmp5 * qiy;
+      fkd[2] = zr * (dmp3 * ci + dmp5 * dir + dmp7 * qir) - dmp3 * diz - 2.0 * dmp5 * qiz;
+      scalek = w.p[k];
+      dmp3 = dmpe[3] - (1.0 - scalek * dmpik[3]) * rr3;
+      dmp5 = dmpe[5] - (1.0 - scalek * dmpik[5]) * rr5;
+      dmp7 = dmpe[7] - (1.0 - scalek * dmpik[7]) * rr7;
+      fip[0] = -xr * (dmp3 * ck - dmp5 * dkr + dmp7 * qkr) - dmp3 * dkx + 2.0 * dmp5 * qkx;
+      fip[1] = -yr * (dmp3 * ck - dmp5 * dkr + dmp7 * qkr) - dmp3 * dky + 2.0 * dmp5 * qky;
+      fip[2] = -zr * (dmp3 * ck - dmp5 * dkr + dmp7 * qkr) - dmp3 * dkz + 2.0 * dmp5 * qkz;
+      fkp[0] = xr * (dmp3 * ci + dmp5 * dir + dmp7 * qir) - dmp3 * dix - 2.0 * dmp5 * qix;
+      fkp[1] = yr * (dmp3 * ci + dmp5 * dir + dmp7 * qir) - dmp3 * diy - 2.0 * dmp5 * qiy;
+      fkp[2] = zr * (dmp3 * ci + dmp5 * dir + dmp7 * qir) - dmp3 * diz - 2.0 * dmp5 * qiz;
+      for (int j = 0; j < 3; ++j) {
+        acc[(size_t)i * 6 + j] += fid[j];
+        acc[(size_t)k * 6 + j] += fkd[j];
+        acc[(size_t)i * 6 + 3 + j] += fip[j];
+        acc[(size_t)k * 6 + 3 + j] += fkp[j];
+      }
+    }
+    reset_dp_scales(s, i, w);
+  });
+}
+
+// newinduce_pme.f:1392-1668 (tmatxb_pme), Thole branch
+void or_tmatxb_pme(OrCtx* c, int nrhs, int dodiag, const double* mu, double* efi) {
+  const OrSystem& s = c->s;
+  const int n = s.n, maxelst = c->maxelst;
+  const double off2 = s.ewaldcut * s.ewaldcut;
+  std::fill(efi, efi + (size_t)n * 3 * nrhs, 0.0);
+  pair_loop(c, 3 * nrhs, efi, [&](int i, ScaleWs& w, double* acc) {
+    set_u_scales(s, i, w, false);
+    for (int kkk = 0; kkk < c->nelst[i]; ++kkk) {
+      int k = c->elst[(size_t)i * maxelst + kkk];
+      double xr = s.x[k] - s.x[i], yr = s.y[k] - s.y[i], zr = s.z[k] - s.z[i];
+      image(c->cell, xr, yr, zr);
+      double r2 = xr * xr + yr * yr + zr * zr;
+      if (r2 > off2) continue;
+      double r = std::sqrt(r2);
+      double rr1 = 1.0 / r, rr2 = rr1 * rr1, rr3 = rr2 * rr1, rr5 = 3.0 * rr2 * rr3;
+      double dmpe[8], dmpik[8];
+      dampewald(7, r, r2, 1.0, s.aewald, dmpe);
+      dampthole(s.pdamp[i], s.pdamp[k], s.thole[i], s.thole[k], 5, r, dmpik);
+      double scalek = w.u[k];
+      double dmp3 = dmpe[3] - (1.0 - scalek * dmpik[3]) * rr3;
+      double dmp5 = dmpe[5] - (1.0 - scalek * dmpik[5]) * rr5;
+      double d1 = -dmp3 + dmp5 * xr * xr, d2 = dmp5 * xr * yr, d3 = dmp5 * xr * zr;
+      double d4 = -dmp3 + dmp5 * yr * yr, d5 = dmp5 * yr * zr, d6 = -dmp3 + dmp5 * zr * zr;
+      for (int rh = 0; rh < nrhs; ++rh) {
+        const double* uk = &mu[((size_t)k * nrhs + rh) * 3];
+        const double* ui = &mu[((size_t)i * nrhs + rh) * 3];
+        double fi0 = d1 * uk[0] + d2 * uk[1] + d3 * uk[2];
+        double fi1 = d2 * uk[0] + d4 * uk[1] + d5 * uk[2];
+        double fi2 = d3 * uk[0] + d5 * uk[1] + d6 * uk[2];
+        double fk0 = d1 * ui[0] + d2 * ui[1] + d3 * ui[2];
+        double fk1 = d2 * ui[0] + d4 * ui[1] + d5 * ui[2];
+        double fk2 = d3 * ui[0] + d5 * ui[1] + d6 * ui[2];
+        double* ai = &acc[((size_t)i * nrhs + rh) * 3];
+        double* ak = &acc[((size_t)k * nrhs + rh) * 3];
+        ai[0] -= fi0; ai[1] -= fi1; ai[2] -= fi2;
+        ak[0] -= fk0; ak[1] -= fk1; ak[2] -= fk2;
+      }
+    }
+    set_u_scales(s, i, w, true);
+  });
+  if (dodiag) {
+    for (int i = 0; i < n; ++i) {
+      double pol = (s.polarity[i] == 0.0) ? 1.0 / kTinyPol : 1.0 / s.polarity[i];
+      for (int rh = 0; rh < nrhs; ++rh)
+        for (int j = 0; j < 3; ++j) efi[((size_t)i * nrhs + rh) * 3 + j] += mu[((size_t)i * nrhs + rh) * 3 + j] * pol;
+    }
+  }
+}
+
+// newinduce_pme.f:1671-1917 (efld0_recip)
+void or_efld0_recip(OrCtx* c, double* cphi) {
+  const OrSystem& s = c->s;
+  int n = s.n;
+  bspline_fill(c);
+  double ctf[10][10], ftc[10][10];
+  cart_to_frac(c, ctf);
+  frac_to_cart(c, ftc);
+  std::vector<double> fmp((size_t)n * 10);
+  for (int i = 0; i < n; ++i) {
+    const double* rp = &s.rpole[(size_t)i * 13];
+    double cmp[10] = {rp[0], rp[1], rp[2], rp[3], rp[4], rp[8], rp[12], 2.0 * rp[5], 2.0 * rp[6], 2.0 * rp[9]};
+    double* f = &fmp[(size_t)i * 10];
+    f[0] = ctf[0][0] * cmp[0];
+    for (int j = 1; j < 4; ++j) {
+      f[j] = 0.0;
+      for (int k = 1; k < 4; ++k) f[j] = f[j] + ctf[j][k] * cmp[k];
+    }
+    for (int j = 4; j < 10; ++j) {
+      f[j] = 0.0;
+      for (int k = 4; k < 10; ++k) f[j] = f[j] + ctf[j][k] * cmp[k];
+    }
+  }
+  // grid_mpole_site (pmestuff.f:163-278)
+  spread_sites(c, [&](int i, const double* t, const double* u, const double* v) {
+    const double* f = &fmp[(size_t)i * 10];
+    double term0 = f[0] * u[0] * v[0] + f[2] * u[1] * v[0] + f[3] * u[0] * v[1] + f[5] * u[2] * v[0] +
+                   f[6] * u[0] * v[2] + f[9] * u[1] * v[1];
+    double term1 = f[1] * u[0] * v[0] + f[7] * u[1] * v[0] + f[8] * u[0] * v[1];
+    double term2 = f[4] * u[0] * v[0];
+    return cd(term0 * t[0] + term1 * t[1] + term2 * t[2], 0.0);
+  });
+  convolve(c);
+  fphi_mpole(c);
+  for (int i = 0; i < n; ++i) {
+    const double* fp = &c->fphirec[(size_t)i * 20];
+    double* cp = &cphi[(size_t)i * 10];
+    cp[0] = ftc[0][0] * fp[0];
+    for (int j = 1; j < 4; ++j) {
+      cp[j] = 0.0;
+      for (int k = 1; k < 4; ++k) cp[j] = cp[j] + ftc[j][k] * fp[k];
+    }
+    for (int j = 4; j < 10; ++j) {
+      cp[j] = 0.0;
+      for (int k = 4; k < 10; ++k) cp[j] = cp[j] + ftc[j][k] * fp[k];
+    }
+  }
+}
+
+// newinduce_pme.f:1919-2128 (tmatxbrecip) with grid_uind_site (pmestuff.f:280)
+// and fphi_uind_site (pmestuff.f:746)
+void or_tmatxbrecip(OrCtx* c, int nrhs, const double* mu, double* dipfield) {
+  const OrSystem& s = c->s;
+  int n = s.n, bs = c->bsorder;
+  if (!c->have_bspline) bspline_fill(c);
+  double a[3][3];
+  int nf[3] = {s.nfft1, s.nfft2, s.nfft3};
+  for (int j = 0; j < 3; ++j)
+    for (int d = 0; d < 3; ++d) a[d][j] = (double)nf[d] * c->recip[j][d];
+  std::vector<double> fu((size_t)n * 6);
+  for (int i = 0; i < n; ++i) {
+    const double* ud = &mu[((size_t)i * nrhs + 0) * 3];
+    const double* up = &mu[((size_t)i * nrhs + (nrhs > 1 ? 1 : 0)) * 3];
+    for (int k = 0; k < 3; ++k) {
+      fu[i * 6 + k] = a[k][0] * ud[0] + a[k][1] * ud[1] + a[k][2] * ud[2];
+      fu[i * 6 + 3 + k] = a[k][0] * up[0] + a[k][1] * up[1] + a[k][2] * up[2];
+    }
+  }
+  spread_sites(c, [&](int i, const double* t, const double* u, const double* v) {
+    const double* fd = &fu[i * 6];
+    const double* fp = &fu[i * 6 + 3];
+    double term01 = fd[1] * u[1] * v[0] + fd[2] * u[0] * v[1];
+    double term11 = fd[0] * u[0] * v[0];
+    double term02 = fp[1] * u[1] * v[0] + fp[2] * u[0] * v[1];
+    double term12 = fp[0] * u[0] * v[0];
+    return cd(term01 * t[0] + term11 * t[1], term02 * t[0] + term12 * t[1]);
+  });
+  convolve(c);
+  int nthr = nthreads_of(&s);
+#pragma omp parallel for num_threads(nthr) schedule(static)
+  for (int i = 0; i < n; ++i) {
+    const double* th1 = &c->theta1[(size_t)i * bs * 4];
+    const double* th2 = &c->theta2[(size_t)i * bs * 4];
+    const double* th3 = &c->theta3[(size_t)i * bs * 4];
+    const int* ig = &c->igrid[i * 3];
+    double tuv100_1 = 0, tuv010_1 = 0, tuv001_1 = 0, tuv100_2 = 0, tuv010_2 = 0, tuv001_2 = 0;
+    for (int it3 = 1; it3 <= bs; ++it3) {
+      int k = gather_index(ig[2], it3, s.nfft3);
+      double v0 = th3[(it3 - 1) * 4 + 0], v1 = th3[(it3 - 1) * 4 + 1];
+      double tu00_1 = 0, tu01_1 = 0, tu10_1 = 0, tu00_2 = 0, tu01_2 = 0, tu10_2 = 0;
+      for (int it2 = 1; it2 <= bs; ++it2) {
+        int j = gather_index(ig[1], it2, s.nfft2);
+        double u0 = th2[(it2 - 1) * 4 + 0], u1 = th2[(it2 - 1) * 4 + 1];
+        double t0_1 = 0, t1_1 = 0, t0_2 = 0, t1_2 = 0;
+        for (int it1 = 1; it1 <= bs; ++it1) {
+          int ii = gather_index(ig[0], it1, s.nfft1);
+          cd g = c->grid[((size_t)k * s.nfft2 + j) * s.nfft1 + ii];
+          double tq_1 = g.real(), tq_2 = g.imag();
+          t0_1 = t0_1 + tq_1 * th1[(it1 - 1) * 4 + 0];
+          t1_1 = t1_1 + tq_1 * th1[(it1 - 1) * 4 + 1];
+          t0_2 = t0_2 + tq_2 * th1[(it1 - 1) * 4 + 0];
+          t1_2 = t1_2 + tq_2 * th1[(it1 - 1) * 4 + 1];
+        }
+        tu00_1 = tu00_1 + t0_1 * u0;
+        tu10_1 = tu10_1 + t1_1 * u0;
+        tu01_1 = tu01_1 + t0_1 * u1;
+        tu00_2 = tu00_2 + t0_2 * u0;
+        tu10_2 = tu10_2 + t1_2 * u0;
+        tu01_2 = tu01_2 + t0_2 * u1;
+      }
+      tuv100_1 = tuv100_1 + tu10_1 * v0;
+      tuv010_1 = tuv010_1 + tu01_1 * v0;
+      tuv001_1 = tuv001_1 + tu00_1 * v1;
+      tuv100_2 = tuv100_2 + tu10_2 * v0;
+      tuv010_2 = tuv010_2 + tu01_2 * v0;
+      tuv001_2 = tuv001_2 + tu00_2 * v1;
+    }
+    double p1[3] = {tuv100_1, tuv010_1, tuv001_1}, p2[3] = {tuv100_2, tuv010_2, tuv001_2};
+    for (int k = 0; k < 3; ++k) {
+      dipfield[((size_t)i * nrhs + 0) * 3 + k] = a[k][0] * p1[0] + a[k][1] * p1[1] + a[k][2] * p1[2];
+      if (nrhs > 1) dipfield[((size_t)i * nrhs + 1) * 3 + k] = a[k][0] * p2[0] + a[k][1] * p2[1] + a[k][2] * p2[2];
+    }
+  }
+}
+
+// newinduce_pme2.f:16-283 (newinduce_pme2) + :285-636 (inducepcg_pme2)
+int or_newinduce_pme2(OrCtx* c, const double* mu_guess, double* uind, double* uinp, double* ef_out,
+                      OrSolveInfo* info) {
+  const OrSystem& s = c->s;
+  const int n = s.n, nrhs = 2;
+  const size_t nv = (size_t)n * nrhs * 3;
+  if (!c->have_list) return OR_E_LIST_OVERFLOW;
+  std::vector<double> ef(nv, 0.0), mu(nv, 0.0), cphi((size_t)n * 10, 0.0);
+  or_efld0_recip(c, cphi.data());
+  or_efld0_direct(c, ef.data());
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < 3; ++j) {
+      ef[(i * 2 + 0) * 3 + j] = ef[(i * 2 + 0) * 3 + j] - cphi[i * 10 + j + 1];
+      ef[(i * 2 + 1) * 3 + j] = ef[(i * 2 + 1) * 3 + j] - cphi[i * 10 + j + 1];
+    }
+  double term = (4.0 / 3.0) * s.aewald * s.aewald * s.aewald / kSqrtPi;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < 3; ++j) {
+      ef[(i * 2 + 0) * 3 + j] = ef[(i * 2 + 0) * 3 + j] + term * s.rpole[(size_t)i * 13 + j + 1];
+      ef[(i * 2 + 1) * 3 + j] = ef[(i * 2 + 1) * 3 + j] + term * s.rpole[(size_t)i * 13 + j + 1];
+    }
+  if (ef_out) std::copy(ef.begin(), ef.end(), ef_out);
+  if (mu_guess) {
+    std::copy(mu_guess, mu_guess + nv, mu.begin());
+  } else {
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < nrhs; ++k)
+        for (int j = 0; j < 3; ++j) mu[(i * 2 + k) * 3 + j] = s.polarity[i] * ef[(i * 2 + k) * 3 + j];
+  }
+  // inducepcg_pme2
+  std::vector<double> res(nv, 0.0), h(nv, 0.0), pp(nv, 0.0), zr(nv, 0.0), dipfield(nv, 0.0), diag(n);
+  for (int i = 0; i < n; ++i) diag[i] = (s.polarity[i] == 0.0) ? kTinyPol : s.polarity[i];
+  double ggold[2] = {0, 0}, ggnew[2], gg[2], alphacg[2], ene[2] = {0, 0}, gnorm[2] = {0, 0};
+  or_tmatxbrecip(c, nrhs, mu.data(), dipfield.data());
+  or_tmatxb_pme(c, nrhs, 1, mu.data(), h.data());
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < nrhs; ++k)
+      for (int j = 0; j < 3; ++j) {
+        size_t q = (i * 2 + k) * 3 + j;
+        h[q] = h[q] + dipfield[q] - term * mu[q];
+        res[q] = ef[q] - h[q];
+        zr[q] = diag[i] * res[q];
+      }
+  pp = zr;
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < nrhs; ++k)
+      for (int j = 0; j < 3; ++j) ggold[k] = ggold[k] + res[(i * 2 + k) * 3 + j] * zr[(i * 2 + k) * 3 + j];
+  int it, converged = 0;
+  double resnrm = 0.0;
+  for (it = 1; it <= s.politer; ++it) {
+    or_tmatxbrecip(c, nrhs, pp.data(), dipfield.data());
+    or_tmatxb_pme(c, nrhs, 1, pp.data(), h.data());
+    for (size_t q = 0; q < nv; ++q) h[q] = h[q] + dipfield[q] - term * pp[q];
+    gg[0] = gg[1] = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < nrhs; ++k)
+        for (int j = 0; j < 3; ++j) gg[k] = gg[k] + pp[(i * 2 + k) * 3 + j] * h[(i * 2 + k) * 3 + j];
+    bool zero = false;
+    for (int k = 0; k < nrhs; ++k) {
+      if (gg[k] == 0.0) zero = true;
+    }
+    if (zero) break;  // reference returns (newinduce_pme2.f:505)
+    for (int k = 0; k < nrhs; ++k) alphacg[k] = ggold[k] / gg[k];
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < nrhs; ++k)
+        for (int j = 0; j < 3; ++j) {
+          size_t q = (i * 2 + k) * 3 + j;
+          mu[q] = mu[q] + alphacg[k] * pp[q];
+          res[q] = res[q] - alphacg[k] * h[q];
+        }
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < nrhs; ++k)
+        for (int j = 0; j < 3; ++j) zr[(i * 2 + k) * 3 + j] = diag[i] * res[(i * 2 + k) * 3 + j];
+    ggnew[0] = ggnew[1] = 0.0;
+    ene[0] = ene[1] = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < nrhs; ++k)
+        for (int j = 0; j < 3; ++j) {
+          size_t q = (i * 2 + k) * 3 + j;
+          ggnew[k] = ggnew[k] + res[q] * zr[q];
+          ene[k] = ene[k] - 0.5 * (mu[q] * (res[q] + ef[q]));
+        }
+    resnrm = 0.0;
+    for (int k = 0; k < nrhs; ++k) {
+      gnorm[k] = std::sqrt(ggnew[k] / (double)(3 * n));
+      resnrm = std::max(resnrm, gnorm[k]);
+    }
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < nrhs; ++k)
+        for (int j = 0; j < 3; ++j) {
+          size_t q = (i * 2 + k) * 3 + j;
+          pp[q] = zr[q] + ggnew[k] / ggold[k] * pp[q];
+        }
+    ggold[0] = ggnew[0];
+    ggold[1] = ggnew[1];
+    if (resnrm < s.poleps) {
+      converged = 1;
+      break;
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < 3; ++j) {
+      uind[i * 3 + j] = mu[(i * 2 + 0) * 3 + j];
+      uinp[i * 3 + j] = mu[(i * 2 + 1) * 3 + j];
+    }
+  if (info) {
+    info->niter = std::min(it, s.politer);
+    info->converged = converged;
+    info->resnrm = resnrm;
+    info->ene[0] = ene[0] * kElectric;
+    info->ene[1] = ene[1] * kElectric;
+  }
+  return OR_OK;
+}
+
+// epolar.f:47-520: epolar0c = eprecip + epreal0c + self (TINFOIL boundary)
+double or_epolar(OrCtx* c, const double* uind, double* ereal_out, double* erecip_out, double* eself_out) {
+  const OrSystem& s = c->s;
+  const int n = s.n, maxelst = c->maxelst;
+  const double off2 = s.ewaldcut * s.ewaldcut;
+  // eprecip (epolar.f:524-712), needs fphirec from the permanent-field PME pass
+  if (c->fphirec.size() != (size_t)n * 20) {
+    std::vector<double> cphi((size_t)n * 10);
+    or_efld0_recip(c, cphi.data());
+  }
+  double a[3][3];
+  int nf[3] = {s.nfft1, s.nfft2, s.nfft3};
+  for (int i = 0; i < 3; ++i)
+    for (int d = 0; d < 3; ++d) a[d][i] = (double)nf[d] * c->recip[i][d];
+  double erec = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double fuind[3];
+    for (int j = 0; j < 3; ++j) fuind[j] = a[j][0] * uind[i * 3 + 0] + a[j][1] * uind[i * 3 + 1] + a[j][2] * uind[i * 3 + 2];
+    for (int k = 0; k < 3; ++k) erec = erec + fuind[k] * c->fphirec[(size_t)i * 20 + k + 1];
+  }
+  erec = 0.5 * kElectric * erec;
+  // epreal0c (epolar.f:207-520), mode MPOLE -> off = mpolecut = ewaldcut
+  const double f = 0.5 * kElectric;
+  double ereal_acc = 0.0;
+  {
+    std::vector<double> e1(1, 0.0);
+    int nthr = nthreads_of(&s);
+    std::vector<double> part(nthr, 0.0);
+#pragma omp parallel num_threads(nthr)
+    {
+      int tid = 0;
+#ifdef _OPENMP
+      tid = omp_get_thread_num();
+#endif
+      ScaleWs w;
+      w.init(n);
+      double ep = 0.0;
+#pragma omp for schedule(dynamic, 64)
+      for (int i = 0; i < n; ++i) {
+        const double* ri = &s.rpole[(size_t)i * 13];
+        double ci = ri[0], dix = ri[1], diy = ri[2], diz = ri[3];
+        double qixx = ri[4], qixy = ri[5], qixz = ri[6], qiyy = ri[8], qiyz = ri[9], qizz = ri[12];
+        double uix = uind[i * 3], uiy = uind[i * 3 + 1], uiz = uind[i * 3 + 2];
+        set_p_scales(s, i, w, false);
+        for (int kkk = 0; kkk < c->nelst[i]; ++kkk) {
+          int k = c->elst[(size_t)i * maxelst + kkk];
+          double xr = s.x[k] - s.x[i], yr = s.y[k] - s.y[i], zr = s.z[k] - s.z[i];
+          image(c->cell, xr, yr, zr);
+          double r2 = xr * xr + yr * yr + zr * zr;
+          if (r2 > off2) continue;
+          double r = std::sqrt(r2);
+          const double* rk = &s.rpole[(size_t)k * 13];
+          double ck = rk[0], dkx = rk[1], dky = rk[2], dkz = rk[3];
+          double qkxx = rk[4], qkxy = rk[5], qkxz = rk[6], qkyy = rk[8], qkyz = rk[9], qkzz = rk[12];
+          double ukx = uind[k * 3], uky = uind[k * 3 + 1], ukz = uind[k * 3 + 2];
+          double dir = dix * xr + diy * yr + diz * zr;
+          double qix = qixx * xr + qixy * yr + qixz * zr;
+          double qiy = qixy * xr + qiyy * yr + qiyz * zr;
+          double qiz = qixz * xr + qiyz * yr + qizz * zr;
+          double qir = qix * xr + qiy * yr + qiz * zr;
+          double dkr = dkx * xr + dky * yr + dkz * zr;
+          double qkx = qkxx * xr + qkxy * yr + qkxz * zr;
+          double qky = qkxy * xr + qkyy * yr + qkyz * zr;
+          double qkz = qkxz * xr + qkyz * yr + qkzz * zr;
+          double qkr = qkx * xr + qky * yr + qkz * zr;
+          double diu = dix * ukx + diy * uky + diz * ukz;
+          double qiu = qix * ukx + qiy * uky + qiz * ukz;
+          double uir = uix * xr + uiy * yr + uiz * zr;
+          double dku = dkx * uix + dky * uiy + dkz * uiz;
+          double qku = qkx * uix + qky * uiy + qkz * uiz;
+          double ukr = ukx * xr + uky * yr + ukz * zr;
+          double dmpe[8], dmpik[8];
+          dampewald(7, r, r2, f, s.aewald, dmpe);
+          dampthole(s.pdamp[i], s.pdamp[k], s.thole[i], s.thole[k], 7, r, dmpik);
+          double scalek = w.p[k];
+          double rr3 = f / (r * r2);
+          double rr5 = 3.0 * rr3 / r2;
+          double rr7 = 5.0 * rr5 / r2;
+          double sr3 = scalek * dmpik[3] * rr3;
+          double sr5 = scalek * dmpik[5] * rr5;
+          double sr7 = scalek * dmpik[7] * rr7;
+          sr3 = dmpe[3] - rr3 + sr3;
+          sr5 = dmpe[5] - rr5 + sr5;
+          sr7 = dmpe[7] - rr7 + sr7;
+          double term1 = ck * uir - ci * ukr + diu + dku;
+          double term2 = 2.0 * (qiu - qku) - uir * dkr - dir * ukr;
+          double term3 = uir * qkr - ukr * qir;
+          ep += term1 * sr3 + term2 * sr5 + term3 * sr7;
+        }
+        set_p_scales(s, i, w, true);
+      }
+      part[tid] = ep;
+    }
+    for (int t = 0; t < nthr; ++t) ereal_acc += part[t];
+  }
+  // self term (epolar.f:131-146)
+  double term = 2.0 * s.aewald * s.aewald;
+  double fterm = -kElectric * s.aewald / kSqrtPi;
+  double eself = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double* rp = &s.rpole[(size_t)i * 13];
+    double uii = rp[1] * uind[i * 3] + rp[2] * uind[i * 3 + 1] + rp[3] * uind[i * 3 + 2];
+    eself = eself + fterm * term * uii / 3.0;
+  }
+  if (ereal_out) *ereal_out = ereal_acc;
+  if (erecip_out) *erecip_out = erec;
+  if (eself_out) *eself_out = eself;
+  return erec + ereal_acc + eself;
+}
+
+// rotpole.f:17-339 (rotmat for Z-then-X and Bisector, rotsite)
+void or_rotpole(int n, const double* x, const double* y, const double* z, const double* pole, const int* zaxis,
+                const int* xaxis, const int* axt, double* rpole) {
+  for (int i = 0; i < n; ++i) {
+    double a[3][3] = {{1, 0, 0}, {0, 0, 0}, {0, 0, 1}};
+    // a[row][col] == reference a(row+1,col+1)
+    a[0][0] = 1.0; a[1][0] = 0.0; a[2][0] = 0.0;
+    a[0][2] = 0.0; a[1][2] = 0.0; a[2][2] = 1.0;
+    double xi = x[i], yi = y[i], zi = z[i];
+    int iz = zaxis[i], ix = xaxis[i];
+    if (axt[i] == 1) {  // Z-then-X
+      double dx = x[iz] - xi, dy = y[iz] - yi, dz = z[iz] - zi;
+      double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+      a[0][2] = dx / r; a[1][2] = dy / r; a[2][2] = dz / r;
+      dx = x[ix] - xi; dy = y[ix] - yi; dz = z[ix] - zi;
+      double dot = dx * a[0][2] + dy * a[1][2] + dz * a[2][2];
+      dx = dx - dot * a[0][2]; dy = dy - dot * a[1][2]; dz = dz - dot * a[2][2];
+      r = std::sqrt(dx * dx + dy * dy + dz * dz);
+      a[0][0] = dx / r; a[1][0] = dy / r; a[2][0] = dz / r;
+    } else if (axt[i] == 2) {  // Bisector
+      double dx = x[iz] - xi, dy = y[iz] - yi, dz = z[iz] - zi;
+      double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+      double dx1 = dx / r, dy1 = dy / r, dz1 = dz / r;
+      dx = x[ix] - xi; dy = y[ix] - yi; dz = z[ix] - zi;
+      r = std::sqrt(dx * dx + dy * dy + dz * dz);
+      double dx2 = dx / r, dy2 = dy / r, dz2 = dz / r;
+      dx = dx1 + dx2; dy = dy1 + dy2; dz = dz1 + dz2;
+      r = std::sqrt(dx * dx + dy * dy + dz * dz);
+      a[0][2] = dx / r; a[1][2] = dy / r; a[2][2] = dz / r;
+      double dot = dx2 * a[0][2] + dy2 * a[1][2] + dz2 * a[2][2];
+      dx = dx2 - dot * a[0][2]; dy = dy2 - dot * a[1][2]; dz = dz2 - dot * a[2][2];
+      r = std::sqrt(dx * dx + dy * dy + dz * dz);
+      a[0][0] = dx / r; a[1][0] = dy / r; a[2][0] = dz / r;
+    }
+    a[0][1] = a[2][0] * a[1][2] - a[1][0] * a[2][2];
+    a[1][1] = a[0][0] * a[2][2] - a[2][0] * a[0][2];
+    a[2][1] = a[1][0] * a[0][2] - a[0][0] * a[1][2];
+    const double* p = &pole[(size_t)i * 13];
+    double* rp = &rpole[(size_t)i * 13];
+    rp[0] = p[0];
+    for (int ii = 0; ii < 3; ++ii) {
+      rp[1 + ii] = 0.0;
+      for (int j = 0; j < 3; ++j) rp[1 + ii] = rp[1 + ii] + p[1 + j] * a[ii][j];
+    }
+    double m2[3][3], r2[3][3];
+    int k = 4;
+    for (int ii = 0; ii < 3; ++ii)
+      for (int j = 0; j < 3; ++j) {
+        m2[ii][j] = p[k];
+        r2[ii][j] = 0.0;
+        k++;
+      }
+    for (int ii = 0; ii < 3; ++ii)
+      for (int j = 0; j < 3; ++j) {
+        if (j < ii) {
+          r2[ii][j] = r2[j][ii];
+        } else {
+          for (int kk = 0; kk < 3; ++kk)
+            for (int m = 0; m < 3; ++m) r2[ii][j] = r2[ii][j] + a[ii][kk] * a[j][m] * m2[kk][m];
+        }
+      }
+    k = 4;
+    for (int ii = 0; ii < 3; ++ii)
+      for (int j = 0; j < 3; ++j) rp[k++] = r2[ii][j];
+  }
+}
+
+}  // extern "C"

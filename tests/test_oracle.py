@@ -1,0 +1,204 @@
+"""Pins the CPU FP64 oracle (oracle/) against independent arithmetic.
+
+The reference ships no golden vectors for this path and cannot be built here,
+so the oracle is checked against: numpy's FFT, libm's erfc, a brute-force
+minimum-image pair search, classical Ewald k-space sums (tests/ewald_ref.py),
+a dense linear solve, and exact invariances.
+"""
+import dataclasses
+import math
+
+import numpy as np
+import pytest
+from scipy.special import erfc as sp_erfc
+
+from oracle import oracle as O
+from tests import ewald_ref
+
+ELECTRIC = 332.063714
+
+
+@pytest.fixture(scope="module")
+def box216(thp):
+    return thp.water.make_water_box(216, cfg=0)
+
+
+def test_fft_matches_numpy():
+    rng = np.random.default_rng(0)
+    for shape in [(8, 6, 10), (16, 16, 16), (24, 20, 18), (5, 7, 9)]:
+        g = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        fwd = O.fft3d(g, -1)
+        np.testing.assert_allclose(fwd, np.fft.fftn(g), rtol=0, atol=1e-10 * np.abs(fwd).max())
+        back = O.fft3d(g, +1)
+        np.testing.assert_allclose(back, np.fft.ifftn(g) * g.size, rtol=0, atol=1e-10 * np.abs(back).max())
+
+
+def test_erfc_matches_libm():
+    for x in np.concatenate([np.linspace(0, 6, 601), [0.3, 0.46875, 0.47, 3.9999, 4.0, 4.0001, 26.0]]):
+        ref = math.erfc(x)
+        got = O.lib().or_erfc(float(x))
+        assert abs(got - ref) <= 1e-14 * max(ref, 1e-300) + 1e-300, (x, got, ref)
+
+
+def test_ewaldcof_default():
+    # kewald.f:575 with the 7 A cutoff gives the 0.5446 of the workload definition
+    a = O.lib().or_ewaldcof(7.0)
+    assert abs(a - 0.5446) < 5e-5
+
+
+def _bruteforce_pairs(ws, cut):
+    pos = ws.positions()
+    L = np.asarray(ws.box)
+    out = []
+    for i in range(ws.n - 1):
+        d = pos[i] - pos[i + 1:]
+        # image.f orthogonal branch, |d| < L here so a single shift suffices
+        d = np.where(np.abs(d) > 0.5 * L, d - np.copysign(L, d), d)
+        r2 = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+        ks = np.nonzero(r2 <= cut * cut)[0] + i + 1
+        out += [(i, k) for k in ks]
+    p = np.array(out)
+    return p[np.lexsort((p[:, 1], p[:, 0]))]
+
+
+def test_pair_set_matches_bruteforce(box216):
+    orc = O.Oracle(box216)
+    st, nelst, _ = orc.mlistcell()
+    assert st == 0
+    ref = _bruteforce_pairs(box216, box216.ewaldcut + box216.lbuffer)
+    np.testing.assert_array_equal(orc.pairs(), ref)
+
+
+def test_list_overflow_and_small_box(thp, box216):
+    orc = O.Oracle(box216)
+    st, _, _ = orc.mlistcell(maxelst=20)
+    assert st == 2  # list overflow (nblist.f:232 fatal in the reference)
+    small = thp.water.make_water_box(64, cfg=0)  # 12.4 A box: half edge < 7.5 A
+    assert O.Oracle(small).mlistcell()[0] == 8
+
+
+def _with_grid(ws, k):
+    return dataclasses.replace(ws, nfft=(k, k, k))
+
+
+def test_pme_dipole_field_converges_to_ewald(box216):
+    rng = np.random.default_rng(1)
+    mu = rng.standard_normal((box216.n, 2, 3)) * 0.05
+    ref = ewald_ref.recip_field(box216.positions(), box216.box, box216.aewald, d=mu[:, 0, :])
+    errs = []
+    for k in (16, 32, 64):
+        orc = O.Oracle(_with_grid(box216, k))
+        dip = orc.tmatxbrecip(mu)  # = grad(phi) = -E_rec
+        errs.append(np.abs(-dip[:, 0, :] - ref).max() / np.abs(ref).max())
+    # order-5 B-splines: the error falls at least like h^4 towards classical Ewald
+    assert errs[0] < 3e-2 and errs[1] < errs[0] / 16 and errs[2] < errs[1] / 16 and errs[2] < 5e-5, errs
+
+
+def test_pme_multipole_field_converges_to_ewald(box216):
+    orc0 = O.Oracle(box216)
+    rp = orc0.rpole
+    ref = ewald_ref.recip_field(box216.positions(), box216.box, box216.aewald, q=rp[:, 0], d=rp[:, 1:4],
+                                Q=rp[:, 4:13].reshape(-1, 3, 3))
+    errs = []
+    for k in (16, 32, 64):
+        cphi = O.Oracle(_with_grid(box216, k)).efld0_recip()
+        errs.append(np.abs(-cphi[:, 1:4] - ref).max() / np.abs(ref).max())
+    # quadrupoles use second spline derivatives: at least h^3 convergence
+    assert errs[0] < 3e-2 and errs[1] < errs[0] / 8 and errs[2] < errs[1] / 8 and errs[2] < 5e-5, errs
+
+
+def _dense_operator(ws, rp, kgrid):
+    """A = alpha^-1 - T built from independent real-space sums and a classical
+    Ewald k-space matrix (64-water box, 16 A edge)."""
+    n = ws.n
+    pos = ws.positions()
+    L = np.asarray(ws.box)
+    a = ws.aewald
+    T = np.zeros((3 * n, 3 * n))
+    for i in range(n):
+        for k in range(n):
+            if i == k:
+                continue
+            r = pos[k] - pos[i]
+            r -= L * np.round(r / L)
+            r2 = r @ r
+            if r2 > ws.ewaldcut ** 2:
+                continue
+            rr = math.sqrt(r2)
+            b0 = sp_erfc(a * rr) / rr
+            ex = math.exp(-a * a * r2)
+            b1 = (b0 + 2 * a / math.sqrt(math.pi) * ex) / r2
+            b2 = (3 * b1 + 4 * a ** 3 / math.sqrt(math.pi) * ex) / r2
+            damp = min(ws.thole[i], ws.thole[k]) * (rr / (ws.pdamp[i] * ws.pdamp[k])) ** 3
+            e = math.exp(-damp)
+            l3, l5 = 1 - e, 1 - e * (1 + damp)
+            dmp3 = b1 - (1 - l3) / rr ** 3
+            dmp5 = b2 - 3 * (1 - l5) / rr ** 5
+            T[3 * i:3 * i + 3, 3 * k:3 * k + 3] = dmp5 * np.outer(r, r) - dmp3 * np.eye(3)
+    k, k2 = ewald_ref.kvectors(ws.box, a, tol=1e-16)
+    V = float(np.prod(L))
+    f = (4 * np.pi / V) * np.exp(-k2 / (4 * a * a)) / k2
+    C, S = np.cos(pos @ k.T), np.sin(pos @ k.T)
+    for p in range(3):
+        for q in range(3):
+            w = f * k[:, p] * k[:, q]
+            T[p::3, q::3] -= (C * w) @ C.T + (S * w) @ S.T
+    term = 4.0 / 3.0 * a ** 3 / math.sqrt(math.pi)
+    A = -T
+    A[np.diag_indices(3 * n)] += np.repeat(1.0 / ws.polarity, 3) - term
+    return A
+
+
+def test_pcg_matches_dense_ewald_solve(thp):
+    ws = thp.water.make_water_box(64, cfg=3, edge=16.0)
+    ws = _with_grid(ws, 64)  # 0.25 A spacing: PME within ~2e-6 of classical Ewald
+    orc = O.Oracle(ws, poleps=1e-11)
+    assert orc.mlistcell()[0] == 0
+    res = orc.solve()
+    assert res["converged"]
+    A = _dense_operator(ws, orc.rpole, 64)
+    for rhs, key in ((0, "uind"), (1, "uinp")):
+        x = np.linalg.solve(A, res["ef"][:, rhs, :].reshape(-1))
+        err = np.abs(x.reshape(-1, 3) - res[key]).max() / np.abs(x).max()
+        assert err < 3e-6, (key, err)
+
+
+def test_converged_residual_and_energy_identity(box216):
+    orc = O.Oracle(box216, poleps=1e-8)
+    assert orc.mlistcell()[0] == 0
+    res = orc.solve()
+    assert res["converged"] and res["niter"] > 3
+    mu = np.stack([res["uind"], res["uinp"]], axis=1)
+    term = 4.0 / 3.0 * box216.aewald ** 3 / math.sqrt(math.pi)
+    h = orc.tmatxb(mu) + orc.tmatxbrecip(mu) - term * mu
+    r = res["ef"] - h
+    rms = np.sqrt(np.sum(r * r * box216.polarity[:, None, None]) / (3 * box216.n) / 2)
+    assert rms < 1e-8
+    e, parts = orc.epolar(res["uind"])
+    ident = -0.5 * ELECTRIC * np.sum(res["uind"] * res["ef"][:, 1, :])
+    assert abs(e - ident) < 1e-10 * abs(e)
+    assert abs(sum(parts.values()) - e) < 1e-12 * abs(e)
+
+
+def test_grid_translation_invariance(box216):
+    # a shift by whole grid spacings leaves PME and real space unchanged
+    k = box216.nfft[0]
+    h = box216.box[0] / k
+    shift = np.array([3 * h, -2 * h, 5 * h])
+    ws2 = box216.with_positions(box216.positions() + shift)
+    e = []
+    for ws in (box216, ws2):
+        orc = O.Oracle(ws)
+        orc.mlistcell()
+        res = orc.solve()
+        e.append(orc.epolar(res["uind"])[0])
+    assert abs(e[0] - e[1]) < 1e-9 * abs(e[0])
+
+
+def test_threads_agree(box216):
+    r = []
+    for nt in (1, 4):
+        orc = O.Oracle(box216, nthreads=nt)
+        orc.mlistcell()
+        r.append(orc.solve()["uind"])
+    np.testing.assert_allclose(r[0], r[1], rtol=0, atol=1e-12)

@@ -1,0 +1,103 @@
+"""AMOEBA water parameters and Tinker-HP defaults used by the polarization path.
+
+Values are force-field data from Tinker-HP's AMOEBA-WATER-2003 parameter file
+(v1.2/params/water03.prm:30-50 scale factors, :135-156 multipoles and
+polarizabilities) and program defaults from v1.2/source (initprm.f:413-470,
+cutoffs.f:40-80, kewald.f:67-91, MOD_units.f:77-82).
+"""
+
+import math
+
+# MOD_units.f:77-82
+BOHR = 0.52917721092
+ELECTRIC = 332.063714
+DEBYE = 4.80321
+
+# water03.prm:135-145, local-frame multipoles in atomic units:
+# charge; dipole (x, y, z); quadrupole rows xx / xy yy / xz yz zz
+WATER_MULTIPOLES = {
+    "O": {
+        "charge": -0.51966,
+        "dipole": (0.00000, 0.00000, 0.14279),
+        "quad": ((0.37928, 0.0, 0.0), (0.0, -0.41809, 0.0), (0.0, 0.0, 0.03881)),
+    },
+    "H": {
+        "charge": 0.25983,
+        "dipole": (-0.03859, 0.00000, -0.05818),
+        "quad": ((-0.03673, 0.0, -0.00203), (0.0, -0.10739, 0.0), (-0.00203, 0.0, 0.14412)),
+    },
+}
+
+# water03.prm:155-156 (polarize: alpha A^3, thole)
+WATER_POLARITY = {"O": 0.837, "H": 0.496}
+WATER_THOLE = {"O": 0.390, "H": 0.390}
+
+# water03.prm:30-50 and initprm.f:417-470 defaults for the unset ones
+SCALES = {
+    "p_scale": (0.0, 0.0, 1.0, 1.0),   # polar-12..15-scale
+    "pi_scale": (0.0, 0.0, 0.5, 1.0),  # polar-12..15-intra (p2i, p3i default 0; 14-intra 0.5)
+    "d_scale": (0.0, 1.0, 1.0, 1.0),   # direct-11..14-scale
+    "u_scale": (1.0, 1.0, 1.0, 1.0),   # mutual-11..14-scale
+}
+
+# frame codes shared with the C-ABI: 1 = Z-then-X, 2 = Bisector
+AXT_Z_THEN_X = 1
+AXT_BISECTOR = 2
+
+# kewald.f:67-73 FFT-friendly grid sizes
+MULTI = (2, 4, 6, 8, 10, 12, 16, 18, 20, 24, 30, 32, 36, 40, 48, 50, 54, 60, 64, 72, 80, 90, 96, 100,
+         108, 120, 128, 144, 150, 160, 162, 180, 192, 200, 216, 240, 250, 256, 270, 288, 300, 320, 324,
+         360, 384, 400, 432, 450, 480, 486, 500, 512, 540, 576, 600, 640, 648, 720, 750, 768, 800, 810,
+         864)
+MINFFT = 16
+
+# defaults of the workload (cutoffs.f:58 ewald-cutoff, list buffer per the configs)
+EWALD_CUTOFF = 7.0
+LIST_BUFFER = 0.5
+VDW_CUTOFF = 9.0
+BSORDER = 5
+POLITER = 500
+
+
+def pme_grid_size(box_edge, spacing=1.2):
+    """Grid points along one edge: kewald.f:144-146 density rule with
+    density = 1/spacing, rounded up to the MULTI list, floor MINFFT (kewald.f:213-226)."""
+    dens = 1.0 / spacing
+    ie = int(box_edge * dens - 1.0e-8) + 1
+    n = MULTI[-1]
+    for k in reversed(MULTI):
+        if k >= ie:
+            n = k
+    return max(n, MINFFT)
+
+
+def local_pole(kind):
+    """13-component local-frame multipole in e, e*A, e*A^2 (kmpole.f:530-537:
+    dipoles times bohr, quadrupoles times bohr^2/3)."""
+    m = WATER_MULTIPOLES[kind]
+    p = [m["charge"]]
+    p += [d * BOHR for d in m["dipole"]]
+    for row in m["quad"]:
+        p += [q * BOHR * BOHR / 3.0 for q in row]
+    return p
+
+
+def ewaldcof(cutoff, erfc=math.erfc):
+    """Ewald coefficient with erfc(a*cutoff)/cutoff < 1e-8 (kewald.f:575-620)."""
+    eps = 1.0e-8
+    ratio = eps + 1.0
+    x = 0.5
+    i = 0
+    while ratio >= eps:
+        i += 1
+        x = 2.0 * x
+        ratio = erfc(x * cutoff) / cutoff
+    xlo, xhi = 0.0, x
+    for _ in range(i + 60):
+        x = (xlo + xhi) / 2.0
+        ratio = erfc(x * cutoff) / cutoff
+        if ratio >= eps:
+            xlo = x
+        else:
+            xhi = x
+    return x
