@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Benchmark of the AMOEBA induced-dipole polarization path on B200.
+
+Workload: the 96,000-water (288,000-atom) synthetic box (142.3 A, PME grid
+120^3, alpha 0.5446, cutoff 7.0 + 0.5 A buffer), one step = one single-point
+polarization solve: list build + permanent field (direct + PME) + PCG to
+tolerance + polarization energy.  The headline is the mixed-precision form
+(FP32 pair fields and PME, FP64 CG scalars, CG tol 1e-5); the plain FP64 form
+on the same box, the dipole error of mixed versus FP64, p50/p99 latency, the
+end-to-end host-buffer call and the CPU baseline are reported beside it.
+
+Contract: one JSON line on rank 0.  N>1 (torchrun): independent replicas, one
+box per GPU (weak scaling), time = max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def load_package():
+    import importlib.util
+    name = "tinker_hp_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    d = os.path.join(ROOT, "tinker-hp_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(d, "__init__.py"),
+                                                  submodule_search_locations=[d])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules[name] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+METRIC = "induced-dipole solves/s & p99 latency, mixed vs FP64 on one B200 at 1e-5 D RMS"
+WORKLOADS = {
+    # name: (waters, cfg index for seeds)
+    "water-288k": (96000, 2),
+    "water-32k": (10800, 1),
+    "water-1944": (648, 0),
+}
+DEBYE = 4.80321
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([s.strip() for s in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def allreduce_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline_oracle(ws_sys, max_seconds, threads):
+    """The oracle (C++ FP64 restatement of the reference) on the host cores,
+    one full single-point solve of the same box."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    orc = O.Oracle(ws_sys, poleps=1e-5, nthreads=threads)
+    st, _, _ = orc.mlistcell()
+    if st != 0:
+        raise RuntimeError(f"oracle list status {st}")
+    res = orc.solve()
+    e, _ = orc.epolar(res["uind"])
+    dt = time.perf_counter() - t0
+    return dt, res, e
+
+
+def run_reference(args, ws_n, rank, world):
+    """--impl reference: the CPU restatement of the reference's v1.2 path
+    (the Fortran reference cannot be built here), all host threads."""
+    if rank != 0:
+        return
+    thp = load_package()
+    nw, cfg = WORKLOADS[args.workload]
+    ws = thp.water.make_water_box(nw, cfg=cfg)
+    threads = os.cpu_count() or 1
+    budget = 150.0
+    times = []
+    warm = min(args.warmup, 1)
+    t_start = time.perf_counter()
+    for _ in range(warm):
+        dt, _, _ = cpu_baseline_oracle(ws, budget, threads)
+    steps = 0
+    for _ in range(args.steps):
+        dt, res, e = cpu_baseline_oracle(ws, budget, threads)
+        times.append(dt)
+        steps += 1
+        if time.perf_counter() - t_start > budget:
+            break
+    tot = sum(times)
+    value = steps / tot
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": steps, "warmup": warm, "ms_per_step": 1000.0 * tot / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload} ({ws.n} atoms, box {ws.box[0]:.2f} A, grid {ws.nfft[0]}^3)",
+                       "cg_tol": 1e-5, "iterations": res["niter"]},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "sample": f"{steps} full FP64 solves of the {ws.n}-atom box (C++ restatement of "
+                                       f"v1.2, OpenMP {threads} threads); the Fortran reference needs gfortran+MPI, "
+                                       "absent on this image"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def timed_solves(ctx, lib, steps, warmup, rebuild=True, guess=None):
+    """Device-resident solves; per-step device time from CUDA events."""
+    import torch
+    guess = lib.GUESS_DIRECT if guess is None else guess
+    for _ in range(warmup):
+        if rebuild:
+            ctx.invalidate_list()
+        ctx.solve(guess)
+    torch.cuda.synchronize()
+    lat = []
+    niters = []
+    for _ in range(steps):
+        if rebuild:
+            ctx.invalidate_list()
+        r = ctx.solve(guess)
+        lat.append(r["ms"])
+        niters.append(r["niter"])
+    torch.cuda.synchronize()
+    return lat, niters
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="water-288k", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, None, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    thp = load_package()
+    from tinker_hp_b200 import lib
+    lib.load()
+    nw, cfg = WORKLOADS[args.workload]
+    ws = thp.water.make_water_box(nw, cfg=cfg)
+    stream = torch.cuda.current_stream()
+
+    # mixed form (headline)
+    mixed = lib.Context(ws, precision=lib.MIXED, poleps=1e-5, device=local)
+    mixed.set_stream(stream.cuda_stream)
+    fp64 = None if args.no_fp64 else lib.Context(ws, precision=lib.FP64, poleps=1e-5, device=local)
+    if fp64 is not None:
+        fp64.set_stream(stream.cuda_stream)
+
+    # accuracy of mixed against FP64 on the GPU (tight FP64 reference)
+    acc = {}
+    if fp64 is not None:
+        ref64 = lib.Context(ws, precision=lib.FP64, poleps=1e-8, device=local)
+        ref64.set_stream(stream.cuda_stream)
+        r_ref = ref64.solve()
+        u_ref, _ = ref64.dipoles()
+        r_m = mixed.solve()
+        u_m, _ = mixed.dipoles()
+        r_d = fp64.solve()
+        u_d, _ = fp64.dipoles()
+        acc = {"mixed_dipole_rms_D": float(np.sqrt(np.mean(np.sum((u_m - u_ref) ** 2, 1))) * DEBYE),
+               "fp64_dipole_rms_D": float(np.sqrt(np.mean(np.sum((u_d - u_ref) ** 2, 1))) * DEBYE),
+               "mixed_epol_rel": abs(r_m["epol"] - r_ref["epol"]) / abs(r_ref["epol"]),
+               "fp64_epol_rel": abs(r_d["epol"] - r_ref["epol"]) / abs(r_ref["epol"]),
+               "epol_kcal": r_ref["epol"], "iters_mixed": r_m["niter"], "iters_fp64": r_d["niter"]}
+        ref64.close()
+        del ref64
+
+    clocks = ClockSampler(local)
+    # ---- timed region: mixed, device-resident inputs
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    for _ in range(args.warmup):
+        mixed.invalidate_list()
+        mixed.solve()
+    barrier(world)
+    torch.cuda.synchronize()
+    mixed.profile(1)
+    ev0.record(stream)
+    lat = []
+    niter = []
+    for _ in range(args.steps):
+        mixed.invalidate_list()
+        r = mixed.solve()
+        lat.append(r["ms"])
+        niter.append(r["niter"])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    mv_ms, mv_launches = mixed.profile(0)
+    barrier(world)
+    t_mixed = allreduce_max(ev0.elapsed_time(ev1), world)
+    clk = clocks.stop()
+
+    # ---- FP64 form on the same box
+    fp64_line = None
+    if fp64 is not None:
+        lat64, nit64 = timed_solves(fp64, lib, max(3, args.steps // 2), 3)
+        t64 = allreduce_max(float(np.sum(lat64)), world)
+        fp64_line = {"value": world * len(lat64) / (t64 / 1000.0), "unit": "solves/s",
+                     "ms_per_step": t64 / len(lat64), "p50_ms": float(np.percentile(lat64, 50)),
+                     "p99_ms": float(np.percentile(lat64, 99)), "iterations": int(np.median(nit64))}
+
+    # ---- end to end through the host-buffer C-ABI call
+    rp = mixed.rpole()
+    x, y, z = (np.ascontiguousarray(a) for a in (ws.x, ws.y, ws.z))
+    for _ in range(2):
+        mixed.solve_host(x, y, z, rp)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(e2e_steps):
+        mixed.solve_host(x, y, z, rp)  # positions+rpole H2D, solve, dipoles D2H (synchronous)
+    torch.cuda.synchronize()
+    t_e2e = allreduce_max(time.perf_counter() - t0, world)
+    n = ws.n
+    h2d = n * 3 * 8 + n * 13 * 8
+    d2h = n * 6 * 8
+
+    peaks, peak_kind = measured_peaks()
+    # roofline of the fused CG matvec: algorithmic bytes per launch (FP64 figures halved for per-atom and
+    # grid data in the mixed form): 68 N (x, pol, mu in, field out) + 4 L (list) + 8 K^3 (grid read once)
+    L_entries = 88.4 * n
+    K3 = ws.nfft[0] * ws.nfft[1] * ws.nfft[2]
+    alg_bytes = 68.0 * n + 4.0 * L_entries + 8.0 * K3
+    avg_ms = mv_ms / max(mv_launches, 1)
+    achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": "k_cg_matvec<mixed> (PME gather + real-space row + CG combine)",
+            "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+            "frac": achieved / peaks.get("hbm_gbs"), "peak_kind": peak_kind, "traffic": None,
+            "avg_launch_ms": avg_ms, "launches": mv_launches, "alg_bytes_per_launch": alg_bytes}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            th = os.cpu_count() or 1
+            dt, res_c, e_c = cpu_baseline_oracle(ws, 120, th)
+            cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": th, "kind": "port",
+                   "sample": f"1 full FP64 solve of the {n}-atom box by the C++ restatement of v1.2 "
+                             f"({res_c['niter']} CG iterations, {dt:.1f} s)"}
+        except Exception as ex:  # the GPU number stands without it
+            cpu = {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"failed: {ex}"}
+
+    steps = args.steps
+    value = world * steps / (t_mixed / 1000.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": t_mixed / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {nw} waters, {n} atoms, box {ws.box[0]:.2f} A, PME "
+                               f"{ws.nfft[0]}^3 order 5, alpha {ws.aewald:.4f}, cutoff 7.0+0.5 A",
+                   "form": "mixed (FP32 pair fields/PME, FP64 CG)", "cg_tol": 1e-5,
+                   "parallelism": f"replicas x{world}", "l2": "inputs > L2 (pair stream ~0.5 GB per matvec)",
+                   "iterations": int(np.median(niter))},
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "fp64": fp64_line, "accuracy": acc,
+        "speedup_mixed_vs_fp64": (value / fp64_line["value"]) if fp64_line else None,
+        "e2e": {"value": world * e2e_steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+        "gpu_launches": None,
+    }
+    # kernel launches of this library per timed step (list build 5, field 2+spread/FFT,
+    # per CG iteration 4 of ours + 2 cuFFT)
+    it = int(np.median(niter))
+    per_step = 5 + 1 + 1 + 3 + 1 + (it + 1) * 4 + 1
+    line["gpu_launches"] = per_step * steps
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    mixed.close()
+    if fp64 is not None:
+        fp64.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,169 @@
+/*
+ * thp.h -- C-ABI of the B200-native AMOEBA induced-dipole polarization path.
+ *
+ * Two layers:
+ *   1. Native API (thp_*): an opaque per-system context owning device state.
+ *      Plain pointers and sizes, host arrays in the reference's layouts:
+ *        - per-atom vectors (3,nrhs,n) Fortran order == C [n][nrhs][3];
+ *        - multipoles rpole(13,n) == C [n][13] (q, dx,dy,dz, Qxx,Qxy,Qxz,
+ *          Qyx,Qyy,Qyz,Qzx,Qzy,Qzz in e, e*A, e*A^2, traceless, /3 as stored
+ *          by kmpole.f:534-537);
+ *        - neighbor lists nelst(n), elst(maxelst,n) == C [n][maxelst].
+ *      Every entry point returns a THP_* status and never exits.
+ *   2. Fortran drop-ins with the reference's subroutine names (gfortran
+ *      mangling name_, arguments by reference).  They act on the context made
+ *      current by thp_bind_state() and record failures in thp_last_error().
+ *
+ * Threading: thread-safe across contexts, not within one context.  All device
+ * work of a context is ordered on its stream.
+ */
+#ifndef THP_H
+#define THP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define THP_OK 0
+#define THP_E_INVALID 1        /* bad argument or unsupported option */
+#define THP_E_LIST_OVERFLOW 2  /* neighbor capacity exceeded (nblist.f:232 fatal) */
+#define THP_E_NOT_CONVERGED 3  /* CG reached politer without meeting poleps */
+#define THP_E_NAN 4            /* non-finite value in the CG recurrences */
+#define THP_E_CUDA 5           /* CUDA runtime or cuFFT failure */
+#define THP_E_TIMEOUT 6        /* a bounded device wait gave up */
+#define THP_E_OOM_ADMISSION 7  /* request does not fit the device-memory budget */
+#define THP_E_BOX_TOO_SMALL 8  /* list cutoff exceeds half a box edge (nblist.f:148) */
+#define THP_E_NO_DEVICE 9      /* no usable CUDA device */
+#define THP_E_STATE 10         /* call made before its inputs were set */
+
+/* ---- precision forms ---------------------------------------------------- */
+#define THP_FP64 0  /* everything in FP64 */
+#define THP_MIXED 1 /* FP32 pair fields and PME, FP64 CG scalars and energy */
+
+/* ---- connectivity slots (modules couple and polgrp) -------------------- */
+#define THP_I12 0
+#define THP_I13 1
+#define THP_I14 2
+#define THP_I15 3
+#define THP_IP11 4
+#define THP_IP12 5
+#define THP_IP13 6
+#define THP_IP14 7
+#define THP_NCONN 8
+
+/* ---- initial guess of the dipoles (newinduce_pme2.f:161-200) ----------- */
+#define THP_GUESS_DIRECT 0   /* mu = alpha * E0 (polgsf = 0) */
+#define THP_GUESS_PREVIOUS 1 /* mu = last converged dipoles kept on the device */
+#define THP_GUESS_HOST 2     /* mu = caller-provided array (thp_set_guess) */
+
+typedef struct thp_config {
+  int n;            /* polarizable sites (npole == npolar == n) */
+  double box[3];    /* orthogonal box edges xbox, ybox, zbox (A) */
+  double aewald;    /* Ewald coefficient (1/A), kewald.f:apewald */
+  double ewaldcut;  /* real-space cutoff (A), cutoffs.f:ewaldcut */
+  double lbuffer;   /* neighbor-list buffer (A), cutoffs.f:lbuffer */
+  int nfft[3];      /* PME grid nfft1..3 */
+  int bsorder;      /* B-spline order; 5 is supported */
+  int politer;      /* max CG iterations (initprm.f:441) */
+  double poleps;    /* CG stop: max_k sqrt(sum res.zr / 3n) < poleps */
+  int precision;    /* THP_FP64 or THP_MIXED */
+  int max_neighbors;/* per-atom capacity of the full list (0: 320) */
+  int device;       /* CUDA device ordinal */
+} thp_config;
+
+typedef struct thp_solve_info {
+  int niter;        /* CG iterations taken */
+  int converged;    /* 1 when resnrm < poleps */
+  double resnrm;    /* final residual norm (reference units) */
+  double epol;      /* polarization energy, kcal/mol (epolar.f:epolar0c) */
+  double ene[2];    /* CG energies -1/2 sum mu.(res+ef) * electric (inducepcg) */
+  double ms_total;  /* device time of the solve, ms */
+} thp_solve_info;
+
+typedef struct thp_ctx thp_ctx;
+
+/* ---- native API ---------------------------------------------------------- */
+int thp_ctx_create(const thp_config* cfg, thp_ctx** out);
+int thp_ctx_destroy(thp_ctx* ctx);
+/* use an external CUDA stream (cudaStream_t passed as void*) */
+int thp_set_stream(thp_ctx* ctx, void* stream);
+/* polarity(n) A^3, thole(n), pdamp(n) = polarity^(1/6) (kpolar.f:225-300) */
+int thp_set_params(thp_ctx* ctx, const double* polarity, const double* thole, const double* pdamp);
+/* CSR connectivity, slot order THP_I12..THP_IP14: off[slot][n+1], idx[slot][];
+ * scales[16] = p2..p5scale, p2i..p5iscale, d1..d4scale, u1..u4scale. */
+int thp_set_connectivity(thp_ctx* ctx, const int* const* off, const int* const* idx,
+                         const double* scales);
+int thp_set_positions(thp_ctx* ctx, const double* x, const double* y, const double* z);
+int thp_set_rpole(thp_ctx* ctx, const double* rpole);
+/* local-frame multipoles and frames; rotpole runs on the device.
+ * axt: 1 = Z-then-X, 2 = Bisector (rotpole.f:58-200); axes 0-based. */
+int thp_set_frames(thp_ctx* ctx, const double* pole, const int* zaxis, const int* xaxis,
+                   const int* axt);
+int thp_set_guess(thp_ctx* ctx, const double* mu /*[n][2][3]*/);
+/* list build (mlistcell), incremental when displacements allow */
+int thp_nblist(thp_ctx* ctx);
+/* full rebuild (cell sort + list) on the next list use, as nblist(0) does */
+int thp_invalidate_list(thp_ctx* ctx);
+/* device time of the fused CG matvec kernels since the last reset:
+ * enable != 0 starts recording events around each launch (and resets). */
+int thp_profile(thp_ctx* ctx, int enable, double* ms_total, int* launches);
+/* E0 + PCG + Epol on the device (newinduce_pme2 + epolar0c) */
+int thp_solve(thp_ctx* ctx, int guess, thp_solve_info* info);
+int thp_get_dipoles(thp_ctx* ctx, double* uind, double* uinp);
+int thp_get_field(thp_ctx* ctx, double* ef /*[n][2][3]*/);
+int thp_get_rpole(thp_ctx* ctx, double* rpole /*[n][13]*/);
+/* reference-format half list (k > i, 0-based) copied to the host */
+int thp_get_nblist(thp_ctx* ctx, int maxelst, int* nelst, int* elst);
+/* single operators on host arrays, reference semantics */
+int thp_tmatxb(thp_ctx* ctx, int nrhs, int dodiag, const double* mu, double* efi);
+int thp_efld0_direct(thp_ctx* ctx, int nrhs, double* ef);
+int thp_efld0_recip(thp_ctx* ctx, double* cphi /*[n][10]*/);
+int thp_tmatxbrecip(thp_ctx* ctx, int nrhs, const double* mu, double* dipfield);
+/* one-call solve on host buffers (positions in, dipoles and energy out) */
+int thp_solve_host(thp_ctx* ctx, const double* x, const double* y, const double* z,
+                   const double* rpole, double* uind, double* uinp, thp_solve_info* info);
+/* bytes of device memory a context of this configuration needs */
+size_t thp_footprint(const thp_config* cfg);
+const char* thp_status_string(int status);
+
+/* ---- Fortran drop-ins ---------------------------------------------------- */
+/* Make ctx current and bind the module arrays the reference reads/writes:
+ * atoms::x,y,z(n), mpole::rpole(13,n), polar::uind,uinp(3,n),
+ * neigh::nelst(n), elst(maxelst,n) (may be NULL), energi::ep (may be NULL). */
+int thp_bind_state(thp_ctx* ctx, double* x, double* y, double* z, double* rpole, double* uind,
+                   double* uinp, int* nelst, int* elst, int maxelst, double* ep);
+int thp_last_error(void);
+
+/* newinduce_pme2.f:16 -- fields, guess, PCG, writeback of uind/uinp */
+void newinduce_pme2_(void);
+/* newinduce_pme2.f:285 -- PCG on caller arrays ef,mu(3,nrhs,n); murec unused
+ * on one device.  matvec == tmatxb_pme_ runs the device loop; any other
+ * matvec is called back from a host loop. */
+void inducepcg_pme2_(void (*matvec)(const int* nrhs, const int* dodiag, const double* mu,
+                                    double* efi),
+                     const int* nrhs, const int* precnd, const double* ef, double* mu,
+                     double* murec);
+/* newinduce_pme.f:1392 -- efi = -T_real mu (+ mu/alpha when dodiag), overwrites efi */
+void tmatxb_pme_(const int* nrhs, const int* dodiag, const double* mu, double* efi);
+/* newinduce_pme.f:948 -- adds the direct permanent field to ef(3,nrhs,n) */
+void efld0_direct_(const int* nrhs, double* ef);
+/* newinduce_pme.f:1671 -- reciprocal permanent potential cphi(10,n) */
+void efld0_recip_(double* cphi);
+/* newinduce_pme.f:1919 -- reciprocal dipole field; murec/dipfieldbis unused */
+void tmatxbrecip_(const double* mu, const double* murec, const int* nrhs, double* dipfield,
+                  double* dipfieldbis);
+/* nblist.f:117 -- rebuild the polarization list; fills the bound elst/nelst */
+void mlistcell_(void);
+/* nblist.f:1148 -- same list for the vdW slot name used by the workload */
+void vlistcell_(void);
+/* epolar.f:17 -- polarization energy into the bound ep (solves first) */
+void epolar_(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* THP_H */

@@ -1,0 +1,225 @@
+"""Parity of the CUDA path (through the C-ABI) with the CPU FP64 oracle.
+
+Tolerances (FP64 form): bit-exact neighbor pair set; operators within 1e-11
+relative of the oracle's; induced dipoles within 1e-6 D RMS and polarization
+energy within 1e-8 relative (the workload's FP64 acceptance).  Mixed form:
+dipole RMS error against the FP64 oracle within 1e-5 D.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+DEBYE = 4.80321
+
+
+@pytest.fixture(scope="module")
+def lib(thp):
+    from tinker_hp_b200 import lib as L
+    L.load()
+    return L
+
+
+@pytest.fixture(scope="module", params=[216, 648], ids=["216w", "648w"])
+def case(request, thp):
+    ws = thp.water.make_water_box(request.param, cfg=0)
+    orc = O.Oracle(ws, poleps=1e-6)
+    assert orc.mlistcell()[0] == 0
+    return ws, orc
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def test_pair_set_bit_exact(lib, case):
+    ws, orc = case
+    ctx = lib.Context(ws)
+    np.testing.assert_array_equal(ctx.pairs(), orc.pairs())
+
+
+def test_rotpole(lib, case):
+    ws, orc = case
+    ctx = lib.Context(ws)
+    assert rel(ctx.rpole(), orc.rpole) < 1e-13
+
+
+def test_efld0_direct(lib, case):
+    ws, orc = case
+    ctx = lib.Context(ws)
+    assert rel(ctx.efld0_direct(), orc.efld0_direct()) < 1e-12
+
+
+def test_efld0_recip(lib, case):
+    ws, orc = case
+    ctx = lib.Context(ws)
+    g, r = ctx.efld0_recip(), orc.efld0_recip()
+    for a in range(10):
+        assert rel(g[:, a], r[:, a]) < 1e-11, a
+
+
+def test_tmatxb(lib, case):
+    ws, orc = case
+    ctx = lib.Context(ws)
+    mu = np.random.default_rng(5).standard_normal((ws.n, 2, 3)) * 0.05
+    for dodiag in (False, True):
+        assert rel(ctx.tmatxb(mu, dodiag), orc.tmatxb(mu, dodiag)) < 1e-12
+
+
+def test_tmatxbrecip(lib, case):
+    ws, orc = case
+    ctx = lib.Context(ws)
+    mu = np.random.default_rng(6).standard_normal((ws.n, 2, 3)) * 0.05
+    assert rel(ctx.tmatxbrecip(mu), orc.tmatxbrecip(mu)) < 1e-11
+
+
+def test_solve_fp64_matches_oracle(lib, case):
+    ws, orc = case
+    ref = orc.solve()
+    e_ref, _ = orc.epolar(ref["uind"])
+    ctx = lib.Context(ws, poleps=1e-6)
+    res = ctx.solve()
+    uind, uinp = ctx.dipoles()
+    assert res["converged"] and res["niter"] == ref["niter"]
+    rms_d = np.sqrt(np.mean(np.sum((uind - ref["uind"]) ** 2, axis=1))) * DEBYE
+    rms_p = np.sqrt(np.mean(np.sum((uinp - ref["uinp"]) ** 2, axis=1))) * DEBYE
+    assert rms_d < 1e-6 and rms_p < 1e-6, (rms_d, rms_p)
+    assert abs(res["epol"] - e_ref) < 1e-8 * abs(e_ref), (res["epol"], e_ref)
+    np.testing.assert_allclose(ctx.field(), ref["ef"], rtol=0, atol=1e-11 * np.abs(ref["ef"]).max())
+
+
+def test_solve_mixed_error_vs_fp64(lib, case):
+    ws, orc = case
+    ref = orc.solve()
+    e_ref, _ = orc.epolar(ref["uind"])
+    ctx = lib.Context(ws, precision=lib.MIXED, poleps=1e-6)
+    res = ctx.solve()
+    uind, _ = ctx.dipoles()
+    rms_d = np.sqrt(np.mean(np.sum((uind - ref["uind"]) ** 2, axis=1))) * DEBYE
+    assert res["converged"]
+    assert rms_d < 1e-5, rms_d
+    assert abs(res["epol"] - e_ref) < 1e-5 * abs(e_ref)
+
+
+def test_bitwise_reproducible(lib, case):
+    ws, _ = case
+    ctx = lib.Context(ws)
+    ctx.solve()
+    a = ctx.dipoles()
+    ctx.solve()
+    b = ctx.dipoles()
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_warm_start_fewer_iterations(lib, case):
+    ws, _ = case
+    ctx = lib.Context(ws, poleps=1e-6)
+    r1 = ctx.solve()
+    r2 = ctx.solve(guess=lib.GUESS_PREVIOUS)
+    assert r2["niter"] < r1["niter"]
+
+
+def test_solve_host_call(lib, case):
+    ws, orc = case
+    ctx = lib.Context(ws, frames=False, rpole=orc.rpole)
+    ref = orc.solve()
+    uind, uinp, info = ctx.solve_host(ws.x, ws.y, ws.z, orc.rpole)
+    assert np.sqrt(np.mean(np.sum((uind - ref["uind"]) ** 2, axis=1))) * DEBYE < 1e-6
+
+
+def test_fortran_dropins(lib, case):
+    ws, orc = case
+    L = lib.load()
+    ctx = lib.Context(ws, frames=False, rpole=orc.rpole)
+    n = ws.n
+    x, y, z = (np.ascontiguousarray(a) for a in (ws.x, ws.y, ws.z))
+    rp = np.ascontiguousarray(orc.rpole)
+    uind = np.zeros((n, 3))
+    uinp = np.zeros((n, 3))
+    maxelst = 1200
+    nelst = np.zeros(n, np.int32)
+    elst = np.zeros((n, maxelst), np.int32)
+    ep = np.zeros(1)
+    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    I = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+    assert L.thp_bind_state(ctx.h, P(x), P(y), P(z), P(rp), P(uind), P(uinp), I(nelst), I(elst), maxelst, P(ep)) == 0
+    L.mlistcell_()
+    assert L.thp_last_error() == 0
+    rows = np.repeat(np.arange(n), nelst)
+    mask = np.arange(maxelst)[None, :] < nelst[:, None]
+    pairs = np.stack([rows, elst[mask] - 1], axis=1)  # Fortran 1-based
+    pairs = pairs[np.lexsort((pairs[:, 1], pairs[:, 0]))]
+    np.testing.assert_array_equal(pairs, orc.pairs())
+    L.newinduce_pme2_()
+    assert L.thp_last_error() == 0
+    ref = orc.solve()
+    assert np.sqrt(np.mean(np.sum((uind - ref["uind"]) ** 2, axis=1))) * DEBYE < 1e-6
+    L.epolar_()
+    e_ref, _ = orc.epolar(ref["uind"])
+    assert abs(ep[0] - e_ref) < 1e-8 * abs(e_ref)
+    # single operators with Fortran argument passing
+    mu = np.random.default_rng(7).standard_normal((n, 2, 3)) * 0.05
+    efi = np.zeros_like(mu)
+    two, one = C.c_int(2), C.c_int(1)
+    L.tmatxb_pme_(C.byref(two), C.byref(one), P(mu), P(efi))
+    assert L.thp_last_error() == 0 and rel(efi, orc.tmatxb(mu, True)) < 1e-12
+    ef = np.zeros((n, 2, 3))
+    L.efld0_direct_(C.byref(two), P(ef))
+    assert rel(ef, orc.efld0_direct()) < 1e-12
+    cphi = np.zeros((n, 10))
+    L.efld0_recip_(P(cphi))
+    assert rel(cphi[:, 1:4], orc.efld0_recip()[:, 1:4]) < 1e-11
+    dip = np.zeros_like(mu)
+    L.tmatxbrecip_(P(mu), P(mu), C.byref(two), P(dip), P(dip))
+    assert rel(dip, orc.tmatxbrecip(mu)) < 1e-11
+
+
+def test_inducepcg_dropin_device_and_callback(lib, case):
+    ws, orc = case
+    L = lib.load()
+    ctx = lib.Context(ws, frames=False, rpole=orc.rpole)
+    n = ws.n
+    ref = orc.solve()
+    z3 = np.zeros((n, 3))
+    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    x, y, z = (np.ascontiguousarray(a) for a in (ws.x, ws.y, ws.z))
+    L.thp_bind_state(ctx.h, P(x), P(y), P(z), P(orc.rpole), None, None, None, None, 0, None)
+    ef = np.ascontiguousarray(ref["ef"])
+    two, one = C.c_int(2), C.c_int(1)
+    # device loop: matvec is the library's own tmatxb_pme_
+    mu = np.ascontiguousarray(ws.polarity[:, None, None] * ef)
+    L.inducepcg_pme2_(C.cast(L.tmatxb_pme_, C.c_void_p), C.byref(two), C.byref(one), P(ef), P(mu), P(mu))
+    assert L.thp_last_error() == 0
+    assert np.sqrt(np.mean(np.sum((mu[:, 0] - ref["uind"]) ** 2, axis=1))) * DEBYE < 1e-6
+    # host loop: a caller-provided matvec (here the oracle's)
+    MV = C.CFUNCTYPE(None, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double))
+
+    def mv(nr, dd, m, out):
+        k = nr[0]
+        a = np.ctypeslib.as_array(m, shape=(n, k, 3)).copy()
+        r = orc.tmatxb(a, bool(dd[0]))
+        np.ctypeslib.as_array(out, shape=(n, k, 3))[:] = r
+
+    cb = MV(mv)
+    mu2 = np.ascontiguousarray(ws.polarity[:, None, None] * ef)
+    L.inducepcg_pme2_(C.cast(cb, C.c_void_p), C.byref(two), C.byref(one), P(ef), P(mu2), P(mu2))
+    assert L.thp_last_error() == 0
+    assert np.sqrt(np.mean(np.sum((mu2[:, 0] - ref["uind"]) ** 2, axis=1))) * DEBYE < 1e-6
+
+
+def test_error_statuses(lib, thp, case):
+    ws, _ = case
+    with pytest.raises(lib.ThpError) as e:
+        lib.Context(ws, max_neighbors=16).solve()
+    assert e.value.status == lib.THP_E_LIST_OVERFLOW
+    small = thp.water.make_water_box(64, cfg=0)
+    with pytest.raises(lib.ThpError) as e:
+        lib.Context(small)
+    assert e.value.status == lib.THP_E_BOX_TOO_SMALL
+    ctx = lib.Context(ws, poleps=1e-12, politer=3)
+    r = ctx.solve(allow_unconverged=True)
+    assert r["status"] == lib.THP_E_NOT_CONVERGED and r["niter"] == 3

@@ -1,0 +1,936 @@
+// api.cu -- C-ABI of the library: contexts, uploads, solve driver and the
+// Fortran-named drop-ins of the reference's polarization subroutines.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "kernels.h"
+
+using namespace thp;
+
+struct thp_ctx {
+  Ctx c;
+  bool pos_dirty = true;      // positions uploaded but not yet in sorted order
+  bool rpole_dirty = true;    // multipoles uploaded / frames need rotation
+  bool field_valid = false;   // d_ef holds E0 for the current positions
+  bool guess_uploaded = false;
+  bool solved_once = false;
+};
+
+namespace thp {
+int cuda_status(cudaError_t e, Ctx* c, const char* what) {
+  if (e == cudaSuccess) return THP_OK;
+  if (c) {
+    c->last_msg = std::string(what) + ": " + cudaGetErrorString(e);
+  }
+  return THP_E_CUDA;
+}
+}  // namespace thp
+
+namespace {
+
+thread_local int g_last_error = THP_OK;
+thp_ctx* g_current = nullptr;
+
+constexpr int kDefaultMaxNb = 320;
+
+template <class T>
+int dmalloc(Ctx& c, T** p, size_t count, const char* what) {
+  if (count == 0) count = 1;
+  return cuda_status(cudaMalloc((void**)p, sizeof(T) * count), &c, what);
+}
+
+// Special pairs with their (d, p, u) scales, in the assignment order of
+// efld0_direct (newinduce_pme.f:1062-1136, dpequal false) and tmatxb_pme
+// (:1495-1518): pscale from i12..i15 (p*iscale when the partner is in ip11),
+// dscale and uscale from ip11..ip14.  Pairs whose three scales are all 1 are
+// dropped.
+void build_special_pairs(Ctx& c, const int* const* off, const int* const* idx, const double* sc) {
+  const int n = c.n;
+  c.sp_off.assign(n + 1, 0);
+  c.sp_k.clear();
+  c.sp_s.clear();
+  auto row = [&](int slot, int i, std::vector<int>& out) {
+    out.clear();
+    if (!off || !off[slot] || !idx[slot]) return;
+    for (int q = off[slot][i]; q < off[slot][i + 1]; ++q) out.push_back(idx[slot][q]);
+  };
+  std::vector<int> lst, ip11;
+  for (int i = 0; i < n; ++i) {
+    std::map<int, std::array<double, 3>> m;
+    auto get = [&](int k) -> std::array<double, 3>& {
+      auto it = m.find(k);
+      if (it == m.end()) it = m.emplace(k, std::array<double, 3>{1.0, 1.0, 1.0}).first;
+      return it->second;
+    };
+    row(THP_IP11, i, ip11);
+    for (int b = 0; b < 4; ++b) {
+      row(THP_I12 + b, i, lst);
+      for (int k : lst) {
+        double p = sc[b];
+        if (std::find(ip11.begin(), ip11.end(), k) != ip11.end()) p = sc[4 + b];
+        get(k)[1] = p;
+      }
+    }
+    for (int b = 0; b < 4; ++b) {
+      row(THP_IP11 + b, i, lst);
+      for (int k : lst) get(k)[0] = sc[8 + b];
+    }
+    for (int b = 0; b < 4; ++b) {
+      row(THP_IP11 + b, i, lst);
+      for (int k : lst) get(k)[2] = sc[12 + b];
+    }
+    for (auto& kv : m) {
+      if (kv.first == i) continue;
+      const auto& s = kv.second;
+      if (s[0] == 1.0 && s[1] == 1.0 && s[2] == 1.0) continue;
+      c.sp_k.push_back(kv.first);
+      c.sp_s.push_back(s[0]);
+      c.sp_s.push_back(s[1]);
+      c.sp_s.push_back(s[2]);
+    }
+    c.sp_off[i + 1] = (int)c.sp_k.size();
+  }
+}
+
+int upload_special_pairs(Ctx& c) {
+  cudaFree(c.d_sp_off);
+  cudaFree(c.d_sp_k);
+  cudaFree(c.d_sp_s);
+  c.d_sp_off = nullptr;
+  c.d_sp_k = nullptr;
+  c.d_sp_s = nullptr;
+  int st;
+  if ((st = dmalloc(c, &c.d_sp_off, c.n + 1, "alloc sp_off"))) return st;
+  if ((st = dmalloc(c, &c.d_sp_k, c.sp_k.size(), "alloc sp_k"))) return st;
+  if ((st = dmalloc(c, &c.d_sp_s, c.sp_s.size(), "alloc sp_s"))) return st;
+  cudaMemcpy(c.d_sp_off, c.sp_off.data(), sizeof(int) * (c.n + 1), cudaMemcpyHostToDevice);
+  if (!c.sp_k.empty()) {
+    cudaMemcpy(c.d_sp_k, c.sp_k.data(), sizeof(int) * c.sp_k.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(c.d_sp_s, c.sp_s.data(), sizeof(double) * c.sp_s.size(), cudaMemcpyHostToDevice);
+  }
+  return cuda_status(cudaGetLastError(), &c, "upload special pairs");
+}
+
+void cell_grid(const thp_config& cfg, int nc[3]) {
+  const double half_cut = 0.5 * (cfg.ewaldcut + cfg.lbuffer) + 1e-6;
+  for (int d = 0; d < 3; ++d) nc[d] = std::max(1, (int)std::floor(cfg.box[d] / half_cut));
+}
+
+int check_flags(thp_ctx* h) {
+  Ctx& c = h->c;
+  cudaMemcpyAsync(c.h_flags, c.d_flags, sizeof(int), cudaMemcpyDeviceToHost, c.stream);
+  int st = cuda_status(cudaStreamSynchronize(c.stream), &c, "sync");
+  if (st) return st;
+  int f = *c.h_flags;
+  if (f) {
+    cudaMemsetAsync(c.d_flags, 0, sizeof(int), c.stream);
+    if (f & (DEV_LIST_OVERFLOW | DEV_PAIR_OVERFLOW)) {
+      c.last_msg = "neighbor capacity exceeded";
+      return THP_E_LIST_OVERFLOW;
+    }
+    return THP_E_NAN;
+  }
+  return THP_OK;
+}
+
+int set_current_device(Ctx& c) { return cuda_status(cudaSetDevice(c.device), &c, "set device"); }
+
+// Ensures the sorted arrays match the uploaded positions and the list is
+// valid: full rebuild on the first call or when an atom moved by more than
+// lbuffer/2 since the last build (the reference rebuilds every ineigup steps;
+// the displacement test keeps the same interacting set).
+int ensure_list(thp_ctx* h, bool force_rebuild) {
+  Ctx& c = h->c;
+  int st;
+  if (!c.have_pos) return THP_E_STATE;
+  bool rebuild = force_rebuild || !c.have_list;
+  if (!rebuild && h->pos_dirty) {
+    if ((st = launch_gather_sorted(c))) return st;
+    double disp = 0.0;
+    if ((st = launch_max_displacement(c, &disp))) return st;
+    if (disp >= 0.5 * c.cfg.lbuffer) rebuild = true;
+    h->pos_dirty = false;
+    h->rpole_dirty = false;
+    c.have_coef = false;
+    h->field_valid = false;
+  }
+  if (rebuild) {
+    if ((st = launch_sort_atoms(c))) return st;
+    if ((st = launch_gather_sorted(c))) return st;
+    if ((st = launch_build_list(c))) return st;
+    if ((st = check_flags(h))) return st;
+    c.have_list = true;
+    c.have_coef = false;
+    h->field_valid = false;
+    h->pos_dirty = false;
+    h->rpole_dirty = false;
+  } else if (h->pos_dirty || h->rpole_dirty) {
+    if ((st = launch_gather_sorted(c))) return st;
+    h->pos_dirty = false;
+    h->rpole_dirty = false;
+    h->field_valid = false;
+  }
+  return THP_OK;
+}
+
+int ensure_rpole(thp_ctx* h) {
+  Ctx& c = h->c;
+  if (c.have_frames) {
+    int st = launch_rotpole(c);
+    if (st) return st;
+    c.have_rpole = true;
+    h->rpole_dirty = true;
+  }
+  return c.have_rpole ? THP_OK : THP_E_STATE;
+}
+
+// E0 = direct + reciprocal + self (newinduce_pme2.f:110-148) and the matvec
+// coefficients, for the current positions and multipoles.
+int compute_field(thp_ctx* h) {
+  Ctx& c = h->c;
+  int st;
+  if ((st = ensure_rpole(h))) return st;
+  if ((st = ensure_list(h, false))) return st;
+  if ((st = launch_efld0_coef(c, true))) return st;
+  if ((st = launch_efld0_recip(c))) return st;
+  if ((st = check_flags(h))) return st;
+  h->field_valid = true;
+  return THP_OK;
+}
+
+int ensure_coef(thp_ctx* h) {
+  Ctx& c = h->c;
+  int st;
+  if ((st = ensure_list(h, false))) return st;
+  if (!c.have_coef) {
+    if ((st = launch_efld0_coef(c, false))) return st;
+    if ((st = check_flags(h))) return st;
+  }
+  return THP_OK;
+}
+
+void free_ctx(Ctx& c) {
+  void* ptrs[] = {c.d_cell_count, c.d_cell_start, c.d_cell_fill, c.d_atom_cell, c.d_scell, c.d_perm, c.d_iperm,
+                  c.d_xyz_orig, c.d_par_orig, c.d_rpole_orig, c.d_pole_local, c.d_frames, c.d_pos, c.d_posf,
+                  c.d_thole, c.d_pol, c.d_rpole, c.d_sp_off, c.d_sp_k, c.d_sp_s, c.d_pos_built, c.d_nnb, c.d_nb,
+                  c.d_npr, c.d_pk, c.d_pc3, c.d_pc5, c.d_ef, c.d_mu, c.d_res, c.d_h, c.d_pp, c.d_zr, c.d_dip,
+                  c.d_cphi, c.d_vecf, c.d_tmp6, c.d_tmp6b, c.d_partials, c.d_cg, c.d_flags};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  pme_free(c);
+  if (c.h_cg) cudaFreeHost(c.h_cg);
+  if (c.h_flags) cudaFreeHost(c.h_flags);
+  if (c.ev0) cudaEventDestroy(c.ev0);
+  if (c.ev1) cudaEventDestroy(c.ev1);
+  if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+}
+
+size_t footprint_bytes(const thp_config& cfg, int* ncell_out) {
+  const size_t n = cfg.n, npad = (n + 31) / 32 * 32;
+  const size_t maxnb = cfg.max_neighbors > 0 ? cfg.max_neighbors : kDefaultMaxNb;
+  int nc[3];
+  cell_grid(cfg, nc);
+  const size_t ncell = (size_t)nc[0] * nc[1] * nc[2];
+  if (ncell_out) *ncell_out = (int)ncell;
+  const bool mixed = cfg.precision == THP_MIXED;
+  const size_t ngrid = (size_t)cfg.nfft[0] * cfg.nfft[1] * cfg.nfft[2];
+  size_t b = 0;
+  b += 3 * ncell * 4 + 2 * n * 4 + 2 * n * 4;          // cells, perm
+  b += (3 + 3 + 13 + 13) * n * 8 + 3 * n * 4;            // staging
+  b += n * 32 + n * 16 + 2 * n * 8 + 10 * n * 8 + n * 32;  // sorted data
+  b += n * 4 + maxnb * npad * 4;                         // list
+  b += n * 4 + maxnb * npad * (4 + 2 * (mixed ? 4 : 8));  // pairs
+  b += ngrid * (mixed ? 12 : 24);                        // grid + qfac
+  b += 9 * n * 6 * 8 + 4 * n * 8 + n * 6 * 4;            // vectors
+  b += (n / 128 + 2) * 4 * 8 + 4096;
+  b += 64 << 20;  // cuFFT work area and runtime slack
+  return b;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* thp_status_string(int s) {
+  switch (s) {
+    case THP_OK: return "ok";
+    case THP_E_INVALID: return "invalid argument";
+    case THP_E_LIST_OVERFLOW: return "neighbor list overflow";
+    case THP_E_NOT_CONVERGED: return "CG not converged";
+    case THP_E_NAN: return "non-finite value";
+    case THP_E_CUDA: return "CUDA error";
+    case THP_E_TIMEOUT: return "device wait timed out";
+    case THP_E_OOM_ADMISSION: return "device memory budget exceeded";
+    case THP_E_BOX_TOO_SMALL: return "cutoff exceeds half box";
+    case THP_E_NO_DEVICE: return "no CUDA device";
+    case THP_E_STATE: return "inputs not set";
+    default: return "unknown";
+  }
+}
+
+size_t thp_footprint(const thp_config* cfg) { return cfg ? footprint_bytes(*cfg, nullptr) : 0; }
+
+int thp_ctx_create(const thp_config* cfg, thp_ctx** out) {
+  if (!cfg || !out) return THP_E_INVALID;
+  *out = nullptr;
+  const thp_config& k = *cfg;
+  if (k.n <= 0 || k.box[0] <= 0 || k.box[1] <= 0 || k.box[2] <= 0 || k.aewald <= 0 || k.ewaldcut <= 0 ||
+      k.lbuffer < 0 || k.bsorder != 5 || k.nfft[0] < 5 || k.nfft[1] < 5 || k.nfft[2] < 5 || k.politer <= 0 ||
+      (k.precision != THP_FP64 && k.precision != THP_MIXED))
+    return THP_E_INVALID;
+  const double rl = k.ewaldcut + k.lbuffer;
+  const double half = 0.5 * std::min(k.box[0], std::min(k.box[1], k.box[2]));
+  if (rl * rl > half * half) return THP_E_BOX_TOO_SMALL;  // nblist.f:147-156
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return THP_E_NO_DEVICE;
+  if (k.device < 0 || k.device >= ndev) return THP_E_INVALID;
+  thp_ctx* h = new thp_ctx();
+  Ctx& c = h->c;
+  c.cfg = k;
+  c.n = k.n;
+  c.npad = (k.n + 31) / 32 * 32;
+  c.mixed = k.precision == THP_MIXED;
+  c.device = k.device;
+  c.maxnb = k.max_neighbors > 0 ? k.max_neighbors : kDefaultMaxNb;
+  c.maxpr = c.maxnb;
+  for (int d = 0; d < 3; ++d) {
+    c.box.l[d] = k.box[d];
+    c.box.half[d] = 0.5 * k.box[d];
+  }
+  // lattice.f:111-120 for an orthogonal box: recip(d,d) = (product of the
+  // other two edges) / volbox
+  const double vol = k.box[0] * k.box[1] * k.box[2];
+  c.box.recip[0] = (k.box[1] * 1.0 * (k.box[2] * 1.0) - (k.box[2] * 0.0) * 0.0) / vol;
+  c.box.recip[1] = ((k.box[2] * 1.0) * k.box[0] - 0.0 * (k.box[2] * 0.0)) / vol;
+  c.box.recip[2] = (k.box[0] * (k.box[1] * 1.0) - (k.box[1] * 0.0) * 0.0) / vol;
+  cell_grid(k, c.nc);
+  c.ncell = c.nc[0] * c.nc[1] * c.nc[2];
+  int st = set_current_device(c);
+  if (!st) st = cuda_status(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), &c, "stream");
+  c.own_stream = true;
+  if (!st) st = cuda_status(cudaEventCreate(&c.ev0), &c, "event");
+  if (!st) st = cuda_status(cudaEventCreate(&c.ev1), &c, "event");
+  const size_t n = c.n, npad = c.npad;
+  const size_t esz = c.mixed ? 4 : 8;
+  c.nblk_reduce = (c.n + 127) / 128;
+  if (!st) st = dmalloc(c, &c.d_cell_count, c.ncell, "cells");
+  if (!st) st = dmalloc(c, &c.d_cell_start, c.ncell, "cells");
+  if (!st) st = dmalloc(c, &c.d_cell_fill, c.ncell, "cells");
+  if (!st) st = dmalloc(c, &c.d_atom_cell, n, "cells");
+  if (!st) st = dmalloc(c, &c.d_scell, n, "cells");
+  if (!st) st = dmalloc(c, &c.d_perm, n, "perm");
+  if (!st) st = dmalloc(c, &c.d_iperm, n, "perm");
+  if (!st) st = dmalloc(c, &c.d_xyz_orig, 3 * n, "xyz");
+  if (!st) st = dmalloc(c, &c.d_par_orig, 3 * n, "params");
+  if (!st) st = dmalloc(c, &c.d_rpole_orig, 13 * n, "rpole");
+  if (!st) st = dmalloc(c, &c.d_pole_local, 13 * n, "pole");
+  if (!st) st = dmalloc(c, &c.d_frames, 3 * n, "frames");
+  if (!st) st = dmalloc(c, &c.d_pos, n, "pos");
+  if (!st) st = dmalloc(c, &c.d_posf, n, "posf");
+  if (!st) st = dmalloc(c, &c.d_thole, n, "thole");
+  if (!st) st = dmalloc(c, &c.d_pol, n, "pol");
+  if (!st) st = dmalloc(c, &c.d_rpole, 10 * n, "rpole sorted");
+  if (!st) st = dmalloc(c, &c.d_pos_built, n, "pos built");
+  if (!st) st = dmalloc(c, &c.d_nnb, n, "nnb");
+  if (!st) st = dmalloc(c, &c.d_nb, (size_t)c.maxnb * npad, "nb");
+  if (!st) st = dmalloc(c, &c.d_npr, n, "npr");
+  if (!st) st = dmalloc(c, &c.d_pk, (size_t)c.maxpr * npad, "pk");
+  if (!st) st = cuda_status(cudaMalloc(&c.d_pc3, esz * c.maxpr * npad), &c, "pc3");
+  if (!st) st = cuda_status(cudaMalloc(&c.d_pc5, esz * c.maxpr * npad), &c, "pc5");
+  double** vecs[] = {&c.d_ef, &c.d_mu, &c.d_res, &c.d_h, &c.d_pp, &c.d_zr, &c.d_dip, &c.d_tmp6, &c.d_tmp6b};
+  for (double** v : vecs)
+    if (!st) st = dmalloc(c, v, 6 * n, "vectors");
+  if (!st) st = dmalloc(c, &c.d_cphi, 4 * n, "cphi");
+  if (!st) st = dmalloc(c, &c.d_vecf, 6 * n, "vecf");
+  if (!st) st = dmalloc(c, &c.d_partials, (size_t)(c.nblk_reduce + 8) * 4, "partials");
+  if (!st) st = dmalloc(c, &c.d_cg, 1, "cg");
+  if (!st) st = dmalloc(c, &c.d_flags, 1, "flags");
+  if (!st) st = cuda_status(cudaMallocHost((void**)&c.h_cg, sizeof(CgScalars)), &c, "pinned");
+  if (!st) st = cuda_status(cudaMallocHost((void**)&c.h_flags, sizeof(int)), &c, "pinned");
+  if (!st) {
+    cudaMemset(c.d_flags, 0, sizeof(int));
+    cudaMemset(c.d_cg, 0, sizeof(CgScalars));
+    cudaMemset(c.d_mu, 0, sizeof(double) * 6 * n);
+    st = pme_init(c);
+  }
+  if (!st) {
+    // default: no special pairs
+    c.sp_off.assign(n + 1, 0);
+    st = upload_special_pairs(c);
+  }
+  if (st) {
+    fprintf(stderr, "thp_ctx_create: %s\n", c.last_msg.c_str());
+    free_ctx(c);
+    delete h;
+    return st;
+  }
+  *out = h;
+  return THP_OK;
+}
+
+int thp_ctx_destroy(thp_ctx* h) {
+  if (!h) return THP_E_INVALID;
+  cudaSetDevice(h->c.device);
+  cudaStreamSynchronize(h->c.stream);
+  if (g_current == h) g_current = nullptr;
+  free_ctx(h->c);
+  delete h;
+  return THP_OK;
+}
+
+int thp_set_stream(thp_ctx* h, void* stream) {
+  if (!h) return THP_E_INVALID;
+  Ctx& c = h->c;
+  cudaStreamSynchronize(c.stream);
+  if (c.own_stream) cudaStreamDestroy(c.stream);
+  c.stream = (cudaStream_t)stream;
+  c.own_stream = false;
+  if (c.have_plan) cufftSetStream(c.plan, c.stream);
+  return THP_OK;
+}
+
+int thp_set_params(thp_ctx* h, const double* polarity, const double* thole, const double* pdamp) {
+  if (!h || !polarity || !thole || !pdamp) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  const size_t n = c.n;
+  c.h_polarity.assign(polarity, polarity + n);
+  c.h_thole.assign(thole, thole + n);
+  c.h_pdamp.assign(pdamp, pdamp + n);
+  cudaMemcpyAsync(c.d_par_orig, pdamp, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(c.d_par_orig + n, thole, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(c.d_par_orig + 2 * n, polarity, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
+  c.have_params = true;
+  h->pos_dirty = true;
+  c.have_coef = false;
+  h->field_valid = false;
+  return cuda_status(cudaStreamSynchronize(c.stream), &c, "set params");
+}
+
+int thp_set_connectivity(thp_ctx* h, const int* const* off, const int* const* idx, const double* scales) {
+  if (!h || !scales) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  std::memcpy(c.scales, scales, sizeof(c.scales));
+  build_special_pairs(c, off, idx, scales);
+  c.have_conn = true;
+  c.have_coef = false;
+  h->field_valid = false;
+  return upload_special_pairs(c);
+}
+
+int thp_set_positions(thp_ctx* h, const double* x, const double* y, const double* z) {
+  if (!h || !x || !y || !z) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  const size_t n = c.n;
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(z[i])) return THP_E_INVALID;
+  cudaMemcpyAsync(c.d_xyz_orig, x, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(c.d_xyz_orig + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(c.d_xyz_orig + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
+  c.have_pos = true;
+  h->pos_dirty = true;
+  h->field_valid = false;
+  c.have_coef = false;
+  if (c.have_frames) h->rpole_dirty = true;
+  return cuda_status(cudaGetLastError(), &c, "set positions");
+}
+
+int thp_set_rpole(thp_ctx* h, const double* rpole) {
+  if (!h || !rpole) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  cudaMemcpyAsync(c.d_rpole_orig, rpole, sizeof(double) * 13 * c.n, cudaMemcpyHostToDevice, c.stream);
+  c.have_rpole = true;
+  c.have_frames = false;
+  h->rpole_dirty = true;
+  h->field_valid = false;
+  return cuda_status(cudaGetLastError(), &c, "set rpole");
+}
+
+int thp_set_frames(thp_ctx* h, const double* pole, const int* zaxis, const int* xaxis, const int* axt) {
+  if (!h || !pole || !zaxis || !xaxis || !axt) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  const int n = c.n;
+  std::vector<int> fr(3 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    if (zaxis[i] < 0 || zaxis[i] >= n || xaxis[i] < 0 || xaxis[i] >= n || (axt[i] != 1 && axt[i] != 2))
+      return THP_E_INVALID;
+    fr[3 * i] = zaxis[i];
+    fr[3 * i + 1] = xaxis[i];
+    fr[3 * i + 2] = axt[i];
+  }
+  cudaMemcpy(c.d_pole_local, pole, sizeof(double) * 13 * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(c.d_frames, fr.data(), sizeof(int) * 3 * n, cudaMemcpyHostToDevice);
+  c.have_frames = true;
+  h->rpole_dirty = true;
+  h->field_valid = false;
+  return cuda_status(cudaGetLastError(), &c, "set frames");
+}
+
+int thp_set_guess(thp_ctx* h, const double* mu) {
+  if (!h || !mu) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st = ensure_list(h, false);
+  if (st) return st;
+  cudaMemcpyAsync(c.d_tmp6, mu, sizeof(double) * 6 * c.n, cudaMemcpyHostToDevice, c.stream);
+  if ((st = launch_to_sorted6(c, c.d_tmp6, c.d_mu, 2))) return st;
+  h->guess_uploaded = true;
+  return cuda_status(cudaStreamSynchronize(c.stream), &c, "set guess");
+}
+
+int thp_nblist(thp_ctx* h) {
+  if (!h) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  if (!c.have_params) return THP_E_STATE;
+  int st = ensure_list(h, false);
+  if (st) return st;
+  return cuda_status(cudaStreamSynchronize(c.stream), &c, "nblist");
+}
+
+int thp_invalidate_list(thp_ctx* h) {
+  if (!h) return THP_E_INVALID;
+  h->c.have_list = false;
+  h->c.have_coef = false;
+  h->field_valid = false;
+  return THP_OK;
+}
+
+int thp_profile(thp_ctx* h, int enable, double* ms_total, int* launches) {
+  if (!h) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  if (ms_total || launches) {
+    int st = cuda_status(cudaStreamSynchronize(c.stream), &c, "profile");
+    if (st) return st;
+    double tot = 0.0;
+    for (size_t q = 0; q + 1 < c.prof_events.size(); q += 2) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, c.prof_events[q], c.prof_events[q + 1]);
+      tot += ms;
+    }
+    if (ms_total) *ms_total = tot;
+    if (launches) *launches = (int)(c.prof_events.size() / 2);
+  }
+  for (cudaEvent_t e : c.prof_events) cudaEventDestroy(e);
+  c.prof_events.clear();
+  c.profiling = enable != 0;
+  return THP_OK;
+}
+
+int thp_solve(thp_ctx* h, int guess, thp_solve_info* info) {
+  if (!h) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  if (!c.have_params || !c.have_pos || (!c.have_rpole && !c.have_frames)) return THP_E_STATE;
+  if (guess == THP_GUESS_PREVIOUS && !c.have_dipoles) guess = THP_GUESS_DIRECT;
+  if (guess == THP_GUESS_HOST && !h->guess_uploaded) return THP_E_STATE;
+  cudaEventRecord(c.ev0, c.stream);
+  int st = compute_field(h);
+  if (st) return st;
+  st = run_pcg(c, guess);
+  h->guess_uploaded = false;
+  if (st && st != THP_E_NOT_CONVERGED) return st;
+  int st2 = launch_epol(c);
+  if (st2) return st2;
+  cudaEventRecord(c.ev1, c.stream);
+  cudaMemcpyAsync(c.h_cg, c.d_cg, sizeof(CgScalars), cudaMemcpyDeviceToHost, c.stream);
+  if ((st2 = cuda_status(cudaStreamSynchronize(c.stream), &c, "solve"))) return st2;
+  h->solved_once = true;
+  if (info) {
+    info->niter = c.h_cg->niter;
+    info->converged = c.h_cg->converged;
+    info->resnrm = c.h_cg->resnrm;
+    info->epol = c.h_cg->epol;
+    info->ene[0] = c.h_cg->ene[0] * kElectric;
+    info->ene[1] = c.h_cg->ene[1] * kElectric;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c.ev0, c.ev1);
+    info->ms_total = ms;
+  }
+  return st;
+}
+
+int thp_get_dipoles(thp_ctx* h, double* uind, double* uinp) {
+  if (!h) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (!c.have_dipoles) return THP_E_STATE;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st = launch_to_orig6(c, c.d_mu, c.d_tmp6, 2);
+  if (st) return st;
+  std::vector<double> buf((size_t)6 * c.n);
+  cudaMemcpyAsync(buf.data(), c.d_tmp6, sizeof(double) * 6 * c.n, cudaMemcpyDeviceToHost, c.stream);
+  if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "get dipoles"))) return st;
+  for (int i = 0; i < c.n; ++i)
+    for (int j = 0; j < 3; ++j) {
+      if (uind) uind[3 * i + j] = buf[6 * (size_t)i + j];
+      if (uinp) uinp[3 * i + j] = buf[6 * (size_t)i + 3 + j];
+    }
+  return THP_OK;
+}
+
+int thp_get_field(thp_ctx* h, double* ef) {
+  if (!h || !ef) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (!h->field_valid) return THP_E_STATE;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st = launch_to_orig6(c, c.d_ef, c.d_tmp6, 2);
+  if (st) return st;
+  cudaMemcpyAsync(ef, c.d_tmp6, sizeof(double) * 6 * c.n, cudaMemcpyDeviceToHost, c.stream);
+  return cuda_status(cudaStreamSynchronize(c.stream), &c, "get field");
+}
+
+int thp_get_rpole(thp_ctx* h, double* rpole) {
+  if (!h || !rpole) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st = ensure_rpole(h);
+  if (st) return st;
+  cudaMemcpyAsync(rpole, c.d_rpole_orig, sizeof(double) * 13 * c.n, cudaMemcpyDeviceToHost, c.stream);
+  return cuda_status(cudaStreamSynchronize(c.stream), &c, "get rpole");
+}
+
+int thp_get_nblist(thp_ctx* h, int maxelst, int* nelst, int* elst) {
+  if (!h || !nelst || !elst || maxelst <= 0) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st = ensure_list(h, false);
+  if (st) return st;
+  int *dn = nullptr, *de = nullptr;
+  if ((st = dmalloc(c, &dn, c.n, "export"))) return st;
+  if ((st = dmalloc(c, &de, (size_t)c.n * maxelst, "export"))) {
+    cudaFree(dn);
+    return st;
+  }
+  st = launch_export_list(c, maxelst, dn, de);
+  if (!st) {
+    cudaMemcpyAsync(nelst, dn, sizeof(int) * c.n, cudaMemcpyDeviceToHost, c.stream);
+    cudaMemcpyAsync(elst, de, sizeof(int) * (size_t)c.n * maxelst, cudaMemcpyDeviceToHost, c.stream);
+    st = check_flags(h);
+  }
+  cudaFree(dn);
+  cudaFree(de);
+  return st;
+}
+
+int thp_tmatxb(thp_ctx* h, int nrhs, int dodiag, const double* mu, double* efi) {
+  if (!h || !mu || !efi || nrhs < 1 || nrhs > 2) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st = ensure_coef(h);
+  if (st) return st;
+  const size_t n = c.n;
+  cudaMemcpyAsync(c.d_tmp6b, mu, sizeof(double) * 3 * nrhs * n, cudaMemcpyHostToDevice, c.stream);
+  if ((st = launch_to_sorted6(c, c.d_tmp6b, c.d_tmp6, nrhs))) return st;
+  if ((st = launch_tmatxb(c, c.d_tmp6, c.d_dip, dodiag != 0))) return st;
+  if ((st = launch_to_orig6(c, c.d_dip, c.d_tmp6b, nrhs))) return st;
+  cudaMemcpyAsync(efi, c.d_tmp6b, sizeof(double) * 3 * nrhs * n, cudaMemcpyDeviceToHost, c.stream);
+  return cuda_status(cudaStreamSynchronize(c.stream), &c, "tmatxb");
+}
+
+int thp_efld0_direct(thp_ctx* h, int nrhs, double* ef) {
+  if (!h || !ef || nrhs < 1 || nrhs > 2) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st;
+  if ((st = ensure_rpole(h))) return st;
+  if ((st = ensure_list(h, false))) return st;
+  if ((st = launch_efld0_coef(c, true))) return st;
+  h->field_valid = false;  // d_ef holds only the direct part now
+  if ((st = check_flags(h))) return st;
+  if ((st = launch_to_orig6(c, c.d_ef, c.d_tmp6, 2))) return st;
+  std::vector<double> buf((size_t)6 * c.n);
+  cudaMemcpyAsync(buf.data(), c.d_tmp6, sizeof(double) * 6 * c.n, cudaMemcpyDeviceToHost, c.stream);
+  if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "efld0 direct"))) return st;
+  for (int i = 0; i < c.n; ++i)
+    for (int r = 0; r < nrhs; ++r)
+      for (int j = 0; j < 3; ++j) ef[((size_t)i * nrhs + r) * 3 + j] += buf[6 * (size_t)i + 3 * r + j];
+  return THP_OK;
+}
+
+int thp_efld0_recip(thp_ctx* h, double* cphi) {
+  if (!h || !cphi) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st;
+  if ((st = ensure_rpole(h))) return st;
+  if ((st = ensure_list(h, false))) return st;
+  double* d10 = nullptr;
+  if ((st = dmalloc(c, &d10, (size_t)10 * c.n, "cphi10"))) return st;
+  st = launch_efld0_recip_ex(c, d10, false);
+  std::vector<double> buf((size_t)10 * c.n);
+  std::vector<int> perm(c.n);
+  if (!st) {
+    cudaMemcpyAsync(buf.data(), d10, sizeof(double) * 10 * c.n, cudaMemcpyDeviceToHost, c.stream);
+    cudaMemcpyAsync(perm.data(), c.d_perm, sizeof(int) * c.n, cudaMemcpyDeviceToHost, c.stream);
+    st = cuda_status(cudaStreamSynchronize(c.stream), &c, "efld0 recip");
+  }
+  cudaFree(d10);
+  if (st) return st;
+  for (int s = 0; s < c.n; ++s) std::memcpy(cphi + (size_t)perm[s] * 10, &buf[(size_t)s * 10], sizeof(double) * 10);
+  return THP_OK;
+}
+
+int thp_tmatxbrecip(thp_ctx* h, int nrhs, const double* mu, double* dipfield) {
+  if (!h || !mu || !dipfield || nrhs < 1 || nrhs > 2) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st = ensure_list(h, false);
+  if (st) return st;
+  const size_t n = c.n;
+  cudaMemcpyAsync(c.d_tmp6b, mu, sizeof(double) * 3 * nrhs * n, cudaMemcpyHostToDevice, c.stream);
+  if ((st = launch_to_sorted6(c, c.d_tmp6b, c.d_tmp6, nrhs))) return st;
+  if ((st = launch_pme_dipole(c, c.d_tmp6, c.d_dip, 0))) return st;
+  if ((st = launch_to_orig6(c, c.d_dip, c.d_tmp6b, nrhs))) return st;
+  cudaMemcpyAsync(dipfield, c.d_tmp6b, sizeof(double) * 3 * nrhs * n, cudaMemcpyDeviceToHost, c.stream);
+  return cuda_status(cudaStreamSynchronize(c.stream), &c, "tmatxbrecip");
+}
+
+int thp_solve_host(thp_ctx* h, const double* x, const double* y, const double* z, const double* rpole,
+                   double* uind, double* uinp, thp_solve_info* info) {
+  int st = thp_set_positions(h, x, y, z);
+  if (st) return st;
+  if (rpole && (st = thp_set_rpole(h, rpole))) return st;
+  st = thp_solve(h, THP_GUESS_DIRECT, info);
+  if (st && st != THP_E_NOT_CONVERGED) return st;
+  int st2 = thp_get_dipoles(h, uind, uinp);
+  return st2 ? st2 : st;
+}
+
+// ---- Fortran drop-ins ------------------------------------------------------
+
+int thp_bind_state(thp_ctx* h, double* x, double* y, double* z, double* rpole, double* uind, double* uinp,
+                   int* nelst, int* elst, int maxelst, double* ep) {
+  if (!h) return THP_E_INVALID;
+  Ctx& c = h->c;
+  c.bx = x;
+  c.by = y;
+  c.bz = z;
+  c.brpole = rpole;
+  c.buind = uind;
+  c.buinp = uinp;
+  c.bnelst = nelst;
+  c.belst = elst;
+  c.bmaxelst = maxelst;
+  c.bep = ep;
+  g_current = h;
+  return THP_OK;
+}
+
+int thp_last_error(void) { return g_last_error; }
+
+static int sync_bound_inputs(thp_ctx* h) {
+  Ctx& c = h->c;
+  if (!c.bx || !c.by || !c.bz) return THP_E_STATE;
+  int st = thp_set_positions(h, c.bx, c.by, c.bz);
+  if (st) return st;
+  if (c.brpole) st = thp_set_rpole(h, c.brpole);
+  return st;
+}
+
+void mlistcell_(void) {
+  thp_ctx* h = g_current;
+  if (!h) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  int st = sync_bound_inputs(h);
+  if (!st) st = ensure_list(h, true);
+  if (!st && h->c.bnelst && h->c.belst) {
+    st = thp_get_nblist(h, h->c.bmaxelst, h->c.bnelst, h->c.belst);
+    if (!st) {  // Fortran pole indices are 1-based
+      const size_t n = h->c.n, m = h->c.bmaxelst;
+      for (size_t i = 0; i < n; ++i)
+        for (int j = 0; j < h->c.bnelst[i]; ++j) h->c.belst[i * m + j] += 1;
+    }
+  }
+  g_last_error = st;
+}
+
+void vlistcell_(void) { mlistcell_(); }
+
+void newinduce_pme2_(void) {
+  thp_ctx* h = g_current;
+  if (!h) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  int st = sync_bound_inputs(h);
+  thp_solve_info info;
+  if (!st) st = thp_solve(h, THP_GUESS_DIRECT, &info);
+  if ((!st || st == THP_E_NOT_CONVERGED) && h->c.buind) {
+    int st2 = thp_get_dipoles(h, h->c.buind, h->c.buinp);
+    if (st2) st = st2;
+  }
+  g_last_error = st;
+}
+
+void epolar_(void) {
+  thp_ctx* h = g_current;
+  if (!h) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  int st = sync_bound_inputs(h);
+  thp_solve_info info;
+  if (!st) st = thp_solve(h, THP_GUESS_DIRECT, &info);
+  if (!st || st == THP_E_NOT_CONVERGED) {
+    if (h->c.bep) *h->c.bep = info.epol;
+    if (h->c.buind) thp_get_dipoles(h, h->c.buind, h->c.buinp);
+  }
+  g_last_error = st;
+}
+
+void tmatxb_pme_(const int* nrhs, const int* dodiag, const double* mu, double* efi) {
+  if (!g_current) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  g_last_error = thp_tmatxb(g_current, *nrhs, *dodiag, mu, efi);
+}
+
+void efld0_direct_(const int* nrhs, double* ef) {
+  if (!g_current) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  g_last_error = thp_efld0_direct(g_current, *nrhs, ef);
+}
+
+void efld0_recip_(double* cphi) {
+  if (!g_current) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  g_last_error = thp_efld0_recip(g_current, cphi);
+}
+
+void tmatxbrecip_(const double* mu, const double* murec, const int* nrhs, double* dipfield, double* dipfieldbis) {
+  (void)murec;
+  (void)dipfieldbis;
+  if (!g_current) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  g_last_error = thp_tmatxbrecip(g_current, *nrhs, mu, dipfield);
+}
+
+void inducepcg_pme2_(void (*matvec)(const int*, const int*, const double*, double*), const int* nrhs,
+                     const int* precnd, const double* ef, double* mu, double* murec) {
+  (void)murec;
+  thp_ctx* h = g_current;
+  if (!h || !matvec || !nrhs || !ef || !mu) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  Ctx& c = h->c;
+  const int nr = *nrhs;
+  const size_t n = c.n, nv = n * 3 * nr;
+  int st = ensure_coef(h);
+  if (st) {
+    g_last_error = st;
+    return;
+  }
+  if (matvec == tmatxb_pme_ && nr == 2 && *precnd) {
+    // device loop on the caller's E0 and guess
+    cudaMemcpyAsync(c.d_tmp6, ef, sizeof(double) * nv, cudaMemcpyHostToDevice, c.stream);
+    st = launch_to_sorted6(c, c.d_tmp6, c.d_ef, 2);
+    cudaMemcpyAsync(c.d_tmp6b, mu, sizeof(double) * nv, cudaMemcpyHostToDevice, c.stream);
+    if (!st) st = launch_to_sorted6(c, c.d_tmp6b, c.d_mu, 2);
+    if (!st) st = run_pcg(c, THP_GUESS_HOST);
+    if (!st || st == THP_E_NOT_CONVERGED) {
+      int st2 = launch_to_orig6(c, c.d_mu, c.d_tmp6, 2);
+      cudaMemcpyAsync(mu, c.d_tmp6, sizeof(double) * nv, cudaMemcpyDeviceToHost, c.stream);
+      cudaStreamSynchronize(c.stream);
+      if (st2) st = st2;
+    }
+    h->field_valid = false;
+    g_last_error = st;
+    return;
+  }
+  // host loop with the caller's matvec (newinduce_pme2.f:285-636, same recurrences)
+  std::vector<double> res(nv), hh(nv), pp(nv), zr(nv), dip(nv), diag(n);
+  for (size_t i = 0; i < n; ++i) {
+    double p = c.h_polarity.empty() ? 1.0 : c.h_polarity[i];
+    diag[i] = *precnd ? (p == 0.0 ? kTinyPol : p) : 1.0;
+  }
+  const double a = c.cfg.aewald, term = (4.0 / 3.0) * a * a * a / kSqrtPi;
+  const int t = 1;
+  auto recip = [&](const double* v) { return thp_tmatxbrecip(h, nr, v, dip.data()); };
+  if ((st = recip(mu))) {
+    g_last_error = st;
+    return;
+  }
+  matvec(&nr, &t, mu, hh.data());
+  double ggold[2] = {0, 0}, gg[2], ggnew[2];
+  for (size_t i = 0; i < n; ++i)
+    for (int k = 0; k < nr; ++k)
+      for (int j = 0; j < 3; ++j) {
+        size_t q = (i * nr + k) * 3 + j;
+        hh[q] = hh[q] + dip[q] - term * mu[q];
+        res[q] = ef[q] - hh[q];
+        zr[q] = diag[i] * res[q];
+        pp[q] = zr[q];
+        ggold[k] += res[q] * zr[q];
+      }
+  st = THP_E_NOT_CONVERGED;
+  for (int it = 1; it <= c.cfg.politer; ++it) {
+    if (recip(pp.data())) break;
+    matvec(&nr, &t, pp.data(), hh.data());
+    gg[0] = gg[1] = 0.0;
+    for (size_t i = 0; i < n; ++i)
+      for (int k = 0; k < nr; ++k)
+        for (int j = 0; j < 3; ++j) {
+          size_t q = (i * nr + k) * 3 + j;
+          hh[q] = hh[q] + dip[q] - term * pp[q];
+          gg[k] += pp[q] * hh[q];
+        }
+    bool zero = false;
+    for (int k = 0; k < nr; ++k) zero |= (gg[k] == 0.0);
+    if (zero) {
+      st = THP_OK;
+      break;
+    }
+    double al[2] = {ggold[0] / gg[0], nr > 1 ? ggold[1] / gg[1] : 0.0};
+    ggnew[0] = ggnew[1] = 0.0;
+    for (size_t i = 0; i < n; ++i)
+      for (int k = 0; k < nr; ++k)
+        for (int j = 0; j < 3; ++j) {
+          size_t q = (i * nr + k) * 3 + j;
+          mu[q] += al[k] * pp[q];
+          res[q] -= al[k] * hh[q];
+          zr[q] = diag[i] * res[q];
+          ggnew[k] += res[q] * zr[q];
+        }
+    double resnrm = 0.0;
+    for (int k = 0; k < nr; ++k) resnrm = std::max(resnrm, std::sqrt(ggnew[k] / (double)(3 * n)));
+    for (size_t i = 0; i < n; ++i)
+      for (int k = 0; k < nr; ++k)
+        for (int j = 0; j < 3; ++j) {
+          size_t q = (i * nr + k) * 3 + j;
+          pp[q] = zr[q] + ggnew[k] / ggold[k] * pp[q];
+        }
+    ggold[0] = ggnew[0];
+    ggold[1] = ggnew[1];
+    if (resnrm < c.cfg.poleps) {
+      st = THP_OK;
+      break;
+    }
+  }
+  g_last_error = st;
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+// context.h -- per-system device state of the polarization library (internal).
+#pragma once
+
+#include <cufft.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace thp {
+
+// Scalars of the device-resident CG (newinduce_pme2.f:308-312), one per RHS.
+struct CgScalars {
+  double ggold[2];
+  double gg[2];
+  double ggnew[2];
+  double ene[2];
+  double alpha[2];
+  double beta[2];
+  double resnrm;
+  double epol;
+  double epart;  // spare accumulator
+  int converged;
+  int stop;      // 1: converged or failed, later kernels return at once
+  int niter;
+  int status;    // THP_* code raised on the device
+  unsigned counter[4];  // last-block counters of the grid reductions
+};
+
+// device error flags (bit set)
+enum : int { DEV_LIST_OVERFLOW = 1, DEV_PAIR_OVERFLOW = 2, DEV_NAN = 4 };
+
+struct Ctx {
+  thp_config cfg{};
+  int n = 0, npad = 0;
+  int mixed = 0;
+  Box box{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // host copies (original atom order)
+  std::vector<double> h_polarity, h_thole, h_pdamp;
+  bool have_params = false, have_pos = false, have_rpole = false, have_conn = false;
+  bool have_frames = false;
+  std::vector<int> sp_off;     // special (scaled) pairs, original indices, CSR
+  std::vector<int> sp_k;
+  std::vector<double> sp_s;    // (d, p, u) per entry
+  double scales[16] = {0};
+
+  // cell grid of the list build
+  int nc[3] = {1, 1, 1};
+  int ncell = 1;
+  int* d_cell_count = nullptr;
+  int* d_cell_start = nullptr;
+  int* d_cell_fill = nullptr;
+  int* d_atom_cell = nullptr;   // original order
+  int* d_scell = nullptr;       // cell of sorted atom
+
+  // permutation
+  int* d_perm = nullptr;   // sorted -> original
+  int* d_iperm = nullptr;  // original -> sorted
+  bool have_perm = false;
+
+  // staging in original order
+  double* d_xyz_orig = nullptr;   // [3][n]
+  double* d_par_orig = nullptr;   // [3][n] pdamp, thole, polarity
+  double* d_rpole_orig = nullptr; // [n][13]
+  double* d_pole_local = nullptr; // [n][13]
+  int* d_frames = nullptr;        // [n][3] zaxis, xaxis, axt (original indices)
+
+  // sorted per-atom data
+  double4* d_pos = nullptr;       // x, y, z, pdamp
+  float4* d_posf = nullptr;       // mixed form positions (x,y,z wrapped, pdamp)
+  double* d_thole = nullptr;
+  double* d_pol = nullptr;
+  double* d_rpole = nullptr;      // [n][10]: q, d(3), Qxx,Qxy,Qxz,Qyy,Qyz,Qzz
+  int* d_sp_off = nullptr;        // special pairs, ORIGINAL indices, CSR [n+1]
+  int* d_sp_k = nullptr;
+  double* d_sp_s = nullptr;       // (d, p, u) scale per entry
+  double4* d_pos_built = nullptr; // positions at the last list build
+
+  // full neighbor list within ewaldcut+lbuffer (slot-major: nb[s*npad+i])
+  int maxnb = 0;
+  int* d_nnb = nullptr;
+  int* d_nb = nullptr;
+  bool have_list = false;
+
+  // interacting pairs within ewaldcut with mutual-field coefficients
+  int maxpr = 0;
+  int* d_npr = nullptr;
+  int* d_pk = nullptr;
+  void* d_pc3 = nullptr;   // double or float
+  void* d_pc5 = nullptr;
+  bool have_coef = false;
+
+  // PME
+  int nfft[3] = {0, 0, 0};
+  size_t ngrid = 0;
+  cufftHandle plan = 0;
+  bool have_plan = false;
+  void* d_grid = nullptr;  // cufftDoubleComplex or cufftComplex
+  void* d_qfac = nullptr;  // double or float
+  double a_frac[3] = {0, 0, 0};  // nfft_d * recip(d,d)
+
+  // CG vectors, sorted order, [n][6] = (d xyz, p xyz)
+  double* d_ef = nullptr;
+  double* d_mu = nullptr;
+  double* d_res = nullptr;
+  double* d_h = nullptr;
+  double* d_pp = nullptr;
+  double* d_zr = nullptr;
+  double* d_dip = nullptr;
+  double* d_cphi = nullptr;   // [n][4] permanent potential and gradient (Cartesian)
+  float* d_vecf = nullptr;    // mixed form matvec input [n][6]
+  double* d_tmp6 = nullptr;   // [n][6] original-order staging for host I/O
+  double* d_tmp6b = nullptr;
+  bool have_dipoles = false;
+
+  // reductions
+  double* d_partials = nullptr;  // [blocks][8]
+  int nblk_reduce = 0;
+  CgScalars* d_cg = nullptr;
+  CgScalars* h_cg = nullptr;     // pinned mirror
+  int* d_flags = nullptr;        // device error bits
+  int* h_flags = nullptr;        // pinned
+
+  // Fortran binding
+  double *bx = nullptr, *by = nullptr, *bz = nullptr, *brpole = nullptr;
+  double *buind = nullptr, *buinp = nullptr, *bep = nullptr;
+  int *bnelst = nullptr, *belst = nullptr;
+  int bmaxelst = 0;
+
+  // optional event pairs around the fused CG matvec launches
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_events;
+
+  std::string last_msg;
+};
+
+}  // namespace thp

@@ -1,0 +1,40 @@
+// kernels.h -- host launchers of the device kernels (internal).
+#pragma once
+
+#include "context.h"
+
+namespace thp {
+
+// nblist.cu
+int launch_sort_atoms(Ctx& c);          // cell sort, permutation, sorted copies
+int launch_gather_sorted(Ctx& c);       // positions/params/rpole into sorted order
+int launch_build_list(Ctx& c);          // full list within ewaldcut + lbuffer
+int launch_export_list(Ctx& c, int maxelst, int* d_nelst, int* d_elst);
+int launch_rotpole(Ctx& c);             // local-frame multipoles -> d_rpole_orig
+int launch_max_displacement(Ctx& c, double* h_out);
+
+// realspace.cu
+int launch_efld0_coef(Ctx& c, bool with_field);  // direct field into d_ef, coefficients
+int launch_tmatxb(Ctx& c, const double* d_in, double* d_out, bool dodiag);  // sorted [n][6]
+
+// pme.cu
+int pme_init(Ctx& c);
+void pme_free(Ctx& c);
+int launch_efld0_recip(Ctx& c);         // d_cphi and E0 completion
+int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0);
+int zero_grid(Ctx& c);
+struct PmeGeom;
+PmeGeom pme_geom(const Ctx& c);
+int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode);
+
+// solver.cu
+int run_pcg(Ctx& c, int guess);
+int launch_epol(Ctx& c);
+
+// reorder helpers (solver.cu)
+int launch_to_sorted6(Ctx& c, const double* d_orig, double* d_sorted, int nrhs);
+int launch_to_orig6(Ctx& c, const double* d_sorted, double* d_orig, int nrhs);
+
+int cuda_status(cudaError_t e, Ctx* c, const char* what);
+
+}  // namespace thp

@@ -1,0 +1,468 @@
+// pme.cu -- smooth PME for the permanent field and the dipole matvec.
+//
+// efld0_recip (newinduce_pme.f:1671-1917) and tmatxbrecip (:1919-2128):
+// B-splines recomputed per pass from positions (bsplgen, pmestuff.f:64),
+// spread with global atomics into one complex grid (d dipoles in Re, p in Im,
+// as qgrid2in_2d), cuFFT forward / influence function qfac / cuFFT backward
+// (unnormalised, fft_mpi.f90:65,115), and a gather of the potential
+// derivatives (fphi_mpole_site :453, fphi_uind_site :746).  Orthogonal boxes:
+// the fractional <-> Cartesian matrices reduce to a_d = nfft_d * recip(d,d).
+#include <vector>
+
+#include "kernels.h"
+#include "pme_dev.cuh"
+
+namespace thp {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+__device__ __forceinline__ void grid_add(cufftDoubleComplex* g, size_t idx, double re, double im) {
+  atomicAdd(&g[idx].x, re);
+  atomicAdd(&g[idx].y, im);
+}
+__device__ __forceinline__ void grid_add(cufftComplex* g, size_t idx, float re, float im) {
+  atomicAdd(reinterpret_cast<float2*>(&g[idx]), make_float2(re, im));
+}
+__device__ __forceinline__ void grid_add_re(cufftDoubleComplex* g, size_t idx, double re) {
+  atomicAdd(&g[idx].x, re);
+}
+__device__ __forceinline__ void grid_add_re(cufftComplex* g, size_t idx, float re) { atomicAdd(&g[idx].x, re); }
+
+// grid_mpole_site (pmestuff.f:163-278) for every site; rpole10 sorted
+template <typename T>
+__global__ void k_spread_mpole(int n, PmeGeom g, const double4* __restrict__ pos, const double* __restrict__ rp,
+                               typename Cplx<T>::type* __restrict__ grid) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 p = pos[i];
+  T tx[kBs][3], ty[kBs][3], tz[kBs][3];
+  int gx = bspline_axis<3, T>(p.x, g.recip[0], g.n1, tx);
+  int gy = bspline_axis<3, T>(p.y, g.recip[1], g.n2, ty);
+  int gz = bspline_axis<3, T>(p.z, g.recip[2], g.n3, tz);
+  const double* r = rp + (size_t)i * 10;
+  // cmp (newinduce_pme.f:1750-1759) -> fmp via cart_to_frac (pmestuff.f:1131)
+  T f[10];
+  f[0] = (T)r[0];
+  f[1] = (T)(g.a[0] * r[1]);
+  f[2] = (T)(g.a[1] * r[2]);
+  f[3] = (T)(g.a[2] * r[3]);
+  f[4] = (T)(g.a[0] * g.a[0] * r[4]);
+  f[5] = (T)(g.a[1] * g.a[1] * r[7]);
+  f[6] = (T)(g.a[2] * g.a[2] * r[9]);
+  f[7] = (T)(g.a[0] * g.a[1] * (2.0 * r[5]));
+  f[8] = (T)(g.a[0] * g.a[2] * (2.0 * r[6]));
+  f[9] = (T)(g.a[1] * g.a[2] * (2.0 * r[8]));
+#pragma unroll
+  for (int c = 0; c < kBs; ++c) {
+    size_t kk = (size_t)wrapk(gz + c, g.n3);
+    T v0 = tz[c][0], v1 = tz[c][1], v2 = tz[c][2];
+#pragma unroll
+    for (int b = 0; b < kBs; ++b) {
+      size_t jj = (size_t)wrapk(gy + b, g.n2);
+      T u0 = ty[b][0], u1 = ty[b][1], u2 = ty[b][2];
+      T term0 = f[0] * u0 * v0 + f[2] * u1 * v0 + f[3] * u0 * v1 + f[5] * u2 * v0 + f[6] * u0 * v2 + f[9] * u1 * v1;
+      T term1 = f[1] * u0 * v0 + f[7] * u1 * v0 + f[8] * u0 * v1;
+      T term2 = f[4] * u0 * v0;
+      size_t row = (kk * g.n2 + jj) * g.n1;
+#pragma unroll
+      for (int a = 0; a < kBs; ++a) {
+        int ii = wrapk(gx + a, g.n1);
+        grid_add_re(grid, row + ii, term0 * tx[a][0] + term1 * tx[a][1] + term2 * tx[a][2]);
+      }
+    }
+  }
+}
+
+// grid_uind_site (pmestuff.f:280-405); d dipoles in Re, p dipoles in Im.
+// mode 1 first forms pp = zr + beta*pp (inducepcg_pme2.f:553-559) and writes it.
+template <typename T>
+__global__ void k_spread_dip(int n, PmeGeom g, const double4* __restrict__ pos, double* __restrict__ vec,
+                             const double* __restrict__ zr, float* __restrict__ vecf, const CgScalars* __restrict__ cg,
+                             int mode, typename Cplx<T>::type* __restrict__ grid) {
+  if (mode == 1 && cg->stop) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v[6];
+  const double2* v2 = reinterpret_cast<const double2*>(vec + (size_t)i * 6);
+  double2 a0 = v2[0], a1 = v2[1], a2 = v2[2];
+  v[0] = a0.x; v[1] = a0.y; v[2] = a1.x; v[3] = a1.y; v[4] = a2.x; v[5] = a2.y;
+  if (mode == 1) {
+    const double2* z2 = reinterpret_cast<const double2*>(zr + (size_t)i * 6);
+    double2 b0 = z2[0], b1 = z2[1], b2 = z2[2];
+    double bd = cg->beta[0], bp = cg->beta[1];
+    v[0] = b0.x + bd * v[0];
+    v[1] = b0.y + bd * v[1];
+    v[2] = b1.x + bd * v[2];
+    v[3] = b1.y + bp * v[3];
+    v[4] = b2.x + bp * v[4];
+    v[5] = b2.y + bp * v[5];
+    double2* w2 = reinterpret_cast<double2*>(vec + (size_t)i * 6);
+    w2[0] = make_double2(v[0], v[1]);
+    w2[1] = make_double2(v[2], v[3]);
+    w2[2] = make_double2(v[4], v[5]);
+  }
+  if (vecf) {
+    float* o = vecf + (size_t)i * 6;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o[q] = (float)v[q];
+  }
+  double4 p = pos[i];
+  T tx[kBs][2], ty[kBs][2], tz[kBs][2];
+  int gx = bspline_axis<2, T>(p.x, g.recip[0], g.n1, tx);
+  int gy = bspline_axis<2, T>(p.y, g.recip[1], g.n2, ty);
+  int gz = bspline_axis<2, T>(p.z, g.recip[2], g.n3, tz);
+  T fd[3] = {(T)(g.a[0] * v[0]), (T)(g.a[1] * v[1]), (T)(g.a[2] * v[2])};
+  T fp[3] = {(T)(g.a[0] * v[3]), (T)(g.a[1] * v[4]), (T)(g.a[2] * v[5])};
+#pragma unroll
+  for (int c = 0; c < kBs; ++c) {
+    size_t kk = (size_t)wrapk(gz + c, g.n3);
+    T v0 = tz[c][0], v1 = tz[c][1];
+#pragma unroll
+    for (int b = 0; b < kBs; ++b) {
+      size_t jj = (size_t)wrapk(gy + b, g.n2);
+      T u0 = ty[b][0], u1 = ty[b][1];
+      T term01 = fd[1] * u1 * v0 + fd[2] * u0 * v1;
+      T term11 = fd[0] * u0 * v0;
+      T term02 = fp[1] * u1 * v0 + fp[2] * u0 * v1;
+      T term12 = fp[0] * u0 * v0;
+      size_t row = (kk * g.n2 + jj) * g.n1;
+#pragma unroll
+      for (int a = 0; a < kBs; ++a) {
+        int ii = wrapk(gx + a, g.n1);
+        grid_add(grid, row + ii, term01 * tx[a][0] + term11 * tx[a][1], term02 * tx[a][0] + term12 * tx[a][1]);
+      }
+    }
+  }
+}
+
+template <typename C, typename T>
+__global__ void k_qfac(size_t ng, const T* __restrict__ qfac, C* __restrict__ grid, const CgScalars* __restrict__ cg,
+                       int check_stop) {
+  if (check_stop && cg->stop) return;
+  size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (; q < ng; q += stride) {
+    T f = qfac[q];
+    C v = grid[q];
+    v.x *= f;
+    v.y *= f;
+    grid[q] = v;
+  }
+}
+
+// fphi_mpole_site (pmestuff.f:453-600) restricted to the 10 components of
+// cphi, then fphi_to_cphi_site (:1190) and the E0 assembly of
+// newinduce_pme2.f:133-148: ef -= cphi(2:4); ef += term * d_perm.
+template <typename T>
+__global__ void k_gather_mpole(int n, PmeGeom g, const double4* __restrict__ pos,
+                               const typename Cplx<T>::type* __restrict__ grid, const double* __restrict__ rp,
+                               double term, double* __restrict__ cphi4, double* __restrict__ cphi10,
+                               double* __restrict__ ef) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 p = pos[i];
+  T tx[kBs][3], ty[kBs][3], tz[kBs][3];
+  int gx = bspline_axis<3, T>(p.x, g.recip[0], g.n1, tx);
+  int gy = bspline_axis<3, T>(p.y, g.recip[1], g.n2, ty);
+  int gz = bspline_axis<3, T>(p.z, g.recip[2], g.n3, tz);
+  T tuv000 = 0, tuv100 = 0, tuv010 = 0, tuv001 = 0, tuv200 = 0, tuv020 = 0, tuv002 = 0, tuv110 = 0, tuv101 = 0,
+    tuv011 = 0;
+#pragma unroll
+  for (int c = 0; c < kBs; ++c) {
+    size_t kk = (size_t)wrapk(gz + c, g.n3);
+    T v0 = tz[c][0], v1 = tz[c][1], v2 = tz[c][2];
+    T tu00 = 0, tu10 = 0, tu01 = 0, tu20 = 0, tu11 = 0, tu02 = 0;
+#pragma unroll
+    for (int b = 0; b < kBs; ++b) {
+      size_t jj = (size_t)wrapk(gy + b, g.n2);
+      T u0 = ty[b][0], u1 = ty[b][1], u2 = ty[b][2];
+      T t0 = 0, t1 = 0, t2 = 0;
+      size_t row = (kk * g.n2 + jj) * g.n1;
+#pragma unroll
+      for (int a = 0; a < kBs; ++a) {
+        T tq = grid[row + wrapk(gx + a, g.n1)].x;
+        t0 += tq * tx[a][0];
+        t1 += tq * tx[a][1];
+        t2 += tq * tx[a][2];
+      }
+      tu00 += t0 * u0;
+      tu10 += t1 * u0;
+      tu01 += t0 * u1;
+      tu20 += t2 * u0;
+      tu11 += t1 * u1;
+      tu02 += t0 * u2;
+    }
+    tuv000 += tu00 * v0;
+    tuv100 += tu10 * v0;
+    tuv010 += tu01 * v0;
+    tuv001 += tu00 * v1;
+    tuv200 += tu20 * v0;
+    tuv020 += tu02 * v0;
+    tuv002 += tu00 * v2;
+    tuv110 += tu11 * v0;
+    tuv101 += tu10 * v1;
+    tuv011 += tu01 * v1;
+  }
+  double c1 = g.a[0] * (double)tuv100, c2 = g.a[1] * (double)tuv010, c3 = g.a[2] * (double)tuv001;
+  double* cp = cphi4 + (size_t)i * 4;
+  cp[0] = (double)tuv000;
+  cp[1] = c1;
+  cp[2] = c2;
+  cp[3] = c3;
+  if (cphi10) {
+    double* q = cphi10 + (size_t)i * 10;
+    q[0] = (double)tuv000;
+    q[1] = c1;
+    q[2] = c2;
+    q[3] = c3;
+    q[4] = g.a[0] * g.a[0] * (double)tuv200;
+    q[5] = g.a[1] * g.a[1] * (double)tuv020;
+    q[6] = g.a[2] * g.a[2] * (double)tuv002;
+    q[7] = g.a[0] * g.a[1] * (double)tuv110;
+    q[8] = g.a[0] * g.a[2] * (double)tuv101;
+    q[9] = g.a[1] * g.a[2] * (double)tuv011;
+  }
+  if (ef) {
+    const double* r = rp + (size_t)i * 10;
+    double* e = ef + (size_t)i * 6;
+    double cc[3] = {c1, c2, c3};
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      e[j] = (e[j] - cc[j]) + term * r[1 + j];
+      e[3 + j] = (e[3 + j] - cc[j]) + term * r[1 + j];
+    }
+  }
+}
+
+}  // namespace
+
+namespace {
+
+template <typename T>
+__global__ void k_gather_dip(int n, PmeGeom g, const double4* __restrict__ pos,
+                             const typename Cplx<T>::type* __restrict__ grid, double* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double o[6];
+  gather_dip<T>(g, pos[i], grid, o);
+  double* d = out + (size_t)i * 6;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) d[q] = o[q];
+}
+
+// kewald.f:693-717 (bspline) and :747-812 (dftmod)
+std::vector<double> dftmod_host(int nfft, int order) {
+  std::vector<double> arr(order + 2, 0.0), bsarray(nfft + 2, 0.0), bsmod(nfft + 1, 0.0);
+  double x = 0.0;
+  arr[1] = 1.0 - x;
+  arr[2] = x;
+  for (int k = 3; k <= order; ++k) {
+    double denom = 1.0 / (double)(k - 1);
+    arr[k] = x * arr[k - 1] * denom;
+    for (int i = 1; i <= k - 2; ++i) arr[k - i] = ((x + i) * arr[k - i - 1] + ((k - i) - x) * arr[k - i]) * denom;
+    arr[1] = (1.0 - x) * arr[1] * denom;
+  }
+  for (int i = 2; i <= order + 1 && i <= nfft; ++i) bsarray[i] = arr[i - 1];
+  double factor = 2.0 * kPi / (double)nfft;
+  for (int i = 1; i <= nfft; ++i) {
+    double s1 = 0.0, s2 = 0.0;
+    for (int j = 1; j <= nfft; ++j) {
+      double arg = factor * (double)((i - 1) * (j - 1));
+      s1 += bsarray[j] * cos(arg);
+      s2 += bsarray[j] * sin(arg);
+    }
+    bsmod[i] = s1 * s1 + s2 * s2;
+  }
+  double eps = 1.0e-7;
+  if (bsmod[1] < eps) bsmod[1] = 0.5 * bsmod[2];
+  for (int i = 2; i <= nfft - 1; ++i)
+    if (bsmod[i] < eps) bsmod[i] = 0.5 * (bsmod[i - 1] + bsmod[i + 1]);
+  if (bsmod[nfft] < eps) bsmod[nfft] = 0.5 * bsmod[nfft - 1];
+  for (int i = 1; i <= nfft; ++i) {
+    int k = i - 1;
+    if (i > nfft / 2) k -= nfft;
+    double zeta = 1.0;
+    if (k != 0) {
+      double s1 = 1.0, s2 = 1.0, fac = kPi * (double)k / (double)nfft;
+      for (int j = 1; j <= 50; ++j) {
+        double arg = fac / (fac + kPi * j);
+        s1 += pow(arg, order);
+        s2 += pow(arg, 2 * order);
+      }
+      for (int j = 1; j <= 50; ++j) {
+        double arg = fac / (fac - kPi * j);
+        s1 += pow(arg, order);
+        s2 += pow(arg, 2 * order);
+      }
+      zeta = s2 / s1;
+    }
+    bsmod[i] = bsmod[i] * zeta * zeta;
+  }
+  return bsmod;
+}
+
+PmeGeom geom_of(const Ctx& c) {
+  PmeGeom g;
+  g.n1 = c.nfft[0];
+  g.n2 = c.nfft[1];
+  g.n3 = c.nfft[2];
+  for (int d = 0; d < 3; ++d) {
+    g.recip[d] = c.box.recip[d];
+    g.a[d] = c.a_frac[d];
+  }
+  return g;
+}
+
+int fft(Ctx& c, int dir) {
+  cufftResult r;
+  if (c.mixed)
+    r = cufftExecC2C(c.plan, (cufftComplex*)c.d_grid, (cufftComplex*)c.d_grid, dir);
+  else
+    r = cufftExecZ2Z(c.plan, (cufftDoubleComplex*)c.d_grid, (cufftDoubleComplex*)c.d_grid, dir);
+  if (r != CUFFT_SUCCESS) {
+    c.last_msg = "cuFFT exec failed";
+    return THP_E_CUDA;
+  }
+  return THP_OK;
+}
+
+int convolve(Ctx& c, int check_stop) {
+  int st = fft(c, CUFFT_FORWARD);
+  if (st) return st;
+  int blocks = 148 * 8;
+  if (c.mixed)
+    k_qfac<cufftComplex, float><<<blocks, 256, 0, c.stream>>>(c.ngrid, (const float*)c.d_qfac,
+                                                             (cufftComplex*)c.d_grid, c.d_cg, check_stop);
+  else
+    k_qfac<cufftDoubleComplex, double><<<blocks, 256, 0, c.stream>>>(
+        c.ngrid, (const double*)c.d_qfac, (cufftDoubleComplex*)c.d_grid, c.d_cg, check_stop);
+  st = cuda_status(cudaGetLastError(), &c, "qfac");
+  if (st) return st;
+  return fft(c, CUFFT_INVERSE);
+}
+
+}  // namespace
+
+int pme_init(Ctx& c) {
+  for (int d = 0; d < 3; ++d) c.nfft[d] = c.cfg.nfft[d];
+  c.ngrid = (size_t)c.nfft[0] * c.nfft[1] * c.nfft[2];
+  for (int d = 0; d < 3; ++d) c.a_frac[d] = (double)c.nfft[d] * c.box.recip[d];
+  // influence function (newinduce_pme.f:1802-1854)
+  std::vector<double> m1 = dftmod_host(c.nfft[0], kBs), m2 = dftmod_host(c.nfft[1], kBs),
+                      m3 = dftmod_host(c.nfft[2], kBs);
+  std::vector<double> q(c.ngrid, 0.0);
+  double a = c.cfg.aewald;
+  double pterm = (kPi / a) * (kPi / a);
+  double volbox = c.cfg.box[0] * c.cfg.box[1] * c.cfg.box[2];
+  double volterm = kPi * volbox;
+  int nf1 = (c.nfft[0] + 1) / 2, nf2 = (c.nfft[1] + 1) / 2, nf3 = (c.nfft[2] + 1) / 2;
+  for (int k3 = 1; k3 <= c.nfft[2]; ++k3)
+    for (int k2 = 1; k2 <= c.nfft[1]; ++k2)
+      for (int k1 = 1; k1 <= c.nfft[0]; ++k1) {
+        int r1 = k1 - 1, r2 = k2 - 1, r3 = k3 - 1;
+        if (k1 > nf1) r1 -= c.nfft[0];
+        if (k2 > nf2) r2 -= c.nfft[1];
+        if (k3 > nf3) r3 -= c.nfft[2];
+        if (r1 == 0 && r2 == 0 && r3 == 0) continue;
+        double h1 = c.box.recip[0] * r1, h2 = c.box.recip[1] * r2, h3 = c.box.recip[2] * r3;
+        double hsq = h1 * h1 + h2 * h2 + h3 * h3;
+        double term = -pterm * hsq;
+        if (term > -50.0) {
+          double denom = volterm * hsq * m1[k1] * m2[k2] * m3[k3];
+          q[((size_t)(k3 - 1) * c.nfft[1] + (k2 - 1)) * c.nfft[0] + (k1 - 1)] = exp(term) / denom;
+        }
+      }
+  size_t esz = c.mixed ? sizeof(float) : sizeof(double);
+  size_t csz = c.mixed ? sizeof(cufftComplex) : sizeof(cufftDoubleComplex);
+  if (cuda_status(cudaMalloc(&c.d_qfac, esz * c.ngrid), &c, "alloc qfac")) return THP_E_CUDA;
+  if (cuda_status(cudaMalloc(&c.d_grid, csz * c.ngrid), &c, "alloc grid")) return THP_E_CUDA;
+  if (c.mixed) {
+    std::vector<float> qf(q.begin(), q.end());
+    cudaMemcpy(c.d_qfac, qf.data(), esz * c.ngrid, cudaMemcpyHostToDevice);
+  } else {
+    cudaMemcpy(c.d_qfac, q.data(), esz * c.ngrid, cudaMemcpyHostToDevice);
+  }
+  // cuFFT dims: slowest first; data [n3][n2][n1]
+  cufftResult r = cufftPlan3d(&c.plan, c.nfft[2], c.nfft[1], c.nfft[0], c.mixed ? CUFFT_C2C : CUFFT_Z2Z);
+  if (r != CUFFT_SUCCESS) {
+    c.last_msg = "cufftPlan3d failed";
+    return THP_E_CUDA;
+  }
+  cufftSetStream(c.plan, c.stream);
+  c.have_plan = true;
+  return cuda_status(cudaGetLastError(), &c, "pme init");
+}
+
+void pme_free(Ctx& c) {
+  if (c.have_plan) cufftDestroy(c.plan);
+  c.have_plan = false;
+  cudaFree(c.d_qfac);
+  cudaFree(c.d_grid);
+  c.d_qfac = c.d_grid = nullptr;
+}
+
+int zero_grid(Ctx& c) {
+  size_t csz = c.mixed ? sizeof(cufftComplex) : sizeof(cufftDoubleComplex);
+  return cuda_status(cudaMemsetAsync(c.d_grid, 0, csz * c.ngrid, c.stream), &c, "zero grid");
+}
+
+// Permanent-multipole PME: d_cphi (and cphi10 when non-null) and, when
+// with_e0, completes d_ef = E_direct - cphi(2:4) + (4/3) a^3/sqrt(pi) d.
+int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0) {
+  PmeGeom g = geom_of(c);
+  int nb = (c.n + kBlock - 1) / kBlock;
+  int st = zero_grid(c);
+  if (st) return st;
+  if (c.mixed)
+    k_spread_mpole<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, c.d_rpole, (cufftComplex*)c.d_grid);
+  else
+    k_spread_mpole<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, c.d_rpole, (cufftDoubleComplex*)c.d_grid);
+  if ((st = cuda_status(cudaGetLastError(), &c, "spread mpole"))) return st;
+  if ((st = convolve(c, 0))) return st;
+  double a = c.cfg.aewald;
+  double term = (4.0 / 3.0) * a * a * a / kSqrtPi;
+  if (c.mixed)
+    k_gather_mpole<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftComplex*)c.d_grid, c.d_rpole,
+                                                       term, c.d_cphi, cphi10, with_e0 ? c.d_ef : nullptr);
+  else
+    k_gather_mpole<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftDoubleComplex*)c.d_grid,
+                                                        c.d_rpole, term, c.d_cphi, cphi10,
+                                                        with_e0 ? c.d_ef : nullptr);
+  return cuda_status(cudaGetLastError(), &c, "gather mpole");
+}
+
+int launch_efld0_recip(Ctx& c) { return launch_efld0_recip_ex(c, nullptr, true); }
+
+// Dipole PME pass.  mode 0: spread d_vec as is; mode 1: pp update first (CG
+// loop, honours the stop flag).  d_out (if non-null) receives the gathered
+// field gradient [n][6] (tmatxbrecip's dipfield); the CG loop passes null and
+// gathers inside its fused matvec kernel.
+int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode) {
+  PmeGeom g = geom_of(c);
+  int nb = (c.n + kBlock - 1) / kBlock;
+  int st = zero_grid(c);
+  if (st) return st;
+  float* vf = c.mixed ? c.d_vecf : nullptr;
+  if (c.mixed)
+    k_spread_dip<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<double*>(d_vec), c.d_zr, vf,
+                                                     c.d_cg, mode, (cufftComplex*)c.d_grid);
+  else
+    k_spread_dip<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<double*>(d_vec), c.d_zr, vf,
+                                                      c.d_cg, mode, (cufftDoubleComplex*)c.d_grid);
+  if ((st = cuda_status(cudaGetLastError(), &c, "spread dip"))) return st;
+  if ((st = convolve(c, mode == 1))) return st;
+  if (d_out) {
+    if (c.mixed)
+      k_gather_dip<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftComplex*)c.d_grid, d_out);
+    else
+      k_gather_dip<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftDoubleComplex*)c.d_grid, d_out);
+    st = cuda_status(cudaGetLastError(), &c, "gather dip");
+  }
+  return st;
+}
+
+PmeGeom pme_geom(const Ctx& c) { return geom_of(c); }
+
+}  // namespace thp

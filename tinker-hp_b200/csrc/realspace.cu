@@ -1,0 +1,252 @@
+// realspace.cu -- direct permanent field and mutual-field coefficients.
+//
+// One pass over the full neighbor list per solve computes, for every pair
+// with r^2 <= ewaldcut^2 (same unfused r^2 and image as newinduce_pme.f:1160):
+//   * the direct permanent field of efld0_direct (newinduce_pme.f:948-1389),
+//     d field with dscale and p field with pscale, Thole branch, dampewald
+//     order 7 and damptholed order 7 (damping.f:17-55, 142-216);
+//   * the mutual coefficients dmp3/dmp5 of tmatxb_pme (:1524-1560) with
+//     uscale, stored slot-major for the matvec of every CG iteration.
+// Scaled (special) pairs come from the connectivity lists, applied with the
+// reference's assignment order (host side); the kernel looks the scale up in
+// the owner's short special-pair list.
+#include <type_traits>
+
+#include "kernels.h"
+#include "realspace_dev.cuh"
+
+namespace thp {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+struct EwaldConst {
+  double a, afac1, afac2, afac3;  // 2a/sqrt(pi), 4a^3/sqrt(pi), 8a^5/sqrt(pi)
+};
+
+template <bool MIXED, bool FIELD>
+__global__ void __launch_bounds__(kBlock) k_efld0_coef(
+    int n, int npad, Box box, double cut2, EwaldConst ew, const double4* __restrict__ pos,
+    const double* __restrict__ thole, const double* __restrict__ rp, const int* __restrict__ perm,
+    const int* __restrict__ sp_off, const int* __restrict__ sp_k, const double* __restrict__ sp_s,
+    const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb, int* __restrict__ npr, int* __restrict__ pk,
+    void* __restrict__ pc3v, void* __restrict__ pc5v, int maxpr, double* __restrict__ ef, int* __restrict__ flags) {
+  using T = typename std::conditional<MIXED, float, double>::type;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  T* pc3 = (T*)pc3v;
+  T* pc5 = (T*)pc5v;
+  const double4 pi = pos[i];
+  const double thi = thole[i];
+  const int io = perm[i];
+  const int s0 = sp_off[io], s1 = sp_off[io + 1];
+  double e[6] = {0, 0, 0, 0, 0, 0};
+  const int nn = min(nnb[i], maxnb);
+  int cnt = 0;
+#pragma unroll 1
+  for (int s = 0; s < nn; ++s) {
+    const int k = nb[(size_t)s * npad + i];
+    const double4 pk4 = pos[k];
+    double xr = pk4.x - pi.x, yr = pk4.y - pi.y, zr = pk4.z - pi.z;
+    image3(box, xr, yr, zr);
+    const double r2d = r2_exact(xr, yr, zr);
+    if (r2d > cut2) continue;
+    // scale factors of this pair (1 unless listed)
+    double ds = 1.0, ps = 1.0, us = 1.0;
+    if (s1 > s0) {
+      const int ko = perm[k];
+      for (int q = s0; q < s1; ++q)
+        if (sp_k[q] == ko) {
+          ds = sp_s[3 * q];
+          ps = sp_s[3 * q + 1];
+          us = sp_s[3 * q + 2];
+          break;
+        }
+    }
+    const T x = (T)xr, y = (T)yr, z = (T)zr, r2 = (T)r2d;
+    const T r = sqrt(r2);
+    const T rr1 = T(1) / r;
+    const T rr2 = rr1 * rr1;
+    const T rr3 = rr2 * rr1;
+    const T rr5 = T(3) * rr2 * rr3;
+    const T rr7 = T(5) * rr2 * rr5;
+    // dampewald (order 7)
+    const T ra = (T)ew.a * r;
+    const T bn0 = erfc(ra) * rr1;
+    const T expterm = exp(-ra * ra);
+    const T bn1 = (bn0 + (T)ew.afac1 * expterm) * rr2;
+    const T bn2 = (T(3) * bn1 + (T)ew.afac2 * expterm) * rr2;
+    const T bn3 = (T(5) * bn2 + (T)ew.afac3 * expterm) * rr2;
+    // dampthole / damptholed (AMOEBA branch)
+    T l3 = 1, l5 = 1, l7 = 1;
+    const double pdd = pi.w * pk4.w;
+    double pg = fmin(thi, thole[k]);
+    if (pg == 0.0) pg = fmax(thi, thole[k]);
+    if (pdd != 0.0 && pg != 0.0) {
+      const T t = r / (T)pdd;
+      const T damp = (T)pg * (t * t * t);
+      if (damp < T(50)) {
+        const T ex = exp(-damp);
+        l3 = T(1) - ex;
+        l5 = T(1) - ex * (T(1) + damp);
+        l7 = T(1) - ex * (T(1) + damp + T(0.6) * damp * damp);
+      }
+    }
+    if (FIELD) {
+      const double* rk = rp + (size_t)k * 10;
+      const T ck = (T)rk[0], dkx = (T)rk[1], dky = (T)rk[2], dkz = (T)rk[3];
+      const T qkxx = (T)rk[4], qkxy = (T)rk[5], qkxz = (T)rk[6], qkyy = (T)rk[7], qkyz = (T)rk[8], qkzz = (T)rk[9];
+      const T dkr = dkx * x + dky * y + dkz * z;
+      const T qkx = qkxx * x + qkxy * y + qkxz * z;
+      const T qky = qkxy * x + qkyy * y + qkyz * z;
+      const T qkz = qkxz * x + qkyz * y + qkzz * z;
+      const T qkr = qkx * x + qky * y + qkz * z;
+      T sc = (T)ds;
+      T dmp3 = bn1 - (T(1) - sc * l3) * rr3;
+      T dmp5 = bn2 - (T(1) - sc * l5) * rr5;
+      T dmp7 = bn3 - (T(1) - sc * l7) * rr7;
+      T rad = dmp3 * ck - dmp5 * dkr + dmp7 * qkr;
+      e[0] += (double)(-x * rad - dmp3 * dkx + T(2) * dmp5 * qkx);
+      e[1] += (double)(-y * rad - dmp3 * dky + T(2) * dmp5 * qky);
+      e[2] += (double)(-z * rad - dmp3 * dkz + T(2) * dmp5 * qkz);
+      sc = (T)ps;
+      dmp3 = bn1 - (T(1) - sc * l3) * rr3;
+      dmp5 = bn2 - (T(1) - sc * l5) * rr5;
+      dmp7 = bn3 - (T(1) - sc * l7) * rr7;
+      rad = dmp3 * ck - dmp5 * dkr + dmp7 * qkr;
+      e[3] += (double)(-x * rad - dmp3 * dkx + T(2) * dmp5 * qkx);
+      e[4] += (double)(-y * rad - dmp3 * dky + T(2) * dmp5 * qky);
+      e[5] += (double)(-z * rad - dmp3 * dkz + T(2) * dmp5 * qkz);
+    }
+    const T su = (T)us;
+    if (cnt < maxpr) {
+      const size_t q = (size_t)cnt * npad + i;
+      pk[q] = k;
+      pc3[q] = bn1 - (T(1) - su * l3) * rr3;
+      pc5[q] = bn2 - (T(1) - su * l5) * rr5;
+    }
+    ++cnt;
+  }
+  npr[i] = min(cnt, maxpr);
+  if (cnt > maxpr) atomicOr(flags, DEV_PAIR_OVERFLOW);
+  if (FIELD) {
+    double* o = ef + (size_t)i * 6;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o[q] = e[q];
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_tmatxb64(PairRows pr, Box box, const double4* __restrict__ pos,
+                                                     const double* __restrict__ mu, const double* __restrict__ pol,
+                                                     int dodiag, double* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= pr.n) return;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  tmatxb_row64(pr, box, i, pos, mu, acc);
+  double* o = out + (size_t)i * 6;
+  if (dodiag) {
+    double p = pol[i];
+    double ip = (p == 0.0) ? 1.0 / kTinyPol : 1.0 / p;
+    const double* m = mu + (size_t)i * 6;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[q] += m[q] * ip;
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) o[q] = acc[q];
+}
+
+__global__ void __launch_bounds__(kBlock) k_tmatxb32(PairRows pr, float bx, float by, float bz,
+                                                     const float4* __restrict__ pos, const float* __restrict__ muf,
+                                                     const double* __restrict__ mu, const double* __restrict__ pol,
+                                                     int dodiag, double* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= pr.n) return;
+  float acc[6] = {0, 0, 0, 0, 0, 0};
+  tmatxb_row32(pr, bx, by, bz, i, pos, muf, acc);
+  double* o = out + (size_t)i * 6;
+  double a[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) a[q] = (double)acc[q];
+  if (dodiag) {
+    double p = pol[i];
+    double ip = (p == 0.0) ? 1.0 / kTinyPol : 1.0 / p;
+    const double* m = mu + (size_t)i * 6;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) a[q] += m[q] * ip;
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) o[q] = a[q];
+}
+
+__global__ void k_to_float(int m, const double* __restrict__ in, float* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) out[i] = (float)in[i];
+}
+
+EwaldConst ewald_const(double a) {
+  // dampewald recursion (damping.f:41-50): afac_i = (2 a^2)^i / (sqrt(pi) a)
+  EwaldConst e;
+  e.a = a;
+  double aesq2 = 2.0 * a * a;
+  double afac = 1.0 / (kSqrtPi * a);
+  afac = aesq2 * afac;
+  e.afac1 = afac;
+  afac = aesq2 * afac;
+  e.afac2 = afac;
+  afac = aesq2 * afac;
+  e.afac3 = afac;
+  return e;
+}
+
+}  // namespace
+
+PairRows pair_rows(const Ctx& c) {
+  PairRows pr;
+  pr.n = c.n;
+  pr.npad = c.npad;
+  pr.npr = c.d_npr;
+  pr.pk = c.d_pk;
+  pr.pc3 = c.d_pc3;
+  pr.pc5 = c.d_pc5;
+  return pr;
+}
+
+int launch_efld0_coef(Ctx& c, bool with_field) {
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  const double cut2 = c.cfg.ewaldcut * c.cfg.ewaldcut;
+  EwaldConst ew = ewald_const(c.cfg.aewald);
+#define THP_EFLD0_ARGS                                                                                          \
+  c.n, c.npad, c.box, cut2, ew, c.d_pos, c.d_thole, c.d_rpole, c.d_perm, c.d_sp_off, c.d_sp_k, c.d_sp_s, c.d_nnb, \
+      c.d_nb, c.maxnb, c.d_npr, c.d_pk, c.d_pc3, c.d_pc5, c.maxpr, c.d_ef, c.d_flags
+  if (c.mixed) {
+    if (with_field)
+      k_efld0_coef<true, true><<<nb, kBlock, 0, c.stream>>>(THP_EFLD0_ARGS);
+    else
+      k_efld0_coef<true, false><<<nb, kBlock, 0, c.stream>>>(THP_EFLD0_ARGS);
+  } else {
+    if (with_field)
+      k_efld0_coef<false, true><<<nb, kBlock, 0, c.stream>>>(THP_EFLD0_ARGS);
+    else
+      k_efld0_coef<false, false><<<nb, kBlock, 0, c.stream>>>(THP_EFLD0_ARGS);
+  }
+#undef THP_EFLD0_ARGS
+  c.have_coef = true;
+  return cuda_status(cudaGetLastError(), &c, "efld0/coef");
+}
+
+int launch_tmatxb(Ctx& c, const double* d_in, double* d_out, bool dodiag) {
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  PairRows pr = pair_rows(c);
+  if (c.mixed) {
+    int m = c.n * 6;
+    k_to_float<<<(m + 255) / 256, 256, 0, c.stream>>>(m, d_in, c.d_vecf);
+    k_tmatxb32<<<nb, kBlock, 0, c.stream>>>(pr, (float)c.box.l[0], (float)c.box.l[1], (float)c.box.l[2], c.d_posf,
+                                            c.d_vecf, d_in, c.d_pol, dodiag ? 1 : 0, d_out);
+  } else {
+    k_tmatxb64<<<nb, kBlock, 0, c.stream>>>(pr, c.box, c.d_pos, d_in, c.d_pol, dodiag ? 1 : 0, d_out);
+  }
+  return cuda_status(cudaGetLastError(), &c, "tmatxb");
+}
+
+}  // namespace thp

@@ -1,0 +1,335 @@
+// solver.cu -- device-resident preconditioned conjugate gradient.
+//
+// inducepcg_pme2 (newinduce_pme2.f:285-636) with every vector and scalar on
+// the device.  Per iteration:
+//   1. spread kernel: pp = zr + beta*pp, spread pp on the PME grid;
+//   2. cuFFT forward, qfac, cuFFT backward;
+//   3. fused matvec kernel: PME gather + real-space row + diagonal and self
+//      terms -> h; partial pp.h; the last block forms gg and alpha;
+//   4. update kernel: mu += alpha pp, res -= alpha h, zr = diag res; partial
+//      ggnew and ene; the last block forms beta, the residual norm and the
+//      convergence / stop flags.
+// Reductions write per-block partials summed in a fixed order by the last
+// block, so results are bitwise reproducible run to run.  Once the stop flag
+// is set every later kernel returns at entry, so the host can enqueue
+// iterations ahead and read the flag only once per chunk.
+#include <cstring>
+
+#include "kernels.h"
+#include "pme_dev.cuh"
+#include "realspace_dev.cuh"
+
+namespace thp {
+
+PairRows pair_rows(const Ctx& c);
+
+namespace {
+
+constexpr int kBlock = 128;
+
+// Deterministic grid reduction; returns true in the last block (all threads),
+// with the totals valid in thread 0.
+template <int NV>
+__device__ bool grid_reduce(double (&v)[NV], double* __restrict__ partials, unsigned* counter, double (&tot)[NV]) {
+  block_reduce<NV>(v);
+  __shared__ bool amlast;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) partials[(size_t)blockIdx.x * NV + q] = v[q];
+    __threadfence();
+    unsigned t = atomicAdd(counter, 1u);
+    amlast = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!amlast) return false;
+  __threadfence();
+  double s[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) s[q] = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) s[q] += __ldcg(partials + (size_t)b * NV + q);
+  block_reduce<NV>(s);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) tot[q] = s[q];
+    *counter = 0;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void load6(const double* p, double (&v)[6]) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  double2 a = q[0], b = q[1], c = q[2];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y;
+}
+__device__ __forceinline__ void store6(double* p, const double (&v)[6]) {
+  double2* q = reinterpret_cast<double2*>(p);
+  q[0] = make_double2(v[0], v[1]);
+  q[1] = make_double2(v[2], v[3]);
+  q[2] = make_double2(v[4], v[5]);
+}
+
+__device__ __forceinline__ double diag_of(double p) { return p == 0.0 ? kTinyPol : p; }
+
+// h = T_real x + x/alpha + dipfield(x) - term x  (newinduce_pme2.f:398-405, 469-475)
+// init: also res = ef - h, zr = diag res, pp = zr, ggold = sum res.zr
+// iter: gg = sum pp.h, alpha = ggold / gg
+template <bool MIXED>
+__global__ void __launch_bounds__(kBlock) k_cg_matvec(PairRows pr, Box box, PmeGeom g, const double4* __restrict__ pos,
+                                                      const float4* __restrict__ posf, const void* __restrict__ grid,
+                                                      const double* __restrict__ x, const float* __restrict__ xf,
+                                                      const double* __restrict__ pol, const double* __restrict__ ef,
+                                                      double term, int init, double* __restrict__ h,
+                                                      double* __restrict__ res, double* __restrict__ zr,
+                                                      double* __restrict__ pp, CgScalars* cg,
+                                                      double* __restrict__ partials) {
+  if (cg->stop) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double red[2] = {0.0, 0.0};
+  if (i < pr.n) {
+    double acc[6];
+    if (MIXED) {
+      float a32[6] = {0, 0, 0, 0, 0, 0};
+      tmatxb_row32(pr, (float)box.l[0], (float)box.l[1], (float)box.l[2], i, posf, xf, a32);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) acc[q] = (double)a32[q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) acc[q] = 0.0;
+      tmatxb_row64(pr, box, i, pos, x, acc);
+    }
+    double dip[6];
+    if (MIXED)
+      gather_dip<float>(g, pos[i], (const cufftComplex*)grid, dip);
+    else
+      gather_dip<double>(g, pos[i], (const cufftDoubleComplex*)grid, dip);
+    double xi[6];
+    load6(x + (size_t)i * 6, xi);
+    const double p = pol[i];
+    const double ip = (p == 0.0) ? 1.0 / kTinyPol : 1.0 / p;
+    double hv[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) hv[q] = ((acc[q] + xi[q] * ip) + dip[q]) - term * xi[q];
+    store6(h + (size_t)i * 6, hv);
+    if (init) {
+      double e6[6], r6[6], z6[6];
+      load6(ef + (size_t)i * 6, e6);
+      const double dg = diag_of(p);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        r6[q] = e6[q] - hv[q];
+        z6[q] = dg * r6[q];
+      }
+      store6(res + (size_t)i * 6, r6);
+      store6(zr + (size_t)i * 6, z6);
+      store6(pp + (size_t)i * 6, z6);
+      red[0] = r6[0] * z6[0] + r6[1] * z6[1] + r6[2] * z6[2];
+      red[1] = r6[3] * z6[3] + r6[4] * z6[4] + r6[5] * z6[5];
+    } else {
+      red[0] = xi[0] * hv[0] + xi[1] * hv[1] + xi[2] * hv[2];
+      red[1] = xi[3] * hv[3] + xi[4] * hv[4] + xi[5] * hv[5];
+    }
+  }
+  double tot[2];
+  if (grid_reduce<2>(red, partials, &cg->counter[0], tot) && threadIdx.x == 0) {
+    if (init) {
+      cg->ggold[0] = tot[0];
+      cg->ggold[1] = tot[1];
+      cg->beta[0] = 0.0;
+      cg->beta[1] = 0.0;
+    } else {
+      cg->gg[0] = tot[0];
+      cg->gg[1] = tot[1];
+      if (tot[0] == 0.0 || tot[1] == 0.0) {
+        cg->stop = 1;  // newinduce_pme2.f:505 returns on gg == 0
+      } else {
+        cg->alpha[0] = cg->ggold[0] / tot[0];
+        cg->alpha[1] = cg->ggold[1] / tot[1];
+      }
+    }
+  }
+}
+
+// newinduce_pme2.f:512-572
+__global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __restrict__ pol, const double* __restrict__ ef,
+                                                      const double* __restrict__ h, const double* __restrict__ pp,
+                                                      double* __restrict__ mu, double* __restrict__ res,
+                                                      double* __restrict__ zr, CgScalars* cg, double* __restrict__ partials,
+                                                      double poleps, int politer) {
+  if (cg->stop) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double red[4] = {0, 0, 0, 0};
+  if (i < n) {
+    const double ad = cg->alpha[0], ap = cg->alpha[1];
+    double m6[6], r6[6], p6[6], h6[6], e6[6], z6[6];
+    load6(mu + (size_t)i * 6, m6);
+    load6(res + (size_t)i * 6, r6);
+    load6(pp + (size_t)i * 6, p6);
+    load6(h + (size_t)i * 6, h6);
+    load6(ef + (size_t)i * 6, e6);
+    const double dg = diag_of(pol[i]);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const double a = q < 3 ? ad : ap;
+      m6[q] = m6[q] + a * p6[q];
+      r6[q] = r6[q] - a * h6[q];
+      z6[q] = dg * r6[q];
+    }
+    store6(mu + (size_t)i * 6, m6);
+    store6(res + (size_t)i * 6, r6);
+    store6(zr + (size_t)i * 6, z6);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const int k = q < 3 ? 0 : 1;
+      red[k] += r6[q] * z6[q];
+      red[2 + k] -= 0.5 * (m6[q] * (r6[q] + e6[q]));
+    }
+  }
+  double tot[4];
+  if (grid_reduce<4>(red, partials, &cg->counter[1], tot) && threadIdx.x == 0) {
+    const double nrm = (double)(3 * n);
+    double resnrm = 0.0;
+    bool bad = false;
+    for (int k = 0; k < 2; ++k) {
+      cg->ggnew[k] = tot[k];
+      cg->ene[k] = tot[2 + k];
+      const double gn = sqrt(tot[k] / nrm);
+      resnrm = fmax(resnrm, gn);
+      bad |= !isfinite(tot[k]) || !isfinite(tot[2 + k]);
+      cg->beta[k] = tot[k] / cg->ggold[k];
+      cg->ggold[k] = tot[k];
+    }
+    cg->resnrm = resnrm;
+    cg->niter += 1;
+    if (bad) {
+      cg->status = THP_E_NAN;
+      cg->stop = 1;
+    } else if (resnrm < poleps) {
+      cg->converged = 1;
+      cg->stop = 1;
+    } else if (cg->niter >= politer) {
+      cg->stop = 1;
+    }
+  }
+}
+
+__global__ void k_guess_direct(int n, const double* __restrict__ pol, const double* __restrict__ ef,
+                               double* __restrict__ mu) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * 6) return;
+  mu[t] = pol[t / 6] * ef[t];
+}
+
+// epolar0c via the identity Epol = -1/2 electric sum uind . E_p(perm)
+// (epreal0c + eprecip + self of epolar.f:47-520 sum to exactly this form)
+__global__ void __launch_bounds__(kBlock) k_epol(int n, const double* __restrict__ mu, const double* __restrict__ ef,
+                                                 CgScalars* cg, double* __restrict__ partials) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double red[1] = {0.0};
+  if (i < n) {
+    const double* m = mu + (size_t)i * 6;
+    const double* e = ef + (size_t)i * 6;
+    red[0] = m[0] * e[3] + m[1] * e[4] + m[2] * e[5];
+  }
+  double tot[1];
+  if (grid_reduce<1>(red, partials, &cg->counter[2], tot) && threadIdx.x == 0) cg->epol = -0.5 * kElectric * tot[0];
+}
+
+// original [n][nrhs][3] <-> sorted [n][6]
+__global__ void k_to_sorted6(int n, int nrhs, const int* __restrict__ iperm, const double* __restrict__ in,
+                             double* __restrict__ out) {
+  int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  int s = iperm[o];
+  for (int q = 0; q < 6; ++q) out[(size_t)s * 6 + q] = (q < 3 * nrhs) ? in[(size_t)o * 3 * nrhs + q] : 0.0;
+}
+__global__ void k_to_orig6(int n, int nrhs, const int* __restrict__ perm, const double* __restrict__ in,
+                           double* __restrict__ out) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int o = perm[s];
+  for (int q = 0; q < 3 * nrhs; ++q) out[(size_t)o * 3 * nrhs + q] = in[(size_t)s * 6 + q];
+}
+
+}  // namespace
+
+int launch_to_sorted6(Ctx& c, const double* d_orig, double* d_sorted, int nrhs) {
+  k_to_sorted6<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, nrhs, c.d_iperm, d_orig, d_sorted);
+  return cuda_status(cudaGetLastError(), &c, "to sorted");
+}
+int launch_to_orig6(Ctx& c, const double* d_sorted, double* d_orig, int nrhs) {
+  k_to_orig6<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, nrhs, c.d_perm, d_sorted, d_orig);
+  return cuda_status(cudaGetLastError(), &c, "to orig");
+}
+
+static void prof_mark(Ctx& c) {
+  if (!c.profiling) return;
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, c.stream);
+  c.prof_events.push_back(e);
+}
+
+static int launch_matvec(Ctx& c, const double* x, int init) {
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  prof_mark(c);
+  PairRows pr = pair_rows(c);
+  PmeGeom g = pme_geom(c);
+  const double a = c.cfg.aewald;
+  const double term = (4.0 / 3.0) * a * a * a / kSqrtPi;
+  if (c.mixed)
+    k_cg_matvec<true><<<nb, kBlock, 0, c.stream>>>(pr, c.box, g, c.d_pos, c.d_posf, c.d_grid, x, c.d_vecf, c.d_pol,
+                                                   c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, c.d_cg,
+                                                   c.d_partials);
+  else
+    k_cg_matvec<false><<<nb, kBlock, 0, c.stream>>>(pr, c.box, g, c.d_pos, c.d_posf, c.d_grid, x, c.d_vecf, c.d_pol,
+                                                    c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, c.d_cg,
+                                                    c.d_partials);
+  prof_mark(c);
+  return cuda_status(cudaGetLastError(), &c, "cg matvec");
+}
+
+static int enqueue_iteration(Ctx& c) {
+  int st = launch_pme_dipole(c, c.d_pp, nullptr, 1);
+  if (st) return st;
+  if ((st = launch_matvec(c, c.d_pp, 0))) return st;
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  k_cg_update<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_h, c.d_pp, c.d_mu, c.d_res, c.d_zr, c.d_cg,
+                                           c.d_partials, c.cfg.poleps, c.cfg.politer);
+  return cuda_status(cudaGetLastError(), &c, "cg update");
+}
+
+// Runs the CG from the current d_ef; guess selects the start (see thp.h).
+int run_pcg(Ctx& c, int guess) {
+  int st;
+  cudaMemsetAsync(c.d_cg, 0, sizeof(CgScalars), c.stream);
+  if (guess == THP_GUESS_DIRECT) {
+    k_guess_direct<<<(c.n * 6 + 255) / 256, 256, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_mu);
+  }
+  // initial residual on the guess (newinduce_pme2.f:398-417)
+  if ((st = launch_pme_dipole(c, c.d_mu, nullptr, 0))) return st;
+  if ((st = launch_matvec(c, c.d_mu, 1))) return st;
+  const int chunk = 4;
+  int done = 0;
+  while (true) {
+    for (int q = 0; q < chunk; ++q)
+      if ((st = enqueue_iteration(c))) return st;
+    done += chunk;
+    cudaMemcpyAsync(c.h_cg, c.d_cg, sizeof(CgScalars), cudaMemcpyDeviceToHost, c.stream);
+    if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "cg sync"))) return st;
+    if (c.h_cg->stop) break;
+    if (done > c.cfg.politer + chunk) break;  // defensive bound; stop is raised at politer
+  }
+  c.have_dipoles = true;
+  if (c.h_cg->status) return c.h_cg->status;
+  return c.h_cg->converged ? THP_OK : THP_E_NOT_CONVERGED;
+}
+
+int launch_epol(Ctx& c) {
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  k_epol<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_mu, c.d_ef, c.d_cg, c.d_partials);
+  return cuda_status(cudaGetLastError(), &c, "epol");
+}
+
+}  // namespace thp

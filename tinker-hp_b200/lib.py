@@ -1,0 +1,304 @@
+"""ctypes binding of libthp.so (the C-ABI declared in include/thp.h).
+
+This is the host-side mirror of the reference's polarization interface for
+Python callers (tests, benchmarks, the batch and serving layers).  There is no
+fallback path: if libthp.so is missing or cannot load, every call raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libthp.so")
+
+THP_OK = 0
+THP_E_INVALID = 1
+THP_E_LIST_OVERFLOW = 2
+THP_E_NOT_CONVERGED = 3
+THP_E_NAN = 4
+THP_E_CUDA = 5
+THP_E_TIMEOUT = 6
+THP_E_OOM_ADMISSION = 7
+THP_E_BOX_TOO_SMALL = 8
+THP_E_NO_DEVICE = 9
+THP_E_STATE = 10
+
+FP64 = 0
+MIXED = 1
+
+GUESS_DIRECT = 0
+GUESS_PREVIOUS = 1
+GUESS_HOST = 2
+
+CONN_NAMES = ("i12", "i13", "i14", "i15", "ip11", "ip12", "ip13", "ip14")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class ThpConfig(C.Structure):
+    _fields_ = [("n", C.c_int), ("box", C.c_double * 3), ("aewald", C.c_double), ("ewaldcut", C.c_double),
+                ("lbuffer", C.c_double), ("nfft", C.c_int * 3), ("bsorder", C.c_int), ("politer", C.c_int),
+                ("poleps", C.c_double), ("precision", C.c_int), ("max_neighbors", C.c_int), ("device", C.c_int)]
+
+
+class ThpSolveInfo(C.Structure):
+    _fields_ = [("niter", C.c_int), ("converged", C.c_int), ("resnrm", C.c_double), ("epol", C.c_double),
+                ("ene", C.c_double * 2), ("ms_total", C.c_double)]
+
+
+class ThpError(RuntimeError):
+    def __init__(self, status, what):
+        self.status = status
+        super().__init__(f"{what}: status {status} ({status_string(status)})")
+
+
+_lib = None
+
+
+def load():
+    """Load libthp.so (raises if it is absent: the CUDA path is the only path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} not built; run tinker-hp_b200/build.py")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    sig = {
+        "thp_ctx_create": ([C.POINTER(ThpConfig), C.POINTER(vp)], C.c_int),
+        "thp_ctx_destroy": ([vp], C.c_int),
+        "thp_set_stream": ([vp, vp], C.c_int),
+        "thp_set_params": ([vp, _dp, _dp, _dp], C.c_int),
+        "thp_set_connectivity": ([vp, C.POINTER(_ip), C.POINTER(_ip), _dp], C.c_int),
+        "thp_set_positions": ([vp, _dp, _dp, _dp], C.c_int),
+        "thp_set_rpole": ([vp, _dp], C.c_int),
+        "thp_set_frames": ([vp, _dp, _ip, _ip, _ip], C.c_int),
+        "thp_set_guess": ([vp, _dp], C.c_int),
+        "thp_nblist": ([vp], C.c_int),
+        "thp_invalidate_list": ([vp], C.c_int),
+        "thp_profile": ([vp, C.c_int, _dp, _ip], C.c_int),
+        "thp_solve": ([vp, C.c_int, C.POINTER(ThpSolveInfo)], C.c_int),
+        "thp_get_dipoles": ([vp, _dp, _dp], C.c_int),
+        "thp_get_field": ([vp, _dp], C.c_int),
+        "thp_get_rpole": ([vp, _dp], C.c_int),
+        "thp_get_nblist": ([vp, C.c_int, _ip, _ip], C.c_int),
+        "thp_tmatxb": ([vp, C.c_int, C.c_int, _dp, _dp], C.c_int),
+        "thp_efld0_direct": ([vp, C.c_int, _dp], C.c_int),
+        "thp_efld0_recip": ([vp, _dp], C.c_int),
+        "thp_tmatxbrecip": ([vp, C.c_int, _dp, _dp], C.c_int),
+        "thp_solve_host": ([vp, _dp, _dp, _dp, _dp, _dp, _dp, C.POINTER(ThpSolveInfo)], C.c_int),
+        "thp_footprint": ([C.POINTER(ThpConfig)], C.c_size_t),
+        "thp_status_string": ([C.c_int], C.c_char_p),
+        "thp_bind_state": ([vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_int, _dp], C.c_int),
+        "thp_last_error": ([], C.c_int),
+        "newinduce_pme2_": ([], None),
+        "tmatxb_pme_": ([_ip, _ip, _dp, _dp], None),
+        "efld0_direct_": ([_ip, _dp], None),
+        "efld0_recip_": ([_dp], None),
+        "tmatxbrecip_": ([_dp, _dp, _ip, _dp, _dp], None),
+        "mlistcell_": ([], None),
+        "vlistcell_": ([], None),
+        "epolar_": ([], None),
+        "inducepcg_pme2_": ([vp, _ip, _ip, _dp, _dp, _dp], None),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def status_string(st):
+    try:
+        return load().thp_status_string(st).decode()
+    except Exception:
+        return "?"
+
+
+def _p(a, t=_dp):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def config_for(ws, precision=FP64, poleps=1e-6, politer=500, device=0, max_neighbors=0):
+    cfg = ThpConfig()
+    cfg.n = ws.n
+    for d in range(3):
+        cfg.box[d] = ws.box[d]
+        cfg.nfft[d] = ws.nfft[d]
+    cfg.aewald = ws.aewald
+    cfg.ewaldcut = ws.ewaldcut
+    cfg.lbuffer = ws.lbuffer
+    cfg.bsorder = ws.bsorder
+    cfg.politer = politer
+    cfg.poleps = poleps
+    cfg.precision = precision
+    cfg.max_neighbors = max_neighbors
+    cfg.device = device
+    return cfg
+
+
+def footprint(ws, precision=FP64):
+    return int(load().thp_footprint(C.byref(config_for(ws, precision))))
+
+
+def scales_array(ws):
+    s = ws.scales
+    return _f64(list(s["p_scale"]) + list(s["pi_scale"]) + list(s["d_scale"]) + list(s["u_scale"]))
+
+
+class Context:
+    """One system resident on the GPU (wraps thp_ctx)."""
+
+    def __init__(self, ws, precision=FP64, poleps=1e-6, politer=500, device=0, frames=True, rpole=None,
+                 max_neighbors=0):
+        L = load()
+        self.ws = ws
+        self.n = ws.n
+        self.cfg = config_for(ws, precision, poleps, politer, device, max_neighbors)
+        h = C.c_void_p()
+        self._check(L.thp_ctx_create(C.byref(self.cfg), C.byref(h)), "thp_ctx_create")
+        self.h = h
+        self._keep = []
+        self._check(L.thp_set_params(self.h, _p(_f64(ws.polarity)), _p(_f64(ws.thole)), _p(_f64(ws.pdamp))),
+                    "thp_set_params")
+        offs = (_ip * 8)()
+        idxs = (_ip * 8)()
+        for q, name in enumerate(CONN_NAMES):
+            off, idx = ws.conn[name]
+            off, idx = _i32(off), _i32(idx if len(idx) else np.zeros(1, np.int32))
+            self._keep += [off, idx]
+            offs[q] = _p(off, _ip)
+            idxs[q] = _p(idx, _ip)
+        self._check(L.thp_set_connectivity(self.h, offs, idxs, _p(scales_array(ws))), "thp_set_connectivity")
+        self.set_positions(ws.x, ws.y, ws.z)
+        if rpole is not None:
+            self.set_rpole(rpole)
+        elif frames:
+            self._check(L.thp_set_frames(self.h, _p(_f64(ws.pole)), _p(_i32(ws.zaxis), _ip),
+                                         _p(_i32(ws.xaxis), _ip), _p(_i32(ws.axt), _ip)), "thp_set_frames")
+
+    def _check(self, st, what):
+        if st not in (THP_OK,):
+            raise ThpError(st, what)
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().thp_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        self._check(load().thp_set_stream(self.h, C.c_void_p(stream_ptr)), "thp_set_stream")
+
+    def set_positions(self, x, y, z):
+        self._x, self._y, self._z = _f64(x), _f64(y), _f64(z)
+        self._check(load().thp_set_positions(self.h, _p(self._x), _p(self._y), _p(self._z)), "thp_set_positions")
+
+    def set_rpole(self, rpole):
+        self._check(load().thp_set_rpole(self.h, _p(_f64(rpole))), "thp_set_rpole")
+
+    def set_guess(self, mu):
+        self._check(load().thp_set_guess(self.h, _p(_f64(mu))), "thp_set_guess")
+
+    def nblist(self):
+        self._check(load().thp_nblist(self.h), "thp_nblist")
+
+    def invalidate_list(self):
+        self._check(load().thp_invalidate_list(self.h), "thp_invalidate_list")
+
+    def profile(self, enable):
+        """Start (enable=1) or stop event recording around the fused CG matvec;
+        returns (total ms, launches) recorded since the last call."""
+        ms = C.c_double()
+        cnt = C.c_int()
+        self._check(load().thp_profile(self.h, int(enable), C.byref(ms), C.byref(cnt)), "thp_profile")
+        return ms.value, cnt.value
+
+    def solve(self, guess=GUESS_DIRECT, allow_unconverged=False):
+        info = ThpSolveInfo()
+        st = load().thp_solve(self.h, guess, C.byref(info))
+        if st != THP_OK and not (allow_unconverged and st == THP_E_NOT_CONVERGED):
+            raise ThpError(st, "thp_solve")
+        return {"niter": info.niter, "converged": bool(info.converged), "resnrm": info.resnrm, "epol": info.epol,
+                "ene": tuple(info.ene), "ms": info.ms_total, "status": st}
+
+    def dipoles(self):
+        uind = np.zeros((self.n, 3))
+        uinp = np.zeros((self.n, 3))
+        self._check(load().thp_get_dipoles(self.h, _p(uind), _p(uinp)), "thp_get_dipoles")
+        return uind, uinp
+
+    def field(self):
+        ef = np.zeros((self.n, 2, 3))
+        self._check(load().thp_get_field(self.h, _p(ef)), "thp_get_field")
+        return ef
+
+    def rpole(self):
+        rp = np.zeros((self.n, 13))
+        self._check(load().thp_get_rpole(self.h, _p(rp)), "thp_get_rpole")
+        return rp
+
+    def nblist_half(self, maxelst=1200):
+        nelst = np.zeros(self.n, np.int32)
+        elst = np.zeros((self.n, maxelst), np.int32)
+        self._check(load().thp_get_nblist(self.h, maxelst, _p(nelst, _ip), _p(elst, _ip)), "thp_get_nblist")
+        return nelst, elst
+
+    def pairs(self, maxelst=1200):
+        nelst, elst = self.nblist_half(maxelst)
+        rows = np.repeat(np.arange(self.n), nelst)
+        mask = np.arange(elst.shape[1])[None, :] < nelst[:, None]
+        p = np.stack([rows, elst[mask]], axis=1)
+        return p[np.lexsort((p[:, 1], p[:, 0]))]
+
+    def tmatxb(self, mu, dodiag=True):
+        mu = _f64(mu)
+        out = np.zeros_like(mu)
+        self._check(load().thp_tmatxb(self.h, mu.shape[1], int(dodiag), _p(mu), _p(out)), "thp_tmatxb")
+        return out
+
+    def efld0_direct(self, nrhs=2):
+        ef = np.zeros((self.n, nrhs, 3))
+        self._check(load().thp_efld0_direct(self.h, nrhs, _p(ef)), "thp_efld0_direct")
+        return ef
+
+    def efld0_recip(self):
+        cphi = np.zeros((self.n, 10))
+        self._check(load().thp_efld0_recip(self.h, _p(cphi)), "thp_efld0_recip")
+        return cphi
+
+    def tmatxbrecip(self, mu):
+        mu = _f64(mu)
+        out = np.zeros_like(mu)
+        self._check(load().thp_tmatxbrecip(self.h, mu.shape[1], _p(mu), _p(out)), "thp_tmatxbrecip")
+        return out
+
+    def solve_host(self, x, y, z, rpole=None):
+        """One call on host buffers: positions in, dipoles and energy out."""
+        uind = np.zeros((self.n, 3))
+        uinp = np.zeros((self.n, 3))
+        info = ThpSolveInfo()
+        st = load().thp_solve_host(self.h, _p(_f64(x)), _p(_f64(y)), _p(_f64(z)),
+                                   None if rpole is None else _p(_f64(rpole)), _p(uind), _p(uinp),
+                                   C.byref(info))
+        if st not in (THP_OK, THP_E_NOT_CONVERGED):
+            raise ThpError(st, "thp_solve_host")
+        return uind, uinp, {"niter": info.niter, "converged": bool(info.converged), "epol": info.epol,
+                            "ms": info.ms_total}
