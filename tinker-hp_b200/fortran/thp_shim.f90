@@ -1,0 +1,189 @@
+! thp_shim.f90 -- ISO_C_BINDING layer between Tinker-HP (v1.2 module state)
+! and libthp.so.  Replaces the calls newinduce_pme2 (epolar.f:108,
+! epolar1.f:145) and mlistcell (nblist.f:109) by thp_newinduce_pme2 and
+! thp_mlistcell.  Not compiled in this repository's image (no Fortran
+! compiler); it follows the C declarations of include/thp.h.
+module thp_shim
+  use iso_c_binding
+  implicit none
+  private
+  public :: thp_init, thp_newinduce_pme2, thp_mlistcell, thp_epolar, thp_finalize
+
+  type, bind(C) :: thp_config
+    integer(c_int) :: n
+    real(c_double) :: box(3)
+    real(c_double) :: aewald, ewaldcut, lbuffer
+    integer(c_int) :: nfft(3)
+    integer(c_int) :: bsorder, politer
+    real(c_double) :: poleps
+    integer(c_int) :: precision, max_neighbors, device
+  end type
+
+  type(c_ptr), save :: ctx = c_null_ptr
+  integer(c_int), allocatable, target, save :: off(:,:), idx(:,:)
+
+  interface
+    integer(c_int) function c_ctx_create(cfg, out) bind(C, name="thp_ctx_create")
+      import :: c_int, c_ptr, thp_config
+      type(thp_config), intent(in) :: cfg
+      type(c_ptr), intent(out) :: out
+    end function
+    integer(c_int) function c_ctx_destroy(h) bind(C, name="thp_ctx_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function c_set_params(h, pol, thl, pdm) bind(C, name="thp_set_params")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, pol, thl, pdm
+    end function
+    integer(c_int) function c_set_connectivity(h, offp, idxp, scales) bind(C, name="thp_set_connectivity")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, offp, idxp, scales
+    end function
+    integer(c_int) function c_bind_state(h, x, y, z, rpole, uind, uinp, nelst, elst, maxelst, ep) &
+        bind(C, name="thp_bind_state")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, x, y, z, rpole, uind, uinp, nelst, elst, ep
+      integer(c_int), value :: maxelst
+    end function
+    subroutine c_newinduce_pme2() bind(C, name="newinduce_pme2_")
+    end subroutine
+    subroutine c_mlistcell() bind(C, name="mlistcell_")
+    end subroutine
+    subroutine c_epolar() bind(C, name="epolar_")
+    end subroutine
+    integer(c_int) function c_last_error() bind(C, name="thp_last_error")
+      import :: c_int
+    end function
+  end interface
+
+contains
+
+  ! called once from mechanic after kpolar/kmpole/kewald/cutoffs
+  subroutine thp_init(mixed)
+    use atoms, only: n
+    use boxes, only: xbox, ybox, zbox
+    use ewald, only: aewald
+    use cutoff, only: ewaldcut, lbuffer
+    use pme, only: nfft1, nfft2, nfft3, bsorder
+    use polar, only: polarity, thole, pdamp
+    use polpot, only: politer, poleps, p2scale, p3scale, p4scale, p5scale, p2iscale, p3iscale, &
+                      p4iscale, p5iscale, d1scale, d2scale, d3scale, d4scale, u1scale, u2scale, &
+                      u3scale, u4scale
+    logical, intent(in) :: mixed
+    type(thp_config), target :: cfg
+    real(c_double), target :: scales(16)
+    type(c_ptr), target :: offp(8), idxp(8)
+    integer :: st
+    cfg%n = n
+    cfg%box = [xbox, ybox, zbox]
+    cfg%aewald = aewald
+    cfg%ewaldcut = ewaldcut
+    cfg%lbuffer = lbuffer
+    cfg%nfft = [nfft1, nfft2, nfft3]
+    cfg%bsorder = bsorder
+    cfg%politer = politer
+    cfg%poleps = poleps
+    cfg%precision = merge(1, 0, mixed)
+    cfg%max_neighbors = 0
+    cfg%device = 0
+    st = c_ctx_create(cfg, ctx)
+    if (st /= 0) call fatal
+    st = c_set_params(ctx, c_loc(polarity), c_loc(thole), c_loc(pdamp))
+    if (st /= 0) call fatal
+    call pack_connectivity(offp, idxp)
+    scales = [p2scale, p3scale, p4scale, p5scale, p2iscale, p3iscale, p4iscale, p5iscale, &
+              d1scale, d2scale, d3scale, d4scale, u1scale, u2scale, u3scale, u4scale]
+    st = c_set_connectivity(ctx, c_loc(offp), c_loc(idxp), c_loc(scales))
+    if (st /= 0) call fatal
+  end subroutine
+
+  ! CSR copies (0-based) of couple::i12..i15 and polgrp::ip11..ip14
+  subroutine pack_connectivity(offp, idxp)
+    use atoms, only: n
+    use couple, only: n12, i12, n13, i13, n14, i14, n15, i15
+    use polgrp, only: np11, ip11, np12, ip12, np13, ip13, np14, ip14
+    type(c_ptr), intent(out) :: offp(8), idxp(8)
+    integer :: s, i, j, m, cap
+    cap = max(size(i12,1), size(i13,1), size(i14,1), size(i15,1), size(ip11,1), size(ip12,1), &
+              size(ip13,1), size(ip14,1))
+    if (allocated(off)) deallocate(off, idx)
+    allocate(off(n+1,8), idx(cap*n,8))
+    do s = 1, 8
+      off(1,s) = 0
+      m = 0
+      do i = 1, n
+        do j = 1, count_of(s, i)
+          m = m + 1
+          idx(m,s) = entry_of(s, j, i) - 1
+        end do
+        off(i+1,s) = m
+      end do
+      offp(s) = c_loc(off(1,s))
+      idxp(s) = c_loc(idx(1,s))
+    end do
+  contains
+    integer function count_of(s, i)
+      integer, intent(in) :: s, i
+      select case (s)
+      case (1); count_of = n12(i)
+      case (2); count_of = n13(i)
+      case (3); count_of = n14(i)
+      case (4); count_of = n15(i)
+      case (5); count_of = np11(i)
+      case (6); count_of = np12(i)
+      case (7); count_of = np13(i)
+      case default; count_of = np14(i)
+      end select
+    end function
+    integer function entry_of(s, j, i)
+      integer, intent(in) :: s, j, i
+      select case (s)
+      case (1); entry_of = i12(j,i)
+      case (2); entry_of = i13(j,i)
+      case (3); entry_of = i14(j,i)
+      case (4); entry_of = i15(j,i)
+      case (5); entry_of = ip11(j,i)
+      case (6); entry_of = ip12(j,i)
+      case (7); entry_of = ip13(j,i)
+      case default; entry_of = ip14(j,i)
+      end select
+    end function
+  end subroutine
+
+  subroutine bind_all()
+    use atoms, only: x, y, z
+    use mpole, only: rpole
+    use polar, only: uind, uinp
+    use neigh, only: nelst, elst, maxelst
+    use energi, only: ep
+    integer :: st
+    st = c_bind_state(ctx, c_loc(x), c_loc(y), c_loc(z), c_loc(rpole), c_loc(uind), c_loc(uinp), &
+                      c_loc(nelst), c_loc(elst), int(maxelst, c_int), c_loc(ep))
+    if (st /= 0) call fatal
+  end subroutine
+
+  subroutine thp_newinduce_pme2
+    call bind_all()
+    call c_newinduce_pme2()
+    if (c_last_error() /= 0 .and. c_last_error() /= 3) call fatal
+  end subroutine
+
+  subroutine thp_mlistcell
+    call bind_all()
+    call c_mlistcell()
+    if (c_last_error() /= 0) call fatal
+  end subroutine
+
+  subroutine thp_epolar
+    call bind_all()
+    call c_epolar()
+    if (c_last_error() /= 0 .and. c_last_error() /= 3) call fatal
+  end subroutine
+
+  subroutine thp_finalize
+    integer :: st
+    if (c_associated(ctx)) st = c_ctx_destroy(ctx)
+    ctx = c_null_ptr
+  end subroutine
+end module thp_shim
