@@ -130,6 +130,25 @@ int thp_solve_host(thp_ctx* ctx, const double* x, const double* y, const double*
 size_t thp_footprint(const thp_config* cfg);
 const char* thp_status_string(int status);
 
+/* ---- allocation-free energy (no counterpart in the reference) ------------ */
+/* For callers that cannot allocate device memory at the point of use: a host
+ * code whose device memory is pooled up front by another runtime (OpenACC /
+ * CUDA-Fortran data regions), work enqueued during a CUDA stream capture, or
+ * a latency-critical loop that must not synchronise on cudaMalloc/cudaFree.
+ * Computes Epol = -1/2 * electric * sum_i uind_i . E_p,i (kcal/mol) from
+ * device arrays d_uind [n][3] and d_ef [n][2][3] (E0 with the p field second,
+ * as ef(3,2,n)) into the device scalar d_epol, on the caller's current device
+ * and stream (cudaStream_t as void*, NULL = legacy default stream).
+ * Allocates nothing: its scratch (per-block partial sums and a counter,
+ * 128 KiB) is a fixed array in the library's device image, held on every GPU
+ * that loads the library until the process exits.  n must be at most
+ * THP_NOALLOC_MAX_ATOMS, otherwise THP_E_INVALID.  The first call on a device
+ * looks up the scratch's device address and should come before any stream
+ * capture.  All calls share the scratch: calls that overlap on the GPU race,
+ * so order them on one stream. */
+#define THP_NOALLOC_MAX_ATOMS 4194304
+int thp_epolar_noalloc(int n, const double* d_uind, const double* d_ef, double* d_epol, void* stream);
+
 /* ---- Fortran drop-ins ---------------------------------------------------- */
 /* Make ctx current and bind the module arrays the reference reads/writes:
  * atoms::x,y,z(n), mpole::rpole(13,n), polar::uind,uinp(3,n),

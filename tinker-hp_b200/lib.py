@@ -23,6 +23,7 @@ THP_E_OOM_ADMISSION = 7
 THP_E_BOX_TOO_SMALL = 8
 THP_E_NO_DEVICE = 9
 THP_E_STATE = 10
+NOALLOC_MAX_ATOMS = 4194304
 
 FP64 = 0
 MIXED = 1
@@ -93,6 +94,7 @@ def load():
         "thp_status_string": ([C.c_int], C.c_char_p),
         "thp_bind_state": ([vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_int, _dp], C.c_int),
         "thp_last_error": ([], C.c_int),
+        "thp_epolar_noalloc": ([C.c_int, vp, vp, vp, vp], C.c_int),
         "newinduce_pme2_": ([], None),
         "tmatxb_pme_": ([_ip, _ip, _dp, _dp], None),
         "efld0_direct_": ([_ip, _dp], None),
