@@ -103,13 +103,17 @@ void build_special_pairs(Ctx& c, const int* const* off, const int* const* idx, c
 int upload_special_pairs(Ctx& c) {
   cudaFree(c.d_sp_off);
   cudaFree(c.d_sp_k);
+  cudaFree(c.d_sp_ks);
   cudaFree(c.d_sp_s);
   c.d_sp_off = nullptr;
   c.d_sp_k = nullptr;
+  c.d_sp_ks = nullptr;
   c.d_sp_s = nullptr;
+  c.have_list = false;  // sorted partner numbers are made at the next sort
   int st;
   if ((st = dmalloc(c, &c.d_sp_off, c.n + 1, "alloc sp_off"))) return st;
   if ((st = dmalloc(c, &c.d_sp_k, c.sp_k.size(), "alloc sp_k"))) return st;
+  if ((st = dmalloc(c, &c.d_sp_ks, c.sp_k.size(), "alloc sp_ks"))) return st;
   if ((st = dmalloc(c, &c.d_sp_s, c.sp_s.size(), "alloc sp_s"))) return st;
   cudaMemcpy(c.d_sp_off, c.sp_off.data(), sizeof(int) * (c.n + 1), cudaMemcpyHostToDevice);
   if (!c.sp_k.empty()) {
@@ -218,7 +222,7 @@ int ensure_coef(thp_ctx* h) {
 }
 
 void free_ctx(Ctx& c) {
-  void* ptrs[] = {c.d_cell_count, c.d_cell_start, c.d_cell_fill, c.d_atom_cell, c.d_scell, c.d_perm, c.d_iperm,
+  void* ptrs[] = {c.d_mrec, c.d_mrecf, c.d_sp_ks, c.d_cell_count, c.d_cell_start, c.d_cell_fill, c.d_atom_cell, c.d_scell, c.d_perm, c.d_iperm,
                   c.d_xyz_orig, c.d_par_orig, c.d_rpole_orig, c.d_pole_local, c.d_frames, c.d_pos, c.d_posf,
                   c.d_thole, c.d_pol, c.d_rpole, c.d_sp_off, c.d_sp_k, c.d_sp_s, c.d_pos_built, c.d_nnb, c.d_nb,
                   c.d_npr, c.d_pk, c.d_pc3, c.d_pc5, c.d_ef, c.d_mu, c.d_res, c.d_h, c.d_pp, c.d_zr, c.d_dip,
@@ -339,6 +343,8 @@ int thp_ctx_create(const thp_config* cfg, thp_ctx** out) {
   if (!st) st = dmalloc(c, &c.d_thole, n, "thole");
   if (!st) st = dmalloc(c, &c.d_pol, n, "pol");
   if (!st) st = dmalloc(c, &c.d_rpole, 10 * n, "rpole sorted");
+  if (!st) st = dmalloc(c, &c.d_mrec, 12 * n, "mrec");
+  if (!st) st = dmalloc(c, &c.d_mrecf, 12 * n, "mrecf");
   if (!st) st = dmalloc(c, &c.d_pos_built, n, "pos built");
   if (!st) st = dmalloc(c, &c.d_nnb, n, "nnb");
   if (!st) st = dmalloc(c, &c.d_nb, (size_t)c.maxnb * npad, "nb");

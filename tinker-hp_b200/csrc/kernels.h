@@ -26,6 +26,7 @@ int zero_grid(Ctx& c);
 struct PmeGeom;
 PmeGeom pme_geom(const Ctx& c);
 int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode);
+int launch_gather_dip(Ctx& c, double* d_out, bool check_stop);
 
 // solver.cu
 int run_pcg(Ctx& c, int guess);

@@ -93,7 +93,7 @@ __global__ void k_gather_sorted(int n, Box box, const int* __restrict__ perm, co
                                 const double* __restrict__ pol, const double* __restrict__ rpole13,
                                 int have_rpole, double4* __restrict__ pos, float4* __restrict__ posf,
                                 double* __restrict__ sthole, double* __restrict__ spol,
-                                double* __restrict__ srpole) {
+                                double* __restrict__ srpole, double* __restrict__ mrec, float* __restrict__ mrecf) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   int o = perm[s];
@@ -119,50 +119,104 @@ __global__ void k_gather_sorted(int n, Box box, const int* __restrict__ perm, co
     q[7] = r[8];
     q[8] = r[9];
     q[9] = r[12];
+    double rec[12] = {thole[o], r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[8], r[9], r[12], 0.0};
+    double2* m2 = reinterpret_cast<double2*>(mrec + (size_t)s * 12);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) m2[k] = make_double2(rec[2 * k], rec[2 * k + 1]);
+    if (mrecf) {
+      float4* f4 = reinterpret_cast<float4*>(mrecf + (size_t)s * 12);
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        f4[k] = make_float4((float)rec[4 * k], (float)rec[4 * k + 1], (float)rec[4 * k + 2], (float)rec[4 * k + 3]);
+    }
   }
 }
 
-__device__ __forceinline__ int unique_offsets(int c, int nc, int* out) {
-  int m = 0;
-  for (int o = -2; o <= 2; ++o) {
-    int v = ((c + o) % nc + nc) % nc;
-    bool dup = false;
-    for (int q = 0; q < m; ++q) dup |= (out[q] == v);
-    if (!dup) out[m++] = v;
-  }
-  return m;
+__global__ void k_sp_to_sorted(int m, const int* __restrict__ iperm, const int* __restrict__ sp_k,
+                               int* __restrict__ sp_ks) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < m) sp_ks[q] = iperm[sp_k[q]];
 }
 
-__global__ void k_build_list(int n, int npad, Box box, double mbuf2, int ncx, int ncy, int ncz,
-                             const double4* __restrict__ pos, const int* __restrict__ scell,
-                             const int* __restrict__ cell_start, const int* __restrict__ cell_count, int maxnb,
-                             int* __restrict__ nnb, int* __restrict__ nb, int* __restrict__ flags) {
+// Candidate search over the +-2 cell neighbourhood.  For every (dz, dy) row
+// the cells cx-2..cx+2 are consecutive in the cell order, so their atoms form
+// one contiguous range of sorted indices (two at a periodic wrap); a thread
+// scans 25 such ranges instead of 125 cells.  Grids narrower than 5 cells in
+// a dimension visit each cell of that dimension once.
+__device__ __forceinline__ void row_ranges(int c, int nc, int& a0, int& a1, int& b0, int& b1) {
+  // cell x-intervals [a0, a1] and [b0, b1] (b empty when b0 > b1)
+  if (nc <= 5) {
+    a0 = 0;
+    a1 = nc - 1;
+    b0 = 1;
+    b1 = 0;
+    return;
+  }
+  int lo = c - 2, hi = c + 2;
+  if (lo < 0) {
+    a0 = 0;
+    a1 = hi;
+    b0 = lo + nc;
+    b1 = nc - 1;
+  } else if (hi >= nc) {
+    a0 = lo;
+    a1 = nc - 1;
+    b0 = 0;
+    b1 = hi - nc;
+  } else {
+    a0 = lo;
+    a1 = hi;
+    b0 = 1;
+    b1 = 0;
+  }
+}
+
+__device__ __forceinline__ int axis_cells(int c, int nc, int q) {
+  // q-th distinct cell of the +-2 window along y or z (q < min(nc, 5))
+  return nc <= 5 ? q : ((c + q - 2) % nc + nc) % nc;
+}
+
+__global__ void __launch_bounds__(128) k_build_list(int n, int npad, Box box, double mbuf2, int ncx, int ncy,
+                                                    int ncz, const double4* __restrict__ pos,
+                                                    const int* __restrict__ scell, const int* __restrict__ cell_start,
+                                                    const int* __restrict__ cell_count, int maxnb,
+                                                    int* __restrict__ nnb, int* __restrict__ nb,
+                                                    int* __restrict__ flags) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double4 pi = pos[i];
-  int c = scell[i];
-  int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
-  int ux[5], uy[5], uz[5];
-  int mx = unique_offsets(cx, ncx, ux), my = unique_offsets(cy, ncy, uy), mz = unique_offsets(cz, ncz, uz);
+  const double4 pi = pos[i];
+  const int c = scell[i];
+  const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
+  int a0, a1, b0, b1;
+  row_ranges(cx, ncx, a0, a1, b0, b1);
+  const int my = min(ncy, 5), mz = min(ncz, 5);
   int cnt = 0;
-  for (int a = 0; a < mz; ++a)
-    for (int b = 0; b < my; ++b)
-      for (int d = 0; d < mx; ++d) {
-        int cell = (uz[a] * ncy + uy[b]) * ncx + ux[d];
-        int st = cell_start[cell], m = cell_count[cell];
-        for (int k = st; k < st + m; ++k) {
+  for (int qz = 0; qz < mz; ++qz) {
+    const int z = axis_cells(cz, ncz, qz);
+    for (int qy = 0; qy < my; ++qy) {
+      const int y = axis_cells(cy, ncy, qy);
+      const int rowbase = (z * ncy + y) * ncx;
+#pragma unroll
+      for (int part = 0; part < 2; ++part) {
+        const int x0 = part ? b0 : a0, x1 = part ? b1 : a1;
+        if (x0 > x1) continue;
+        const int k0 = cell_start[rowbase + x0];
+        const int k1 = cell_start[rowbase + x1] + cell_count[rowbase + x1];
+        for (int k = k0; k < k1; ++k) {
           if (k == i) continue;
-          double4 pk = pos[k];
+          const double4 pk = pos[k];
           // midpointimage (domdecstuff.f:1773): pos = xi - xk, imaged
           double xr = __dadd_rn(pi.x, -pk.x), yr = __dadd_rn(pi.y, -pk.y), zr = __dadd_rn(pi.z, -pk.z);
           image3(box, xr, yr, zr);
-          double r2 = r2_exact(xr, yr, zr);
+          const double r2 = r2_exact(xr, yr, zr);
           if (r2 <= mbuf2) {
             if (cnt < maxnb) nb[(size_t)cnt * npad + i] = k;
             ++cnt;
           }
         }
       }
+    }
+  }
   nnb[i] = cnt;
   if (cnt > maxnb) atomicOr(flags, DEV_LIST_OVERFLOW);
 }
@@ -272,6 +326,8 @@ int launch_sort_atoms(Ctx& c) {
   k_cell_sort<<<(c.ncell + kBlock - 1) / kBlock, kBlock, 0, s>>>(c.ncell, c.d_cell_start, c.d_cell_count,
                                                                  c.d_perm, c.d_iperm, c.d_scell);
   c.have_perm = true;
+  const int m = (int)c.sp_k.size();
+  if (m > 0) k_sp_to_sorted<<<(m + 255) / 256, 256, 0, s>>>(m, c.d_iperm, c.d_sp_k, c.d_sp_ks);
   return cuda_status(cudaGetLastError(), &c, "sort atoms");
 }
 
@@ -282,7 +338,8 @@ int launch_gather_sorted(Ctx& c) {
   k_gather_sorted<<<nb, kBlock, 0, c.stream>>>(n, c.box, c.d_perm, c.d_xyz_orig, c.d_par_orig,
                                                c.d_par_orig + n, c.d_par_orig + 2 * n, c.d_rpole_orig,
                                                c.have_rpole ? 1 : 0, c.d_pos, c.mixed ? c.d_posf : nullptr,
-                                               c.d_thole, c.d_pol, c.d_rpole);
+                                               c.d_thole, c.d_pol, c.d_rpole, c.d_mrec,
+                                               c.mixed ? c.d_mrecf : nullptr);
   return cuda_status(cudaGetLastError(), &c, "gather sorted");
 }
 
@@ -290,7 +347,7 @@ int launch_build_list(Ctx& c) {
   const int n = c.n;
   const double rl = c.cfg.ewaldcut + c.cfg.lbuffer;
   const double mbuf2 = rl * rl;
-  k_build_list<<<(n + kBlock - 1) / kBlock, kBlock, 0, c.stream>>>(
+  k_build_list<<<(n + 127) / 128, 128, 0, c.stream>>>(
       n, c.npad, c.box, mbuf2, c.nc[0], c.nc[1], c.nc[2], c.d_pos, c.d_scell, c.d_cell_start, c.d_cell_count,
       c.maxnb, c.d_nnb, c.d_nb, c.d_flags);
   cudaMemcpyAsync(c.d_pos_built, c.d_pos, sizeof(double4) * n, cudaMemcpyDeviceToDevice, c.stream);

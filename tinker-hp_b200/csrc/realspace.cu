@@ -25,11 +25,34 @@ struct EwaldConst {
   double a, afac1, afac2, afac3;  // 2a/sqrt(pi), 4a^3/sqrt(pi), 8a^5/sqrt(pi)
 };
 
+template <bool MIXED>
+struct Rec;
+template <>
+struct Rec<false> {  // FP64 record: thole, q, d(3), Q(6)
+  double th, q, dx, dy, dz, qxx, qxy, qxz, qyy, qyz, qzz;
+  __device__ __forceinline__ void load(const double* m, const float*, int k) {
+    const double2* p = reinterpret_cast<const double2*>(m + (size_t)k * 12);
+    double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3), e = __ldg(p + 4), f = __ldg(p + 5);
+    th = a.x; q = a.y; dx = b.x; dy = b.y; dz = c.x; qxx = c.y; qxy = d.x; qxz = d.y; qyy = e.x; qyz = e.y;
+    qzz = f.x;
+  }
+};
+template <>
+struct Rec<true> {  // FP32 record of the mixed form
+  float th, q, dx, dy, dz, qxx, qxy, qxz, qyy, qyz, qzz;
+  __device__ __forceinline__ void load(const double*, const float* m, int k) {
+    const float4* p = reinterpret_cast<const float4*>(m + (size_t)k * 12);
+    float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    th = a.x; q = a.y; dx = a.z; dy = a.w; dz = b.x; qxx = b.y; qxy = b.z; qxz = b.w; qyy = c.x; qyz = c.y;
+    qzz = c.z;
+  }
+};
+
 template <bool MIXED, bool FIELD>
 __global__ void __launch_bounds__(kBlock) k_efld0_coef(
     int n, int npad, Box box, double cut2, EwaldConst ew, const double4* __restrict__ pos,
-    const double* __restrict__ thole, const double* __restrict__ rp, const int* __restrict__ perm,
-    const int* __restrict__ sp_off, const int* __restrict__ sp_k, const double* __restrict__ sp_s,
+    const double* __restrict__ mrec, const float* __restrict__ mrecf, const int* __restrict__ perm,
+    const int* __restrict__ sp_off, const int* __restrict__ sp_ks, const double* __restrict__ sp_s,
     const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb, int* __restrict__ npr, int* __restrict__ pk,
     void* __restrict__ pc3v, void* __restrict__ pc5v, int maxpr, double* __restrict__ ef, int* __restrict__ flags) {
   using T = typename std::conditional<MIXED, float, double>::type;
@@ -38,7 +61,7 @@ __global__ void __launch_bounds__(kBlock) k_efld0_coef(
   T* pc3 = (T*)pc3v;
   T* pc5 = (T*)pc5v;
   const double4 pi = pos[i];
-  const double thi = thole[i];
+  const double thi = mrec[(size_t)i * 12];
   const int io = perm[i];
   const int s0 = sp_off[io], s1 = sp_off[io + 1];
   double e[6] = {0, 0, 0, 0, 0, 0};
@@ -46,24 +69,23 @@ __global__ void __launch_bounds__(kBlock) k_efld0_coef(
   int cnt = 0;
 #pragma unroll 1
   for (int s = 0; s < nn; ++s) {
-    const int k = nb[(size_t)s * npad + i];
+    const int k = __ldg(nb + (size_t)s * npad + i);
     const double4 pk4 = pos[k];
     double xr = pk4.x - pi.x, yr = pk4.y - pi.y, zr = pk4.z - pi.z;
     image3(box, xr, yr, zr);
     const double r2d = r2_exact(xr, yr, zr);
     if (r2d > cut2) continue;
-    // scale factors of this pair (1 unless listed)
+    // scale factors of this pair (1 unless listed), partners in sorted numbering
     double ds = 1.0, ps = 1.0, us = 1.0;
-    if (s1 > s0) {
-      const int ko = perm[k];
-      for (int q = s0; q < s1; ++q)
-        if (sp_k[q] == ko) {
-          ds = sp_s[3 * q];
-          ps = sp_s[3 * q + 1];
-          us = sp_s[3 * q + 2];
-          break;
-        }
-    }
+    for (int q = s0; q < s1; ++q)
+      if (__ldg(sp_ks + q) == k) {
+        ds = sp_s[3 * q];
+        ps = sp_s[3 * q + 1];
+        us = sp_s[3 * q + 2];
+        break;
+      }
+    Rec<MIXED> rk;
+    rk.load(mrec, mrecf, k);
     const T x = (T)xr, y = (T)yr, z = (T)zr, r2 = (T)r2d;
     const T r = sqrt(r2);
     const T rr1 = T(1) / r;
@@ -81,8 +103,8 @@ __global__ void __launch_bounds__(kBlock) k_efld0_coef(
     // dampthole / damptholed (AMOEBA branch)
     T l3 = 1, l5 = 1, l7 = 1;
     const double pdd = pi.w * pk4.w;
-    double pg = fmin(thi, thole[k]);
-    if (pg == 0.0) pg = fmax(thi, thole[k]);
+    double pg = fmin(thi, (double)rk.th);
+    if (pg == 0.0) pg = fmax(thi, (double)rk.th);
     if (pdd != 0.0 && pg != 0.0) {
       const T t = r / (T)pdd;
       const T damp = (T)pg * (t * t * t);
@@ -94,13 +116,11 @@ __global__ void __launch_bounds__(kBlock) k_efld0_coef(
       }
     }
     if (FIELD) {
-      const double* rk = rp + (size_t)k * 10;
-      const T ck = (T)rk[0], dkx = (T)rk[1], dky = (T)rk[2], dkz = (T)rk[3];
-      const T qkxx = (T)rk[4], qkxy = (T)rk[5], qkxz = (T)rk[6], qkyy = (T)rk[7], qkyz = (T)rk[8], qkzz = (T)rk[9];
+      const T ck = rk.q, dkx = rk.dx, dky = rk.dy, dkz = rk.dz;
       const T dkr = dkx * x + dky * y + dkz * z;
-      const T qkx = qkxx * x + qkxy * y + qkxz * z;
-      const T qky = qkxy * x + qkyy * y + qkyz * z;
-      const T qkz = qkxz * x + qkyz * y + qkzz * z;
+      const T qkx = rk.qxx * x + rk.qxy * y + rk.qxz * z;
+      const T qky = rk.qxy * x + rk.qyy * y + rk.qyz * z;
+      const T qkz = rk.qxz * x + rk.qyz * y + rk.qzz * z;
       const T qkr = qkx * x + qky * y + qkz * z;
       T sc = (T)ds;
       T dmp3 = bn1 - (T(1) - sc * l3) * rr3;
@@ -217,7 +237,7 @@ int launch_efld0_coef(Ctx& c, bool with_field) {
   const double cut2 = c.cfg.ewaldcut * c.cfg.ewaldcut;
   EwaldConst ew = ewald_const(c.cfg.aewald);
 #define THP_EFLD0_ARGS                                                                                          \
-  c.n, c.npad, c.box, cut2, ew, c.d_pos, c.d_thole, c.d_rpole, c.d_perm, c.d_sp_off, c.d_sp_k, c.d_sp_s, c.d_nnb, \
+  c.n, c.npad, c.box, cut2, ew, c.d_pos, c.d_mrec, c.d_mrecf, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_s, c.d_nnb, \
       c.d_nb, c.maxnb, c.d_npr, c.d_pk, c.d_pc3, c.d_pc5, c.maxpr, c.d_ef, c.d_flags
   if (c.mixed) {
     if (with_field)

@@ -6,7 +6,7 @@
 //   2. cuFFT forward, qfac, cuFFT backward;
 //   3. fused matvec kernel: PME gather + real-space row + diagonal and self
 //      terms -> h; partial pp.h; the last block forms gg and alpha;
-//   4. update kernel: mu += alpha pp, res -= alpha h, zr = diag res; partial
+//   5. update kernel: mu += alpha pp, res -= alpha h, zr = diag res; partial
 //      ggnew and ene; the last block forms beta, the residual norm and the
 //      convergence / stop flags.
 // Reductions write per-block partials summed in a fixed order by the last
@@ -76,8 +76,8 @@ __device__ __forceinline__ double diag_of(double p) { return p == 0.0 ? kTinyPol
 // init: also res = ef - h, zr = diag res, pp = zr, ggold = sum res.zr
 // iter: gg = sum pp.h, alpha = ggold / gg
 template <bool MIXED>
-__global__ void __launch_bounds__(kBlock) k_cg_matvec(PairRows pr, Box box, PmeGeom g, const double4* __restrict__ pos,
-                                                      const float4* __restrict__ posf, const void* __restrict__ grid,
+__global__ void __launch_bounds__(kBlock) k_cg_matvec(PairRows pr, Box box, const double4* __restrict__ pos,
+                                                      const float4* __restrict__ posf, const double* __restrict__ dipf,
                                                       const double* __restrict__ x, const float* __restrict__ xf,
                                                       const double* __restrict__ pol, const double* __restrict__ ef,
                                                       double term, int init, double* __restrict__ h,
@@ -99,12 +99,8 @@ __global__ void __launch_bounds__(kBlock) k_cg_matvec(PairRows pr, Box box, PmeG
       for (int q = 0; q < 6; ++q) acc[q] = 0.0;
       tmatxb_row64(pr, box, i, pos, x, acc);
     }
-    double dip[6];
-    if (MIXED)
-      gather_dip<float>(g, pos[i], (const cufftComplex*)grid, dip);
-    else
-      gather_dip<double>(g, pos[i], (const cufftDoubleComplex*)grid, dip);
-    double xi[6];
+    double dip[6], xi[6];
+    load6(dipf + (size_t)i * 6, dip);
     load6(x + (size_t)i * 6, xi);
     const double p = pol[i];
     const double ip = (p == 0.0) ? 1.0 / kTinyPol : 1.0 / p;
@@ -273,17 +269,18 @@ static void prof_mark(Ctx& c) {
 
 static int launch_matvec(Ctx& c, const double* x, int init) {
   const int nb = (c.n + kBlock - 1) / kBlock;
+  int st = launch_gather_dip(c, c.d_dip, init == 0);
+  if (st) return st;
   prof_mark(c);
   PairRows pr = pair_rows(c);
-  PmeGeom g = pme_geom(c);
   const double a = c.cfg.aewald;
   const double term = (4.0 / 3.0) * a * a * a / kSqrtPi;
   if (c.mixed)
-    k_cg_matvec<true><<<nb, kBlock, 0, c.stream>>>(pr, c.box, g, c.d_pos, c.d_posf, c.d_grid, x, c.d_vecf, c.d_pol,
+    k_cg_matvec<true><<<nb, kBlock, 0, c.stream>>>(pr, c.box, c.d_pos, c.d_posf, c.d_dip, x, c.d_vecf, c.d_pol,
                                                    c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, c.d_cg,
                                                    c.d_partials);
   else
-    k_cg_matvec<false><<<nb, kBlock, 0, c.stream>>>(pr, c.box, g, c.d_pos, c.d_posf, c.d_grid, x, c.d_vecf, c.d_pol,
+    k_cg_matvec<false><<<nb, kBlock, 0, c.stream>>>(pr, c.box, c.d_pos, c.d_posf, c.d_dip, x, c.d_vecf, c.d_pol,
                                                     c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, c.d_cg,
                                                     c.d_partials);
   prof_mark(c);
