@@ -45,6 +45,7 @@ METRIC = "induced-dipole solves/s & p99 latency, mixed vs FP64 on one B200 at 1e
 WORKLOADS = {
     # name: (waters, cfg index for seeds)
     "water-288k": (96000, 2),
+    "water-96k": (32000, 2),
     "water-32k": (10800, 1),
     "water-1944": (648, 0),
 }

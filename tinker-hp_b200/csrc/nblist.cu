@@ -106,6 +106,8 @@ __global__ void k_gather_sorted(int n, Box box, const int* __restrict__ perm, co
   }
   sthole[s] = thole[o];
   spol[s] = pol[o];
+  // pair-pass record: thole always, multipoles once they are known
+  double rec[12] = {thole[o], 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (have_rpole) {
     const double* r = rpole13 + (size_t)o * 13;
     double* q = srpole + (size_t)s * 10;
@@ -119,16 +121,18 @@ __global__ void k_gather_sorted(int n, Box box, const int* __restrict__ perm, co
     q[7] = r[8];
     q[8] = r[9];
     q[9] = r[12];
-    double rec[12] = {thole[o], r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[8], r[9], r[12], 0.0};
-    double2* m2 = reinterpret_cast<double2*>(mrec + (size_t)s * 12);
+    const double m[10] = {r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[8], r[9], r[12]};
 #pragma unroll
-    for (int k = 0; k < 6; ++k) m2[k] = make_double2(rec[2 * k], rec[2 * k + 1]);
-    if (mrecf) {
-      float4* f4 = reinterpret_cast<float4*>(mrecf + (size_t)s * 12);
+    for (int k = 0; k < 10; ++k) rec[1 + k] = m[k];
+  }
+  double2* m2 = reinterpret_cast<double2*>(mrec + (size_t)s * 12);
 #pragma unroll
-      for (int k = 0; k < 3; ++k)
-        f4[k] = make_float4((float)rec[4 * k], (float)rec[4 * k + 1], (float)rec[4 * k + 2], (float)rec[4 * k + 3]);
-    }
+  for (int k = 0; k < 6; ++k) m2[k] = make_double2(rec[2 * k], rec[2 * k + 1]);
+  if (mrecf) {
+    float4* f4 = reinterpret_cast<float4*>(mrecf + (size_t)s * 12);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      f4[k] = make_float4((float)rec[4 * k], (float)rec[4 * k + 1], (float)rec[4 * k + 2], (float)rec[4 * k + 3]);
   }
 }
 

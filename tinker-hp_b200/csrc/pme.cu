@@ -76,50 +76,68 @@ __global__ void k_spread_mpole(int n, PmeGeom g, const double4* __restrict__ pos
 }
 
 // grid_uind_site (pmestuff.f:280-405); d dipoles in Re, p dipoles in Im.
-// One warp per site: lanes 0..5 load (mode 1: update pp = zr + beta*pp,
-// inducepcg_pme2.f:553-559) the six dipole components, every lane forms the
-// order-5 weights, and the 125 stencil points are spread x-fastest in four
-// rounds so that each atomic instruction touches a few contiguous grid rows.
+// One thread per site (the 125 atomics of neighbouring threads land in
+// different L2 slices; a warp-per-site variant that made them contiguous
+// measured 1.6x slower).  mode 1 first forms pp = zr + beta*pp
+// (inducepcg_pme2.f:553-559) and writes it back.
 template <typename T>
-__global__ void __launch_bounds__(256) k_spread_dip(int n, PmeGeom g, const double4* __restrict__ pos,
+__global__ void __launch_bounds__(128) k_spread_dip(int n, PmeGeom g, const double4* __restrict__ pos,
                                                    double* __restrict__ vec, const double* __restrict__ zr,
                                                    float* __restrict__ vecf, const CgScalars* __restrict__ cg,
                                                    int mode, typename Cplx<T>::type* __restrict__ grid) {
   if (mode == 1 && cg->stop) return;
-  const int lane = threadIdx.x & 31;
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double v = 0.0;
-  if (lane < 6) {
-    v = vec[(size_t)i * 6 + lane];
-    if (mode == 1) {
-      v = zr[(size_t)i * 6 + lane] + cg->beta[lane < 3 ? 0 : 1] * v;
-      vec[(size_t)i * 6 + lane] = v;
-    }
-    if (vecf) vecf[(size_t)i * 6 + lane] = (float)v;
+  double v[6];
+  const double2* v2 = reinterpret_cast<const double2*>(vec + (size_t)i * 6);
+  double2 a0 = v2[0], a1 = v2[1], a2 = v2[2];
+  v[0] = a0.x; v[1] = a0.y; v[2] = a1.x; v[3] = a1.y; v[4] = a2.x; v[5] = a2.y;
+  if (mode == 1) {
+    const double2* z2 = reinterpret_cast<const double2*>(zr + (size_t)i * 6);
+    double2 b0 = z2[0], b1 = z2[1], b2 = z2[2];
+    double bd = cg->beta[0], bp = cg->beta[1];
+    v[0] = b0.x + bd * v[0];
+    v[1] = b0.y + bd * v[1];
+    v[2] = b1.x + bd * v[2];
+    v[3] = b1.y + bp * v[3];
+    v[4] = b2.x + bp * v[4];
+    v[5] = b2.y + bp * v[5];
+    double2* w2 = reinterpret_cast<double2*>(vec + (size_t)i * 6);
+    w2[0] = make_double2(v[0], v[1]);
+    w2[1] = make_double2(v[2], v[3]);
+    w2[2] = make_double2(v[4], v[5]);
   }
-  double vv[6];
+  if (vecf) {
+    float2* o = reinterpret_cast<float2*>(vecf + (size_t)i * 6);
+    o[0] = make_float2((float)v[0], (float)v[1]);
+    o[1] = make_float2((float)v[2], (float)v[3]);
+    o[2] = make_float2((float)v[4], (float)v[5]);
+  }
+  double4 p = pos[i];
+  T tx[kBs][2], ty[kBs][2], tz[kBs][2];
+  int gx = bspline_axis<2, T>(p.x, g.recip[0], g.n1, tx);
+  int gy = bspline_axis<2, T>(p.y, g.recip[1], g.n2, ty);
+  int gz = bspline_axis<2, T>(p.z, g.recip[2], g.n3, tz);
+  T fd[3] = {(T)(g.a[0] * v[0]), (T)(g.a[1] * v[1]), (T)(g.a[2] * v[2])};
+  T fp[3] = {(T)(g.a[0] * v[3]), (T)(g.a[1] * v[4]), (T)(g.a[2] * v[5])};
 #pragma unroll
-  for (int q = 0; q < 6; ++q) vv[q] = __shfl_sync(0xffffffffu, v, q);
-  const double4 p = pos[i];
-  T x0[kBs], x1[kBs], x2[kBs], y0[kBs], y1[kBs], y2[kBs], z0[kBs], z1[kBs], z2[kBs];
-  const int gx = bspline_axis_split<2, T>(p.x, g.recip[0], g.n1, x0, x1, x2);
-  const int gy = bspline_axis_split<2, T>(p.y, g.recip[1], g.n2, y0, y1, y2);
-  const int gz = bspline_axis_split<2, T>(p.z, g.recip[2], g.n3, z0, z1, z2);
-  const T fd0 = (T)(g.a[0] * vv[0]), fd1 = (T)(g.a[1] * vv[1]), fd2 = (T)(g.a[2] * vv[2]);
-  const T fp0 = (T)(g.a[0] * vv[3]), fp1 = (T)(g.a[1] * vv[4]), fp2 = (T)(g.a[2] * vv[5]);
+  for (int c = 0; c < kBs; ++c) {
+    size_t kk = (size_t)wrapk(gz + c, g.n3);
+    T v0 = tz[c][0], v1 = tz[c][1];
 #pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const int q = lane + 32 * r;
-    if (q < kBs * kBs * kBs) {
-      const int a = q % kBs, b = (q / kBs) % kBs, c = q / (kBs * kBs);
-      const T t0 = pick5(x0, a), t1 = pick5(x1, a);
-      const T u0 = pick5(y0, b), u1 = pick5(y1, b);
-      const T v0 = pick5(z0, c), v1 = pick5(z1, c);
-      const T re = (fd1 * u1 * v0 + fd2 * u0 * v1) * t0 + fd0 * u0 * v0 * t1;
-      const T im = (fp1 * u1 * v0 + fp2 * u0 * v1) * t0 + fp0 * u0 * v0 * t1;
-      const size_t idx = ((size_t)wrapk(gz + c, g.n3) * g.n2 + wrapk(gy + b, g.n2)) * g.n1 + wrapk(gx + a, g.n1);
-      grid_add(grid, idx, re, im);
+    for (int b = 0; b < kBs; ++b) {
+      size_t jj = (size_t)wrapk(gy + b, g.n2);
+      T u0 = ty[b][0], u1 = ty[b][1];
+      T term01 = fd[1] * u1 * v0 + fd[2] * u0 * v1;
+      T term11 = fd[0] * u0 * v0;
+      T term02 = fp[1] * u1 * v0 + fp[2] * u0 * v1;
+      T term12 = fp[0] * u0 * v0;
+      size_t row = (kk * g.n2 + jj) * g.n1;
+#pragma unroll
+      for (int a = 0; a < kBs; ++a) {
+        int ii = wrapk(gx + a, g.n1);
+        grid_add(grid, row + ii, term01 * tx[a][0] + term11 * tx[a][1], term02 * tx[a][0] + term12 * tx[a][1]);
+      }
     }
   }
 }
@@ -227,55 +245,22 @@ __global__ void k_gather_mpole(int n, PmeGeom g, const double4* __restrict__ pos
 
 namespace {
 
-// fphi_uind_site (pmestuff.f:746-1045) field part, one warp per site: each
-// lane sums its stencil points, then a warp reduction; output dipfield [n][6]
-// (tmatxbrecip.f:2094-2121 fractional -> Cartesian).
+// fphi_uind_site (pmestuff.f:746-1045) field part, one thread per site,
+// output dipfield [n][6] (tmatxbrecip, newinduce_pme.f:2094-2121).
 template <typename T>
-__global__ void __launch_bounds__(256) k_gather_dip(int n, PmeGeom g, const double4* __restrict__ pos,
+__global__ void __launch_bounds__(128) k_gather_dip(int n, PmeGeom g, const double4* __restrict__ pos,
                                                     const typename Cplx<T>::type* __restrict__ grid,
                                                     double* __restrict__ out, const CgScalars* __restrict__ cg,
                                                     int check_stop) {
   if (check_stop && cg->stop) return;
-  const int lane = threadIdx.x & 31;
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double4 p = pos[i];
-  T x0[kBs], x1[kBs], x2[kBs], y0[kBs], y1[kBs], y2[kBs], z0[kBs], z1[kBs], z2[kBs];
-  const int gx = bspline_axis_split<2, T>(p.x, g.recip[0], g.n1, x0, x1, x2);
-  const int gy = bspline_axis_split<2, T>(p.y, g.recip[1], g.n2, y0, y1, y2);
-  const int gz = bspline_axis_split<2, T>(p.z, g.recip[2], g.n3, z0, z1, z2);
-  T s[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const int q = lane + 32 * r;
-    if (q < kBs * kBs * kBs) {
-      const int a = q % kBs, b = (q / kBs) % kBs, c = q / (kBs * kBs);
-      const T t0 = pick5(x0, a), t1 = pick5(x1, a);
-      const T u0 = pick5(y0, b), u1 = pick5(y1, b);
-      const T v0 = pick5(z0, c), v1 = pick5(z1, c);
-      const size_t idx = ((size_t)wrapk(gz + c, g.n3) * g.n2 + wrapk(gy + b, g.n2)) * g.n1 + wrapk(gx + a, g.n1);
-      const auto gq = grid[idx];
-      const T w100 = t1 * u0 * v0, w010 = t0 * u1 * v0, w001 = t0 * u0 * v1;
-      s[0] += gq.x * w100;
-      s[1] += gq.x * w010;
-      s[2] += gq.x * w001;
-      s[3] += gq.y * w100;
-      s[4] += gq.y * w010;
-      s[5] += gq.y * w001;
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < 6; ++q)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
-  if (lane < 6) {
-    T val = s[0];
-#pragma unroll
-    for (int q = 1; q < 6; ++q) val = lane == q ? s[q] : val;
-    const int d = lane % 3;
-    const double ad = d == 0 ? g.a[0] : (d == 1 ? g.a[1] : g.a[2]);
-    out[(size_t)i * 6 + lane] = ad * (double)val;
-  }
+  double o[6];
+  gather_dip<T>(g, pos[i], grid, o);
+  double2* d = reinterpret_cast<double2*>(out + (size_t)i * 6);
+  d[0] = make_double2(o[0], o[1]);
+  d[1] = make_double2(o[2], o[3]);
+  d[2] = make_double2(o[4], o[5]);
 }
 
 // kewald.f:693-717 (bspline) and :747-812 (dftmod)
@@ -471,12 +456,11 @@ int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode) {
   int st = zero_grid(c);
   if (st) return st;
   float* vf = c.mixed ? c.d_vecf : nullptr;
-  const int nw = (int)(((size_t)c.n * 32 + 255) / 256);  // one warp per site
   if (c.mixed)
-    k_spread_dip<float><<<nw, 256, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<double*>(d_vec), c.d_zr, vf,
+    k_spread_dip<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<double*>(d_vec), c.d_zr, vf,
                                                   c.d_cg, mode, (cufftComplex*)c.d_grid);
   else
-    k_spread_dip<double><<<nw, 256, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<double*>(d_vec), c.d_zr, vf,
+    k_spread_dip<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<double*>(d_vec), c.d_zr, vf,
                                                    c.d_cg, mode, (cufftDoubleComplex*)c.d_grid);
   if ((st = cuda_status(cudaGetLastError(), &c, "spread dip"))) return st;
   if ((st = convolve(c, mode == 1))) return st;
@@ -486,12 +470,12 @@ int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode) {
 
 int launch_gather_dip(Ctx& c, double* d_out, bool check_stop) {
   PmeGeom g = geom_of(c);
-  const int nw = (int)(((size_t)c.n * 32 + 255) / 256);
+  const int nb = (c.n + kBlock - 1) / kBlock;
   if (c.mixed)
-    k_gather_dip<float><<<nw, 256, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftComplex*)c.d_grid, d_out, c.d_cg,
+    k_gather_dip<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftComplex*)c.d_grid, d_out, c.d_cg,
                                                   check_stop ? 1 : 0);
   else
-    k_gather_dip<double><<<nw, 256, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftDoubleComplex*)c.d_grid, d_out,
+    k_gather_dip<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftDoubleComplex*)c.d_grid, d_out,
                                                    c.d_cg, check_stop ? 1 : 0);
   return cuda_status(cudaGetLastError(), &c, "gather dip");
 }

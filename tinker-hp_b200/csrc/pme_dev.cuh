@@ -155,31 +155,4 @@ __device__ __forceinline__ void gather_dip(const PmeGeom& g, double4 p, const ty
 }
 
 
-// Select th[m] for a runtime stencil index m in 0..4 without local memory.
-template <typename T>
-__device__ __forceinline__ T pick5(const T (&v)[kBs], int m) {
-  T r = v[0];
-  r = m == 1 ? v[1] : r;
-  r = m == 2 ? v[2] : r;
-  r = m == 3 ? v[3] : r;
-  r = m == 4 ? v[4] : r;
-  return r;
-}
-
-// One axis of bspline_fill_site for a warp-per-atom pass: the weights of all
-// five stencil points, split by derivative level into plain arrays.
-template <int LEVEL, typename T>
-__device__ __forceinline__ int bspline_axis_split(double coord, double recip, int nfft, T (&l0)[kBs], T (&l1)[kBs],
-                                                  T (&l2)[kBs]) {
-  T th[kBs][LEVEL];
-  int g = bspline_axis<LEVEL, T>(coord, recip, nfft, th);
-#pragma unroll
-  for (int m = 0; m < kBs; ++m) {
-    l0[m] = th[m][0];
-    l1[m] = th[m][1];
-    l2[m] = LEVEL > 2 ? th[m][LEVEL > 2 ? 2 : 0] : T(0);
-  }
-  return g;
-}
-
 }  // namespace thp
