@@ -225,3 +225,31 @@ def test_error_statuses(lib, thp, case):
     ctx = lib.Context(ws, poleps=1e-12, politer=3)
     r = ctx.solve(allow_unconverged=True)
     assert r["status"] == lib.THP_E_NOT_CONVERGED and r["niter"] == 3
+
+
+def test_pair_set_bit_exact_large_box(lib, thp):
+    # 32,400 atoms: 18^3 cells, FP32 screen active, periodic row wraps
+    ws = thp.water.make_water_box(10800, cfg=1)
+    orc = O.Oracle(ws)
+    assert orc.mlistcell()[0] == 0
+    ctx = lib.Context(ws)
+    np.testing.assert_array_equal(ctx.pairs(), orc.pairs())
+
+
+def test_pair_set_cutoff_ties(lib, thp):
+    # crafted pairs at r = 7.5 A exactly (kept, r^2 <= (7.0+0.5)^2) and one ulp
+    # beyond (dropped), along x and across the periodic boundary
+    ws = thp.water.make_water_box(216, cfg=0)
+    pos = ws.positions().copy()
+    L = ws.box[0]
+    o_a, o_b, o_c, o_d = 3 * 10, 3 * 50, 3 * 100, 3 * 150
+    pos[o_b] = pos[o_a] + np.array([7.5, 0.0, 0.0])
+    pos[o_c] = pos[o_a] + np.array([0.0, np.nextafter(7.5, 10.0), 0.0])
+    pos[o_d] = pos[o_a] + np.array([0.0, 0.0, L - 7.5])  # 7.5 through the boundary
+    ws2 = ws.with_positions(pos)
+    orc = O.Oracle(ws2)
+    assert orc.mlistcell()[0] == 0
+    ref = set(map(tuple, orc.pairs()))
+    assert (o_a, o_b) in ref and (o_a, o_c) not in ref
+    ctx = lib.Context(ws2)
+    np.testing.assert_array_equal(ctx.pairs(), orc.pairs())

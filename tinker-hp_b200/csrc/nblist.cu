@@ -7,6 +7,8 @@
 // are counting-sorted into cells of edge >= (ewaldcut+lbuffer)/2 and the list
 // is a FULL list (both directions), slot-major nb[s*npad + i] so that a warp
 // of consecutive atoms reads one coalesced row per slot.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace thp {
@@ -180,15 +182,22 @@ __device__ __forceinline__ int axis_cells(int c, int nc, int q) {
   return nc <= 5 ? q : ((c + q - 2) % nc + nc) % nc;
 }
 
-__global__ void __launch_bounds__(128) k_build_list(int n, int npad, Box box, double mbuf2, int ncx, int ncy,
-                                                    int ncz, const double4* __restrict__ pos,
-                                                    const int* __restrict__ scell, const int* __restrict__ cell_start,
+__global__ void __launch_bounds__(128) k_build_list(int n, int npad, Box box, double mbuf2, int prefilter,
+                                                    float lo, float hi, int ncx,
+                                                    int ncy, int ncz, const double4* __restrict__ pos,
+                                                    const float4* __restrict__ posf, const int* __restrict__ scell,
+                                                    const int* __restrict__ cell_start,
                                                     const int* __restrict__ cell_count, int maxnb,
                                                     int* __restrict__ nnb, int* __restrict__ nb,
                                                     int* __restrict__ flags) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 pi = pos[i];
+  const float4 fi = posf[i];
+  const float bx = (float)box.l[0], by = (float)box.l[1], bz = (float)box.l[2];
+  const float hx = 0.5f * bx, hy = 0.5f * by, hz = 0.5f * bz;
+  // FP32 screen: accept below lo, reject above hi, exact FP64 test between
+  // (lo/hi bracket mbuf2 by twice the FP32 error bound of r^2, set on the host)
   const int c = scell[i];
   const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
   int a0, a1, b0, b1;
@@ -206,14 +215,30 @@ __global__ void __launch_bounds__(128) k_build_list(int n, int npad, Box box, do
         if (x0 > x1) continue;
         const int k0 = cell_start[rowbase + x0];
         const int k1 = cell_start[rowbase + x1] + cell_count[rowbase + x1];
+#pragma unroll 4
         for (int k = k0; k < k1; ++k) {
           if (k == i) continue;
-          const double4 pk = pos[k];
-          // midpointimage (domdecstuff.f:1773): pos = xi - xk, imaged
-          double xr = __dadd_rn(pi.x, -pk.x), yr = __dadd_rn(pi.y, -pk.y), zr = __dadd_rn(pi.z, -pk.z);
-          image3(box, xr, yr, zr);
-          const double r2 = r2_exact(xr, yr, zr);
-          if (r2 <= mbuf2) {
+          bool take;
+          if (prefilter) {
+            const float4 fk = posf[k];
+            float xr = fi.x - fk.x, yr = fi.y - fk.y, zr = fi.z - fk.z;
+            xr = fabsf(xr) > hx ? xr - copysignf(bx, xr) : xr;
+            yr = fabsf(yr) > hy ? yr - copysignf(by, yr) : yr;
+            zr = fabsf(zr) > hz ? zr - copysignf(bz, zr) : zr;
+            const float r2f = xr * xr + yr * yr + zr * zr;
+            if (r2f > hi) continue;
+            take = r2f < lo;
+          } else {
+            take = false;
+          }
+          if (!take) {
+            const double4 pk = pos[k];
+            // midpointimage (domdecstuff.f:1773): pos = xi - xk, imaged
+            double xr = __dadd_rn(pi.x, -pk.x), yr = __dadd_rn(pi.y, -pk.y), zr = __dadd_rn(pi.z, -pk.z);
+            image3(box, xr, yr, zr);
+            take = r2_exact(xr, yr, zr) <= mbuf2;
+          }
+          if (take) {
             if (cnt < maxnb) nb[(size_t)cnt * npad + i] = k;
             ++cnt;
           }
@@ -341,7 +366,7 @@ int launch_gather_sorted(Ctx& c) {
   // d_par_orig holds pdamp, thole, polarity planes in original order
   k_gather_sorted<<<nb, kBlock, 0, c.stream>>>(n, c.box, c.d_perm, c.d_xyz_orig, c.d_par_orig,
                                                c.d_par_orig + n, c.d_par_orig + 2 * n, c.d_rpole_orig,
-                                               c.have_rpole ? 1 : 0, c.d_pos, c.mixed ? c.d_posf : nullptr,
+                                               c.have_rpole ? 1 : 0, c.d_pos, c.d_posf,
                                                c.d_thole, c.d_pol, c.d_rpole, c.d_mrec,
                                                c.mixed ? c.d_mrecf : nullptr);
   return cuda_status(cudaGetLastError(), &c, "gather sorted");
@@ -351,9 +376,18 @@ int launch_build_list(Ctx& c) {
   const int n = c.n;
   const double rl = c.cfg.ewaldcut + c.cfg.lbuffer;
   const double mbuf2 = rl * rl;
+  // the FP32 screen needs every list pair far from the half-box wrap point
+  const double hmin = std::min(c.box.half[0], std::min(c.box.half[1], c.box.half[2]));
+  const int prefilter = hmin > rl + 1.0 ? 1 : 0;
+  // |x| <= L/2 in FP32: each coordinate of a difference is off by at most
+  // 4 * 2^-24 * Lmax (two roundings, the wrap by L); r^2 then by 2 rl dr + dr^2
+  const double lmax = std::max(c.box.l[0], std::max(c.box.l[1], c.box.l[2]));
+  const double dr = 1.7320508075688772 * 4.0 * lmax * 5.9604644775390625e-08;
+  const double band = std::max(1e-5, 2.0 * (2.0 * rl * dr + dr * dr) / mbuf2);
+  const float lo = (float)(mbuf2 * (1.0 - band)), hi = (float)(mbuf2 * (1.0 + band));
   k_build_list<<<(n + 127) / 128, 128, 0, c.stream>>>(
-      n, c.npad, c.box, mbuf2, c.nc[0], c.nc[1], c.nc[2], c.d_pos, c.d_scell, c.d_cell_start, c.d_cell_count,
-      c.maxnb, c.d_nnb, c.d_nb, c.d_flags);
+      n, c.npad, c.box, mbuf2, prefilter, lo, hi, c.nc[0], c.nc[1], c.nc[2], c.d_pos, c.d_posf, c.d_scell, c.d_cell_start,
+      c.d_cell_count, c.maxnb, c.d_nnb, c.d_nb, c.d_flags);
   cudaMemcpyAsync(c.d_pos_built, c.d_pos, sizeof(double4) * n, cudaMemcpyDeviceToDevice, c.stream);
   return cuda_status(cudaGetLastError(), &c, "build list");
 }

@@ -18,17 +18,26 @@ namespace {
 
 constexpr int kBlock = 128;
 
+// Fire-and-forget reductions (PTX red): the spread never reads the old value,
+// so no thread waits on the atomic's return.
+__device__ __forceinline__ void red_add(double* a, double v) {
+  asm volatile("red.global.add.f64 [%0], %1;" ::"l"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ void red_add(float* a, float v) {
+  asm volatile("red.global.add.f32 [%0], %1;" ::"l"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ void red_add2(float* a, float x, float y) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(a), "f"(x), "f"(y) : "memory");
+}
 __device__ __forceinline__ void grid_add(cufftDoubleComplex* g, size_t idx, double re, double im) {
-  atomicAdd(&g[idx].x, re);
-  atomicAdd(&g[idx].y, im);
+  red_add(&g[idx].x, re);
+  red_add(&g[idx].y, im);
 }
 __device__ __forceinline__ void grid_add(cufftComplex* g, size_t idx, float re, float im) {
-  atomicAdd(reinterpret_cast<float2*>(&g[idx]), make_float2(re, im));
+  red_add2(&g[idx].x, re, im);
 }
-__device__ __forceinline__ void grid_add_re(cufftDoubleComplex* g, size_t idx, double re) {
-  atomicAdd(&g[idx].x, re);
-}
-__device__ __forceinline__ void grid_add_re(cufftComplex* g, size_t idx, float re) { atomicAdd(&g[idx].x, re); }
+__device__ __forceinline__ void grid_add_re(cufftDoubleComplex* g, size_t idx, double re) { red_add(&g[idx].x, re); }
+__device__ __forceinline__ void grid_add_re(cufftComplex* g, size_t idx, float re) { red_add(&g[idx].x, re); }
 
 // grid_mpole_site (pmestuff.f:163-278) for every site; rpole10 sorted
 template <typename T>

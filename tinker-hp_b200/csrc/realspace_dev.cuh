@@ -11,6 +11,14 @@
 
 #include "common.cuh"
 
+// pairs loaded ahead per thread in the matvec rows (FP64 / FP32 forms)
+#ifndef THP_MATVEC_G64
+#define THP_MATVEC_G64 2
+#endif
+#ifndef THP_MATVEC_G32
+#define THP_MATVEC_G32 4
+#endif
+
 namespace thp {
 
 struct PairRows {
@@ -21,7 +29,9 @@ struct PairRows {
   const void* pc5;  // coefficient dmp5
 };
 
-// FP64 row: positions double4, mu [n][6] double
+// FP64 row: positions double4, mu [n][6] double.  Pairs are taken in groups
+// of THP_MATVEC_G64 with every load of the group issued before the arithmetic, so each
+// thread keeps several gathers in flight.
 __device__ __forceinline__ void tmatxb_row64(const PairRows& pr, const Box& box, int i,
                                              const double4* __restrict__ pos, const double* __restrict__ mu,
                                              double (&acc)[6]) {
@@ -30,29 +40,48 @@ __device__ __forceinline__ void tmatxb_row64(const PairRows& pr, const Box& box,
   const int* __restrict__ pk = pr.pk;
   const double* __restrict__ c3p = (const double*)pr.pc3;
   const double* __restrict__ c5p = (const double*)pr.pc5;
-#pragma unroll 1
-  for (int s = 0; s < m; ++s) {
-    const size_t q = (size_t)s * pr.npad + i;
-    const int k = __ldg(pk + q);
-    const double c3 = __ldg(c3p + q), c5 = __ldg(c5p + q);
-    const double4 pk4 = pos[k];
-    double xr = pk4.x - pi.x, yr = pk4.y - pi.y, zr = pk4.z - pi.z;
-    image3(box, xr, yr, zr);
-    const double2* m2 = reinterpret_cast<const double2*>(mu + (size_t)k * 6);
-    const double2 u0 = m2[0], u1 = m2[1], u2 = m2[2];
-    const double dd = xr * u0.x + yr * u0.y + zr * u1.x;
-    const double dp = xr * u1.y + yr * u2.x + zr * u2.y;
-    const double sd = c5 * dd, sp = c5 * dp;
-    acc[0] += c3 * u0.x - sd * xr;
-    acc[1] += c3 * u0.y - sd * yr;
-    acc[2] += c3 * u1.x - sd * zr;
-    acc[3] += c3 * u1.y - sp * xr;
-    acc[4] += c3 * u2.x - sp * yr;
-    acc[5] += c3 * u2.y - sp * zr;
+  constexpr int G = THP_MATVEC_G64;
+  int s = 0;
+  for (; s < m; s += G) {
+    int k[G];
+    double c3[G], c5[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const bool ok = s + g < m;
+      const size_t q = (size_t)(ok ? s + g : s) * pr.npad + i;
+      k[g] = __ldg(pk + q);
+      c3[g] = ok ? __ldg(c3p + q) : 0.0;
+      c5[g] = ok ? __ldg(c5p + q) : 0.0;
+    }
+    double4 pk4[G];
+    double2 u0[G], u1[G], u2[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      pk4[g] = pos[k[g]];
+      const double2* m2 = reinterpret_cast<const double2*>(mu + (size_t)k[g] * 6);
+      u0[g] = m2[0];
+      u1[g] = m2[1];
+      u2[g] = m2[2];
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      double xr = pk4[g].x - pi.x, yr = pk4[g].y - pi.y, zr = pk4[g].z - pi.z;
+      image3(box, xr, yr, zr);
+      const double dd = xr * u0[g].x + yr * u0[g].y + zr * u1[g].x;
+      const double dp = xr * u1[g].y + yr * u2[g].x + zr * u2[g].y;
+      const double sd = c5[g] * dd, sp = c5[g] * dp;
+      acc[0] += c3[g] * u0[g].x - sd * xr;
+      acc[1] += c3[g] * u0[g].y - sd * yr;
+      acc[2] += c3[g] * u1[g].x - sd * zr;
+      acc[3] += c3[g] * u1[g].y - sp * xr;
+      acc[4] += c3[g] * u2[g].x - sp * yr;
+      acc[5] += c3[g] * u2[g].y - sp * zr;
+    }
   }
 }
 
-// FP32 row (mixed form): positions float4 wrapped into the box, mu [n][6] float
+// FP32 row (mixed form): positions float4 wrapped into the box, mu [n][6]
+// float; THP_MATVEC_G32 pairs in flight per thread.
 __device__ __forceinline__ void tmatxb_row32(const PairRows& pr, float bx, float by, float bz, int i,
                                              const float4* __restrict__ pos, const float* __restrict__ mu,
                                              float (&acc)[6]) {
@@ -62,27 +91,44 @@ __device__ __forceinline__ void tmatxb_row32(const PairRows& pr, float bx, float
   const float* __restrict__ c3p = (const float*)pr.pc3;
   const float* __restrict__ c5p = (const float*)pr.pc5;
   const float hx = 0.5f * bx, hy = 0.5f * by, hz = 0.5f * bz;
-#pragma unroll 2
-  for (int s = 0; s < m; ++s) {
-    const size_t q = (size_t)s * pr.npad + i;
-    const int k = __ldg(pk + q);
-    const float c3 = __ldg(c3p + q), c5 = __ldg(c5p + q);
-    const float4 pk4 = pos[k];
-    float xr = pk4.x - pi.x, yr = pk4.y - pi.y, zr = pk4.z - pi.z;
-    xr = fabsf(xr) > hx ? xr - copysignf(bx, xr) : xr;
-    yr = fabsf(yr) > hy ? yr - copysignf(by, yr) : yr;
-    zr = fabsf(zr) > hz ? zr - copysignf(bz, zr) : zr;
-    const float2* m2 = reinterpret_cast<const float2*>(mu + (size_t)k * 6);
-    const float2 u0 = m2[0], u1 = m2[1], u2 = m2[2];
-    const float dd = xr * u0.x + yr * u0.y + zr * u1.x;
-    const float dp = xr * u1.y + yr * u2.x + zr * u2.y;
-    const float sd = c5 * dd, sp = c5 * dp;
-    acc[0] += c3 * u0.x - sd * xr;
-    acc[1] += c3 * u0.y - sd * yr;
-    acc[2] += c3 * u1.x - sd * zr;
-    acc[3] += c3 * u1.y - sp * xr;
-    acc[4] += c3 * u2.x - sp * yr;
-    acc[5] += c3 * u2.y - sp * zr;
+  constexpr int G = THP_MATVEC_G32;
+  for (int s = 0; s < m; s += G) {
+    int k[G];
+    float c3[G], c5[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const bool ok = s + g < m;
+      const size_t q = (size_t)(ok ? s + g : s) * pr.npad + i;
+      k[g] = __ldg(pk + q);
+      c3[g] = ok ? __ldg(c3p + q) : 0.f;
+      c5[g] = ok ? __ldg(c5p + q) : 0.f;
+    }
+    float4 pk4[G];
+    float2 u0[G], u1[G], u2[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      pk4[g] = pos[k[g]];
+      const float2* m2 = reinterpret_cast<const float2*>(mu + (size_t)k[g] * 6);
+      u0[g] = m2[0];
+      u1[g] = m2[1];
+      u2[g] = m2[2];
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      float xr = pk4[g].x - pi.x, yr = pk4[g].y - pi.y, zr = pk4[g].z - pi.z;
+      xr = fabsf(xr) > hx ? xr - copysignf(bx, xr) : xr;
+      yr = fabsf(yr) > hy ? yr - copysignf(by, yr) : yr;
+      zr = fabsf(zr) > hz ? zr - copysignf(bz, zr) : zr;
+      const float dd = xr * u0[g].x + yr * u0[g].y + zr * u1[g].x;
+      const float dp = xr * u1[g].y + yr * u2[g].x + zr * u2[g].y;
+      const float sd = c5[g] * dd, sp = c5[g] * dp;
+      acc[0] += c3[g] * u0[g].x - sd * xr;
+      acc[1] += c3[g] * u0[g].y - sd * yr;
+      acc[2] += c3[g] * u1[g].x - sd * zr;
+      acc[3] += c3[g] * u1[g].y - sp * xr;
+      acc[4] += c3[g] * u2[g].x - sp * yr;
+      acc[5] += c3[g] * u2[g].y - sp * zr;
+    }
   }
 }
 
