@@ -200,6 +200,42 @@ def run_reference(args, ws_n, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def batched_throughput(lib, systems, copies, steps, warmup=2):
+    """Batched form: `copies` resident contexts per system solved together by
+    thp_solve_batch (each on its own stream); host-timed over whole batches."""
+    ctxs = [lib.Context(ws, precision=lib.MIXED, poleps=CG_TOL) for ws in systems for _ in range(copies)]
+    for _ in range(warmup):
+        lib.solve_batch(ctxs)
+    t0 = time.perf_counter()
+    iters = []
+    for _ in range(steps):
+        infos = lib.solve_batch(ctxs)
+        iters += [f["niter"] for f in infos]
+    dt = time.perf_counter() - t0
+    for c in ctxs:
+        c.close()
+    return {"solves": len(ctxs) * steps, "seconds": dt, "solves_per_s": len(ctxs) * steps / dt,
+            "ms_per_batch": 1000.0 * dt / steps, "median_iters": float(np.median(iters))}
+
+
+def serving_run(lib, thp, count, workers=8):
+    """Serving form: seeded Poisson stream (200 req/s, 1k-60k atoms, 30 %
+    repeats perturbed by 0.01 A RMS) through the continuous-batching server
+    with a 120 GB device budget."""
+    from tinker_hp_b200 import serve
+    reqs = serve.poisson_stream(count)
+    srv = serve.Server(precision=lib.MIXED, poleps=CG_TOL, budget_bytes=120 << 30, workers=workers)
+    srv.run(reqs[: min(8, len(reqs))], realtime=False)  # warm the kernels
+    srv.close()
+    srv = serve.Server(precision=lib.MIXED, poleps=CG_TOL, budget_bytes=120 << 30, workers=workers)
+    out = srv.run(reqs, realtime=True)
+    srv.close()
+    summ = serve.summarize(out)
+    summ.update({"requests": len(reqs), "rate_req_per_s": 200.0, "workers": workers,
+                 "atoms": "1,000-60,000 log-uniform", "repeats": "30 % (0.01 A RMS perturbation, warm start)"})
+    return summ
+
+
 def timed_solves(ctx, lib, steps, warmup, rebuild=True, guess=None):
     """Device-resident solves; per-step device time from CUDA events."""
     import torch
@@ -230,6 +266,7 @@ def main():
     ap.add_argument("--workload", default="water-288k", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -248,7 +285,8 @@ def main():
     lib.load()
     nw, cfg = WORKLOADS[args.workload]
     ws = thp.water.make_water_box(nw, cfg=cfg)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
 
     # mixed form (headline)
     mixed = lib.Context(ws, precision=lib.MIXED, poleps=CG_TOL, device=local)
@@ -357,6 +395,19 @@ def main():
             cpu = {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"failed: {ex}"}
 
+    extras = {}
+    if not args.no_extras:
+        b2 = batched_throughput(lib, [ws], 2, max(2, args.steps // 6))
+        b4 = batched_throughput(lib, [ws], 4, max(2, args.steps // 10))
+        extras["batched_288k"] = {"copies_2": b2, "copies_4": b4}
+        batch64 = thp.water.make_batch(64, seed=4003)
+        extras["batch_64_boxes"] = batched_throughput(lib, batch64, 1, 3)
+        extras["batch_64_boxes"]["atoms"] = f"{sum(w.n for w in batch64)} over 64 boxes (300-6000 each)"
+        extras["serving"] = serving_run(lib, thp, 120)
+        if fp64 is not None:
+            best = max(b2["solves_per_s"], b4["solves_per_s"])
+            extras["batched_288k"]["speedup_vs_fp64_plain"] = best / (world * len(lat64) / (t64 / 1000.0))
+
     steps = args.steps
     value = world * steps / (t_mixed / 1000.0)
     line = {
@@ -369,7 +420,7 @@ def main():
                    "parallelism": f"replicas x{world}", "l2": "inputs > L2 (pair stream ~0.5 GB per matvec)",
                    "iterations": int(np.median(niter))},
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-        "fp64": fp64_line, "accuracy": acc,
+        "fp64": fp64_line, "accuracy": acc, "extras": extras,
         "speedup_mixed_vs_fp64": (value / fp64_line["value"]) if fp64_line else None,
         "e2e": {"value": world * e2e_steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},

@@ -123,6 +123,14 @@ int thp_tmatxb(thp_ctx* ctx, int nrhs, int dodiag, const double* mu, double* efi
 int thp_efld0_direct(thp_ctx* ctx, int nrhs, double* ef);
 int thp_efld0_recip(thp_ctx* ctx, double* cphi /*[n][10]*/);
 int thp_tmatxbrecip(thp_ctx* ctx, int nrhs, const double* mu, double* dipfield);
+/* Solve several resident systems together (batched form): each context runs
+ * on its own stream; the fields of all systems are enqueued first, then CG
+ * chunks (replayed CUDA graphs) for every unconverged system per round, with
+ * one host check of all stop flags per round.  The list is rebuilt for every
+ * system (single-point solves).  infos[i] receives system i's result;
+ * returns the first non-OK status (THP_E_NOT_CONVERGED only if nothing
+ * worse happened). */
+int thp_solve_batch(thp_ctx** ctxs, int count, int guess, thp_solve_info* infos);
 /* one-call solve on host buffers (positions in, dipoles and energy out) */
 int thp_solve_host(thp_ctx* ctx, const double* x, const double* y, const double* z,
                    const double* rpole, double* uind, double* uinp, thp_solve_info* info);

@@ -1,0 +1,108 @@
+"""Batched and served forms: the server's admission / residency logic on the
+CPU with a fake solver, and on the GPU that every result is the same alone
+and in the mix (within the CG tolerance) and that batched solves equal
+single solves."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+DEBYE = 4.80321
+
+
+class FakeCtx:
+    live = 0
+    max_live_bytes = 0
+
+    def __init__(self, ws, log):
+        self.ws, self.log, self.busy = ws, log, threading.Lock()
+        self.solves = 0
+
+    def set_positions(self, x, y, z):
+        pass
+
+    def solve(self, guess, allow_unconverged=False):
+        assert self.busy.acquire(blocking=False), "one context used by two workers at once"
+        try:
+            self.log.append((id(self), guess))
+            time.sleep(0.002)
+            self.solves += 1
+            return {"niter": 3 if guess else 8, "epol": -1.0, "status": 0}
+        finally:
+            self.busy.release()
+
+    def dipoles(self):
+        return np.zeros((self.ws.n, 3)), None
+
+    def close(self):
+        pass
+
+
+def test_server_admission_and_residency(thp):
+    from tinker_hp_b200 import serve, lib
+    reqs = serve.poisson_stream(40, rate=2000.0, nmin=1000, nmax=3000, seed=7)
+    log = []
+    sizes = {}
+
+    def fp(ws):
+        return ws.n * 1000
+
+    budget = 4 * 3000 * 1000  # about four systems resident at once
+    srv = serve.Server(budget_bytes=budget, workers=6, context_factory=lambda ws: FakeCtx(ws, log),
+                       footprint_fn=fp)
+    out = srv.run(reqs, realtime=False)
+    assert len(out) == len(reqs) and all(r.status == 0 for r in out)
+    assert srv.used <= budget
+    # repeats found their system resident or rebuilt it after eviction
+    assert any(g == lib.GUESS_PREVIOUS for _, g in log)
+    s = serve.summarize(out)
+    assert s["completed"] == len(reqs) and s["p99_ms"] >= s["p50_ms"]
+    srv.close()
+
+
+def test_server_rejects_oversize(thp):
+    from tinker_hp_b200 import serve, lib
+    reqs = serve.poisson_stream(2, nmin=1000, nmax=1200, seed=3)
+    srv = serve.Server(budget_bytes=10, workers=1, context_factory=lambda ws: FakeCtx(ws, []),
+                       footprint_fn=lambda ws: 100)
+    with pytest.raises(lib.ThpError) as e:
+        srv.run(reqs, realtime=False)
+    assert e.value.status == lib.THP_E_OOM_ADMISSION
+
+
+@pytest.mark.gpu
+def test_batch_equals_single(thp):
+    from tinker_hp_b200 import lib
+    systems = thp.water.make_batch(6, seed=4003)
+    ctxs = [lib.Context(ws, precision=lib.MIXED, poleps=3e-6) for ws in systems]
+    infos = lib.solve_batch(ctxs)
+    for ws, ctx, info in zip(systems, ctxs, infos):
+        ub, _ = ctx.dipoles()
+        single = lib.Context(ws, precision=lib.MIXED, poleps=3e-6)
+        r = single.solve()
+        us, _ = single.dipoles()
+        assert info["converged"] and info["niter"] == r["niter"]
+        assert np.sqrt(np.mean(np.sum((ub - us) ** 2, 1))) * DEBYE < 1e-9
+        assert abs(info["epol"] - r["epol"]) < 1e-9 * abs(r["epol"])
+
+
+@pytest.mark.gpu
+def test_served_results_same_alone_and_in_mix(thp):
+    from tinker_hp_b200 import serve, lib
+    reqs = serve.poisson_stream(16, rate=500.0, nmin=1000, nmax=6000, seed=11)
+    srv = serve.Server(precision=lib.MIXED, poleps=3e-6, workers=4)
+    out = {r.rid: r for r in srv.run(reqs, realtime=True)}
+    srv.close()
+    for q in reqs:
+        alone = lib.Context(q.ws, precision=lib.FP64, poleps=1e-8)
+        alone.solve()
+        ua, _ = alone.dipoles()
+        r = out[q.rid]
+        assert r.status == lib.THP_OK
+        err = np.sqrt(np.mean(np.sum((r.uind - ua) ** 2, 1))) * DEBYE
+        assert err < 1e-5, (q.rid, q.repeat, err)
+    reps = [out[q.rid].niter for q in reqs if q.repeat]
+    fresh = [out[q.rid].niter for q in reqs if not q.repeat]
+    if reps:
+        assert np.mean(reps) < np.mean(fresh)

@@ -230,6 +230,7 @@ void free_ctx(Ctx& c) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   pme_free(c);
+  if (c.chunk_exec) cudaGraphExecDestroy(c.chunk_exec);
   if (c.h_cg) cudaFreeHost(c.h_cg);
   if (c.h_flags) cudaFreeHost(c.h_flags);
   if (c.ev0) cudaEventDestroy(c.ev0);
@@ -568,6 +569,120 @@ int thp_solve(thp_ctx* h, int guess, thp_solve_info* info) {
     info->ms_total = ms;
   }
   return st;
+}
+
+// E0 and the CG start of one system, fully asynchronous (forced list
+// rebuild, no host read-back); the overflow flags are checked after the solve.
+static int solve_front_async(thp_ctx* h, int guess) {
+  Ctx& c = h->c;
+  int st;
+  if (c.have_frames) {
+    if ((st = launch_rotpole(c))) return st;
+    c.have_rpole = true;
+  }
+  if ((st = launch_sort_atoms(c))) return st;
+  if ((st = launch_gather_sorted(c))) return st;
+  if ((st = launch_build_list(c))) return st;
+  c.have_list = true;
+  h->pos_dirty = false;
+  h->rpole_dirty = false;
+  if ((st = launch_efld0_coef(c, true))) return st;
+  if ((st = launch_efld0_recip(c))) return st;
+  h->field_valid = true;
+  return pcg_begin(c, guess);
+}
+
+int thp_solve_batch(thp_ctx** hs, int count, int guess, thp_solve_info* infos) {
+  if (!hs || count <= 0) return THP_E_INVALID;
+  std::vector<int> st(count, THP_OK), rounds(count, 0);
+  std::vector<char> active(count, 0);
+  for (int i = 0; i < count; ++i) {
+    thp_ctx* h = hs[i];
+    if (!h) {
+      st[i] = THP_E_INVALID;
+      continue;
+    }
+    Ctx& c = h->c;
+    if (set_current_device(c)) {
+      st[i] = THP_E_CUDA;
+      continue;
+    }
+    if (!c.have_params || !c.have_pos || (!c.have_rpole && !c.have_frames)) {
+      st[i] = THP_E_STATE;
+      continue;
+    }
+    int g = guess;
+    if (g == THP_GUESS_PREVIOUS && !c.have_dipoles) g = THP_GUESS_DIRECT;
+    if (g == THP_GUESS_HOST && !h->guess_uploaded) {
+      st[i] = THP_E_STATE;
+      continue;
+    }
+    cudaEventRecord(c.ev0, c.stream);
+    st[i] = solve_front_async(h, g);
+    h->guess_uploaded = false;
+    active[i] = st[i] == THP_OK;
+  }
+  for (bool any = true; any;) {
+    any = false;
+    for (int i = 0; i < count; ++i) {
+      if (!active[i]) continue;
+      Ctx& c = hs[i]->c;
+      set_current_device(c);
+      if ((st[i] = pcg_chunk_async(c))) active[i] = 0;
+    }
+    for (int i = 0; i < count; ++i) {
+      if (!active[i]) continue;
+      Ctx& c = hs[i]->c;
+      set_current_device(c);
+      if ((st[i] = cuda_status(cudaStreamSynchronize(c.stream), &c, "batch sync"))) {
+        active[i] = 0;
+        continue;
+      }
+      rounds[i] += kCgChunk;
+      if (c.h_cg->stop || rounds[i] > c.cfg.politer + kCgChunk) active[i] = 0;
+      any |= active[i] != 0;
+    }
+  }
+  for (int i = 0; i < count; ++i) {
+    if (st[i]) continue;
+    Ctx& c = hs[i]->c;
+    set_current_device(c);
+    st[i] = pcg_status(c);
+    if (st[i] && st[i] != THP_E_NOT_CONVERGED) continue;
+    int s2 = launch_epol(c);
+    if (s2) {
+      st[i] = s2;
+      continue;
+    }
+    cudaEventRecord(c.ev1, c.stream);
+    cudaMemcpyAsync(c.h_cg, c.d_cg, sizeof(CgScalars), cudaMemcpyDeviceToHost, c.stream);
+  }
+  int worst = THP_OK;
+  for (int i = 0; i < count; ++i) {
+    if (!st[i] || st[i] == THP_E_NOT_CONVERGED) {
+      thp_ctx* h = hs[i];
+      Ctx& c = h->c;
+      set_current_device(c);
+      int f = check_flags(h);  // synchronises the stream
+      if (f) st[i] = f;
+      h->solved_once = true;
+      if (infos) {
+        infos[i].niter = c.h_cg->niter;
+        infos[i].converged = c.h_cg->converged;
+        infos[i].resnrm = c.h_cg->resnrm;
+        infos[i].epol = c.h_cg->epol;
+        infos[i].ene[0] = c.h_cg->ene[0] * kElectric;
+        infos[i].ene[1] = c.h_cg->ene[1] * kElectric;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c.ev0, c.ev1);
+        infos[i].ms_total = ms;
+      }
+    } else if (infos) {
+      infos[i] = thp_solve_info{};
+    }
+    if (st[i] && (worst == THP_OK || worst == THP_E_NOT_CONVERGED)) worst = st[i];
+  }
+  return worst;
 }
 
 int thp_get_dipoles(thp_ctx* h, double* uind, double* uinp) {

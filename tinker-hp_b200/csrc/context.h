@@ -28,6 +28,9 @@ struct CgScalars {
   unsigned counter[4];  // last-block counters of the grid reductions
 };
 
+// CG iterations per host check of the stop flag
+constexpr int kCgChunk = 4;
+
 // device error flags (bit set)
 enum : int { DEV_LIST_OVERFLOW = 1, DEV_PAIR_OVERFLOW = 2, DEV_NAN = 4 };
 
@@ -135,6 +138,9 @@ struct Ctx {
   double *buind = nullptr, *buinp = nullptr, *bep = nullptr;
   int *bnelst = nullptr, *belst = nullptr;
   int bmaxelst = 0;
+
+  // CUDA graph of one CG chunk (captured on first use)
+  cudaGraphExec_t chunk_exec = nullptr;
 
   // optional event pairs around the fused CG matvec launches
   bool profiling = false;

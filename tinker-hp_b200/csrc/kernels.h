@@ -30,6 +30,9 @@ int launch_gather_dip(Ctx& c, double* d_out, bool check_stop);
 
 // solver.cu
 int run_pcg(Ctx& c, int guess);
+int pcg_begin(Ctx& c, int guess);
+int pcg_chunk_async(Ctx& c);
+int pcg_status(Ctx& c);
 int launch_epol(Ctx& c);
 
 // reorder helpers (solver.cu)

@@ -297,30 +297,72 @@ static int enqueue_iteration(Ctx& c) {
   return cuda_status(cudaGetLastError(), &c, "cg update");
 }
 
-// Runs the CG from the current d_ef; guess selects the start (see thp.h).
-int run_pcg(Ctx& c, int guess) {
+// Initial residual on the guess (newinduce_pme2.f:161-200, 398-417), async.
+int pcg_begin(Ctx& c, int guess) {
   int st;
   cudaMemsetAsync(c.d_cg, 0, sizeof(CgScalars), c.stream);
   if (guess == THP_GUESS_DIRECT) {
     k_guess_direct<<<(c.n * 6 + 255) / 256, 256, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_mu);
   }
-  // initial residual on the guess (newinduce_pme2.f:398-417)
   if ((st = launch_pme_dipole(c, c.d_mu, nullptr, 0))) return st;
-  if ((st = launch_matvec(c, c.d_mu, 1))) return st;
-  const int chunk = 4;
-  int done = 0;
-  while (true) {
-    for (int q = 0; q < chunk; ++q)
-      if ((st = enqueue_iteration(c))) return st;
-    done += chunk;
-    cudaMemcpyAsync(c.h_cg, c.d_cg, sizeof(CgScalars), cudaMemcpyDeviceToHost, c.stream);
-    if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "cg sync"))) return st;
-    if (c.h_cg->stop) break;
-    if (done > c.cfg.politer + chunk) break;  // defensive bound; stop is raised at politer
+  return launch_matvec(c, c.d_mu, 1);
+}
+
+static int enqueue_chunk(Ctx& c) {
+  int st;
+  for (int q = 0; q < kCgChunk; ++q)
+    if ((st = enqueue_iteration(c))) return st;
+  return cuda_status(cudaMemcpyAsync(c.h_cg, c.d_cg, sizeof(CgScalars), cudaMemcpyDeviceToHost, c.stream), &c,
+                     "cg scalars");
+}
+
+// kCgChunk iterations plus the copy of the CG scalars to pinned host memory,
+// replayed from a CUDA graph captured on first use (all buffers and the cuFFT
+// plan are fixed for the life of the context).  Returns without waiting.
+int pcg_chunk_async(Ctx& c) {
+  // no capture while profiling, nor on the legacy default stream
+  if (c.profiling || c.stream == nullptr) return enqueue_chunk(c);
+  if (!c.chunk_exec) {
+    cudaGraph_t g = nullptr;
+    int st = cuda_status(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal), &c, "capture");
+    if (st) return st;
+    int st_enq = enqueue_chunk(c);
+    st = cuda_status(cudaStreamEndCapture(c.stream, &g), &c, "end capture");
+    if (st_enq || st) {
+      if (g) cudaGraphDestroy(g);
+      return st_enq ? st_enq : st;
+    }
+    st = cuda_status(cudaGraphInstantiate(&c.chunk_exec, g, 0), &c, "instantiate");
+    cudaGraphDestroy(g);
+    if (st) {
+      c.chunk_exec = nullptr;
+      return st;
+    }
   }
+  return cuda_status(cudaGraphLaunch(c.chunk_exec, c.stream), &c, "graph launch");
+}
+
+int pcg_status(Ctx& c) {
   c.have_dipoles = true;
   if (c.h_cg->status) return c.h_cg->status;
   return c.h_cg->converged ? THP_OK : THP_E_NOT_CONVERGED;
+}
+
+// Runs the CG from the current d_ef; guess selects the start (see thp.h).
+// The host reads the stop flag once per chunk of kCgChunk iterations; kernels
+// after the stop return at entry.
+int run_pcg(Ctx& c, int guess) {
+  int st = pcg_begin(c, guess);
+  if (st) return st;
+  int done = 0;
+  while (true) {
+    if ((st = pcg_chunk_async(c))) return st;
+    done += kCgChunk;
+    if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "cg sync"))) return st;
+    if (c.h_cg->stop) break;
+    if (done > c.cfg.politer + kCgChunk) break;  // defensive bound; stop is raised at politer
+  }
+  return pcg_status(c);
 }
 
 int launch_epol(Ctx& c) {

@@ -89,6 +89,7 @@ def load():
         "thp_efld0_direct": ([vp, C.c_int, _dp], C.c_int),
         "thp_efld0_recip": ([vp, _dp], C.c_int),
         "thp_tmatxbrecip": ([vp, C.c_int, _dp, _dp], C.c_int),
+        "thp_solve_batch": ([C.POINTER(vp), C.c_int, C.c_int, C.POINTER(ThpSolveInfo)], C.c_int),
         "thp_solve_host": ([vp, _dp, _dp, _dp, _dp, _dp, _dp, C.POINTER(ThpSolveInfo)], C.c_int),
         "thp_footprint": ([C.POINTER(ThpConfig)], C.c_size_t),
         "thp_status_string": ([C.c_int], C.c_char_p),
@@ -152,6 +153,19 @@ def config_for(ws, precision=FP64, poleps=1e-6, politer=500, device=0, max_neigh
 
 def footprint(ws, precision=FP64):
     return int(load().thp_footprint(C.byref(config_for(ws, precision))))
+
+
+def solve_batch(contexts, guess=GUESS_DIRECT, allow_unconverged=False):
+    """Solve several resident systems together (thp_solve_batch)."""
+    L = load()
+    n = len(contexts)
+    hs = (C.c_void_p * n)(*[c.h for c in contexts])
+    infos = (ThpSolveInfo * n)()
+    st = L.thp_solve_batch(hs, n, guess, infos)
+    if st != THP_OK and not (allow_unconverged and st == THP_E_NOT_CONVERGED):
+        raise ThpError(st, "thp_solve_batch")
+    return [{"niter": f.niter, "converged": bool(f.converged), "resnrm": f.resnrm, "epol": f.epol,
+             "ene": tuple(f.ene), "ms": f.ms_total} for f in infos]
 
 
 def scales_array(ws):

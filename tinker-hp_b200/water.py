@@ -168,12 +168,21 @@ def _assemble(nw, edge, xyz, grid_spacing, ewaldcut, lbuffer, aewald):
     conn = water_connectivity_fast(nw)
     k = pme_k = P.pme_grid_size(edge, grid_spacing)
     if aewald is None:
-        aewald = P.ewaldcof(ewaldcut)
+        aewald = _ewaldcof_cached(ewaldcut)
     return WaterSystem(n=n, nw=nw, box=(edge, edge, edge), x=np.ascontiguousarray(xyz[:, 0]),
                        y=np.ascontiguousarray(xyz[:, 1]), z=np.ascontiguousarray(xyz[:, 2]),
                        pole=pole, zaxis=zaxis, xaxis=xaxis, axt=axt, polarity=polarity, thole=thole,
                        pdamp=pdamp, mol=mol, conn=conn, aewald=aewald, ewaldcut=ewaldcut,
                        lbuffer=lbuffer, nfft=(k, pme_k, k))
+
+
+_EWALD_CACHE = {}
+
+
+def _ewaldcof_cached(cut):
+    if cut not in _EWALD_CACHE:
+        _EWALD_CACHE[cut] = P.ewaldcof(cut)
+    return _EWALD_CACHE[cut]
 
 
 def water_connectivity(nw):
@@ -217,3 +226,28 @@ def water_connectivity_fast(nw):
     empty = (np.zeros(n + 1, np.int32), np.zeros(0, np.int32))
     return {"i12": (off12, idx12), "i13": (off13, idx13), "i14": empty, "i15": empty,
             "ip11": (off11, idx11), "ip12": empty, "ip13": empty, "ip14": empty}
+
+
+def min_box_edge(ewaldcut=P.EWALD_CUTOFF, lbuffer=P.LIST_BUFFER, margin=0.2):
+    """Smallest cubic edge with the list cutoff inside half a box
+    (the reference's minimum-image check, nblist.f:147-156)."""
+    return 2.0 * (ewaldcut + lbuffer) + margin
+
+
+def batch_sizes(count=64, nmin=300, nmax=6000, seed=4003):
+    """Atom counts drawn log-uniform in [nmin, nmax], rounded to whole waters."""
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(np.log(nmin), np.log(nmax), size=count))
+    return [max(1, int(round(v / 3.0))) for v in n]
+
+
+def make_batch(count=64, nmin=300, nmax=6000, seed=4003):
+    """Independent boxes of uneven size, each built like the single box at its
+    own edge; edges below min_box_edge() are widened to it (lower density)
+    because the 7.0 + 0.5 A list must fit in half a box."""
+    out = []
+    for q, nw in enumerate(batch_sizes(count, nmin, nmax, seed)):
+        edge = max(box_edge(nw), min_box_edge())
+        out.append(make_water_box(nw, edge=edge, seed_lattice=seed * 100 + 2 * q,
+                                  seed_orient=seed * 100 + 2 * q + 1))
+    return out
