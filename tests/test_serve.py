@@ -83,8 +83,9 @@ def test_batch_equals_single(thp):
         r = single.solve()
         us, _ = single.dipoles()
         assert info["converged"] and info["niter"] == r["niter"]
-        assert np.sqrt(np.mean(np.sum((ub - us) ** 2, 1))) * DEBYE < 1e-9
-        assert abs(info["epol"] - r["epol"]) < 1e-9 * abs(r["epol"])
+        # same kernels; only the order of the FP32 grid atomics differs
+        assert np.sqrt(np.mean(np.sum((ub - us) ** 2, 1))) * DEBYE < 1e-7
+        assert abs(info["epol"] - r["epol"]) < 1e-7 * abs(r["epol"])
 
 
 @pytest.mark.gpu

@@ -4,7 +4,8 @@ Construction: rigid waters (O-H 0.9572 A, H-O-H 104.52 deg); oxygens on a
 jittered cubic lattice (n_side = ceil(Nw^(1/3)), a seeded subset of sites,
 jitter rejection-sampled so that the minimum O-O distance is >= 2.5 A) at
 0.997 g/cm^3 (0.033328 waters/A^3) in a cubic box of edge (Nw/rho)^(1/3)
-centred on the origin; uniform random orientations (one seeded unit
+centred on the origin (widened, at lower density, when Nw lies just above a
+perfect cube and the lattice spacing would fall below 2.75 A); uniform random orientations (one seeded unit
 quaternion per molecule).  Atom order is O, H1, H2 per molecule, as in
 Tinker water .xyz files.
 
@@ -24,6 +25,7 @@ RHO_WATER = 0.033328  # waters per A^3 at 0.997 g/cm^3 (M = 18.015 g/mol)
 R_OH = 0.9572
 THETA_HOH = 104.52
 MIN_OO = 2.5
+MIN_SPACING = 2.75  # smallest oxygen lattice spacing the jitter sampling accepts
 
 
 @dataclasses.dataclass
@@ -117,9 +119,10 @@ def make_water_box(nw, cfg=0, edge=None, grid_spacing=1.2, ewaldcut=P.EWALD_CUTO
                    seed_orient=None):
     """Build a seeded water box of `nw` molecules (seeds 1000+cfg, 2000+cfg)."""
     edge = box_edge(nw) if edge is None else float(edge)
+    nside = int(math.ceil(nw ** (1.0 / 3.0) - 1e-9))
+    edge = max(edge, MIN_SPACING * nside)
     rng_l = np.random.default_rng(1000 + cfg if seed_lattice is None else seed_lattice)
     rng_o = np.random.default_rng(2000 + cfg if seed_orient is None else seed_orient)
-    nside = int(math.ceil(nw ** (1.0 / 3.0) - 1e-9))
     a = edge / nside
     sites = np.sort(rng_l.choice(nside ** 3, size=nw, replace=False))
     ijk = np.stack([sites // (nside * nside), (sites // nside) % nside, sites % nside], axis=1)
