@@ -52,7 +52,7 @@ WORKLOADS = {
 DEBYE = 4.80321
 # CG stop threshold (Tinker's poleps units) for both forms: chosen so that the
 # dipoles are within 1e-5 D RMS of the fully converged FP64 answer on the box
-CG_TOL = 3e-6
+CG_TOL = 2e-6
 
 
 class ClockSampler:
