@@ -67,6 +67,7 @@ def lib():
         L.or_newinduce_pme2.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.POINTER(OrSolveInfo)]
         L.or_epolar.restype = C.c_double
         L.or_epolar.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+        L.or_epolar1.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, _dp, _dp]
         L.or_rotpole.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _dp]
         L.or_ewaldcof.restype = C.c_double
         L.or_ewaldcof.argtypes = [C.c_double]
@@ -203,6 +204,20 @@ class Oracle:
             raise RuntimeError(f"oracle solve failed with status {st}")
         return {"uind": uind, "uinp": uinp, "ef": ef, "niter": info.niter,
                 "converged": bool(info.converged), "resnrm": info.resnrm, "ene": tuple(info.ene)}
+
+    def epolar1(self, uind, uinp):
+        """Energy and gradient dE/dx [n,3] (kcal/mol/A), epolar1c."""
+        uind = np.ascontiguousarray(uind, dtype=np.float64)
+        uinp = np.ascontiguousarray(uinp, dtype=np.float64)
+        dep = np.zeros((self.ws.n, 3))
+        ep = C.c_double()
+        ws = self.ws
+        st = lib().or_epolar1(self.ctx, _p(uind), _p(uinp), _p(np.ascontiguousarray(ws.zaxis, np.int32), _ip),
+                              _p(np.ascontiguousarray(ws.xaxis, np.int32), _ip),
+                              _p(np.ascontiguousarray(ws.axt, np.int32), _ip), _p(dep), C.byref(ep))
+        if st != 0:
+            raise RuntimeError(f"oracle epolar1 status {st}")
+        return ep.value, dep
 
     def epolar(self, uind):
         uind = np.ascontiguousarray(uind, dtype=np.float64)

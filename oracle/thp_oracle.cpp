@@ -1428,3 +1428,519 @@ void or_rotpole(int n, const double* x, const double* y, const double* z, const 
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Polarization forces: epolar1c (epolar1.f:57-372) = eprecip1 (:397-1213)
+// + epreal1c (:1215-2540, Thole branch, dpequal false) + self energy and
+// self torque (:181-206), torques distributed by torque (torque.f:6-390).
+// Virial terms are not restated.
+namespace {
+
+// torque.f:6-390 for Z-then-X and Bisector frames (the water frames);
+// frame atoms 0-based; adds the forces of a torque on site i into de[n][3]
+void torque_site(const double* x, const double* y, const double* z, int ib, int ia, int ic, int axt,
+                 const double trq[3], double* de) {
+  double u[3] = {x[ia] - x[ib], y[ia] - y[ib], z[ia] - z[ib]};
+  double usiz = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+  double v[3] = {x[ic] - x[ib], y[ic] - y[ib], z[ic] - z[ib]};
+  double vsiz = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  double w[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+  double wsiz = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  for (int j = 0; j < 3; ++j) {
+    u[j] /= usiz;
+    v[j] /= vsiz;
+    w[j] /= wsiz;
+  }
+  double uv[3] = {v[1] * u[2] - v[2] * u[1], v[2] * u[0] - v[0] * u[2], v[0] * u[1] - v[1] * u[0]};
+  double uw[3] = {w[1] * u[2] - w[2] * u[1], w[2] * u[0] - w[0] * u[2], w[0] * u[1] - w[1] * u[0]};
+  double vw[3] = {w[1] * v[2] - w[2] * v[1], w[2] * v[0] - w[0] * v[2], w[0] * v[1] - w[1] * v[0]};
+  double uvsiz = std::sqrt(uv[0] * uv[0] + uv[1] * uv[1] + uv[2] * uv[2]);
+  double uwsiz = std::sqrt(uw[0] * uw[0] + uw[1] * uw[1] + uw[2] * uw[2]);
+  double vwsiz = std::sqrt(vw[0] * vw[0] + vw[1] * vw[1] + vw[2] * vw[2]);
+  for (int j = 0; j < 3; ++j) {
+    uv[j] /= uvsiz;
+    uw[j] /= uwsiz;
+    vw[j] /= vwsiz;
+  }
+  double uvcos = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+  double uvsin = std::sqrt(1.0 - uvcos * uvcos);
+  double dphidu = -trq[0] * u[0] - trq[1] * u[1] - trq[2] * u[2];
+  double dphidv = -trq[0] * v[0] - trq[1] * v[1] - trq[2] * v[2];
+  double dphidw = -trq[0] * w[0] - trq[1] * w[1] - trq[2] * w[2];
+  for (int j = 0; j < 3; ++j) {
+    double du, dv;
+    if (axt == 1) {  // Z-then-X
+      du = uv[j] * dphidv / (usiz * uvsin) + uw[j] * dphidw / usiz;
+      dv = -uv[j] * dphidu / (vsiz * uvsin);
+    } else {  // Bisector
+      du = uv[j] * dphidv / (usiz * uvsin) + 0.5 * uw[j] * dphidw / usiz;
+      dv = -uv[j] * dphidu / (vsiz * uvsin) + 0.5 * vw[j] * dphidw / vsiz;
+    }
+    de[ia * 3 + j] += du;
+    de[ic * 3 + j] += dv;
+    de[ib * 3 + j] -= du + dv;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxis, const int* xaxis,
+               const int* axt, double* dep, double* ep_out) {
+  const OrSystem& s = c->s;
+  const int n = s.n, bs = c->bsorder, maxelst = c->maxelst;
+  if (!c->have_list) return OR_E_LIST_OVERFLOW;
+  std::fill(dep, dep + (size_t)n * 3, 0.0);
+  double ep = 0.0;
+  // permanent-multipole potential fphirec (20 per site) from efld0_recip
+  {
+    std::vector<double> cphi((size_t)n * 10);
+    or_efld0_recip(c, cphi.data());
+  }
+  std::vector<double> fphirec = c->fphirec;
+  // ---- eprecip1 ---------------------------------------------------------
+  {
+    static const int deriv1[10] = {2, 5, 8, 9, 11, 16, 18, 14, 15, 20};
+    static const int deriv2[10] = {3, 8, 6, 10, 14, 12, 19, 16, 20, 17};
+    static const int deriv3[10] = {4, 9, 10, 7, 15, 17, 13, 20, 18, 19};
+    const double f = kElectric;
+    double a[3][3];
+    int nf[3] = {s.nfft1, s.nfft2, s.nfft3};
+    for (int i = 0; i < 3; ++i)
+      for (int d = 0; d < 3; ++d) a[d][i] = (double)nf[d] * c->recip[i][d];
+    double ctf[10][10], ftc[10][10];
+    cart_to_frac(c, ctf);
+    frac_to_cart(c, ftc);
+    std::vector<double> cmp((size_t)n * 10), fmp((size_t)n * 10), fu((size_t)n * 6);
+    for (int i = 0; i < n; ++i) {
+      const double* rp = &s.rpole[(size_t)i * 13];
+      double* cm = &cmp[(size_t)i * 10];
+      cm[0] = rp[0]; cm[1] = rp[1]; cm[2] = rp[2]; cm[3] = rp[3]; cm[4] = rp[4]; cm[5] = rp[8];
+      cm[6] = rp[12]; cm[7] = 2.0 * rp[5]; cm[8] = 2.0 * rp[6]; cm[9] = 2.0 * rp[9];
+      double* fm = &fmp[(size_t)i * 10];
+      fm[0] = ctf[0][0] * cm[0];
+      for (int j = 1; j < 4; ++j) {
+        fm[j] = 0.0;
+        for (int k = 1; k < 4; ++k) fm[j] += ctf[j][k] * cm[k];
+      }
+      for (int j = 4; j < 10; ++j) {
+        fm[j] = 0.0;
+        for (int k = 4; k < 10; ++k) fm[j] += ctf[j][k] * cm[k];
+      }
+      for (int j = 0; j < 3; ++j) {
+        fu[i * 6 + j] = a[j][0] * uind[i * 3] + a[j][1] * uind[i * 3 + 1] + a[j][2] * uind[i * 3 + 2];
+        fu[i * 6 + 3 + j] = a[j][0] * uinp[i * 3] + a[j][1] * uinp[i * 3 + 1] + a[j][2] * uinp[i * 3 + 2];
+      }
+    }
+    if (!c->have_bspline) bspline_fill(c);
+    spread_sites(c, [&](int i, const double* t, const double* u, const double* v) {
+      const double* fd = &fu[i * 6];
+      const double* fp = &fu[i * 6 + 3];
+      double term01 = fd[1] * u[1] * v[0] + fd[2] * u[0] * v[1];
+      double term11 = fd[0] * u[0] * v[0];
+      double term02 = fp[1] * u[1] * v[0] + fp[2] * u[0] * v[1];
+      double term12 = fp[0] * u[0] * v[0];
+      return cd(term01 * t[0] + term11 * t[1], term02 * t[0] + term12 * t[1]);
+    });
+    convolve(c);
+    double erec = 0.0;
+    std::vector<double> fphid(10), fphip(10), fsum(20), fper(20);
+    for (int i = 0; i < n; ++i) {
+      // fphi_uind_site (pmestuff.f:746-1045), all components
+      const double* th1 = &c->theta1[(size_t)i * bs * 4];
+      const double* th2 = &c->theta2[(size_t)i * bs * 4];
+      const double* th3 = &c->theta3[(size_t)i * bs * 4];
+      const int* ig = &c->igrid[i * 3];
+      double T1[10] = {0}, T2[10] = {0}, S[20] = {0};
+      // T1/T2 index: 1..9 = 100,010,001,200,020,002,110,101,011 (fdip_phi(2:10))
+      for (int it3 = 1; it3 <= bs; ++it3) {
+        int k = gather_index(ig[2], it3, s.nfft3);
+        double v0 = th3[(it3 - 1) * 4], v1 = th3[(it3 - 1) * 4 + 1], v2 = th3[(it3 - 1) * 4 + 2],
+               v3 = th3[(it3 - 1) * 4 + 3];
+        double tu1[6] = {0}, tu2[6] = {0}, tu[10] = {0};  // 00,10,01,20,11,02 ; sum: +30,21,12,03
+        for (int it2 = 1; it2 <= bs; ++it2) {
+          int j = gather_index(ig[1], it2, s.nfft2);
+          double u0 = th2[(it2 - 1) * 4], u1 = th2[(it2 - 1) * 4 + 1], u2 = th2[(it2 - 1) * 4 + 2],
+                 u3 = th2[(it2 - 1) * 4 + 3];
+          double t1a[3] = {0}, t1b[3] = {0}, t3 = 0.0;
+          for (int it1 = 1; it1 <= bs; ++it1) {
+            int ii = gather_index(ig[0], it1, s.nfft1);
+            cd g = c->grid[((size_t)k * s.nfft2 + j) * s.nfft1 + ii];
+            const double* w = &th1[(it1 - 1) * 4];
+            t1a[0] += g.real() * w[0];
+            t1a[1] += g.real() * w[1];
+            t1a[2] += g.real() * w[2];
+            t1b[0] += g.imag() * w[0];
+            t1b[1] += g.imag() * w[1];
+            t1b[2] += g.imag() * w[2];
+            t3 += (g.real() + g.imag()) * w[3];
+          }
+          tu1[0] += t1a[0] * u0; tu1[1] += t1a[1] * u0; tu1[2] += t1a[0] * u1;
+          tu1[3] += t1a[2] * u0; tu1[4] += t1a[1] * u1; tu1[5] += t1a[0] * u2;
+          tu2[0] += t1b[0] * u0; tu2[1] += t1b[1] * u0; tu2[2] += t1b[0] * u1;
+          tu2[3] += t1b[2] * u0; tu2[4] += t1b[1] * u1; tu2[5] += t1b[0] * u2;
+          double t0 = t1a[0] + t1b[0], t1 = t1a[1] + t1b[1], t2 = t1a[2] + t1b[2];
+          tu[0] += t0 * u0; tu[1] += t1 * u0; tu[2] += t0 * u1; tu[3] += t2 * u0; tu[4] += t1 * u1;
+          tu[5] += t0 * u2; tu[6] += t3 * u0; tu[7] += t2 * u1; tu[8] += t1 * u2; tu[9] += t0 * u3;
+        }
+        // (_1): 100,010,001,200,020,002,110,101,011
+        T1[1] += tu1[1] * v0; T1[2] += tu1[2] * v0; T1[3] += tu1[0] * v1; T1[4] += tu1[3] * v0;
+        T1[5] += tu1[5] * v0; T1[6] += tu1[0] * v2; T1[7] += tu1[4] * v0; T1[8] += tu1[1] * v1;
+        T1[9] += tu1[2] * v1;
+        T2[1] += tu2[1] * v0; T2[2] += tu2[2] * v0; T2[3] += tu2[0] * v1; T2[4] += tu2[3] * v0;
+        T2[5] += tu2[5] * v0; T2[6] += tu2[0] * v2; T2[7] += tu2[4] * v0; T2[8] += tu2[1] * v1;
+        T2[9] += tu2[2] * v1;
+        // sum: 000,100,010,001,200,020,002,110,101,011,300,030,003,210,201,120,021,102,012,111
+        S[0] += tu[0] * v0; S[1] += tu[1] * v0; S[2] += tu[2] * v0; S[3] += tu[0] * v1;
+        S[4] += tu[3] * v0; S[5] += tu[5] * v0; S[6] += tu[0] * v2; S[7] += tu[4] * v0;
+        S[8] += tu[1] * v1; S[9] += tu[2] * v1; S[10] += tu[6] * v0; S[11] += tu[9] * v0;
+        S[12] += tu[0] * v3; S[13] += tu[7] * v0; S[14] += tu[3] * v1; S[15] += tu[8] * v0;
+        S[16] += tu[5] * v1; S[17] += tu[1] * v2; S[18] += tu[2] * v2; S[19] += tu[4] * v1;
+      }
+      // 1-based arrays as in the reference: fphid(2:10), fphidprec(1:20), fphirec(1:20)
+      double FD[11], FP[11], FS[21], FR[21];
+      for (int q = 1; q <= 9; ++q) {
+        FD[q + 1] = f * T1[q];
+        FP[q + 1] = f * T2[q];
+      }
+      for (int q = 0; q < 20; ++q) {
+        FS[q + 1] = f * S[q];
+        FR[q + 1] = f * fphirec[(size_t)i * 20 + q];
+      }
+      const double* fd = &fu[i * 6];
+      const double* fp = &fu[i * 6 + 3];
+      double f1 = 0.0, f2 = 0.0, f3 = 0.0;
+      for (int k = 1; k <= 3; ++k) {
+        int j1 = deriv1[k], j2 = deriv2[k], j3 = deriv3[k];
+        erec += fd[k - 1] * FR[k + 1];
+        f1 += (fd[k - 1] + fp[k - 1]) * FR[j1] + fd[k - 1] * FP[j1] + fp[k - 1] * FD[j1];
+        f2 += (fd[k - 1] + fp[k - 1]) * FR[j2] + fd[k - 1] * FP[j2] + fp[k - 1] * FD[j2];
+        f3 += (fd[k - 1] + fp[k - 1]) * FR[j3] + fd[k - 1] * FP[j3] + fp[k - 1] * FD[j3];
+      }
+      const double* fm = &fmp[(size_t)i * 10];
+      for (int k = 1; k <= 10; ++k) {
+        f1 += fm[k - 1] * FS[deriv1[k - 1]];
+        f2 += fm[k - 1] * FS[deriv2[k - 1]];
+        f3 += fm[k - 1] * FS[deriv3[k - 1]];
+      }
+      f1 = 0.5 * (double)s.nfft1 * f1;
+      f2 = 0.5 * (double)s.nfft2 * f2;
+      f3 = 0.5 * (double)s.nfft3 * f3;
+      dep[i * 3 + 0] += c->recip[0][0] * f1 + c->recip[0][1] * f2 + c->recip[0][2] * f3;
+      dep[i * 3 + 1] += c->recip[1][0] * f1 + c->recip[1][1] * f2 + c->recip[1][2] * f3;
+      dep[i * 3 + 2] += c->recip[2][0] * f1 + c->recip[2][1] * f2 + c->recip[2][2] * f3;
+      // torque from the dipole-grid potential on the permanent moments
+      double fh[10];
+      for (int q = 0; q < 10; ++q) fh[q] = 0.5 * FS[q + 1];
+      double cp[10];
+      cp[0] = ftc[0][0] * fh[0];
+      for (int j = 1; j < 4; ++j) {
+        cp[j] = 0.0;
+        for (int k = 1; k < 4; ++k) cp[j] += ftc[j][k] * fh[k];
+      }
+      for (int j = 4; j < 10; ++j) {
+        cp[j] = 0.0;
+        for (int k = 4; k < 10; ++k) cp[j] += ftc[j][k] * fh[k];
+      }
+      const double* cm = &cmp[(size_t)i * 10];
+      double trq[3];
+      // 1-based: cmp(1..10) = cm[0..9], cphidprec(1..10) = cp[0..9]
+      trq[0] = cm[3] * cp[2] - cm[2] * cp[3] + 2.0 * (cm[6] - cm[5]) * cp[9] + cm[8] * cp[7] + cm[9] * cp[5] -
+               cm[7] * cp[8] - cm[9] * cp[6];
+      trq[1] = cm[1] * cp[3] - cm[3] * cp[1] + 2.0 * (cm[4] - cm[6]) * cp[8] + cm[7] * cp[9] + cm[8] * cp[6] -
+               cm[8] * cp[4] - cm[9] * cp[7];
+      trq[2] = cm[2] * cp[1] - cm[1] * cp[2] + 2.0 * (cm[5] - cm[4]) * cp[7] + cm[7] * cp[4] + cm[9] * cp[8] -
+               cm[7] * cp[5] - cm[8] * cp[9];
+      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], trq, dep);
+    }
+    ep += 0.5 * erec;
+  }
+  // ---- epreal1c (Thole branch) -------------------------------------------
+  {
+    const double f = 0.5 * kElectric;
+    const double off2 = s.ewaldcut * s.ewaldcut;
+    std::vector<double> ufld((size_t)n * 3, 0.0), dufld((size_t)n * 6, 0.0);
+    ScaleWs w;
+    w.init(n);
+    for (int i = 0; i < n; ++i) {
+      const double* ri = &s.rpole[(size_t)i * 13];
+      double ci = ri[0], dix = ri[1], diy = ri[2], diz = ri[3];
+      double qixx = ri[4], qixy = ri[5], qixz = ri[6], qiyy = ri[8], qiyz = ri[9], qizz = ri[12];
+      double uix = uind[i * 3], uiy = uind[i * 3 + 1], uiz = uind[i * 3 + 2];
+      double uixp = uinp[i * 3], uiyp = uinp[i * 3 + 1], uizp = uinp[i * 3 + 2];
+      double pdi = s.pdamp[i], pti = s.thole[i];
+      set_dp_scales(s, i, w);
+      set_u_scales(s, i, w, false);
+      for (int kkk = 0; kkk < c->nelst[i]; ++kkk) {
+        int k = c->elst[(size_t)i * maxelst + kkk];
+        double xr = s.x[k] - s.x[i], yr = s.y[k] - s.y[i], zr = s.z[k] - s.z[i];
+        image(c->cell, xr, yr, zr);
+        double r2 = xr * xr + yr * yr + zr * zr;
+        if (r2 > off2) continue;
+        double r = std::sqrt(r2);
+        const double* rk = &s.rpole[(size_t)k * 13];
+        double ck = rk[0], dkx = rk[1], dky = rk[2], dkz = rk[3];
+        double qkxx = rk[4], qkxy = rk[5], qkxz = rk[6], qkyy = rk[8], qkyz = rk[9], qkzz = rk[12];
+        double ukx = uind[k * 3], uky = uind[k * 3 + 1], ukz = uind[k * 3 + 2];
+        double ukxp = uinp[k * 3], ukyp = uinp[k * 3 + 1], ukzp = uinp[k * 3 + 2];
+        double dir = dix * xr + diy * yr + diz * zr;
+        double qix = qixx * xr + qixy * yr + qixz * zr;
+        double qiy = qixy * xr + qiyy * yr + qiyz * zr;
+        double qiz = qixz * xr + qiyz * yr + qizz * zr;
+        double qir = qix * xr + qiy * yr + qiz * zr;
+        double dkr = dkx * xr + dky * yr + dkz * zr;
+        double qkx = qkxx * xr + qkxy * yr + qkxz * zr;
+        double qky = qkxy * xr + qkyy * yr + qkyz * zr;
+        double qkz = qkxz * xr + qkyz * yr + qkzz * zr;
+        double qkr = qkx * xr + qky * yr + qkz * zr;
+        double uir = uix * xr + uiy * yr + uiz * zr;
+        double uirp = uixp * xr + uiyp * yr + uizp * zr;
+        double ukr = ukx * xr + uky * yr + ukz * zr;
+        double ukrp = ukxp * xr + ukyp * yr + ukzp * zr;
+        double rr1 = f / r;
+        double rr3 = rr1 / r2;
+        double rr5 = 3.0 * rr3 / r2;
+        double rr7 = 5.0 * rr5 / r2;
+        double rr9 = 7.0 * rr7 / r2;
+        double dmpe[10];
+        dampewald(9, r, r2, f, s.aewald, dmpe);
+        double sc3 = 1.0, sc5 = 1.0, sc7 = 1.0;
+        double rc3[3] = {0, 0, 0}, rc5[3] = {0, 0, 0}, rc7[3] = {0, 0, 0};
+        double damp = pdi * s.pdamp[k];
+        double pgamma = std::min(pti, s.thole[k]);
+        if (pgamma == 0.0) pgamma = std::max(pti, s.thole[k]);
+        if (damp != 0.0 && pgamma != 0.0) {
+          double t = r / damp;
+          damp = pgamma * (t * t * t);
+          if (damp < 50.0) {
+            double expdamp = std::exp(-damp);
+            sc3 = 1.0 - expdamp;
+            sc5 = 1.0 - (1.0 + damp) * expdamp;
+            sc7 = 1.0 - (1.0 + damp + 0.6 * damp * damp) * expdamp;
+            double temp3 = 3.0 * damp * expdamp / r2;
+            double temp5 = damp;
+            double temp7 = -0.2 + 0.6 * damp;
+            rc3[0] = xr * temp3; rc3[1] = yr * temp3; rc3[2] = zr * temp3;
+            for (int j = 0; j < 3; ++j) {
+              rc5[j] = rc3[j] * temp5;
+              rc7[j] = rc5[j] * temp7;
+            }
+          }
+        }
+        double ps = w.p[k], ds = w.d[k], us = w.u[k];
+        double psc3 = 1.0 - sc3 * ps, psc5 = 1.0 - sc5 * ps, psc7 = 1.0 - sc7 * ps;
+        double dsc3 = 1.0 - sc3 * ds, dsc5 = 1.0 - sc5 * ds, dsc7 = 1.0 - sc7 * ds;
+        double usc3 = 1.0 - sc3 * us, usc5 = 1.0 - sc5 * us;
+        double psr3 = dmpe[3] - psc3 * rr3, psr5 = dmpe[5] - psc5 * rr5, psr7 = dmpe[7] - psc7 * rr7;
+        double dsr3 = dmpe[3] - dsc3 * rr3, dsr5 = dmpe[5] - dsc5 * rr5, dsr7 = dmpe[7] - dsc7 * rr7;
+        double usr5 = dmpe[5] - usc5 * rr5;
+        double prc3[3], prc5[3], prc7[3], drc3[3], drc5[3], drc7[3], urc3[3], urc5[3];
+        for (int j = 0; j < 3; ++j) {
+          prc3[j] = rc3[j] * ps; prc5[j] = rc5[j] * ps; prc7[j] = rc7[j] * ps;
+          drc3[j] = rc3[j] * ds; drc5[j] = rc5[j] * ds; drc7[j] = rc7[j] * ds;
+          urc3[j] = rc3[j] * us; urc5[j] = rc5[j] * us;
+        }
+        (void)usc3;
+        // induced field at i and k for the torques
+        double tix3 = psr3 * ukx + dsr3 * ukxp, tiy3 = psr3 * uky + dsr3 * ukyp, tiz3 = psr3 * ukz + dsr3 * ukzp;
+        double tkx3 = psr3 * uix + dsr3 * uixp, tky3 = psr3 * uiy + dsr3 * uiyp, tkz3 = psr3 * uiz + dsr3 * uizp;
+        double tuir = -psr5 * ukr - dsr5 * ukrp;
+        double tukr = -psr5 * uir - dsr5 * uirp;
+        ufld[i * 3 + 0] += tix3 + xr * tuir;
+        ufld[i * 3 + 1] += tiy3 + yr * tuir;
+        ufld[i * 3 + 2] += tiz3 + zr * tuir;
+        ufld[k * 3 + 0] += tkx3 + xr * tukr;
+        ufld[k * 3 + 1] += tky3 + yr * tukr;
+        ufld[k * 3 + 2] += tkz3 + zr * tukr;
+        // energy with the p-scaled permanent field (damptholed order 7)
+        {
+          double dmpik[8];
+          dampthole(pdi, s.pdamp[k], pti, s.thole[k], 7, r, dmpik);
+          double scalek = ps;
+          double dmp3 = dmpe[3] - (1.0 - scalek * dmpik[3]) * rr3;
+          double dmp5 = dmpe[5] - (1.0 - scalek * dmpik[5]) * rr5;
+          double dmp7 = dmpe[7] - (1.0 - scalek * dmpik[7]) * rr7;
+          double fip[3], fkp[3];
+          fip[0] = -xr * (dmp3 * ck - dmp5 * dkr + dmp7 * qkr) - dmp3 * dkx + 2.0 * dmp5 * qkx;
+          fip[1] = -yr * (dmp3 * ck - dmp5 * dkr + dmp7 * qkr) - dmp3 * dky + 2.0 * dmp5 * qky;
+          fip[2] = -zr * (dmp3 * ck - dmp5 * dkr + dmp7 * qkr) - dmp3 * dkz + 2.0 * dmp5 * qkz;
+          fkp[0] = xr * (dmp3 * ci + dmp5 * dir + dmp7 * qir) - dmp3 * dix - 2.0 * dmp5 * qix;
+          fkp[1] = yr * (dmp3 * ci + dmp5 * dir + dmp7 * qir) - dmp3 * diy - 2.0 * dmp5 * qiy;
+          fkp[2] = zr * (dmp3 * ci + dmp5 * dir + dmp7 * qir) - dmp3 * diz - 2.0 * dmp5 * qiz;
+          double e = 0.0;
+          for (int j = 0; j < 3; ++j) e = e - uind[i * 3 + j] * fip[j] - uind[k * 3 + j] * fkp[j];
+          ep += e;
+        }
+        double tix5 = 2.0 * (psr5 * ukx + dsr5 * ukxp), tiy5 = 2.0 * (psr5 * uky + dsr5 * ukyp),
+               tiz5 = 2.0 * (psr5 * ukz + dsr5 * ukzp);
+        double tkx5 = 2.0 * (psr5 * uix + dsr5 * uixp), tky5 = 2.0 * (psr5 * uiy + dsr5 * uiyp),
+               tkz5 = 2.0 * (psr5 * uiz + dsr5 * uizp);
+        tuir = -psr7 * ukr - dsr7 * ukrp;
+        tukr = -psr7 * uir - dsr7 * uirp;
+        double* dfi = &dufld[i * 6];
+        double* dfk = &dufld[k * 6];
+        dfi[0] += xr * tix5 + xr * xr * tuir;
+        dfi[1] += xr * tiy5 + yr * tix5 + 2.0 * xr * yr * tuir;
+        dfi[2] += yr * tiy5 + yr * yr * tuir;
+        dfi[3] += xr * tiz5 + zr * tix5 + 2.0 * xr * zr * tuir;
+        dfi[4] += yr * tiz5 + zr * tiy5 + 2.0 * yr * zr * tuir;
+        dfi[5] += zr * tiz5 + zr * zr * tuir;
+        dfk[0] -= xr * tkx5 + xr * xr * tukr;
+        dfk[1] -= xr * tky5 + yr * tkx5 + 2.0 * xr * yr * tukr;
+        dfk[2] -= yr * tky5 + yr * yr * tukr;
+        dfk[3] -= xr * tkz5 + zr * tkx5 + 2.0 * xr * zr * tukr;
+        dfk[4] -= yr * tkz5 + zr * tky5 + 2.0 * yr * zr * tukr;
+        dfk[5] -= zr * tkz5 + zr * zr * tukr;
+        // gradient of the permanent field times the dipoles: d part (uinp) and p part (uind)
+        auto perm_part = [&](double sc3_, double sc5_, double sc7_, double sr3, double sr5, double sr7,
+                             const double* xc3, const double* xc5, const double* xc7, double vkx, double vky,
+                             double vkz, double vix, double viy, double viz, double out[3]) {
+          double term1 = dmpe[5] - sc3_ * rr5;
+          double term2 = dmpe[7] - sc5_ * rr7;
+          double term3 = -sr3 + term1 * xr * xr - rr3 * xr * xc3[0];
+          double term4 = rr3 * xc3[0] - term1 * xr - sr5 * xr;
+          double term5 = term2 * xr * xr - sr5 - rr5 * xr * xc5[0];
+          double term6 = (dmpe[9] - sc7_ * rr9) * xr * xr - dmpe[7] - rr7 * xr * xc7[0];
+          double term7 = rr5 * xc5[0] - 2.0 * dmpe[7] * xr + (sc5_ + 1.5 * sc7_) * rr7 * xr;
+          double tixx = ci * term3 + dix * term4 + dir * term5 + 2.0 * sr5 * qixx + (qiy * yr + qiz * zr) * sc7_ * rr7 +
+                        2.0 * qix * term7 + qir * term6;
+          double tkxx = ck * term3 - dkx * term4 - dkr * term5 + 2.0 * sr5 * qkxx + (qky * yr + qkz * zr) * sc7_ * rr7 +
+                        2.0 * qkx * term7 + qkr * term6;
+          term3 = -sr3 + term1 * yr * yr - rr3 * yr * xc3[1];
+          term4 = rr3 * xc3[1] - term1 * yr - sr5 * yr;
+          term5 = term2 * yr * yr - sr5 - rr5 * yr * xc5[1];
+          term6 = (dmpe[9] - sc7_ * rr9) * yr * yr - dmpe[7] - rr7 * yr * xc7[1];
+          term7 = rr5 * xc5[1] - 2.0 * dmpe[7] * yr + (sc5_ + 1.5 * sc7_) * rr7 * yr;
+          double tiyy = ci * term3 + diy * term4 + dir * term5 + 2.0 * sr5 * qiyy + (qix * xr + qiz * zr) * sc7_ * rr7 +
+                        2.0 * qiy * term7 + qir * term6;
+          double tkyy = ck * term3 - dky * term4 - dkr * term5 + 2.0 * sr5 * qkyy + (qkx * xr + qkz * zr) * sc7_ * rr7 +
+                        2.0 * qky * term7 + qkr * term6;
+          term3 = -sr3 + term1 * zr * zr - rr3 * zr * xc3[2];
+          term4 = rr3 * xc3[2] - term1 * zr - sr5 * zr;
+          term5 = term2 * zr * zr - sr5 - rr5 * zr * xc5[2];
+          term6 = (dmpe[9] - sc7_ * rr9) * zr * zr - dmpe[7] - rr7 * zr * xc7[2];
+          term7 = rr5 * xc5[2] - 2.0 * dmpe[7] * zr + (sc5_ + 1.5 * sc7_) * rr7 * zr;
+          double tizz = ci * term3 + diz * term4 + dir * term5 + 2.0 * sr5 * qizz + (qix * xr + qiy * yr) * sc7_ * rr7 +
+                        2.0 * qiz * term7 + qir * term6;
+          double tkzz = ck * term3 - dkz * term4 - dkr * term5 + 2.0 * sr5 * qkzz + (qkx * xr + qky * yr) * sc7_ * rr7 +
+                        2.0 * qkz * term7 + qkr * term6;
+          term3 = term1 * xr * yr - rr3 * yr * xc3[0];
+          term4 = rr3 * xc3[0] - term1 * xr;
+          term5 = term2 * xr * yr - rr5 * yr * xc5[0];
+          term6 = (dmpe[9] - sc7_ * rr9) * xr * yr - rr7 * yr * xc7[0];
+          term7 = rr5 * xc5[0] - term2 * xr;
+          double tixy = ci * term3 - sr5 * dix * yr + diy * term4 + dir * term5 + 2.0 * sr5 * qixy -
+                        2.0 * sr7 * yr * qix + 2.0 * qiy * term7 + qir * term6;
+          double tkxy = ck * term3 + sr5 * dkx * yr - dky * term4 - dkr * term5 + 2.0 * sr5 * qkxy -
+                        2.0 * sr7 * yr * qkx + 2.0 * qky * term7 + qkr * term6;
+          term3 = term1 * xr * zr - rr3 * zr * xc3[0];
+          term5 = term2 * xr * zr - rr5 * zr * xc5[0];
+          term6 = (dmpe[9] - sc7_ * rr9) * xr * zr - rr7 * zr * xc7[0];
+          double tixz = ci * term3 - sr5 * dix * zr + diz * term4 + dir * term5 + 2.0 * sr5 * qixz -
+                        2.0 * sr7 * zr * qix + 2.0 * qiz * term7 + qir * term6;
+          double tkxz = ck * term3 + sr5 * dkx * zr - dkz * term4 - dkr * term5 + 2.0 * sr5 * qkxz -
+                        2.0 * sr7 * zr * qkx + 2.0 * qkz * term7 + qkr * term6;
+          term3 = term1 * yr * zr - rr3 * zr * xc3[1];
+          term4 = rr3 * xc3[1] - term1 * yr;
+          term5 = term2 * yr * zr - rr5 * zr * xc5[1];
+          term6 = (dmpe[9] - sc7_ * rr9) * yr * zr - rr7 * zr * xc7[1];
+          term7 = rr5 * xc5[1] - term2 * yr;
+          double tiyz = ci * term3 - sr5 * diy * zr + diz * term4 + dir * term5 + 2.0 * sr5 * qiyz -
+                        2.0 * sr7 * zr * qiy + 2.0 * qiz * term7 + qir * term6;
+          double tkyz = ck * term3 + sr5 * dky * zr - dkz * term4 - dkr * term5 + 2.0 * sr5 * qkyz -
+                        2.0 * sr7 * zr * qky + 2.0 * qkz * term7 + qkr * term6;
+          out[0] = tixx * vkx + tixy * vky + tixz * vkz - tkxx * vix - tkxy * viy - tkxz * viz;
+          out[1] = tixy * vkx + tiyy * vky + tiyz * vkz - tkxy * vix - tkyy * viy - tkyz * viz;
+          out[2] = tixz * vkx + tiyz * vky + tizz * vkz - tkxz * vix - tkyz * viy - tkzz * viz;
+        };
+        double frc[3], dp[3];
+        perm_part(dsc3, dsc5, dsc7, dsr3, dsr5, dsr7, drc3, drc5, drc7, ukxp, ukyp, ukzp, uixp, uiyp, uizp, frc);
+        perm_part(psc3, psc5, psc7, psr3, psr5, psr7, prc3, prc5, prc7, ukx, uky, ukz, uix, uiy, uiz, dp);
+        for (int j = 0; j < 3; ++j) frc[j] += dp[j];
+        // mutual part: uind . grad T . uinp with uscale
+        {
+          double term1 = dmpe[5] - usc3 * rr5;
+          double term2 = dmpe[7] - usc5 * rr7;
+          double term3 = usr5 + term1;
+          double term4 = rr3 * us;
+          double term5 = -xr * term3 + rc3[0] * term4;
+          double term6 = -usr5 + xr * xr * term2 - rr5 * xr * urc5[0];
+          double tixx = uix * term5 + uir * term6;
+          double tkxx = ukx * term5 + ukr * term6;
+          term5 = -yr * term3 + rc3[1] * term4;
+          term6 = -usr5 + yr * yr * term2 - rr5 * yr * urc5[1];
+          double tiyy = uiy * term5 + uir * term6;
+          double tkyy = uky * term5 + ukr * term6;
+          term5 = -zr * term3 + rc3[2] * term4;
+          term6 = -usr5 + zr * zr * term2 - rr5 * zr * urc5[2];
+          double tizz = uiz * term5 + uir * term6;
+          double tkzz = ukz * term5 + ukr * term6;
+          term4 = -usr5 * yr;
+          term5 = -xr * term1 + rr3 * urc3[0];
+          term6 = xr * yr * term2 - rr5 * yr * urc5[0];
+          double tixy = uix * term4 + uiy * term5 + uir * term6;
+          double tkxy = ukx * term4 + uky * term5 + ukr * term6;
+          term4 = -usr5 * zr;
+          term6 = xr * zr * term2 - rr5 * zr * urc5[0];
+          double tixz = uix * term4 + uiz * term5 + uir * term6;
+          double tkxz = ukx * term4 + ukz * term5 + ukr * term6;
+          term5 = -yr * term1 + rr3 * urc3[1];
+          term6 = yr * zr * term2 - rr5 * zr * urc5[1];
+          double tiyz = uiy * term4 + uiz * term5 + uir * term6;
+          double tkyz = uky * term4 + ukz * term5 + ukr * term6;
+          frc[0] += tixx * ukxp + tixy * ukyp + tixz * ukzp + tkxx * uixp + tkxy * uiyp + tkxz * uizp;
+          frc[1] += tixy * ukxp + tiyy * ukyp + tiyz * ukzp + tkxy * uixp + tkyy * uiyp + tkyz * uizp;
+          frc[2] += tixz * ukxp + tiyz * ukyp + tizz * ukzp + tkxz * uixp + tkyz * uiyp + tkzz * uizp;
+        }
+        for (int j = 0; j < 3; ++j) {
+          dep[i * 3 + j] -= frc[j];
+          dep[k * 3 + j] += frc[j];
+        }
+      }
+      reset_dp_scales(s, i, w);
+      set_u_scales(s, i, w, true);
+    }
+    // torque of the induced field and gradient on the permanent moments
+    for (int i = 0; i < n; ++i) {
+      const double* ri = &s.rpole[(size_t)i * 13];
+      double dix = ri[1], diy = ri[2], diz = ri[3];
+      double qixx = ri[4], qixy = ri[5], qixz = ri[6], qiyy = ri[8], qiyz = ri[9], qizz = ri[12];
+      const double* uf = &ufld[i * 3];
+      const double* du = &dufld[i * 6];
+      double tep[3];
+      tep[0] = diz * uf[1] - diy * uf[2] + qixz * du[1] - qixy * du[3] + 2.0 * qiyz * (du[2] - du[5]) +
+               (qizz - qiyy) * du[4];
+      tep[1] = dix * uf[2] - diz * uf[0] - qiyz * du[1] + qixy * du[4] + 2.0 * qixz * (du[5] - du[0]) +
+               (qixx - qizz) * du[3];
+      tep[2] = diy * uf[0] - dix * uf[1] + qiyz * du[3] - qixz * du[4] + 2.0 * qixy * (du[0] - du[2]) +
+               (qiyy - qixx) * du[1];
+      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], tep, dep);
+    }
+  }
+  // ---- self energy and self torque (epolar1.f:181-206) --------------------
+  {
+    const double f = kElectric;
+    double term = 2.0 * s.aewald * s.aewald;
+    double fterm = -f * s.aewald / kSqrtPi;
+    for (int i = 0; i < n; ++i) {
+      const double* rp = &s.rpole[(size_t)i * 13];
+      double uii = rp[1] * uind[i * 3] + rp[2] * uind[i * 3 + 1] + rp[3] * uind[i * 3 + 2];
+      ep += fterm * term * uii / 3.0;
+    }
+    term = (4.0 / 3.0) * f * s.aewald * s.aewald * s.aewald / kSqrtPi;
+    for (int i = 0; i < n; ++i) {
+      const double* rp = &s.rpole[(size_t)i * 13];
+      double dix = rp[1], diy = rp[2], diz = rp[3];
+      double uix = 0.5 * (uind[i * 3] + uinp[i * 3]);
+      double uiy = 0.5 * (uind[i * 3 + 1] + uinp[i * 3 + 1]);
+      double uiz = 0.5 * (uind[i * 3 + 2] + uinp[i * 3 + 2]);
+      double trq[3] = {term * (diy * uiz - diz * uiy), term * (diz * uix - dix * uiz), term * (dix * uiy - diy * uix)};
+      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], trq, dep);
+    }
+  }
+  if (ep_out) *ep_out = ep;
+  return OR_OK;
+}
+
+}  // extern "C"

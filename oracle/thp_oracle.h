@@ -90,6 +90,12 @@ int or_newinduce_pme2(OrCtx* c, const double* mu_guess, double* uind, double* ui
  * of the last or_efld0_recip call. Returns also the three parts. */
 double or_epolar(OrCtx* c, const double* uind, double* ereal, double* erecip, double* eself);
 
+/* epolar1c (epolar1.f:57-372): polarization energy and its gradient dep
+ * [n][3] (kcal/mol/A) from converged uind/uinp; frames (zaxis, xaxis, axt
+ * as in or_rotpole) distribute the torques (torque.f:6). */
+int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxis, const int* xaxis,
+               const int* axt, double* dep, double* ep);
+
 /* rotpole for the water frames used here (Bisector and Z-then-X),
  * pole [n][13] local frame -> rpole [n][13] global frame.
  * axt: 1 = Z-then-X, 2 = Bisector. zaxis/xaxis 0-based. */

@@ -202,3 +202,32 @@ def test_threads_agree(box216):
         orc.mlistcell()
         r.append(orc.solve()["uind"])
     np.testing.assert_allclose(r[0], r[1], rtol=0, atol=1e-12)
+
+
+def _energy(ws, poleps=1e-10):
+    orc = O.Oracle(ws, poleps=poleps)
+    assert orc.mlistcell()[0] == 0
+    res = orc.solve()
+    return orc.epolar(res["uind"])[0], orc, res
+
+
+def test_epolar1_energy_matches_epolar0(box216):
+    e0, orc, res = _energy(box216)
+    e1, dep = orc.epolar1(res["uind"], res["uinp"])
+    assert abs(e1 - e0) < 1e-10 * abs(e0)
+
+
+def test_epolar1_gradient_matches_finite_differences(box216):
+    _, orc, res = _energy(box216)
+    _, dep = orc.epolar1(res["uind"], res["uinp"])
+    pos0 = box216.positions()
+    h = 1e-4
+    for atom in (0, 1, 2, 301, 646):
+        for d in range(3):
+            e = []
+            for sgn in (1, -1):
+                p = pos0.copy()
+                p[atom, d] += sgn * h
+                e.append(_energy(box216.with_positions(p))[0])
+            fd = (e[0] - e[1]) / (2 * h)
+            assert abs(fd - dep[atom, d]) < 1e-5 * np.abs(dep).max() + 1e-6, (atom, d, fd, dep[atom, d])
