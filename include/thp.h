@@ -131,6 +131,32 @@ int thp_tmatxbrecip(thp_ctx* ctx, int nrhs, const double* mu, double* dipfield);
  * returns the first non-OK status (THP_E_NOT_CONVERGED only if nothing
  * worse happened). */
 int thp_solve_batch(thp_ctx** ctxs, int count, int guess, thp_solve_info* infos);
+/* Gradient of the polarization energy, epolar1c (epolar1.f:57-372): eprecip1
+ * (:397), epreal1c (:1215, Thole branch), the self torque (:190-206) and the
+ * torque-to-force conversion of torque.f:6, for the dipoles of the last solve
+ * at the current positions.  dep [n][3] (kcal/mol/A, x fastest as dep(3,n))
+ * on the host, original atom order; ep (may be NULL) receives that solve's
+ * energy.  The torques need the frame atoms given to thp_set_frames (kept
+ * when thp_set_rpole later replaces the multipoles).  THP_E_STATE without
+ * frames or without a solve since the last position / multipole change.
+ * Gradients accumulate in 64-bit fixed point (2^-34 kcal/mol/A) in both
+ * precisions, so the order of the per-atom additions does not matter. */
+int thp_get_gradient(thp_ctx* ctx, double* dep, double* ep);
+/* same gradient into device memory d_dep [n][3], enqueued on the context's
+ * stream without a host synchronisation */
+int thp_get_gradient_device(thp_ctx* ctx, double* d_dep);
+/* Velocity-Verlet NVE dynamics driven by the polarization gradient alone
+ * (verlet.f:17-200 with gradient = epolar1): per step a half kick, a drift of
+ * the positions on the device, a solve warm-started from the previous step's
+ * dipoles (list rebuilt when an atom moved more than lbuffer/2), the gradient,
+ * and the second half kick.  Starts with a solve and gradient at the current
+ * positions.  mass [n] g/mol; vel [n][3] A/ps, updated in place; dt in ps.
+ * energies [nsteps][3] (may be NULL): epol, kinetic, total (kcal/mol) after
+ * each step; niters [nsteps] (may be NULL): CG iterations of each solve.
+ * thp_get_positions reads the advanced positions back. */
+int thp_md_verlet(thp_ctx* ctx, int nsteps, double dt, const double* mass, double* vel,
+                  double* energies, int* niters);
+int thp_get_positions(thp_ctx* ctx, double* x, double* y, double* z);
 /* one-call solve on host buffers (positions in, dipoles and energy out) */
 int thp_solve_host(thp_ctx* ctx, const double* x, const double* y, const double* z,
                    const double* rpole, double* uind, double* uinp, thp_solve_info* info);
@@ -164,6 +190,8 @@ int thp_epolar_noalloc(int n, const double* d_uind, const double* d_ef, double* 
 int thp_bind_state(thp_ctx* ctx, double* x, double* y, double* z, double* rpole, double* uind,
                    double* uinp, int* nelst, int* elst, int maxelst, double* ep);
 int thp_last_error(void);
+/* bind deriv::dep(3,n), written by epolar1_ */
+int thp_bind_gradient(thp_ctx* ctx, double* dep);
 
 /* newinduce_pme2.f:16 -- fields, guess, PCG, writeback of uind/uinp */
 void newinduce_pme2_(void);
@@ -189,6 +217,9 @@ void mlistcell_(void);
 void vlistcell_(void);
 /* epolar.f:17 -- polarization energy into the bound ep (solves first) */
 void epolar_(void);
+/* epolar1.f:17 -- solve, then energy into the bound ep and the gradient into
+ * the bound dep (overwritten, as epolar1c zeroes it first) */
+void epolar1_(void);
 
 #ifdef __cplusplus
 }

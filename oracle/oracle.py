@@ -224,3 +224,35 @@ class Oracle:
         er, ek, es = C.c_double(), C.c_double(), C.c_double()
         e = lib().or_epolar(self.ctx, _p(uind), C.byref(er), C.byref(ek), C.byref(es))
         return e, {"real": er.value, "recip": ek.value, "self": es.value}
+
+
+def verlet(ws, vel, mass, dt, nsteps, poleps=1e-8):
+    """Velocity-Verlet NVE with the polarization gradient as the only force
+    (verlet.f:17-200; a = -convert * dE/dx / m, units.f:76), each step solved
+    from the direct guess.  Returns (positions [n,3], velocities [n,3],
+    energies [nsteps,3] = epol/kinetic/total)."""
+    convert = 418.4
+    m = np.asarray(mass, dtype=np.float64)[:, None]
+    v = np.array(vel, dtype=np.float64)
+    pos = ws.positions().copy()
+
+    def grad(p):
+        w = ws.with_positions(p)
+        o = Oracle(w, poleps=poleps)
+        if o.mlistcell()[0] != 0:
+            raise RuntimeError("oracle list overflow")
+        r = o.solve()
+        ep, dep = o.epolar1(r["uind"], r["uinp"])
+        o.close()
+        return ep, dep
+
+    _, g = grad(pos)
+    out = np.zeros((nsteps, 3))
+    for s in range(nsteps):
+        v += -convert * g / m * (0.5 * dt)
+        pos += v * dt
+        ep, g = grad(pos)
+        v += -convert * g / m * (0.5 * dt)
+        ek = 0.5 * np.sum(m * v * v) / convert
+        out[s] = (ep, ek, ep + ek)
+    return pos, v, out

@@ -226,7 +226,8 @@ void free_ctx(Ctx& c) {
                   c.d_xyz_orig, c.d_par_orig, c.d_rpole_orig, c.d_pole_local, c.d_frames, c.d_pos, c.d_posf,
                   c.d_thole, c.d_pol, c.d_rpole, c.d_sp_off, c.d_sp_k, c.d_sp_s, c.d_pos_built, c.d_nnb, c.d_nb,
                   c.d_npr, c.d_pk, c.d_pc3, c.d_pc5, c.d_ef, c.d_mu, c.d_res, c.d_h, c.d_pp, c.d_zr, c.d_dip,
-                  c.d_cphi, c.d_vecf, c.d_tmp6, c.d_tmp6b, c.d_partials, c.d_cg, c.d_flags};
+                  c.d_cphi, c.d_vecf, c.d_tmp6, c.d_tmp6b, c.d_partials, c.d_cg, c.d_flags,
+                  c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   pme_free(c);
@@ -481,6 +482,7 @@ int thp_set_frames(thp_ctx* h, const double* pole, const int* zaxis, const int* 
   cudaMemcpy(c.d_pole_local, pole, sizeof(double) * 13 * n, cudaMemcpyHostToDevice);
   cudaMemcpy(c.d_frames, fr.data(), sizeof(int) * 3 * n, cudaMemcpyHostToDevice);
   c.have_frames = true;
+  c.have_axes = true;
   h->rpole_dirty = true;
   h->field_valid = false;
   return cuda_status(cudaGetLastError(), &c, "set frames");
@@ -703,6 +705,105 @@ int thp_get_dipoles(thp_ctx* h, double* uind, double* uinp) {
   return THP_OK;
 }
 
+int thp_get_gradient_device(thp_ctx* h, double* d_dep) {
+  if (!h || !d_dep) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (!c.have_axes || !c.have_dipoles || !h->field_valid || !h->solved_once) return THP_E_STATE;
+  if (set_current_device(c)) return THP_E_CUDA;
+  return launch_forces(c, d_dep);
+}
+
+int thp_get_gradient(thp_ctx* h, double* dep, double* ep) {
+  if (!h || !dep) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (set_current_device(c)) return THP_E_CUDA;
+  if (!c.d_grad) {
+    int st = cuda_status(cudaMalloc((void**)&c.d_grad, sizeof(double) * 3 * c.n), &c, "alloc gradient");
+    if (st) return st;
+  }
+  int st = thp_get_gradient_device(h, c.d_grad);
+  if (st) return st;
+  cudaMemcpyAsync(dep, c.d_grad, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost, c.stream);
+  if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "gradient"))) return st;
+  if (ep) *ep = c.h_cg->epol;
+  return THP_OK;
+}
+
+int thp_get_positions(thp_ctx* h, double* x, double* y, double* z) {
+  if (!h || !x || !y || !z) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (!c.have_pos) return THP_E_STATE;
+  if (set_current_device(c)) return THP_E_CUDA;
+  const size_t n = c.n;
+  cudaMemcpyAsync(x, c.d_xyz_orig, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream);
+  cudaMemcpyAsync(y, c.d_xyz_orig + n, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream);
+  cudaMemcpyAsync(z, c.d_xyz_orig + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream);
+  return cuda_status(cudaStreamSynchronize(c.stream), &c, "get positions");
+}
+
+int thp_md_verlet(thp_ctx* h, int nsteps, double dt, const double* mass, double* vel, double* energies,
+                  int* niters) {
+  if (!h || !mass || !vel || nsteps < 0 || !(dt > 0.0)) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (!c.have_axes || !c.have_params || !c.have_pos) return THP_E_STATE;
+  if (set_current_device(c)) return THP_E_CUDA;
+  const size_t n = c.n;
+  for (size_t i = 0; i < n; ++i)
+    if (!(mass[i] > 0.0)) return THP_E_INVALID;
+  double *d_mass = nullptr, *d_vel = nullptr, *d_grad = nullptr, *d_scr = nullptr;
+  const size_t nscr = (n + 255) / 256 + 2;
+  int st = cuda_status(cudaMalloc((void**)&d_mass, sizeof(double) * n), &c, "md alloc");
+  if (!st) st = cuda_status(cudaMalloc((void**)&d_vel, sizeof(double) * 3 * n), &c, "md alloc");
+  if (!st) st = cuda_status(cudaMalloc((void**)&d_grad, sizeof(double) * 3 * n), &c, "md alloc");
+  if (!st) st = cuda_status(cudaMalloc((void**)&d_scr, sizeof(double) * nscr), &c, "md alloc");
+  if (!st) {
+    cudaMemcpyAsync(d_mass, mass, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
+    cudaMemcpyAsync(d_vel, vel, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c.stream);
+    st = cuda_status(cudaGetLastError(), &c, "md upload");
+  }
+  const int guess = THP_GUESS_PREVIOUS;
+  thp_solve_info info;
+  // gradient at the starting positions (mdinit's first gradient call)
+  if (!st) {
+    st = thp_solve(h, guess, &info);
+    if (st == THP_E_NOT_CONVERGED) st = THP_OK;
+  }
+  if (!st) st = launch_forces(c, d_grad);
+  for (int step = 0; step < nsteps && !st; ++step) {
+    if ((st = launch_kick(c, 0.5 * dt, d_mass, d_grad, d_vel))) break;
+    if ((st = launch_drift(c, dt, d_vel))) break;
+    h->pos_dirty = true;
+    h->field_valid = false;
+    c.have_coef = false;
+    if (c.have_frames) h->rpole_dirty = true;
+    st = thp_solve(h, guess, &info);
+    if (st && st != THP_E_NOT_CONVERGED) break;
+    st = THP_OK;
+    if ((st = launch_forces(c, d_grad))) break;
+    if ((st = launch_kick(c, 0.5 * dt, d_mass, d_grad, d_vel))) break;
+    if ((st = launch_ekin(c, d_mass, d_vel, d_scr))) break;
+    double ek = 0.0;
+    cudaMemcpyAsync(&ek, d_scr, sizeof(double), cudaMemcpyDeviceToHost, c.stream);
+    if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "md step"))) break;
+    if (energies) {
+      energies[3 * (size_t)step] = info.epol;
+      energies[3 * (size_t)step + 1] = ek;
+      energies[3 * (size_t)step + 2] = info.epol + ek;
+    }
+    if (niters) niters[step] = info.niter;
+  }
+  if (!st) {
+    cudaMemcpyAsync(vel, d_vel, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c.stream);
+    st = cuda_status(cudaStreamSynchronize(c.stream), &c, "md download");
+  }
+  cudaStreamSynchronize(c.stream);
+  cudaFree(d_mass);
+  cudaFree(d_vel);
+  cudaFree(d_grad);
+  cudaFree(d_scr);
+  return st;
+}
+
 int thp_get_field(thp_ctx* h, double* ef) {
   if (!h || !ef) return THP_E_INVALID;
   Ctx& c = h->c;
@@ -853,6 +954,12 @@ int thp_bind_state(thp_ctx* h, double* x, double* y, double* z, double* rpole, d
 
 int thp_last_error(void) { return g_last_error; }
 
+int thp_bind_gradient(thp_ctx* h, double* dep) {
+  if (!h) return THP_E_INVALID;
+  h->c.bdep = dep;
+  return THP_OK;
+}
+
 static int sync_bound_inputs(thp_ctx* h) {
   Ctx& c = h->c;
   if (!c.bx || !c.by || !c.bz) return THP_E_STATE;
@@ -911,6 +1018,25 @@ void epolar_(void) {
   if (!st || st == THP_E_NOT_CONVERGED) {
     if (h->c.bep) *h->c.bep = info.epol;
     if (h->c.buind) thp_get_dipoles(h, h->c.buind, h->c.buinp);
+  }
+  g_last_error = st;
+}
+
+void epolar1_(void) {
+  thp_ctx* h = g_current;
+  if (!h) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  int st = sync_bound_inputs(h);
+  thp_solve_info info;
+  if (!st) st = thp_solve(h, THP_GUESS_DIRECT, &info);
+  if (!st || st == THP_E_NOT_CONVERGED) {
+    int st2 = THP_OK;
+    if (h->c.bdep) st2 = thp_get_gradient(h, h->c.bdep, nullptr);
+    if (!st2 && h->c.bep) *h->c.bep = info.epol;
+    if (!st2 && h->c.buind) st2 = thp_get_dipoles(h, h->c.buind, h->c.buinp);
+    if (st2) st = st2;
   }
   g_last_error = st;
 }

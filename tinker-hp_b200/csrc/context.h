@@ -47,7 +47,8 @@ struct Ctx {
   // host copies (original atom order)
   std::vector<double> h_polarity, h_thole, h_pdamp;
   bool have_params = false, have_pos = false, have_rpole = false, have_conn = false;
-  bool have_frames = false;
+  bool have_frames = false;    // rpole comes from rotpole of d_pole_local
+  bool have_axes = false;      // d_frames holds the frame atoms (torques need them)
   std::vector<int> sp_off;     // special (scaled) pairs, original indices, CSR
   std::vector<int> sp_k;
   std::vector<double> sp_s;    // (d, p, u) per entry
@@ -133,11 +134,19 @@ struct Ctx {
   int* d_flags = nullptr;        // device error bits
   int* h_flags = nullptr;        // pinned
 
+  // polarization gradient (allocated on first use)
+  double* d_fphirec = nullptr;    // [n][20] permanent-multipole potential, fractional
+  unsigned long long* d_depfix = nullptr;  // [n][3] 64-bit fixed-point gradient, sorted
+  double* d_trq = nullptr;        // [n][3] reciprocal-space torque
+  int* d_frs = nullptr;           // [n][3] frame atoms (sorted indices), axis type
+  double* d_grad = nullptr;       // [n][3] gradient, original order
+
   // Fortran binding
   double *bx = nullptr, *by = nullptr, *bz = nullptr, *brpole = nullptr;
   double *buind = nullptr, *buinp = nullptr, *bep = nullptr;
   int *bnelst = nullptr, *belst = nullptr;
   int bmaxelst = 0;
+  double* bdep = nullptr;
 
   // CUDA graph of one CG chunk (captured on first use)
   cudaGraphExec_t chunk_exec = nullptr;

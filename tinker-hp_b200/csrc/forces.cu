@@ -1,0 +1,588 @@
+// forces.cu -- polarization energy gradient on the device (epolar1c).
+//
+// Restates epolar1c (epolar1.f:57-372) for a converged solve:
+//   * eprecip1 (epolar1.f:397-1213): the dipole grid of uind (Re) / uinp (Im)
+//     gathered to all 20 potential derivatives (fphi_uind_site), combined with
+//     the permanent-multipole potential fphirec kept from the field pass;
+//   * epreal1c (epolar1.f:1215-2540, Thole branch): per pair the gradient of
+//     the d- and p-scaled permanent field on uinp / uind and of the mutual
+//     tensor (uscale) on uind x uinp, plus the induced field and its gradient
+//     at every site for the torques;
+//   * self torque (epolar1.f:190-206), and torque (torque.f:6-390) for the
+//     Z-then-X and Bisector frames.
+// One thread owns atom i over the full neighbor list (each pair is evaluated
+// from both ends, the i-side terms only).  The three torques of a site are
+// summed before one torque distribution.  Gradients are accumulated in 64-bit
+// fixed point with 2^-34 kcal/mol/A resolution, so the order in which threads
+// add their contributions does not change the sums.
+#include <type_traits>
+
+#include "kernels.h"
+#include "pme_dev.cuh"
+
+namespace thp {
+
+namespace {
+
+constexpr int kBlock = 128;
+constexpr double kFix = 17179869184.0;  // 2^34
+
+__device__ __forceinline__ void fix_add(unsigned long long* a, double v) {
+  atomicAdd(a, (unsigned long long)(long long)llrint(v * kFix));
+}
+
+// torque.f:6-390, Z-then-X (axt 1) and Bisector (axt 2); site ib, z atom ia,
+// x atom ic; adds d(energy)/d(coordinates) of the torque trq.
+__device__ void torque_dist(const double4* __restrict__ pos, int ib, int ia, int ic, int axt, const double trq[3],
+                            unsigned long long* __restrict__ dep) {
+  const double4 pb = pos[ib], pa = pos[ia], pc = pos[ic];
+  double u[3] = {pa.x - pb.x, pa.y - pb.y, pa.z - pb.z};
+  double v[3] = {pc.x - pb.x, pc.y - pb.y, pc.z - pb.z};
+  const double usiz = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+  const double vsiz = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  double w[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+  const double wsiz = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    u[j] /= usiz;
+    v[j] /= vsiz;
+    w[j] /= wsiz;
+  }
+  double uv[3] = {v[1] * u[2] - v[2] * u[1], v[2] * u[0] - v[0] * u[2], v[0] * u[1] - v[1] * u[0]};
+  double uw[3] = {w[1] * u[2] - w[2] * u[1], w[2] * u[0] - w[0] * u[2], w[0] * u[1] - w[1] * u[0]};
+  double vw[3] = {w[1] * v[2] - w[2] * v[1], w[2] * v[0] - w[0] * v[2], w[0] * v[1] - w[1] * v[0]};
+  const double uvsiz = sqrt(uv[0] * uv[0] + uv[1] * uv[1] + uv[2] * uv[2]);
+  const double uwsiz = sqrt(uw[0] * uw[0] + uw[1] * uw[1] + uw[2] * uw[2]);
+  const double vwsiz = sqrt(vw[0] * vw[0] + vw[1] * vw[1] + vw[2] * vw[2]);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    uv[j] /= uvsiz;
+    uw[j] /= uwsiz;
+    vw[j] /= vwsiz;
+  }
+  const double uvcos = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+  const double uvsin = sqrt(1.0 - uvcos * uvcos);
+  const double dphidu = -trq[0] * u[0] - trq[1] * u[1] - trq[2] * u[2];
+  const double dphidv = -trq[0] * v[0] - trq[1] * v[1] - trq[2] * v[2];
+  const double dphidw = -trq[0] * w[0] - trq[1] * w[1] - trq[2] * w[2];
+  const double hw = axt == 2 ? 0.5 : 1.0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    double du = uv[j] * dphidv / (usiz * uvsin) + hw * uw[j] * dphidw / usiz;
+    double dv = -uv[j] * dphidu / (vsiz * uvsin);
+    if (axt == 2) dv += 0.5 * vw[j] * dphidw / vsiz;
+    fix_add(dep + 3 * ia + j, du);
+    fix_add(dep + 3 * ic + j, dv);
+    fix_add(dep + 3 * ib + j, -du - dv);
+  }
+}
+
+// fphi_uind_site (pmestuff.f:746-1045) in full and the force / torque of
+// eprecip1 (epolar1.f:636-720).  fphirec: [n][20] permanent potential
+// (unscaled), written by the field pass.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_force_recip(int n, PmeGeom g, const double4* __restrict__ pos,
+                                                        const typename Cplx<T>::type* __restrict__ grid,
+                                                        const double* __restrict__ fphirec,
+                                                        const double* __restrict__ mu, const double* __restrict__ rp,
+                                                        double* __restrict__ trq_out,
+                                                        unsigned long long* __restrict__ dep) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 p = pos[i];
+  T tx[kBs][4], ty[kBs][4], tz[kBs][4];
+  const int gx = bspline_axis<4, T>(p.x, g.recip[0], g.n1, tx);
+  const int gy = bspline_axis<4, T>(p.y, g.recip[1], g.n2, ty);
+  const int gz = bspline_axis<4, T>(p.z, g.recip[2], g.n3, tz);
+  // T1/T2: 100,010,001,200,020,002,110,101,011 of the d / p grids; S: 20 of their sum
+  T T1[9] = {0}, T2[9] = {0}, S[20] = {0};
+#pragma unroll
+  for (int c = 0; c < kBs; ++c) {
+    const size_t kk = (size_t)wrapk(gz + c, g.n3);
+    const T v0 = tz[c][0], v1 = tz[c][1], v2 = tz[c][2], v3 = tz[c][3];
+    T a1[6] = {0}, a2[6] = {0}, s[10] = {0};
+#pragma unroll
+    for (int b = 0; b < kBs; ++b) {
+      const size_t jj = (size_t)wrapk(gy + b, g.n2);
+      const T u0 = ty[b][0], u1 = ty[b][1], u2 = ty[b][2], u3 = ty[b][3];
+      T ta[3] = {0, 0, 0}, tb[3] = {0, 0, 0}, t3 = 0;
+      const size_t row = (kk * g.n2 + jj) * g.n1;
+#pragma unroll
+      for (int a = 0; a < kBs; ++a) {
+        const auto q = grid[row + wrapk(gx + a, g.n1)];
+        ta[0] += q.x * tx[a][0];
+        ta[1] += q.x * tx[a][1];
+        ta[2] += q.x * tx[a][2];
+        tb[0] += q.y * tx[a][0];
+        tb[1] += q.y * tx[a][1];
+        tb[2] += q.y * tx[a][2];
+        t3 += (q.x + q.y) * tx[a][3];
+      }
+      a1[0] += ta[0] * u0; a1[1] += ta[1] * u0; a1[2] += ta[0] * u1;
+      a1[3] += ta[2] * u0; a1[4] += ta[1] * u1; a1[5] += ta[0] * u2;
+      a2[0] += tb[0] * u0; a2[1] += tb[1] * u0; a2[2] += tb[0] * u1;
+      a2[3] += tb[2] * u0; a2[4] += tb[1] * u1; a2[5] += tb[0] * u2;
+      const T t0 = ta[0] + tb[0], t1 = ta[1] + tb[1], t2 = ta[2] + tb[2];
+      s[0] += t0 * u0; s[1] += t1 * u0; s[2] += t0 * u1; s[3] += t2 * u0; s[4] += t1 * u1;
+      s[5] += t0 * u2; s[6] += t3 * u0; s[7] += t2 * u1; s[8] += t1 * u2; s[9] += t0 * u3;
+    }
+    T1[0] += a1[1] * v0; T1[1] += a1[2] * v0; T1[2] += a1[0] * v1; T1[3] += a1[3] * v0; T1[4] += a1[5] * v0;
+    T1[5] += a1[0] * v2; T1[6] += a1[4] * v0; T1[7] += a1[1] * v1; T1[8] += a1[2] * v1;
+    T2[0] += a2[1] * v0; T2[1] += a2[2] * v0; T2[2] += a2[0] * v1; T2[3] += a2[3] * v0; T2[4] += a2[5] * v0;
+    T2[5] += a2[0] * v2; T2[6] += a2[4] * v0; T2[7] += a2[1] * v1; T2[8] += a2[2] * v1;
+    S[0] += s[0] * v0; S[1] += s[1] * v0; S[2] += s[2] * v0; S[3] += s[0] * v1; S[4] += s[3] * v0;
+    S[5] += s[5] * v0; S[6] += s[0] * v2; S[7] += s[4] * v0; S[8] += s[1] * v1; S[9] += s[2] * v1;
+    S[10] += s[6] * v0; S[11] += s[9] * v0; S[12] += s[0] * v3; S[13] += s[7] * v0; S[14] += s[3] * v1;
+    S[15] += s[8] * v0; S[16] += s[5] * v1; S[17] += s[1] * v2; S[18] += s[2] * v2; S[19] += s[4] * v1;
+  }
+  // 1-based views as in the reference (scaled by electric)
+  const double f = kElectric;
+  double FD[11], FP[11], FS[21], FR[21];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    FD[q + 2] = f * (double)T1[q];
+    FP[q + 2] = f * (double)T2[q];
+  }
+#pragma unroll
+  for (int q = 0; q < 20; ++q) {
+    FS[q + 1] = f * (double)S[q];
+    FR[q + 1] = f * fphirec[(size_t)i * 20 + q];
+  }
+  const double* m = mu + (size_t)i * 6;
+  const double fd[3] = {g.a[0] * m[0], g.a[1] * m[1], g.a[2] * m[2]};
+  const double fp[3] = {g.a[0] * m[3], g.a[1] * m[4], g.a[2] * m[5]};
+  const int d1[10] = {2, 5, 8, 9, 11, 16, 18, 14, 15, 20};
+  const int d2[10] = {3, 8, 6, 10, 14, 12, 19, 16, 20, 17};
+  const int d3[10] = {4, 9, 10, 7, 15, 17, 13, 20, 18, 19};
+  double f1 = 0.0, f2 = 0.0, f3 = 0.0;
+#pragma unroll
+  for (int k = 1; k <= 3; ++k) {
+    const double sdp = fd[k - 1] + fp[k - 1];
+    f1 += sdp * FR[d1[k]] + fd[k - 1] * FP[d1[k]] + fp[k - 1] * FD[d1[k]];
+    f2 += sdp * FR[d2[k]] + fd[k - 1] * FP[d2[k]] + fp[k - 1] * FD[d2[k]];
+    f3 += sdp * FR[d3[k]] + fd[k - 1] * FP[d3[k]] + fp[k - 1] * FD[d3[k]];
+  }
+  // fmp of the permanent moments (cart_to_frac, orthogonal box)
+  const double* r = rp + (size_t)i * 10;
+  const double cm[10] = {r[0], r[1], r[2], r[3], r[4], r[7], r[9], 2.0 * r[5], 2.0 * r[6], 2.0 * r[8]};
+  const double fm[10] = {cm[0], g.a[0] * cm[1], g.a[1] * cm[2], g.a[2] * cm[3], g.a[0] * g.a[0] * cm[4],
+                         g.a[1] * g.a[1] * cm[5], g.a[2] * g.a[2] * cm[6], g.a[0] * g.a[1] * cm[7],
+                         g.a[0] * g.a[2] * cm[8], g.a[1] * g.a[2] * cm[9]};
+#pragma unroll
+  for (int k = 0; k < 10; ++k) {
+    f1 += fm[k] * FS[d1[k]];
+    f2 += fm[k] * FS[d2[k]];
+    f3 += fm[k] * FS[d3[k]];
+  }
+  f1 = 0.5 * (double)g.n1 * f1;
+  f2 = 0.5 * (double)g.n2 * f2;
+  f3 = 0.5 * (double)g.n3 * f3;
+  fix_add(dep + 3 * i + 0, g.recip[0] * f1);
+  fix_add(dep + 3 * i + 1, g.recip[1] * f2);
+  fix_add(dep + 3 * i + 2, g.recip[2] * f3);
+  // cphidprec = fphi_to_cphi(fphidprec/2), torque on the permanent moments
+  double cp[10];
+  cp[0] = 0.5 * FS[1];
+  cp[1] = g.a[0] * 0.5 * FS[2];
+  cp[2] = g.a[1] * 0.5 * FS[3];
+  cp[3] = g.a[2] * 0.5 * FS[4];
+  cp[4] = g.a[0] * g.a[0] * 0.5 * FS[5];
+  cp[5] = g.a[1] * g.a[1] * 0.5 * FS[6];
+  cp[6] = g.a[2] * g.a[2] * 0.5 * FS[7];
+  cp[7] = g.a[0] * g.a[1] * 0.5 * FS[8];
+  cp[8] = g.a[0] * g.a[2] * 0.5 * FS[9];
+  cp[9] = g.a[1] * g.a[2] * 0.5 * FS[10];
+  double* t = trq_out + (size_t)i * 3;
+  t[0] = cm[3] * cp[2] - cm[2] * cp[3] + 2.0 * (cm[6] - cm[5]) * cp[9] + cm[8] * cp[7] + cm[9] * cp[5] -
+         cm[7] * cp[8] - cm[9] * cp[6];
+  t[1] = cm[1] * cp[3] - cm[3] * cp[1] + 2.0 * (cm[4] - cm[6]) * cp[8] + cm[7] * cp[9] + cm[8] * cp[6] -
+         cm[8] * cp[4] - cm[9] * cp[7];
+  t[2] = cm[2] * cp[1] - cm[1] * cp[2] + 2.0 * (cm[5] - cm[4]) * cp[7] + cm[7] * cp[4] + cm[9] * cp[8] -
+         cm[7] * cp[5] - cm[8] * cp[9];
+}
+
+// fphi_mpole_site (pmestuff.f:453-600): the 20 fractional potential
+// derivatives of the permanent-multipole grid, unscaled.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_fphi_mpole20(int n, PmeGeom g, const double4* __restrict__ pos,
+                                                         const typename Cplx<T>::type* __restrict__ grid,
+                                                         double* __restrict__ fphi) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 p = pos[i];
+  T tx[kBs][4], ty[kBs][4], tz[kBs][4];
+  const int gx = bspline_axis<4, T>(p.x, g.recip[0], g.n1, tx);
+  const int gy = bspline_axis<4, T>(p.y, g.recip[1], g.n2, ty);
+  const int gz = bspline_axis<4, T>(p.z, g.recip[2], g.n3, tz);
+  T S[20] = {0};
+#pragma unroll
+  for (int c = 0; c < kBs; ++c) {
+    const size_t kk = (size_t)wrapk(gz + c, g.n3);
+    const T v0 = tz[c][0], v1 = tz[c][1], v2 = tz[c][2], v3 = tz[c][3];
+    T s[10] = {0};  // 00,10,01,20,11,02,30,21,12,03
+#pragma unroll
+    for (int b = 0; b < kBs; ++b) {
+      const size_t jj = (size_t)wrapk(gy + b, g.n2);
+      const T u0 = ty[b][0], u1 = ty[b][1], u2 = ty[b][2], u3 = ty[b][3];
+      T t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+      const size_t row = (kk * g.n2 + jj) * g.n1;
+#pragma unroll
+      for (int a = 0; a < kBs; ++a) {
+        const T q = grid[row + wrapk(gx + a, g.n1)].x;
+        t0 += q * tx[a][0];
+        t1 += q * tx[a][1];
+        t2 += q * tx[a][2];
+        t3 += q * tx[a][3];
+      }
+      s[0] += t0 * u0; s[1] += t1 * u0; s[2] += t0 * u1; s[3] += t2 * u0; s[4] += t1 * u1;
+      s[5] += t0 * u2; s[6] += t3 * u0; s[7] += t2 * u1; s[8] += t1 * u2; s[9] += t0 * u3;
+    }
+    S[0] += s[0] * v0; S[1] += s[1] * v0; S[2] += s[2] * v0; S[3] += s[0] * v1; S[4] += s[3] * v0;
+    S[5] += s[5] * v0; S[6] += s[0] * v2; S[7] += s[4] * v0; S[8] += s[1] * v1; S[9] += s[2] * v1;
+    S[10] += s[6] * v0; S[11] += s[9] * v0; S[12] += s[0] * v3; S[13] += s[7] * v0; S[14] += s[3] * v1;
+    S[15] += s[8] * v0; S[16] += s[5] * v1; S[17] += s[1] * v2; S[18] += s[2] * v2; S[19] += s[4] * v1;
+  }
+  double* f = fphi + (size_t)i * 20;
+#pragma unroll
+  for (int q = 0; q < 20; ++q) f[q] = (double)S[q];
+}
+
+struct EwC {
+  double a, f1, f2, f3, f4;  // 2 a^2 powers / (sqrt(pi) a) of dampewald order 9
+};
+
+// epreal1c pair terms seen from atom i over its full list, the self torque,
+// and the torque distribution of the summed torque of site i.
+template <bool MIXED>
+__global__ void __launch_bounds__(kBlock) k_force_real(
+    int n, int npad, Box box, double off2, EwC ew, const double4* __restrict__ pos,
+    const typename std::conditional<MIXED, float, double>::type* __restrict__ mrec, const double* __restrict__ mu,
+    const int* __restrict__ perm, const int* __restrict__ sp_off, const int* __restrict__ sp_ks,
+    const double* __restrict__ sp_s, const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb,
+    const int* __restrict__ frs, const double* __restrict__ trq_recip, unsigned long long* __restrict__ dep) {
+  using T = typename std::conditional<MIXED, float, double>::type;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 pi4 = pos[i];
+  const T* ri = mrec + (size_t)i * 12;
+  const T pti = (T)ri[0], ci = (T)ri[1], dix = (T)ri[2], diy = (T)ri[3], diz = (T)ri[4];
+  const T qixx = (T)ri[5], qixy = (T)ri[6], qixz = (T)ri[7], qiyy = (T)ri[8], qiyz = (T)ri[9], qizz = (T)ri[10];
+  const double* mi = mu + (size_t)i * 6;
+  const T uix = (T)mi[0], uiy = (T)mi[1], uiz = (T)mi[2], uixp = (T)mi[3], uiyp = (T)mi[4], uizp = (T)mi[5];
+  const T pdi = (T)pi4.w;
+  const int io = perm[i];
+  const int s0 = sp_off[io], s1 = sp_off[io + 1];
+  const T f = (T)(0.5 * kElectric);
+  double gx = 0.0, gy = 0.0, gz = 0.0;
+  T uf[3] = {0, 0, 0}, duf[6] = {0, 0, 0, 0, 0, 0};
+  const int nn = min(nnb[i], maxnb);
+#pragma unroll 1
+  for (int s = 0; s < nn; ++s) {
+    const int k = __ldg(nb + (size_t)s * npad + i);
+    const double4 pk4 = pos[k];
+    double xrd = pk4.x - pi4.x, yrd = pk4.y - pi4.y, zrd = pk4.z - pi4.z;
+    image3(box, xrd, yrd, zrd);
+    const double r2d = r2_exact(xrd, yrd, zrd);
+    if (r2d > off2) continue;
+    T ds = 1, ps = 1, us = 1;
+    for (int q = s0; q < s1; ++q)
+      if (__ldg(sp_ks + q) == k) {
+        ds = (T)sp_s[3 * q];
+        ps = (T)sp_s[3 * q + 1];
+        us = (T)sp_s[3 * q + 2];
+        break;
+      }
+    const T* rk = mrec + (size_t)k * 12;
+    const T ptk = (T)rk[0], ck = (T)rk[1], dkx = (T)rk[2], dky = (T)rk[3], dkz = (T)rk[4];
+    const T qkxx = (T)rk[5], qkxy = (T)rk[6], qkxz = (T)rk[7], qkyy = (T)rk[8], qkyz = (T)rk[9], qkzz = (T)rk[10];
+    const double* mk = mu + (size_t)k * 6;
+    const T ukx = (T)mk[0], uky = (T)mk[1], ukz = (T)mk[2], ukxp = (T)mk[3], ukyp = (T)mk[4], ukzp = (T)mk[5];
+    const T xr = (T)xrd, yr = (T)yrd, zr = (T)zrd, r2 = (T)r2d;
+    const T r = sqrt(r2);
+    const T dir = dix * xr + diy * yr + diz * zr;
+    const T qix = qixx * xr + qixy * yr + qixz * zr, qiy = qixy * xr + qiyy * yr + qiyz * zr,
+            qiz = qixz * xr + qiyz * yr + qizz * zr;
+    const T qir = qix * xr + qiy * yr + qiz * zr;
+    const T dkr = dkx * xr + dky * yr + dkz * zr;
+    const T qkx = qkxx * xr + qkxy * yr + qkxz * zr, qky = qkxy * xr + qkyy * yr + qkyz * zr,
+            qkz = qkxz * xr + qkyz * yr + qkzz * zr;
+    const T qkr = qkx * xr + qky * yr + qkz * zr;
+    const T uir = uix * xr + uiy * yr + uiz * zr, uirp = uixp * xr + uiyp * yr + uizp * zr;
+    const T ukr = ukx * xr + uky * yr + ukz * zr, ukrp = ukxp * xr + ukyp * yr + ukzp * zr;
+    const T rr1 = f / r, rr3 = rr1 / r2, rr5 = T(3) * rr3 / r2, rr7 = T(5) * rr5 / r2, rr9 = T(7) * rr7 / r2;
+    // dampewald(9, r, r2, f) (damping.f:17-55)
+    const T ra = (T)ew.a * r;
+    const T ex = exp(-ra * ra);
+    const T b0 = erfc(ra) / r;
+    const T b1 = (b0 + (T)ew.f1 * ex) / r2, b2 = (T(3) * b1 + (T)ew.f2 * ex) / r2,
+            b3 = (T(5) * b2 + (T)ew.f3 * ex) / r2, b4 = (T(7) * b3 + (T)ew.f4 * ex) / r2;
+    const T e3 = f * b1, e5 = f * b2, e7 = f * b3, e9 = f * b4;
+    // Thole factors and their r-derivatives (epolar1.f:1620-1660)
+    T sc3 = 1, sc5 = 1, sc7 = 1, rc3[3] = {0, 0, 0}, rc5[3] = {0, 0, 0}, rc7[3] = {0, 0, 0};
+    T l3d = 1, l5d = 1, l7d = 1;  // damptholed order 7 for the energy-field (same values)
+    T damp = pdi * (T)pk4.w;
+    T pg = min(pti, ptk);
+    if (pg == T(0)) pg = max(pti, ptk);
+    if (damp != T(0) && pg != T(0)) {
+      const T t = r / damp;
+      damp = pg * (t * t * t);
+      if (damp < T(50)) {
+        const T ed = exp(-damp);
+        sc3 = T(1) - ed;
+        sc5 = T(1) - (T(1) + damp) * ed;
+        sc7 = T(1) - (T(1) + damp + T(0.6) * damp * damp) * ed;
+        const T temp3 = T(3) * damp * ed / r2, temp5 = damp, temp7 = T(-0.2) + T(0.6) * damp;
+        rc3[0] = xr * temp3;
+        rc3[1] = yr * temp3;
+        rc3[2] = zr * temp3;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          rc5[j] = rc3[j] * temp5;
+          rc7[j] = rc5[j] * temp7;
+        }
+        l3d = sc3;
+        l5d = sc5;
+        l7d = sc7;
+      }
+    }
+    (void)l3d;
+    (void)l5d;
+    (void)l7d;
+    const T psc3 = T(1) - sc3 * ps, psc5 = T(1) - sc5 * ps, psc7 = T(1) - sc7 * ps;
+    const T dsc3 = T(1) - sc3 * ds, dsc5 = T(1) - sc5 * ds, dsc7 = T(1) - sc7 * ds;
+    const T usc3 = T(1) - sc3 * us, usc5 = T(1) - sc5 * us;
+    const T psr3 = e3 - psc3 * rr3, psr5 = e5 - psc5 * rr5, psr7 = e7 - psc7 * rr7;
+    const T dsr3 = e3 - dsc3 * rr3, dsr5 = e5 - dsc5 * rr5, dsr7 = e7 - dsc7 * rr7;
+    const T usr5 = e5 - usc5 * rr5;
+    // induced field and gradient at i (ufld, dufld)
+    {
+      const T tix3 = psr3 * ukx + dsr3 * ukxp, tiy3 = psr3 * uky + dsr3 * ukyp, tiz3 = psr3 * ukz + dsr3 * ukzp;
+      const T tuir3 = -psr5 * ukr - dsr5 * ukrp;
+      uf[0] += tix3 + xr * tuir3;
+      uf[1] += tiy3 + yr * tuir3;
+      uf[2] += tiz3 + zr * tuir3;
+      const T tix5 = T(2) * (psr5 * ukx + dsr5 * ukxp), tiy5 = T(2) * (psr5 * uky + dsr5 * ukyp),
+              tiz5 = T(2) * (psr5 * ukz + dsr5 * ukzp);
+      const T tuir = -psr7 * ukr - dsr7 * ukrp;
+      duf[0] += xr * tix5 + xr * xr * tuir;
+      duf[1] += xr * tiy5 + yr * tix5 + T(2) * xr * yr * tuir;
+      duf[2] += yr * tiy5 + yr * yr * tuir;
+      duf[3] += xr * tiz5 + zr * tix5 + T(2) * xr * zr * tuir;
+      duf[4] += yr * tiz5 + zr * tiy5 + T(2) * yr * zr * tuir;
+      duf[5] += zr * tiz5 + zr * zr * tuir;
+    }
+    // permanent-field gradient parts (d with uinp, p with uind)
+    T frc[3] = {0, 0, 0};
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+      const T s3 = part ? psc3 : dsc3, s5 = part ? psc5 : dsc5, s7 = part ? psc7 : dsc7;
+      const T sr3 = part ? psr3 : dsr3, sr5 = part ? psr5 : dsr5, sr7 = part ? psr7 : dsr7;
+      const T sc = part ? ps : ds;
+      const T vkx = part ? ukx : ukxp, vky = part ? uky : ukyp, vkz = part ? ukz : ukzp;
+      const T vix = part ? uix : uixp, viy = part ? uiy : uiyp, viz = part ? uiz : uizp;
+      const T term1 = e5 - s3 * rr5, term2 = e7 - s5 * rr7, e9s = e9 - s7 * rr9;
+      const T x3[3] = {rc3[0] * sc, rc3[1] * sc, rc3[2] * sc};
+      const T x5[3] = {rc5[0] * sc, rc5[1] * sc, rc5[2] * sc};
+      const T x7[3] = {rc7[0] * sc, rc7[1] * sc, rc7[2] * sc};
+      T term3 = -sr3 + term1 * xr * xr - rr3 * xr * x3[0];
+      T term4 = rr3 * x3[0] - term1 * xr - sr5 * xr;
+      T term5 = term2 * xr * xr - sr5 - rr5 * xr * x5[0];
+      T term6 = e9s * xr * xr - e7 - rr7 * xr * x7[0];
+      T term7 = rr5 * x5[0] - T(2) * e7 * xr + (s5 + T(1.5) * s7) * rr7 * xr;
+      const T tixx = ci * term3 + dix * term4 + dir * term5 + T(2) * sr5 * qixx + (qiy * yr + qiz * zr) * s7 * rr7 +
+                     T(2) * qix * term7 + qir * term6;
+      const T tkxx = ck * term3 - dkx * term4 - dkr * term5 + T(2) * sr5 * qkxx + (qky * yr + qkz * zr) * s7 * rr7 +
+                     T(2) * qkx * term7 + qkr * term6;
+      term3 = -sr3 + term1 * yr * yr - rr3 * yr * x3[1];
+      term4 = rr3 * x3[1] - term1 * yr - sr5 * yr;
+      term5 = term2 * yr * yr - sr5 - rr5 * yr * x5[1];
+      term6 = e9s * yr * yr - e7 - rr7 * yr * x7[1];
+      term7 = rr5 * x5[1] - T(2) * e7 * yr + (s5 + T(1.5) * s7) * rr7 * yr;
+      const T tiyy = ci * term3 + diy * term4 + dir * term5 + T(2) * sr5 * qiyy + (qix * xr + qiz * zr) * s7 * rr7 +
+                     T(2) * qiy * term7 + qir * term6;
+      const T tkyy = ck * term3 - dky * term4 - dkr * term5 + T(2) * sr5 * qkyy + (qkx * xr + qkz * zr) * s7 * rr7 +
+                     T(2) * qky * term7 + qkr * term6;
+      term3 = -sr3 + term1 * zr * zr - rr3 * zr * x3[2];
+      term4 = rr3 * x3[2] - term1 * zr - sr5 * zr;
+      term5 = term2 * zr * zr - sr5 - rr5 * zr * x5[2];
+      term6 = e9s * zr * zr - e7 - rr7 * zr * x7[2];
+      term7 = rr5 * x5[2] - T(2) * e7 * zr + (s5 + T(1.5) * s7) * rr7 * zr;
+      const T tizz = ci * term3 + diz * term4 + dir * term5 + T(2) * sr5 * qizz + (qix * xr + qiy * yr) * s7 * rr7 +
+                     T(2) * qiz * term7 + qir * term6;
+      const T tkzz = ck * term3 - dkz * term4 - dkr * term5 + T(2) * sr5 * qkzz + (qkx * xr + qky * yr) * s7 * rr7 +
+                     T(2) * qkz * term7 + qkr * term6;
+      term3 = term1 * xr * yr - rr3 * yr * x3[0];
+      term4 = rr3 * x3[0] - term1 * xr;
+      term5 = term2 * xr * yr - rr5 * yr * x5[0];
+      term6 = e9s * xr * yr - rr7 * yr * x7[0];
+      term7 = rr5 * x5[0] - term2 * xr;
+      const T tixy = ci * term3 - sr5 * dix * yr + diy * term4 + dir * term5 + T(2) * sr5 * qixy -
+                     T(2) * sr7 * yr * qix + T(2) * qiy * term7 + qir * term6;
+      const T tkxy = ck * term3 + sr5 * dkx * yr - dky * term4 - dkr * term5 + T(2) * sr5 * qkxy -
+                     T(2) * sr7 * yr * qkx + T(2) * qky * term7 + qkr * term6;
+      term3 = term1 * xr * zr - rr3 * zr * x3[0];
+      term5 = term2 * xr * zr - rr5 * zr * x5[0];
+      term6 = e9s * xr * zr - rr7 * zr * x7[0];
+      const T tixz = ci * term3 - sr5 * dix * zr + diz * term4 + dir * term5 + T(2) * sr5 * qixz -
+                     T(2) * sr7 * zr * qix + T(2) * qiz * term7 + qir * term6;
+      const T tkxz = ck * term3 + sr5 * dkx * zr - dkz * term4 - dkr * term5 + T(2) * sr5 * qkxz -
+                     T(2) * sr7 * zr * qkx + T(2) * qkz * term7 + qkr * term6;
+      term3 = term1 * yr * zr - rr3 * zr * x3[1];
+      term4 = rr3 * x3[1] - term1 * yr;
+      term5 = term2 * yr * zr - rr5 * zr * x5[1];
+      term6 = e9s * yr * zr - rr7 * zr * x7[1];
+      term7 = rr5 * x5[1] - term2 * yr;
+      const T tiyz = ci * term3 - sr5 * diy * zr + diz * term4 + dir * term5 + T(2) * sr5 * qiyz -
+                     T(2) * sr7 * zr * qiy + T(2) * qiz * term7 + qir * term6;
+      const T tkyz = ck * term3 + sr5 * dky * zr - dkz * term4 - dkr * term5 + T(2) * sr5 * qkyz -
+                     T(2) * sr7 * zr * qky + T(2) * qkz * term7 + qkr * term6;
+      frc[0] += tixx * vkx + tixy * vky + tixz * vkz - tkxx * vix - tkxy * viy - tkxz * viz;
+      frc[1] += tixy * vkx + tiyy * vky + tiyz * vkz - tkxy * vix - tkyy * viy - tkyz * viz;
+      frc[2] += tixz * vkx + tiyz * vky + tizz * vkz - tkxz * vix - tkyz * viy - tkzz * viz;
+    }
+    // mutual part (uscale)
+    {
+      const T term1 = e5 - usc3 * rr5, term2 = e7 - usc5 * rr7, term3 = usr5 + term1;
+      T term4 = rr3 * us;
+      T term5 = -xr * term3 + rc3[0] * term4;
+      T term6 = -usr5 + xr * xr * term2 - rr5 * xr * rc5[0] * us;
+      const T tixx = uix * term5 + uir * term6, tkxx = ukx * term5 + ukr * term6;
+      term5 = -yr * term3 + rc3[1] * term4;
+      term6 = -usr5 + yr * yr * term2 - rr5 * yr * rc5[1] * us;
+      const T tiyy = uiy * term5 + uir * term6, tkyy = uky * term5 + ukr * term6;
+      term5 = -zr * term3 + rc3[2] * term4;
+      term6 = -usr5 + zr * zr * term2 - rr5 * zr * rc5[2] * us;
+      const T tizz = uiz * term5 + uir * term6, tkzz = ukz * term5 + ukr * term6;
+      term4 = -usr5 * yr;
+      term5 = -xr * term1 + rr3 * rc3[0] * us;
+      term6 = xr * yr * term2 - rr5 * yr * rc5[0] * us;
+      const T tixy = uix * term4 + uiy * term5 + uir * term6, tkxy = ukx * term4 + uky * term5 + ukr * term6;
+      term4 = -usr5 * zr;
+      term6 = xr * zr * term2 - rr5 * zr * rc5[0] * us;
+      const T tixz = uix * term4 + uiz * term5 + uir * term6, tkxz = ukx * term4 + ukz * term5 + ukr * term6;
+      term5 = -yr * term1 + rr3 * rc3[1] * us;
+      term6 = yr * zr * term2 - rr5 * zr * rc5[1] * us;
+      const T tiyz = uiy * term4 + uiz * term5 + uir * term6, tkyz = uky * term4 + ukz * term5 + ukr * term6;
+      frc[0] += tixx * ukxp + tixy * ukyp + tixz * ukzp + tkxx * uixp + tkxy * uiyp + tkxz * uizp;
+      frc[1] += tixy * ukxp + tiyy * ukyp + tiyz * ukzp + tkxy * uixp + tkyy * uiyp + tkyz * uizp;
+      frc[2] += tixz * ukxp + tiyz * ukyp + tizz * ukzp + tkxz * uixp + tkyz * uiyp + tkzz * uizp;
+    }
+    gx -= (double)frc[0];
+    gy -= (double)frc[1];
+    gz -= (double)frc[2];
+  }
+  fix_add(dep + 3 * i + 0, gx);
+  fix_add(dep + 3 * i + 1, gy);
+  fix_add(dep + 3 * i + 2, gz);
+  // torques: real-space induced field (epolar1.f:2427-2470) + reciprocal + self
+  const double* u6 = mu + (size_t)i * 6;
+  const double sterm = (4.0 / 3.0) * kElectric * ew.a * ew.a * ew.a / kSqrtPi;
+  const double hx = 0.5 * (u6[0] + u6[3]), hy = 0.5 * (u6[1] + u6[4]), hz = 0.5 * (u6[2] + u6[5]);
+  const double rdx = (double)ri[2], rdy = (double)ri[3], rdz = (double)ri[4];
+  double tep[3];
+  tep[0] = (double)(diz * uf[1] - diy * uf[2] + qixz * duf[1] - qixy * duf[3] + T(2) * qiyz * (duf[2] - duf[5]) +
+                    (qizz - qiyy) * duf[4]);
+  tep[1] = (double)(dix * uf[2] - diz * uf[0] - qiyz * duf[1] + qixy * duf[4] + T(2) * qixz * (duf[5] - duf[0]) +
+                    (qixx - qizz) * duf[3]);
+  tep[2] = (double)(diy * uf[0] - dix * uf[1] + qiyz * duf[3] - qixz * duf[4] + T(2) * qixy * (duf[0] - duf[2]) +
+                    (qiyy - qixx) * duf[1]);
+  tep[0] += trq_recip[(size_t)i * 3 + 0] + sterm * (rdy * hz - rdz * hy);
+  tep[1] += trq_recip[(size_t)i * 3 + 1] + sterm * (rdz * hx - rdx * hz);
+  tep[2] += trq_recip[(size_t)i * 3 + 2] + sterm * (rdx * hy - rdy * hx);
+  const int iz = frs[3 * i], ix = frs[3 * i + 1], axt = frs[3 * i + 2];
+  if (axt == 1 || axt == 2) torque_dist(pos, i, iz, ix, axt, tep, dep);
+}
+
+// sorted frame atoms: frs[s] = (iperm[zaxis], iperm[xaxis], axt) of perm[s]
+__global__ void k_frames_sorted(int n, const int* __restrict__ perm, const int* __restrict__ iperm,
+                                const int* __restrict__ frames, int* __restrict__ frs) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int o = perm[s];
+  frs[3 * s] = iperm[frames[3 * o]];
+  frs[3 * s + 1] = iperm[frames[3 * o + 1]];
+  frs[3 * s + 2] = frames[3 * o + 2];
+}
+
+__global__ void k_dep_out(int n, const int* __restrict__ perm, const unsigned long long* __restrict__ dep,
+                          double* __restrict__ out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int o = perm[s];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) out[3 * (size_t)o + j] = (double)(long long)dep[3 * (size_t)s + j] / kFix;
+}
+
+}  // namespace
+
+template <typename P>
+static int alloc_once(Ctx& c, P** p, size_t count, const char* what) {
+  if (*p) return THP_OK;
+  return cuda_status(cudaMalloc((void**)p, sizeof(P) * count), &c, what);
+}
+
+// Gradient of the polarization energy for the converged dipoles in d_mu
+// (sorted); writes dE/dx [n][3] in ORIGINAL atom order into d_out.
+int launch_forces(Ctx& c, double* d_out) {
+  int st;
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  if (!c.have_axes) return THP_E_STATE;
+  const size_t n = c.n;
+  if ((st = alloc_once(c, &c.d_fphirec, 20 * n, "alloc fphirec"))) return st;
+  if ((st = alloc_once(c, &c.d_depfix, 3 * n, "alloc gradient"))) return st;
+  if ((st = alloc_once(c, &c.d_trq, 3 * n, "alloc torque"))) return st;
+  if ((st = alloc_once(c, &c.d_frs, 3 * n, "alloc frames"))) return st;
+  unsigned long long* dep = c.d_depfix;
+  if ((st = cuda_status(cudaMemsetAsync(dep, 0, sizeof(unsigned long long) * 3 * n, c.stream), &c, "zero gradient")))
+    return st;
+  k_frames_sorted<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, c.d_iperm, c.d_frames, c.d_frs);
+  PmeGeom g = pme_geom(c);
+  // permanent-multipole potential, 20 derivatives per site
+  if ((st = launch_mpole_grid(c))) return st;
+  if (c.mixed)
+    k_fphi_mpole20<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftComplex*)c.d_grid, c.d_fphirec);
+  else
+    k_fphi_mpole20<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftDoubleComplex*)c.d_grid,
+                                                        c.d_fphirec);
+  if ((st = cuda_status(cudaGetLastError(), &c, "fphi mpole"))) return st;
+  // dipole grid of uind (Re) / uinp (Im), convolved
+  if ((st = launch_pme_dipole(c, c.d_mu, nullptr, 0))) return st;
+  if (c.mixed)
+    k_force_recip<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftComplex*)c.d_grid, c.d_fphirec,
+                                                      c.d_mu, c.d_rpole, c.d_trq, dep);
+  else
+    k_force_recip<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftDoubleComplex*)c.d_grid,
+                                                       c.d_fphirec, c.d_mu, c.d_rpole, c.d_trq, dep);
+  if ((st = cuda_status(cudaGetLastError(), &c, "force recip"))) return st;
+  EwC ew;
+  const double a = c.cfg.aewald;
+  double aesq2 = 2.0 * a * a, afac = 1.0 / (kSqrtPi * a);
+  ew.a = a;
+  afac *= aesq2;
+  ew.f1 = afac;
+  afac *= aesq2;
+  ew.f2 = afac;
+  afac *= aesq2;
+  ew.f3 = afac;
+  afac *= aesq2;
+  ew.f4 = afac;
+  const double off2 = c.cfg.ewaldcut * c.cfg.ewaldcut;
+#define THP_FORCE_ARGS                                                                                          \
+  c.n, c.npad, c.box, off2, ew, c.d_pos, MREC, c.d_mu, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_s, c.d_nnb, c.d_nb, \
+      c.maxnb, c.d_frs, c.d_trq, dep
+  if (c.mixed) {
+#define MREC c.d_mrecf
+    k_force_real<true><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
+#undef MREC
+  } else {
+#define MREC c.d_mrec
+    k_force_real<false><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
+#undef MREC
+  }
+#undef THP_FORCE_ARGS
+  if ((st = cuda_status(cudaGetLastError(), &c, "force real"))) return st;
+  k_dep_out<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, dep, d_out);
+  return cuda_status(cudaGetLastError(), &c, "force out");
+}
+
+}  // namespace thp

@@ -22,11 +22,20 @@ int pme_init(Ctx& c);
 void pme_free(Ctx& c);
 int launch_efld0_recip(Ctx& c);         // d_cphi and E0 completion
 int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0);
+int launch_mpole_grid(Ctx& c);          // permanent-multipole grid, convolved (grid holds the potential)
 int zero_grid(Ctx& c);
 struct PmeGeom;
 PmeGeom pme_geom(const Ctx& c);
 int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode);
 int launch_gather_dip(Ctx& c, double* d_out, bool check_stop);
+
+// forces.cu
+int launch_forces(Ctx& c, double* d_out);  // dE/dx [n][3], original order, for the dipoles in d_mu
+
+// md.cu
+int launch_kick(Ctx& c, double half_dt, const double* d_mass, const double* d_grad, double* d_vel);
+int launch_drift(Ctx& c, double dt, const double* d_vel);          // advances d_xyz_orig
+int launch_ekin(Ctx& c, const double* d_mass, const double* d_vel, double* d_scratch);
 
 // solver.cu
 int run_pcg(Ctx& c, int guess);

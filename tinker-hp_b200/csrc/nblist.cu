@@ -346,6 +346,13 @@ int launch_sort_atoms(Ctx& c) {
   const int n = c.n;
   const int nb = (n + kBlock - 1) / kBlock;
   cudaStream_t s = c.stream;
+  // the last dipoles (warm start) follow their atoms into the new order; the
+  // CG residual buffer is free between solves and holds them meanwhile
+  const bool keep_mu = c.have_perm && c.have_dipoles;
+  if (keep_mu) {
+    int st = launch_to_orig6(c, c.d_mu, c.d_res, 2);
+    if (st) return st;
+  }
   cudaMemsetAsync(c.d_cell_count, 0, sizeof(int) * c.ncell, s);
   cudaMemsetAsync(c.d_cell_fill, 0, sizeof(int) * c.ncell, s);
   k_cell_count<<<nb, kBlock, 0, s>>>(n, c.box, c.nc[0], c.nc[1], c.nc[2], c.d_xyz_orig, c.d_atom_cell,
@@ -357,7 +364,9 @@ int launch_sort_atoms(Ctx& c) {
   c.have_perm = true;
   const int m = (int)c.sp_k.size();
   if (m > 0) k_sp_to_sorted<<<(m + 255) / 256, 256, 0, s>>>(m, c.d_iperm, c.d_sp_k, c.d_sp_ks);
-  return cuda_status(cudaGetLastError(), &c, "sort atoms");
+  int st = cuda_status(cudaGetLastError(), &c, "sort atoms");
+  if (!st && keep_mu) st = launch_to_sorted6(c, c.d_res, c.d_mu, 2);
+  return st;
 }
 
 int launch_gather_sorted(Ctx& c) {

@@ -430,7 +430,7 @@ int zero_grid(Ctx& c) {
 
 // Permanent-multipole PME: d_cphi (and cphi10 when non-null) and, when
 // with_e0, completes d_ef = E_direct - cphi(2:4) + (4/3) a^3/sqrt(pi) d.
-int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0) {
+int launch_mpole_grid(Ctx& c) {
   PmeGeom g = geom_of(c);
   int nb = (c.n + kBlock - 1) / kBlock;
   int st = zero_grid(c);
@@ -440,7 +440,14 @@ int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0) {
   else
     k_spread_mpole<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, c.d_rpole, (cufftDoubleComplex*)c.d_grid);
   if ((st = cuda_status(cudaGetLastError(), &c, "spread mpole"))) return st;
-  if ((st = convolve(c, 0))) return st;
+  return convolve(c, 0);
+}
+
+int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0) {
+  PmeGeom g = geom_of(c);
+  int nb = (c.n + kBlock - 1) / kBlock;
+  int st = launch_mpole_grid(c);
+  if (st) return st;
   double a = c.cfg.aewald;
   double term = (4.0 / 3.0) * a * a * a / kSqrtPi;
   if (c.mixed)

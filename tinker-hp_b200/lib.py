@@ -82,6 +82,10 @@ def load():
         "thp_profile": ([vp, C.c_int, _dp, _ip], C.c_int),
         "thp_solve": ([vp, C.c_int, C.POINTER(ThpSolveInfo)], C.c_int),
         "thp_get_dipoles": ([vp, _dp, _dp], C.c_int),
+        "thp_get_gradient": ([vp, _dp, _dp], C.c_int),
+        "thp_get_gradient_device": ([vp, vp], C.c_int),
+        "thp_md_verlet": ([vp, C.c_int, C.c_double, _dp, _dp, _dp, _ip], C.c_int),
+        "thp_get_positions": ([vp, _dp, _dp, _dp], C.c_int),
         "thp_get_field": ([vp, _dp], C.c_int),
         "thp_get_rpole": ([vp, _dp], C.c_int),
         "thp_get_nblist": ([vp, C.c_int, _ip, _ip], C.c_int),
@@ -95,6 +99,7 @@ def load():
         "thp_status_string": ([C.c_int], C.c_char_p),
         "thp_bind_state": ([vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_int, _dp], C.c_int),
         "thp_last_error": ([], C.c_int),
+        "thp_bind_gradient": ([vp, _dp], C.c_int),
         "thp_epolar_noalloc": ([C.c_int, vp, vp, vp, vp], C.c_int),
         "newinduce_pme2_": ([], None),
         "tmatxb_pme_": ([_ip, _ip, _dp, _dp], None),
@@ -104,6 +109,7 @@ def load():
         "mlistcell_": ([], None),
         "vlistcell_": ([], None),
         "epolar_": ([], None),
+        "epolar1_": ([], None),
         "inducepcg_pme2_": ([vp, _ip, _ip, _dp, _dp, _dp], None),
     }
     for name, (args, res) in sig.items():
@@ -260,6 +266,29 @@ class Context:
         uinp = np.zeros((self.n, 3))
         self._check(load().thp_get_dipoles(self.h, _p(uind), _p(uinp)), "thp_get_dipoles")
         return uind, uinp
+
+    def gradient(self):
+        """(Epol, dEpol/dx [n,3] kcal/mol/A) for the dipoles of the last solve."""
+        dep = np.zeros((self.n, 3))
+        ep = C.c_double()
+        self._check(load().thp_get_gradient(self.h, _p(dep), C.byref(ep)), "thp_get_gradient")
+        return ep.value, dep
+
+    def md_verlet(self, nsteps, dt, mass, vel):
+        """Velocity-Verlet NVE steps on the device (dt in ps).  Returns
+        (velocities [n,3], energies [nsteps,3] = epol/kinetic/total, CG
+        iterations [nsteps]); positions() gives the advanced positions."""
+        vel = np.ascontiguousarray(vel, dtype=np.float64).copy()
+        en = np.zeros((nsteps, 3))
+        it = np.zeros(nsteps, np.int32)
+        self._check(load().thp_md_verlet(self.h, nsteps, dt, _p(_f64(mass)), _p(vel), _p(en), _p(it, _ip)),
+                    "thp_md_verlet")
+        return vel, en, it
+
+    def positions(self):
+        x, y, z = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        self._check(load().thp_get_positions(self.h, _p(x), _p(y), _p(z)), "thp_get_positions")
+        return np.stack([x, y, z], axis=1)
 
     def field(self):
         ef = np.zeros((self.n, 2, 3))

@@ -28,6 +28,13 @@ WATER_MULTIPOLES = {
     },
 }
 
+# water03.prm:80-81 (atom masses, g/mol)
+WATER_MASS = {"O": 15.995, "H": 1.008}
+
+# units.f:71,76: Boltzmann constant in g A^2/ps^2/mol/K and kcal/mol -> g A^2/ps^2
+BOLTZMANN = 0.831446215
+CONVERT = 418.4
+
 # water03.prm:155-156 (polarize: alpha A^3, thole)
 WATER_POLARITY = {"O": 0.837, "H": 0.496}
 WATER_THOLE = {"O": 0.390, "H": 0.390}

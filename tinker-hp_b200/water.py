@@ -231,6 +231,22 @@ def water_connectivity_fast(nw):
             "ip11": (off11, idx11), "ip12": empty, "ip13": empty, "ip14": empty}
 
 
+def masses(ws):
+    """Atom masses [n] g/mol (water03.prm:80-81); atoms are O, H, H per molecule."""
+    m = np.full(ws.n, P.WATER_MASS["H"])
+    m[0::3] = P.WATER_MASS["O"]
+    return m
+
+
+def maxwell_velocities(mass, kelvin=300.0, seed=3001):
+    """Velocities [n,3] A/ps from the Maxwell-Boltzmann distribution at
+    `kelvin` (mdinit.f:550-560, maxwell.f:23-52: each Cartesian component is
+    normal with variance kB T / m)."""
+    rng = np.random.default_rng(seed)
+    sigma = np.sqrt(P.BOLTZMANN * kelvin / np.asarray(mass, dtype=np.float64))
+    return rng.standard_normal((len(mass), 3)) * sigma[:, None]
+
+
 def min_box_edge(ewaldcut=P.EWALD_CUTOFF, lbuffer=P.LIST_BUFFER, margin=0.2):
     """Smallest cubic edge with the list cutoff inside half a box
     (the reference's minimum-image check, nblist.f:147-156)."""
