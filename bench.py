@@ -50,9 +50,11 @@ WORKLOADS = {
     "water-1944": (648, 0),
 }
 DEBYE = 4.80321
-# CG stop threshold (Tinker's poleps units) for both forms: chosen so that the
-# dipoles are within 1e-5 D RMS of the fully converged FP64 answer on the box
-CG_TOL = 2e-6
+# CG stop threshold (Tinker's poleps, internal e*A units) for both forms: the
+# dipole error against the fully converged FP64 answer tracks it (about 4x in
+# Debye, identical in both forms) and stays at 3-4e-6 D on every box measured,
+# inside the 1e-5 D acceptance; 2e-6 lands at 1.05-1.17e-5 D on some boxes
+CG_TOL = 1e-6
 
 
 class ClockSampler:

@@ -192,6 +192,8 @@ int thp_bind_state(thp_ctx* ctx, double* x, double* y, double* z, double* rpole,
 int thp_last_error(void);
 /* bind deriv::dep(3,n), written by epolar1_ */
 int thp_bind_gradient(thp_ctx* ctx, double* dep);
+/* bind pme::qgrid2in_2d(2,n1,n2,n3), read by fphi_uind_site_ */
+int thp_bind_grid(thp_ctx* ctx, double* qgrid);
 
 /* newinduce_pme2.f:16 -- fields, guess, PCG, writeback of uind/uinp */
 void newinduce_pme2_(void);
@@ -211,6 +213,26 @@ void efld0_recip_(double* cphi);
 /* newinduce_pme.f:1919 -- reciprocal dipole field; murec/dipfieldbis unused */
 void tmatxbrecip_(const double* mu, const double* murec, const int* nrhs, double* dipfield,
                   double* dipfieldbis);
+/* pmestuff.f:280 grid_uind_site, batched: adds the fractional dipoles
+ * fuind/fuinp(3,nsites) of atoms isite(nsites) (1-based) into the caller's
+ * grid qgrid(2,n1,n2,n3) (one rank: the whole grid is local).  B-splines come
+ * from the bound positions.  Spread on the device (FP64); the grid crosses
+ * the bus once per call. */
+void grid_uind_sites_(const int* nsites, const int* isite, const double* fuind, const double* fuinp,
+                      double* qgrid);
+/* pmestuff.f:746 fphi_uind_site, batched: fdip_phi1/2(10,nsites) and
+ * fdip_sum_phi(20,nsites) of the caller's grid at atoms isite (1-based);
+ * slot 1 of fdip_phi1/2 is zero as the reference leaves it unset. */
+void fphi_uind_sites_(const int* nsites, const int* isite, const double* qgrid, double* fdip_phi1,
+                      double* fdip_phi2, double* fdip_sum_phi);
+/* the reference's per-site signatures (impi unused: B-splines are recomputed
+ * from the positions).  Each call moves the whole grid across the bus, so
+ * they exist for completeness; the batched forms above are the fast path.
+ * fphi_uind_site_ reads the grid bound by thp_bind_grid. */
+void grid_uind_site_(const int* isite, const int* impi, const double* fuind, const double* fuinp,
+                     double* qgrid2loc);
+void fphi_uind_site_(const int* isite, const int* impi, double* fdip_phi1, double* fdip_phi2,
+                     double* fdip_sum_phi);
 /* nblist.f:117 -- rebuild the polarization list; fills the bound elst/nelst */
 void mlistcell_(void);
 /* nblist.f:1148 -- same list for the vdW slot name used by the workload */

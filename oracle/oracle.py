@@ -69,6 +69,8 @@ def lib():
         L.or_epolar.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         L.or_epolar1.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, _dp, _dp]
         L.or_rotpole.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _dp]
+        L.or_grid_uind_sites.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp, _dp]
+        L.or_fphi_uind_sites.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp, _dp, _dp]
         L.or_ewaldcof.restype = C.c_double
         L.or_ewaldcof.argtypes = [C.c_double]
         L.or_erfc.restype = C.c_double
@@ -218,6 +220,29 @@ class Oracle:
         if st != 0:
             raise RuntimeError(f"oracle epolar1 status {st}")
         return ep.value, dep
+
+    def grid_uind_sites(self, sites, fuind, fuinp, grid):
+        """grid_uind_site for 0-based `sites`: adds into a copy of the complex
+        grid [n3,n2,n1] and returns it."""
+        sites = np.ascontiguousarray(sites, dtype=np.int32)
+        g = np.ascontiguousarray(grid, dtype=np.complex128).copy()
+        st = lib().or_grid_uind_sites(self.ctx, len(sites), _p(sites, _ip), _p(np.ascontiguousarray(fuind, float)),
+                                      _p(np.ascontiguousarray(fuinp, float)), g.ctypes.data_as(_dp))
+        if st != 0:
+            raise RuntimeError("oracle grid_uind_sites: bad site")
+        return g
+
+    def fphi_uind_sites(self, sites, grid):
+        """fphi_uind_site for 0-based `sites` on a complex grid [n3,n2,n1]:
+        (fdip_phi1 [ns,10], fdip_phi2 [ns,10], fdip_sum_phi [ns,20])."""
+        sites = np.ascontiguousarray(sites, dtype=np.int32)
+        g = np.ascontiguousarray(grid, dtype=np.complex128)
+        p1, p2, sm = np.zeros((len(sites), 10)), np.zeros((len(sites), 10)), np.zeros((len(sites), 20))
+        st = lib().or_fphi_uind_sites(self.ctx, len(sites), _p(sites, _ip), g.ctypes.data_as(_dp), _p(p1), _p(p2),
+                                      _p(sm))
+        if st != 0:
+            raise RuntimeError("oracle fphi_uind_sites: bad site")
+        return p1, p2, sm
 
     def epolar(self, uind):
         uind = np.ascontiguousarray(uind, dtype=np.float64)

@@ -584,6 +584,11 @@ void spread_sites(OrCtx* c, F&& site_terms) {
   }
 }
 
+// fphi_uind_site (pmestuff.f:746-1045) for site i on grid g: phi1/phi2 hold
+// fdip_phi1/2(1:10) (index 0 unused, 1..9 = 100,010,001,200,020,002,110,101,
+// 011 of the Re / Im grid), sum holds fdip_sum_phi(1:20) of Re + Im.
+void fphi_dip_site(const OrCtx* c, int i, const cd* g, double phi1[10], double phi2[10], double sum[20]);
+
 void convolve(OrCtx* c) {
   const OrSystem& s = c->s;
   int nthr = nthreads_of(&s);
@@ -1484,7 +1489,117 @@ void torque_site(const double* x, const double* y, const double* z, int ib, int 
 
 }  // namespace
 
+namespace {
+
+void fphi_dip_site(const OrCtx* c, int i, const cd* g, double phi1[10], double phi2[10], double sum[20]) {
+  const OrSystem& s = c->s;
+  const int bs = c->bsorder;
+  const double* th1 = &c->theta1[(size_t)i * bs * 4];
+  const double* th2 = &c->theta2[(size_t)i * bs * 4];
+  const double* th3 = &c->theta3[(size_t)i * bs * 4];
+  const int* ig = &c->igrid[i * 3];
+  double* T1 = phi1;
+  double* T2 = phi2;
+  double* S = sum;
+  for (int q = 0; q < 10; ++q) T1[q] = T2[q] = 0.0;
+  for (int q = 0; q < 20; ++q) S[q] = 0.0;
+  for (int it3 = 1; it3 <= bs; ++it3) {
+    int k = gather_index(ig[2], it3, s.nfft3);
+    double v0 = th3[(it3 - 1) * 4], v1 = th3[(it3 - 1) * 4 + 1], v2 = th3[(it3 - 1) * 4 + 2],
+           v3 = th3[(it3 - 1) * 4 + 3];
+    double tu1[6] = {0}, tu2[6] = {0}, tu[10] = {0};  // 00,10,01,20,11,02 ; sum: +30,21,12,03
+    for (int it2 = 1; it2 <= bs; ++it2) {
+      int j = gather_index(ig[1], it2, s.nfft2);
+      double u0 = th2[(it2 - 1) * 4], u1 = th2[(it2 - 1) * 4 + 1], u2 = th2[(it2 - 1) * 4 + 2],
+             u3 = th2[(it2 - 1) * 4 + 3];
+      double t1a[3] = {0}, t1b[3] = {0}, t3 = 0.0;
+      for (int it1 = 1; it1 <= bs; ++it1) {
+        int ii = gather_index(ig[0], it1, s.nfft1);
+        cd q = g[((size_t)k * s.nfft2 + j) * s.nfft1 + ii];
+        const double* w = &th1[(it1 - 1) * 4];
+        t1a[0] += q.real() * w[0];
+        t1a[1] += q.real() * w[1];
+        t1a[2] += q.real() * w[2];
+        t1b[0] += q.imag() * w[0];
+        t1b[1] += q.imag() * w[1];
+        t1b[2] += q.imag() * w[2];
+        t3 += (q.real() + q.imag()) * w[3];
+      }
+      tu1[0] += t1a[0] * u0; tu1[1] += t1a[1] * u0; tu1[2] += t1a[0] * u1;
+      tu1[3] += t1a[2] * u0; tu1[4] += t1a[1] * u1; tu1[5] += t1a[0] * u2;
+      tu2[0] += t1b[0] * u0; tu2[1] += t1b[1] * u0; tu2[2] += t1b[0] * u1;
+      tu2[3] += t1b[2] * u0; tu2[4] += t1b[1] * u1; tu2[5] += t1b[0] * u2;
+      double t0 = t1a[0] + t1b[0], t1 = t1a[1] + t1b[1], t2 = t1a[2] + t1b[2];
+      tu[0] += t0 * u0; tu[1] += t1 * u0; tu[2] += t0 * u1; tu[3] += t2 * u0; tu[4] += t1 * u1;
+      tu[5] += t0 * u2; tu[6] += t3 * u0; tu[7] += t2 * u1; tu[8] += t1 * u2; tu[9] += t0 * u3;
+    }
+    // (_1): 100,010,001,200,020,002,110,101,011
+    T1[1] += tu1[1] * v0; T1[2] += tu1[2] * v0; T1[3] += tu1[0] * v1; T1[4] += tu1[3] * v0;
+    T1[5] += tu1[5] * v0; T1[6] += tu1[0] * v2; T1[7] += tu1[4] * v0; T1[8] += tu1[1] * v1;
+    T1[9] += tu1[2] * v1;
+    T2[1] += tu2[1] * v0; T2[2] += tu2[2] * v0; T2[3] += tu2[0] * v1; T2[4] += tu2[3] * v0;
+    T2[5] += tu2[5] * v0; T2[6] += tu2[0] * v2; T2[7] += tu2[4] * v0; T2[8] += tu2[1] * v1;
+    T2[9] += tu2[2] * v1;
+    // sum: 000,100,010,001,200,020,002,110,101,011,300,030,003,210,201,120,021,102,012,111
+    S[0] += tu[0] * v0; S[1] += tu[1] * v0; S[2] += tu[2] * v0; S[3] += tu[0] * v1;
+    S[4] += tu[3] * v0; S[5] += tu[5] * v0; S[6] += tu[0] * v2; S[7] += tu[4] * v0;
+    S[8] += tu[1] * v1; S[9] += tu[2] * v1; S[10] += tu[6] * v0; S[11] += tu[9] * v0;
+    S[12] += tu[0] * v3; S[13] += tu[7] * v0; S[14] += tu[3] * v1; S[15] += tu[8] * v0;
+    S[16] += tu[5] * v1; S[17] += tu[1] * v2; S[18] += tu[2] * v2; S[19] += tu[4] * v1;
+  }
+}
+
+}  // namespace
+
 extern "C" {
+
+int or_grid_uind_sites(OrCtx* c, int nsites, const int* isite, const double* fuind, const double* fuinp,
+                       double* grid) {
+  const OrSystem& s = c->s;
+  const int bs = c->bsorder;
+  if (!c->have_bspline) bspline_fill(c);
+  cd* g = reinterpret_cast<cd*>(grid);
+  // grid_uind_site (pmestuff.f:280-405), one rank: every stencil point is local
+  for (int q = 0; q < nsites; ++q) {
+    const int i = isite[q];
+    if (i < 0 || i >= s.n) return 1;
+    const double* fd = fuind + 3 * (size_t)q;
+    const double* fp = fuinp + 3 * (size_t)q;
+    const double* t1 = &c->theta1[(size_t)i * bs * 4];
+    const double* t2 = &c->theta2[(size_t)i * bs * 4];
+    const double* t3 = &c->theta3[(size_t)i * bs * 4];
+    const int* ig = &c->igrid[i * 3];
+    for (int it3 = 0; it3 < bs; ++it3) {
+      int k = stencil_index(c, ig[2], it3, s.nfft3);
+      double v0 = t3[it3 * 4], v1 = t3[it3 * 4 + 1];
+      for (int it2 = 0; it2 < bs; ++it2) {
+        int j = stencil_index(c, ig[1], it2, s.nfft2);
+        double u0 = t2[it2 * 4], u1 = t2[it2 * 4 + 1];
+        double term01 = fd[1] * u1 * v0 + fd[2] * u0 * v1;
+        double term11 = fd[0] * u0 * v0;
+        double term02 = fp[1] * u1 * v0 + fp[2] * u0 * v1;
+        double term12 = fp[0] * u0 * v0;
+        for (int it1 = 0; it1 < bs; ++it1) {
+          int ii = stencil_index(c, ig[0], it1, s.nfft1);
+          double tt0 = t1[it1 * 4], tt1 = t1[it1 * 4 + 1];
+          g[((size_t)k * s.nfft2 + j) * s.nfft1 + ii] += cd(term01 * tt0 + term11 * tt1, term02 * tt0 + term12 * tt1);
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+int or_fphi_uind_sites(OrCtx* c, int nsites, const int* isite, const double* grid, double* phi1, double* phi2,
+                       double* sum) {
+  if (!c->have_bspline) bspline_fill(c);
+  const cd* g = reinterpret_cast<const cd*>(grid);
+  for (int q = 0; q < nsites; ++q) {
+    if (isite[q] < 0 || isite[q] >= c->s.n) return 1;
+    fphi_dip_site(c, isite[q], g, phi1 + 10 * (size_t)q, phi2 + 10 * (size_t)q, sum + 20 * (size_t)q);
+  }
+  return 0;
+}
 
 int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxis, const int* xaxis,
                const int* axt, double* dep, double* ep_out) {
@@ -1547,57 +1662,8 @@ int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxi
     double erec = 0.0;
     std::vector<double> fphid(10), fphip(10), fsum(20), fper(20);
     for (int i = 0; i < n; ++i) {
-      // fphi_uind_site (pmestuff.f:746-1045), all components
-      const double* th1 = &c->theta1[(size_t)i * bs * 4];
-      const double* th2 = &c->theta2[(size_t)i * bs * 4];
-      const double* th3 = &c->theta3[(size_t)i * bs * 4];
-      const int* ig = &c->igrid[i * 3];
-      double T1[10] = {0}, T2[10] = {0}, S[20] = {0};
-      // T1/T2 index: 1..9 = 100,010,001,200,020,002,110,101,011 (fdip_phi(2:10))
-      for (int it3 = 1; it3 <= bs; ++it3) {
-        int k = gather_index(ig[2], it3, s.nfft3);
-        double v0 = th3[(it3 - 1) * 4], v1 = th3[(it3 - 1) * 4 + 1], v2 = th3[(it3 - 1) * 4 + 2],
-               v3 = th3[(it3 - 1) * 4 + 3];
-        double tu1[6] = {0}, tu2[6] = {0}, tu[10] = {0};  // 00,10,01,20,11,02 ; sum: +30,21,12,03
-        for (int it2 = 1; it2 <= bs; ++it2) {
-          int j = gather_index(ig[1], it2, s.nfft2);
-          double u0 = th2[(it2 - 1) * 4], u1 = th2[(it2 - 1) * 4 + 1], u2 = th2[(it2 - 1) * 4 + 2],
-                 u3 = th2[(it2 - 1) * 4 + 3];
-          double t1a[3] = {0}, t1b[3] = {0}, t3 = 0.0;
-          for (int it1 = 1; it1 <= bs; ++it1) {
-            int ii = gather_index(ig[0], it1, s.nfft1);
-            cd g = c->grid[((size_t)k * s.nfft2 + j) * s.nfft1 + ii];
-            const double* w = &th1[(it1 - 1) * 4];
-            t1a[0] += g.real() * w[0];
-            t1a[1] += g.real() * w[1];
-            t1a[2] += g.real() * w[2];
-            t1b[0] += g.imag() * w[0];
-            t1b[1] += g.imag() * w[1];
-            t1b[2] += g.imag() * w[2];
-            t3 += (g.real() + g.imag()) * w[3];
-          }
-          tu1[0] += t1a[0] * u0; tu1[1] += t1a[1] * u0; tu1[2] += t1a[0] * u1;
-          tu1[3] += t1a[2] * u0; tu1[4] += t1a[1] * u1; tu1[5] += t1a[0] * u2;
-          tu2[0] += t1b[0] * u0; tu2[1] += t1b[1] * u0; tu2[2] += t1b[0] * u1;
-          tu2[3] += t1b[2] * u0; tu2[4] += t1b[1] * u1; tu2[5] += t1b[0] * u2;
-          double t0 = t1a[0] + t1b[0], t1 = t1a[1] + t1b[1], t2 = t1a[2] + t1b[2];
-          tu[0] += t0 * u0; tu[1] += t1 * u0; tu[2] += t0 * u1; tu[3] += t2 * u0; tu[4] += t1 * u1;
-          tu[5] += t0 * u2; tu[6] += t3 * u0; tu[7] += t2 * u1; tu[8] += t1 * u2; tu[9] += t0 * u3;
-        }
-        // (_1): 100,010,001,200,020,002,110,101,011
-        T1[1] += tu1[1] * v0; T1[2] += tu1[2] * v0; T1[3] += tu1[0] * v1; T1[4] += tu1[3] * v0;
-        T1[5] += tu1[5] * v0; T1[6] += tu1[0] * v2; T1[7] += tu1[4] * v0; T1[8] += tu1[1] * v1;
-        T1[9] += tu1[2] * v1;
-        T2[1] += tu2[1] * v0; T2[2] += tu2[2] * v0; T2[3] += tu2[0] * v1; T2[4] += tu2[3] * v0;
-        T2[5] += tu2[5] * v0; T2[6] += tu2[0] * v2; T2[7] += tu2[4] * v0; T2[8] += tu2[1] * v1;
-        T2[9] += tu2[2] * v1;
-        // sum: 000,100,010,001,200,020,002,110,101,011,300,030,003,210,201,120,021,102,012,111
-        S[0] += tu[0] * v0; S[1] += tu[1] * v0; S[2] += tu[2] * v0; S[3] += tu[0] * v1;
-        S[4] += tu[3] * v0; S[5] += tu[5] * v0; S[6] += tu[0] * v2; S[7] += tu[4] * v0;
-        S[8] += tu[1] * v1; S[9] += tu[2] * v1; S[10] += tu[6] * v0; S[11] += tu[9] * v0;
-        S[12] += tu[0] * v3; S[13] += tu[7] * v0; S[14] += tu[3] * v1; S[15] += tu[8] * v0;
-        S[16] += tu[5] * v1; S[17] += tu[1] * v2; S[18] += tu[2] * v2; S[19] += tu[4] * v1;
-      }
+      double T1[10], T2[10], S[20];
+      fphi_dip_site(c, i, c->grid.data(), T1, T2, S);
       // 1-based arrays as in the reference: fphid(2:10), fphidprec(1:20), fphirec(1:20)
       double FD[11], FP[11], FS[21], FR[21];
       for (int q = 1; q <= 9; ++q) {

@@ -96,6 +96,16 @@ double or_epolar(OrCtx* c, const double* uind, double* ereal, double* erecip, do
 int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxis, const int* xaxis,
                const int* axt, double* dep, double* ep);
 
+/* grid_uind_site (pmestuff.f:280-405) for nsites sites (0-based atom
+ * numbers): adds the fractional dipoles fuind/fuinp (3 per site) into the
+ * interleaved complex grid [n3][n2][n1] (qgrid2in_2d(2,n1,n2,n3)). */
+int or_grid_uind_sites(OrCtx* c, int nsites, const int* isite, const double* fuind, const double* fuinp,
+                       double* grid);
+/* fphi_uind_site (pmestuff.f:746-1045) for nsites sites on a caller grid:
+ * phi1/phi2 [nsites][10] (fdip_phi1/2, slot 0 unused), sum [nsites][20]. */
+int or_fphi_uind_sites(OrCtx* c, int nsites, const int* isite, const double* grid, double* phi1, double* phi2,
+                       double* sum);
+
 /* rotpole for the water frames used here (Bisector and Z-then-X),
  * pole [n][13] local frame -> rpole [n][13] global frame.
  * axt: 1 = Z-then-X, 2 = Bisector. zaxis/xaxis 0-based. */

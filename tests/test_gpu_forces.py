@@ -53,7 +53,7 @@ def test_gradient_mixed_error_vs_fp64(lib, case):
     ws, orc = case
     ref = orc.solve()
     _, dep_ref = orc.epolar1(ref["uind"], ref["uinp"])
-    ctx = lib.Context(ws, precision=lib.MIXED, poleps=2e-6)
+    ctx = lib.Context(ws, precision=lib.MIXED, poleps=1e-6)
     assert ctx.solve()["converged"]
     _, dep = ctx.gradient()
     err = np.sqrt(np.mean(np.sum((dep - dep_ref) ** 2, axis=1)))

@@ -231,3 +231,18 @@ def test_epolar1_gradient_matches_finite_differences(box216):
                 e.append(_energy(box216.with_positions(p))[0])
             fd = (e[0] - e[1]) / (2 * h)
             assert abs(fd - dep[atom, d]) < 1e-5 * np.abs(dep).max() + 1e-6, (atom, d, fd, dep[atom, d])
+
+
+def test_energy_independent_of_ewald_alpha(thp):
+    # Epol is a physical quantity: at a converged real-space cutoff (9 A) and
+    # grid (0.45 A spacing) the Ewald split alpha must not change it.  The
+    # measured spread over alpha in {0.45, 0.5446, 0.65} is 1.1e-6 relative.
+    es = []
+    for a in (0.45, 0.5446, 0.65):
+        ws = thp.water.make_water_box(216, cfg=0, edge=22.0, ewaldcut=9.0, grid_spacing=0.45, aewald=a)
+        orc = O.Oracle(ws, poleps=1e-10)
+        assert orc.mlistcell(maxelst=4000)[0] == 0
+        res = orc.solve()
+        es.append(orc.epolar(res["uind"])[0])
+    es = np.array(es)
+    assert (es.max() - es.min()) < 3e-6 * abs(es.mean()), es

@@ -75,11 +75,11 @@ def test_server_rejects_oversize(thp):
 def test_batch_equals_single(thp):
     from tinker_hp_b200 import lib
     systems = thp.water.make_batch(6, seed=4003)
-    ctxs = [lib.Context(ws, precision=lib.MIXED, poleps=2e-6) for ws in systems]
+    ctxs = [lib.Context(ws, precision=lib.MIXED, poleps=1e-6) for ws in systems]
     infos = lib.solve_batch(ctxs)
     for ws, ctx, info in zip(systems, ctxs, infos):
         ub, _ = ctx.dipoles()
-        single = lib.Context(ws, precision=lib.MIXED, poleps=2e-6)
+        single = lib.Context(ws, precision=lib.MIXED, poleps=1e-6)
         r = single.solve()
         us, _ = single.dipoles()
         assert info["converged"] and info["niter"] == r["niter"]
@@ -92,7 +92,7 @@ def test_batch_equals_single(thp):
 def test_served_results_same_alone_and_in_mix(thp):
     from tinker_hp_b200 import serve, lib
     reqs = serve.poisson_stream(16, rate=500.0, nmin=1000, nmax=6000, seed=11)
-    srv = serve.Server(precision=lib.MIXED, poleps=2e-6, workers=4)
+    srv = serve.Server(precision=lib.MIXED, poleps=1e-6, workers=4)
     out = {r.rid: r for r in srv.run(reqs, realtime=True)}
     srv.close()
     for q in reqs:
@@ -106,7 +106,7 @@ def test_served_results_same_alone_and_in_mix(thp):
         assert err < 1e-5, (q.rid, q.repeat, err)
         if not q.repeat:
             # the same request alone on an idle GPU: same solver path
-            alone = lib.Context(q.ws, precision=lib.MIXED, poleps=2e-6)
+            alone = lib.Context(q.ws, precision=lib.MIXED, poleps=1e-6)
             alone.solve()
             ua, _ = alone.dipoles()
             assert np.sqrt(np.mean(np.sum((r.uind - ua) ** 2, 1))) * DEBYE < 1e-7

@@ -227,7 +227,7 @@ void free_ctx(Ctx& c) {
                   c.d_thole, c.d_pol, c.d_rpole, c.d_sp_off, c.d_sp_k, c.d_sp_s, c.d_pos_built, c.d_nnb, c.d_nb,
                   c.d_npr, c.d_pk, c.d_pc3, c.d_pc5, c.d_ef, c.d_mu, c.d_res, c.d_h, c.d_pp, c.d_zr, c.d_dip,
                   c.d_cphi, c.d_vecf, c.d_tmp6, c.d_tmp6b, c.d_partials, c.d_cg, c.d_flags,
-                  c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad};
+                  c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad, c.d_sgrid, c.d_sscratch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   pme_free(c);
@@ -954,6 +954,12 @@ int thp_bind_state(thp_ctx* h, double* x, double* y, double* z, double* rpole, d
 
 int thp_last_error(void) { return g_last_error; }
 
+int thp_bind_grid(thp_ctx* h, double* qgrid) {
+  if (!h) return THP_E_INVALID;
+  h->c.bqgrid = qgrid;
+  return THP_OK;
+}
+
 int thp_bind_gradient(thp_ctx* h, double* dep) {
   if (!h) return THP_E_INVALID;
   h->c.bdep = dep;
@@ -1039,6 +1045,110 @@ void epolar1_(void) {
     if (st2) st = st2;
   }
   g_last_error = st;
+}
+
+// Staging for the per-site PME routines: the FP64 grid, the 0-based site
+// numbers (validated) and `doubles` values per site, on the device.
+static int site_staging(thp_ctx* h, int nsites, const int* isite, int doubles, int** d_site, double** d_vals) {
+  Ctx& c = h->c;
+  if (nsites < 0 || (nsites > 0 && !isite)) return THP_E_INVALID;
+  if (!c.have_pos) return THP_E_STATE;
+  std::vector<int> s0(std::max(nsites, 1));
+  for (int q = 0; q < nsites; ++q) {
+    if (isite[q] < 1 || isite[q] > c.n) return THP_E_INVALID;
+    s0[q] = isite[q] - 1;  // Fortran atom numbers are 1-based
+  }
+  if (!c.d_sgrid) {
+    int st = cuda_status(cudaMalloc((void**)&c.d_sgrid, sizeof(cufftDoubleComplex) * c.ngrid), &c, "site grid");
+    if (st) return st;
+  }
+  const size_t need = ((size_t)nsites * 4 + 255) / 256 * 256 + sizeof(double) * doubles * (size_t)std::max(nsites, 1);
+  if (c.sscratch_bytes < need) {
+    cudaFree(c.d_sscratch);
+    c.d_sscratch = nullptr;
+    c.sscratch_bytes = 0;
+    int st = cuda_status(cudaMalloc(&c.d_sscratch, need), &c, "site scratch");
+    if (st) return st;
+    c.sscratch_bytes = need;
+  }
+  *d_site = static_cast<int*>(c.d_sscratch);
+  *d_vals = reinterpret_cast<double*>(static_cast<char*>(c.d_sscratch) + ((size_t)nsites * 4 + 255) / 256 * 256);
+  cudaMemcpyAsync(*d_site, s0.data(), sizeof(int) * nsites, cudaMemcpyHostToDevice, c.stream);
+  return cuda_status(cudaStreamSynchronize(c.stream), &c, "site upload");
+}
+
+void grid_uind_sites_(const int* nsites, const int* isite, const double* fuind, const double* fuinp, double* qgrid) {
+  thp_ctx* h = g_current;
+  if (!h || !nsites || !qgrid || (*nsites > 0 && (!fuind || !fuinp))) {
+    g_last_error = h ? THP_E_INVALID : THP_E_STATE;
+    return;
+  }
+  Ctx& c = h->c;
+  const int ns = *nsites;
+  int st = c.bx ? thp_set_positions(h, c.bx, c.by, c.bz) : THP_OK;
+  int* d_site = nullptr;
+  double* d_fu = nullptr;
+  if (!st) st = site_staging(h, ns, isite, 6, &d_site, &d_fu);
+  if (!st) {
+    cudaMemcpyAsync(d_fu, fuind, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, c.stream);
+    cudaMemcpyAsync(d_fu + 3 * (size_t)ns, fuinp, sizeof(double) * 3 * ns, cudaMemcpyHostToDevice, c.stream);
+    cudaMemsetAsync(c.d_sgrid, 0, sizeof(cufftDoubleComplex) * c.ngrid, c.stream);
+    st = launch_grid_uind_sites(c, ns, d_site, d_fu, d_fu + 3 * (size_t)ns, c.d_sgrid);
+  }
+  if (!st) {
+    c.h_sgrid.resize(2 * c.ngrid);
+    cudaMemcpyAsync(c.h_sgrid.data(), c.d_sgrid, sizeof(cufftDoubleComplex) * c.ngrid, cudaMemcpyDeviceToHost,
+                    c.stream);
+    st = cuda_status(cudaStreamSynchronize(c.stream), &c, "grid_uind_sites");
+  }
+  if (!st)  // grid_uind_site adds into qgrid2loc
+    for (size_t q = 0; q < 2 * c.ngrid; ++q) qgrid[q] += c.h_sgrid[q];
+  g_last_error = st;
+}
+
+void fphi_uind_sites_(const int* nsites, const int* isite, const double* qgrid, double* fdip_phi1, double* fdip_phi2,
+                      double* fdip_sum_phi) {
+  thp_ctx* h = g_current;
+  if (!h || !nsites || !qgrid || (*nsites > 0 && (!fdip_phi1 || !fdip_phi2 || !fdip_sum_phi))) {
+    g_last_error = h ? THP_E_INVALID : THP_E_STATE;
+    return;
+  }
+  Ctx& c = h->c;
+  const int ns = *nsites;
+  int st = c.bx ? thp_set_positions(h, c.bx, c.by, c.bz) : THP_OK;
+  int* d_site = nullptr;
+  double* d_out = nullptr;
+  if (!st) st = site_staging(h, ns, isite, 40, &d_site, &d_out);
+  if (!st) {
+    cudaMemcpyAsync(c.d_sgrid, qgrid, sizeof(cufftDoubleComplex) * c.ngrid, cudaMemcpyHostToDevice, c.stream);
+    st = launch_fphi_uind_sites(c, ns, d_site, c.d_sgrid, d_out, d_out + 10 * (size_t)ns, d_out + 20 * (size_t)ns);
+  }
+  if (!st) {
+    cudaMemcpyAsync(fdip_phi1, d_out, sizeof(double) * 10 * ns, cudaMemcpyDeviceToHost, c.stream);
+    cudaMemcpyAsync(fdip_phi2, d_out + 10 * (size_t)ns, sizeof(double) * 10 * ns, cudaMemcpyDeviceToHost, c.stream);
+    cudaMemcpyAsync(fdip_sum_phi, d_out + 20 * (size_t)ns, sizeof(double) * 20 * ns, cudaMemcpyDeviceToHost,
+                    c.stream);
+    st = cuda_status(cudaStreamSynchronize(c.stream), &c, "fphi_uind_sites");
+  }
+  g_last_error = st;
+}
+
+void grid_uind_site_(const int* isite, const int* impi, const double* fuind, const double* fuinp,
+                     double* qgrid2loc) {
+  (void)impi;
+  const int one = 1;
+  grid_uind_sites_(&one, isite, fuind, fuinp, qgrid2loc);
+}
+
+void fphi_uind_site_(const int* isite, const int* impi, double* fdip_phi1, double* fdip_phi2,
+                     double* fdip_sum_phi) {
+  (void)impi;
+  const int one = 1;
+  if (!g_current || !g_current->c.bqgrid) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  fphi_uind_sites_(&one, isite, g_current->c.bqgrid, fdip_phi1, fdip_phi2, fdip_sum_phi);
 }
 
 void tmatxb_pme_(const int* nrhs, const int* dodiag, const double* mu, double* efi) {

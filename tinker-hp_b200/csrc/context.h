@@ -141,12 +141,19 @@ struct Ctx {
   int* d_frs = nullptr;           // [n][3] frame atoms (sorted indices), axis type
   double* d_grad = nullptr;       // [n][3] gradient, original order
 
+  // batched per-site PME routines on a caller grid (allocated on first use)
+  cufftDoubleComplex* d_sgrid = nullptr;  // FP64 copy of qgrid2in_2d
+  void* d_sscratch = nullptr;             // site numbers and per-site values
+  size_t sscratch_bytes = 0;
+  std::vector<double> h_sgrid;            // host staging of the grid
+
   // Fortran binding
   double *bx = nullptr, *by = nullptr, *bz = nullptr, *brpole = nullptr;
   double *buind = nullptr, *buinp = nullptr, *bep = nullptr;
   int *bnelst = nullptr, *belst = nullptr;
   int bmaxelst = 0;
   double* bdep = nullptr;
+  double* bqgrid = nullptr;  // pme::qgrid2in_2d(2,n1,n2,n3), read by fphi_uind_site_
 
   // CUDA graph of one CG chunk (captured on first use)
   cudaGraphExec_t chunk_exec = nullptr;

@@ -32,6 +32,12 @@ int launch_gather_dip(Ctx& c, double* d_out, bool check_stop);
 // forces.cu
 int launch_forces(Ctx& c, double* d_out);  // dE/dx [n][3], original order, for the dipoles in d_mu
 
+// sites.cu
+int launch_grid_uind_sites(Ctx& c, int nsites, const int* d_site, const double* d_fuind, const double* d_fuinp,
+                           cufftDoubleComplex* d_sgrid);
+int launch_fphi_uind_sites(Ctx& c, int nsites, const int* d_site, const cufftDoubleComplex* d_sgrid, double* d_phi1,
+                           double* d_phi2, double* d_sum);
+
 // md.cu
 int launch_kick(Ctx& c, double half_dt, const double* d_mass, const double* d_grad, double* d_vel);
 int launch_drift(Ctx& c, double dt, const double* d_vel);          // advances d_xyz_orig

@@ -100,6 +100,11 @@ def load():
         "thp_bind_state": ([vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_int, _dp], C.c_int),
         "thp_last_error": ([], C.c_int),
         "thp_bind_gradient": ([vp, _dp], C.c_int),
+        "thp_bind_grid": ([vp, _dp], C.c_int),
+        "grid_uind_sites_": ([_ip, _ip, _dp, _dp, _dp], None),
+        "fphi_uind_sites_": ([_ip, _ip, _dp, _dp, _dp, _dp], None),
+        "grid_uind_site_": ([_ip, _ip, _dp, _dp, _dp], None),
+        "fphi_uind_site_": ([_ip, _ip, _dp, _dp, _dp], None),
         "thp_epolar_noalloc": ([C.c_int, vp, vp, vp, vp], C.c_int),
         "newinduce_pme2_": ([], None),
         "tmatxb_pme_": ([_ip, _ip, _dp, _dp], None),

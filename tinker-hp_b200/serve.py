@@ -80,7 +80,7 @@ def poisson_stream(count, rate=200.0, nmin=1000, nmax=60000, repeat_frac=0.3, pe
 class Server:
     """Admission, residency and worker pool (see module docstring)."""
 
-    def __init__(self, precision=L.MIXED, poleps=2e-6, budget_bytes=120 << 30, workers=8, device=0,
+    def __init__(self, precision=L.MIXED, poleps=1e-6, budget_bytes=120 << 30, workers=8, device=0,
                  context_factory=None, footprint_fn=None):
         self.precision = precision
         self.poleps = poleps
