@@ -1,13 +1,15 @@
 ! thp_shim.f90 -- ISO_C_BINDING layer between Tinker-HP (v1.2 module state)
 ! and libthp.so.  Replaces the calls newinduce_pme2 (epolar.f:108,
-! epolar1.f:145) and mlistcell (nblist.f:109) by thp_newinduce_pme2 and
-! thp_mlistcell.  Not compiled in this repository's image (no Fortran
+! epolar1.f:145), mlistcell (nblist.f:109) and epolar1 (gradient.f:165) by
+! thp_newinduce_pme2, thp_mlistcell and thp_epolar1, and offers the batched
+! per-site PME routines.  Not compiled in this repository's image (no Fortran
 ! compiler); it follows the C declarations of include/thp.h.
 module thp_shim
   use iso_c_binding
   implicit none
   private
-  public :: thp_init, thp_newinduce_pme2, thp_mlistcell, thp_epolar, thp_finalize
+  public :: thp_init, thp_newinduce_pme2, thp_mlistcell, thp_epolar, thp_epolar1, thp_finalize
+  public :: thp_grid_uind_sites, thp_fphi_uind_sites
 
   type, bind(C) :: thp_config
     integer(c_int) :: n
@@ -52,6 +54,28 @@ module thp_shim
     end subroutine
     subroutine c_epolar() bind(C, name="epolar_")
     end subroutine
+    subroutine c_epolar1() bind(C, name="epolar1_")
+    end subroutine
+    integer(c_int) function c_set_frames(h, pole, zax, xax, axt) bind(C, name="thp_set_frames")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, pole, zax, xax, axt
+    end function
+    integer(c_int) function c_bind_gradient(h, dep) bind(C, name="thp_bind_gradient")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, dep
+    end function
+    subroutine c_grid_uind_sites(ns, isite, fuind, fuinp, qgrid) bind(C, name="grid_uind_sites_")
+      import :: c_int, c_double
+      integer(c_int), intent(in) :: ns, isite(*)
+      real(c_double), intent(in) :: fuind(3,*), fuinp(3,*)
+      real(c_double), intent(inout) :: qgrid(*)
+    end subroutine
+    subroutine c_fphi_uind_sites(ns, isite, qgrid, phi1, phi2, sphi) bind(C, name="fphi_uind_sites_")
+      import :: c_int, c_double
+      integer(c_int), intent(in) :: ns, isite(*)
+      real(c_double), intent(in) :: qgrid(*)
+      real(c_double), intent(out) :: phi1(10,*), phi2(10,*), sphi(20,*)
+    end subroutine
     integer(c_int) function c_last_error() bind(C, name="thp_last_error")
       import :: c_int
     end function
@@ -95,6 +119,26 @@ contains
     scales = [p2scale, p3scale, p4scale, p5scale, p2iscale, p3iscale, p4iscale, p5iscale, &
               d1scale, d2scale, d3scale, d4scale, u1scale, u2scale, u3scale, u4scale]
     st = c_set_connectivity(ctx, c_loc(offp), c_loc(idxp), c_loc(scales))
+    if (st /= 0) call fatal
+    call set_frames()
+  end subroutine
+
+  ! frame atoms for the torques (and rotpole on the device): mpole::pole,
+  ! zaxis, xaxis, polaxe ('Z-then-X' -> 1, 'Bisector' -> 2), 0-based atoms
+  subroutine set_frames()
+    use atoms, only: n
+    use mpole, only: pole, zaxis, xaxis, polaxe
+    real(c_double), allocatable, target :: pl(:,:)
+    integer(c_int), allocatable, target :: zx(:), xx(:), ax(:)
+    integer :: i, st
+    allocate(pl(13,n), zx(n), xx(n), ax(n))
+    do i = 1, n  ! every atom carries a multipole in the water workloads
+      pl(:,i) = pole(:,i)
+      zx(i) = zaxis(i) - 1
+      xx(i) = xaxis(i) - 1
+      ax(i) = merge(2, 1, polaxe(i) == 'Bisector')
+    end do
+    st = c_set_frames(ctx, c_loc(pl), c_loc(zx), c_loc(xx), c_loc(ax))
     if (st /= 0) call fatal
   end subroutine
 
@@ -179,6 +223,41 @@ contains
     call bind_all()
     call c_epolar()
     if (c_last_error() /= 0 .and. c_last_error() /= 3) call fatal
+  end subroutine
+
+  ! epolar1 (gradient.f:165): energy into ep, gradient into deriv::dep
+  subroutine thp_epolar1
+    use deriv, only: dep
+    integer :: st
+    call bind_all()
+    st = c_bind_gradient(ctx, c_loc(dep))
+    if (st /= 0) call fatal
+    call c_epolar1()
+    if (c_last_error() /= 0 .and. c_last_error() /= 3) call fatal
+  end subroutine
+
+  ! grid_uind_site over a whole site list (pmestuff.f:280), one rank
+  subroutine thp_grid_uind_sites(ns, isite, fuind, fuinp, qgrid)
+    integer, intent(in) :: ns, isite(ns)
+    real*8, intent(in) :: fuind(3,ns), fuinp(3,ns)
+    real*8, intent(inout) :: qgrid(*)
+    integer(c_int), allocatable :: s(:)
+    call bind_all()
+    s = int(isite, c_int)
+    call c_grid_uind_sites(int(ns, c_int), s, fuind, fuinp, qgrid)
+    if (c_last_error() /= 0) call fatal
+  end subroutine
+
+  ! fphi_uind_site over a whole site list (pmestuff.f:746), one rank
+  subroutine thp_fphi_uind_sites(ns, isite, qgrid, phi1, phi2, sphi)
+    integer, intent(in) :: ns, isite(ns)
+    real*8, intent(in) :: qgrid(*)
+    real*8, intent(out) :: phi1(10,ns), phi2(10,ns), sphi(20,ns)
+    integer(c_int), allocatable :: s(:)
+    call bind_all()
+    s = int(isite, c_int)
+    call c_fphi_uind_sites(int(ns, c_int), s, qgrid, phi1, phi2, sphi)
+    if (c_last_error() /= 0) call fatal
   end subroutine
 
   subroutine thp_finalize
