@@ -373,16 +373,22 @@ def main():
     d2h = n * 6 * 8
 
     peaks, peak_kind = measured_peaks()
-    # roofline of the fused CG matvec: algorithmic bytes per launch (FP64 figures halved for per-atom and
-    # grid data in the mixed form): 68 N (x, pol, mu in, field out) + 4 L (list) + 8 K^3 (grid read once)
+    # roofline of the mixed CG matvec (real-space row + CG combine; the PME gather is its own
+    # kernel): algorithmic bytes per launch, the FP64 a3 figure 136 N + 4 L with per-atom data
+    # halved in the mixed form: 68 N (positions, polarity, mu in, field out) + 4 L (half list,
+    # 88.4 entries per atom at 7.5 A)
     L_entries = 88.4 * n
-    K3 = ws.nfft[0] * ws.nfft[1] * ws.nfft[2]
-    alg_bytes = 68.0 * n + 4.0 * L_entries + 8.0 * K3
+    alg_bytes = 68.0 * n + 4.0 * L_entries
     avg_ms = mv_ms / max(mv_launches, 1)
     achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
-    roof = {"bound": "hbm", "kernel": "k_cg_matvec<mixed> (PME gather + real-space row + CG combine)",
+    # DRAM bytes per launch (read + write) from one ncu capture of this kernel on the 96,000-atom
+    # box (196.9 MB per launch), scaled by the atom count: the traffic is the streamed FP32 pair
+    # coefficients (12 B per directed pair) plus per-atom data, both proportional to n
+    traffic = 196.9e6 * n / 96000.0
+    roof = {"bound": "hbm", "kernel": "k_cg_matvec<mixed> (real-space row + CG combine)",
             "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-            "frac": achieved / peaks.get("hbm_gbs"), "peak_kind": peak_kind, "traffic": None,
+            "frac": achieved / peaks.get("hbm_gbs"), "peak_kind": peak_kind, "traffic": traffic,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, 96k-atom capture scaled by n",
             "avg_launch_ms": avg_ms, "launches": mv_launches, "alg_bytes_per_launch": alg_bytes}
 
     cpu = None
