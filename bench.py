@@ -373,8 +373,8 @@ def main():
     d2h = n * 6 * 8
 
     peaks, peak_kind = measured_peaks()
-    # roofline of the mixed CG matvec (real-space row + CG combine; the PME gather is its own
-    # kernel): algorithmic bytes per launch, the FP64 a3 figure 136 N + 4 L with per-atom data
+    # roofline of the real-space row of the mixed CG matvec (the PME branch runs beside it on
+    # another stream; the combine is its own kernel): algorithmic bytes per launch, the FP64 a3 figure 136 N + 4 L with per-atom data
     # halved in the mixed form: 68 N (positions, polarity, mu in, field out) + 4 L (half list,
     # 88.4 entries per atom at 7.5 A)
     L_entries = 88.4 * n
@@ -385,7 +385,7 @@ def main():
     # box (196.9 MB per launch), scaled by the atom count: the traffic is the streamed FP32 pair
     # coefficients (12 B per directed pair) plus per-atom data, both proportional to n
     traffic = 196.9e6 * n / 96000.0
-    roof = {"bound": "hbm", "kernel": "k_cg_matvec<mixed> (real-space row + CG combine)",
+    roof = {"bound": "hbm", "kernel": "k_real_row<mixed> (real-space row of the CG matvec)",
             "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
             "frac": achieved / peaks.get("hbm_gbs"), "peak_kind": peak_kind, "traffic": traffic,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, 96k-atom capture scaled by n",

@@ -108,7 +108,7 @@ int thp_set_guess(thp_ctx* ctx, const double* mu /*[n][2][3]*/);
 int thp_nblist(thp_ctx* ctx);
 /* full rebuild (cell sort + list) on the next list use, as nblist(0) does */
 int thp_invalidate_list(thp_ctx* ctx);
-/* device time of the fused CG matvec kernels since the last reset:
+/* device time of the real-space CG matvec kernels since the last reset:
  * enable != 0 starts recording events around each launch (and resets). */
 int thp_profile(thp_ctx* ctx, int enable, double* ms_total, int* launches);
 /* E0 + PCG + Epol on the device (newinduce_pme2 + epolar0c) */

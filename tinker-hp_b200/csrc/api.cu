@@ -234,6 +234,9 @@ void free_ctx(Ctx& c) {
   if (c.chunk_exec) cudaGraphExecDestroy(c.chunk_exec);
   if (c.h_cg) cudaFreeHost(c.h_cg);
   if (c.h_flags) cudaFreeHost(c.h_flags);
+  if (c.ev_fork) cudaEventDestroy(c.ev_fork);
+  if (c.ev_join) cudaEventDestroy(c.ev_join);
+  if (c.stream2) cudaStreamDestroy(c.stream2);
   if (c.ev0) cudaEventDestroy(c.ev0);
   if (c.ev1) cudaEventDestroy(c.ev1);
   if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
@@ -323,6 +326,9 @@ int thp_ctx_create(const thp_config* cfg, thp_ctx** out) {
   int st = set_current_device(c);
   if (!st) st = cuda_status(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), &c, "stream");
   c.own_stream = true;
+  if (!st) st = cuda_status(cudaStreamCreateWithFlags(&c.stream2, cudaStreamNonBlocking), &c, "stream");
+  if (!st) st = cuda_status(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming), &c, "event");
+  if (!st) st = cuda_status(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming), &c, "event");
   if (!st) st = cuda_status(cudaEventCreate(&c.ev0), &c, "event");
   if (!st) st = cuda_status(cudaEventCreate(&c.ev1), &c, "event");
   const size_t n = c.n, npad = c.npad;

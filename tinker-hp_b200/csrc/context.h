@@ -43,6 +43,10 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // side stream of the CG iteration: the real-space row runs there while the
+  // PME branch runs on `stream` (fork / join events, captured in the graph)
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
   // host copies (original atom order)
   std::vector<double> h_polarity, h_thole, h_pdamp;

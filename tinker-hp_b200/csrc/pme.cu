@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(128) k_spread_dip(int n, PmeGeom g, const doub
                                                    double* __restrict__ vec, const double* __restrict__ zr,
                                                    float* __restrict__ vecf, const CgScalars* __restrict__ cg,
                                                    int mode, typename Cplx<T>::type* __restrict__ grid) {
-  if (mode == 1 && cg->stop) return;
+  if (mode >= 1 && cg->stop) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double v[6];
@@ -462,8 +462,9 @@ int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0) {
 
 int launch_efld0_recip(Ctx& c) { return launch_efld0_recip_ex(c, nullptr, true); }
 
-// Dipole PME pass.  mode 0: spread d_vec as is; mode 1: pp update first (CG
-// loop, honours the stop flag).  d_out (if non-null) receives the gathered
+// Dipole PME pass.  mode 0: spread d_vec as is (the mixed form also writes
+// its FP32 copy); mode 1: pp update first (CG loop, honours the stop flag);
+// mode 2: spread as is, no FP32 copy, honours the stop flag.  d_out (if non-null) receives the gathered
 // field gradient [n][6] (tmatxbrecip's dipfield); the CG loop passes null and
 // gathers inside its fused matvec kernel.
 int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode) {
@@ -471,7 +472,7 @@ int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode) {
   int nb = (c.n + kBlock - 1) / kBlock;
   int st = zero_grid(c);
   if (st) return st;
-  float* vf = c.mixed ? c.d_vecf : nullptr;
+  float* vf = (c.mixed && mode != 2) ? c.d_vecf : nullptr;
   if (c.mixed)
     k_spread_dip<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<double*>(d_vec), c.d_zr, vf,
                                                   c.d_cg, mode, (cufftComplex*)c.d_grid);
@@ -479,7 +480,7 @@ int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode) {
     k_spread_dip<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<double*>(d_vec), c.d_zr, vf,
                                                    c.d_cg, mode, (cufftDoubleComplex*)c.d_grid);
   if ((st = cuda_status(cudaGetLastError(), &c, "spread dip"))) return st;
-  if ((st = convolve(c, mode == 1))) return st;
+  if ((st = convolve(c, mode >= 1))) return st;
   if (d_out) st = launch_gather_dip(c, d_out, false);
   return st;
 }

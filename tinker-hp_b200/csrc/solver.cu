@@ -2,22 +2,32 @@
 //
 // inducepcg_pme2 (newinduce_pme2.f:285-636) with every vector and scalar on
 // the device.  Per iteration:
-//   1. spread kernel: pp = zr + beta*pp, spread pp on the PME grid;
-//   2. cuFFT forward, qfac, cuFFT backward;
-//   3. fused matvec kernel: PME gather + real-space row + diagonal and self
-//      terms -> h; partial pp.h; the last block forms gg and alpha;
-//   5. update kernel: mu += alpha pp, res -= alpha h, zr = diag res; partial
+//   1. pp = zr + beta*pp (and the FP32 copy of the mixed form);
+//   2. fork: the real-space row T_real pp runs on the side stream while the
+//      main stream spreads pp on the PME grid, runs cuFFT forward, qfac,
+//      cuFFT backward and gathers the dipole field;
+//   3. join, then the combine kernel: h = T_real pp + pp/alpha + dipfield -
+//      self term; partial pp.h; the last block forms gg and alpha;
+//   4. update kernel: mu += alpha pp, res -= alpha h, zr = diag res; partial
 //      ggnew and ene; the last block forms beta, the residual norm and the
 //      convergence / stop flags.
 // Reductions write per-block partials summed in a fixed order by the last
-// block, so results are bitwise reproducible run to run.  Once the stop flag
-// is set every later kernel returns at entry, so the host can enqueue
-// iterations ahead and read the flag only once per chunk.
+// block, so the CG scalars do not depend on thread scheduling.  Once the
+// stop flag is set every later kernel returns at entry, so the host can
+// enqueue iterations ahead and read the flag only once per chunk.
 #include <cstring>
 
 #include "kernels.h"
 #include "pme_dev.cuh"
 #include "realspace_dev.cuh"
+
+// Systems of at least THP_OVERLAP_MIN_ATOMS atoms run the real-space row of
+// each CG matvec on a side stream, concurrent with the PME branch.  Smaller
+// systems are launch-bound (and overlap with each other when batched), so
+// they use one fused matvec kernel after the PME branch.
+#ifndef THP_OVERLAP_MIN_ATOMS
+#define THP_OVERLAP_MIN_ATOMS 20000
+#endif
 
 namespace thp {
 
@@ -100,6 +110,106 @@ __global__ void __launch_bounds__(kBlock) k_cg_matvec(PairRows pr, Box box, cons
       tmatxb_row64(pr, box, i, pos, x, acc);
     }
     double dip[6], xi[6];
+    load6(dipf + (size_t)i * 6, dip);
+    load6(x + (size_t)i * 6, xi);
+    const double p = pol[i];
+    const double ip = (p == 0.0) ? 1.0 / kTinyPol : 1.0 / p;
+    double hv[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) hv[q] = ((acc[q] + xi[q] * ip) + dip[q]) - term * xi[q];
+    store6(h + (size_t)i * 6, hv);
+    if (init) {
+      double e6[6], r6[6], z6[6];
+      load6(ef + (size_t)i * 6, e6);
+      const double dg = diag_of(p);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        r6[q] = e6[q] - hv[q];
+        z6[q] = dg * r6[q];
+      }
+      store6(res + (size_t)i * 6, r6);
+      store6(zr + (size_t)i * 6, z6);
+      store6(pp + (size_t)i * 6, z6);
+      red[0] = r6[0] * z6[0] + r6[1] * z6[1] + r6[2] * z6[2];
+      red[1] = r6[3] * z6[3] + r6[4] * z6[4] + r6[5] * z6[5];
+    } else {
+      red[0] = xi[0] * hv[0] + xi[1] * hv[1] + xi[2] * hv[2];
+      red[1] = xi[3] * hv[3] + xi[4] * hv[4] + xi[5] * hv[5];
+    }
+  }
+  double tot[2];
+  if (grid_reduce<2>(red, partials, &cg->counter[0], tot) && threadIdx.x == 0) {
+    if (init) {
+      cg->ggold[0] = tot[0];
+      cg->ggold[1] = tot[1];
+      cg->beta[0] = 0.0;
+      cg->beta[1] = 0.0;
+    } else {
+      cg->gg[0] = tot[0];
+      cg->gg[1] = tot[1];
+      if (tot[0] == 0.0 || tot[1] == 0.0) {
+        cg->stop = 1;  // newinduce_pme2.f:505 returns on gg == 0
+      } else {
+        cg->alpha[0] = cg->ggold[0] / tot[0];
+        cg->alpha[1] = cg->ggold[1] / tot[1];
+      }
+    }
+  }
+}
+
+// pp = zr + beta pp (newinduce_pme2.f:553-559) and, for the mixed form, the
+// FP32 copy the real-space row reads; update 0 only writes the copy of x.
+__global__ void __launch_bounds__(256) k_pp_update(int n, int update, const double* __restrict__ zr,
+                                                  double* __restrict__ x, float* __restrict__ xf,
+                                                  const CgScalars* __restrict__ cg) {
+  if (update && cg->stop) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 6 * n) return;
+  double v = x[t];
+  if (update) {
+    v = zr[t] + cg->beta[(t % 6) < 3 ? 0 : 1] * v;
+    x[t] = v;
+  }
+  if (xf) xf[t] = (float)v;
+}
+
+// real-space part of h only: hreal = T_real x (tmatxb_pme without the diagonal)
+template <bool MIXED>
+__global__ void __launch_bounds__(kBlock) k_real_row(PairRows pr, Box box, const double4* __restrict__ pos,
+                                                     const float4* __restrict__ posf, const double* __restrict__ x,
+                                                     const float* __restrict__ xf, const CgScalars* __restrict__ cg,
+                                                     int check_stop, double* __restrict__ hreal) {
+  if (check_stop && cg->stop) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= pr.n) return;
+  double acc[6];
+  if (MIXED) {
+    float a32[6] = {0, 0, 0, 0, 0, 0};
+    tmatxb_row32(pr, (float)box.l[0], (float)box.l[1], (float)box.l[2], i, posf, xf, a32);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[q] = (double)a32[q];
+  } else {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[q] = 0.0;
+    tmatxb_row64(pr, box, i, pos, x, acc);
+  }
+  store6(hreal + (size_t)i * 6, acc);
+}
+
+// h = hreal + x/alpha + dipfield(x) - term x, then the reductions of
+// k_cg_matvec (init: residual, zr, pp and ggold; iter: gg and alpha)
+__global__ void __launch_bounds__(kBlock) k_cg_combine(int n, const double* __restrict__ dipf,
+                                                       const double* __restrict__ x, const double* __restrict__ pol,
+                                                       const double* __restrict__ ef, double term, int init,
+                                                       double* __restrict__ h, double* __restrict__ res,
+                                                       double* __restrict__ zr, double* __restrict__ pp, CgScalars* cg,
+                                                       double* __restrict__ partials) {
+  if (cg->stop) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double red[2] = {0.0, 0.0};
+  if (i < n) {
+    double acc[6], dip[6], xi[6];
+    load6(h + (size_t)i * 6, acc);
     load6(dipf + (size_t)i * 6, dip);
     load6(x + (size_t)i * 6, xi);
     const double p = pol[i];
@@ -259,19 +369,48 @@ int launch_to_orig6(Ctx& c, const double* d_sorted, double* d_orig, int nrhs) {
   return cuda_status(cudaGetLastError(), &c, "to orig");
 }
 
-static void prof_mark(Ctx& c) {
+static void prof_mark(Ctx& c, cudaStream_t s) {
   if (!c.profiling) return;
   cudaEvent_t e;
   cudaEventCreate(&e);
-  cudaEventRecord(e, c.stream);
+  cudaEventRecord(e, s);
   c.prof_events.push_back(e);
+}
+
+static bool overlapped(const Ctx& c) { return c.n >= THP_OVERLAP_MIN_ATOMS; }
+
+// One application of the CG matrix with the real-space row on the side
+// stream and the PME branch (spread, FFTs, gather) on the main stream; x and,
+// for the mixed form, its FP32 copy are final when this is enqueued.
+static int matvec_overlapped(Ctx& c, double* x, int init) {
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  int st;
+  cudaEventRecord(c.ev_fork, c.stream);
+  cudaStreamWaitEvent(c.stream2, c.ev_fork, 0);
+  PairRows pr = pair_rows(c);
+  prof_mark(c, c.stream2);
+  if (c.mixed)
+    k_real_row<true><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_posf, x, c.d_vecf, c.d_cg, !init, c.d_h);
+  else
+    k_real_row<false><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_posf, x, c.d_vecf, c.d_cg, !init, c.d_h);
+  prof_mark(c, c.stream2);
+  if ((st = cuda_status(cudaGetLastError(), &c, "real row"))) return st;
+  cudaEventRecord(c.ev_join, c.stream2);
+  if ((st = launch_pme_dipole(c, x, nullptr, 2))) return st;
+  if ((st = launch_gather_dip(c, c.d_dip, true))) return st;
+  cudaStreamWaitEvent(c.stream, c.ev_join, 0);
+  const double a = c.cfg.aewald;
+  const double term = (4.0 / 3.0) * a * a * a / kSqrtPi;
+  k_cg_combine<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_dip, x, c.d_pol, c.d_ef, term, init, c.d_h, c.d_res, c.d_zr,
+                                            c.d_pp, c.d_cg, c.d_partials);
+  return cuda_status(cudaGetLastError(), &c, "cg combine");
 }
 
 static int launch_matvec(Ctx& c, const double* x, int init) {
   const int nb = (c.n + kBlock - 1) / kBlock;
   int st = launch_gather_dip(c, c.d_dip, init == 0);
   if (st) return st;
-  prof_mark(c);
+  prof_mark(c, c.stream);
   PairRows pr = pair_rows(c);
   const double a = c.cfg.aewald;
   const double term = (4.0 / 3.0) * a * a * a / kSqrtPi;
@@ -283,14 +422,21 @@ static int launch_matvec(Ctx& c, const double* x, int init) {
     k_cg_matvec<false><<<nb, kBlock, 0, c.stream>>>(pr, c.box, c.d_pos, c.d_posf, c.d_dip, x, c.d_vecf, c.d_pol,
                                                     c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, c.d_cg,
                                                     c.d_partials);
-  prof_mark(c);
+  prof_mark(c, c.stream);
   return cuda_status(cudaGetLastError(), &c, "cg matvec");
 }
 
 static int enqueue_iteration(Ctx& c) {
-  int st = launch_pme_dipole(c, c.d_pp, nullptr, 1);
-  if (st) return st;
-  if ((st = launch_matvec(c, c.d_pp, 0))) return st;
+  int st;
+  if (overlapped(c)) {
+    k_pp_update<<<(6 * c.n + 255) / 256, 256, 0, c.stream>>>(c.n, 1, c.d_zr, c.d_pp, c.mixed ? c.d_vecf : nullptr,
+                                                            c.d_cg);
+    if ((st = cuda_status(cudaGetLastError(), &c, "pp update"))) return st;
+    if ((st = matvec_overlapped(c, c.d_pp, 0))) return st;
+  } else {
+    if ((st = launch_pme_dipole(c, c.d_pp, nullptr, 1))) return st;
+    if ((st = launch_matvec(c, c.d_pp, 0))) return st;
+  }
   const int nb = (c.n + kBlock - 1) / kBlock;
   k_cg_update<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_h, c.d_pp, c.d_mu, c.d_res, c.d_zr, c.d_cg,
                                            c.d_partials, c.cfg.poleps, c.cfg.politer);
@@ -303,6 +449,13 @@ int pcg_begin(Ctx& c, int guess) {
   cudaMemsetAsync(c.d_cg, 0, sizeof(CgScalars), c.stream);
   if (guess == THP_GUESS_DIRECT) {
     k_guess_direct<<<(c.n * 6 + 255) / 256, 256, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_mu);
+  }
+  if (overlapped(c)) {
+    if (c.mixed) {
+      k_pp_update<<<(6 * c.n + 255) / 256, 256, 0, c.stream>>>(c.n, 0, c.d_zr, c.d_mu, c.d_vecf, c.d_cg);
+      if ((st = cuda_status(cudaGetLastError(), &c, "mu copy"))) return st;
+    }
+    return matvec_overlapped(c, c.d_mu, 1);
   }
   if ((st = launch_pme_dipole(c, c.d_mu, nullptr, 0))) return st;
   return launch_matvec(c, c.d_mu, 1);

@@ -251,7 +251,7 @@ class Context:
         self._check(load().thp_invalidate_list(self.h), "thp_invalidate_list")
 
     def profile(self, enable):
-        """Start (enable=1) or stop event recording around the fused CG matvec;
+        """Start (enable=1) or stop event recording around the real-space CG matvec row;
         returns (total ms, launches) recorded since the last call."""
         ms = C.c_double()
         cnt = C.c_int()
