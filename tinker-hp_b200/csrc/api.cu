@@ -232,6 +232,7 @@ void free_ctx(Ctx& c) {
     if (p) cudaFree(p);
   pme_free(c);
   if (c.chunk_exec) cudaGraphExecDestroy(c.chunk_exec);
+  if (c.loop_exec) cudaGraphExecDestroy(c.loop_exec);
   if (c.h_cg) cudaFreeHost(c.h_cg);
   if (c.h_flags) cudaFreeHost(c.h_flags);
   if (c.ev_fork) cudaEventDestroy(c.ev_fork);
@@ -629,6 +630,26 @@ int thp_solve_batch(thp_ctx** hs, int count, int guess, thp_solve_info* infos) {
     st[i] = solve_front_async(h, g);
     h->guess_uploaded = false;
     active[i] = st[i] == THP_OK;
+  }
+  // the whole CG loop of each system as one graph launch where available;
+  // the others take chunk rounds with a host check of the stop flags
+  std::vector<char> looped(count, 0);
+  for (int i = 0; i < count; ++i) {
+    if (!active[i]) continue;
+    Ctx& c = hs[i]->c;
+    set_current_device(c);
+    const int r = pcg_loop_async(c);
+    if (r >= 0) {
+      active[i] = 0;
+      looped[i] = r == 0;
+      if (r > 0) st[i] = r;
+    }
+  }
+  for (int i = 0; i < count; ++i) {
+    if (!looped[i]) continue;
+    Ctx& c = hs[i]->c;
+    set_current_device(c);
+    st[i] = cuda_status(cudaStreamSynchronize(c.stream), &c, "batch sync");
   }
   for (bool any = true; any;) {
     any = false;

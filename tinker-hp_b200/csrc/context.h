@@ -26,6 +26,7 @@ struct CgScalars {
   int niter;
   int status;    // THP_* code raised on the device
   unsigned counter[4];  // last-block counters of the grid reductions
+  int loops;            // bodies run by the device-side CG loop
 };
 
 // CG iterations per host check of the stop flag
@@ -161,6 +162,10 @@ struct Ctx {
 
   // CUDA graph of one CG chunk (captured on first use)
   cudaGraphExec_t chunk_exec = nullptr;
+  // the whole CG loop as one graph (conditional WHILE node); loop_state:
+  // 0 not built yet, 1 built, -1 not available (the chunked graph is used)
+  cudaGraphExec_t loop_exec = nullptr;
+  int loop_state = 0;
 
   // optional event pairs around the fused CG matvec launches
   bool profiling = false;

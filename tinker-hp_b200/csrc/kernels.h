@@ -47,6 +47,7 @@ int launch_ekin(Ctx& c, const double* d_mass, const double* d_vel, double* d_scr
 int run_pcg(Ctx& c, int guess);
 int pcg_begin(Ctx& c, int guess);
 int pcg_chunk_async(Ctx& c);
+int pcg_loop_async(Ctx& c);  // whole CG loop in one graph launch; -1 when unavailable
 int pcg_status(Ctx& c);
 int launch_epol(Ctx& c);
 

@@ -25,6 +25,12 @@
 // each CG matvec on a side stream, concurrent with the PME branch.  Smaller
 // systems are launch-bound (and overlap with each other when batched), so
 // they use one fused matvec kernel after the PME branch.
+// 1: the CG loop runs on the device as one graph with a conditional WHILE
+// node; 0: graph-replayed chunks of kCgChunk iterations with a host check
+#ifndef THP_DEVICE_LOOP
+#define THP_DEVICE_LOOP 1
+#endif
+
 #ifndef THP_OVERLAP_MIN_ATOMS
 #define THP_OVERLAP_MIN_ATOMS 20000
 #endif
@@ -320,6 +326,17 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __res
   }
 }
 
+// Last node of the device-side loop body: keep looping while the CG has not
+// stopped, and never more than max_loops bodies (a hard bound on the loop,
+// whatever the kernels before it did).
+__global__ void k_loop_cond(CgScalars* cg, cudaGraphConditionalHandle handle, int max_loops) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int l = ++cg->loops;
+  unsigned keep = (cg->stop == 0 && l < max_loops) ? 1u : 0u;
+  if (!keep) cg->stop = 1;
+  cudaGraphSetConditional(handle, keep);
+}
+
 __global__ void k_guess_direct(int n, const double* __restrict__ pol, const double* __restrict__ ef,
                                double* __restrict__ mu) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -495,6 +512,55 @@ int pcg_chunk_async(Ctx& c) {
   return cuda_status(cudaGraphLaunch(c.chunk_exec, c.stream), &c, "graph launch");
 }
 
+// Builds the CG loop graph: a conditional WHILE node whose body is one
+// iteration plus k_loop_cond.  Returns false (and leaves the chunked graph
+// in charge) when the runtime refuses any step.
+static bool build_loop_graph(Ctx& c) {
+  cudaGraph_t g = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
+  bool ok = false;
+  cudaGraphConditionalHandle handle;
+  cudaGraphNodeParams p = {};
+  cudaGraphNode_t node;
+  if (cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault) == cudaSuccess) {
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = handle;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    if (cudaGraphAddNode(&node, g, nullptr, 0, &p) == cudaSuccess) {
+      cudaGraph_t body = p.conditional.phGraph_out[0];
+      if (cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+          cudaSuccess) {
+        int st = enqueue_iteration(c);
+        if (!st) k_loop_cond<<<1, 32, 0, c.stream>>>(c.d_cg, handle, c.cfg.politer + 2);
+        cudaGraph_t out = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(c.stream, &out);
+        ok = !st && e == cudaSuccess && cudaGetLastError() == cudaSuccess;
+      }
+    }
+  }
+  if (ok) ok = cudaGraphInstantiate(&c.loop_exec, g, 0) == cudaSuccess;
+  if (!ok) {
+    c.loop_exec = nullptr;
+    cudaGetLastError();  // clear a refused step so later status checks see only their own errors
+  }
+  cudaGraphDestroy(g);
+  return ok;
+}
+
+// Runs the rest of the CG after pcg_begin on the device: one launch of the
+// loop graph and the copy of the CG scalars to pinned host memory; returns
+// without waiting.  -1 when the loop graph is not available.
+int pcg_loop_async(Ctx& c) {
+  if (!THP_DEVICE_LOOP || c.profiling || c.stream == nullptr) return -1;
+  if (c.loop_state == 0) c.loop_state = build_loop_graph(c) ? 1 : -1;
+  if (c.loop_state < 0) return -1;
+  int st = cuda_status(cudaGraphLaunch(c.loop_exec, c.stream), &c, "loop graph launch");
+  if (st) return st;
+  return cuda_status(cudaMemcpyAsync(c.h_cg, c.d_cg, sizeof(CgScalars), cudaMemcpyDeviceToHost, c.stream), &c,
+                     "cg scalars");
+}
+
 int pcg_status(Ctx& c) {
   c.have_dipoles = true;
   if (c.h_cg->status) return c.h_cg->status;
@@ -507,6 +573,12 @@ int pcg_status(Ctx& c) {
 int run_pcg(Ctx& c, int guess) {
   int st = pcg_begin(c, guess);
   if (st) return st;
+  st = pcg_loop_async(c);
+  if (st >= 0) {
+    if (st) return st;
+    if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "cg sync"))) return st;
+    return pcg_status(c);
+  }
   int done = 0;
   while (true) {
     if ((st = pcg_chunk_async(c))) return st;
