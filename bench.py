@@ -222,17 +222,20 @@ def batched_throughput(lib, systems, copies, steps, warmup=2):
 
 def serving_run(lib, thp, count, workers=8):
     """Serving form: seeded Poisson stream (200 req/s, 1k-60k atoms, 30 %
-    repeats perturbed by 0.01 A RMS) through the continuous-batching server
-    with a 120 GB device budget."""
+    repeats perturbed by 0.01 A RMS) through the native request loop with a
+    120 GB device budget."""
     from tinker_hp_b200 import serve
     reqs = serve.poisson_stream(count)
     srv = serve.Server(precision=lib.MIXED, poleps=CG_TOL, budget_bytes=120 << 30, workers=workers)
     srv.run(reqs[: min(8, len(reqs))], realtime=False)  # warm the kernels
     srv.close()
-    srv = serve.Server(precision=lib.MIXED, poleps=CG_TOL, budget_bytes=120 << 30, workers=workers)
+    srv = serve.Server(precision=lib.MIXED, poleps=CG_TOL, budget_bytes=120 << 30, workers=workers, max_resident=16)
     out = srv.run(reqs, realtime=True)
+    stats = srv.stats()
     srv.close()
     summ = serve.summarize(out)
+    summ["contexts"] = {k: stats[k] for k in ("created", "reused", "evicted", "resident", "pooled")}
+    summ["max_resident"] = 16
     summ.update({"requests": len(reqs), "rate_req_per_s": 200.0, "workers": workers,
                  "atoms": "1,000-60,000 log-uniform", "repeats": "30 % (0.01 A RMS perturbation, warm start)"})
     return summ

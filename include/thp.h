@@ -89,6 +89,14 @@ typedef struct thp_ctx thp_ctx;
 /* ---- native API ---------------------------------------------------------- */
 int thp_ctx_create(const thp_config* cfg, thp_ctx** out);
 int thp_ctx_destroy(thp_ctx* ctx);
+/* Re-target a context to another system (same precision and device): every
+ * device buffer that is large enough and the cuFFT plan of an unchanged grid
+ * are kept, so no device memory is freed or allocated unless the new system
+ * is larger.  All system state is cleared (parameters, connectivity,
+ * positions, multipoles, list, dipoles, bindings), as after thp_ctx_create. */
+int thp_ctx_reset(thp_ctx* ctx, const thp_config* cfg);
+/* device bytes the context holds at its current capacity */
+size_t thp_ctx_footprint(thp_ctx* ctx);
 /* use an external CUDA stream (cudaStream_t passed as void*) */
 int thp_set_stream(thp_ctx* ctx, void* stream);
 /* polarity(n) A^3, thole(n), pdamp(n) = polarity^(1/6) (kpolar.f:225-300) */
@@ -163,6 +171,78 @@ int thp_solve_host(thp_ctx* ctx, const double* x, const double* y, const double*
 /* bytes of device memory a context of this configuration needs */
 size_t thp_footprint(const thp_config* cfg);
 const char* thp_status_string(int status);
+
+/* ---- serving: a request loop over resident systems ---------------------- */
+/* A system's topology and parameters (arrays are copied at registration).
+ * cfg gives n, box, aewald, cutoffs, nfft, bsorder and max_neighbors; the
+ * server's precision, poleps, politer and device replace cfg's. */
+typedef struct thp_system {
+  thp_config cfg;
+  const double* polarity;      /* [n] */
+  const double* thole;         /* [n] */
+  const double* pdamp;         /* [n] */
+  const int* const* conn_off;  /* as thp_set_connectivity */
+  const int* const* conn_idx;
+  const double* scales;        /* [16] */
+  const double* pole;          /* [n][13] local frame, as thp_set_frames */
+  const int* zaxis;
+  const int* xaxis;
+  const int* axt;
+} thp_system;
+
+typedef struct thp_server_config {
+  int precision;        /* THP_FP64 or THP_MIXED */
+  double poleps;
+  int politer;
+  int device;
+  size_t budget_bytes;  /* device memory all resident and pooled contexts may hold */
+  int workers;          /* host threads driving the GPU; each system has its own stream */
+  int max_resident;     /* systems kept on the device beyond the one being served (0: the
+                           budget alone decides); past it the least recently used idle
+                           system's context is re-targeted rather than a new one created */
+} thp_server_config;
+
+typedef struct thp_result {
+  int status;
+  int niter;
+  int warm;             /* 1: started from the system's previous dipoles */
+  double epol;
+  double queue_ms;      /* submit -> a worker took the request */
+  double latency_ms;    /* submit -> dipoles in the caller's buffers */
+  double wait_ms;       /* taken -> the system's context was free and in budget */
+  double setup_ms;      /* context created or re-targeted and the system loaded (0 when resident) */
+  double solve_ms;      /* positions, solve and dipoles */
+} thp_result;
+
+typedef struct thp_server_stats {
+  long completed, failed;
+  double p50_ms, p99_ms;   /* latency over the completed requests */
+  int resident, pooled;    /* contexts holding a system / idle for reuse */
+  long created, reused, evicted;
+  size_t bytes;            /* device bytes held by resident and pooled contexts */
+} thp_server_stats;
+
+typedef struct thp_server thp_server;
+
+/* Starts the worker threads; touches no device until the first request. */
+int thp_server_create(const thp_server_config* cfg, thp_server** out);
+/* Registers (or replaces) the system under key; copies every array. */
+int thp_server_register(thp_server* s, unsigned long long key, const thp_system* sys);
+/* Queues one single-point solve of system key at positions x, y, z (copied).
+ * uind/uinp [n][3] (may be NULL) receive the dipoles and must stay valid
+ * until thp_server_wait returns for the ticket.  Admission: a system whose
+ * footprint exceeds the budget fails at once with THP_E_OOM_ADMISSION; others
+ * wait until enough idle systems are evicted.  An evicted system's context
+ * goes to a pool and is re-targeted (thp_ctx_reset) for the next system
+ * instead of being freed.  A repeat of a resident system starts from its
+ * previous dipoles. */
+int thp_server_submit(thp_server* s, unsigned long long key, const double* x, const double* y,
+                      const double* z, double* uind, double* uinp, unsigned long long* ticket);
+/* Blocks until the request finishes; res receives its outcome. */
+int thp_server_wait(thp_server* s, unsigned long long ticket, thp_result* res);
+int thp_server_query(thp_server* s, thp_server_stats* out);
+/* Waits for queued work, then frees every context. */
+int thp_server_destroy(thp_server* s);
 
 /* ---- allocation-free energy (no counterpart in the reference) ------------ */
 /* For callers that cannot allocate device memory at the point of use: a host

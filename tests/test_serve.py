@@ -1,74 +1,43 @@
-"""Batched and served forms: the server's admission / residency logic on the
-CPU with a fake solver, and on the GPU that every result is the same alone
-and in the mix (within the CG tolerance) and that batched solves equal
-single solves."""
-import threading
-import time
+"""Batched and served forms.
 
+CPU: the native request loop's admission checks and error reporting (no
+device is needed to reject an oversize request, and a request that finds no
+device fails with THP_E_NO_DEVICE instead of crashing).  GPU: every served
+result is the same alone and in the mix (within the CG tolerance), contexts
+evicted under a tight budget are re-targeted for new systems and still give
+the same answers, and batched solves equal single solves."""
 import numpy as np
 import pytest
 
 DEBYE = 4.80321
 
 
-class FakeCtx:
-    live = 0
-    max_live_bytes = 0
-
-    def __init__(self, ws, log):
-        self.ws, self.log, self.busy = ws, log, threading.Lock()
-        self.solves = 0
-
-    def set_positions(self, x, y, z):
-        pass
-
-    def solve(self, guess, allow_unconverged=False):
-        assert self.busy.acquire(blocking=False), "one context used by two workers at once"
-        try:
-            self.log.append((id(self), guess))
-            time.sleep(0.002)
-            self.solves += 1
-            return {"niter": 3 if guess else 8, "epol": -1.0, "status": 0}
-        finally:
-            self.busy.release()
-
-    def dipoles(self):
-        return np.zeros((self.ws.n, 3)), None
-
-    def close(self):
-        pass
-
-
-def test_server_admission_and_residency(thp):
+def test_server_rejects_oversize_and_unknown(thp):
     from tinker_hp_b200 import serve, lib
-    reqs = serve.poisson_stream(40, rate=2000.0, nmin=1000, nmax=3000, seed=7)
-    log = []
-    sizes = {}
-
-    def fp(ws):
-        return ws.n * 1000
-
-    budget = 4 * 3000 * 1000  # about four systems resident at once
-    srv = serve.Server(budget_bytes=budget, workers=6, context_factory=lambda ws: FakeCtx(ws, log),
-                       footprint_fn=fp)
-    out = srv.run(reqs, realtime=False)
-    assert len(out) == len(reqs) and all(r.status == 0 for r in out)
-    assert srv.used <= budget
-    # repeats found their system resident or rebuilt it after eviction
-    assert any(g == lib.GUESS_PREVIOUS for _, g in log)
-    s = serve.summarize(out)
-    assert s["completed"] == len(reqs) and s["p99_ms"] >= s["p50_ms"]
+    ws = thp.water.make_water_box(400)
+    srv = serve.Server(budget_bytes=1000, workers=1)
+    with pytest.raises(lib.ThpError) as e:
+        srv.submit("big", ws)
+    assert e.value.status == lib.THP_E_OOM_ADMISSION
+    import ctypes as C
+    t = C.c_ulonglong()
+    x = np.zeros(ws.n)
+    st = lib.load().thp_server_submit(srv.h, 12345, lib._p(x), lib._p(x), lib._p(x), None, None, C.byref(t))
+    assert st == lib.THP_E_INVALID
     srv.close()
 
 
-def test_server_rejects_oversize(thp):
+def test_server_reports_device_status(thp):
+    # on a machine without a GPU the request fails cleanly with NO_DEVICE;
+    # on a GPU it is solved
     from tinker_hp_b200 import serve, lib
-    reqs = serve.poisson_stream(2, nmin=1000, nmax=1200, seed=3)
-    srv = serve.Server(budget_bytes=10, workers=1, context_factory=lambda ws: FakeCtx(ws, []),
-                       footprint_fn=lambda ws: 100)
-    with pytest.raises(lib.ThpError) as e:
-        srv.run(reqs, realtime=False)
-    assert e.value.status == lib.THP_E_OOM_ADMISSION
+    ws = thp.water.make_water_box(400)
+    srv = serve.Server(workers=2)
+    out = srv.run([serve.Request(0, 0.0, "a", ws)], realtime=False)
+    assert out[0].status in (lib.THP_OK, lib.THP_E_NO_DEVICE)
+    st = srv.stats()
+    assert st["completed"] + st["failed"] == 1
+    srv.close()
 
 
 @pytest.mark.gpu
@@ -95,6 +64,7 @@ def test_served_results_same_alone_and_in_mix(thp):
     srv = serve.Server(precision=lib.MIXED, poleps=1e-6, workers=4)
     out = {r.rid: r for r in srv.run(reqs, realtime=True)}
     srv.close()
+    assert all(out[q.rid].warm == q.repeat for q in reqs)
     for q in reqs:
         r = out[q.rid]
         assert r.status == lib.THP_OK
@@ -114,3 +84,48 @@ def test_served_results_same_alone_and_in_mix(thp):
     fresh = [out[q.rid].niter for q in reqs if not q.repeat]
     if reps:
         assert np.mean(reps) < np.mean(fresh)
+
+
+@pytest.mark.gpu
+def test_server_reuses_contexts_under_a_tight_budget(thp):
+    from tinker_hp_b200 import serve, lib
+    reqs = serve.poisson_stream(24, rate=1000.0, nmin=1000, nmax=8000, repeat_frac=0.3, seed=13)
+    biggest = max(lib.footprint(q.ws, lib.MIXED) for q in reqs)
+    srv = serve.Server(precision=lib.MIXED, poleps=1e-6, workers=3, budget_bytes=3 * biggest)
+    out = {r.rid: r for r in srv.run(reqs, realtime=False)}
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    assert st["evicted"] > 0 and st["reused"] > 0, st
+    assert st["bytes"] <= 3 * biggest
+    for q in reqs:
+        alone = lib.Context(q.ws, precision=lib.MIXED, poleps=1e-6)
+        alone.solve()
+        ua, _ = alone.dipoles()
+        d = np.sqrt(np.mean(np.sum((out[q.rid].uind - ua) ** 2, 1))) * DEBYE
+        # a warm start converges to the same answer within the CG tolerance
+        assert d < (1e-5 if out[q.rid].warm else 1e-7), (q.rid, out[q.rid].warm, d)
+
+
+@pytest.mark.gpu
+def test_context_retarget_matches_fresh_context(thp):
+    # one context serves a small, a larger and another small system in turn
+    # (thp_ctx_reset grows buffers and re-plans the FFT only when needed)
+    from tinker_hp_b200 import lib
+    boxes = [thp.water.make_water_box(216, cfg=0), thp.water.make_water_box(648, cfg=1),
+             thp.water.make_water_box(300, cfg=2)]
+    ctx = lib.Context(boxes[0])
+    for k, ws in enumerate(boxes):
+        if k:
+            ctx.retarget(ws)
+        r = ctx.solve()
+        u, p = ctx.dipoles()
+        fresh = lib.Context(ws)
+        rf = fresh.solve()
+        uf, pf = fresh.dipoles()
+        assert r["niter"] == rf["niter"]
+        assert np.abs(u - uf).max() < 1e-12 * np.abs(uf).max() and np.abs(p - pf).max() < 1e-12 * np.abs(pf).max()
+        assert abs(r["epol"] - rf["epol"]) < 1e-12 * abs(rf["epol"])
+        _, g = ctx.gradient()
+        _, gf = fresh.gradient()
+        assert np.abs(g - gf).max() < 1e-9 * np.abs(gf).max()

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -101,26 +102,36 @@ void build_special_pairs(Ctx& c, const int* const* off, const int* const* idx, c
 }
 
 int upload_special_pairs(Ctx& c) {
-  cudaFree(c.d_sp_off);
-  cudaFree(c.d_sp_k);
-  cudaFree(c.d_sp_ks);
-  cudaFree(c.d_sp_s);
-  c.d_sp_off = nullptr;
-  c.d_sp_k = nullptr;
-  c.d_sp_ks = nullptr;
-  c.d_sp_s = nullptr;
   c.have_list = false;  // sorted partner numbers are made at the next sort
   int st;
-  if ((st = dmalloc(c, &c.d_sp_off, c.n + 1, "alloc sp_off"))) return st;
-  if ((st = dmalloc(c, &c.d_sp_k, c.sp_k.size(), "alloc sp_k"))) return st;
-  if ((st = dmalloc(c, &c.d_sp_ks, c.sp_k.size(), "alloc sp_ks"))) return st;
-  if ((st = dmalloc(c, &c.d_sp_s, c.sp_s.size(), "alloc sp_s"))) return st;
-  cudaMemcpy(c.d_sp_off, c.sp_off.data(), sizeof(int) * (c.n + 1), cudaMemcpyHostToDevice);
-  if (!c.sp_k.empty()) {
-    cudaMemcpy(c.d_sp_k, c.sp_k.data(), sizeof(int) * c.sp_k.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(c.d_sp_s, c.sp_s.data(), sizeof(double) * c.sp_s.size(), cudaMemcpyHostToDevice);
+  // buffers are kept while large enough, so re-targeting a context does not
+  // free device memory (cudaFree waits for the whole device)
+  if ((size_t)c.n + 1 > c.cap_sp_off) {
+    cudaFree(c.d_sp_off);
+    c.d_sp_off = nullptr;
+    c.cap_sp_off = 0;
+    if ((st = dmalloc(c, &c.d_sp_off, c.n + 1, "alloc sp_off"))) return st;
+    c.cap_sp_off = c.n + 1;
   }
-  return cuda_status(cudaGetLastError(), &c, "upload special pairs");
+  const size_t m = std::max<size_t>(1, c.sp_k.size());
+  if (m > c.cap_sp) {
+    cudaFree(c.d_sp_k);
+    cudaFree(c.d_sp_ks);
+    cudaFree(c.d_sp_s);
+    c.d_sp_k = c.d_sp_ks = nullptr;
+    c.d_sp_s = nullptr;
+    c.cap_sp = 0;
+    if ((st = dmalloc(c, &c.d_sp_k, m, "alloc sp_k"))) return st;
+    if ((st = dmalloc(c, &c.d_sp_ks, m, "alloc sp_ks"))) return st;
+    if ((st = dmalloc(c, &c.d_sp_s, 3 * m, "alloc sp_s"))) return st;
+    c.cap_sp = m;
+  }
+  cudaMemcpyAsync(c.d_sp_off, c.sp_off.data(), sizeof(int) * (c.n + 1), cudaMemcpyHostToDevice, c.stream);
+  if (!c.sp_k.empty()) {
+    cudaMemcpyAsync(c.d_sp_k, c.sp_k.data(), sizeof(int) * c.sp_k.size(), cudaMemcpyHostToDevice, c.stream);
+    cudaMemcpyAsync(c.d_sp_s, c.sp_s.data(), sizeof(double) * c.sp_s.size(), cudaMemcpyHostToDevice, c.stream);
+  }
+  return cuda_status(cudaStreamSynchronize(c.stream), &c, "upload special pairs");
 }
 
 void cell_grid(const thp_config& cfg, int nc[3]) {
@@ -221,20 +232,49 @@ int ensure_coef(thp_ctx* h) {
   return THP_OK;
 }
 
+// Pinned blocks for the per-context CG scalars and flags are recycled
+// process-wide: cudaMallocHost is slow and serialises with other threads.
+namespace {
+std::mutex g_pinned_mu;
+std::vector<void*> g_pinned_free;
+constexpr size_t kPinnedBlock = 4096;
+}  // namespace
+
+static int pinned_take(Ctx& c) {
+  {
+    std::lock_guard<std::mutex> g(g_pinned_mu);
+    if (!g_pinned_free.empty()) {
+      c.h_pinned = g_pinned_free.back();
+      g_pinned_free.pop_back();
+    }
+  }
+  if (!c.h_pinned) {
+    int st = cuda_status(cudaMallocHost(&c.h_pinned, kPinnedBlock), &c, "pinned");
+    if (st) return st;
+  }
+  c.h_cg = static_cast<CgScalars*>(c.h_pinned);
+  c.h_flags = reinterpret_cast<int*>(static_cast<char*>(c.h_pinned) + 2048);
+  return THP_OK;
+}
+
+static void pinned_give(Ctx& c) {
+  if (!c.h_pinned) return;
+  std::lock_guard<std::mutex> g(g_pinned_mu);
+  g_pinned_free.push_back(c.h_pinned);
+  c.h_pinned = nullptr;
+  c.h_cg = nullptr;
+  c.h_flags = nullptr;
+}
+
 void free_ctx(Ctx& c) {
-  void* ptrs[] = {c.d_mrec, c.d_mrecf, c.d_sp_ks, c.d_cell_count, c.d_cell_start, c.d_cell_fill, c.d_atom_cell, c.d_scell, c.d_perm, c.d_iperm,
-                  c.d_xyz_orig, c.d_par_orig, c.d_rpole_orig, c.d_pole_local, c.d_frames, c.d_pos, c.d_posf,
-                  c.d_thole, c.d_pol, c.d_rpole, c.d_sp_off, c.d_sp_k, c.d_sp_s, c.d_pos_built, c.d_nnb, c.d_nb,
-                  c.d_npr, c.d_pk, c.d_pc3, c.d_pc5, c.d_ef, c.d_mu, c.d_res, c.d_h, c.d_pp, c.d_zr, c.d_dip,
-                  c.d_cphi, c.d_vecf, c.d_tmp6, c.d_tmp6b, c.d_partials, c.d_cg, c.d_flags,
-                  c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad, c.d_sgrid, c.d_sscratch};
+  void* ptrs[] = {c.slab_cells, c.slab_atoms, c.slab_pairs, c.d_sp_off, c.d_sp_k, c.d_sp_ks, c.d_sp_s, c.d_cg,
+                  c.d_flags, c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad, c.d_sgrid, c.d_sscratch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   pme_free(c);
   if (c.chunk_exec) cudaGraphExecDestroy(c.chunk_exec);
   if (c.loop_exec) cudaGraphExecDestroy(c.loop_exec);
-  if (c.h_cg) cudaFreeHost(c.h_cg);
-  if (c.h_flags) cudaFreeHost(c.h_flags);
+  pinned_give(c);
   if (c.ev_fork) cudaEventDestroy(c.ev_fork);
   if (c.ev_join) cudaEventDestroy(c.ev_join);
   if (c.stream2) cudaStreamDestroy(c.stream2);
@@ -289,10 +329,7 @@ const char* thp_status_string(int s) {
 
 size_t thp_footprint(const thp_config* cfg) { return cfg ? footprint_bytes(*cfg, nullptr) : 0; }
 
-int thp_ctx_create(const thp_config* cfg, thp_ctx** out) {
-  if (!cfg || !out) return THP_E_INVALID;
-  *out = nullptr;
-  const thp_config& k = *cfg;
+static int check_config(const thp_config& k) {
   if (k.n <= 0 || k.box[0] <= 0 || k.box[1] <= 0 || k.box[2] <= 0 || k.aewald <= 0 || k.ewaldcut <= 0 ||
       k.lbuffer < 0 || k.bsorder != 5 || k.nfft[0] < 5 || k.nfft[1] < 5 || k.nfft[2] < 5 || k.politer <= 0 ||
       (k.precision != THP_FP64 && k.precision != THP_MIXED))
@@ -303,8 +340,11 @@ int thp_ctx_create(const thp_config* cfg, thp_ctx** out) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return THP_E_NO_DEVICE;
   if (k.device < 0 || k.device >= ndev) return THP_E_INVALID;
-  thp_ctx* h = new thp_ctx();
-  Ctx& c = h->c;
+  return THP_OK;
+}
+
+// System geometry and sizes from a configuration (no device work).
+static void apply_config(Ctx& c, const thp_config& k) {
   c.cfg = k;
   c.n = k.n;
   c.npad = (k.n + 31) / 32 * 32;
@@ -324,7 +364,128 @@ int thp_ctx_create(const thp_config* cfg, thp_ctx** out) {
   c.box.recip[2] = (k.box[0] * (k.box[1] * 1.0) - (k.box[1] * 0.0) * 0.0) / vol;
   cell_grid(k, c.nc);
   c.ncell = c.nc[0] * c.nc[1] * c.nc[2];
-  int st = set_current_device(c);
+  c.nblk_reduce = (c.n + 127) / 128;
+}
+
+extern "C++" {
+template <class... P>
+static void free_all(P**... p) {
+  ((cudaFree(*p), *p = nullptr), ...);
+}
+}
+
+// Grows each buffer group that is smaller than the current sizes need; a
+// group that is large enough is kept as it is.
+struct SlabItem {
+  void** ptr;
+  size_t bytes;
+};
+
+// One cudaMalloc for a group of arrays, each starting on a 256-byte boundary.
+static int alloc_slab(Ctx& c, void** base, std::initializer_list<SlabItem> items, const char* what) {
+  auto up = [](size_t b) { return (std::max<size_t>(b, 1) + 255) / 256 * 256; };
+  size_t total = 0;
+  for (const SlabItem& it : items) total += up(it.bytes);
+  void* b = nullptr;
+  int st = cuda_status(cudaMalloc(&b, total), &c, what);
+  if (st) return st;
+  size_t off = 0;
+  for (const SlabItem& it : items) {
+    *it.ptr = static_cast<char*>(b) + off;
+    off += up(it.bytes);
+  }
+  *base = b;
+  return THP_OK;
+}
+
+extern "C++" {
+template <class T>
+static SlabItem item(T** p, size_t count) {
+  return SlabItem{reinterpret_cast<void**>(p), count * sizeof(T)};
+}
+}
+
+// Grows each buffer group that is smaller than the current sizes need; a
+// group that is large enough is kept as it is.
+static int size_buffers(Ctx& c) {
+  int st = THP_OK;
+  const size_t n = c.n, npad = c.npad;
+  const size_t esz = c.mixed ? 4 : 8;
+  if ((size_t)c.ncell > c.cap_ncell) {
+    cudaFree(c.slab_cells);
+    c.slab_cells = nullptr;
+    c.cap_ncell = 0;
+    const size_t m = c.ncell;
+    st = alloc_slab(c, &c.slab_cells, {item(&c.d_cell_count, m), item(&c.d_cell_start, m), item(&c.d_cell_fill, m)},
+                    "cells");
+    if (!st) c.cap_ncell = c.ncell;
+  }
+  if (!st && n > c.cap_n) {
+    cudaFree(c.slab_atoms);
+    c.slab_atoms = nullptr;
+    // buffers made on first use are sized by n as well
+    free_all(&c.d_fphirec, &c.d_depfix, &c.d_trq, &c.d_frs, &c.d_grad);
+    c.cap_n = 0;
+    st = alloc_slab(c, &c.slab_atoms,
+                    {item(&c.d_atom_cell, n), item(&c.d_scell, n), item(&c.d_perm, n), item(&c.d_iperm, n),
+                     item(&c.d_xyz_orig, 3 * n), item(&c.d_par_orig, 3 * n), item(&c.d_rpole_orig, 13 * n),
+                     item(&c.d_pole_local, 13 * n), item(&c.d_frames, 3 * n), item(&c.d_pos, n),
+                     item(&c.d_posf, n), item(&c.d_thole, n), item(&c.d_pol, n), item(&c.d_rpole, 10 * n),
+                     item(&c.d_mrec, 12 * n), item(&c.d_mrecf, 12 * n), item(&c.d_pos_built, n),
+                     item(&c.d_nnb, n), item(&c.d_npr, n), item(&c.d_ef, 6 * n), item(&c.d_mu, 6 * n),
+                     item(&c.d_res, 6 * n), item(&c.d_h, 6 * n), item(&c.d_pp, 6 * n), item(&c.d_zr, 6 * n),
+                     item(&c.d_dip, 6 * n), item(&c.d_tmp6, 6 * n), item(&c.d_tmp6b, 6 * n), item(&c.d_cphi, 4 * n),
+                     item(&c.d_vecf, 6 * n), item(&c.d_partials, (size_t)(c.nblk_reduce + 8) * 4)},
+                    "per-atom buffers");
+    if (!st) c.cap_n = n;
+  }
+  const size_t pairs = (size_t)c.maxnb * npad;
+  if (!st && pairs > c.cap_pairs) {
+    cudaFree(c.slab_pairs);
+    c.slab_pairs = nullptr;
+    c.cap_pairs = 0;
+    st = alloc_slab(c, &c.slab_pairs,
+                    {item(&c.d_nb, pairs), item(&c.d_pk, pairs), SlabItem{&c.d_pc3, esz * pairs},
+                     SlabItem{&c.d_pc5, esz * pairs}},
+                    "pair buffers");
+    if (!st) c.cap_pairs = pairs;
+  }
+  if (!st && !c.d_cg) st = dmalloc(c, &c.d_cg, 1, "cg");
+  if (!st && !c.d_flags) st = dmalloc(c, &c.d_flags, 1, "flags");
+  if (!st && !c.h_pinned) st = pinned_take(c);
+  return st;
+}
+
+// Clears everything that belongs to the system a context serves, after
+// apply_config/size_buffers/pme_init: no parameters, positions,
+// multipoles, list or dipoles; no special pairs.
+static int clear_system_state(thp_ctx* h) {
+  Ctx& c = h->c;
+  c.have_params = c.have_pos = c.have_rpole = c.have_conn = c.have_frames = c.have_axes = false;
+  c.have_perm = c.have_list = c.have_coef = c.have_dipoles = false;
+  h->pos_dirty = h->rpole_dirty = true;
+  h->field_valid = h->guess_uploaded = h->solved_once = false;
+  c.bx = c.by = c.bz = c.brpole = c.buind = c.buinp = c.bep = c.bdep = c.bqgrid = nullptr;
+  c.bnelst = c.belst = nullptr;
+  c.bmaxelst = 0;
+  cudaMemsetAsync(c.d_flags, 0, sizeof(int), c.stream);
+  cudaMemsetAsync(c.d_cg, 0, sizeof(CgScalars), c.stream);
+  cudaMemsetAsync(c.d_mu, 0, sizeof(double) * 6 * c.n, c.stream);
+  c.sp_off.assign(c.n + 1, 0);
+  c.sp_k.clear();
+  c.sp_s.clear();
+  return upload_special_pairs(c);  // synchronises the stream
+}
+
+int thp_ctx_create(const thp_config* cfg, thp_ctx** out) {
+  if (!cfg || !out) return THP_E_INVALID;
+  *out = nullptr;
+  int st = check_config(*cfg);
+  if (st) return st;
+  thp_ctx* h = new thp_ctx();
+  Ctx& c = h->c;
+  apply_config(c, *cfg);
+  st = set_current_device(c);
   if (!st) st = cuda_status(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), &c, "stream");
   c.own_stream = true;
   if (!st) st = cuda_status(cudaStreamCreateWithFlags(&c.stream2, cudaStreamNonBlocking), &c, "stream");
@@ -332,56 +493,9 @@ int thp_ctx_create(const thp_config* cfg, thp_ctx** out) {
   if (!st) st = cuda_status(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming), &c, "event");
   if (!st) st = cuda_status(cudaEventCreate(&c.ev0), &c, "event");
   if (!st) st = cuda_status(cudaEventCreate(&c.ev1), &c, "event");
-  const size_t n = c.n, npad = c.npad;
-  const size_t esz = c.mixed ? 4 : 8;
-  c.nblk_reduce = (c.n + 127) / 128;
-  if (!st) st = dmalloc(c, &c.d_cell_count, c.ncell, "cells");
-  if (!st) st = dmalloc(c, &c.d_cell_start, c.ncell, "cells");
-  if (!st) st = dmalloc(c, &c.d_cell_fill, c.ncell, "cells");
-  if (!st) st = dmalloc(c, &c.d_atom_cell, n, "cells");
-  if (!st) st = dmalloc(c, &c.d_scell, n, "cells");
-  if (!st) st = dmalloc(c, &c.d_perm, n, "perm");
-  if (!st) st = dmalloc(c, &c.d_iperm, n, "perm");
-  if (!st) st = dmalloc(c, &c.d_xyz_orig, 3 * n, "xyz");
-  if (!st) st = dmalloc(c, &c.d_par_orig, 3 * n, "params");
-  if (!st) st = dmalloc(c, &c.d_rpole_orig, 13 * n, "rpole");
-  if (!st) st = dmalloc(c, &c.d_pole_local, 13 * n, "pole");
-  if (!st) st = dmalloc(c, &c.d_frames, 3 * n, "frames");
-  if (!st) st = dmalloc(c, &c.d_pos, n, "pos");
-  if (!st) st = dmalloc(c, &c.d_posf, n, "posf");
-  if (!st) st = dmalloc(c, &c.d_thole, n, "thole");
-  if (!st) st = dmalloc(c, &c.d_pol, n, "pol");
-  if (!st) st = dmalloc(c, &c.d_rpole, 10 * n, "rpole sorted");
-  if (!st) st = dmalloc(c, &c.d_mrec, 12 * n, "mrec");
-  if (!st) st = dmalloc(c, &c.d_mrecf, 12 * n, "mrecf");
-  if (!st) st = dmalloc(c, &c.d_pos_built, n, "pos built");
-  if (!st) st = dmalloc(c, &c.d_nnb, n, "nnb");
-  if (!st) st = dmalloc(c, &c.d_nb, (size_t)c.maxnb * npad, "nb");
-  if (!st) st = dmalloc(c, &c.d_npr, n, "npr");
-  if (!st) st = dmalloc(c, &c.d_pk, (size_t)c.maxpr * npad, "pk");
-  if (!st) st = cuda_status(cudaMalloc(&c.d_pc3, esz * c.maxpr * npad), &c, "pc3");
-  if (!st) st = cuda_status(cudaMalloc(&c.d_pc5, esz * c.maxpr * npad), &c, "pc5");
-  double** vecs[] = {&c.d_ef, &c.d_mu, &c.d_res, &c.d_h, &c.d_pp, &c.d_zr, &c.d_dip, &c.d_tmp6, &c.d_tmp6b};
-  for (double** v : vecs)
-    if (!st) st = dmalloc(c, v, 6 * n, "vectors");
-  if (!st) st = dmalloc(c, &c.d_cphi, 4 * n, "cphi");
-  if (!st) st = dmalloc(c, &c.d_vecf, 6 * n, "vecf");
-  if (!st) st = dmalloc(c, &c.d_partials, (size_t)(c.nblk_reduce + 8) * 4, "partials");
-  if (!st) st = dmalloc(c, &c.d_cg, 1, "cg");
-  if (!st) st = dmalloc(c, &c.d_flags, 1, "flags");
-  if (!st) st = cuda_status(cudaMallocHost((void**)&c.h_cg, sizeof(CgScalars)), &c, "pinned");
-  if (!st) st = cuda_status(cudaMallocHost((void**)&c.h_flags, sizeof(int)), &c, "pinned");
-  if (!st) {
-    cudaMemset(c.d_flags, 0, sizeof(int));
-    cudaMemset(c.d_cg, 0, sizeof(CgScalars));
-    cudaMemset(c.d_mu, 0, sizeof(double) * 6 * n);
-    st = pme_init(c);
-  }
-  if (!st) {
-    // default: no special pairs
-    c.sp_off.assign(n + 1, 0);
-    st = upload_special_pairs(c);
-  }
+  if (!st) st = size_buffers(c);
+  if (!st) st = pme_init(c);
+  if (!st) st = clear_system_state(h);
   if (st) {
     fprintf(stderr, "thp_ctx_create: %s\n", c.last_msg.c_str());
     free_ctx(c);
@@ -390,6 +504,45 @@ int thp_ctx_create(const thp_config* cfg, thp_ctx** out) {
   }
   *out = h;
   return THP_OK;
+}
+
+int thp_ctx_reset(thp_ctx* h, const thp_config* cfg) {
+  if (!h || !cfg) return THP_E_INVALID;
+  Ctx& c = h->c;
+  int st = check_config(*cfg);
+  if (st) return st;
+  if ((cfg->precision == THP_MIXED) != (c.mixed != 0) || cfg->device != c.device) return THP_E_INVALID;
+  if (set_current_device(c)) return THP_E_CUDA;
+  if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "reset"))) return st;
+  // graphs hold this system's sizes and launch shapes
+  if (c.chunk_exec) cudaGraphExecDestroy(c.chunk_exec);
+  if (c.loop_exec) cudaGraphExecDestroy(c.loop_exec);
+  c.chunk_exec = c.loop_exec = nullptr;
+  c.loop_state = 0;
+  for (cudaEvent_t e : c.prof_events) cudaEventDestroy(e);
+  c.prof_events.clear();
+  c.profiling = false;
+  const size_t old_ngrid = c.ngrid;
+  apply_config(c, *cfg);
+  if ((st = size_buffers(c))) return st;
+  if ((st = pme_init(c))) return st;
+  if (c.ngrid > old_ngrid && c.d_sgrid) {
+    cudaFree(c.d_sgrid);
+    c.d_sgrid = nullptr;
+  }
+  if (g_current == h) g_current = nullptr;
+  return clear_system_state(h);
+}
+
+size_t thp_ctx_footprint(thp_ctx* h) {
+  if (!h) return 0;
+  thp_config k = h->c.cfg;
+  k.n = (int)std::max<size_t>(h->c.cap_n, (size_t)k.n);
+  const size_t ng = std::max<size_t>(h->c.cap_ngrid, 1);
+  // the grid term of the footprint depends only on the product of the dims
+  k.nfft[0] = (int)ng;
+  k.nfft[1] = k.nfft[2] = 1;
+  return footprint_bytes(k, nullptr);
 }
 
 int thp_ctx_destroy(thp_ctx* h) {

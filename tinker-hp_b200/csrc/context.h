@@ -38,6 +38,15 @@ enum : int { DEV_LIST_OVERFLOW = 1, DEV_PAIR_OVERFLOW = 2, DEV_NAN = 4 };
 struct Ctx {
   thp_config cfg{};
   int n = 0, npad = 0;
+  // allocated capacities (a context re-targeted to a new system keeps every
+  // buffer that is large enough)
+  size_t cap_n = 0, cap_ncell = 0, cap_pairs = 0, cap_sp = 0, cap_sp_off = 0;
+  // one allocation per buffer group (cells, per-atom arrays, pair arrays);
+  // the d_* pointers of a group point into its slab
+  void* slab_cells = nullptr;
+  void* slab_atoms = nullptr;
+  void* slab_pairs = nullptr;
+  void* h_pinned = nullptr;  // pinned block holding h_cg and h_flags
   int mixed = 0;
   Box box{};
   int device = 0;
@@ -113,6 +122,8 @@ struct Ctx {
   size_t ngrid = 0;
   cufftHandle plan = 0;
   bool have_plan = false;
+  int plan_dims[3] = {0, 0, 0};
+  size_t cap_ngrid = 0;
   void* d_grid = nullptr;  // cufftDoubleComplex or cufftComplex
   void* d_qfac = nullptr;  // double or float
   double a_frac[3] = {0, 0, 0};  // nfft_d * recip(d,d)

@@ -9,6 +9,8 @@
 // the fractional <-> Cartesian matrices reduce to a_d = nfft_d * recip(d,d).
 #include <vector>
 
+#include <mutex>
+
 #include "kernels.h"
 #include "pme_dev.cuh"
 
@@ -363,6 +365,64 @@ int convolve(Ctx& c, int check_stop) {
   return fft(c, CUFFT_INVERSE);
 }
 
+// Process-wide cache of cuFFT plans by device, dimensions and type: a
+// context that is destroyed or re-targeted to another grid gives its plan
+// back, and the next context of that shape takes it instead of planning
+// again (planning allocates a work area and can take milliseconds).
+struct PlanKey {
+  int device, n1, n2, n3, mixed;
+  bool operator==(const PlanKey& o) const {
+    return device == o.device && n1 == o.n1 && n2 == o.n2 && n3 == o.n3 && mixed == o.mixed;
+  }
+};
+std::mutex g_plan_mu;
+std::vector<std::pair<PlanKey, cufftHandle>> g_plans;
+constexpr size_t kMaxCachedPlans = 64;
+
+bool take_plan(const PlanKey& k, cufftHandle* out) {
+  std::lock_guard<std::mutex> g(g_plan_mu);
+  for (size_t q = 0; q < g_plans.size(); ++q)
+    if (g_plans[q].first == k) {
+      *out = g_plans[q].second;
+      g_plans.erase(g_plans.begin() + q);
+      return true;
+    }
+  return false;
+}
+
+void give_plan(const PlanKey& k, cufftHandle plan) {
+  std::lock_guard<std::mutex> g(g_plan_mu);
+  if (g_plans.size() >= kMaxCachedPlans) {
+    cufftDestroy(g_plans.front().second);
+    g_plans.erase(g_plans.begin());
+  }
+  g_plans.emplace_back(k, plan);
+}
+
+PlanKey plan_key(const Ctx& c) { return PlanKey{c.device, c.plan_dims[0], c.plan_dims[1], c.plan_dims[2], c.mixed}; }
+
+// qfac(k) = exp(-pi^2 h^2 / a^2) / (pi V h^2 bsmod1 bsmod2 bsmod3), zero at
+// h = 0 and where the exponent is below -50 (newinduce_pme.f:1802-1854)
+template <typename T>
+__global__ void k_qfac_init(int n1, int n2, int n3, const double* __restrict__ bsm, double r1, double r2, double r3,
+                            double pterm, double volterm, T* __restrict__ q) {
+  const size_t ng = (size_t)n1 * n2 * n3;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < ng; t += (size_t)gridDim.x * blockDim.x) {
+    const int k1 = (int)(t % n1), k2 = (int)((t / n1) % n2), k3 = (int)(t / ((size_t)n1 * n2));
+    const int m1 = k1 < (n1 + 1) / 2 ? k1 : k1 - n1;
+    const int m2 = k2 < (n2 + 1) / 2 ? k2 : k2 - n2;
+    const int m3 = k3 < (n3 + 1) / 2 ? k3 : k3 - n3;
+    double v = 0.0;
+    if (m1 != 0 || m2 != 0 || m3 != 0) {
+      const double h1 = r1 * m1, h2 = r2 * m2, h3 = r3 * m3;
+      const double hsq = h1 * h1 + h2 * h2 + h3 * h3;
+      const double term = -pterm * hsq;
+      if (term > -50.0) v = exp(term) / (volterm * hsq * bsm[k1] * bsm[n1 + k2] * bsm[n1 + n2 + k3]);
+    }
+    q[t] = (T)v;
+  }
+}
+
 }  // namespace
 
 int pme_init(Ctx& c) {
@@ -372,55 +432,67 @@ int pme_init(Ctx& c) {
   // influence function (newinduce_pme.f:1802-1854)
   std::vector<double> m1 = dftmod_host(c.nfft[0], kBs), m2 = dftmod_host(c.nfft[1], kBs),
                       m3 = dftmod_host(c.nfft[2], kBs);
-  std::vector<double> q(c.ngrid, 0.0);
-  double a = c.cfg.aewald;
-  double pterm = (kPi / a) * (kPi / a);
-  double volbox = c.cfg.box[0] * c.cfg.box[1] * c.cfg.box[2];
-  double volterm = kPi * volbox;
-  int nf1 = (c.nfft[0] + 1) / 2, nf2 = (c.nfft[1] + 1) / 2, nf3 = (c.nfft[2] + 1) / 2;
-  for (int k3 = 1; k3 <= c.nfft[2]; ++k3)
-    for (int k2 = 1; k2 <= c.nfft[1]; ++k2)
-      for (int k1 = 1; k1 <= c.nfft[0]; ++k1) {
-        int r1 = k1 - 1, r2 = k2 - 1, r3 = k3 - 1;
-        if (k1 > nf1) r1 -= c.nfft[0];
-        if (k2 > nf2) r2 -= c.nfft[1];
-        if (k3 > nf3) r3 -= c.nfft[2];
-        if (r1 == 0 && r2 == 0 && r3 == 0) continue;
-        double h1 = c.box.recip[0] * r1, h2 = c.box.recip[1] * r2, h3 = c.box.recip[2] * r3;
-        double hsq = h1 * h1 + h2 * h2 + h3 * h3;
-        double term = -pterm * hsq;
-        if (term > -50.0) {
-          double denom = volterm * hsq * m1[k1] * m2[k2] * m3[k3];
-          q[((size_t)(k3 - 1) * c.nfft[1] + (k2 - 1)) * c.nfft[0] + (k1 - 1)] = exp(term) / denom;
-        }
-      }
   size_t esz = c.mixed ? sizeof(float) : sizeof(double);
   size_t csz = c.mixed ? sizeof(cufftComplex) : sizeof(cufftDoubleComplex);
-  if (cuda_status(cudaMalloc(&c.d_qfac, esz * c.ngrid), &c, "alloc qfac")) return THP_E_CUDA;
-  if (cuda_status(cudaMalloc(&c.d_grid, csz * c.ngrid), &c, "alloc grid")) return THP_E_CUDA;
-  if (c.mixed) {
-    std::vector<float> qf(q.begin(), q.end());
-    cudaMemcpy(c.d_qfac, qf.data(), esz * c.ngrid, cudaMemcpyHostToDevice);
-  } else {
-    cudaMemcpy(c.d_qfac, q.data(), esz * c.ngrid, cudaMemcpyHostToDevice);
+  // grid buffers are kept while they are large enough (a re-targeted
+  // context reuses them)
+  if (c.ngrid > c.cap_ngrid) {
+    cudaFree(c.d_qfac);
+    cudaFree(c.d_grid);
+    c.d_qfac = c.d_grid = nullptr;
+    c.cap_ngrid = 0;
+    if (cuda_status(cudaMalloc(&c.d_qfac, esz * c.ngrid), &c, "alloc qfac")) return THP_E_CUDA;
+    if (cuda_status(cudaMalloc(&c.d_grid, csz * c.ngrid), &c, "alloc grid")) return THP_E_CUDA;
+    c.cap_ngrid = c.ngrid;
   }
-  // cuFFT dims: slowest first; data [n3][n2][n1]
-  cufftResult r = cufftPlan3d(&c.plan, c.nfft[2], c.nfft[1], c.nfft[0], c.mixed ? CUFFT_C2C : CUFFT_Z2Z);
-  if (r != CUFFT_SUCCESS) {
-    c.last_msg = "cufftPlan3d failed";
-    return THP_E_CUDA;
+  // influence function on the device (newinduce_pme.f:1802-1854): the
+  // B-spline moduli go through the front of the grid buffer
+  std::vector<double> bsm(m1.begin() + 1, m1.begin() + 1 + c.nfft[0]);
+  bsm.insert(bsm.end(), m2.begin() + 1, m2.begin() + 1 + c.nfft[1]);
+  bsm.insert(bsm.end(), m3.begin() + 1, m3.begin() + 1 + c.nfft[2]);
+  double* d_bsm = reinterpret_cast<double*>(c.d_grid);  // ngrid complex >= n1+n2+n3 doubles
+  cudaMemcpyAsync(d_bsm, bsm.data(), sizeof(double) * bsm.size(), cudaMemcpyHostToDevice, c.stream);
+  const double a = c.cfg.aewald;
+  const double pterm = (kPi / a) * (kPi / a);
+  const double volterm = kPi * (c.cfg.box[0] * c.cfg.box[1] * c.cfg.box[2]);
+  const int blocks = (int)std::min<size_t>((c.ngrid + 255) / 256, 148 * 16);
+  if (c.mixed)
+    k_qfac_init<float><<<blocks, 256, 0, c.stream>>>(c.nfft[0], c.nfft[1], c.nfft[2], d_bsm, c.box.recip[0],
+                                                     c.box.recip[1], c.box.recip[2], pterm, volterm,
+                                                     (float*)c.d_qfac);
+  else
+    k_qfac_init<double><<<blocks, 256, 0, c.stream>>>(c.nfft[0], c.nfft[1], c.nfft[2], d_bsm, c.box.recip[0],
+                                                      c.box.recip[1], c.box.recip[2], pterm, volterm,
+                                                      (double*)c.d_qfac);
+  if (cuda_status(cudaStreamSynchronize(c.stream), &c, "qfac")) return THP_E_CUDA;
+  // cuFFT dims: slowest first; data [n3][n2][n1]; the plan is kept when the
+  // grid dimensions are unchanged
+  const bool same = c.have_plan && c.plan_dims[0] == c.nfft[0] && c.plan_dims[1] == c.nfft[1] &&
+                    c.plan_dims[2] == c.nfft[2];
+  if (!same) {
+    if (c.have_plan) give_plan(plan_key(c), c.plan);
+    c.have_plan = false;
+    for (int d = 0; d < 3; ++d) c.plan_dims[d] = c.nfft[d];
+    if (!take_plan(plan_key(c), &c.plan)) {
+      cufftResult r = cufftPlan3d(&c.plan, c.nfft[2], c.nfft[1], c.nfft[0], c.mixed ? CUFFT_C2C : CUFFT_Z2Z);
+      if (r != CUFFT_SUCCESS) {
+        c.last_msg = "cufftPlan3d failed";
+        return THP_E_CUDA;
+      }
+    }
+    c.have_plan = true;
   }
   cufftSetStream(c.plan, c.stream);
-  c.have_plan = true;
   return cuda_status(cudaGetLastError(), &c, "pme init");
 }
 
 void pme_free(Ctx& c) {
-  if (c.have_plan) cufftDestroy(c.plan);
+  if (c.have_plan) give_plan(plan_key(c), c.plan);
   c.have_plan = false;
   cudaFree(c.d_qfac);
   cudaFree(c.d_grid);
   c.d_qfac = c.d_grid = nullptr;
+  c.cap_ngrid = 0;
 }
 
 int zero_grid(Ctx& c) {

@@ -49,6 +49,29 @@ class ThpSolveInfo(C.Structure):
                 ("ene", C.c_double * 2), ("ms_total", C.c_double)]
 
 
+class ThpSystem(C.Structure):
+    _fields_ = [("cfg", ThpConfig), ("polarity", _dp), ("thole", _dp), ("pdamp", _dp),
+                ("conn_off", C.POINTER(_ip)), ("conn_idx", C.POINTER(_ip)), ("scales", _dp), ("pole", _dp),
+                ("zaxis", _ip), ("xaxis", _ip), ("axt", _ip)]
+
+
+class ThpServerConfig(C.Structure):
+    _fields_ = [("precision", C.c_int), ("poleps", C.c_double), ("politer", C.c_int), ("device", C.c_int),
+                ("budget_bytes", C.c_size_t), ("workers", C.c_int), ("max_resident", C.c_int)]
+
+
+class ThpResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("niter", C.c_int), ("warm", C.c_int), ("epol", C.c_double),
+                ("queue_ms", C.c_double), ("latency_ms", C.c_double), ("wait_ms", C.c_double),
+                ("setup_ms", C.c_double), ("solve_ms", C.c_double)]
+
+
+class ThpServerStats(C.Structure):
+    _fields_ = [("completed", C.c_long), ("failed", C.c_long), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("resident", C.c_int), ("pooled", C.c_int), ("created", C.c_long), ("reused", C.c_long),
+                ("evicted", C.c_long), ("bytes", C.c_size_t)]
+
+
 class ThpError(RuntimeError):
     def __init__(self, status, what):
         self.status = status
@@ -70,6 +93,8 @@ def load():
     sig = {
         "thp_ctx_create": ([C.POINTER(ThpConfig), C.POINTER(vp)], C.c_int),
         "thp_ctx_destroy": ([vp], C.c_int),
+        "thp_ctx_reset": ([vp, C.POINTER(ThpConfig)], C.c_int),
+        "thp_ctx_footprint": ([vp], C.c_size_t),
         "thp_set_stream": ([vp, vp], C.c_int),
         "thp_set_params": ([vp, _dp, _dp, _dp], C.c_int),
         "thp_set_connectivity": ([vp, C.POINTER(_ip), C.POINTER(_ip), _dp], C.c_int),
@@ -106,6 +131,12 @@ def load():
         "grid_uind_site_": ([_ip, _ip, _dp, _dp, _dp], None),
         "fphi_uind_site_": ([_ip, _ip, _dp, _dp, _dp], None),
         "thp_epolar_noalloc": ([C.c_int, vp, vp, vp, vp], C.c_int),
+        "thp_server_create": ([C.POINTER(ThpServerConfig), C.POINTER(vp)], C.c_int),
+        "thp_server_register": ([vp, C.c_ulonglong, C.POINTER(ThpSystem)], C.c_int),
+        "thp_server_submit": ([vp, C.c_ulonglong, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_ulonglong)], C.c_int),
+        "thp_server_wait": ([vp, C.c_ulonglong, C.POINTER(ThpResult)], C.c_int),
+        "thp_server_query": ([vp, C.POINTER(ThpServerStats)], C.c_int),
+        "thp_server_destroy": ([vp], C.c_int),
         "newinduce_pme2_": ([], None),
         "tmatxb_pme_": ([_ip, _ip, _dp, _dp], None),
         "efld0_direct_": ([_ip, _dp], None),
@@ -190,12 +221,27 @@ class Context:
     def __init__(self, ws, precision=FP64, poleps=1e-6, politer=500, device=0, frames=True, rpole=None,
                  max_neighbors=0):
         L = load()
-        self.ws = ws
-        self.n = ws.n
         self.cfg = config_for(ws, precision, poleps, politer, device, max_neighbors)
         h = C.c_void_p()
         self._check(L.thp_ctx_create(C.byref(self.cfg), C.byref(h)), "thp_ctx_create")
         self.h = h
+        self._setup(ws, frames, rpole)
+
+    def retarget(self, ws, frames=True, rpole=None, max_neighbors=0):
+        """Serve another system with this context (thp_ctx_reset): buffers
+        that are large enough and an unchanged FFT plan are kept."""
+        self.cfg = config_for(ws, self.cfg.precision, self.cfg.poleps, self.cfg.politer, self.cfg.device,
+                              max_neighbors)
+        self._check(load().thp_ctx_reset(self.h, C.byref(self.cfg)), "thp_ctx_reset")
+        self._setup(ws, frames, rpole)
+
+    def footprint(self):
+        return load().thp_ctx_footprint(self.h)
+
+    def _setup(self, ws, frames, rpole):
+        L = load()
+        self.ws = ws
+        self.n = ws.n
         self._keep = []
         self._check(L.thp_set_params(self.h, _p(_f64(ws.polarity)), _p(_f64(ws.thole)), _p(_f64(ws.pdamp))),
                     "thp_set_params")
@@ -352,3 +398,26 @@ class Context:
             raise ThpError(st, "thp_solve_host")
         return uind, uinp, {"niter": info.niter, "converged": bool(info.converged), "epol": info.epol,
                             "ms": info.ms_total}
+
+
+def system_struct(ws, keep):
+    """thp_system for a water.WaterSystem; `keep` collects the arrays the
+    pointers refer to (they must live until the call that copies them)."""
+    sysd = ThpSystem()
+    sysd.cfg = config_for(ws)
+    arr = {k: _f64(getattr(ws, k)) for k in ("polarity", "thole", "pdamp", "pole")}
+    ax = {k: _i32(getattr(ws, k)) for k in ("zaxis", "xaxis", "axt")}
+    sc = scales_array(ws)
+    offs, idxs = (_ip * 8)(), (_ip * 8)()
+    for q, name in enumerate(CONN_NAMES):
+        off, idx = ws.conn[name]
+        off, idx = _i32(off), _i32(idx if len(idx) else np.zeros(1, np.int32))
+        keep += [off, idx]
+        offs[q], idxs[q] = _p(off, _ip), _p(idx, _ip)
+    keep += list(arr.values()) + list(ax.values()) + [sc, offs, idxs]
+    sysd.polarity, sysd.thole, sysd.pdamp, sysd.pole = (_p(arr[k]) for k in ("polarity", "thole", "pdamp", "pole"))
+    sysd.zaxis, sysd.xaxis, sysd.axt = (_p(ax[k], _ip) for k in ("zaxis", "xaxis", "axt"))
+    sysd.scales = _p(sc)
+    sysd.conn_off = C.cast(offs, C.POINTER(_ip))
+    sysd.conn_idx = C.cast(idxs, C.POINTER(_ip))
+    return sysd

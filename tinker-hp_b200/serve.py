@@ -1,22 +1,17 @@
-"""Continuous-batching server for single-point polarization solves.
+"""Serving of single-point polarization solves over the native request loop.
 
-Requests (water boxes of any size) arrive over time.  The server:
-  * admits a request when a worker slot is free and the system's device
-    footprint (thp_footprint) fits the memory budget next to the resident
-    systems, evicting idle least-recently-used systems when needed;
-  * keeps each system resident (topology, parameters, lists, last dipoles)
-    so a repeat of a system with moved coordinates is warm-started from its
-    previous dipoles (THP_GUESS_PREVIOUS);
-  * runs admitted requests on worker threads, each system on its own CUDA
-    stream, so requests that arrive while others are on the GPU overlap with
-    them on the device (the ctypes calls release the GIL).
-Latency is completion time minus arrival time.
+The loop itself is C++ (thp_server_* in csrc/server.cu): admission by device
+footprint against a memory budget, residency of each system's topology,
+parameters, list and last dipoles (a repeat is warm-started), worker threads
+that drive the GPU with one stream per system, and a pool of idle contexts
+that new systems are re-targeted onto instead of allocating and freeing
+device memory.  This module feeds it a request stream in real time and
+collects the results; latency is measured inside the loop, from submission to
+the dipoles in the caller's buffer.
 """
+import ctypes as C
 import dataclasses
-import heapq
-import threading
 import time
-from collections import OrderedDict
 
 import numpy as np
 
@@ -37,18 +32,25 @@ class Request:
 class Result:
     rid: int
     key: str
-    arrival: float
-    start: float
-    end: float
+    arrival: float          # seconds after stream start, when it was submitted
+    queue_ms: float
+    latency_ms: float
     niter: int
     epol: float
     uind: np.ndarray
     status: int
     repeat: bool
+    warm: bool
+    setup_ms: float = 0.0
+    solve_ms: float = 0.0
 
     @property
     def latency(self):
-        return self.end - self.arrival
+        return self.latency_ms * 1e-3
+
+    @property
+    def end(self):
+        return self.arrival + self.latency
 
 
 def poisson_stream(count, rate=200.0, nmin=1000, nmax=60000, repeat_frac=0.3, perturb=0.01, seed=5004,
@@ -78,120 +80,95 @@ def poisson_stream(count, rate=200.0, nmin=1000, nmax=60000, repeat_frac=0.3, pe
 
 
 class Server:
-    """Admission, residency and worker pool (see module docstring)."""
+    """Python face of thp_server (see module docstring)."""
 
-    def __init__(self, precision=L.MIXED, poleps=1e-6, budget_bytes=120 << 30, workers=8, device=0,
-                 context_factory=None, footprint_fn=None):
-        self.precision = precision
-        self.poleps = poleps
-        self.budget = budget_bytes
-        self.workers = workers
-        self.device = device
-        self._make = context_factory or (lambda ws: L.Context(ws, precision=precision, poleps=poleps,
-                                                              device=device))
-        self._footprint = footprint_fn or (lambda ws: L.footprint(ws, precision))
-        self.resident = OrderedDict()  # key -> [ctx, bytes, busy]
-        self.used = 0
-        self.lock = threading.Condition()
-        self.results = []
+    def __init__(self, precision=L.MIXED, poleps=1e-6, politer=500, budget_bytes=120 << 30, workers=8, device=0,
+                 max_resident=16):
+        cfg = L.ThpServerConfig(precision, poleps, politer, device, budget_bytes, workers, max_resident)
+        h = C.c_void_p()
+        st = L.load().thp_server_create(C.byref(cfg), C.byref(h))
+        if st:
+            raise L.ThpError(st, "thp_server_create")
+        self.h = h
+        self.keys = {}
 
-    # -- residency ---------------------------------------------------------
-    def _acquire(self, req):
-        """Blocks until the system is resident and idle; returns its context."""
-        need = self._footprint(req.ws)
-        if need > self.budget:
-            raise L.ThpError(L.THP_E_OOM_ADMISSION, f"request {req.rid} needs {need} bytes")
-        with self.lock:
-            while True:
-                ent = self.resident.get(req.key)
-                if ent is not None:
-                    if not ent[2]:
-                        ent[2] = True
-                        self.resident.move_to_end(req.key)
-                        return ent[0], False
-                    self.lock.wait()
-                    continue
-                if self.used + need <= self.budget:
-                    self.used += need
-                    self.resident[req.key] = [None, need, True]
-                    break
-                victim = next((k for k, e in self.resident.items() if not e[2]), None)
-                if victim is None:
-                    self.lock.wait()
-                    continue
-                ctx, nbytes, _ = self.resident.pop(victim)
-                self.used -= nbytes
-                ctx.close()
-        try:
-            ctx = self._make(req.ws)
-        except Exception:
-            with self.lock:
-                self.used -= need
-                self.resident.pop(req.key, None)
-                self.lock.notify_all()
-            raise
-        with self.lock:
-            self.resident[req.key][0] = ctx
-        return ctx, True
+    def register(self, key, ws):
+        keep = []
+        sysd = L.system_struct(ws, keep)
+        code = self.keys.setdefault(key, len(self.keys) + 1)
+        st = L.load().thp_server_register(self.h, code, C.byref(sysd))
+        if st:
+            raise L.ThpError(st, "thp_server_register")
+        return code
 
-    def _release(self, key):
-        with self.lock:
-            ent = self.resident.get(key)
-            if ent is not None:
-                ent[2] = False
-            self.lock.notify_all()
+    def submit(self, key, ws):
+        """Queues one solve; returns (ticket, uind buffer)."""
+        code = self.keys.get(key) or self.register(key, ws)
+        xyz = [np.ascontiguousarray(a, dtype=np.float64) for a in (ws.x, ws.y, ws.z)]
+        uind = np.zeros((ws.n, 3))
+        t = C.c_ulonglong()
+        st = L.load().thp_server_submit(self.h, code, *(L._p(a) for a in xyz), L._p(uind), None, C.byref(t))
+        if st:
+            raise L.ThpError(st, "thp_server_submit")
+        return t.value, uind
 
-    # -- serving ----------------------------------------------------------
-    def _work(self, req, t0):
-        start = time.perf_counter() - t0
-        ctx, fresh = self._acquire(req)
-        try:
-            if not fresh:
-                ctx.set_positions(req.ws.x, req.ws.y, req.ws.z)
-            guess = L.GUESS_DIRECT if fresh else L.GUESS_PREVIOUS
-            r = ctx.solve(guess, allow_unconverged=True)
-            uind, _ = ctx.dipoles()
-            st = r["status"]
-        except L.ThpError as e:  # quarantine: the request fails, the server keeps going
-            r, uind, st = {"niter": 0, "epol": float("nan")}, None, e.status
-        finally:
-            self._release(req.key)
-        end = time.perf_counter() - t0
-        return Result(req.rid, req.key, req.arrival, start, end, r["niter"], r["epol"], uind, st, req.repeat)
+    def wait(self, ticket):
+        r = L.ThpResult()
+        st = L.load().thp_server_wait(self.h, ticket, C.byref(r))
+        if st:
+            raise L.ThpError(st, "thp_server_wait")
+        return r
 
     def run(self, requests, realtime=True):
-        """Serve the stream; returns results in completion order."""
-        import concurrent.futures as cf
+        """Serve the stream (submitting each request at its arrival time when
+        realtime); returns one Result per request."""
         reqs = sorted(requests, key=lambda q: q.arrival)
+        for q in reqs:  # registration copies the topology; do it before the clock starts
+            if q.key not in self.keys:
+                self.register(q.key, q.ws)
         t0 = time.perf_counter()
+        pending = []
+        for q in reqs:
+            if realtime:
+                delay = q.arrival - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+            submitted = time.perf_counter() - t0
+            ticket, uind = self.submit(q.key, q.ws)
+            pending.append((q, submitted, ticket, uind))
         out = []
-        with cf.ThreadPoolExecutor(max_workers=self.workers) as ex:
-            futs = []
-            for q in reqs:
-                if realtime:
-                    delay = q.arrival - (time.perf_counter() - t0)
-                    if delay > 0:
-                        time.sleep(delay)
-                futs.append(ex.submit(self._work, q, t0))
-            for f in cf.as_completed(futs):
-                out.append(f.result())
-        self.results = out
+        for q, submitted, ticket, uind in pending:
+            r = self.wait(ticket)
+            out.append(Result(q.rid, q.key, submitted, r.queue_ms, r.latency_ms, r.niter, r.epol,
+                              uind if r.status == L.THP_OK else None, r.status, q.repeat, bool(r.warm),
+                              r.setup_ms, r.solve_ms))
         return out
 
+    def stats(self):
+        s = L.ThpServerStats()
+        L.load().thp_server_query(self.h, C.byref(s))
+        return {k: getattr(s, k) for k, _ in L.ThpServerStats._fields_}
+
     def close(self):
-        with self.lock:
-            for ctx, _, _ in self.resident.values():
-                if ctx is not None:
-                    ctx.close()
-            self.resident.clear()
-            self.used = 0
+        if getattr(self, "h", None):
+            L.load().thp_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def summarize(results):
-    ok = [r for r in results if r.status in (L.THP_OK, L.THP_E_NOT_CONVERGED)]
-    lat = np.array([r.latency for r in ok]) * 1e3
+    ok = [r for r in results if r.status == L.THP_OK]
+    lat = np.array([r.latency_ms for r in ok])
     span = max(r.end for r in results) - min(r.arrival for r in results)
     return {"completed": len(ok), "failed": len(results) - len(ok), "solves_per_s": len(ok) / span,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_iters": float(np.mean([r.niter for r in ok])),
-            "repeat_iters": float(np.mean([r.niter for r in ok if r.repeat])) if any(r.repeat for r in ok) else None}
+            "repeat_iters": float(np.mean([r.niter for r in ok if r.repeat])) if any(r.repeat for r in ok) else None,
+            "warm_fraction": float(np.mean([r.warm for r in ok])),
+            "mean_setup_ms": float(np.mean([r.setup_ms for r in ok])),
+            "mean_solve_ms": float(np.mean([r.solve_ms for r in ok]))}
