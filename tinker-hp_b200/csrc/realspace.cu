@@ -21,6 +21,14 @@ namespace {
 
 constexpr int kBlock = 128;
 
+// list entries whose loads are issued together in the field / coefficient pass
+#ifndef THP_EFLD0_G32
+#define THP_EFLD0_G32 2
+#endif
+#ifndef THP_EFLD0_G64
+#define THP_EFLD0_G64 1
+#endif
+
 struct EwaldConst {
   double a, afac1, afac2, afac3;  // 2a/sqrt(pi), 4a^3/sqrt(pi), 8a^5/sqrt(pi)
 };
@@ -53,9 +61,10 @@ __global__ void __launch_bounds__(kBlock) k_efld0_coef(
     int n, int npad, Box box, double cut2, EwaldConst ew, const double4* __restrict__ pos,
     const double* __restrict__ mrec, const float* __restrict__ mrecf, const int* __restrict__ perm,
     const int* __restrict__ sp_off, const int* __restrict__ sp_ks, const double* __restrict__ sp_s,
-    const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb, int* __restrict__ npr, int* __restrict__ pk,
-    void* __restrict__ pc3v, void* __restrict__ pc5v, int maxpr, double* __restrict__ ef, int* __restrict__ flags) {
+    const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb, int* __restrict__ npr,
+    int* __restrict__ pk_out, void* __restrict__ pc3v, void* __restrict__ pc5v, int maxpr, double* __restrict__ ef, int* __restrict__ flags) {
   using T = typename std::conditional<MIXED, float, double>::type;
+  constexpr int G = MIXED ? THP_EFLD0_G32 : THP_EFLD0_G64;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   T* pc3 = (T*)pc3v;
@@ -68,85 +77,98 @@ __global__ void __launch_bounds__(kBlock) k_efld0_coef(
   const int nn = min(nnb[i], maxnb);
   int cnt = 0;
 #pragma unroll 1
-  for (int s = 0; s < nn; ++s) {
-    const int k = __ldg(nb + (size_t)s * npad + i);
-    const double4 pk4 = pos[k];
-    double xr = pk4.x - pi.x, yr = pk4.y - pi.y, zr = pk4.z - pi.z;
-    image3(box, xr, yr, zr);
-    const double r2d = r2_exact(xr, yr, zr);
-    if (r2d > cut2) continue;
-    // scale factors of this pair (1 unless listed), partners in sorted numbering
-    double ds = 1.0, ps = 1.0, us = 1.0;
-    for (int q = s0; q < s1; ++q)
-      if (__ldg(sp_ks + q) == k) {
-        ds = sp_s[3 * q];
-        ps = sp_s[3 * q + 1];
-        us = sp_s[3 * q + 2];
-        break;
+  for (int sb = 0; sb < nn; sb += G) {
+    // every load of the group is issued before the arithmetic of any pair
+    int kk[G];
+    double4 pk[G];
+    Rec<MIXED> rk[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) kk[g] = sb + g < nn ? __ldg(nb + (size_t)(sb + g) * npad + i) : i;
+#pragma unroll
+    for (int g = 0; g < G; ++g) pk[g] = pos[kk[g]];
+#pragma unroll
+    for (int g = 0; g < G; ++g) rk[g].load(mrec, mrecf, kk[g]);
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      if (sb + g >= nn) break;
+      const int k = kk[g];
+      const double4 pk4 = pk[g];
+      double xr = pk4.x - pi.x, yr = pk4.y - pi.y, zr = pk4.z - pi.z;
+      image3(box, xr, yr, zr);
+      const double r2d = r2_exact(xr, yr, zr);
+      if (r2d > cut2) continue;
+      // scale factors of this pair (1 unless listed), partners in sorted numbering
+      double ds = 1.0, ps = 1.0, us = 1.0;
+      for (int q = s0; q < s1; ++q)
+        if (__ldg(sp_ks + q) == k) {
+          ds = sp_s[3 * q];
+          ps = sp_s[3 * q + 1];
+          us = sp_s[3 * q + 2];
+          break;
+        }
+      const Rec<MIXED>& r_k = rk[g];
+      const T x = (T)xr, y = (T)yr, z = (T)zr, r2 = (T)r2d;
+      const T r = sqrt(r2);
+      const T rr1 = T(1) / r;
+      const T rr2 = rr1 * rr1;
+      const T rr3 = rr2 * rr1;
+      const T rr5 = T(3) * rr2 * rr3;
+      const T rr7 = T(5) * rr2 * rr5;
+      // dampewald (order 7)
+      const T ra = (T)ew.a * r;
+      const T bn0 = erfc(ra) * rr1;
+      const T expterm = exp(-ra * ra);
+      const T bn1 = (bn0 + (T)ew.afac1 * expterm) * rr2;
+      const T bn2 = (T(3) * bn1 + (T)ew.afac2 * expterm) * rr2;
+      const T bn3 = (T(5) * bn2 + (T)ew.afac3 * expterm) * rr2;
+      // dampthole / damptholed (AMOEBA branch)
+      T l3 = 1, l5 = 1, l7 = 1;
+      const double pdd = pi.w * pk4.w;
+      double pg = fmin(thi, (double)r_k.th);
+      if (pg == 0.0) pg = fmax(thi, (double)r_k.th);
+      if (pdd != 0.0 && pg != 0.0) {
+        const T t = r / (T)pdd;
+        const T damp = (T)pg * (t * t * t);
+        if (damp < T(50)) {
+          const T ex = exp(-damp);
+          l3 = T(1) - ex;
+          l5 = T(1) - ex * (T(1) + damp);
+          l7 = T(1) - ex * (T(1) + damp + T(0.6) * damp * damp);
+        }
       }
-    Rec<MIXED> rk;
-    rk.load(mrec, mrecf, k);
-    const T x = (T)xr, y = (T)yr, z = (T)zr, r2 = (T)r2d;
-    const T r = sqrt(r2);
-    const T rr1 = T(1) / r;
-    const T rr2 = rr1 * rr1;
-    const T rr3 = rr2 * rr1;
-    const T rr5 = T(3) * rr2 * rr3;
-    const T rr7 = T(5) * rr2 * rr5;
-    // dampewald (order 7)
-    const T ra = (T)ew.a * r;
-    const T bn0 = erfc(ra) * rr1;
-    const T expterm = exp(-ra * ra);
-    const T bn1 = (bn0 + (T)ew.afac1 * expterm) * rr2;
-    const T bn2 = (T(3) * bn1 + (T)ew.afac2 * expterm) * rr2;
-    const T bn3 = (T(5) * bn2 + (T)ew.afac3 * expterm) * rr2;
-    // dampthole / damptholed (AMOEBA branch)
-    T l3 = 1, l5 = 1, l7 = 1;
-    const double pdd = pi.w * pk4.w;
-    double pg = fmin(thi, (double)rk.th);
-    if (pg == 0.0) pg = fmax(thi, (double)rk.th);
-    if (pdd != 0.0 && pg != 0.0) {
-      const T t = r / (T)pdd;
-      const T damp = (T)pg * (t * t * t);
-      if (damp < T(50)) {
-        const T ex = exp(-damp);
-        l3 = T(1) - ex;
-        l5 = T(1) - ex * (T(1) + damp);
-        l7 = T(1) - ex * (T(1) + damp + T(0.6) * damp * damp);
+      if (FIELD) {
+        const T ck = r_k.q, dkx = r_k.dx, dky = r_k.dy, dkz = r_k.dz;
+        const T dkr = dkx * x + dky * y + dkz * z;
+        const T qkx = r_k.qxx * x + r_k.qxy * y + r_k.qxz * z;
+        const T qky = r_k.qxy * x + r_k.qyy * y + r_k.qyz * z;
+        const T qkz = r_k.qxz * x + r_k.qyz * y + r_k.qzz * z;
+        const T qkr = qkx * x + qky * y + qkz * z;
+        T sc = (T)ds;
+        T dmp3 = bn1 - (T(1) - sc * l3) * rr3;
+        T dmp5 = bn2 - (T(1) - sc * l5) * rr5;
+        T dmp7 = bn3 - (T(1) - sc * l7) * rr7;
+        T rad = dmp3 * ck - dmp5 * dkr + dmp7 * qkr;
+        e[0] += (double)(-x * rad - dmp3 * dkx + T(2) * dmp5 * qkx);
+        e[1] += (double)(-y * rad - dmp3 * dky + T(2) * dmp5 * qky);
+        e[2] += (double)(-z * rad - dmp3 * dkz + T(2) * dmp5 * qkz);
+        sc = (T)ps;
+        dmp3 = bn1 - (T(1) - sc * l3) * rr3;
+        dmp5 = bn2 - (T(1) - sc * l5) * rr5;
+        dmp7 = bn3 - (T(1) - sc * l7) * rr7;
+        rad = dmp3 * ck - dmp5 * dkr + dmp7 * qkr;
+        e[3] += (double)(-x * rad - dmp3 * dkx + T(2) * dmp5 * qkx);
+        e[4] += (double)(-y * rad - dmp3 * dky + T(2) * dmp5 * qky);
+        e[5] += (double)(-z * rad - dmp3 * dkz + T(2) * dmp5 * qkz);
       }
+      const T su = (T)us;
+      if (cnt < maxpr) {
+        const size_t q = (size_t)cnt * npad + i;
+        pk_out[q] = k;
+        pc3[q] = bn1 - (T(1) - su * l3) * rr3;
+        pc5[q] = bn2 - (T(1) - su * l5) * rr5;
+      }
+      ++cnt;
     }
-    if (FIELD) {
-      const T ck = rk.q, dkx = rk.dx, dky = rk.dy, dkz = rk.dz;
-      const T dkr = dkx * x + dky * y + dkz * z;
-      const T qkx = rk.qxx * x + rk.qxy * y + rk.qxz * z;
-      const T qky = rk.qxy * x + rk.qyy * y + rk.qyz * z;
-      const T qkz = rk.qxz * x + rk.qyz * y + rk.qzz * z;
-      const T qkr = qkx * x + qky * y + qkz * z;
-      T sc = (T)ds;
-      T dmp3 = bn1 - (T(1) - sc * l3) * rr3;
-      T dmp5 = bn2 - (T(1) - sc * l5) * rr5;
-      T dmp7 = bn3 - (T(1) - sc * l7) * rr7;
-      T rad = dmp3 * ck - dmp5 * dkr + dmp7 * qkr;
-      e[0] += (double)(-x * rad - dmp3 * dkx + T(2) * dmp5 * qkx);
-      e[1] += (double)(-y * rad - dmp3 * dky + T(2) * dmp5 * qky);
-      e[2] += (double)(-z * rad - dmp3 * dkz + T(2) * dmp5 * qkz);
-      sc = (T)ps;
-      dmp3 = bn1 - (T(1) - sc * l3) * rr3;
-      dmp5 = bn2 - (T(1) - sc * l5) * rr5;
-      dmp7 = bn3 - (T(1) - sc * l7) * rr7;
-      rad = dmp3 * ck - dmp5 * dkr + dmp7 * qkr;
-      e[3] += (double)(-x * rad - dmp3 * dkx + T(2) * dmp5 * qkx);
-      e[4] += (double)(-y * rad - dmp3 * dky + T(2) * dmp5 * qky);
-      e[5] += (double)(-z * rad - dmp3 * dkz + T(2) * dmp5 * qkz);
-    }
-    const T su = (T)us;
-    if (cnt < maxpr) {
-      const size_t q = (size_t)cnt * npad + i;
-      pk[q] = k;
-      pc3[q] = bn1 - (T(1) - su * l3) * rr3;
-      pc5[q] = bn2 - (T(1) - su * l5) * rr5;
-    }
-    ++cnt;
   }
   npr[i] = min(cnt, maxpr);
   if (cnt > maxpr) atomicOr(flags, DEV_PAIR_OVERFLOW);
