@@ -241,6 +241,34 @@ def serving_run(lib, thp, count, workers=8):
     return summ
 
 
+def md_run(lib, thp, nsteps=20, predictor=None):
+    """Config 1 dynamics: 10,800 waters (32,400 atoms), FP64, velocity Verlet
+    at 1 fs from Maxwell velocities at 300 K (seed 3001), each solve started
+    from the previous step's dipoles or from a predictor.  The polarization
+    gradient is the only force, which is attractive, so unbonded water
+    collapses after some 60 fs: the run is kept to the first 20 fs."""
+    ws = thp.water.make_water_box(10800, cfg=1)
+    mass = thp.water.masses(ws)
+    vel = thp.water.maxwell_velocities(mass, 300.0, seed=3001)
+    ctx = lib.Context(ws, precision=lib.FP64, poleps=1e-6)
+    if predictor:
+        ctx.set_predictor(getattr(lib, f"PRED_{predictor}"))
+    ctx.md_verlet(2, 0.001, mass, vel)  # warm the kernels and graphs
+    ctx.close()
+    ctx = lib.Context(ws, precision=lib.FP64, poleps=1e-6)
+    if predictor:
+        ctx.set_predictor(getattr(lib, f"PRED_{predictor}"))
+    t0 = time.perf_counter()
+    _, en, it = ctx.md_verlet(nsteps, 0.001, mass, vel)
+    wall = time.perf_counter() - t0
+    ctx.close()
+    ms = wall / nsteps * 1e3
+    return {"steps": nsteps, "ms_per_step": ms, "ns_per_day": 1e-6 * 86400.0 / (ms * 1e-3),
+            "guess": predictor or "previous step", "mean_iters": float(np.mean(it)),
+            "iters": [int(x) for x in it], "energy_drift_rel": float(abs(en[-1, 2] - en[0, 2]) / abs(en[0, 1])),
+            "atoms": ws.n, "dt_fs": 1.0}
+
+
 def timed_solves(ctx, lib, steps, warmup, rebuild=True, guess=None):
     """Device-resident solves; per-step device time from CUDA events."""
     import torch
@@ -415,6 +443,7 @@ def main():
         extras["batch_64_boxes"] = batched_throughput(lib, batch64, 1, 3)
         extras["batch_64_boxes"]["atoms"] = f"{sum(w.n for w in batch64)} over 64 boxes (300-6000 each)"
         extras["serving"] = serving_run(lib, thp, 120)
+        extras["md_config1"] = {"previous": md_run(lib, thp), "aspc": md_run(lib, thp, predictor="ASPC")}
         if fp64 is not None:
             best = max(b2["solves_per_s"], b4["solves_per_s"])
             extras["batched_288k"]["speedup_vs_fp64_plain"] = best / (world * len(lat64) / (t64 / 1000.0))

@@ -59,6 +59,15 @@ extern "C" {
 #define THP_GUESS_DIRECT 0   /* mu = alpha * E0 (polgsf = 0) */
 #define THP_GUESS_PREVIOUS 1 /* mu = last converged dipoles kept on the device */
 #define THP_GUESS_HOST 2     /* mu = caller-provided array (thp_set_guess) */
+#define THP_GUESS_PREDICT 3  /* predictor over the stored solutions (thp_set_predictor); the direct
+                                guess until seven are stored (newinduce_pme2.f:165-190) */
+
+/* predictors of the dipoles in dynamics (ulspred, newinduce_pme2.f:910;
+ * coefficients kpolar.f:405-425) */
+#define THP_PRED_NONE 0
+#define THP_PRED_ASPC 1
+#define THP_PRED_GEAR 2
+#define THP_PRED_LSQR 3
 
 typedef struct thp_config {
   int n;            /* polarizable sites (npole == npolar == n) */
@@ -112,6 +121,11 @@ int thp_set_rpole(thp_ctx* ctx, const double* rpole);
 int thp_set_frames(thp_ctx* ctx, const double* pole, const int* zaxis, const int* xaxis,
                    const int* axt);
 int thp_set_guess(thp_ctx* ctx, const double* mu /*[n][2][3]*/);
+/* Chooses the predictor (THP_PRED_*) and clears the stored solutions.  With a
+ * predictor set, every solve stores its dipoles (the last seven are kept, in
+ * original atom order, so list rebuilds do not disturb them) and
+ * THP_GUESS_PREDICT extrapolates from them. */
+int thp_set_predictor(thp_ctx* ctx, int mode);
 /* list build (mlistcell), incremental when displacements allow */
 int thp_nblist(thp_ctx* ctx);
 /* full rebuild (cell sort + list) on the next list use, as nblist(0) does */
@@ -155,8 +169,9 @@ int thp_get_gradient(thp_ctx* ctx, double* dep, double* ep);
 int thp_get_gradient_device(thp_ctx* ctx, double* d_dep);
 /* Velocity-Verlet NVE dynamics driven by the polarization gradient alone
  * (verlet.f:17-200 with gradient = epolar1): per step a half kick, a drift of
- * the positions on the device, a solve warm-started from the previous step's
- * dipoles (list rebuilt when an atom moved more than lbuffer/2), the gradient,
+ * the positions on the device, a solve warm-started from the predictor when
+ * one is set (thp_set_predictor), else from the previous step's dipoles
+ * (list rebuilt when an atom moved more than lbuffer/2), the gradient,
  * and the second half kick.  Starts with a solve and gradient at the current
  * positions.  mass [n] g/mol; vel [n][3] A/ps, updated in place; dt in ps.
  * energies [nsteps][3] (may be NULL): epol, kinetic, total (kcal/mol) after
@@ -226,7 +241,8 @@ typedef struct thp_server thp_server;
 
 /* Starts the worker threads; touches no device until the first request. */
 int thp_server_create(const thp_server_config* cfg, thp_server** out);
-/* Registers (or replaces) the system under key; copies every array. */
+/* Registers (or replaces) the system under key; copies every array and
+ * plans the system's FFT shape ahead of its first request. */
 int thp_server_register(thp_server* s, unsigned long long key, const thp_system* sys);
 /* Queues one single-point solve of system key at positions x, y, z (copied).
  * uind/uinp [n][3] (may be NULL) receive the dipoles and must stay valid

@@ -251,33 +251,68 @@ class Oracle:
         return e, {"real": er.value, "recip": ek.value, "self": es.value}
 
 
-def verlet(ws, vel, mass, dt, nsteps, poleps=1e-8):
+# kpolar.f:405-425
+GEAR = (6.0, -15.0, 20.0, -15.0, 6.0, -1.0, 0.0)
+ASPC = (22.0 / 7.0, -55.0 / 14.0, 55.0 / 21.0, -22.0 / 21.0, 5.0 / 21.0, -1.0 / 42.0, 0.0)
+MAXUALT = 7  # MOD_uprior.f:33
+
+
+def predict(history, mode):
+    """ulspred (newinduce_pme2.f:910-1010) and the guess of :165-178:
+    history is a list of [n,2,3] solutions, newest first, of length 7."""
+    m = len(history)
+    if mode in ("ASPC", "GEAR"):
+        b = ASPC if mode == "ASPC" else GEAR
+        bd = bp = np.array(b[: m - 1])
+    else:  # least-squares fit of the newest solution on the six before it
+        coef = []
+        for r in (0, 1):
+            a = np.array([h[:, r, :].ravel() for h in history])
+            c = a @ a.T
+            coef.append(np.linalg.solve(c[1:, 1:], c[0, 1:]))
+        bd, bp = coef
+    g = np.zeros_like(history[0])
+    for k in range(m - 1):
+        g[:, 0, :] += bd[k] * history[k][:, 0, :]
+        g[:, 1, :] += bp[k] * history[k][:, 1, :]
+    return g
+
+
+def verlet(ws, vel, mass, dt, nsteps, poleps=1e-8, predictor=None):
     """Velocity-Verlet NVE with the polarization gradient as the only force
-    (verlet.f:17-200; a = -convert * dE/dx / m, units.f:76), each step solved
-    from the direct guess.  Returns (positions [n,3], velocities [n,3],
-    energies [nsteps,3] = epol/kinetic/total)."""
+    (verlet.f:17-200; a = -convert * dE/dx / m, units.f:76).  Each solve
+    starts from the direct guess, or, with a predictor ("ASPC", "GEAR",
+    "LSQR"), from its extrapolation once seven solutions are stored.  Returns
+    (positions [n,3], velocities [n,3], energies [nsteps,3] =
+    epol/kinetic/total, CG iterations [nsteps])."""
     convert = 418.4
     m = np.asarray(mass, dtype=np.float64)[:, None]
     v = np.array(vel, dtype=np.float64)
     pos = ws.positions().copy()
+    history = []
 
     def grad(p):
         w = ws.with_positions(p)
         o = Oracle(w, poleps=poleps)
         if o.mlistcell()[0] != 0:
             raise RuntimeError("oracle list overflow")
-        r = o.solve()
+        guess = predict(history, predictor) if predictor and len(history) == MAXUALT else None
+        r = o.solve(guess)
+        if predictor:
+            history.insert(0, np.stack([r["uind"], r["uinp"]], axis=1))
+            del history[MAXUALT:]
         ep, dep = o.epolar1(r["uind"], r["uinp"])
         o.close()
-        return ep, dep
+        return ep, dep, r["niter"]
 
-    _, g = grad(pos)
+    _, g, _ = grad(pos)
     out = np.zeros((nsteps, 3))
+    its = np.zeros(nsteps, dtype=int)
     for s in range(nsteps):
         v += -convert * g / m * (0.5 * dt)
         pos += v * dt
-        ep, g = grad(pos)
+        ep, g, its[s] = grad(pos)
         v += -convert * g / m * (0.5 * dt)
         ek = 0.5 * np.sum(m * v * v) / convert
         out[s] = (ep, ek, ep + ek)
-    return pos, v, out
+    return pos, v, out, its

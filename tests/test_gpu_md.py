@@ -26,7 +26,7 @@ def test_md_matches_oracle_verlet(lib, thp):
     mass = thp.water.masses(ws)
     vel = thp.water.maxwell_velocities(mass, 300.0, seed=3001)
     dt, nsteps = 0.001, 5
-    pos_ref, vel_ref, en_ref = O.verlet(ws, vel, mass, dt, nsteps, poleps=1e-8)
+    pos_ref, vel_ref, en_ref, _ = O.verlet(ws, vel, mass, dt, nsteps, poleps=1e-8)
     ctx = lib.Context(ws, poleps=1e-8)
     v, en, it = ctx.md_verlet(nsteps, dt, mass, vel)
     pos = ctx.positions()
@@ -63,3 +63,26 @@ def test_md_rejects_bad_input(lib, thp):
     with pytest.raises(lib.ThpError) as e:
         ctx.md_verlet(1, -0.001, mass, np.zeros((ws.n, 3)))
     assert e.value.status == lib.THP_E_INVALID
+
+
+@pytest.mark.parametrize("mode", ["ASPC", "GEAR", "LSQR"])
+def test_md_predictor_matches_oracle(lib, thp, mode):
+    # 12 steps: the predictor takes over from step 7 (seven stored solutions)
+    ws = thp.water.make_water_box(216, cfg=0)
+    mass = thp.water.masses(ws)
+    vel = thp.water.maxwell_velocities(mass, 300.0, seed=3001)
+    nsteps = 12
+    pos_ref, _, en_ref, it_ref = O.verlet(ws, vel, mass, 0.001, nsteps, poleps=1e-8, predictor=mode)
+    ctx = lib.Context(ws, poleps=1e-8)
+    ctx.set_predictor(getattr(lib, f"PRED_{mode}"))
+    _, en, it = ctx.md_verlet(nsteps, 0.001, mass, vel)
+    assert np.abs(ctx.positions() - pos_ref).max() < 1e-7
+    np.testing.assert_allclose(en, en_ref, rtol=1e-7)
+    # same guesses, same CG: iteration counts agree (a count can move by one
+    # when a residual lands next to the threshold)
+    assert np.abs(it - it_ref).max() <= 1, (it, it_ref)
+    plain = lib.Context(ws, poleps=1e-8)
+    _, _, it_prev = plain.md_verlet(nsteps, 0.001, mass, vel)
+    print(mode, "iterations", it.tolist(), "previous-dipole guess", it_prev.tolist())
+    if mode == "ASPC":
+        assert it[7:].mean() < it_prev[7:].mean()

@@ -268,7 +268,8 @@ static void pinned_give(Ctx& c) {
 
 void free_ctx(Ctx& c) {
   void* ptrs[] = {c.slab_cells, c.slab_atoms, c.slab_pairs, c.d_sp_off, c.d_sp_k, c.d_sp_ks, c.d_sp_s, c.d_cg,
-                  c.d_flags, c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad, c.d_sgrid, c.d_sscratch};
+                  c.d_flags, c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad, c.d_sgrid, c.d_sscratch,
+                  c.d_alt};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   pme_free(c);
@@ -463,6 +464,7 @@ static int clear_system_state(thp_ctx* h) {
   Ctx& c = h->c;
   c.have_params = c.have_pos = c.have_rpole = c.have_conn = c.have_frames = c.have_axes = false;
   c.have_perm = c.have_list = c.have_coef = c.have_dipoles = false;
+  c.pred_mode = c.nualt = c.alt_head = 0;
   h->pos_dirty = h->rpole_dirty = true;
   h->field_valid = h->guess_uploaded = h->solved_once = false;
   c.bx = c.by = c.bz = c.brpole = c.buind = c.buinp = c.bep = c.bdep = c.bqgrid = nullptr;
@@ -700,19 +702,40 @@ int thp_profile(thp_ctx* h, int enable, double* ms_total, int* launches) {
   return THP_OK;
 }
 
+int thp_set_predictor(thp_ctx* h, int mode) {
+  if (!h || mode < THP_PRED_NONE || mode > THP_PRED_LSQR) return THP_E_INVALID;
+  h->c.pred_mode = mode;
+  h->c.nualt = 0;
+  h->c.alt_head = 0;
+  return THP_OK;
+}
+
+// THP_GUESS_PREDICT after the field (and any re-sort): the predicted dipoles
+// when the history is full, else the direct guess (newinduce_pme2.f:165-190).
+static int resolve_predict(Ctx& c, int* guess) {
+  if (*guess != THP_GUESS_PREDICT) return THP_OK;
+  const int r = predictor_guess(c);
+  if (r > 0) return r;
+  *guess = r == 0 ? THP_GUESS_PREVIOUS : THP_GUESS_DIRECT;  // PREVIOUS: start from d_mu as written
+  return THP_OK;
+}
+
 int thp_solve(thp_ctx* h, int guess, thp_solve_info* info) {
   if (!h) return THP_E_INVALID;
   Ctx& c = h->c;
   if (set_current_device(c)) return THP_E_CUDA;
   if (!c.have_params || !c.have_pos || (!c.have_rpole && !c.have_frames)) return THP_E_STATE;
+  if (guess < THP_GUESS_DIRECT || guess > THP_GUESS_PREDICT) return THP_E_INVALID;
   if (guess == THP_GUESS_PREVIOUS && !c.have_dipoles) guess = THP_GUESS_DIRECT;
   if (guess == THP_GUESS_HOST && !h->guess_uploaded) return THP_E_STATE;
   cudaEventRecord(c.ev0, c.stream);
   int st = compute_field(h);
   if (st) return st;
+  if ((st = resolve_predict(c, &guess))) return st;
   st = run_pcg(c, guess);
   h->guess_uploaded = false;
   if (st && st != THP_E_NOT_CONVERGED) return st;
+  if (int sp = predictor_push(c)) return sp;
   int st2 = launch_epol(c);
   if (st2) return st2;
   cudaEventRecord(c.ev1, c.stream);
@@ -751,6 +774,7 @@ static int solve_front_async(thp_ctx* h, int guess) {
   if ((st = launch_efld0_coef(c, true))) return st;
   if ((st = launch_efld0_recip(c))) return st;
   h->field_valid = true;
+  if ((st = resolve_predict(c, &guess))) return st;
   return pcg_begin(c, guess);
 }
 
@@ -774,6 +798,10 @@ int thp_solve_batch(thp_ctx** hs, int count, int guess, thp_solve_info* infos) {
       continue;
     }
     int g = guess;
+    if (g < THP_GUESS_DIRECT || g > THP_GUESS_PREDICT) {
+      st[i] = THP_E_INVALID;
+      continue;
+    }
     if (g == THP_GUESS_PREVIOUS && !c.have_dipoles) g = THP_GUESS_DIRECT;
     if (g == THP_GUESS_HOST && !h->guess_uploaded) {
       st[i] = THP_E_STATE;
@@ -831,6 +859,10 @@ int thp_solve_batch(thp_ctx** hs, int count, int guess, thp_solve_info* infos) {
     set_current_device(c);
     st[i] = pcg_status(c);
     if (st[i] && st[i] != THP_E_NOT_CONVERGED) continue;
+    if (int sp = predictor_push(c)) {
+      st[i] = sp;
+      continue;
+    }
     int s2 = launch_epol(c);
     if (s2) {
       st[i] = s2;
@@ -941,7 +973,7 @@ int thp_md_verlet(thp_ctx* h, int nsteps, double dt, const double* mass, double*
     cudaMemcpyAsync(d_vel, vel, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c.stream);
     st = cuda_status(cudaGetLastError(), &c, "md upload");
   }
-  const int guess = THP_GUESS_PREVIOUS;
+  const int guess = c.pred_mode ? THP_GUESS_PREDICT : THP_GUESS_PREVIOUS;
   thp_solve_info info;
   // gradient at the starting positions (mdinit's first gradient call)
   if (!st) {

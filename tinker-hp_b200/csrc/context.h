@@ -35,6 +35,9 @@ constexpr int kCgChunk = 4;
 // device error flags (bit set)
 enum : int { DEV_LIST_OVERFLOW = 1, DEV_PAIR_OVERFLOW = 2, DEV_NAN = 4 };
 
+// dipole solutions kept for the predictor (MOD_uprior.f: maxualt)
+constexpr int kMaxAlt = 7;
+
 struct Ctx {
   thp_config cfg{};
   int n = 0, npad = 0;
@@ -149,6 +152,12 @@ struct Ctx {
   CgScalars* h_cg = nullptr;     // pinned mirror
   int* d_flags = nullptr;        // device error bits
   int* h_flags = nullptr;        // pinned
+
+  // predictor history: kMaxAlt solutions [slot][n][6] in ORIGINAL order
+  int pred_mode = 0;
+  int nualt = 0, alt_head = 0;
+  double* d_alt = nullptr;
+  size_t alt_cap = 0;
 
   // polarization gradient (allocated on first use)
   double* d_fphirec = nullptr;    // [n][20] permanent-multipole potential, fractional

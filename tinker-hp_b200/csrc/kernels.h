@@ -19,6 +19,7 @@ int launch_tmatxb(Ctx& c, const double* d_in, double* d_out, bool dodiag);  // s
 
 // pme.cu
 int pme_init(Ctx& c);
+int plan_prefetch(int device, const int nfft[3], int mixed);  // puts a plan of that shape in the cache
 void pme_free(Ctx& c);
 int launch_efld0_recip(Ctx& c);         // d_cphi and E0 completion
 int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0);
@@ -37,6 +38,10 @@ int launch_grid_uind_sites(Ctx& c, int nsites, const int* d_site, const double* 
                            cufftDoubleComplex* d_sgrid);
 int launch_fphi_uind_sites(Ctx& c, int nsites, const int* d_site, const cufftDoubleComplex* d_sgrid, double* d_phi1,
                            double* d_phi2, double* d_sum);
+
+// predict.cu
+int predictor_push(Ctx& c);   // d_mu becomes the newest stored solution
+int predictor_guess(Ctx& c);  // predicted d_mu; -1 when fewer than kMaxAlt are stored
 
 // md.cu
 int launch_kick(Ctx& c, double half_dt, const double* d_mass, const double* d_grad, double* d_vel);

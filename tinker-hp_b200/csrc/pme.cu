@@ -401,6 +401,13 @@ void give_plan(const PlanKey& k, cufftHandle plan) {
 
 PlanKey plan_key(const Ctx& c) { return PlanKey{c.device, c.plan_dims[0], c.plan_dims[1], c.plan_dims[2], c.mixed}; }
 
+bool plan_cached(const PlanKey& k) {
+  std::lock_guard<std::mutex> g(g_plan_mu);
+  for (const auto& p : g_plans)
+    if (p.first == k) return true;
+  return false;
+}
+
 // qfac(k) = exp(-pi^2 h^2 / a^2) / (pi V h^2 bsmod1 bsmod2 bsmod3), zero at
 // h = 0 and where the exponent is below -50 (newinduce_pme.f:1802-1854)
 template <typename T>
@@ -484,6 +491,19 @@ int pme_init(Ctx& c) {
   }
   cufftSetStream(c.plan, c.stream);
   return cuda_status(cudaGetLastError(), &c, "pme init");
+}
+
+// Plans one grid shape ahead of use (a server does this when a system is
+// registered, so the first request of a new shape does not wait for it).
+int plan_prefetch(int device, const int nfft[3], int mixed) {
+  const PlanKey k{device, nfft[0], nfft[1], nfft[2], mixed};
+  if (plan_cached(k)) return THP_OK;
+  if (cudaSetDevice(device) != cudaSuccess) return THP_E_CUDA;
+  cufftHandle plan;
+  if (cufftPlan3d(&plan, nfft[2], nfft[1], nfft[0], mixed ? CUFFT_C2C : CUFFT_Z2Z) != CUFFT_SUCCESS)
+    return THP_E_CUDA;
+  give_plan(k, plan);
+  return THP_OK;
 }
 
 void pme_free(Ctx& c) {

@@ -23,6 +23,10 @@
 
 #include "thp.h"
 
+namespace thp {
+int plan_prefetch(int device, const int nfft[3], int mixed);
+}
+
 namespace {
 
 using Clock = std::chrono::steady_clock;
@@ -348,6 +352,10 @@ int thp_server_register(thp_server* s, unsigned long long key, const thp_system*
   }
   const thp_config k = server_cfg(s->cfg, sys->cfg);
   rec->footprint = thp_footprint(&k);
+  // the FFT plan of this shape is made now, not by the first request: a new
+  // shape can take tens of milliseconds to plan (a missing device only
+  // means the requests will report it)
+  thp::plan_prefetch(k.device, k.nfft, k.precision == THP_MIXED);
   std::lock_guard<std::mutex> g(s->m);
   s->systems[key] = rec;  // requests already queued keep the record they were given
   return THP_OK;

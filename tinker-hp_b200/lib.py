@@ -31,6 +31,8 @@ MIXED = 1
 GUESS_DIRECT = 0
 GUESS_PREVIOUS = 1
 GUESS_HOST = 2
+GUESS_PREDICT = 3
+PRED_NONE, PRED_ASPC, PRED_GEAR, PRED_LSQR = 0, 1, 2, 3
 
 CONN_NAMES = ("i12", "i13", "i14", "i15", "ip11", "ip12", "ip13", "ip14")
 
@@ -102,6 +104,7 @@ def load():
         "thp_set_rpole": ([vp, _dp], C.c_int),
         "thp_set_frames": ([vp, _dp, _ip, _ip, _ip], C.c_int),
         "thp_set_guess": ([vp, _dp], C.c_int),
+        "thp_set_predictor": ([vp, C.c_int], C.c_int),
         "thp_nblist": ([vp], C.c_int),
         "thp_invalidate_list": ([vp], C.c_int),
         "thp_profile": ([vp, C.c_int, _dp, _ip], C.c_int),
@@ -286,6 +289,9 @@ class Context:
 
     def set_rpole(self, rpole):
         self._check(load().thp_set_rpole(self.h, _p(_f64(rpole))), "thp_set_rpole")
+
+    def set_predictor(self, mode):
+        self._check(load().thp_set_predictor(self.h, int(mode)), "thp_set_predictor")
 
     def set_guess(self, mu):
         self._check(load().thp_set_guess(self.h, _p(_f64(mu))), "thp_set_guess")
