@@ -230,12 +230,13 @@ def serving_run(lib, thp, count, workers=8):
     srv.run(reqs[: min(8, len(reqs))], realtime=False)  # warm the kernels
     srv.close()
     srv = serve.Server(precision=lib.MIXED, poleps=CG_TOL, budget_bytes=120 << 30, workers=workers, max_resident=16)
-    out = srv.run(reqs, realtime=True)
+    out = srv.run(reqs, realtime=True, warm=24)
     stats = srv.stats()
     srv.close()
     summ = serve.summarize(out)
     summ["contexts"] = {k: stats[k] for k in ("created", "reused", "evicted", "resident", "pooled")}
     summ["max_resident"] = 16
+    summ["warm_pool"] = "24 contexts sized for the largest system, created at start-up before the stream"
     summ.update({"requests": len(reqs), "rate_req_per_s": 200.0, "workers": workers,
                  "atoms": "1,000-60,000 log-uniform", "repeats": "30 % (0.01 A RMS perturbation, warm start)"})
     return summ

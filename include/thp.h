@@ -254,6 +254,10 @@ int thp_server_register(thp_server* s, unsigned long long key, const thp_system*
  * previous dipoles. */
 int thp_server_submit(thp_server* s, unsigned long long key, const double* x, const double* y,
                       const double* z, double* uind, double* uinp, unsigned long long* ticket);
+/* Start-up: creates up to count idle contexts sized for the largest
+ * registered system (within the budget) and pools them, so the first
+ * requests of new systems re-target a context instead of creating one. */
+int thp_server_warm(thp_server* s, int count);
 /* Blocks until the request finishes; res receives its outcome. */
 int thp_server_wait(thp_server* s, unsigned long long ticket, thp_result* res);
 int thp_server_query(thp_server* s, thp_server_stats* out);

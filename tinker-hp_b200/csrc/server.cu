@@ -385,6 +385,36 @@ int thp_server_submit(thp_server* s, unsigned long long key, const double* x, co
   return THP_OK;
 }
 
+int thp_server_warm(thp_server* s, int count) {
+  if (!s || count < 0) return THP_E_INVALID;
+  std::shared_ptr<SysRec> big;
+  {
+    std::lock_guard<std::mutex> g(s->m);
+    for (auto& kv : s->systems)
+      if (!big || kv.second->footprint > big->footprint) big = kv.second;
+  }
+  if (!big) return THP_E_STATE;
+  const thp_config k = server_cfg(s->cfg, big->cfg);
+  for (int q = 0; q < count; ++q) {
+    {
+      std::lock_guard<std::mutex> g(s->m);
+      if (s->used + big->footprint > s->cfg.budget_bytes) break;
+      s->used += big->footprint;  // reserved before the slow creation
+    }
+    thp_ctx* h = nullptr;
+    const int st = thp_ctx_create(&k, &h);
+    std::lock_guard<std::mutex> g(s->m);
+    if (st) {
+      s->used -= big->footprint;
+      return st;
+    }
+    s->pool.push_back(Pooled{h, big->footprint});
+    ++s->created;
+  }
+  s->cv_room.notify_all();
+  return THP_OK;
+}
+
 int thp_server_wait(thp_server* s, unsigned long long ticket, thp_result* res) {
   if (!s) return THP_E_INVALID;
   std::unique_lock<std::mutex> lk(s->m);

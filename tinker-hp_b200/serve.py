@@ -112,6 +112,12 @@ class Server:
             raise L.ThpError(st, "thp_server_submit")
         return t.value, uind
 
+    def warm(self, count):
+        """Pre-creates `count` pooled contexts for the largest registered system."""
+        st = L.load().thp_server_warm(self.h, int(count))
+        if st:
+            raise L.ThpError(st, "thp_server_warm")
+
     def wait(self, ticket):
         r = L.ThpResult()
         st = L.load().thp_server_wait(self.h, ticket, C.byref(r))
@@ -119,13 +125,17 @@ class Server:
             raise L.ThpError(st, "thp_server_wait")
         return r
 
-    def run(self, requests, realtime=True):
+    def run(self, requests, realtime=True, warm=0):
         """Serve the stream (submitting each request at its arrival time when
-        realtime); returns one Result per request."""
+        realtime); returns one Result per request.  Registration (and `warm`
+        pooled contexts) happen before the clock starts, as at a server's
+        start-up."""
         reqs = sorted(requests, key=lambda q: q.arrival)
-        for q in reqs:  # registration copies the topology; do it before the clock starts
+        for q in reqs:
             if q.key not in self.keys:
                 self.register(q.key, q.ws)
+        if warm:
+            self.warm(warm)
         t0 = time.perf_counter()
         pending = []
         for q in reqs:
