@@ -43,3 +43,83 @@ def recip_field(pos, box, alpha, q=None, d=None, Q=None, chunk=4096):
         t = np.conj(ph) * w[None, :]  # e^{ik.r_i} * f * S
         E += -np.real(1j * t) @ kk
     return E
+
+
+def _thole(pdi, pdk, ti, tk, r):
+    """dampthole factors l3, l5, l7 (damping.f:74-124, AMOEBA branch)."""
+    damp = pdi * pdk
+    pg = min(ti, tk)
+    if pg == 0.0:
+        pg = max(ti, tk)
+    if damp == 0.0 or pg == 0.0:
+        return 1.0, 1.0, 1.0
+    a = pg * (r / damp) ** 3
+    if a >= 50.0:
+        return 1.0, 1.0, 1.0
+    e = np.exp(-a)
+    return 1.0 - e, 1.0 - (1.0 + a) * e, 1.0 - (1.0 + a + 0.6 * a * a) * e
+
+
+def pair_scales(ws):
+    """d, p and u scale of every pair [n,n], assigned as efld0_direct /
+    tmatxb_pme do (newinduce_pme.f:1062-1136, 1495-1518): p from the 1-2..1-5
+    lists (the intra-group value when the partner is in ip11), d and u from
+    the polarization-group lists ip11..ip14."""
+    n = ws.n
+    d = np.ones((n, n))
+    p = np.ones((n, n))
+    u = np.ones((n, n))
+
+    def partners(name, i):
+        off, idx = ws.conn[name]
+        return idx[off[i]:off[i + 1]]
+
+    for i in range(n):
+        ip11 = set(partners("ip11", i).tolist())
+        for b, name in enumerate(("i12", "i13", "i14", "i15")):
+            for k in partners(name, i):
+                p[i, k] = ws.scales["pi_scale"][b] if k in ip11 else ws.scales["p_scale"][b]
+        for b, name in enumerate(("ip11", "ip12", "ip13", "ip14")):
+            for k in partners(name, i):
+                d[i, k] = ws.scales["d_scale"][b]
+                u[i, k] = ws.scales["u_scale"][b]
+    return d, p, u
+
+
+def isolated_epol(ws, rpole, electric=332.063714):
+    """Polarization energy of the same molecules in vacuum (no periodic
+    images, no cutoff): the permanent field of charges, dipoles and
+    quadrupoles with Thole damping and the pair scales, a dense solve of
+    (1/alpha - T) mu = E for the d and p dipoles, and Epol = -1/2 electric
+    sum mu_d . E_p."""
+    n = ws.n
+    pos = ws.positions()
+    q = rpole[:, 0]
+    dp = rpole[:, 1:4]
+    Q = rpole[:, 4:13].reshape(n, 3, 3)
+    ds, ps, us = pair_scales(ws)
+    E = np.zeros((2, n, 3))
+    T = np.zeros((3 * n, 3 * n))
+    for i in range(n):
+        for k in range(n):
+            if i == k:
+                continue
+            x = pos[k] - pos[i]
+            r2 = x @ x
+            r = np.sqrt(r2)
+            rr3 = 1.0 / (r * r2)
+            rr5 = 3.0 * rr3 / r2
+            rr7 = 5.0 * rr5 / r2
+            l3, l5, l7 = _thole(ws.pdamp[i], ws.pdamp[k], ws.thole[i], ws.thole[k], r)
+            dkr = dp[k] @ x
+            qk = Q[k] @ x
+            qkr = x @ qk
+            for t, s in enumerate((ds[i, k], ps[i, k])):
+                d3, d5, d7 = s * l3 * rr3, s * l5 * rr5, s * l7 * rr7
+                rad = d3 * q[k] - d5 * dkr + d7 * qkr
+                E[t, i] += -x * rad - d3 * dp[k] + 2.0 * d5 * qk
+            s = us[i, k]
+            T[3 * i:3 * i + 3, 3 * k:3 * k + 3] = s * l5 * rr5 * np.outer(x, x) - s * l3 * rr3 * np.eye(3)
+    A = np.diag(np.repeat(1.0 / ws.polarity, 3)) - T
+    mu_d = np.linalg.solve(A, E[0].ravel()).reshape(n, 3)
+    return -0.5 * electric * np.sum(mu_d * E[1])

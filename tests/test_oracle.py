@@ -246,3 +246,38 @@ def test_energy_independent_of_ewald_alpha(thp):
         es.append(orc.epolar(res["uind"])[0])
     es = np.array(es)
     assert (es.max() - es.min()) < 3e-6 * abs(es.mean()), es
+
+
+def test_two_waters_reach_the_isolated_limit(thp):
+    # Two waters at a hydrogen-bond distance in growing periodic boxes: the
+    # Ewald/PME energy differs from the vacuum energy (direct summation, no
+    # images, tests/ewald_ref.py) by the dipolar image term ~ 1/L^3; the two
+    # boxes' extrapolation reproduces the vacuum value.  Measured: 2.6e-3 and
+    # 1.1e-3 relative at L = 30, 40 A (ratio 2.35 for (40/30)^3 = 2.37), 1.8e-5
+    # after the extrapolation.
+    W = thp.water
+    R, th = W.R_OH, math.radians(W.THETA_HOH) / 2
+    h1 = np.array([R * math.sin(th), 0, R * math.cos(th)])
+    h2 = np.array([-R * math.sin(th), 0, R * math.cos(th)])
+
+    def rot(a, b):
+        ca, sa, cb, sb = math.cos(a), math.sin(a), math.cos(b), math.sin(b)
+        return np.array([[ca, -sa, 0], [sa, ca, 0], [0, 0, 1]]) @ np.array([[1, 0, 0], [0, cb, -sb], [0, sb, cb]])
+
+    o1 = np.array([0.3, -0.2, 0.1])
+    o2 = o1 + np.array([2.85, 0.4, -0.3])
+    xyz = np.array([o1, o1 + rot(0.3, 1.1) @ h1, o1 + rot(0.3, 1.1) @ h2,
+                    o2, o2 + rot(2.0, -0.7) @ h1, o2 + rot(2.0, -0.7) @ h2])
+    es = {}
+    for L in (30.0, 40.0):
+        ws = W._assemble(2, L, xyz, 0.5, 7.0, 0.5, None)
+        orc = O.Oracle(ws, poleps=1e-12)
+        assert orc.mlistcell()[0] == 0
+        res = orc.solve()
+        es[L] = orc.epolar(res["uind"])[0]
+        if L == 30.0:
+            eiso = ewald_ref.isolated_epol(ws, orc.rpole)
+    ratio = (es[30.0] - eiso) / (es[40.0] - eiso)
+    assert abs(ratio / (40.0 / 30.0) ** 3 - 1.0) < 0.03, ratio
+    einf = (es[40.0] * 40.0 ** 3 - es[30.0] * 30.0 ** 3) / (40.0 ** 3 - 30.0 ** 3)
+    assert abs(einf - eiso) < 5e-5 * abs(eiso), (einf, eiso)

@@ -182,7 +182,12 @@ __device__ __forceinline__ int axis_cells(int c, int nc, int q) {
   return nc <= 5 ? q : ((c + q - 2) % nc + nc) % nc;
 }
 
-__global__ void __launch_bounds__(128) k_build_list(int n, int npad, Box box, double mbuf2, int prefilter,
+// minimum resident blocks per SM asked of the compiler (0: its own choice)
+#ifndef THP_LIST_MINB
+#define THP_LIST_MINB 0
+#endif
+
+__global__ void __launch_bounds__(128, THP_LIST_MINB) k_build_list(int n, int npad, Box box, double mbuf2, int prefilter,
                                                     float lo, float hi, int ncx,
                                                     int ncy, int ncz, const double4* __restrict__ pos,
                                                     const float4* __restrict__ posf, const int* __restrict__ scell,

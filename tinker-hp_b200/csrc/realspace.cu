@@ -56,8 +56,13 @@ struct Rec<true> {  // FP32 record of the mixed form
   }
 };
 
+// minimum resident blocks per SM asked of the compiler (0: its own choice)
+#ifndef THP_EFLD0_MINB
+#define THP_EFLD0_MINB 0
+#endif
+
 template <bool MIXED, bool FIELD>
-__global__ void __launch_bounds__(kBlock) k_efld0_coef(
+__global__ void __launch_bounds__(kBlock, THP_EFLD0_MINB) k_efld0_coef(
     int n, int npad, Box box, double cut2, EwaldConst ew, const double4* __restrict__ pos,
     const double* __restrict__ mrec, const float* __restrict__ mrecf, const int* __restrict__ perm,
     const int* __restrict__ sp_off, const int* __restrict__ sp_ks, const double* __restrict__ sp_s,

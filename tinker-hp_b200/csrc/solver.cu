@@ -31,6 +31,11 @@
 #define THP_DEVICE_LOOP 1
 #endif
 
+// minimum resident blocks per SM asked of the compiler for the real-space row
+#ifndef THP_ROW_MINB
+#define THP_ROW_MINB 0
+#endif
+
 #ifndef THP_OVERLAP_MIN_ATOMS
 #define THP_OVERLAP_MIN_ATOMS 20000
 #endif
@@ -181,7 +186,7 @@ __global__ void __launch_bounds__(256) k_pp_update(int n, int update, const doub
 
 // real-space part of h only: hreal = T_real x (tmatxb_pme without the diagonal)
 template <bool MIXED>
-__global__ void __launch_bounds__(kBlock) k_real_row(PairRows pr, Box box, const double4* __restrict__ pos,
+__global__ void __launch_bounds__(kBlock, THP_ROW_MINB) k_real_row(PairRows pr, Box box, const double4* __restrict__ pos,
                                                      const float4* __restrict__ posf, const double* __restrict__ x,
                                                      const float* __restrict__ xf, const CgScalars* __restrict__ cg,
                                                      int check_stop, double* __restrict__ hreal) {
