@@ -362,7 +362,6 @@ def main():
         mixed.solve()
     barrier(world)
     torch.cuda.synchronize()
-    mixed.profile(1)
     ev0.record(stream)
     lat = []
     niter = []
@@ -373,10 +372,21 @@ def main():
         niter.append(r["niter"])
     ev1.record(stream)
     torch.cuda.synchronize()
-    mv_ms, mv_launches = mixed.profile(0)
     barrier(world)
     t_mixed = allreduce_max(ev0.elapsed_time(ev1), world)
     clk = clocks.stop()
+    # roofline of the real-space row: its launches are event-timed in a
+    # separate pass (the event-timed path runs without the device-side loop
+    # graph, so it stays out of the timed region above)
+    mixed.profile(1)
+    work_launches = 0
+    for _ in range(3):
+        mixed.invalidate_list()
+        work_launches += mixed.solve()["niter"] + 1  # the initial matvec and one per iteration
+    mv_ms, mv_launches = mixed.profile(0)
+    # launches enqueued after the stop flag return at entry (a few us each);
+    # the average is taken over the launches that did the work
+    mv_launches = max(1, min(mv_launches, work_launches))
 
     # ---- FP64 form on the same box
     fp64_line = None
