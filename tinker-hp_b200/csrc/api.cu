@@ -275,6 +275,9 @@ void free_ctx(Ctx& c) {
   pme_free(c);
   if (c.chunk_exec) cudaGraphExecDestroy(c.chunk_exec);
   if (c.loop_exec) cudaGraphExecDestroy(c.loop_exec);
+  for (auto& row : c.front_exec)
+    for (auto& ex : row)
+      if (ex) cudaGraphExecDestroy(ex);
   pinned_give(c);
   if (c.ev_fork) cudaEventDestroy(c.ev_fork);
   if (c.ev_join) cudaEventDestroy(c.ev_join);
@@ -282,6 +285,18 @@ void free_ctx(Ctx& c) {
   if (c.ev0) cudaEventDestroy(c.ev0);
   if (c.ev1) cudaEventDestroy(c.ev1);
   if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+}
+
+// graphs that hold a system's structure (rotpole on/off, special pairs,
+// sizes) are dropped when it changes
+static void drop_front_graphs(Ctx& c) {
+  for (auto& row : c.front_exec)
+    for (auto& ex : row)
+      if (ex) {
+        cudaGraphExecDestroy(ex);
+        ex = nullptr;
+      }
+  c.front_failed = false;
 }
 
 size_t footprint_bytes(const thp_config& cfg, int* ncell_out) {
@@ -521,6 +536,7 @@ int thp_ctx_reset(thp_ctx* h, const thp_config* cfg) {
   if (c.loop_exec) cudaGraphExecDestroy(c.loop_exec);
   c.chunk_exec = c.loop_exec = nullptr;
   c.loop_state = 0;
+  drop_front_graphs(c);
   for (cudaEvent_t e : c.prof_events) cudaEventDestroy(e);
   c.prof_events.clear();
   c.profiling = false;
@@ -589,6 +605,7 @@ int thp_set_params(thp_ctx* h, const double* polarity, const double* thole, cons
 int thp_set_connectivity(thp_ctx* h, const int* const* off, const int* const* idx, const double* scales) {
   if (!h || !scales) return THP_E_INVALID;
   Ctx& c = h->c;
+  drop_front_graphs(c);
   if (set_current_device(c)) return THP_E_CUDA;
   std::memcpy(c.scales, scales, sizeof(c.scales));
   build_special_pairs(c, off, idx, scales);
@@ -619,6 +636,7 @@ int thp_set_positions(thp_ctx* h, const double* x, const double* y, const double
 int thp_set_rpole(thp_ctx* h, const double* rpole) {
   if (!h || !rpole) return THP_E_INVALID;
   Ctx& c = h->c;
+  drop_front_graphs(c);
   if (set_current_device(c)) return THP_E_CUDA;
   cudaMemcpyAsync(c.d_rpole_orig, rpole, sizeof(double) * 13 * c.n, cudaMemcpyHostToDevice, c.stream);
   c.have_rpole = true;
@@ -631,6 +649,7 @@ int thp_set_rpole(thp_ctx* h, const double* rpole) {
 int thp_set_frames(thp_ctx* h, const double* pole, const int* zaxis, const int* xaxis, const int* axt) {
   if (!h || !pole || !zaxis || !xaxis || !axt) return THP_E_INVALID;
   Ctx& c = h->c;
+  drop_front_graphs(c);
   if (set_current_device(c)) return THP_E_CUDA;
   const int n = c.n;
   std::vector<int> fr(3 * (size_t)n);
@@ -758,7 +777,7 @@ int thp_solve(thp_ctx* h, int guess, thp_solve_info* info) {
 
 // E0 and the CG start of one system, fully asynchronous (forced list
 // rebuild, no host read-back); the overflow flags are checked after the solve.
-static int solve_front_async(thp_ctx* h, int guess) {
+static int solve_front_eager(thp_ctx* h, int guess) {
   Ctx& c = h->c;
   int st;
   if (c.have_frames) {
@@ -777,6 +796,51 @@ static int solve_front_async(thp_ctx* h, int guess) {
   if ((st = resolve_predict(c, &guess))) return st;
   return pcg_begin(c, guess);
 }
+
+#ifndef THP_FRONT_GRAPH
+#define THP_FRONT_GRAPH 1
+#endif
+
+// The front of a batched solve (rotpole, sort, list, fields, CG start) as one
+// CUDA graph per guess mode and per whether the last dipoles follow a
+// re-sort, captured on first use: a batch of many small systems would
+// otherwise spend its time in the host's launch calls.  The predictor's
+// guess (host-side coefficients) and profiling take the eager path.
+static int solve_front_async(thp_ctx* h, int guess) {
+  Ctx& c = h->c;
+  const int keep_mu = (c.have_perm && c.have_dipoles) ? 1 : 0;
+  if (!THP_FRONT_GRAPH || guess < THP_GUESS_DIRECT || guess > THP_GUESS_HOST || c.profiling || !c.stream ||
+      c.front_failed)
+    return solve_front_eager(h, guess);
+  cudaGraphExec_t& ex = c.front_exec[guess][keep_mu];
+  if (!ex) {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      c.front_failed = true;
+      cudaGetLastError();
+      return solve_front_eager(h, guess);
+    }
+    const int st = solve_front_eager(h, guess);
+    const cudaError_t e = cudaStreamEndCapture(c.stream, &g);
+    if (st || e != cudaSuccess || cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
+      ex = nullptr;
+      c.front_failed = true;
+      cudaGetLastError();
+      if (g) cudaGraphDestroy(g);
+      if (st) return st;
+      return solve_front_eager(h, guess);  // the refused capture did not run: run it now
+    }
+    cudaGraphDestroy(g);
+  }
+  // the host-side state the front leaves behind
+  if (c.have_frames) c.have_rpole = true;
+  c.have_perm = c.have_list = true;
+  h->pos_dirty = h->rpole_dirty = false;
+  h->field_valid = true;
+  return cuda_status(cudaGraphLaunch(ex, c.stream), &c, "front graph launch");
+}
+
+
 
 int thp_solve_batch(thp_ctx** hs, int count, int guess, thp_solve_info* infos) {
   if (!hs || count <= 0) return THP_E_INVALID;

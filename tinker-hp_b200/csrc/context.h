@@ -186,6 +186,9 @@ struct Ctx {
   // 0 not built yet, 1 built, -1 not available (the chunked graph is used)
   cudaGraphExec_t loop_exec = nullptr;
   int loop_state = 0;
+  // front of a batched solve per guess mode and dipole carry (api.cu)
+  cudaGraphExec_t front_exec[3][2] = {};
+  bool front_failed = false;
 
   // optional event pairs around the fused CG matvec launches
   bool profiling = false;
