@@ -236,6 +236,41 @@ def test_pair_set_bit_exact_large_box(lib, thp):
     np.testing.assert_array_equal(ctx.pairs(), orc.pairs())
 
 
+@pytest.fixture(scope="module")
+def large_case(thp):
+    ws = thp.water.make_water_box(10800, cfg=1)
+    orc = O.Oracle(ws, poleps=1e-6)
+    assert orc.mlistcell()[0] == 0
+    ref = orc.solve()
+    e_ref, _ = orc.epolar(ref["uind"])
+    return ws, ref, e_ref
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_solve_large_box_overlapped_rows(lib, large_case, precision):
+    # 32,400 atoms: the CG runs the real-space row on the side stream with the
+    # pair stream staged through shared memory, concurrent with the PME branch
+    ws, ref, e_ref = large_case
+    prec = lib.FP64 if precision == "fp64" else lib.MIXED
+    ctx = lib.Context(ws, precision=prec, poleps=1e-6)
+    res = ctx.solve()
+    uind, uinp = ctx.dipoles()
+    rms_d = np.sqrt(np.mean(np.sum((uind - ref["uind"]) ** 2, axis=1))) * DEBYE
+    rms_p = np.sqrt(np.mean(np.sum((uinp - ref["uinp"]) ** 2, axis=1))) * DEBYE
+    assert res["converged"]
+    if prec == lib.FP64:
+        assert res["niter"] == ref["niter"]
+        assert rms_d < 1e-6 and rms_p < 1e-6, (rms_d, rms_p)
+        assert abs(res["epol"] - e_ref) < 1e-8 * abs(e_ref), (res["epol"], e_ref)
+    else:
+        assert rms_d < 1e-5 and rms_p < 1e-5, (rms_d, rms_p)
+        assert abs(res["epol"] - e_ref) < 1e-5 * abs(e_ref)
+    # a repeat agrees up to the order of the grid atomics (FP64 / FP32)
+    ctx.solve()
+    u2, _ = ctx.dipoles()
+    assert rel(u2, uind) < (1e-9 if prec == lib.FP64 else 1e-4)
+
+
 def test_pair_set_cutoff_ties(lib, thp):
     # crafted pairs at r = 7.5 A exactly (kept, r^2 <= (7.0+0.5)^2) and one ulp
     # beyond (dropped), along x and across the periodic boundary

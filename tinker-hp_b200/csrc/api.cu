@@ -158,10 +158,72 @@ int check_flags(thp_ctx* h) {
 
 int set_current_device(Ctx& c) { return cuda_status(cudaSetDevice(c.device), &c, "set device"); }
 
+// Brings the sorted arrays up to date with the uploaded positions and
+// decides whether the list must be rebuilt: on the first call or when an atom
+// moved by more than lbuffer/2 since the last build (the reference rebuilds
+// every ineigup steps; the displacement test keeps the same interacting set).
+// On *rebuild the atoms are re-sorted, and the caller launches the build.
+static int prepare_list(thp_ctx* h, bool force_rebuild, bool* rebuild_out) {
+  Ctx& c = h->c;
+  int st;
+  if (!c.have_pos) return THP_E_STATE;
+  bool rebuild = force_rebuild || !c.have_list;
+  if (!rebuild && h->pos_dirty) {
+    if ((st = launch_gather_sorted(c))) return st;
+    double disp = 0.0;
+    if ((st = launch_max_displacement(c, &disp))) return st;
+    if (disp >= 0.5 * c.cfg.lbuffer) rebuild = true;
+    h->pos_dirty = false;
+    h->rpole_dirty = false;
+    c.have_coef = false;
+    h->field_valid = false;
+  }
+  if (rebuild) {
+    if ((st = launch_sort_atoms(c))) return st;
+    if ((st = launch_gather_sorted(c))) return st;
+    c.have_list = false;
+    c.have_coef = false;
+    h->field_valid = false;
+  } else if (h->pos_dirty || h->rpole_dirty) {
+    if ((st = launch_gather_sorted(c))) return st;
+    h->field_valid = false;
+  }
+  h->pos_dirty = false;
+  h->rpole_dirty = false;
+  *rebuild_out = rebuild;
+  return THP_OK;
+}
+
+// E0 = direct + reciprocal + self (newinduce_pme2.f:110-148) and the matvec
+// coefficients, after the list build when `build` is set.  A system whose CG
+// rows run on the side stream runs the list build and the direct pass there
+// too, concurrent with the spread and FFTs of the permanent multipoles on the
+// main stream; the gather that completes E0 follows the join.  Returns with
+// the main stream joined, on error as well.
+#ifndef THP_FRONT_OVERLAP
+#define THP_FRONT_OVERLAP 1
+#endif
+
+static int launch_fields(Ctx& c, bool build) {
+  int st;
+  if (!THP_FRONT_OVERLAP || !overlap_rows(c)) {
+    if (build && (st = launch_build_list(c))) return st;
+    if ((st = launch_efld0_coef(c, true))) return st;
+    return launch_efld0_recip(c);
+  }
+  cudaEventRecord(c.ev_fork, c.stream);
+  cudaStreamWaitEvent(c.stream2, c.ev_fork, 0);
+  st = build ? launch_build_list_on(c, c.stream2) : THP_OK;
+  if (!st) st = launch_efld0_coef_on(c, true, c.stream2);
+  cudaEventRecord(c.ev_join, c.stream2);
+  int st2 = launch_mpole_grid(c);
+  cudaStreamWaitEvent(c.stream, c.ev_join, 0);
+  if (st || st2) return st ? st : st2;
+  return launch_gather_mpole(c, nullptr, true);
+}
+
 // Ensures the sorted arrays match the uploaded positions and the list is
-// valid: full rebuild on the first call or when an atom moved by more than
-// lbuffer/2 since the last build (the reference rebuilds every ineigup steps;
-// the displacement test keeps the same interacting set).
+// valid (see prepare_list).
 int ensure_list(thp_ctx* h, bool force_rebuild) {
   Ctx& c = h->c;
   int st;
@@ -213,9 +275,10 @@ int compute_field(thp_ctx* h) {
   Ctx& c = h->c;
   int st;
   if ((st = ensure_rpole(h))) return st;
-  if ((st = ensure_list(h, false))) return st;
-  if ((st = launch_efld0_coef(c, true))) return st;
-  if ((st = launch_efld0_recip(c))) return st;
+  bool rebuild = false;
+  if ((st = prepare_list(h, false, &rebuild))) return st;
+  if ((st = launch_fields(c, rebuild))) return st;
+  c.have_list = true;
   if ((st = check_flags(h))) return st;
   h->field_valid = true;
   return THP_OK;
@@ -315,7 +378,7 @@ size_t footprint_bytes(const thp_config& cfg, int* ncell_out) {
   b += n * 4 + maxnb * npad * 4;                         // list
   b += n * 4 + maxnb * npad * (4 + 2 * (mixed ? 4 : 8));  // pairs
   b += ngrid * (mixed ? 12 : 24);                        // grid + qfac
-  b += 9 * n * 6 * 8 + 4 * n * 8 + n * 6 * 4;            // vectors
+  b += 9 * n * 6 * 8 + 4 * n * 8 + n * 6 * 4 + n * 9 * 4;  // vectors, FP32 row input
   b += (n / 128 + 2) * 4 * 8 + 4096;
   b += 64 << 20;  // cuFFT work area and runtime slack
   return b;
@@ -451,7 +514,8 @@ static int size_buffers(Ctx& c) {
                      item(&c.d_nnb, n), item(&c.d_npr, n), item(&c.d_ef, 6 * n), item(&c.d_mu, 6 * n),
                      item(&c.d_res, 6 * n), item(&c.d_h, 6 * n), item(&c.d_pp, 6 * n), item(&c.d_zr, 6 * n),
                      item(&c.d_dip, 6 * n), item(&c.d_tmp6, 6 * n), item(&c.d_tmp6b, 6 * n), item(&c.d_cphi, 4 * n),
-                     item(&c.d_vecf, 6 * n), item(&c.d_partials, (size_t)(c.nblk_reduce + 8) * 4)},
+                     item(&c.d_vecf, 6 * n), item(&c.d_rec, 8 * n), item(&c.d_mpz, n),
+                     item(&c.d_partials, (size_t)(c.nblk_reduce + 8) * 4)},
                     "per-atom buffers");
     if (!st) c.cap_n = n;
   }
@@ -786,12 +850,10 @@ static int solve_front_eager(thp_ctx* h, int guess) {
   }
   if ((st = launch_sort_atoms(c))) return st;
   if ((st = launch_gather_sorted(c))) return st;
-  if ((st = launch_build_list(c))) return st;
-  c.have_list = true;
   h->pos_dirty = false;
   h->rpole_dirty = false;
-  if ((st = launch_efld0_coef(c, true))) return st;
-  if ((st = launch_efld0_recip(c))) return st;
+  if ((st = launch_fields(c, true))) return st;
+  c.have_list = true;
   h->field_valid = true;
   if ((st = resolve_predict(c, &guess))) return st;
   return pcg_begin(c, guess);

@@ -141,6 +141,10 @@ struct Ctx {
   double* d_dip = nullptr;
   double* d_cphi = nullptr;   // [n][4] permanent potential and gradient (Cartesian)
   float* d_vecf = nullptr;    // mixed form matvec input [n][6]
+  // mixed form matvec input of the overlapped CG rows: per atom one 32-byte
+  // record {x, y, z (wrapped), d dipole, p dipole x, y} and the p dipole z
+  float* d_rec = nullptr;     // [n][8]
+  float* d_mpz = nullptr;     // [n]
   double* d_tmp6 = nullptr;   // [n][6] original-order staging for host I/O
   double* d_tmp6b = nullptr;
   bool have_dipoles = false;

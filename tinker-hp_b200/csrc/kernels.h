@@ -8,13 +8,15 @@ namespace thp {
 // nblist.cu
 int launch_sort_atoms(Ctx& c);          // cell sort, permutation, sorted copies
 int launch_gather_sorted(Ctx& c);       // positions/params/rpole into sorted order
-int launch_build_list(Ctx& c);          // full list within ewaldcut + lbuffer
+int launch_build_list(Ctx& c);
+int launch_build_list_on(Ctx& c, cudaStream_t s);          // full list within ewaldcut + lbuffer
 int launch_export_list(Ctx& c, int maxelst, int* d_nelst, int* d_elst);
 int launch_rotpole(Ctx& c);             // local-frame multipoles -> d_rpole_orig
 int launch_max_displacement(Ctx& c, double* h_out);
 
 // realspace.cu
-int launch_efld0_coef(Ctx& c, bool with_field);  // direct field into d_ef, coefficients
+int launch_efld0_coef(Ctx& c, bool with_field);
+int launch_efld0_coef_on(Ctx& c, bool with_field, cudaStream_t s);  // direct field into d_ef, coefficients
 int launch_tmatxb(Ctx& c, const double* d_in, double* d_out, bool dodiag);  // sorted [n][6]
 
 // pme.cu
@@ -24,6 +26,8 @@ void pme_free(Ctx& c);
 int launch_efld0_recip(Ctx& c);         // d_cphi and E0 completion
 int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0);
 int launch_mpole_grid(Ctx& c);          // permanent-multipole grid, convolved (grid holds the potential)
+int launch_gather_mpole(Ctx& c, double* cphi10, bool with_e0);  // cphi from the convolved grid, E0 completion
+bool overlap_rows(const Ctx& c);  // the system runs real-space passes on the side stream
 int zero_grid(Ctx& c);
 struct PmeGeom;
 PmeGeom pme_geom(const Ctx& c);

@@ -386,7 +386,9 @@ int launch_gather_sorted(Ctx& c) {
   return cuda_status(cudaGetLastError(), &c, "gather sorted");
 }
 
-int launch_build_list(Ctx& c) {
+int launch_build_list(Ctx& c) { return launch_build_list_on(c, c.stream); }
+
+int launch_build_list_on(Ctx& c, cudaStream_t s) {
   const int n = c.n;
   const double rl = c.cfg.ewaldcut + c.cfg.lbuffer;
   const double mbuf2 = rl * rl;
@@ -399,10 +401,10 @@ int launch_build_list(Ctx& c) {
   const double dr = 1.7320508075688772 * 4.0 * lmax * 5.9604644775390625e-08;
   const double band = std::max(1e-5, 2.0 * (2.0 * rl * dr + dr * dr) / mbuf2);
   const float lo = (float)(mbuf2 * (1.0 - band)), hi = (float)(mbuf2 * (1.0 + band));
-  k_build_list<<<(n + 127) / 128, 128, 0, c.stream>>>(
+  k_build_list<<<(n + 127) / 128, 128, 0, s>>>(
       n, c.npad, c.box, mbuf2, prefilter, lo, hi, c.nc[0], c.nc[1], c.nc[2], c.d_pos, c.d_posf, c.d_scell, c.d_cell_start,
       c.d_cell_count, c.maxnb, c.d_nnb, c.d_nb, c.d_flags);
-  cudaMemcpyAsync(c.d_pos_built, c.d_pos, sizeof(double4) * n, cudaMemcpyDeviceToDevice, c.stream);
+  cudaMemcpyAsync(c.d_pos_built, c.d_pos, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
   return cuda_status(cudaGetLastError(), &c, "build list");
 }
 

@@ -584,10 +584,14 @@ int launch_mpole_grid(Ctx& c) {
 }
 
 int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0) {
-  PmeGeom g = geom_of(c);
-  int nb = (c.n + kBlock - 1) / kBlock;
   int st = launch_mpole_grid(c);
   if (st) return st;
+  return launch_gather_mpole(c, cphi10, with_e0);
+}
+
+int launch_gather_mpole(Ctx& c, double* cphi10, bool with_e0) {
+  PmeGeom g = geom_of(c);
+  int nb = (c.n + kBlock - 1) / kBlock;
   double a = c.cfg.aewald;
   double term = (4.0 / 3.0) * a * a * a / kSqrtPi;
   if (c.mixed)

@@ -259,7 +259,9 @@ PairRows pair_rows(const Ctx& c) {
   return pr;
 }
 
-int launch_efld0_coef(Ctx& c, bool with_field) {
+int launch_efld0_coef(Ctx& c, bool with_field) { return launch_efld0_coef_on(c, with_field, c.stream); }
+
+int launch_efld0_coef_on(Ctx& c, bool with_field, cudaStream_t s) {
   const int nb = (c.n + kBlock - 1) / kBlock;
   const double cut2 = c.cfg.ewaldcut * c.cfg.ewaldcut;
   EwaldConst ew = ewald_const(c.cfg.aewald);
@@ -268,14 +270,14 @@ int launch_efld0_coef(Ctx& c, bool with_field) {
       c.d_nb, c.maxnb, c.d_npr, c.d_pk, c.d_pc3, c.d_pc5, c.maxpr, c.d_ef, c.d_flags
   if (c.mixed) {
     if (with_field)
-      k_efld0_coef<true, true><<<nb, kBlock, 0, c.stream>>>(THP_EFLD0_ARGS);
+      k_efld0_coef<true, true><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS);
     else
-      k_efld0_coef<true, false><<<nb, kBlock, 0, c.stream>>>(THP_EFLD0_ARGS);
+      k_efld0_coef<true, false><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS);
   } else {
     if (with_field)
-      k_efld0_coef<false, true><<<nb, kBlock, 0, c.stream>>>(THP_EFLD0_ARGS);
+      k_efld0_coef<false, true><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS);
     else
-      k_efld0_coef<false, false><<<nb, kBlock, 0, c.stream>>>(THP_EFLD0_ARGS);
+      k_efld0_coef<false, false><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS);
   }
 #undef THP_EFLD0_ARGS
   c.have_coef = true;

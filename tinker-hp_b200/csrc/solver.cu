@@ -168,27 +168,48 @@ __global__ void __launch_bounds__(kBlock) k_cg_matvec(PairRows pr, Box box, cons
   }
 }
 
-// pp = zr + beta pp (newinduce_pme2.f:553-559) and, for the mixed form, the
-// FP32 copy the real-space row reads; update 0 only writes the copy of x.
-__global__ void __launch_bounds__(256) k_pp_update(int n, int update, const double* __restrict__ zr,
-                                                  double* __restrict__ x, float* __restrict__ xf,
+// pp = zr + beta pp (newinduce_pme2.f:553-559) of the overlapped FP64 rows.
+__global__ void __launch_bounds__(256) k_pp_update(int n, const double* __restrict__ zr, double* __restrict__ x,
                                                   const CgScalars* __restrict__ cg) {
-  if (update && cg->stop) return;
+  if (cg->stop) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 6 * n) return;
-  double v = x[t];
+  x[t] = zr[t] + cg->beta[(t % 6) < 3 ? 0 : 1] * x[t];
+}
+
+// The same update for the overlapped rows of the mixed form, which read the
+// FP32 dipoles from the per-atom records (rec, mpz) with the wrapped FP32
+// position beside them; one thread per atom.  update 0 only writes the
+// records of x.
+__global__ void __launch_bounds__(256) k_pp_rec(int n, int update, const double* __restrict__ zr,
+                                               double* __restrict__ x, const float4* __restrict__ posf,
+                                               float* __restrict__ rec, float* __restrict__ mpz,
+                                               const CgScalars* __restrict__ cg) {
+  if (update && cg->stop) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v[6];
+  load6(x + (size_t)i * 6, v);
   if (update) {
-    v = zr[t] + cg->beta[(t % 6) < 3 ? 0 : 1] * v;
-    x[t] = v;
+    double z[6];
+    load6(zr + (size_t)i * 6, z);
+    const double bd = cg->beta[0], bp = cg->beta[1];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) v[q] = z[q] + (q < 3 ? bd : bp) * v[q];
+    store6(x + (size_t)i * 6, v);
   }
-  if (xf) xf[t] = (float)v;
+  const float4 p = posf[i];
+  float4* r = reinterpret_cast<float4*>(rec + (size_t)i * 8);
+  r[0] = make_float4(p.x, p.y, p.z, (float)v[0]);
+  r[1] = make_float4((float)v[1], (float)v[2], (float)v[3], (float)v[4]);
+  mpz[i] = (float)v[5];
 }
 
 // real-space part of h only: hreal = T_real x (tmatxb_pme without the diagonal)
 template <bool MIXED>
 __global__ void __launch_bounds__(kBlock, THP_ROW_MINB) k_real_row(PairRows pr, Box box, const double4* __restrict__ pos,
-                                                     const float4* __restrict__ posf, const double* __restrict__ x,
-                                                     const float* __restrict__ xf, const CgScalars* __restrict__ cg,
+                                                     const float* __restrict__ rec, const double* __restrict__ x,
+                                                     const float* __restrict__ mpz, const CgScalars* __restrict__ cg,
                                                      int check_stop, double* __restrict__ hreal) {
   if (check_stop && cg->stop) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -196,7 +217,7 @@ __global__ void __launch_bounds__(kBlock, THP_ROW_MINB) k_real_row(PairRows pr, 
   double acc[6];
   if (MIXED) {
     float a32[6] = {0, 0, 0, 0, 0, 0};
-    tmatxb_row32(pr, (float)box.l[0], (float)box.l[1], (float)box.l[2], i, posf, xf, a32);
+    tmatxb_row32_rec(pr, (float)box.l[0], (float)box.l[1], (float)box.l[2], i, rec, mpz, a32);
 #pragma unroll
     for (int q = 0; q < 6; ++q) acc[q] = (double)a32[q];
   } else {
@@ -399,7 +420,8 @@ static void prof_mark(Ctx& c, cudaStream_t s) {
   c.prof_events.push_back(e);
 }
 
-static bool overlapped(const Ctx& c) { return c.n >= THP_OVERLAP_MIN_ATOMS; }
+bool overlap_rows(const Ctx& c) { return c.n >= THP_OVERLAP_MIN_ATOMS; }
+static bool overlapped(const Ctx& c) { return overlap_rows(c); }
 
 // One application of the CG matrix with the real-space row on the side
 // stream and the PME branch (spread, FFTs, gather) on the main stream; x and,
@@ -412,9 +434,9 @@ static int matvec_overlapped(Ctx& c, double* x, int init) {
   PairRows pr = pair_rows(c);
   prof_mark(c, c.stream2);
   if (c.mixed)
-    k_real_row<true><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_posf, x, c.d_vecf, c.d_cg, !init, c.d_h);
+    k_real_row<true><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, x, c.d_mpz, c.d_cg, !init, c.d_h);
   else
-    k_real_row<false><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_posf, x, c.d_vecf, c.d_cg, !init, c.d_h);
+    k_real_row<false><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, nullptr, x, nullptr, c.d_cg, !init, c.d_h);
   prof_mark(c, c.stream2);
   if ((st = cuda_status(cudaGetLastError(), &c, "real row"))) return st;
   cudaEventRecord(c.ev_join, c.stream2);
@@ -451,8 +473,10 @@ static int launch_matvec(Ctx& c, const double* x, int init) {
 static int enqueue_iteration(Ctx& c) {
   int st;
   if (overlapped(c)) {
-    k_pp_update<<<(6 * c.n + 255) / 256, 256, 0, c.stream>>>(c.n, 1, c.d_zr, c.d_pp, c.mixed ? c.d_vecf : nullptr,
-                                                            c.d_cg);
+    if (c.mixed)
+      k_pp_rec<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, 1, c.d_zr, c.d_pp, c.d_posf, c.d_rec, c.d_mpz, c.d_cg);
+    else
+      k_pp_update<<<(6 * c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.d_zr, c.d_pp, c.d_cg);
     if ((st = cuda_status(cudaGetLastError(), &c, "pp update"))) return st;
     if ((st = matvec_overlapped(c, c.d_pp, 0))) return st;
   } else {
@@ -474,7 +498,7 @@ int pcg_begin(Ctx& c, int guess) {
   }
   if (overlapped(c)) {
     if (c.mixed) {
-      k_pp_update<<<(6 * c.n + 255) / 256, 256, 0, c.stream>>>(c.n, 0, c.d_zr, c.d_mu, c.d_vecf, c.d_cg);
+      k_pp_rec<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, 0, c.d_zr, c.d_mu, c.d_posf, c.d_rec, c.d_mpz, c.d_cg);
       if ((st = cuda_status(cudaGetLastError(), &c, "mu copy"))) return st;
     }
     return matvec_overlapped(c, c.d_mu, 1);
