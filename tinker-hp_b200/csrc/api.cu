@@ -374,7 +374,7 @@ size_t footprint_bytes(const thp_config& cfg, int* ncell_out) {
   size_t b = 0;
   b += 3 * ncell * 4 + 2 * n * 4 + 2 * n * 4;          // cells, perm
   b += (3 + 3 + 13 + 13) * n * 8 + 3 * n * 4;            // staging
-  b += n * 32 + n * 16 + 2 * n * 8 + 10 * n * 8 + n * 32;  // sorted data
+  b += n * 32 + n * 16 + 2 * n * 8 + 10 * n * 8 + n * 32 + n * 64;  // sorted data
   b += n * 4 + maxnb * npad * 4;                         // list
   b += n * 4 + maxnb * npad * (4 + 2 * (mixed ? 4 : 8));  // pairs
   b += ngrid * (mixed ? 12 : 24);                        // grid + qfac
@@ -510,7 +510,7 @@ static int size_buffers(Ctx& c) {
                      item(&c.d_xyz_orig, 3 * n), item(&c.d_par_orig, 3 * n), item(&c.d_rpole_orig, 13 * n),
                      item(&c.d_pole_local, 13 * n), item(&c.d_frames, 3 * n), item(&c.d_pos, n),
                      item(&c.d_posf, n), item(&c.d_thole, n), item(&c.d_pol, n), item(&c.d_rpole, 10 * n),
-                     item(&c.d_mrec, 12 * n), item(&c.d_mrecf, 12 * n), item(&c.d_pos_built, n),
+                     item(&c.d_mrec, 12 * n), item(&c.d_mrecf, 12 * n), item(&c.d_erec, 16 * n), item(&c.d_pos_built, n),
                      item(&c.d_nnb, n), item(&c.d_npr, n), item(&c.d_ef, 6 * n), item(&c.d_mu, 6 * n),
                      item(&c.d_res, 6 * n), item(&c.d_h, 6 * n), item(&c.d_pp, 6 * n), item(&c.d_zr, 6 * n),
                      item(&c.d_dip, 6 * n), item(&c.d_tmp6, 6 * n), item(&c.d_tmp6b, 6 * n), item(&c.d_cphi, 4 * n),

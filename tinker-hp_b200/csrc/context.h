@@ -100,6 +100,7 @@ struct Ctx {
   double* d_rpole = nullptr;      // [n][10]: q, d(3), Qxx,Qxy,Qxz,Qyy,Qyz,Qzz
   double* d_mrec = nullptr;       // [n][12]: thole, q, d(3), Q(6), 0 -- pair-pass record (96 B)
   float* d_mrecf = nullptr;       // [n][12] FP32 copy for the mixed form (48 B)
+  float* d_erec = nullptr;        // [n][16] mixed direct-field record (64 B, see k_gather_sorted)
   int* d_sp_ks = nullptr;         // special partners renumbered to sorted indices
   int* d_sp_off = nullptr;        // special pairs, ORIGINAL indices, CSR [n+1]
   int* d_sp_k = nullptr;

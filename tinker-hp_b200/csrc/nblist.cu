@@ -95,7 +95,8 @@ __global__ void k_gather_sorted(int n, Box box, const int* __restrict__ perm, co
                                 const double* __restrict__ pol, const double* __restrict__ rpole13,
                                 int have_rpole, double4* __restrict__ pos, float4* __restrict__ posf,
                                 double* __restrict__ sthole, double* __restrict__ spol,
-                                double* __restrict__ srpole, double* __restrict__ mrec, float* __restrict__ mrecf) {
+                                double* __restrict__ srpole, double* __restrict__ mrec, float* __restrict__ mrecf,
+                                float* __restrict__ erec) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   int o = perm[s];
@@ -135,6 +136,18 @@ __global__ void k_gather_sorted(int n, Box box, const int* __restrict__ perm, co
 #pragma unroll
     for (int k = 0; k < 3; ++k)
       f4[k] = make_float4((float)rec[4 * k], (float)rec[4 * k + 1], (float)rec[4 * k + 2], (float)rec[4 * k + 3]);
+  }
+  if (erec) {
+    // mixed direct-field record: wrapped position, 1/pdamp (0 for no
+    // damping), thole, charge, dipole, quadrupole
+    double wx = x, wy = y, wz = z;
+    image3(box, wx, wy, wz);
+    const double pd = pdamp[o];
+    float4* f4 = reinterpret_cast<float4*>(erec + (size_t)s * 16);
+    f4[0] = make_float4((float)wx, (float)wy, (float)wz, pd != 0.0 ? (float)(1.0 / pd) : 0.f);
+    f4[1] = make_float4((float)rec[0], (float)rec[1], (float)rec[2], (float)rec[3]);
+    f4[2] = make_float4((float)rec[4], (float)rec[5], (float)rec[6], (float)rec[7]);
+    f4[3] = make_float4((float)rec[8], (float)rec[9], (float)rec[10], 0.f);
   }
 }
 
@@ -382,7 +395,7 @@ int launch_gather_sorted(Ctx& c) {
                                                c.d_par_orig + n, c.d_par_orig + 2 * n, c.d_rpole_orig,
                                                c.have_rpole ? 1 : 0, c.d_pos, c.d_posf,
                                                c.d_thole, c.d_pol, c.d_rpole, c.d_mrec,
-                                               c.mixed ? c.d_mrecf : nullptr);
+                                               c.mixed ? c.d_mrecf : nullptr, c.mixed ? c.d_erec : nullptr);
   return cuda_status(cudaGetLastError(), &c, "gather sorted");
 }
 

@@ -56,6 +56,12 @@ struct Rec<true> {  // FP32 record of the mixed form
   }
 };
 
+// 1: the mixed form's pass runs k_efld0_coef32 (FP32 pair terms); 0: the
+// FP64-geometry pass shared with the FP64 form
+#ifndef THP_EFLD0_F32
+#define THP_EFLD0_F32 1
+#endif
+
 // minimum resident blocks per SM asked of the compiler (0: its own choice)
 #ifndef THP_EFLD0_MINB
 #define THP_EFLD0_MINB 0
@@ -184,6 +190,170 @@ __global__ void __launch_bounds__(kBlock, THP_EFLD0_MINB) k_efld0_coef(
   }
 }
 
+// Mixed form of the same pass, restated for FP32 throughout the pair terms:
+//   * partner data from one 64-byte record (two 256-bit loads): the wrapped
+//     FP32 position and 1/pdamp, thole, charge, dipole and quadrupole;
+//   * the displacement and the 7.0 A test in FP32 (only list pairs within
+//     ulps of the cutoff can change side; their terms are ~1e-10 of the
+//     field there);
+//   * the Thole argument as r * (1/pdamp_i) * (1/pdamp_k);
+//   * the special partners of the atom held in registers (the first
+//     kSpCache of them; a longer list is searched past those);
+//   * d and p fields computed once when the pair's two scales agree (every
+//     pair but the few special pairs with dscale != pscale);
+//   * FP32 field sums over runs of kFlush list entries, added into FP64.
+// The FP32 coefficients written for the CG rows follow the same formulas.
+constexpr int kSpCache = 4;
+constexpr int kFlush = 8;
+
+template <bool FIELD>
+__global__ void __launch_bounds__(kBlock, THP_EFLD0_MINB) k_efld0_coef32(
+    int n, int npad, float bx, float by, float bz, float cut2, EwaldConst ew, const float* __restrict__ erec,
+    const int* __restrict__ perm, const int* __restrict__ sp_off, const int* __restrict__ sp_ks,
+    const double* __restrict__ sp_s, const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb,
+    int* __restrict__ npr, int* __restrict__ pk_out, float* __restrict__ pc3, float* __restrict__ pc5, int maxpr,
+    double* __restrict__ ef, int* __restrict__ flags) {
+  constexpr int G = THP_EFLD0_G32;
+  static_assert(kFlush % G == 0, "flush runs are whole groups");
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 pi = *reinterpret_cast<const float4*>(erec + (size_t)i * 16);
+  const float thi = erec[(size_t)i * 16 + 4];
+  const int io = perm[i];
+  const int s0 = sp_off[io], s1 = sp_off[io + 1];
+  int spk[kSpCache];
+#pragma unroll
+  for (int v = 0; v < kSpCache; ++v) spk[v] = s0 + v < s1 ? __ldg(sp_ks + s0 + v) : -1;
+  const bool sp_more = s1 - s0 > kSpCache;
+  const float hx = 0.5f * bx, hy = 0.5f * by, hz = 0.5f * bz;
+  const float ea = (float)ew.a, af1 = (float)ew.afac1, af2 = (float)ew.afac2, af3 = (float)ew.afac3;
+  double e[6] = {0, 0, 0, 0, 0, 0};
+  const int nn = min(nnb[i], maxnb);
+  int cnt = 0;
+#pragma unroll 1
+  for (int sf = 0; sf < nn; sf += kFlush) {
+    float f[6] = {0, 0, 0, 0, 0, 0};
+    const int se = min(sf + kFlush, nn);
+#pragma unroll 1
+    for (int sb = sf; sb < se; sb += G) {
+      int kk[G];
+      float v[G][16];
+#pragma unroll
+      for (int g = 0; g < G; ++g) kk[g] = sb + g < se ? __ldg(nb + (size_t)(sb + g) * npad + i) : i;
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        ld_rec8(erec + (size_t)kk[g] * 16, *reinterpret_cast<float(*)[8]>(&v[g][0]));
+        ld_rec8(erec + (size_t)kk[g] * 16 + 8, *reinterpret_cast<float(*)[8]>(&v[g][8]));
+      }
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        if (sb + g >= se) break;
+        const int k = kk[g];
+        float x = v[g][0] - pi.x, y = v[g][1] - pi.y, z = v[g][2] - pi.z;
+        x = fabsf(x) > hx ? x - copysignf(bx, x) : x;
+        y = fabsf(y) > hy ? y - copysignf(by, y) : y;
+        z = fabsf(z) > hz ? z - copysignf(bz, z) : z;
+        const float r2 = x * x + y * y + z * z;
+        if (r2 > cut2) continue;
+        int q = -1;
+#pragma unroll
+        for (int w = 0; w < kSpCache; ++w)
+          if (spk[w] == k) q = s0 + w;
+        if (q < 0 && sp_more)
+          for (int w = s0 + kSpCache; w < s1; ++w)
+            if (__ldg(sp_ks + w) == k) {
+              q = w;
+              break;
+            }
+        float ds = 1.f, ps = 1.f, us = 1.f;
+        if (q >= 0) {
+          ds = (float)sp_s[3 * q];
+          ps = (float)sp_s[3 * q + 1];
+          us = (float)sp_s[3 * q + 2];
+        }
+        const float r = sqrtf(r2);
+        const float rr1 = 1.f / r;
+        const float rr2 = rr1 * rr1;
+        const float rr3 = rr2 * rr1;
+        const float rr5 = 3.f * rr2 * rr3;
+        const float rr7 = 5.f * rr2 * rr5;
+        // dampewald (order 7)
+        const float ra = ea * r;
+        const float bn0 = erfcf(ra) * rr1;
+        const float expterm = expf(-ra * ra);
+        const float bn1 = (bn0 + af1 * expterm) * rr2;
+        const float bn2 = (3.f * bn1 + af2 * expterm) * rr2;
+        const float bn3 = (5.f * bn2 + af3 * expterm) * rr2;
+        // dampthole / damptholed (AMOEBA branch)
+        float l3 = 1.f, l5 = 1.f, l7 = 1.f;
+        const float ipd = pi.w * v[g][3];
+        float pg = fminf(thi, v[g][4]);
+        if (pg == 0.f) pg = fmaxf(thi, v[g][4]);
+        if (ipd != 0.f && pg != 0.f) {
+          const float t = r * ipd;
+          const float damp = pg * (t * t * t);
+          if (damp < 50.f) {
+            const float ex = expf(-damp);
+            l3 = 1.f - ex;
+            l5 = 1.f - ex * (1.f + damp);
+            l7 = 1.f - ex * (1.f + damp + 0.6f * damp * damp);
+          }
+        }
+        if (FIELD) {
+          const float ck = v[g][5], dkx = v[g][6], dky = v[g][7], dkz = v[g][8];
+          const float qxx = v[g][9], qxy = v[g][10], qxz = v[g][11], qyy = v[g][12], qyz = v[g][13],
+                      qzz = v[g][14];
+          const float dkr = dkx * x + dky * y + dkz * z;
+          const float qkx = qxx * x + qxy * y + qxz * z;
+          const float qky = qxy * x + qyy * y + qyz * z;
+          const float qkz = qxz * x + qyz * y + qzz * z;
+          const float qkr = qkx * x + qky * y + qkz * z;
+          float dmp3 = bn1 - (1.f - ds * l3) * rr3;
+          float dmp5 = bn2 - (1.f - ds * l5) * rr5;
+          float dmp7 = bn3 - (1.f - ds * l7) * rr7;
+          float rad = dmp3 * ck - dmp5 * dkr + dmp7 * qkr;
+          const float fx = -x * rad - dmp3 * dkx + 2.f * dmp5 * qkx;
+          const float fy = -y * rad - dmp3 * dky + 2.f * dmp5 * qky;
+          const float fz = -z * rad - dmp3 * dkz + 2.f * dmp5 * qkz;
+          f[0] += fx;
+          f[1] += fy;
+          f[2] += fz;
+          if (ps == ds) {
+            f[3] += fx;
+            f[4] += fy;
+            f[5] += fz;
+          } else {
+            dmp3 = bn1 - (1.f - ps * l3) * rr3;
+            dmp5 = bn2 - (1.f - ps * l5) * rr5;
+            dmp7 = bn3 - (1.f - ps * l7) * rr7;
+            rad = dmp3 * ck - dmp5 * dkr + dmp7 * qkr;
+            f[3] += -x * rad - dmp3 * dkx + 2.f * dmp5 * qkx;
+            f[4] += -y * rad - dmp3 * dky + 2.f * dmp5 * qky;
+            f[5] += -z * rad - dmp3 * dkz + 2.f * dmp5 * qkz;
+          }
+        }
+        if (cnt < maxpr) {
+          const size_t o = (size_t)cnt * npad + i;
+          pk_out[o] = k;
+          pc3[o] = bn1 - (1.f - us * l3) * rr3;
+          pc5[o] = bn2 - (1.f - us * l5) * rr5;
+        }
+        ++cnt;
+      }
+    }
+    if (FIELD)
+#pragma unroll
+      for (int u = 0; u < 6; ++u) e[u] += (double)f[u];
+  }
+  npr[i] = min(cnt, maxpr);
+  if (cnt > maxpr) atomicOr(flags, DEV_PAIR_OVERFLOW);
+  if (FIELD) {
+    double* o = ef + (size_t)i * 6;
+#pragma unroll
+    for (int u = 0; u < 6; ++u) o[u] = e[u];
+  }
+}
+
 __global__ void __launch_bounds__(kBlock) k_tmatxb64(PairRows pr, Box box, const double4* __restrict__ pos,
                                                      const double* __restrict__ mu, const double* __restrict__ pol,
                                                      int dodiag, double* __restrict__ out) {
@@ -269,10 +439,22 @@ int launch_efld0_coef_on(Ctx& c, bool with_field, cudaStream_t s) {
   c.n, c.npad, c.box, cut2, ew, c.d_pos, c.d_mrec, c.d_mrecf, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_s, c.d_nnb, \
       c.d_nb, c.maxnb, c.d_npr, c.d_pk, c.d_pc3, c.d_pc5, c.maxpr, c.d_ef, c.d_flags
   if (c.mixed) {
+#if THP_EFLD0_F32
+    const float bx = (float)c.box.l[0], by = (float)c.box.l[1], bz = (float)c.box.l[2];
+#define THP_EFLD0_ARGS32                                                                                        \
+  c.n, c.npad, bx, by, bz, (float)cut2, ew, c.d_erec, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_s, c.d_nnb, c.d_nb, \
+      c.maxnb, c.d_npr, c.d_pk, (float*)c.d_pc3, (float*)c.d_pc5, c.maxpr, c.d_ef, c.d_flags
+    if (with_field)
+      k_efld0_coef32<true><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS32);
+    else
+      k_efld0_coef32<false><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS32);
+#undef THP_EFLD0_ARGS32
+#else
     if (with_field)
       k_efld0_coef<true, true><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS);
     else
       k_efld0_coef<true, false><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS);
+#endif
   } else {
     if (with_field)
       k_efld0_coef<false, true><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS);
