@@ -36,6 +36,12 @@
 #define THP_ROW_MINB 0
 #endif
 
+// 1: the overlapped matvec gathers the PME dipole field inside its combine
+// kernel, after the real-space row; 0: a separate gather beside the row
+#ifndef THP_GATHER_COMBINE
+#define THP_GATHER_COMBINE 1
+#endif
+
 #ifndef THP_OVERLAP_MIN_ATOMS
 #define THP_OVERLAP_MIN_ATOMS 20000
 #endif
@@ -229,8 +235,13 @@ __global__ void __launch_bounds__(kBlock, THP_ROW_MINB) k_real_row(PairRows pr, 
 }
 
 // h = hreal + x/alpha + dipfield(x) - term x, then the reductions of
-// k_cg_matvec (init: residual, zr, pp and ggold; iter: gg and alpha)
-__global__ void __launch_bounds__(kBlock) k_cg_combine(int n, const double* __restrict__ dipf,
+// k_cg_matvec (init: residual, zr, pp and ggold; iter: gg and alpha).
+// GATHER 0 reads dipfield from dipf; 1 / 2 gather it here from the
+// convolved FP32 / FP64 grid (the work of k_gather_dip, without the round
+// trip of dipfield through memory).
+template <int GATHER>
+__global__ void __launch_bounds__(kBlock) k_cg_combine(int n, const double* __restrict__ dipf, PmeGeom g,
+                                                       const double4* __restrict__ pos, const void* __restrict__ grid,
                                                        const double* __restrict__ x, const double* __restrict__ pol,
                                                        const double* __restrict__ ef, double term, int init,
                                                        double* __restrict__ h, double* __restrict__ res,
@@ -241,8 +252,13 @@ __global__ void __launch_bounds__(kBlock) k_cg_combine(int n, const double* __re
   double red[2] = {0.0, 0.0};
   if (i < n) {
     double acc[6], dip[6], xi[6];
+    if constexpr (GATHER == 1)
+      gather_dip<float>(g, pos[i], reinterpret_cast<const cufftComplex*>(grid), dip);
+    else if constexpr (GATHER == 2)
+      gather_dip<double>(g, pos[i], reinterpret_cast<const cufftDoubleComplex*>(grid), dip);
+    else
+      load6(dipf + (size_t)i * 6, dip);
     load6(h + (size_t)i * 6, acc);
-    load6(dipf + (size_t)i * 6, dip);
     load6(x + (size_t)i * 6, xi);
     const double p = pol[i];
     const double ip = (p == 0.0) ? 1.0 / kTinyPol : 1.0 / p;
@@ -441,12 +457,24 @@ static int matvec_overlapped(Ctx& c, double* x, int init) {
   if ((st = cuda_status(cudaGetLastError(), &c, "real row"))) return st;
   cudaEventRecord(c.ev_join, c.stream2);
   if ((st = launch_pme_dipole(c, x, nullptr, 2))) return st;
-  if ((st = launch_gather_dip(c, c.d_dip, true))) return st;
-  cudaStreamWaitEvent(c.stream, c.ev_join, 0);
   const double a = c.cfg.aewald;
   const double term = (4.0 / 3.0) * a * a * a / kSqrtPi;
-  k_cg_combine<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_dip, x, c.d_pol, c.d_ef, term, init, c.d_h, c.d_res, c.d_zr,
-                                            c.d_pp, c.d_cg, c.d_partials);
+  const PmeGeom g = pme_geom(c);
+#define THP_COMBINE_ARGS                                                                                        \
+  c.n, c.d_dip, g, c.d_pos, c.d_grid, x, c.d_pol, c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, c.d_cg, \
+      c.d_partials
+  if (THP_GATHER_COMBINE) {
+    cudaStreamWaitEvent(c.stream, c.ev_join, 0);
+    if (c.mixed)
+      k_cg_combine<1><<<nb, kBlock, 0, c.stream>>>(THP_COMBINE_ARGS);
+    else
+      k_cg_combine<2><<<nb, kBlock, 0, c.stream>>>(THP_COMBINE_ARGS);
+  } else {
+    if ((st = launch_gather_dip(c, c.d_dip, true))) return st;
+    cudaStreamWaitEvent(c.stream, c.ev_join, 0);
+    k_cg_combine<0><<<nb, kBlock, 0, c.stream>>>(THP_COMBINE_ARGS);
+  }
+#undef THP_COMBINE_ARGS
   return cuda_status(cudaGetLastError(), &c, "cg combine");
 }
 
