@@ -180,7 +180,10 @@ int thp_get_gradient_device(thp_ctx* ctx, double* d_dep);
 int thp_md_verlet(thp_ctx* ctx, int nsteps, double dt, const double* mass, double* vel,
                   double* energies, int* niters);
 int thp_get_positions(thp_ctx* ctx, double* x, double* y, double* z);
-/* one-call solve on host buffers (positions in, dipoles and energy out) */
+/* one-call solve on host buffers (positions in, dipoles and energy out).
+ * The buffers are copied as they are: pinned buffers are DMA'd.  Non-finite
+ * coordinates are detected on the device and return THP_E_INVALID, as
+ * thp_set_positions does on the host. */
 int thp_solve_host(thp_ctx* ctx, const double* x, const double* y, const double* z,
                    const double* rpole, double* uind, double* uinp, thp_solve_info* info);
 /* bytes of device memory a context of this configuration needs */
@@ -244,9 +247,11 @@ int thp_server_create(const thp_server_config* cfg, thp_server** out);
 /* Registers (or replaces) the system under key; copies every array and
  * plans the system's FFT shape ahead of its first request. */
 int thp_server_register(thp_server* s, unsigned long long key, const thp_system* sys);
-/* Queues one single-point solve of system key at positions x, y, z (copied).
- * uind/uinp [n][3] (may be NULL) receive the dipoles and must stay valid
- * until thp_server_wait returns for the ticket.  Admission: a system whose
+/* Queues one single-point solve of system key at positions x, y, z.  They
+ * are read when the request starts (pinned buffers are DMA'd); like
+ * uind/uinp [n][3] (may be NULL), which receive the dipoles, they must stay
+ * valid until thp_server_wait returns for the ticket.  Non-finite
+ * coordinates fail the request with THP_E_INVALID.  Admission: a system whose
  * footprint exceeds the budget fails at once with THP_E_OOM_ADMISSION; others
  * wait until enough idle systems are evicted.  An evicted system's context
  * goes to a pool and is re-targeted (thp_ctx_reset) for the next system

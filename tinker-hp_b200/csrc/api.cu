@@ -147,6 +147,10 @@ int check_flags(thp_ctx* h) {
   int f = *c.h_flags;
   if (f) {
     cudaMemsetAsync(c.d_flags, 0, sizeof(int), c.stream);
+    if (f & DEV_BAD_INPUT) {
+      c.last_msg = "non-finite coordinates";
+      return THP_E_INVALID;
+    }
     if (f & (DEV_LIST_OVERFLOW | DEV_PAIR_OVERFLOW)) {
       c.last_msg = "neighbor capacity exceeded";
       return THP_E_LIST_OVERFLOW;
@@ -679,13 +683,19 @@ int thp_set_connectivity(thp_ctx* h, const int* const* off, const int* const* id
   return upload_special_pairs(c);
 }
 
-int thp_set_positions(thp_ctx* h, const double* x, const double* y, const double* z) {
+// Uploads the coordinates; host_check rejects non-finite values before the
+// copy, otherwise the sorted gather flags them on the device and the next
+// flag check returns THP_E_INVALID.  (Also used by the request loop.)
+}  // extern "C"
+namespace thp {
+int upload_positions(thp_ctx* h, const double* x, const double* y, const double* z, bool host_check) {
   if (!h || !x || !y || !z) return THP_E_INVALID;
   Ctx& c = h->c;
   if (set_current_device(c)) return THP_E_CUDA;
   const size_t n = c.n;
-  for (size_t i = 0; i < n; ++i)
-    if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(z[i])) return THP_E_INVALID;
+  if (host_check)
+    for (size_t i = 0; i < n; ++i)
+      if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(z[i])) return THP_E_INVALID;
   cudaMemcpyAsync(c.d_xyz_orig, x, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
   cudaMemcpyAsync(c.d_xyz_orig + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
   cudaMemcpyAsync(c.d_xyz_orig + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
@@ -695,6 +705,12 @@ int thp_set_positions(thp_ctx* h, const double* x, const double* y, const double
   c.have_coef = false;
   if (c.have_frames) h->rpole_dirty = true;
   return cuda_status(cudaGetLastError(), &c, "set positions");
+}
+}  // namespace thp
+extern "C" {
+
+int thp_set_positions(thp_ctx* h, const double* x, const double* y, const double* z) {
+  return thp::upload_positions(h, x, y, z, true);
 }
 
 int thp_set_rpole(thp_ctx* h, const double* rpole) {
@@ -1030,17 +1046,14 @@ int thp_get_dipoles(thp_ctx* h, double* uind, double* uinp) {
   Ctx& c = h->c;
   if (!c.have_dipoles) return THP_E_STATE;
   if (set_current_device(c)) return THP_E_CUDA;
-  int st = launch_to_orig6(c, c.d_mu, c.d_tmp6, 2);
+  // laid out on the device as the caller's two [n][3] arrays, then copied
+  // straight into them (a DMA when the caller's buffers are pinned)
+  int st = launch_split_dipoles(c, c.d_mu, c.d_tmp6);
   if (st) return st;
-  std::vector<double> buf((size_t)6 * c.n);
-  cudaMemcpyAsync(buf.data(), c.d_tmp6, sizeof(double) * 6 * c.n, cudaMemcpyDeviceToHost, c.stream);
-  if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "get dipoles"))) return st;
-  for (int i = 0; i < c.n; ++i)
-    for (int j = 0; j < 3; ++j) {
-      if (uind) uind[3 * i + j] = buf[6 * (size_t)i + j];
-      if (uinp) uinp[3 * i + j] = buf[6 * (size_t)i + 3 + j];
-    }
-  return THP_OK;
+  const size_t b = sizeof(double) * 3 * c.n;
+  if (uind) cudaMemcpyAsync(uind, c.d_tmp6, b, cudaMemcpyDeviceToHost, c.stream);
+  if (uinp) cudaMemcpyAsync(uinp, c.d_tmp6 + 3 * (size_t)c.n, b, cudaMemcpyDeviceToHost, c.stream);
+  return cuda_status(cudaStreamSynchronize(c.stream), &c, "get dipoles");
 }
 
 int thp_get_gradient_device(thp_ctx* h, double* d_dep) {
@@ -1261,7 +1274,7 @@ int thp_tmatxbrecip(thp_ctx* h, int nrhs, const double* mu, double* dipfield) {
 
 int thp_solve_host(thp_ctx* h, const double* x, const double* y, const double* z, const double* rpole,
                    double* uind, double* uinp, thp_solve_info* info) {
-  int st = thp_set_positions(h, x, y, z);
+  int st = thp::upload_positions(h, x, y, z, false);
   if (st) return st;
   if (rpole && (st = thp_set_rpole(h, rpole))) return st;
   st = thp_solve(h, THP_GUESS_DIRECT, info);

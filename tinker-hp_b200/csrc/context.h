@@ -33,7 +33,7 @@ struct CgScalars {
 constexpr int kCgChunk = 4;
 
 // device error flags (bit set)
-enum : int { DEV_LIST_OVERFLOW = 1, DEV_PAIR_OVERFLOW = 2, DEV_NAN = 4 };
+enum : int { DEV_LIST_OVERFLOW = 1, DEV_PAIR_OVERFLOW = 2, DEV_NAN = 4, DEV_BAD_INPUT = 8 };
 
 // dipole solutions kept for the predictor (MOD_uprior.f: maxualt)
 constexpr int kMaxAlt = 7;

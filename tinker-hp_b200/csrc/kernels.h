@@ -63,6 +63,7 @@ int launch_epol(Ctx& c);
 // reorder helpers (solver.cu)
 int launch_to_sorted6(Ctx& c, const double* d_orig, double* d_sorted, int nrhs);
 int launch_to_orig6(Ctx& c, const double* d_sorted, double* d_orig, int nrhs);
+int launch_split_dipoles(Ctx& c, const double* d_sorted, double* d_out);  // uind [n][3] then uinp [n][3], original order
 
 int cuda_status(cudaError_t e, Ctx* c, const char* what);
 

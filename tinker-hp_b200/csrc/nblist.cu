@@ -96,11 +96,12 @@ __global__ void k_gather_sorted(int n, Box box, const int* __restrict__ perm, co
                                 int have_rpole, double4* __restrict__ pos, float4* __restrict__ posf,
                                 double* __restrict__ sthole, double* __restrict__ spol,
                                 double* __restrict__ srpole, double* __restrict__ mrec, float* __restrict__ mrecf,
-                                float* __restrict__ erec) {
+                                float* __restrict__ erec, int* __restrict__ flags) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   int o = perm[s];
   double x = xyz[o], y = xyz[n + o], z = xyz[2 * n + o];
+  if (!isfinite(x) || !isfinite(y) || !isfinite(z)) atomicOr(flags, DEV_BAD_INPUT);
   pos[s] = make_double4(x, y, z, pdamp[o]);
   if (posf) {
     double wx = x, wy = y, wz = z;
@@ -395,7 +396,8 @@ int launch_gather_sorted(Ctx& c) {
                                                c.d_par_orig + n, c.d_par_orig + 2 * n, c.d_rpole_orig,
                                                c.have_rpole ? 1 : 0, c.d_pos, c.d_posf,
                                                c.d_thole, c.d_pol, c.d_rpole, c.d_mrec,
-                                               c.mixed ? c.d_mrecf : nullptr, c.mixed ? c.d_erec : nullptr);
+                                               c.mixed ? c.d_mrecf : nullptr, c.mixed ? c.d_erec : nullptr,
+                                               c.d_flags);
   return cuda_status(cudaGetLastError(), &c, "gather sorted");
 }
 

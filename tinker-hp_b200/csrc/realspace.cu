@@ -20,6 +20,11 @@ namespace thp {
 namespace {
 
 constexpr int kBlock = 128;
+// threads per block of the field / coefficient pass
+#ifndef THP_EFLD0_BLOCK
+#define THP_EFLD0_BLOCK 128
+#endif
+constexpr int kFieldBlock = THP_EFLD0_BLOCK;
 
 // list entries whose loads are issued together in the field / coefficient pass
 #ifndef THP_EFLD0_G32
@@ -68,7 +73,7 @@ struct Rec<true> {  // FP32 record of the mixed form
 #endif
 
 template <bool MIXED, bool FIELD>
-__global__ void __launch_bounds__(kBlock, THP_EFLD0_MINB) k_efld0_coef(
+__global__ void __launch_bounds__(kFieldBlock, THP_EFLD0_MINB) k_efld0_coef(
     int n, int npad, Box box, double cut2, EwaldConst ew, const double4* __restrict__ pos,
     const double* __restrict__ mrec, const float* __restrict__ mrecf, const int* __restrict__ perm,
     const int* __restrict__ sp_off, const int* __restrict__ sp_ks, const double* __restrict__ sp_s,
@@ -207,7 +212,7 @@ constexpr int kSpCache = 4;
 constexpr int kFlush = 8;
 
 template <bool FIELD>
-__global__ void __launch_bounds__(kBlock, THP_EFLD0_MINB) k_efld0_coef32(
+__global__ void __launch_bounds__(kFieldBlock, THP_EFLD0_MINB) k_efld0_coef32(
     int n, int npad, float bx, float by, float bz, float cut2, EwaldConst ew, const float* __restrict__ erec,
     const int* __restrict__ perm, const int* __restrict__ sp_off, const int* __restrict__ sp_ks,
     const double* __restrict__ sp_s, const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb,
@@ -432,7 +437,7 @@ PairRows pair_rows(const Ctx& c) {
 int launch_efld0_coef(Ctx& c, bool with_field) { return launch_efld0_coef_on(c, with_field, c.stream); }
 
 int launch_efld0_coef_on(Ctx& c, bool with_field, cudaStream_t s) {
-  const int nb = (c.n + kBlock - 1) / kBlock;
+  const int nb = (c.n + kFieldBlock - 1) / kFieldBlock;
   const double cut2 = c.cfg.ewaldcut * c.cfg.ewaldcut;
   EwaldConst ew = ewald_const(c.cfg.aewald);
 #define THP_EFLD0_ARGS                                                                                          \
@@ -445,21 +450,21 @@ int launch_efld0_coef_on(Ctx& c, bool with_field, cudaStream_t s) {
   c.n, c.npad, bx, by, bz, (float)cut2, ew, c.d_erec, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_s, c.d_nnb, c.d_nb, \
       c.maxnb, c.d_npr, c.d_pk, (float*)c.d_pc3, (float*)c.d_pc5, c.maxpr, c.d_ef, c.d_flags
     if (with_field)
-      k_efld0_coef32<true><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS32);
+      k_efld0_coef32<true><<<nb, kFieldBlock, 0, s>>>(THP_EFLD0_ARGS32);
     else
-      k_efld0_coef32<false><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS32);
+      k_efld0_coef32<false><<<nb, kFieldBlock, 0, s>>>(THP_EFLD0_ARGS32);
 #undef THP_EFLD0_ARGS32
 #else
     if (with_field)
-      k_efld0_coef<true, true><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS);
+      k_efld0_coef<true, true><<<nb, kFieldBlock, 0, s>>>(THP_EFLD0_ARGS);
     else
-      k_efld0_coef<true, false><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS);
+      k_efld0_coef<true, false><<<nb, kFieldBlock, 0, s>>>(THP_EFLD0_ARGS);
 #endif
   } else {
     if (with_field)
-      k_efld0_coef<false, true><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS);
+      k_efld0_coef<false, true><<<nb, kFieldBlock, 0, s>>>(THP_EFLD0_ARGS);
     else
-      k_efld0_coef<false, false><<<nb, kBlock, 0, s>>>(THP_EFLD0_ARGS);
+      k_efld0_coef<false, false><<<nb, kFieldBlock, 0, s>>>(THP_EFLD0_ARGS);
   }
 #undef THP_EFLD0_ARGS
   c.have_coef = true;

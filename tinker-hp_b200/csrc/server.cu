@@ -25,6 +25,7 @@
 
 namespace thp {
 int plan_prefetch(int device, const int nfft[3], int mixed);
+int upload_positions(thp_ctx* h, const double* x, const double* y, const double* z, bool host_check);
 }
 
 namespace {
@@ -49,7 +50,7 @@ struct SysRec {
 
 struct Req {
   unsigned long long ticket = 0, key = 0;
-  std::vector<double> x, y, z;
+  const double *x = nullptr, *y = nullptr, *z = nullptr;  // the caller's, read when the request starts
   double* uind = nullptr;
   double* uinp = nullptr;
   Clock::time_point submitted, started;
@@ -254,7 +255,7 @@ void thp_server::worker() {
     }
     const Clock::time_point t_setup = Clock::now();
     thp_solve_info info{};
-    if (!st) st = thp_set_positions(h, r->x.data(), r->y.data(), r->z.data());
+    if (!st) st = thp::upload_positions(h, r->x, r->y, r->z, false);
     if (!st) {
       st = thp_solve(h, warm ? THP_GUESS_PREVIOUS : THP_GUESS_DIRECT, &info);
       if (st == THP_E_NOT_CONVERGED) st = THP_OK;  // reported through info.converged
@@ -372,9 +373,9 @@ int thp_server_submit(thp_server* s, unsigned long long key, const double* x, co
   const size_t n = it->second->cfg.n;
   r->ticket = s->next_ticket++;
   r->key = key;
-  r->x.assign(x, x + n);
-  r->y.assign(y, y + n);
-  r->z.assign(z, z + n);
+  r->x = x;
+  r->y = y;
+  r->z = z;
   r->uind = uind;
   r->uinp = uinp;
   r->submitted = Clock::now();

@@ -417,7 +417,26 @@ __global__ void k_to_orig6(int n, int nrhs, const int* __restrict__ perm, const 
   for (int q = 0; q < 3 * nrhs; ++q) out[(size_t)o * 3 * nrhs + q] = in[(size_t)s * 6 + q];
 }
 
+// sorted [n][6] -> original-order d dipoles [n][3] followed by p dipoles [n][3]
+__global__ void k_split_dipoles(int n, const int* __restrict__ perm, const double* __restrict__ in,
+                                double* __restrict__ out) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const size_t o = (size_t)perm[s] * 3;
+  const double* v = in + (size_t)s * 6;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    out[o + q] = v[q];
+    out[(size_t)3 * n + o + q] = v[3 + q];
+  }
+}
+
 }  // namespace
+
+int launch_split_dipoles(Ctx& c, const double* d_sorted, double* d_out) {
+  k_split_dipoles<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.d_perm, d_sorted, d_out);
+  return cuda_status(cudaGetLastError(), &c, "split dipoles");
+}
 
 int launch_to_sorted6(Ctx& c, const double* d_orig, double* d_sorted, int nrhs) {
   k_to_sorted6<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, nrhs, c.d_iperm, d_orig, d_sorted);

@@ -393,10 +393,18 @@ class Context:
         self._check(load().thp_tmatxbrecip(self.h, mu.shape[1], _p(mu), _p(out)), "thp_tmatxbrecip")
         return out
 
-    def solve_host(self, x, y, z, rpole=None):
-        """One call on host buffers: positions in, dipoles and energy out."""
-        uind = np.zeros((self.n, 3))
-        uinp = np.zeros((self.n, 3))
+    def solve_host(self, x, y, z, rpole=None, out=None):
+        """One call on host buffers: positions in, dipoles and energy out.
+        `out` = (uind, uinp) C-contiguous float64 [n,3] arrays to fill (for
+        example views of pinned memory, which the copies DMA into)."""
+        if out is None:
+            uind = np.zeros((self.n, 3))
+            uinp = np.zeros((self.n, 3))
+        else:
+            uind, uinp = out
+            for a in out:
+                if a.dtype != np.float64 or a.shape != (self.n, 3) or not a.flags.c_contiguous:
+                    raise ValueError("out arrays must be C-contiguous float64 [n, 3]")
         info = ThpSolveInfo()
         st = load().thp_solve_host(self.h, _p(_f64(x)), _p(_f64(y)), _p(_f64(z)),
                                    None if rpole is None else _p(_f64(rpole)), _p(uind), _p(uinp),

@@ -91,6 +91,7 @@ class Server:
             raise L.ThpError(st, "thp_server_create")
         self.h = h
         self.keys = {}
+        self._live = {}  # ticket -> buffers the native loop reads or fills
 
     def register(self, key, ws):
         keep = []
@@ -101,15 +102,21 @@ class Server:
             raise L.ThpError(st, "thp_server_register")
         return code
 
-    def submit(self, key, ws):
-        """Queues one solve; returns (ticket, uind buffer)."""
+    def submit(self, key, ws, xyz=None, uind=None):
+        """Queues one solve; returns (ticket, uind buffer).  The coordinate
+        and dipole buffers are the loop's until wait() returns: given ones
+        (`xyz` = three C-contiguous float64 [n] arrays, `uind` [n,3], e.g.
+        pinned) are used as they are, otherwise copies are made and kept."""
         code = self.keys.get(key) or self.register(key, ws)
-        xyz = [np.ascontiguousarray(a, dtype=np.float64) for a in (ws.x, ws.y, ws.z)]
-        uind = np.zeros((ws.n, 3))
+        if xyz is None:
+            xyz = [np.ascontiguousarray(a, dtype=np.float64) for a in (ws.x, ws.y, ws.z)]
+        if uind is None:
+            uind = np.zeros((ws.n, 3))
         t = C.c_ulonglong()
         st = L.load().thp_server_submit(self.h, code, *(L._p(a) for a in xyz), L._p(uind), None, C.byref(t))
         if st:
             raise L.ThpError(st, "thp_server_submit")
+        self._live[t.value] = (xyz, uind)
         return t.value, uind
 
     def warm(self, count):
@@ -121,6 +128,7 @@ class Server:
     def wait(self, ticket):
         r = L.ThpResult()
         st = L.load().thp_server_wait(self.h, ticket, C.byref(r))
+        self._live.pop(ticket, None)
         if st:
             raise L.ThpError(st, "thp_server_wait")
         return r
