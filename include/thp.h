@@ -57,7 +57,9 @@ extern "C" {
 
 /* ---- initial guess of the dipoles (newinduce_pme2.f:161-200) ----------- */
 #define THP_GUESS_DIRECT 0   /* mu = alpha * E0 (polgsf = 0) */
-#define THP_GUESS_PREVIOUS 1 /* mu = last converged dipoles kept on the device */
+#define THP_GUESS_PREVIOUS 1 /* mu = last converged dipoles kept on the device, plus the
+                                polarizability times the change of the direct field E0 since
+                                their solve (a first-order correction for moved atoms) */
 #define THP_GUESS_HOST 2     /* mu = caller-provided array (thp_set_guess) */
 #define THP_GUESS_PREDICT 3  /* predictor over the stored solutions (thp_set_predictor); the direct
                                 guess until seven are stored (newinduce_pme2.f:165-190) */

@@ -382,7 +382,7 @@ size_t footprint_bytes(const thp_config& cfg, int* ncell_out) {
   b += n * 4 + maxnb * npad * 4;                         // list
   b += n * 4 + maxnb * npad * (4 + 2 * (mixed ? 4 : 8));  // pairs
   b += ngrid * (mixed ? 12 : 24);                        // grid + qfac
-  b += 9 * n * 6 * 8 + 4 * n * 8 + n * 6 * 4 + n * 9 * 4;  // vectors, FP32 row input
+  b += 10 * n * 6 * 8 + 4 * n * 8 + n * 6 * 4 + n * 9 * 4;  // vectors, FP32 row input
   b += (n / 128 + 2) * 4 * 8 + 4096;
   b += 64 << 20;  // cuFFT work area and runtime slack
   return b;
@@ -518,7 +518,7 @@ static int size_buffers(Ctx& c) {
                      item(&c.d_nnb, n), item(&c.d_npr, n), item(&c.d_ef, 6 * n), item(&c.d_mu, 6 * n),
                      item(&c.d_res, 6 * n), item(&c.d_h, 6 * n), item(&c.d_pp, 6 * n), item(&c.d_zr, 6 * n),
                      item(&c.d_dip, 6 * n), item(&c.d_tmp6, 6 * n), item(&c.d_tmp6b, 6 * n), item(&c.d_cphi, 4 * n),
-                     item(&c.d_vecf, 6 * n), item(&c.d_rec, 8 * n), item(&c.d_mpz, n),
+                     item(&c.d_vecf, 6 * n), item(&c.d_rec, 8 * n), item(&c.d_mpz, n), item(&c.d_ef_prev, 6 * n),
                      item(&c.d_partials, (size_t)(c.nblk_reduce + 8) * 4)},
                     "per-atom buffers");
     if (!st) c.cap_n = n;
@@ -546,7 +546,7 @@ static int size_buffers(Ctx& c) {
 static int clear_system_state(thp_ctx* h) {
   Ctx& c = h->c;
   c.have_params = c.have_pos = c.have_rpole = c.have_conn = c.have_frames = c.have_axes = false;
-  c.have_perm = c.have_list = c.have_coef = c.have_dipoles = false;
+  c.have_perm = c.have_list = c.have_coef = c.have_dipoles = c.have_ef_prev = false;
   c.pred_mode = c.nualt = c.alt_head = 0;
   h->pos_dirty = h->rpole_dirty = true;
   h->field_valid = h->guess_uploaded = h->solved_once = false;
@@ -815,7 +815,7 @@ static int resolve_predict(Ctx& c, int* guess) {
   if (*guess != THP_GUESS_PREDICT) return THP_OK;
   const int r = predictor_guess(c);
   if (r > 0) return r;
-  *guess = r == 0 ? THP_GUESS_PREVIOUS : THP_GUESS_DIRECT;  // PREVIOUS: start from d_mu as written
+  *guess = r == 0 ? THP_GUESS_HOST : THP_GUESS_DIRECT;  // HOST: start from d_mu as written
   return THP_OK;
 }
 

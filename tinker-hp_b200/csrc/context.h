@@ -145,6 +145,9 @@ struct Ctx {
   // mixed form matvec input of the overlapped CG rows: per atom one 32-byte
   // record {x, y, z (wrapped), d dipole, p dipole x, y} and the p dipole z
   float* d_rec = nullptr;     // [n][8]
+  // E0 of the last CG start (sorted order), for the corrected warm start
+  double* d_ef_prev = nullptr;  // [n][6]
+  bool have_ef_prev = false;
   float* d_mpz = nullptr;     // [n]
   double* d_tmp6 = nullptr;   // [n][6] original-order staging for host I/O
   double* d_tmp6b = nullptr;

@@ -368,10 +368,16 @@ int launch_sort_atoms(Ctx& c) {
   // the last dipoles (warm start) follow their atoms into the new order; the
   // CG residual buffer is free between solves and holds them meanwhile
   const bool keep_mu = c.have_perm && c.have_dipoles;
+  const bool keep_ef = c.have_perm && c.have_ef_prev;  // so does the last E0 (d_zr is free too)
   if (keep_mu) {
     int st = launch_to_orig6(c, c.d_mu, c.d_res, 2);
     if (st) return st;
   }
+  if (keep_ef) {
+    int st = launch_to_orig6(c, c.d_ef_prev, c.d_zr, 2);
+    if (st) return st;
+  }
+  if (!c.have_perm) c.have_ef_prev = false;
   cudaMemsetAsync(c.d_cell_count, 0, sizeof(int) * c.ncell, s);
   cudaMemsetAsync(c.d_cell_fill, 0, sizeof(int) * c.ncell, s);
   k_cell_count<<<nb, kBlock, 0, s>>>(n, c.box, c.nc[0], c.nc[1], c.nc[2], c.d_xyz_orig, c.d_atom_cell,
@@ -385,6 +391,7 @@ int launch_sort_atoms(Ctx& c) {
   if (m > 0) k_sp_to_sorted<<<(m + 255) / 256, 256, 0, s>>>(m, c.d_iperm, c.d_sp_k, c.d_sp_ks);
   int st = cuda_status(cudaGetLastError(), &c, "sort atoms");
   if (!st && keep_mu) st = launch_to_sorted6(c, c.d_res, c.d_mu, 2);
+  if (!st && keep_ef) st = launch_to_sorted6(c, c.d_zr, c.d_ef_prev, 2);
   return st;
 }
 

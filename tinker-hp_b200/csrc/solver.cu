@@ -386,6 +386,17 @@ __global__ void k_guess_direct(int n, const double* __restrict__ pol, const doub
   mu[t] = pol[t / 6] * ef[t];
 }
 
+// Warm start corrected to first order for the change of the direct field
+// since the last solve: mu += alpha (E0 - E0_prev).  Then E0_prev = E0.
+__global__ void k_guess_delta(int n, const double* __restrict__ pol, const double* __restrict__ ef,
+                              double* __restrict__ ef_prev, double* __restrict__ mu) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * 6) return;
+  const double e = ef[t];
+  mu[t] += pol[t / 6] * (e - ef_prev[t]);
+  ef_prev[t] = e;
+}
+
 // epolar0c via the identity Epol = -1/2 electric sum uind . E_p(perm)
 // (epreal0c + eprecip + self of epolar.f:47-520 sum to exactly this form)
 __global__ void __launch_bounds__(kBlock) k_epol(int n, const double* __restrict__ mu, const double* __restrict__ ef,
@@ -543,6 +554,15 @@ int pcg_begin(Ctx& c, int guess) {
   if (guess == THP_GUESS_DIRECT) {
     k_guess_direct<<<(c.n * 6 + 255) / 256, 256, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_mu);
   }
+  // the last dipoles plus alpha times the change of E0 since their solve
+  // (about one CG iteration fewer for a small displacement of the atoms);
+  // every start records this solve's E0 for the next one
+  if (guess == THP_GUESS_PREVIOUS && c.have_ef_prev)
+    k_guess_delta<<<(c.n * 6 + 255) / 256, 256, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_ef_prev, c.d_mu);
+  else
+    cudaMemcpyAsync(c.d_ef_prev, c.d_ef, sizeof(double) * 6 * c.n, cudaMemcpyDeviceToDevice, c.stream);
+  c.have_ef_prev = true;
+  if ((st = cuda_status(cudaGetLastError(), &c, "cg start"))) return st;
   if (overlapped(c)) {
     if (c.mixed) {
       k_pp_rec<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, 0, c.d_zr, c.d_mu, c.d_posf, c.d_rec, c.d_mpz, c.d_cg);
