@@ -242,14 +242,17 @@ def serving_run(lib, thp, count, workers=8):
     return summ
 
 
-def served_repeats(lib, ws, precision, count=20, perturb=0.01, seed=5011):
-    """Served repeats of one resident system: after a cold first request, each
-    request carries the box's coordinates with a fresh Gaussian perturbation
-    of `perturb` A RMS (as the repeats of the serving stream), one in flight
-    at a time.  The server keeps the system's list (reused while no atom has
+def served_repeats(lib, boxes0, precision, count=20, perturb=0.01, seed=5011):
+    """Served repeats of resident systems: after a cold first request per
+    system, each request carries one system's coordinates with a fresh
+    Gaussian perturbation of `perturb` A RMS (as the repeats of the serving
+    stream).  The server keeps each system's list (reused while no atom has
     moved half the 0.5 A buffer since the build) and its last dipoles (the
-    warm start).  Returns the throughput, latencies and the dipole error of
-    the last request against an FP64 solve of its coordinates to 1e-8."""
+    warm start).  With one system one request is in flight at a time; with
+    several, all requests are submitted at once (systems interleaved), one
+    worker per system, and requests of different systems overlap on the
+    device.  Returns the throughput, latencies and the dipole error of the
+    last request against an FP64 solve of its coordinates to 1e-8."""
     import torch
     from tinker_hp_b200 import serve
 
@@ -259,34 +262,44 @@ def served_repeats(lib, ws, precision, count=20, perturb=0.01, seed=5011):
         return t
 
     rng = np.random.default_rng(seed)
-    base = ws.positions()
-    boxes = [ws.with_positions(base + rng.normal(0.0, perturb / np.sqrt(3.0), size=(ws.n, 3)))
-             for _ in range(count)]
-    xyz = [[pinned(np.asarray(a, dtype=np.float64)) for a in (b.x, b.y, b.z)] for b in boxes]
-    uind = pinned(np.zeros((ws.n, 3)))
-    srv = serve.Server(precision=precision, poleps=CG_TOL, budget_bytes=120 << 30, workers=1, max_resident=2)
-    srv.register("box", ws)
-    t, _ = srv.submit("box", ws)
-    srv.wait(t)
-    lat, iters, warm = [], [], []
+    nsys = len(boxes0)
+    reqs = []  # (system, box, pinned xyz, pinned uind)
+    for q in range(count):
+        k = q % nsys
+        ws = boxes0[k]
+        b = ws.with_positions(ws.positions() + rng.normal(0.0, perturb / np.sqrt(3.0), size=(ws.n, 3)))
+        reqs.append((k, b, [pinned(np.asarray(a, dtype=np.float64)) for a in (b.x, b.y, b.z)],
+                     pinned(np.zeros((ws.n, 3)))))
+    srv = serve.Server(precision=precision, poleps=CG_TOL, budget_bytes=120 << 30, workers=nsys,
+                       max_resident=nsys + 1)
+    for k, ws in enumerate(boxes0):
+        srv.register(f"box{k}", ws)
+    for t in [srv.submit(f"box{k}", ws)[0] for k, ws in enumerate(boxes0)]:
+        srv.wait(t)
+    res = []
     t0 = time.perf_counter()
-    for wq, q in zip(boxes, xyz):
-        ticket, _ = srv.submit("box", wq, xyz=q, uind=uind)
-        r = srv.wait(ticket)
-        lat.append(r.latency_ms)
-        iters.append(r.niter)
-        warm.append(bool(r.warm))
+    if nsys == 1:
+        for k, b, xyz, ui in reqs:
+            ticket, _ = srv.submit(f"box{k}", b, xyz=xyz, uind=ui)
+            res.append(srv.wait(ticket))
+    else:
+        tickets = [srv.submit(f"box{k}", b, xyz=xyz, uind=ui)[0] for k, b, xyz, ui in reqs]
+        res = [srv.wait(t) for t in tickets]
     wall = time.perf_counter() - t0
     srv.close()
-    ref = lib.Context(boxes[-1], precision=lib.FP64, poleps=1e-8)
+    _, last, _, ulast = reqs[-1]
+    ref = lib.Context(last, precision=lib.FP64, poleps=1e-8)
     ref.solve()
     ue, _ = ref.dipoles()
     ref.close()
-    err = float(np.sqrt(np.mean(np.sum((uind - ue) ** 2, axis=1))) * DEBYE)
-    return {"requests": count, "solves_per_s": count / wall, "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "mean_iters": float(np.mean(iters)),
-            "warm_fraction": float(np.mean(warm)), "dipole_rms_D_vs_fp64_1e-8": err,
-            "perturbation": f"{perturb} A RMS per request around the box, one request in flight",
+    err = float(np.sqrt(np.mean(np.sum((ulast - ue) ** 2, axis=1))) * DEBYE)
+    lat = [r.latency_ms for r in res]
+    sol = [r.solve_ms for r in res]
+    return {"systems": nsys, "requests": count, "solves_per_s": count / wall,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "solve_p50_ms": float(np.percentile(sol, 50)), "mean_iters": float(np.mean([r.niter for r in res])),
+            "warm_fraction": float(np.mean([bool(r.warm) for r in res])), "dipole_rms_D_vs_fp64_1e-8": err,
+            "perturbation": f"{perturb} A RMS per request around its box",
             "host_buffers": "pinned coordinates in, pinned dipoles out"}
 
 
@@ -509,8 +522,11 @@ def main():
         extras["batch_64_boxes"] = batched_throughput(lib, batch64, 1, 3)
         extras["batch_64_boxes"]["atoms"] = f"{sum(w.n for w in batch64)} over 64 boxes (300-6000 each)"
         extras["serving"] = serving_run(lib, thp, 120)
-        extras["served_288k_repeats"] = {"mixed": served_repeats(lib, ws, lib.MIXED),
-                                         "fp64": served_repeats(lib, ws, lib.FP64)}
+        ws2 = thp.water.make_water_box(nw, cfg=cfg, seed_lattice=7001, seed_orient=7002)
+        extras["served_288k_repeats"] = {"mixed": served_repeats(lib, [ws], lib.MIXED),
+                                         "fp64": served_repeats(lib, [ws], lib.FP64),
+                                         "mixed_2_systems": served_repeats(lib, [ws, ws2], lib.MIXED, count=24),
+                                         "fp64_2_systems": served_repeats(lib, [ws, ws2], lib.FP64, count=24)}
         extras["md_config1"] = {"previous": md_run(lib, thp), "aspc": md_run(lib, thp, predictor="ASPC")}
         if fp64 is not None:
             best = max(b2["solves_per_s"], b4["solves_per_s"])
@@ -519,6 +535,9 @@ def main():
             sr = extras["served_288k_repeats"]
             sr["mixed_vs_fp64_plain"] = sr["mixed"]["solves_per_s"] / plain64
             sr["mixed_vs_fp64_served"] = sr["mixed"]["solves_per_s"] / sr["fp64"]["solves_per_s"]
+            sr["mixed_2_systems_vs_fp64_plain"] = sr["mixed_2_systems"]["solves_per_s"] / plain64
+            sr["mixed_2_systems_vs_fp64_2_systems"] = (sr["mixed_2_systems"]["solves_per_s"]
+                                                       / sr["fp64_2_systems"]["solves_per_s"])
 
     steps = args.steps
     value = world * steps / (t_mixed / 1000.0)
