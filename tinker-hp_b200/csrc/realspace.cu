@@ -235,6 +235,11 @@ __global__ void __launch_bounds__(kFieldBlock, THP_EFLD0_MINB) k_efld0_coef32(
   double e[6] = {0, 0, 0, 0, 0, 0};
   const int nn = min(nnb[i], maxnb);
   int cnt = 0;
+  // list entries one group ahead: the list streams from DRAM, and its load
+  // would otherwise sit in front of every group's record gathers
+  int nxt[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) nxt[g] = g < nn ? __ldg(nb + (size_t)g * npad + i) : i;
 #pragma unroll 1
   for (int sf = 0; sf < nn; sf += kFlush) {
     float f[6] = {0, 0, 0, 0, 0, 0};
@@ -244,7 +249,9 @@ __global__ void __launch_bounds__(kFieldBlock, THP_EFLD0_MINB) k_efld0_coef32(
       int kk[G];
       float v[G][16];
 #pragma unroll
-      for (int g = 0; g < G; ++g) kk[g] = sb + g < se ? __ldg(nb + (size_t)(sb + g) * npad + i) : i;
+      for (int g = 0; g < G; ++g) kk[g] = nxt[g];
+#pragma unroll
+      for (int g = 0; g < G; ++g) nxt[g] = sb + G + g < nn ? __ldg(nb + (size_t)(sb + G + g) * npad + i) : i;
 #pragma unroll
       for (int g = 0; g < G; ++g) {
         ld_rec8(erec + (size_t)kk[g] * 16, *reinterpret_cast<float(*)[8]>(&v[g][0]));
