@@ -150,6 +150,30 @@ __device__ __forceinline__ void tmatxb_row32(const PairRows& pr, float bx, float
   }
 }
 
+// Stream loads of the CG rows, read once per matvec.  NOL1: not kept in L1,
+// so the partner records gathered beside them stay resident (used when the
+// stream streams from DRAM; an L2-resident stream does better cached).
+template <bool NOL1>
+__device__ __forceinline__ int ld_stream(const int* p) {
+  if constexpr (NOL1) {
+    int v;
+    asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+  } else {
+    return __ldg(p);
+  }
+}
+template <bool NOL1>
+__device__ __forceinline__ float ld_stream(const float* p) {
+  if constexpr (NOL1) {
+    float v;
+    asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+  } else {
+    return __ldg(p);
+  }
+}
+
 // 256-bit read-only load of one 32-byte aligned record
 __device__ __forceinline__ void ld_rec8(const float* p, float (&v)[8]) {
   asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -164,6 +188,7 @@ __device__ __forceinline__ void ld_rec8(const float* p, float (&v)[8]) {
 // wavefront per distinct cache line touched, so halving them halves the
 // pipe's work.  The arithmetic and the order of the sums are those of
 // pairs32.
+template <bool NOL1>
 __device__ __forceinline__ void tmatxb_row32_rec(const PairRows& pr, float bx, float by, float bz, int i,
                                                  const float* __restrict__ rec, const float* __restrict__ mpz,
                                                  float (&acc)[6]) {
@@ -181,9 +206,9 @@ __device__ __forceinline__ void tmatxb_row32_rec(const PairRows& pr, float bx, f
     for (int g = 0; g < G; ++g) {
       const bool ok = s + g < m;
       const size_t q = (size_t)(ok ? s + g : s) * pr.npad + i;
-      k[g] = __ldg(pk + q);
-      c3[g] = ok ? __ldg(c3p + q) : 0.f;
-      c5[g] = ok ? __ldg(c5p + q) : 0.f;
+      k[g] = ld_stream<NOL1>(pk + q);
+      c3[g] = ok ? ld_stream<NOL1>(c3p + q) : 0.f;
+      c5[g] = ok ? ld_stream<NOL1>(c5p + q) : 0.f;
     }
     float v[G][8], w[G];
 #pragma unroll

@@ -42,6 +42,12 @@
 #define THP_GATHER_COMBINE 1
 #endif
 
+// systems of at least this many atoms read the mixed row's pair stream
+// (~1.7 kB per atom, far beyond L2 from here on) without allocating in L1
+#ifndef THP_STREAM_NO_L1_ATOMS
+#define THP_STREAM_NO_L1_ATOMS 80000
+#endif
+
 #ifndef THP_OVERLAP_MIN_ATOMS
 #define THP_OVERLAP_MIN_ATOMS 20000
 #endif
@@ -212,7 +218,7 @@ __global__ void __launch_bounds__(256) k_pp_rec(int n, int update, const double*
 }
 
 // real-space part of h only: hreal = T_real x (tmatxb_pme without the diagonal)
-template <bool MIXED>
+template <bool MIXED, bool NOL1>
 __global__ void __launch_bounds__(kBlock, THP_ROW_MINB) k_real_row(PairRows pr, Box box, const double4* __restrict__ pos,
                                                      const float* __restrict__ rec, const double* __restrict__ x,
                                                      const float* __restrict__ mpz, const CgScalars* __restrict__ cg,
@@ -223,7 +229,7 @@ __global__ void __launch_bounds__(kBlock, THP_ROW_MINB) k_real_row(PairRows pr, 
   double acc[6];
   if (MIXED) {
     float a32[6] = {0, 0, 0, 0, 0, 0};
-    tmatxb_row32_rec(pr, (float)box.l[0], (float)box.l[1], (float)box.l[2], i, rec, mpz, a32);
+    tmatxb_row32_rec<NOL1>(pr, (float)box.l[0], (float)box.l[1], (float)box.l[2], i, rec, mpz, a32);
 #pragma unroll
     for (int q = 0; q < 6; ++q) acc[q] = (double)a32[q];
   } else {
@@ -479,10 +485,15 @@ static int matvec_overlapped(Ctx& c, double* x, int init) {
   cudaStreamWaitEvent(c.stream2, c.ev_fork, 0);
   PairRows pr = pair_rows(c);
   prof_mark(c, c.stream2);
-  if (c.mixed)
-    k_real_row<true><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, x, c.d_mpz, c.d_cg, !init, c.d_h);
+  if (c.mixed && c.n >= THP_STREAM_NO_L1_ATOMS)
+    k_real_row<true, true><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, x, c.d_mpz, c.d_cg, !init,
+                                                         c.d_h);
+  else if (c.mixed)
+    k_real_row<true, false><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, x, c.d_mpz, c.d_cg, !init,
+                                                          c.d_h);
   else
-    k_real_row<false><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, nullptr, x, nullptr, c.d_cg, !init, c.d_h);
+    k_real_row<false, false><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, nullptr, x, nullptr, c.d_cg, !init,
+                                                           c.d_h);
   prof_mark(c, c.stream2);
   if ((st = cuda_status(cudaGetLastError(), &c, "real row"))) return st;
   cudaEventRecord(c.ev_join, c.stream2);
