@@ -558,10 +558,14 @@ def main():
         "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
         "gpu_launches": None,
     }
-    # kernel launches of this library per timed step (list build 5, field 2+spread/FFT,
-    # per CG iteration 4 of ours + 2 cuFFT)
+    # kernels of this library per timed step (cuFFT's not counted): rotpole 1;
+    # re-sort 9 (count/scan/fill/sort, special pairs, dipoles and last E0
+    # carried out of and back into sorted order); sorted gather 1; list,
+    # E_direct, multipole spread, qfac, multipole gather 5; CG start 6 (guess,
+    # records, row, spread, qfac, combine); 7 per iteration (records, row,
+    # spread, qfac, combine, update, loop condition); Epol 1
     it = int(np.median(niter))
-    per_step = 5 + 1 + 1 + 3 + 1 + (it + 1) * 4 + 1
+    per_step = 1 + 9 + 1 + 5 + 6 + 7 * it + 1
     line["gpu_launches"] = per_step * steps
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -139,11 +139,9 @@ void cell_grid(const thp_config& cfg, int nc[3]) {
   for (int d = 0; d < 3; ++d) nc[d] = std::max(1, (int)std::floor(cfg.box[d] / half_cut));
 }
 
-int check_flags(thp_ctx* h) {
-  Ctx& c = h->c;
-  cudaMemcpyAsync(c.h_flags, c.d_flags, sizeof(int), cudaMemcpyDeviceToHost, c.stream);
-  int st = cuda_status(cudaStreamSynchronize(c.stream), &c, "sync");
-  if (st) return st;
+// Maps the device error bits copied into h_flags to a status (and clears
+// them on the device).
+static int flags_status(Ctx& c) {
   int f = *c.h_flags;
   if (f) {
     cudaMemsetAsync(c.d_flags, 0, sizeof(int), c.stream);
@@ -158,6 +156,14 @@ int check_flags(thp_ctx* h) {
     return THP_E_NAN;
   }
   return THP_OK;
+}
+
+int check_flags(thp_ctx* h) {
+  Ctx& c = h->c;
+  cudaMemcpyAsync(c.h_flags, c.d_flags, sizeof(int), cudaMemcpyDeviceToHost, c.stream);
+  int st = cuda_status(cudaStreamSynchronize(c.stream), &c, "sync");
+  if (st) return st;
+  return flags_status(c);
 }
 
 int set_current_device(Ctx& c) { return cuda_status(cudaSetDevice(c.device), &c, "set device"); }
@@ -274,8 +280,10 @@ int ensure_rpole(thp_ctx* h) {
 }
 
 // E0 = direct + reciprocal + self (newinduce_pme2.f:110-148) and the matvec
-// coefficients, for the current positions and multipoles.
-int compute_field(thp_ctx* h) {
+// coefficients, for the current positions and multipoles.  check: read the
+// device error bits now (a host sync); otherwise the caller reads them with
+// its own later sync.
+int compute_field(thp_ctx* h, bool check = true) {
   Ctx& c = h->c;
   int st;
   if ((st = ensure_rpole(h))) return st;
@@ -283,8 +291,10 @@ int compute_field(thp_ctx* h) {
   if ((st = prepare_list(h, false, &rebuild))) return st;
   if ((st = launch_fields(c, rebuild))) return st;
   c.have_list = true;
-  if ((st = check_flags(h))) return st;
-  h->field_valid = true;
+  if (check) {
+    if ((st = check_flags(h))) return st;
+    h->field_valid = true;
+  }
   return THP_OK;
 }
 
@@ -828,18 +838,25 @@ int thp_solve(thp_ctx* h, int guess, thp_solve_info* info) {
   if (guess == THP_GUESS_PREVIOUS && !c.have_dipoles) guess = THP_GUESS_DIRECT;
   if (guess == THP_GUESS_HOST && !h->guess_uploaded) return THP_E_STATE;
   cudaEventRecord(c.ev0, c.stream);
-  int st = compute_field(h);
+  // one host sync per solve: the list/pair overflow bits and the CG scalars
+  // are read together after Epol (the predictor's least-squares fit and the
+  // host-checked CG chunks, where used, sync on their own)
+  int st = compute_field(h, false);
   if (st) return st;
   if ((st = resolve_predict(c, &guess))) return st;
-  st = run_pcg(c, guess);
+  bool pending = false;
+  if ((st = run_pcg_async(c, guess, &pending))) return st;
   h->guess_uploaded = false;
-  if (st && st != THP_E_NOT_CONVERGED) return st;
-  if (int sp = predictor_push(c)) return sp;
-  int st2 = launch_epol(c);
-  if (st2) return st2;
+  if ((st = predictor_push(c))) return st;
+  if ((st = launch_epol(c))) return st;
   cudaEventRecord(c.ev1, c.stream);
   cudaMemcpyAsync(c.h_cg, c.d_cg, sizeof(CgScalars), cudaMemcpyDeviceToHost, c.stream);
-  if ((st2 = cuda_status(cudaStreamSynchronize(c.stream), &c, "solve"))) return st2;
+  cudaMemcpyAsync(c.h_flags, c.d_flags, sizeof(int), cudaMemcpyDeviceToHost, c.stream);
+  if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "solve"))) return st;
+  if ((st = flags_status(c))) return st;
+  h->field_valid = true;
+  st = pcg_status(c);
+  if (st && st != THP_E_NOT_CONVERGED) return st;
   h->solved_once = true;
   if (info) {
     info->niter = c.h_cg->niter;

@@ -54,6 +54,8 @@ int launch_ekin(Ctx& c, const double* d_mass, const double* d_vel, double* d_scr
 
 // solver.cu
 int run_pcg(Ctx& c, int guess);
+int run_pcg_async(Ctx& c, int guess, bool* pending);  // see solver.cu
+int pcg_status(Ctx& c);
 int pcg_begin(Ctx& c, int guess);
 int pcg_chunk_async(Ctx& c);
 int pcg_loop_async(Ctx& c);  // whole CG loop in one graph launch; -1 when unavailable

@@ -60,6 +60,58 @@ __global__ void k_scan_single(int m, const int* __restrict__ in, int* __restrict
   }
 }
 
+// The same scan over many blocks: each block scans 1024 cells (k_scan_tiles,
+// writing its total), one block scans the totals (k_scan_totals), and every
+// block adds its offset (k_scan_offsets).  Used up to 1024 x 1024 cells.
+__device__ __forceinline__ int block_excl_scan_1024(int v, int* s_warp, int* total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int t = s_warp[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    s_warp[lane] = t;  // inclusive totals of the warps
+  }
+  __syncthreads();
+  const int before = w > 0 ? s_warp[w - 1] : 0;
+  *total = s_warp[31];
+  return before + x - v;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_tiles(int m, const int* __restrict__ in, int* __restrict__ out,
+                                                      int* __restrict__ tile_sum) {
+  __shared__ int s_warp[32];
+  const int i = blockIdx.x * 1024 + threadIdx.x;
+  const int v = i < m ? in[i] : 0;
+  int total;
+  const int e = block_excl_scan_1024(v, s_warp, &total);
+  if (i < m) out[i] = e;
+  if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_totals(int nt, int* __restrict__ tile_sum) {
+  __shared__ int s_warp[32];
+  const int v = threadIdx.x < nt ? tile_sum[threadIdx.x] : 0;
+  int total;
+  const int e = block_excl_scan_1024(v, s_warp, &total);
+  if (threadIdx.x < nt) tile_sum[threadIdx.x] = e;
+}
+
+__global__ void k_scan_offsets(int m, int* __restrict__ out, const int* __restrict__ tile_sum) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) out[i] += tile_sum[i >> 10];
+}
+
 __global__ void k_cell_fill(int n, const int* __restrict__ atom_cell, const int* __restrict__ cell_start,
                             int* __restrict__ cell_fill, int* __restrict__ perm) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -382,7 +434,17 @@ int launch_sort_atoms(Ctx& c) {
   cudaMemsetAsync(c.d_cell_fill, 0, sizeof(int) * c.ncell, s);
   k_cell_count<<<nb, kBlock, 0, s>>>(n, c.box, c.nc[0], c.nc[1], c.nc[2], c.d_xyz_orig, c.d_atom_cell,
                                      c.d_cell_count);
-  k_scan_single<<<1, 1024, 0, s>>>(c.ncell, c.d_cell_count, c.d_cell_start);
+  const int ntile = (c.ncell + 1023) / 1024;
+  // the tile totals live in the reduction partials (free outside the CG),
+  // which hold 8 ints per 128 atoms plus 64
+  if (ntile <= 1024 && (size_t)ntile <= 8 * ((size_t)c.nblk_reduce + 8)) {
+    int* tile_sum = reinterpret_cast<int*>(c.d_partials);
+    k_scan_tiles<<<ntile, 1024, 0, s>>>(c.ncell, c.d_cell_count, c.d_cell_start, tile_sum);
+    k_scan_totals<<<1, 1024, 0, s>>>(ntile, tile_sum);
+    k_scan_offsets<<<(c.ncell + 255) / 256, 256, 0, s>>>(c.ncell, c.d_cell_start, tile_sum);
+  } else {
+    k_scan_single<<<1, 1024, 0, s>>>(c.ncell, c.d_cell_count, c.d_cell_start);
+  }
   k_cell_fill<<<nb, kBlock, 0, s>>>(n, c.d_atom_cell, c.d_cell_start, c.d_cell_fill, c.d_perm);
   k_cell_sort<<<(c.ncell + kBlock - 1) / kBlock, kBlock, 0, s>>>(c.ncell, c.d_cell_start, c.d_cell_count,
                                                                  c.d_perm, c.d_iperm, c.d_scell);

@@ -677,6 +677,29 @@ int pcg_status(Ctx& c) {
 // Runs the CG from the current d_ef; guess selects the start (see thp.h).
 // The host reads the stop flag once per chunk of kCgChunk iterations; kernels
 // after the stop return at entry.
+// Like run_pcg, but with the device loop available it only enqueues the CG
+// and the copy of its scalars (*pending = true); the caller synchronises and
+// then reads pcg_status.
+int run_pcg_async(Ctx& c, int guess, bool* pending) {
+  *pending = false;
+  int st = pcg_begin(c, guess);
+  if (st) return st;
+  st = pcg_loop_async(c);
+  if (st >= 0) {
+    *pending = st == THP_OK;
+    return st;
+  }
+  int done = 0;
+  while (true) {
+    if ((st = pcg_chunk_async(c))) return st;
+    done += kCgChunk;
+    if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "cg sync"))) return st;
+    if (c.h_cg->stop) break;
+    if (done > c.cfg.politer + kCgChunk) break;  // defensive bound; stop is raised at politer
+  }
+  return THP_OK;
+}
+
 int run_pcg(Ctx& c, int guess) {
   int st = pcg_begin(c, guess);
   if (st) return st;
