@@ -125,6 +125,46 @@ def test_warm_start_fewer_iterations(lib, case):
     assert r2["niter"] < r1["niter"]
 
 
+def test_warm_start_after_displacement(lib, thp, case):
+    # the previous dipoles plus alpha * (E0 - E0_prev) start the CG: after a
+    # 0.01 A displacement the warm solve needs fewer iterations than a cold
+    # one, and both stop at poleps 1e-6 equally close to the converged answer
+    ws, _ = case
+    rng = np.random.default_rng(11)
+    moved = ws.with_positions(ws.positions() + rng.normal(0.0, 0.01 / np.sqrt(3.0), size=(ws.n, 3)))
+    warm = lib.Context(ws, poleps=1e-6)
+    warm.solve()
+    warm.set_positions(moved.x, moved.y, moved.z)
+    rw = warm.solve(guess=lib.GUESS_PREVIOUS)
+    uw, pw = warm.dipoles()
+    cold = lib.Context(moved, poleps=1e-6)
+    rc = cold.solve()
+    uc, pc = cold.dipoles()
+    exact = lib.Context(moved, poleps=1e-10)
+    exact.solve()
+    ue, pe = exact.dipoles()
+    assert rw["converged"] and rw["niter"] < rc["niter"], (rw["niter"], rc["niter"])
+
+    def rms(a, b):
+        return np.sqrt(np.mean(np.sum((a - b) ** 2, axis=1))) * DEBYE
+
+    for a, c, e in ((uw, uc, ue), (pw, pc, pe)):
+        assert rms(a, e) < 1e-5 and rms(a, e) < 2.0 * rms(c, e) + 1e-6, (rms(a, e), rms(c, e))
+
+
+def test_solve_host_rejects_nonfinite_coordinates(lib, case):
+    ws, orc = case
+    ctx = lib.Context(ws, frames=False, rpole=orc.rpole)
+    x = np.array(ws.x, dtype=np.float64)
+    x[7] = np.nan
+    with pytest.raises(lib.ThpError) as e:
+        ctx.solve_host(x, ws.y, ws.z, orc.rpole)
+    assert e.value.status == lib.THP_E_INVALID
+    # the context recovers with valid coordinates
+    uind, _, info = ctx.solve_host(ws.x, ws.y, ws.z, orc.rpole)
+    assert info["converged"] and np.isfinite(uind).all()
+
+
 def test_solve_host_call(lib, case):
     ws, orc = case
     ctx = lib.Context(ws, frames=False, rpole=orc.rpole)

@@ -87,6 +87,35 @@ def test_served_results_same_alone_and_in_mix(thp):
 
 
 @pytest.mark.gpu
+def test_server_fills_caller_buffers_in_place(thp):
+    # coordinates and dipoles in the caller's own arrays (read and written
+    # when the request runs); two overlapping systems, each repeated
+    from tinker_hp_b200 import serve, lib
+    boxes = [thp.water.make_water_box(2000, cfg=0), thp.water.make_water_box(1500, cfg=1)]
+    srv = serve.Server(precision=lib.MIXED, poleps=1e-6, workers=2)
+    for k, ws in enumerate(boxes):
+        srv.register(f"s{k}", ws)
+    rng = np.random.default_rng(3)
+    work = []
+    for rep in range(3):
+        for k, ws in enumerate(boxes):
+            moved = ws.with_positions(ws.positions() + rng.normal(0.0, 0.005, size=(ws.n, 3)))
+            xyz = [np.ascontiguousarray(a, dtype=np.float64) for a in (moved.x, moved.y, moved.z)]
+            uind = np.full((ws.n, 3), np.nan)
+            ticket, out = srv.submit(f"s{k}", moved, xyz=xyz, uind=uind)
+            assert out is uind
+            work.append((ticket, moved, uind, rep > 0))
+    for ticket, moved, uind, repeat in work:
+        r = srv.wait(ticket)
+        assert r.status == lib.THP_OK and bool(r.warm) == repeat
+        exact = lib.Context(moved, precision=lib.FP64, poleps=1e-8)
+        exact.solve()
+        ue, _ = exact.dipoles()
+        assert np.sqrt(np.mean(np.sum((uind - ue) ** 2, 1))) * DEBYE < 1e-5
+    srv.close()
+
+
+@pytest.mark.gpu
 def test_server_reuses_contexts_under_a_tight_budget(thp):
     from tinker_hp_b200 import serve, lib
     reqs = serve.poisson_stream(24, rate=1000.0, nmin=1000, nmax=8000, repeat_frac=0.3, seed=13)
