@@ -92,6 +92,10 @@ __global__ void __launch_bounds__(kFieldBlock, THP_EFLD0_MINB) k_efld0_coef(
   double e[6] = {0, 0, 0, 0, 0, 0};
   const int nn = min(nnb[i], maxnb);
   int cnt = 0;
+  // list entries one group ahead of their gathers (the list streams from DRAM)
+  int nxt[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) nxt[g] = g < nn ? __ldg(nb + (size_t)g * npad + i) : i;
 #pragma unroll 1
   for (int sb = 0; sb < nn; sb += G) {
     // every load of the group is issued before the arithmetic of any pair
@@ -99,7 +103,9 @@ __global__ void __launch_bounds__(kFieldBlock, THP_EFLD0_MINB) k_efld0_coef(
     double4 pk[G];
     Rec<MIXED> rk[G];
 #pragma unroll
-    for (int g = 0; g < G; ++g) kk[g] = sb + g < nn ? __ldg(nb + (size_t)(sb + g) * npad + i) : i;
+    for (int g = 0; g < G; ++g) kk[g] = nxt[g];
+#pragma unroll
+    for (int g = 0; g < G; ++g) nxt[g] = sb + G + g < nn ? __ldg(nb + (size_t)(sb + G + g) * npad + i) : i;
 #pragma unroll
     for (int g = 0; g < G; ++g) pk[g] = pos[kk[g]];
 #pragma unroll
