@@ -1,13 +1,16 @@
 // solver.cu -- device-resident preconditioned conjugate gradient.
 //
 // inducepcg_pme2 (newinduce_pme2.f:285-636) with every vector and scalar on
-// the device.  Per iteration:
-//   1. pp = zr + beta*pp (and the FP32 copy of the mixed form);
+// the device.  Per iteration (systems of THP_OVERLAP_MIN_ATOMS atoms and
+// more; smaller ones run one fused matvec kernel after the PME branch):
+//   1. pp = zr + beta*pp (the mixed form also writes the 32-byte partner
+//      records of its FP32 real-space row);
 //   2. fork: the real-space row T_real pp runs on the side stream while the
-//      main stream spreads pp on the PME grid, runs cuFFT forward, qfac,
-//      cuFFT backward and gathers the dipole field;
-//   3. join, then the combine kernel: h = T_real pp + pp/alpha + dipfield -
-//      self term; partial pp.h; the last block forms gg and alpha;
+//      main stream spreads pp on the PME grid, runs cuFFT forward, qfac and
+//      cuFFT backward;
+//   3. join, then the combine kernel gathers the dipole field from the grid
+//      and forms h = T_real pp + pp/alpha + dipfield - self term; partial
+//      pp.h; the last block forms gg and alpha;
 //   4. update kernel: mu += alpha pp, res -= alpha h, zr = diag res; partial
 //      ggnew and ene; the last block forms beta, the residual norm and the
 //      convergence / stop flags.
@@ -476,8 +479,9 @@ bool overlap_rows(const Ctx& c) { return c.n >= THP_OVERLAP_MIN_ATOMS; }
 static bool overlapped(const Ctx& c) { return overlap_rows(c); }
 
 // One application of the CG matrix with the real-space row on the side
-// stream and the PME branch (spread, FFTs, gather) on the main stream; x and,
-// for the mixed form, its FP32 copy are final when this is enqueued.
+// stream and the PME branch (spread, FFTs) on the main stream; x and, for
+// the mixed form, its partner records (k_pp_rec) are final when this is
+// enqueued.
 static int matvec_overlapped(Ctx& c, double* x, int init) {
   const int nb = (c.n + kBlock - 1) / kBlock;
   int st;
