@@ -8,7 +8,6 @@
 #include <cstdio>
 #include <cstring>
 #include <initializer_list>
-#include <map>
 #include <mutex>
 #include <vector>
 
@@ -64,12 +63,22 @@ void build_special_pairs(Ctx& c, const int* const* off, const int* const* idx, c
     for (int q = off[slot][i]; q < off[slot][i + 1]; ++q) out.push_back(idx[slot][q]);
   };
   std::vector<int> lst, ip11;
+  // this atom's partners with their (d, p, u) scales, 1 until a rule sets
+  // one; a short list searched linearly and reused across atoms (no per-atom
+  // allocation: servers build this for every new system)
+  struct Ent {
+    int k;
+    std::array<double, 3> s;
+  };
+  std::vector<Ent> m;
+  m.reserve(64);
   for (int i = 0; i < n; ++i) {
-    std::map<int, std::array<double, 3>> m;
+    m.clear();
     auto get = [&](int k) -> std::array<double, 3>& {
-      auto it = m.find(k);
-      if (it == m.end()) it = m.emplace(k, std::array<double, 3>{1.0, 1.0, 1.0}).first;
-      return it->second;
+      for (Ent& e : m)
+        if (e.k == k) return e.s;
+      m.push_back(Ent{k, {1.0, 1.0, 1.0}});
+      return m.back().s;
     };
     row(THP_IP11, i, ip11);
     for (int b = 0; b < 4; ++b) {
@@ -88,11 +97,12 @@ void build_special_pairs(Ctx& c, const int* const* off, const int* const* idx, c
       row(THP_IP11 + b, i, lst);
       for (int k : lst) get(k)[2] = sc[12 + b];
     }
-    for (auto& kv : m) {
-      if (kv.first == i) continue;
-      const auto& s = kv.second;
+    std::sort(m.begin(), m.end(), [](const Ent& a, const Ent& b) { return a.k < b.k; });  // ascending partners
+    for (const Ent& e : m) {
+      if (e.k == i) continue;
+      const auto& s = e.s;
       if (s[0] == 1.0 && s[1] == 1.0 && s[2] == 1.0) continue;
-      c.sp_k.push_back(kv.first);
+      c.sp_k.push_back(e.k);
       c.sp_s.push_back(s[0]);
       c.sp_s.push_back(s[1]);
       c.sp_s.push_back(s[2]);
