@@ -547,7 +547,7 @@ def main():
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": f"{args.workload}: {nw} waters, {n} atoms, box {ws.box[0]:.2f} A, PME "
                                f"{ws.nfft[0]}^3 order 5, alpha {ws.aewald:.4f}, cutoff 7.0+0.5 A",
-                   "form": "mixed (FP32 pair fields/PME, FP64 CG)", "cg_tol": CG_TOL,
+                   "form": "mixed (FP32 pair fields/PME/CG vectors, FP64 CG scalars)", "cg_tol": CG_TOL,
                    "parallelism": f"replicas x{world}", "l2": "inputs > L2 (pair stream ~0.5 GB per matvec)",
                    "iterations": int(np.median(niter))},
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),

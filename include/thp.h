@@ -42,7 +42,7 @@ extern "C" {
 
 /* ---- precision forms ---------------------------------------------------- */
 #define THP_FP64 0  /* everything in FP64 */
-#define THP_MIXED 1 /* FP32 pair fields and PME, FP64 CG scalars and energy */
+#define THP_MIXED 1 /* FP32 pair fields, PME and CG vectors, FP64 CG scalars, mu and energy */
 
 /* ---- connectivity slots (modules couple and polgrp) -------------------- */
 #define THP_I12 0

@@ -402,7 +402,7 @@ size_t footprint_bytes(const thp_config& cfg, int* ncell_out) {
   b += n * 4 + maxnb * npad * 4;                         // list
   b += n * 4 + maxnb * npad * (4 + 2 * (mixed ? 4 : 8));  // pairs
   b += ngrid * (mixed ? 12 : 24);                        // grid + qfac
-  b += 10 * n * 6 * 8 + 4 * n * 8 + n * 6 * 4 + n * 9 * 4;  // vectors, FP32 row input
+  b += 10 * n * 6 * 8 + 4 * n * 8 + n * 6 * 4 + n * 9 * 4 + 4 * n * 6 * 4;  // vectors, FP32 row input and CG vectors
   b += (n / 128 + 2) * 4 * 8 + 4096;
   b += 64 << 20;  // cuFFT work area and runtime slack
   return b;
@@ -539,6 +539,7 @@ static int size_buffers(Ctx& c) {
                      item(&c.d_res, 6 * n), item(&c.d_h, 6 * n), item(&c.d_pp, 6 * n), item(&c.d_zr, 6 * n),
                      item(&c.d_dip, 6 * n), item(&c.d_tmp6, 6 * n), item(&c.d_tmp6b, 6 * n), item(&c.d_cphi, 4 * n),
                      item(&c.d_vecf, 6 * n), item(&c.d_rec, 8 * n), item(&c.d_mpz, n), item(&c.d_ef_prev, 6 * n),
+                     item(&c.d_ppf, 6 * n), item(&c.d_hf, 6 * n), item(&c.d_resf, 6 * n), item(&c.d_zrf, 6 * n),
                      item(&c.d_partials, (size_t)(c.nblk_reduce + 8) * 4)},
                     "per-atom buffers");
     if (!st) c.cap_n = n;

@@ -149,6 +149,9 @@ struct Ctx {
   double* d_ef_prev = nullptr;  // [n][6]
   bool have_ef_prev = false;
   float* d_mpz = nullptr;     // [n]
+  // the mixed form's overlapped CG keeps its search direction, h, residual
+  // and preconditioned residual in FP32 (dot products and scalars in FP64)
+  float *d_ppf = nullptr, *d_hf = nullptr, *d_resf = nullptr, *d_zrf = nullptr;  // [n][6]
   double* d_tmp6 = nullptr;   // [n][6] original-order staging for host I/O
   double* d_tmp6b = nullptr;
   bool have_dipoles = false;

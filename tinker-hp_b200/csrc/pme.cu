@@ -113,32 +113,42 @@ __global__ void k_spread_mpole(int n, PmeGeom g, const double4* __restrict__ pos
 // different L2 slices; a warp-per-site variant that made them contiguous
 // measured 1.6x slower).  mode 1 first forms pp = zr + beta*pp
 // (inducepcg_pme2.f:553-559) and writes it back.
-template <typename T>
+// V: the stored type of vec (FP32 for the mixed form's overlapped CG, which
+// spreads in mode 2 only)
+template <typename T, typename V = double>
 __global__ void __launch_bounds__(128) k_spread_dip(int n, PmeGeom g, const double4* __restrict__ pos,
-                                                   double* __restrict__ vec, const double* __restrict__ zr,
+                                                   V* __restrict__ vec, const double* __restrict__ zr,
                                                    float* __restrict__ vecf, const CgScalars* __restrict__ cg,
                                                    int mode, typename Cplx<T>::type* __restrict__ grid) {
   if (mode >= 1 && cg->stop) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double v[6];
-  const double2* v2 = reinterpret_cast<const double2*>(vec + (size_t)i * 6);
-  double2 a0 = v2[0], a1 = v2[1], a2 = v2[2];
-  v[0] = a0.x; v[1] = a0.y; v[2] = a1.x; v[3] = a1.y; v[4] = a2.x; v[5] = a2.y;
-  if (mode == 1) {
-    const double2* z2 = reinterpret_cast<const double2*>(zr + (size_t)i * 6);
-    double2 b0 = z2[0], b1 = z2[1], b2 = z2[2];
-    double bd = cg->beta[0], bp = cg->beta[1];
-    v[0] = b0.x + bd * v[0];
-    v[1] = b0.y + bd * v[1];
-    v[2] = b1.x + bd * v[2];
-    v[3] = b1.y + bp * v[3];
-    v[4] = b2.x + bp * v[4];
-    v[5] = b2.y + bp * v[5];
-    double2* w2 = reinterpret_cast<double2*>(vec + (size_t)i * 6);
-    w2[0] = make_double2(v[0], v[1]);
-    w2[1] = make_double2(v[2], v[3]);
-    w2[2] = make_double2(v[4], v[5]);
+  if constexpr (std::is_same<V, float>::value) {
+    const float2* v2 = reinterpret_cast<const float2*>(vec + (size_t)i * 6);
+    const float2 a0 = v2[0], a1 = v2[1], a2 = v2[2];
+    v[0] = a0.x; v[1] = a0.y; v[2] = a1.x; v[3] = a1.y; v[4] = a2.x; v[5] = a2.y;
+  } else {
+    const double2* v2 = reinterpret_cast<const double2*>(vec + (size_t)i * 6);
+    double2 a0 = v2[0], a1 = v2[1], a2 = v2[2];
+    v[0] = a0.x; v[1] = a0.y; v[2] = a1.x; v[3] = a1.y; v[4] = a2.x; v[5] = a2.y;
+  }
+  if constexpr (std::is_same<V, double>::value) {
+    if (mode == 1) {
+      const double2* z2 = reinterpret_cast<const double2*>(zr + (size_t)i * 6);
+      double2 b0 = z2[0], b1 = z2[1], b2 = z2[2];
+      double bd = cg->beta[0], bp = cg->beta[1];
+      v[0] = b0.x + bd * v[0];
+      v[1] = b0.y + bd * v[1];
+      v[2] = b1.x + bd * v[2];
+      v[3] = b1.y + bp * v[3];
+      v[4] = b2.x + bp * v[4];
+      v[5] = b2.y + bp * v[5];
+      double2* w2 = reinterpret_cast<double2*>(vec + (size_t)i * 6);
+      w2[0] = make_double2(v[0], v[1]);
+      w2[1] = make_double2(v[2], v[3]);
+      w2[2] = make_double2(v[4], v[5]);
+    }
   }
   if (vecf) {
     float2* o = reinterpret_cast<float2*>(vecf + (size_t)i * 6);
@@ -627,6 +637,19 @@ int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode) {
   if ((st = convolve(c, mode >= 1))) return st;
   if (d_out) st = launch_gather_dip(c, d_out, false);
   return st;
+}
+
+// The overlapped mixed CG's spread of its FP32 search direction (mode 2:
+// stop flag honoured, no update, no FP32 copy), then the convolution.
+int launch_pme_dipole_f32(Ctx& c, const float* d_vec) {
+  PmeGeom g = geom_of(c);
+  int nb = (c.n + kBlock - 1) / kBlock;
+  int st = zero_grid(c);
+  if (st) return st;
+  k_spread_dip<float, float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<float*>(d_vec), nullptr,
+                                                         nullptr, c.d_cg, 2, (cufftComplex*)c.d_grid);
+  if ((st = cuda_status(cudaGetLastError(), &c, "spread dip"))) return st;
+  return convolve(c, true);
 }
 
 int launch_gather_dip(Ctx& c, double* d_out, bool check_stop) {

@@ -39,12 +39,6 @@
 #define THP_ROW_MINB 0
 #endif
 
-// 1: the overlapped matvec gathers the PME dipole field inside its combine
-// kernel, after the real-space row; 0: a separate gather beside the row
-#ifndef THP_GATHER_COMBINE
-#define THP_GATHER_COMBINE 1
-#endif
-
 // systems of at least this many atoms read the mixed row's pair stream
 // (~1.7 kB per atom, far beyond L2 from here on) without allocating in L1
 #ifndef THP_STREAM_NO_L1_ATOMS
@@ -104,6 +98,19 @@ __device__ __forceinline__ void store6(double* p, const double (&v)[6]) {
   q[0] = make_double2(v[0], v[1]);
   q[1] = make_double2(v[2], v[3]);
   q[2] = make_double2(v[4], v[5]);
+}
+
+// FP32-stored vectors of the mixed form's overlapped CG, computed in FP64
+__device__ __forceinline__ void load6(const float* p, double (&v)[6]) {
+  const float2* q = reinterpret_cast<const float2*>(p);
+  const float2 a = q[0], b = q[1], c = q[2];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y;
+}
+__device__ __forceinline__ void store6(float* p, const double (&v)[6]) {
+  float2* q = reinterpret_cast<float2*>(p);
+  q[0] = make_float2((float)v[0], (float)v[1]);
+  q[1] = make_float2((float)v[2], (float)v[3]);
+  q[2] = make_float2((float)v[4], (float)v[5]);
 }
 
 __device__ __forceinline__ double diag_of(double p) { return p == 0.0 ? kTinyPol : p; }
@@ -196,8 +203,9 @@ __global__ void __launch_bounds__(256) k_pp_update(int n, const double* __restri
 // FP32 dipoles from the per-atom records (rec, mpz) with the wrapped FP32
 // position beside them; one thread per atom.  update 0 only writes the
 // records of x.
-__global__ void __launch_bounds__(256) k_pp_rec(int n, int update, const double* __restrict__ zr,
-                                               double* __restrict__ x, const float4* __restrict__ posf,
+template <typename V>
+__global__ void __launch_bounds__(256) k_pp_rec(int n, int update, const V* __restrict__ zr,
+                                               V* __restrict__ x, const float4* __restrict__ posf,
                                                float* __restrict__ rec, float* __restrict__ mpz,
                                                const CgScalars* __restrict__ cg) {
   if (update && cg->stop) return;
@@ -221,11 +229,11 @@ __global__ void __launch_bounds__(256) k_pp_rec(int n, int update, const double*
 }
 
 // real-space part of h only: hreal = T_real x (tmatxb_pme without the diagonal)
-template <bool MIXED, bool NOL1>
+template <bool MIXED, bool NOL1, typename HV>
 __global__ void __launch_bounds__(kBlock, THP_ROW_MINB) k_real_row(PairRows pr, Box box, const double4* __restrict__ pos,
                                                      const float* __restrict__ rec, const double* __restrict__ x,
                                                      const float* __restrict__ mpz, const CgScalars* __restrict__ cg,
-                                                     int check_stop, double* __restrict__ hreal) {
+                                                     int check_stop, HV* __restrict__ hreal) {
   if (check_stop && cg->stop) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= pr.n) return;
@@ -248,13 +256,13 @@ __global__ void __launch_bounds__(kBlock, THP_ROW_MINB) k_real_row(PairRows pr, 
 // GATHER 0 reads dipfield from dipf; 1 / 2 gather it here from the
 // convolved FP32 / FP64 grid (the work of k_gather_dip, without the round
 // trip of dipfield through memory).
-template <int GATHER>
+template <int GATHER, typename XV, typename V>
 __global__ void __launch_bounds__(kBlock) k_cg_combine(int n, const double* __restrict__ dipf, PmeGeom g,
                                                        const double4* __restrict__ pos, const void* __restrict__ grid,
-                                                       const double* __restrict__ x, const double* __restrict__ pol,
+                                                       const XV* __restrict__ x, const double* __restrict__ pol,
                                                        const double* __restrict__ ef, double term, int init,
-                                                       double* __restrict__ h, double* __restrict__ res,
-                                                       double* __restrict__ zr, double* __restrict__ pp, CgScalars* cg,
+                                                       V* __restrict__ h, V* __restrict__ res, V* __restrict__ zr,
+                                                       V* __restrict__ pp, CgScalars* cg,
                                                        double* __restrict__ partials) {
   if (cg->stop) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -315,10 +323,11 @@ __global__ void __launch_bounds__(kBlock) k_cg_combine(int n, const double* __re
 }
 
 // newinduce_pme2.f:512-572
+template <typename V>
 __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __restrict__ pol, const double* __restrict__ ef,
-                                                      const double* __restrict__ h, const double* __restrict__ pp,
-                                                      double* __restrict__ mu, double* __restrict__ res,
-                                                      double* __restrict__ zr, CgScalars* cg, double* __restrict__ partials,
+                                                      const V* __restrict__ h, const V* __restrict__ pp,
+                                                      double* __restrict__ mu, V* __restrict__ res,
+                                                      V* __restrict__ zr, CgScalars* cg, double* __restrict__ partials,
                                                       double poleps, int politer) {
   if (cg->stop) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -482,7 +491,8 @@ static bool overlapped(const Ctx& c) { return overlap_rows(c); }
 // stream and the PME branch (spread, FFTs) on the main stream; x and, for
 // the mixed form, its partner records (k_pp_rec) are final when this is
 // enqueued.
-static int matvec_overlapped(Ctx& c, double* x, int init) {
+template <typename XV>
+static int matvec_overlapped(Ctx& c, const XV* x, int init) {
   const int nb = (c.n + kBlock - 1) / kBlock;
   int st;
   cudaEventRecord(c.ev_fork, c.stream);
@@ -490,36 +500,34 @@ static int matvec_overlapped(Ctx& c, double* x, int init) {
   PairRows pr = pair_rows(c);
   prof_mark(c, c.stream2);
   if (c.mixed && c.n >= THP_STREAM_NO_L1_ATOMS)
-    k_real_row<true, true><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, x, c.d_mpz, c.d_cg, !init,
-                                                         c.d_h);
+    k_real_row<true, true, float><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, nullptr, c.d_mpz, c.d_cg,
+                                                                !init, c.d_hf);
   else if (c.mixed)
-    k_real_row<true, false><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, x, c.d_mpz, c.d_cg, !init,
-                                                          c.d_h);
-  else
-    k_real_row<false, false><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, nullptr, x, nullptr, c.d_cg, !init,
-                                                           c.d_h);
+    k_real_row<true, false, float><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, nullptr, c.d_mpz,
+                                                                 c.d_cg, !init, c.d_hf);
+  else if constexpr (std::is_same<XV, double>::value)
+    k_real_row<false, false, double><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, nullptr, x, nullptr, c.d_cg,
+                                                                   !init, c.d_h);
   prof_mark(c, c.stream2);
   if ((st = cuda_status(cudaGetLastError(), &c, "real row"))) return st;
   cudaEventRecord(c.ev_join, c.stream2);
-  if ((st = launch_pme_dipole(c, x, nullptr, 2))) return st;
+  if constexpr (std::is_same<XV, float>::value)
+    st = launch_pme_dipole_f32(c, x);
+  else
+    st = launch_pme_dipole(c, x, nullptr, 2);
+  if (st) return st;
   const double a = c.cfg.aewald;
   const double term = (4.0 / 3.0) * a * a * a / kSqrtPi;
   const PmeGeom g = pme_geom(c);
-#define THP_COMBINE_ARGS                                                                                        \
-  c.n, c.d_dip, g, c.d_pos, c.d_grid, x, c.d_pol, c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, c.d_cg, \
-      c.d_partials
-  if (THP_GATHER_COMBINE) {
-    cudaStreamWaitEvent(c.stream, c.ev_join, 0);
-    if (c.mixed)
-      k_cg_combine<1><<<nb, kBlock, 0, c.stream>>>(THP_COMBINE_ARGS);
-    else
-      k_cg_combine<2><<<nb, kBlock, 0, c.stream>>>(THP_COMBINE_ARGS);
-  } else {
-    if ((st = launch_gather_dip(c, c.d_dip, true))) return st;
-    cudaStreamWaitEvent(c.stream, c.ev_join, 0);
-    k_cg_combine<0><<<nb, kBlock, 0, c.stream>>>(THP_COMBINE_ARGS);
-  }
-#undef THP_COMBINE_ARGS
+  cudaStreamWaitEvent(c.stream, c.ev_join, 0);
+  if (c.mixed)
+    k_cg_combine<1, XV, float><<<nb, kBlock, 0, c.stream>>>(c.n, nullptr, g, c.d_pos, c.d_grid, x, c.d_pol, c.d_ef,
+                                                            term, init, c.d_hf, c.d_resf, c.d_zrf, c.d_ppf, c.d_cg,
+                                                            c.d_partials);
+  else if constexpr (std::is_same<XV, double>::value)
+    k_cg_combine<2, double, double><<<nb, kBlock, 0, c.stream>>>(c.n, nullptr, g, c.d_pos, c.d_grid, x, c.d_pol,
+                                                                 c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp,
+                                                                 c.d_cg, c.d_partials);
   return cuda_status(cudaGetLastError(), &c, "cg combine");
 }
 
@@ -545,20 +553,26 @@ static int launch_matvec(Ctx& c, const double* x, int init) {
 
 static int enqueue_iteration(Ctx& c) {
   int st;
-  if (overlapped(c)) {
-    if (c.mixed)
-      k_pp_rec<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, 1, c.d_zr, c.d_pp, c.d_posf, c.d_rec, c.d_mpz, c.d_cg);
-    else
-      k_pp_update<<<(6 * c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.d_zr, c.d_pp, c.d_cg);
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  if (overlapped(c) && c.mixed) {
+    k_pp_rec<float><<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, 1, c.d_zrf, c.d_ppf, c.d_posf, c.d_rec, c.d_mpz,
+                                                             c.d_cg);
     if ((st = cuda_status(cudaGetLastError(), &c, "pp update"))) return st;
-    if ((st = matvec_overlapped(c, c.d_pp, 0))) return st;
+    if ((st = matvec_overlapped<float>(c, c.d_ppf, 0))) return st;
+    k_cg_update<float><<<nb, kBlock, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_hf, c.d_ppf, c.d_mu, c.d_resf,
+                                                    c.d_zrf, c.d_cg, c.d_partials, c.cfg.poleps, c.cfg.politer);
+    return cuda_status(cudaGetLastError(), &c, "cg update");
+  }
+  if (overlapped(c)) {
+    k_pp_update<<<(6 * c.n + 255) / 256, 256, 0, c.stream>>>(c.n, c.d_zr, c.d_pp, c.d_cg);
+    if ((st = cuda_status(cudaGetLastError(), &c, "pp update"))) return st;
+    if ((st = matvec_overlapped<double>(c, c.d_pp, 0))) return st;
   } else {
     if ((st = launch_pme_dipole(c, c.d_pp, nullptr, 1))) return st;
     if ((st = launch_matvec(c, c.d_pp, 0))) return st;
   }
-  const int nb = (c.n + kBlock - 1) / kBlock;
-  k_cg_update<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_h, c.d_pp, c.d_mu, c.d_res, c.d_zr, c.d_cg,
-                                           c.d_partials, c.cfg.poleps, c.cfg.politer);
+  k_cg_update<double><<<nb, kBlock, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_h, c.d_pp, c.d_mu, c.d_res, c.d_zr,
+                                                   c.d_cg, c.d_partials, c.cfg.poleps, c.cfg.politer);
   return cuda_status(cudaGetLastError(), &c, "cg update");
 }
 
@@ -580,10 +594,11 @@ int pcg_begin(Ctx& c, int guess) {
   if ((st = cuda_status(cudaGetLastError(), &c, "cg start"))) return st;
   if (overlapped(c)) {
     if (c.mixed) {
-      k_pp_rec<<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, 0, c.d_zr, c.d_mu, c.d_posf, c.d_rec, c.d_mpz, c.d_cg);
+      k_pp_rec<double><<<(c.n + 255) / 256, 256, 0, c.stream>>>(c.n, 0, nullptr, c.d_mu, c.d_posf, c.d_rec, c.d_mpz,
+                                                                c.d_cg);
       if ((st = cuda_status(cudaGetLastError(), &c, "mu copy"))) return st;
     }
-    return matvec_overlapped(c, c.d_mu, 1);
+    return matvec_overlapped<double>(c, c.d_mu, 1);
   }
   if ((st = launch_pme_dipole(c, c.d_mu, nullptr, 0))) return st;
   return launch_matvec(c, c.d_mu, 1);
