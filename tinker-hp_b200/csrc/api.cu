@@ -6,6 +6,7 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <initializer_list>
 #include <mutex>
@@ -52,11 +53,11 @@ int dmalloc(Ctx& c, T** p, size_t count, const char* what) {
 // (:1495-1518): pscale from i12..i15 (p*iscale when the partner is in ip11),
 // dscale and uscale from ip11..ip14.  Pairs whose three scales are all 1 are
 // dropped.
-void build_special_pairs(Ctx& c, const int* const* off, const int* const* idx, const double* sc) {
-  const int n = c.n;
-  c.sp_off.assign(n + 1, 0);
-  c.sp_k.clear();
-  c.sp_s.clear();
+static void special_pairs(int n, const int* const* off, const int* const* idx, const double* sc,
+                          std::vector<int>& sp_off, std::vector<int>& sp_k, std::vector<double>& sp_s) {
+  sp_off.assign(n + 1, 0);
+  sp_k.clear();
+  sp_s.clear();
   auto row = [&](int slot, int i, std::vector<int>& out) {
     out.clear();
     if (!off || !off[slot] || !idx[slot]) return;
@@ -102,17 +103,22 @@ void build_special_pairs(Ctx& c, const int* const* off, const int* const* idx, c
       if (e.k == i) continue;
       const auto& s = e.s;
       if (s[0] == 1.0 && s[1] == 1.0 && s[2] == 1.0) continue;
-      c.sp_k.push_back(e.k);
-      c.sp_s.push_back(s[0]);
-      c.sp_s.push_back(s[1]);
-      c.sp_s.push_back(s[2]);
+      sp_k.push_back(e.k);
+      sp_s.push_back(s[0]);
+      sp_s.push_back(s[1]);
+      sp_s.push_back(s[2]);
     }
-    c.sp_off[i + 1] = (int)c.sp_k.size();
+    sp_off[i + 1] = (int)sp_k.size();
   }
 }
 
-int upload_special_pairs(Ctx& c) {
-  c.have_list = false;  // sorted partner numbers are made at the next sort
+void build_special_pairs(Ctx& c, const int* const* off, const int* const* idx, const double* sc) {
+  special_pairs(c.n, off, idx, sc, c.sp_off, c.sp_k, c.sp_s);
+}
+
+// Device buffers for the special pairs of the context's system (kept while
+// large enough).
+static int reserve_special_pairs(Ctx& c) {
   int st;
   // buffers are kept while large enough, so re-targeting a context does not
   // free device memory (cudaFree waits for the whole device)
@@ -136,6 +142,13 @@ int upload_special_pairs(Ctx& c) {
     if ((st = dmalloc(c, &c.d_sp_s, 3 * m, "alloc sp_s"))) return st;
     c.cap_sp = m;
   }
+  return THP_OK;
+}
+
+int upload_special_pairs(Ctx& c) {
+  c.have_list = false;  // sorted partner numbers are made at the next sort
+  int st = reserve_special_pairs(c);
+  if (st) return st;
   cudaMemcpyAsync(c.d_sp_off, c.sp_off.data(), sizeof(int) * (c.n + 1), cudaMemcpyHostToDevice, c.stream);
   if (!c.sp_k.empty()) {
     cudaMemcpyAsync(c.d_sp_k, c.sp_k.data(), sizeof(int) * c.sp_k.size(), cudaMemcpyHostToDevice, c.stream);
@@ -709,6 +722,129 @@ int thp_set_connectivity(thp_ctx* h, const int* const* off, const int* const* id
 // flag check returns THP_E_INVALID.  (Also used by the request loop.)
 }  // extern "C"
 namespace thp {
+
+// A system's inputs prepared once on the host for the request loop: checked,
+// special pairs built, frames packed, all in pinned memory when the driver
+// gives it.  Loading the image onto a context is then a few asynchronous
+// copies on the context's stream with no host wait, where thp_set_params,
+// thp_set_connectivity and thp_set_frames each build, stage and synchronise.
+struct SystemImage {
+  int n = 0, m = 0;
+  double scales[16] = {};
+  bool pinned = false;
+  double* par = nullptr;   // [3n] pdamp, thole, polarity (the d_par_orig planes)
+  double* pole = nullptr;  // [13n] local-frame multipoles
+  int* frames = nullptr;   // [3n] z-axis, x-axis, frame type
+  int* sp_off = nullptr;   // [n+1]
+  int* sp_k = nullptr;     // [m]
+  double* sp_s = nullptr;  // [3m]
+  void* block = nullptr;
+};
+
+void image_free(SystemImage* img) {
+  if (!img) return;
+  if (img->pinned)
+    cudaFreeHost(img->block);
+  else
+    std::free(img->block);
+  delete img;
+}
+
+int image_create(const thp_config& cfg, const double* polarity, const double* thole, const double* pdamp,
+                 const int* const* off, const int* const* idx, const double* scales, const double* pole,
+                 const int* zaxis, const int* xaxis, const int* axt, SystemImage** out) {
+  *out = nullptr;
+  const int n = cfg.n;
+  if (n <= 0 || !polarity || !thole || !pdamp || !scales || !pole || !zaxis || !xaxis || !axt)
+    return THP_E_INVALID;
+  for (int i = 0; i < n; ++i)
+    if (zaxis[i] < 0 || zaxis[i] >= n || xaxis[i] < 0 || xaxis[i] >= n || (axt[i] != 1 && axt[i] != 2))
+      return THP_E_INVALID;
+  std::vector<int> so, sk;
+  std::vector<double> ss;
+  special_pairs(n, off, idx, scales, so, sk, ss);
+  auto* img = new SystemImage();
+  img->n = n;
+  img->m = (int)sk.size();
+  std::memcpy(img->scales, scales, sizeof(img->scales));
+  const size_t nd = 3 * (size_t)n + 13 * (size_t)n + 3 * (size_t)img->m;
+  const size_t ni = 3 * (size_t)n + (size_t)n + 1 + (size_t)img->m;
+  const size_t bytes = nd * sizeof(double) + ni * sizeof(int);
+  if (cudaHostAlloc(&img->block, bytes, cudaHostAllocDefault) == cudaSuccess) {
+    img->pinned = true;
+  } else {
+    cudaGetLastError();  // no device here: the requests will report it
+    img->block = std::malloc(bytes);
+    if (!img->block) {
+      delete img;
+      return THP_E_INVALID;
+    }
+  }
+  double* d = static_cast<double*>(img->block);
+  img->par = d;
+  img->pole = d + 3 * (size_t)n;
+  img->sp_s = img->pole + 13 * (size_t)n;
+  int* q = reinterpret_cast<int*>(img->sp_s + 3 * (size_t)img->m);
+  img->frames = q;
+  img->sp_off = q + 3 * (size_t)n;
+  img->sp_k = img->sp_off + n + 1;
+  std::memcpy(img->par, pdamp, sizeof(double) * n);
+  std::memcpy(img->par + n, thole, sizeof(double) * n);
+  std::memcpy(img->par + 2 * (size_t)n, polarity, sizeof(double) * n);
+  std::memcpy(img->pole, pole, sizeof(double) * 13 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    img->frames[3 * i] = zaxis[i];
+    img->frames[3 * i + 1] = xaxis[i];
+    img->frames[3 * i + 2] = axt[i];
+  }
+  std::memcpy(img->sp_off, so.data(), sizeof(int) * (n + 1));
+  if (img->m) {
+    std::memcpy(img->sp_k, sk.data(), sizeof(int) * img->m);
+    std::memcpy(img->sp_s, ss.data(), sizeof(double) * 3 * (size_t)img->m);
+  }
+  *out = img;
+  return THP_OK;
+}
+
+// Parameters, connectivity and frames of the image onto a context sized for
+// it (the state thp_set_params, thp_set_connectivity and thp_set_frames
+// leave), stream-ordered before the context's next solve.
+int image_load(thp_ctx* h, const SystemImage* img) {
+  if (!h || !img) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (img->n != c.n) return THP_E_INVALID;
+  drop_front_graphs(c);
+  if (set_current_device(c)) return THP_E_CUDA;
+  const size_t n = c.n;
+  c.h_pdamp.assign(img->par, img->par + n);
+  c.h_thole.assign(img->par + n, img->par + 2 * n);
+  c.h_polarity.assign(img->par + 2 * n, img->par + 3 * n);
+  cudaMemcpyAsync(c.d_par_orig, img->par, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c.stream);
+  c.have_params = true;
+  std::memcpy(c.scales, img->scales, sizeof(c.scales));
+  c.sp_off.assign(img->sp_off, img->sp_off + n + 1);
+  c.sp_k.assign(img->sp_k, img->sp_k + img->m);
+  c.sp_s.assign(img->sp_s, img->sp_s + 3 * (size_t)img->m);
+  c.have_conn = true;
+  int st = reserve_special_pairs(c);
+  if (st) return st;
+  cudaMemcpyAsync(c.d_sp_off, img->sp_off, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c.stream);
+  if (img->m) {
+    cudaMemcpyAsync(c.d_sp_k, img->sp_k, sizeof(int) * img->m, cudaMemcpyHostToDevice, c.stream);
+    cudaMemcpyAsync(c.d_sp_s, img->sp_s, sizeof(double) * 3 * img->m, cudaMemcpyHostToDevice, c.stream);
+  }
+  cudaMemcpyAsync(c.d_pole_local, img->pole, sizeof(double) * 13 * n, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(c.d_frames, img->frames, sizeof(int) * 3 * n, cudaMemcpyHostToDevice, c.stream);
+  c.have_frames = true;
+  c.have_axes = true;
+  c.have_list = false;
+  c.have_coef = false;
+  h->pos_dirty = true;
+  h->rpole_dirty = true;
+  h->field_valid = false;
+  return cuda_status(cudaGetLastError(), &c, "load system");
+}
+
 int upload_positions(thp_ctx* h, const double* x, const double* y, const double* z, bool host_check) {
   if (!h || !x || !y || !z) return THP_E_INVALID;
   Ctx& c = h->c;

@@ -26,6 +26,12 @@
 namespace thp {
 int plan_prefetch(int device, const int nfft[3], int mixed);
 int upload_positions(thp_ctx* h, const double* x, const double* y, const double* z, bool host_check);
+struct SystemImage;
+int image_create(const thp_config& cfg, const double* polarity, const double* thole, const double* pdamp,
+                 const int* const* off, const int* const* idx, const double* scales, const double* pole,
+                 const int* zaxis, const int* xaxis, const int* axt, SystemImage** out);
+void image_free(SystemImage* img);
+int image_load(thp_ctx* h, const SystemImage* img);
 }
 
 namespace {
@@ -40,12 +46,13 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
+// A registered system: its configuration and its inputs prepared for fast
+// loading onto a context (thp::SystemImage, pinned host memory).
 struct SysRec {
   thp_config cfg{};
-  std::vector<double> polarity, thole, pdamp, scales, pole;
-  std::vector<int> zaxis, xaxis, axt;
-  std::vector<int> off[8], idx[8];
+  thp::SystemImage* img = nullptr;
   size_t footprint = 0;
+  ~SysRec() { thp::image_free(img); }
 };
 
 struct Req {
@@ -111,18 +118,7 @@ thp_config server_cfg(const thp_server_config& s, const thp_config& sys) {
 }  // namespace
 
 // Sets every system input of a fresh or re-targeted context.
-int thp_server::load_system(thp_ctx* h, const SysRec& sys) {
-  int st = thp_set_params(h, sys.polarity.data(), sys.thole.data(), sys.pdamp.data());
-  if (st) return st;
-  const int* offp[8];
-  const int* idxp[8];
-  for (int q = 0; q < 8; ++q) {
-    offp[q] = sys.off[q].data();
-    idxp[q] = sys.idx[q].empty() ? nullptr : sys.idx[q].data();
-  }
-  if ((st = thp_set_connectivity(h, offp, idxp, sys.scales.data()))) return st;
-  return thp_set_frames(h, sys.pole.data(), sys.zaxis.data(), sys.xaxis.data(), sys.axt.data());
-}
+int thp_server::load_system(thp_ctx* h, const SysRec& sys) { return thp::image_load(h, sys.img); }
 
 // Under the lock: makes the system resident and marks it busy.  On return
 // with THP_OK, slot is its entry; fresh is true when the caller must load
@@ -329,28 +325,15 @@ int thp_server_register(thp_server* s, unsigned long long key, const thp_system*
   auto rec = std::make_shared<SysRec>();
   const size_t n = sys->cfg.n;
   rec->cfg = sys->cfg;
-  rec->polarity.assign(sys->polarity, sys->polarity + n);
-  rec->thole.assign(sys->thole, sys->thole + n);
-  rec->pdamp.assign(sys->pdamp, sys->pdamp + n);
-  rec->scales.assign(sys->scales, sys->scales + 16);
-  rec->pole.assign(sys->pole, sys->pole + 13 * n);
-  rec->zaxis.assign(sys->zaxis, sys->zaxis + n);
-  rec->xaxis.assign(sys->xaxis, sys->xaxis + n);
-  rec->axt.assign(sys->axt, sys->axt + n);
   for (int q = 0; q < 8; ++q) {
     const int* off = sys->conn_off[q];
-    if (!off) {
-      rec->off[q].assign(n + 1, 0);
-      continue;
-    }
-    rec->off[q].assign(off, off + n + 1);
+    if (!off) continue;
     const int m = off[n];
-    if (m < 0) return THP_E_INVALID;
-    if (m > 0) {
-      if (!sys->conn_idx[q]) return THP_E_INVALID;
-      rec->idx[q].assign(sys->conn_idx[q], sys->conn_idx[q] + m);
-    }
+    if (m < 0 || (m > 0 && !sys->conn_idx[q])) return THP_E_INVALID;
   }
+  int st = thp::image_create(sys->cfg, sys->polarity, sys->thole, sys->pdamp, sys->conn_off, sys->conn_idx,
+                             sys->scales, sys->pole, sys->zaxis, sys->xaxis, sys->axt, &rec->img);
+  if (st) return st;
   const thp_config k = server_cfg(s->cfg, sys->cfg);
   rec->footprint = thp_footprint(&k);
   // the FFT plan of this shape is made now, not by the first request: a new
