@@ -9,6 +9,7 @@
 // the fractional <-> Cartesian matrices reduce to a_d = nfft_d * recip(d,d).
 #include <vector>
 
+#include <map>
 #include <mutex>
 #include <type_traits>
 
@@ -490,13 +491,25 @@ __global__ void k_qfac_init(int n1, int n2, int n3, const double* __restrict__ b
 
 }  // namespace
 
+// B-spline moduli by grid length, computed once per process (an O(K^2)
+// trigonometric sum per axis; servers re-target contexts to new grids often)
+static const std::vector<double>& dftmod_cached(int nfft) {
+  static std::mutex mu;
+  static std::map<int, std::vector<double>> cache;
+  std::lock_guard<std::mutex> g(mu);
+  auto it = cache.find(nfft);
+  if (it == cache.end()) it = cache.emplace(nfft, dftmod_host(nfft, kBs)).first;
+  return it->second;  // map nodes are stable: the reference outlives the lock
+}
+
 int pme_init(Ctx& c) {
   for (int d = 0; d < 3; ++d) c.nfft[d] = c.cfg.nfft[d];
   c.ngrid = (size_t)c.nfft[0] * c.nfft[1] * c.nfft[2];
   for (int d = 0; d < 3; ++d) c.a_frac[d] = (double)c.nfft[d] * c.box.recip[d];
   // influence function (newinduce_pme.f:1802-1854)
-  std::vector<double> m1 = dftmod_host(c.nfft[0], kBs), m2 = dftmod_host(c.nfft[1], kBs),
-                      m3 = dftmod_host(c.nfft[2], kBs);
+  const std::vector<double>& m1 = dftmod_cached(c.nfft[0]);
+  const std::vector<double>& m2 = dftmod_cached(c.nfft[1]);
+  const std::vector<double>& m3 = dftmod_cached(c.nfft[2]);
   size_t esz = c.mixed ? sizeof(float) : sizeof(double);
   size_t csz = c.mixed ? sizeof(cufftComplex) : sizeof(cufftDoubleComplex);
   // grid buffers are kept while they are large enough (a re-targeted
@@ -529,7 +542,9 @@ int pme_init(Ctx& c) {
     k_qfac_init<double><<<blocks, 256, 0, c.stream>>>(c.nfft[0], c.nfft[1], c.nfft[2], d_bsm, c.box.recip[0],
                                                       c.box.recip[1], c.box.recip[2], pterm, volterm,
                                                       (double*)c.d_qfac);
-  if (cuda_status(cudaStreamSynchronize(c.stream), &c, "qfac")) return THP_E_CUDA;
+  // no host wait: the influence function is ready, stream-ordered, for the
+  // context's next solve (bsm is copied out before the call returns)
+  if (cuda_status(cudaGetLastError(), &c, "qfac")) return THP_E_CUDA;
   // cuFFT dims: slowest first; data [n3][n2][n1]; the plan is kept when the
   // grid dimensions are unchanged
   const bool same = c.have_plan && c.plan_dims[0] == c.nfft[0] && c.plan_dims[1] == c.nfft[1] &&
