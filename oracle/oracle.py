@@ -35,6 +35,7 @@ class OrSystem(C.Structure):
         ("vdwcut", C.c_double),
         ("nfft1", C.c_int), ("nfft2", C.c_int), ("nfft3", C.c_int), ("bsorder", C.c_int),
         ("politer", C.c_int), ("poleps", C.c_double), ("nthreads", C.c_int),
+        ("m_scale", C.c_double * 4),
     ]
 
 
@@ -68,6 +69,7 @@ def lib():
         L.or_epolar.restype = C.c_double
         L.or_epolar.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         L.or_epolar1.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, _dp, _dp]
+        L.or_empole1.argtypes = [C.c_void_p, _ip, _ip, _ip, _dp, _dp]
         L.or_rotpole.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _dp]
         L.or_grid_uind_sites.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp, _dp]
         L.or_fphi_uind_sites.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp, _dp, _dp]
@@ -131,7 +133,7 @@ class Oracle:
             self._keep += [off, idx]
             s.conn_off[q] = _p(off, _ip)
             s.conn_idx[q] = _p(idx, _ip)
-        for key in ("p_scale", "pi_scale", "d_scale", "u_scale"):
+        for key in ("p_scale", "pi_scale", "d_scale", "u_scale", "m_scale"):
             arr = getattr(s, key)
             for q in range(4):
                 arr[q] = ws.scales[key][q]
@@ -220,6 +222,19 @@ class Oracle:
         if st != 0:
             raise RuntimeError(f"oracle epolar1 status {st}")
         return ep.value, dep
+
+    def empole1(self):
+        """Permanent-multipole energy and gradient, empole1c: returns
+        (em, dem [n,3], parts) with parts = (real, recip, self) kcal/mol."""
+        dem = np.zeros((self.ws.n, 3))
+        parts = np.zeros(4)
+        ws = self.ws
+        st = lib().or_empole1(self.ctx, _p(np.ascontiguousarray(ws.zaxis, np.int32), _ip),
+                              _p(np.ascontiguousarray(ws.xaxis, np.int32), _ip),
+                              _p(np.ascontiguousarray(ws.axt, np.int32), _ip), _p(dem), _p(parts))
+        if st != 0:
+            raise RuntimeError(f"oracle empole1 status {st}")
+        return parts[0], dem, tuple(parts[1:])
 
     def grid_uind_sites(self, sites, fuind, fuinp, grid):
         """grid_uind_site for 0-based `sites`: adds into a copy of the complex

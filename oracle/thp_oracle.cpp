@@ -2009,4 +2009,225 @@ int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxi
   return OR_OK;
 }
 
+// ===========================================================================
+// Permanent-multipole energy and gradient: empole1c (empole1.f:42-340) for the
+// TINFOIL boundary, without charge penetration, charge flux or lambda terms:
+// emrecip1 (:349-861), emreal1c (:873-1555, standard branch) over the half
+// list, the Ewald self energy (:134-160), torques distributed by torque
+// (torque.f:6-390).  Virial terms are not restated.
+int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, double* dem, double* parts) {
+  const OrSystem& s = c->s;
+  const int n = s.n, maxelst = c->maxelst;
+  if (!c->have_list) return OR_E_LIST_OVERFLOW;
+  std::fill(dem, dem + (size_t)n * 3, 0.0);
+  const double f = kElectric;  // electric / dielec, dielec = 1
+  double erecip = 0.0, ereal = 0.0, eself = 0.0;
+  // ---- emrecip1 ----------------------------------------------------------
+  {
+    // the multipole grid, convolved, and fphirec(20) (unscaled)
+    std::vector<double> cphi0((size_t)n * 10);
+    or_efld0_recip(c, cphi0.data());
+    static const int deriv1[10] = {2, 5, 8, 9, 11, 16, 18, 14, 15, 20};
+    static const int deriv2[10] = {3, 8, 6, 10, 14, 12, 19, 16, 20, 17};
+    static const int deriv3[10] = {4, 9, 10, 7, 15, 17, 13, 20, 18, 19};
+    double ctf[10][10], ftc[10][10];
+    cart_to_frac(c, ctf);
+    frac_to_cart(c, ftc);
+    const int nf[3] = {s.nfft1, s.nfft2, s.nfft3};
+    std::vector<double> demrec((size_t)n * 3, 0.0);
+    for (int i = 0; i < n; ++i) {
+      const double* rp = &s.rpole[(size_t)i * 13];
+      const double cm[10] = {rp[0], rp[1], rp[2], rp[3], rp[4], rp[8], rp[12], 2.0 * rp[5], 2.0 * rp[6], 2.0 * rp[9]};
+      double fm[10];
+      fm[0] = ctf[0][0] * cm[0];
+      for (int j = 1; j < 4; ++j) {
+        fm[j] = 0.0;
+        for (int k = 1; k < 4; ++k) fm[j] += ctf[j][k] * cm[k];
+      }
+      for (int j = 4; j < 10; ++j) {
+        fm[j] = 0.0;
+        for (int k = 4; k < 10; ++k) fm[j] += ctf[j][k] * cm[k];
+      }
+      // fphirec = electric * fphirec; 1-based view FR[1..20]
+      double FR[21];
+      for (int q = 0; q < 20; ++q) FR[q + 1] = f * c->fphirec[(size_t)i * 20 + q];
+      double cp[10];  // fphi_to_cphi_site
+      cp[0] = ftc[0][0] * FR[1];
+      for (int j = 1; j < 4; ++j) {
+        cp[j] = 0.0;
+        for (int k = 1; k < 4; ++k) cp[j] += ftc[j][k] * FR[k + 1];
+      }
+      for (int j = 4; j < 10; ++j) {
+        cp[j] = 0.0;
+        for (int k = 4; k < 10; ++k) cp[j] += ftc[j][k] * FR[k + 1];
+      }
+      double f1 = 0.0, f2 = 0.0, f3 = 0.0;
+      for (int k = 0; k < 10; ++k) {
+        erecip += fm[k] * FR[k + 1];
+        f1 += fm[k] * FR[deriv1[k]];
+        f2 += fm[k] * FR[deriv2[k]];
+        f3 += fm[k] * FR[deriv3[k]];
+      }
+      f1 = (double)nf[0] * f1;
+      f2 = (double)nf[1] * f2;
+      f3 = (double)nf[2] * f3;
+      demrec[i * 3 + 0] += c->recip[0][0] * f1 + c->recip[0][1] * f2 + c->recip[0][2] * f3;
+      demrec[i * 3 + 1] += c->recip[1][0] * f1 + c->recip[1][1] * f2 + c->recip[1][2] * f3;
+      demrec[i * 3 + 2] += c->recip[2][0] * f1 + c->recip[2][1] * f2 + c->recip[2][2] * f3;
+      double trq[3];
+      trq[0] = cm[3] * cp[2] - cm[2] * cp[3] + 2.0 * (cm[6] - cm[5]) * cp[9] + cm[8] * cp[7] + cm[9] * cp[5] -
+               cm[7] * cp[8] - cm[9] * cp[6];
+      trq[1] = cm[1] * cp[3] - cm[3] * cp[1] + 2.0 * (cm[4] - cm[6]) * cp[8] + cm[7] * cp[9] + cm[8] * cp[6] -
+               cm[8] * cp[4] - cm[9] * cp[7];
+      trq[2] = cm[2] * cp[1] - cm[1] * cp[2] + 2.0 * (cm[5] - cm[4]) * cp[7] + cm[7] * cp[4] + cm[9] * cp[8] -
+               cm[7] * cp[5] - cm[8] * cp[9];
+      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], trq, demrec.data());  // torque_rec
+    }
+    erecip = 0.5 * erecip;
+    for (size_t q = 0; q < (size_t)n * 3; ++q) dem[q] += demrec[q];
+  }
+  // ---- emreal1c (standard branch) ----------------------------------------
+  {
+    const double off2 = s.ewaldcut * s.ewaldcut;
+    std::vector<double> mscale(n, 1.0), tem((size_t)n * 3, 0.0);
+    const int mslot[4] = {OR_I12, OR_I13, OR_I14, OR_I15};
+    for (int i = 0; i < n; ++i) {
+      const double* ri = &s.rpole[(size_t)i * 13];
+      const double ci = ri[0], dix = ri[1], diy = ri[2], diz = ri[3];
+      const double qixx = ri[4], qixy = ri[5], qixz = ri[6], qiyy = ri[8], qiyz = ri[9], qizz = ri[12];
+      for (int b = 0; b < 4; ++b) for_conn(s, mslot[b], i, [&](int k) { mscale[k] = s.m_scale[b]; });
+      for (int kkk = 0; kkk < c->nelst[i]; ++kkk) {
+        const int k = c->elst[(size_t)i * maxelst + kkk];
+        double xr = s.x[k] - s.x[i], yr = s.y[k] - s.y[i], zr = s.z[k] - s.z[i];
+        image(c->cell, xr, yr, zr);
+        const double r2 = xr * xr + yr * yr + zr * zr;
+        if (!(r2 <= off2)) continue;
+        const double r = std::sqrt(r2);
+        const double* rk = &s.rpole[(size_t)k * 13];
+        const double ck = rk[0], dkx = rk[1], dky = rk[2], dkz = rk[3];
+        const double qkxx = rk[4], qkxy = rk[5], qkxz = rk[6], qkyy = rk[8], qkyz = rk[9], qkzz = rk[12];
+        // intermediates involving moments and separation distance
+        const double dir = dix * xr + diy * yr + diz * zr;
+        const double qix = qixx * xr + qixy * yr + qixz * zr;
+        const double qiy = qixy * xr + qiyy * yr + qiyz * zr;
+        const double qiz = qixz * xr + qiyz * yr + qizz * zr;
+        const double qir = qix * xr + qiy * yr + qiz * zr;
+        const double dkr = dkx * xr + dky * yr + dkz * zr;
+        const double qkx = qkxx * xr + qkxy * yr + qkxz * zr;
+        const double qky = qkxy * xr + qkyy * yr + qkyz * zr;
+        const double qkz = qkxz * xr + qkyz * yr + qkzz * zr;
+        const double qkr = qkx * xr + qky * yr + qkz * zr;
+        const double dik = dix * dkx + diy * dky + diz * dkz;
+        const double qik = qix * qkx + qiy * qky + qiz * qkz;
+        const double diqk = dix * qkx + diy * qky + diz * qkz;
+        const double dkqi = dkx * qix + dky * qiy + dkz * qiz;
+        const double qiqk = 2.0 * (qixy * qkxy + qixz * qkxz + qiyz * qkyz) + qixx * qkxx + qiyy * qkyy + qizz * qkzz;
+        // additional intermediates involving moments and distance
+        const double dirx = diy * zr - diz * yr, diry = diz * xr - dix * zr, dirz = dix * yr - diy * xr;
+        const double dkrx = dky * zr - dkz * yr, dkry = dkz * xr - dkx * zr, dkrz = dkx * yr - dky * xr;
+        const double dikx = diy * dkz - diz * dky, diky = diz * dkx - dix * dkz, dikz = dix * dky - diy * dkx;
+        const double qirx = qiz * yr - qiy * zr, qiry = qix * zr - qiz * xr, qirz = qiy * xr - qix * yr;
+        const double qkrx = qkz * yr - qky * zr, qkry = qkx * zr - qkz * xr, qkrz = qky * xr - qkx * yr;
+        const double qikx = qky * qiz - qkz * qiy, qiky = qkz * qix - qkx * qiz, qikz = qkx * qiy - qky * qix;
+        const double qixk = qixx * qkx + qixy * qky + qixz * qkz;
+        const double qiyk = qixy * qkx + qiyy * qky + qiyz * qkz;
+        const double qizk = qixz * qkx + qiyz * qky + qizz * qkz;
+        const double qkxi = qkxx * qix + qkxy * qiy + qkxz * qiz;
+        const double qkyi = qkxy * qix + qkyy * qiy + qkyz * qiz;
+        const double qkzi = qkxz * qix + qkyz * qiy + qkzz * qiz;
+        const double qikrx = qizk * yr - qiyk * zr, qikry = qixk * zr - qizk * xr, qikrz = qiyk * xr - qixk * yr;
+        const double qkirx = qkzi * yr - qkyi * zr, qkiry = qkxi * zr - qkzi * xr, qkirz = qkyi * xr - qkxi * yr;
+        const double diqkx = dix * qkxx + diy * qkxy + diz * qkxz;
+        const double diqky = dix * qkxy + diy * qkyy + diz * qkyz;
+        const double diqkz = dix * qkxz + diy * qkyz + diz * qkzz;
+        const double dkqix = dkx * qixx + dky * qixy + dkz * qixz;
+        const double dkqiy = dkx * qixy + dky * qiyy + dkz * qiyz;
+        const double dkqiz = dkx * qixz + dky * qiyz + dkz * qizz;
+        const double diqkrx = diqkz * yr - diqky * zr, diqkry = diqkx * zr - diqkz * xr,
+                     diqkrz = diqky * xr - diqkx * yr;
+        const double dkqirx = dkqiz * yr - dkqiy * zr, dkqiry = dkqix * zr - dkqiz * xr,
+                     dkqirz = dkqiy * xr - dkqix * yr;
+        const double dqikx = diy * qkz - diz * qky + dky * qiz - dkz * qiy -
+                             2.0 * (qixy * qkxz + qiyy * qkyz + qiyz * qkzz - qixz * qkxy - qiyz * qkyy - qizz * qkyz);
+        const double dqiky = diz * qkx - dix * qkz + dkz * qix - dkx * qiz -
+                             2.0 * (qixz * qkxx + qiyz * qkxy + qizz * qkxz - qixx * qkxz - qixy * qkyz - qixz * qkzz);
+        const double dqikz = dix * qky - diy * qkx + dkx * qiy - dky * qix -
+                             2.0 * (qixx * qkxy + qixy * qkyy + qixz * qkyz - qixy * qkxx - qiyy * qkxy - qiyz * qkxz);
+        // reciprocal distance terms and the Ewald damping (dampewald order 11)
+        double rr1 = f / r;
+        double rr3 = rr1 / r2;
+        double rr5 = 3.0 * rr3 / r2;
+        double rr7 = 5.0 * rr5 / r2;
+        double rr9 = 7.0 * rr7 / r2;
+        double rr11 = 9.0 * rr9 / r2;
+        double dmpe[12];
+        dampewald(11, r, r2, f, s.aewald, dmpe);
+        const double term1 = ci * ck;
+        const double term2 = ck * dir - ci * dkr + dik;
+        const double term3 = ci * qkr + ck * qir - dir * dkr + 2.0 * (dkqi - diqk + qiqk);
+        const double term4 = dir * qkr - dkr * qir - 4.0 * qik;
+        const double term5 = qir * qkr;
+        const double scalek = 1.0 - mscale[k];
+        rr1 = dmpe[1] - scalek * rr1;
+        rr3 = dmpe[3] - scalek * rr3;
+        rr5 = dmpe[5] - scalek * rr5;
+        rr7 = dmpe[7] - scalek * rr7;
+        rr9 = dmpe[9] - scalek * rr9;
+        rr11 = dmpe[11] - scalek * rr11;
+        const double e = term1 * rr1 + term2 * rr3 + term3 * rr5 + term4 * rr7 + term5 * rr9;
+        const double de = term1 * rr3 + term2 * rr5 + term3 * rr7 + term4 * rr9 + term5 * rr11;
+        const double t1 = -ck * rr3 + dkr * rr5 - qkr * rr7;
+        const double t2 = ci * rr3 + dir * rr5 + qir * rr7;
+        const double t3 = 2.0 * rr5;
+        const double t4 = -2.0 * (ck * rr5 - dkr * rr7 + qkr * rr9);
+        const double t5 = -2.0 * (ci * rr5 + dir * rr7 + qir * rr9);
+        const double t6 = 4.0 * rr7;
+        ereal += e;
+        const double frcx = de * xr + t1 * dix + t2 * dkx + t3 * (diqkx - dkqix) + t4 * qix + t5 * qkx +
+                            t6 * (qixk + qkxi);
+        const double frcy = de * yr + t1 * diy + t2 * dky + t3 * (diqky - dkqiy) + t4 * qiy + t5 * qky +
+                            t6 * (qiyk + qkyi);
+        const double frcz = de * zr + t1 * diz + t2 * dkz + t3 * (diqkz - dkqiz) + t4 * qiz + t5 * qkz +
+                            t6 * (qizk + qkzi);
+        tem[i * 3 + 0] += -rr3 * dikx + t1 * dirx + t3 * (dqikx + dkqirx) - t4 * qirx - t6 * (qikrx + qikx);
+        tem[i * 3 + 1] += -rr3 * diky + t1 * diry + t3 * (dqiky + dkqiry) - t4 * qiry - t6 * (qikry + qiky);
+        tem[i * 3 + 2] += -rr3 * dikz + t1 * dirz + t3 * (dqikz + dkqirz) - t4 * qirz - t6 * (qikrz + qikz);
+        tem[k * 3 + 0] += rr3 * dikx + t2 * dkrx - t3 * (dqikx + diqkrx) - t5 * qkrx - t6 * (qkirx - qikx);
+        tem[k * 3 + 1] += rr3 * diky + t2 * dkry - t3 * (dqiky + diqkry) - t5 * qkry - t6 * (qkiry - qiky);
+        tem[k * 3 + 2] += rr3 * dikz + t2 * dkrz - t3 * (dqikz + diqkrz) - t5 * qkrz - t6 * (qkirz - qikz);
+        dem[i * 3 + 0] += frcx;
+        dem[i * 3 + 1] += frcy;
+        dem[i * 3 + 2] += frcz;
+        dem[k * 3 + 0] -= frcx;
+        dem[k * 3 + 1] -= frcy;
+        dem[k * 3 + 2] -= frcz;
+      }
+      for (int b = 0; b < 4; ++b) for_conn(s, mslot[b], i, [&](int k) { mscale[k] = 1.0; });
+    }
+    for (int i = 0; i < n; ++i)
+      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], &tem[(size_t)i * 3], dem);
+  }
+  // ---- self energy (empole1.f:134-160) -------------------------------------
+  {
+    const double term = 2.0 * s.aewald * s.aewald;
+    const double fterm = -f * s.aewald / kSqrtPi;
+    for (int i = 0; i < n; ++i) {
+      const double* rp = &s.rpole[(size_t)i * 13];
+      const double ci = rp[0], dix = rp[1], diy = rp[2], diz = rp[3];
+      const double qixx = rp[4], qixy = rp[5], qixz = rp[6], qiyy = rp[8], qiyz = rp[9], qizz = rp[12];
+      const double cii = ci * ci;
+      const double dii = dix * dix + diy * diy + diz * diz;
+      const double qii = 2.0 * (qixy * qixy + qixz * qixz + qiyz * qiyz) + qixx * qixx + qiyy * qiyy + qizz * qizz;
+      eself += fterm * (cii + term * (dii / 3.0 + 2.0 * term * qii / 5.0));
+    }
+  }
+  if (parts) {
+    parts[0] = ereal + erecip + eself;
+    parts[1] = ereal;
+    parts[2] = erecip;
+    parts[3] = eself;
+  }
+  return OR_OK;
+}
+
 }  // extern "C"

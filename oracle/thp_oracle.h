@@ -53,6 +53,7 @@ typedef struct OrSystem {
   int politer;
   double poleps;
   int nthreads;       /* OpenMP threads for the CPU baseline; 1 = scalar */
+  double m_scale[4];  /* m2scale..m5scale (initprm.f:413-416, water03.prm:34-37) */
 } OrSystem;
 
 typedef struct OrSolveInfo {
@@ -95,6 +96,11 @@ double or_epolar(OrCtx* c, const double* uind, double* ereal, double* erecip, do
  * as in or_rotpole) distribute the torques (torque.f:6). */
 int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxis, const int* xaxis,
                const int* axt, double* dep, double* ep);
+
+/* empole1c (empole1.f:42-340): permanent-multipole energy and gradient dem
+ * [n][3] (kcal/mol/A) at the current positions, TINFOIL boundary; needs the
+ * list (or_mlistcell).  parts (may be NULL) [4]: total, real, recip, self. */
+int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, double* dem, double* parts);
 
 /* grid_uind_site (pmestuff.f:280-405) for nsites sites (0-based atom
  * numbers): adds the fractional dipoles fuind/fuinp (3 per site) into the

@@ -123,3 +123,65 @@ def isolated_epol(ws, rpole, electric=332.063714):
     A = np.diag(np.repeat(1.0 / ws.polarity, 3)) - T
     mu_d = np.linalg.solve(A, E[0].ravel()).reshape(n, 3)
     return -0.5 * electric * np.sum(mu_d * E[1])
+
+
+def recip_energy(pos, box, alpha, q, d, Q, electric=332.063714, chunk=4096):
+    """Classical Ewald reciprocal energy of point multipoles,
+    (electric/2) sum_k f(k) |S(k)|^2 with f = 4 pi exp(-k^2/4a^2) / (V k^2)."""
+    k, k2 = kvectors(box, alpha)
+    V = float(np.prod(box))
+    f = (4 * np.pi / V) * np.exp(-k2 / (4 * alpha * alpha)) / k2
+    e = 0.0
+    for s in range(0, len(k), chunk):
+        kk, ff = k[s:s + chunk], f[s:s + chunk]
+        ph = np.exp(-1j * pos @ kk.T)
+        amp = q[:, None] - 1j * (d @ kk.T) - np.einsum("ka,nab,kb->nk", kk, Q, kk)
+        S = np.sum(amp * ph, axis=0)
+        e += np.sum(ff * np.abs(S) ** 2)
+    return 0.5 * electric * e
+
+
+def isolated_empole(ws, rpole, electric=332.063714):
+    """Permanent-multipole energy of the same molecules in vacuum (no images,
+    no cutoff) by direct summation over pairs of sites, with the 1-2..1-5
+    mpole scales: per pair q_i phi_k + d_i.grad phi_k + Q_i : grad grad phi_k
+    from the Cartesian derivatives of 1/R, where site k's potential is
+    phi_k(R) = q_k/R - d_k.grad(1/R) + Q_k : grad grad (1/R) (R = r - r_k)."""
+    n = ws.n
+    pos = ws.positions()
+    q = rpole[:, 0]
+    dp = rpole[:, 1:4]
+    Q = rpole[:, 4:13].reshape(n, 3, 3)
+    ms = np.ones((n, n))
+    for b, name in enumerate(("i12", "i13", "i14", "i15")):
+        off, idx = ws.conn[name]
+        for i in range(n):
+            for k in idx[off[i]:off[i + 1]]:
+                ms[i, k] = ws.scales["m_scale"][b]
+    I = np.eye(3)
+    e = 0.0
+    for i in range(n):
+        for k in range(i + 1, n):
+            if ms[i, k] == 0.0:
+                continue
+            R = pos[i] - pos[k]
+            r = np.sqrt(R @ R)
+            # derivatives of 1/r up to fourth order (rank-n tensors)
+            t0 = 1.0 / r
+            t1 = -R / r ** 3
+            t2 = 3 * np.outer(R, R) / r ** 5 - I / r ** 3
+            t3 = (-15 * np.einsum("a,b,c->abc", R, R, R) / r ** 7
+                  + 3 * (np.einsum("a,bc->abc", R, I) + np.einsum("b,ac->abc", R, I)
+                         + np.einsum("c,ab->abc", R, I)) / r ** 5)
+            RRRR = np.einsum("a,b,c,d->abcd", R, R, R, R)
+            RRI = (np.einsum("a,b,cd->abcd", R, R, I) + np.einsum("a,c,bd->abcd", R, R, I)
+                   + np.einsum("a,d,bc->abcd", R, R, I) + np.einsum("b,c,ad->abcd", R, R, I)
+                   + np.einsum("b,d,ac->abcd", R, R, I) + np.einsum("c,d,ab->abcd", R, R, I))
+            II = np.einsum("ab,cd->abcd", I, I) + np.einsum("ac,bd->abcd", I, I) + np.einsum("ad,bc->abcd", I, I)
+            t4 = 105 * RRRR / r ** 9 - 15 * RRI / r ** 7 + 3 * II / r ** 5
+            # potential of k and its derivatives at i: phi = q T0 - d.T1 + Q:T2
+            phi = q[k] * t0 - dp[k] @ t1 + np.einsum("ab,ab", Q[k], t2)
+            g1 = q[k] * t1 - np.einsum("b,ab->a", dp[k], t2) + np.einsum("bc,abc->a", Q[k], t3)
+            g2 = q[k] * t2 - np.einsum("c,abc->ab", dp[k], t3) + np.einsum("cd,abcd->ab", Q[k], t4)
+            e += ms[i, k] * (q[i] * phi + dp[i] @ g1 + np.einsum("ab,ab", Q[i], g2))
+    return electric * e

@@ -281,3 +281,100 @@ def test_two_waters_reach_the_isolated_limit(thp):
     assert abs(ratio / (40.0 / 30.0) ** 3 - 1.0) < 0.03, ratio
     einf = (es[40.0] * 40.0 ** 3 - es[30.0] * 30.0 ** 3) / (40.0 ** 3 - 30.0 ** 3)
     assert abs(einf - eiso) < 5e-5 * abs(eiso), (einf, eiso)
+
+
+# ---- permanent-multipole energy and gradient (empole1c) --------------------
+
+def _empole(ws):
+    orc = O.Oracle(ws)
+    assert orc.mlistcell(maxelst=4000)[0] == 0
+    return orc.empole1()
+
+
+def test_empole1_gradient_matches_finite_differences(box216):
+    # the positions move the frames too (rotpole), so the torque terms are
+    # checked with the pair and grid forces
+    _, dem, _ = _empole(box216)
+    pos0 = box216.positions()
+    h = 1e-5
+    for atom in (0, 1, 2, 301, 646):
+        for d in range(3):
+            e = []
+            for sgn in (1, -1):
+                p = pos0.copy()
+                p[atom, d] += sgn * h
+                e.append(_empole(box216.with_positions(p))[0])
+            fd = (e[0] - e[1]) / (2 * h)
+            assert abs(fd - dem[atom, d]) < 1e-6 * np.abs(dem).max() + 1e-6, (atom, d, fd, dem[atom, d])
+
+
+def test_empole_recip_converges_to_classical_ewald(box216):
+    orc0 = O.Oracle(box216)
+    rp = orc0.rpole
+    ref = ewald_ref.recip_energy(box216.positions(), box216.box, box216.aewald, rp[:, 0], rp[:, 1:4],
+                                 rp[:, 4:13].reshape(-1, 3, 3))
+    errs = []
+    for k in (16, 32, 64):
+        _, _, (_, erec, _) = _empole(_with_grid(box216, k))
+        errs.append(abs(erec - ref) / abs(ref))
+    assert errs[0] < 1e-2 and errs[1] < errs[0] / 8 and errs[2] < errs[1] / 8 and errs[2] < 1e-6, errs
+
+
+def test_empole_energy_independent_of_ewald_alpha(thp):
+    # The real, reciprocal and self parts each move by hundreds of kcal/mol
+    # between these alphas; with the reciprocal part summed classically
+    # (tests/ewald_ref.py) their total must not.  Measured: 1e-10 relative to
+    # that spread (the PME reciprocal part itself is pinned by the
+    # convergence test above; at 0.45 A spacing it moves by 6e-3 kcal/mol).
+    es, reals = [], []
+    for a in (0.5, 0.5446, 0.65):
+        ws = thp.water.make_water_box(216, cfg=0, edge=22.0, ewaldcut=9.0, grid_spacing=0.45, aewald=a)
+        orc = O.Oracle(ws)
+        assert orc.mlistcell(maxelst=4000)[0] == 0
+        _, _, (ereal, _, eself) = orc.empole1()
+        rp = orc.rpole
+        erec = ewald_ref.recip_energy(ws.positions(), ws.box, a, rp[:, 0], rp[:, 1:4], rp[:, 4:13].reshape(-1, 3, 3))
+        es.append(ereal + erec + eself)
+        reals.append(ereal)
+    spread = np.ptp(reals)
+    assert spread > 100.0, reals
+    assert np.ptp(es) < 1e-9 * spread, (es, reals)
+
+
+def test_empole_two_waters_reach_the_isolated_limit(thp):
+    # The Ewald energy of two waters in growing periodic boxes approaches the
+    # vacuum direct sum (tests/ewald_ref.py) through image terms in 1/L^3 and
+    # 1/L^5 (the molecules carry dipoles and quadrupoles); a fit over three
+    # boxes recovers the vacuum value (measured: 4e-8 relative).  The
+    # reciprocal part is summed classically here: for six atoms the PME
+    # self-interaction error is position dependent, about 1e-4 kcal/mol at
+    # 0.5 A spacing, next to image terms of 1e-2.
+    W = thp.water
+    R, th = W.R_OH, math.radians(W.THETA_HOH) / 2
+    h1 = np.array([R * math.sin(th), 0, R * math.cos(th)])
+    h2 = np.array([-R * math.sin(th), 0, R * math.cos(th)])
+
+    def rot(a, b):
+        ca, sa, cb, sb = math.cos(a), math.sin(a), math.cos(b), math.sin(b)
+        return np.array([[ca, -sa, 0], [sa, ca, 0], [0, 0, 1]]) @ np.array([[1, 0, 0], [0, cb, -sb], [0, sb, cb]])
+
+    o1 = np.array([0.3, -0.2, 0.1])
+    o2 = o1 + np.array([2.85, 0.4, -0.3])
+    xyz = np.array([o1, o1 + rot(0.3, 1.1) @ h1, o1 + rot(0.3, 1.1) @ h2,
+                    o2, o2 + rot(2.0, -0.7) @ h1, o2 + rot(2.0, -0.7) @ h2])
+    es = {}
+    for L in (30.0, 40.0, 60.0):
+        ws = W._assemble(2, L, xyz, 0.5, 7.0, 0.5, None)
+        orc = O.Oracle(ws)
+        assert orc.mlistcell()[0] == 0
+        _, _, (ereal, _, eself) = orc.empole1()
+        rp = orc.rpole
+        erec = ewald_ref.recip_energy(ws.positions(), ws.box, ws.aewald, rp[:, 0], rp[:, 1:4],
+                                      rp[:, 4:13].reshape(-1, 3, 3))
+        es[L] = ereal + erec + eself
+        if L == 30.0:
+            eiso = ewald_ref.isolated_empole(ws, rp)
+    Ls = np.array(sorted(es))
+    fit = np.linalg.solve(np.stack([np.ones(3), Ls ** -3, Ls ** -5], axis=1), np.array([es[L] for L in Ls]))
+    assert abs(es[30.0] - eiso) > 1e-3 * abs(eiso), (es, eiso)  # the image term is visible
+    assert abs(fit[0] - eiso) < 1e-6 * abs(eiso), (fit, eiso)

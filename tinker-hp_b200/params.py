@@ -45,6 +45,7 @@ SCALES = {
     "pi_scale": (0.0, 0.0, 0.5, 1.0),  # polar-12..15-intra (p2i, p3i default 0; 14-intra 0.5)
     "d_scale": (0.0, 1.0, 1.0, 1.0),   # direct-11..14-scale
     "u_scale": (1.0, 1.0, 1.0, 1.0),   # mutual-11..14-scale
+    "m_scale": (0.0, 0.0, 0.4, 0.8),   # mpole-12..15-scale (water03.prm:34-37)
 }
 
 # frame codes shared with the C-ABI: 1 = Z-then-X, 2 = Bisector
