@@ -331,6 +331,34 @@ def md_run(lib, thp, nsteps=20, predictor=None):
             "atoms": ws.n, "dt_fs": 1.0}
 
 
+def empole_run(lib, ws, reps=10):
+    """Permanent-multipole energy and gradient (empole1c) of the box, FP64 and
+    mixed: wall time per call through the C-ABI with the list already built
+    (each call: rotpole, multipole spread + FFTs + 20-term gather, the pair
+    terms, energy, and the gradient into a pinned host array)."""
+    import torch
+    out = {}
+    res = {}
+    for name, prec in (("fp64", lib.FP64), ("mixed", lib.MIXED)):
+        ctx = lib.Context(ws, precision=prec)
+        buf = torch.empty((ws.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+        ctx.empole1(out=buf)
+        ctx.empole1(out=buf)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            em, dem = ctx.empole1(out=buf)
+        dt = (time.perf_counter() - t0) / reps
+        res[name] = (em, dem.copy())
+        out[name] = {"ms_per_call": dt * 1e3, "em_kcal_mol": em}
+        ctx.close()
+    (e64, d64), (em, dm) = res["fp64"], res["mixed"]
+    out["mixed_energy_err_kcal_mol"] = em - e64
+    out["mixed_force_rms_rel_err"] = float(np.sqrt(np.mean(np.sum((dm - d64) ** 2, axis=1)))
+                                           / np.sqrt(np.mean(np.sum(d64 ** 2, axis=1))))
+    out["atoms"] = ws.n
+    return out
+
+
 def timed_solves(ctx, lib, steps, warmup, rebuild=True, guess=None):
     """Device-resident solves; per-step device time from CUDA events."""
     import torch
@@ -528,6 +556,7 @@ def main():
                                          "mixed_2_systems": served_repeats(lib, [ws, ws2], lib.MIXED, count=24),
                                          "fp64_2_systems": served_repeats(lib, [ws, ws2], lib.FP64, count=24)}
         extras["md_config1"] = {"previous": md_run(lib, thp), "aspc": md_run(lib, thp, predictor="ASPC")}
+        extras["empole1"] = empole_run(lib, ws)
         if fp64 is not None:
             best = max(b2["solves_per_s"], b4["solves_per_s"])
             plain64 = world * len(lat64) / (t64 / 1000.0)

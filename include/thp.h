@@ -169,6 +169,21 @@ int thp_get_gradient(thp_ctx* ctx, double* dep, double* ep);
 /* same gradient into device memory d_dep [n][3], enqueued on the context's
  * stream without a host synchronisation */
 int thp_get_gradient_device(thp_ctx* ctx, double* d_dep);
+/* m2scale..m5scale [4] of the permanent-multipole pair terms (mplpot module;
+ * defaults initprm.f:413-416: 0, 0, 1, 1; AMOEBA water03.prm:34-37: 0, 0,
+ * 0.4, 0.8).  The 1-2..1-5 lists come from thp_set_connectivity. */
+int thp_set_mpole_scales(thp_ctx* ctx, const double* m);
+/* Permanent-multipole energy and gradient, empole1c (empole1.f:42-340):
+ * emrecip1 (:349), emreal1c (:873, standard branch, mscale), the Ewald self
+ * energy (:134-160) and torque (torque.f:6), TINFOIL boundary, at the current
+ * positions and multipoles (rotpole on the device when frames are set).
+ * em (kcal/mol) and dem [n][3] (kcal/mol/A, original order; either may be
+ * NULL).  Needs frames (thp_set_frames) and connectivity; THP_E_STATE
+ * otherwise.  The list is built or reused as for a solve.  The mixed form
+ * evaluates the unscaled pairs and the grid in FP32 and the 1-2..1-5 pairs,
+ * the reciprocal-space sums and the self term in FP64; gradients accumulate
+ * in 64-bit fixed point as thp_get_gradient's. */
+int thp_empole1(thp_ctx* ctx, double* em, double* dem);
 /* Velocity-Verlet NVE dynamics driven by the polarization gradient alone
  * (verlet.f:17-200 with gradient = epolar1): per step a half kick, a drift of
  * the positions on the device, a solve warm-started from the predictor when
@@ -299,6 +314,8 @@ int thp_bind_state(thp_ctx* ctx, double* x, double* y, double* z, double* rpole,
 int thp_last_error(void);
 /* bind deriv::dep(3,n), written by epolar1_ */
 int thp_bind_gradient(thp_ctx* ctx, double* dep);
+/* bind energi::em and deriv::dem(3,n), written by empole1_ (may be NULL) */
+int thp_bind_mpole(thp_ctx* ctx, double* em, double* dem);
 /* bind pme::qgrid2in_2d(2,n1,n2,n3), read by fphi_uind_site_ */
 int thp_bind_grid(thp_ctx* ctx, double* qgrid);
 
@@ -344,6 +361,9 @@ void fphi_uind_site_(const int* isite, const int* impi, double* fdip_phi1, doubl
 void mlistcell_(void);
 /* nblist.f:1148 -- same list for the vdW slot name used by the workload */
 void vlistcell_(void);
+/* empole1.f:10 -- permanent-multipole energy into the bound em and its
+ * gradient into the bound dem (overwritten, as empole1c zeroes it) */
+void empole1_(void);
 /* epolar.f:17 -- polarization energy into the bound ep (solves first) */
 void epolar_(void);
 /* epolar1.f:17 -- solve, then energy into the bound ep and the gradient into

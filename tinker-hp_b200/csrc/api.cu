@@ -51,13 +51,17 @@ int dmalloc(Ctx& c, T** p, size_t count, const char* what) {
 // Special pairs with their (d, p, u) scales, in the assignment order of
 // efld0_direct (newinduce_pme.f:1062-1136, dpequal false) and tmatxb_pme
 // (:1495-1518): pscale from i12..i15 (p*iscale when the partner is in ip11),
-// dscale and uscale from ip11..ip14.  Pairs whose three scales are all 1 are
-// dropped.
+// dscale and uscale from ip11..ip14.  Each entry also carries the 1-2..1-5
+// class that selects m2scale..m5scale in emreal1c (empole1.f:1040-1051; a
+// later list overrides an earlier one, as there).  Pairs whose three scales
+// are all 1 and that are in no 1-2..1-5 list are dropped.
 static void special_pairs(int n, const int* const* off, const int* const* idx, const double* sc,
-                          std::vector<int>& sp_off, std::vector<int>& sp_k, std::vector<double>& sp_s) {
+                          std::vector<int>& sp_off, std::vector<int>& sp_k, std::vector<double>& sp_s,
+                          std::vector<int>& sp_c) {
   sp_off.assign(n + 1, 0);
   sp_k.clear();
   sp_s.clear();
+  sp_c.clear();
   auto row = [&](int slot, int i, std::vector<int>& out) {
     out.clear();
     if (!off || !off[slot] || !idx[slot]) return;
@@ -65,21 +69,23 @@ static void special_pairs(int n, const int* const* off, const int* const* idx, c
   };
   std::vector<int> lst, ip11;
   // this atom's partners with their (d, p, u) scales, 1 until a rule sets
-  // one; a short list searched linearly and reused across atoms (no per-atom
-  // allocation: servers build this for every new system)
+  // one, and their bond class; a short list searched linearly and reused
+  // across atoms (no per-atom allocation: servers build this for every new
+  // system)
   struct Ent {
     int k;
     std::array<double, 3> s;
+    int mc;
   };
   std::vector<Ent> m;
   m.reserve(64);
   for (int i = 0; i < n; ++i) {
     m.clear();
-    auto get = [&](int k) -> std::array<double, 3>& {
+    auto get = [&](int k) -> Ent& {
       for (Ent& e : m)
-        if (e.k == k) return e.s;
-      m.push_back(Ent{k, {1.0, 1.0, 1.0}});
-      return m.back().s;
+        if (e.k == k) return e;
+      m.push_back(Ent{k, {1.0, 1.0, 1.0}, 4});
+      return m.back();
     };
     row(THP_IP11, i, ip11);
     for (int b = 0; b < 4; ++b) {
@@ -87,33 +93,36 @@ static void special_pairs(int n, const int* const* off, const int* const* idx, c
       for (int k : lst) {
         double p = sc[b];
         if (std::find(ip11.begin(), ip11.end(), k) != ip11.end()) p = sc[4 + b];
-        get(k)[1] = p;
+        Ent& e = get(k);
+        e.s[1] = p;
+        e.mc = b;
       }
     }
     for (int b = 0; b < 4; ++b) {
       row(THP_IP11 + b, i, lst);
-      for (int k : lst) get(k)[0] = sc[8 + b];
+      for (int k : lst) get(k).s[0] = sc[8 + b];
     }
     for (int b = 0; b < 4; ++b) {
       row(THP_IP11 + b, i, lst);
-      for (int k : lst) get(k)[2] = sc[12 + b];
+      for (int k : lst) get(k).s[2] = sc[12 + b];
     }
     std::sort(m.begin(), m.end(), [](const Ent& a, const Ent& b) { return a.k < b.k; });  // ascending partners
     for (const Ent& e : m) {
       if (e.k == i) continue;
       const auto& s = e.s;
-      if (s[0] == 1.0 && s[1] == 1.0 && s[2] == 1.0) continue;
+      if (s[0] == 1.0 && s[1] == 1.0 && s[2] == 1.0 && e.mc == 4) continue;
       sp_k.push_back(e.k);
       sp_s.push_back(s[0]);
       sp_s.push_back(s[1]);
       sp_s.push_back(s[2]);
+      sp_c.push_back(e.mc);
     }
     sp_off[i + 1] = (int)sp_k.size();
   }
 }
 
 void build_special_pairs(Ctx& c, const int* const* off, const int* const* idx, const double* sc) {
-  special_pairs(c.n, off, idx, sc, c.sp_off, c.sp_k, c.sp_s);
+  special_pairs(c.n, off, idx, sc, c.sp_off, c.sp_k, c.sp_s, c.sp_c);
 }
 
 // Device buffers for the special pairs of the context's system (kept while
@@ -134,12 +143,14 @@ static int reserve_special_pairs(Ctx& c) {
     cudaFree(c.d_sp_k);
     cudaFree(c.d_sp_ks);
     cudaFree(c.d_sp_s);
-    c.d_sp_k = c.d_sp_ks = nullptr;
+    cudaFree(c.d_sp_c);
+    c.d_sp_k = c.d_sp_ks = c.d_sp_c = nullptr;
     c.d_sp_s = nullptr;
     c.cap_sp = 0;
     if ((st = dmalloc(c, &c.d_sp_k, m, "alloc sp_k"))) return st;
     if ((st = dmalloc(c, &c.d_sp_ks, m, "alloc sp_ks"))) return st;
     if ((st = dmalloc(c, &c.d_sp_s, 3 * m, "alloc sp_s"))) return st;
+    if ((st = dmalloc(c, &c.d_sp_c, m, "alloc sp_c"))) return st;
     c.cap_sp = m;
   }
   return THP_OK;
@@ -153,6 +164,7 @@ int upload_special_pairs(Ctx& c) {
   if (!c.sp_k.empty()) {
     cudaMemcpyAsync(c.d_sp_k, c.sp_k.data(), sizeof(int) * c.sp_k.size(), cudaMemcpyHostToDevice, c.stream);
     cudaMemcpyAsync(c.d_sp_s, c.sp_s.data(), sizeof(double) * c.sp_s.size(), cudaMemcpyHostToDevice, c.stream);
+    cudaMemcpyAsync(c.d_sp_c, c.sp_c.data(), sizeof(int) * c.sp_c.size(), cudaMemcpyHostToDevice, c.stream);
   }
   return cuda_status(cudaStreamSynchronize(c.stream), &c, "upload special pairs");
 }
@@ -367,9 +379,9 @@ static void pinned_give(Ctx& c) {
 }
 
 void free_ctx(Ctx& c) {
-  void* ptrs[] = {c.slab_cells, c.slab_atoms, c.slab_pairs, c.d_sp_off, c.d_sp_k, c.d_sp_ks, c.d_sp_s, c.d_cg,
-                  c.d_flags, c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad, c.d_sgrid, c.d_sscratch,
-                  c.d_alt};
+  void* ptrs[] = {c.slab_cells, c.slab_atoms, c.slab_pairs, c.d_sp_off, c.d_sp_k, c.d_sp_ks, c.d_sp_s, c.d_sp_c,
+                  c.d_cg, c.d_flags, c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad, c.d_sgrid, c.d_sscratch,
+                  c.d_alt, c.d_empart};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   pme_free(c);
@@ -540,7 +552,8 @@ static int size_buffers(Ctx& c) {
     cudaFree(c.slab_atoms);
     c.slab_atoms = nullptr;
     // buffers made on first use are sized by n as well
-    free_all(&c.d_fphirec, &c.d_depfix, &c.d_trq, &c.d_frs, &c.d_grad);
+    free_all(&c.d_fphirec, &c.d_depfix, &c.d_trq, &c.d_frs, &c.d_grad, &c.d_empart);
+    c.d_em = nullptr;
     c.cap_n = 0;
     st = alloc_slab(c, &c.slab_atoms,
                     {item(&c.d_atom_cell, n), item(&c.d_scell, n), item(&c.d_perm, n), item(&c.d_iperm, n),
@@ -585,6 +598,9 @@ static int clear_system_state(thp_ctx* h) {
   h->pos_dirty = h->rpole_dirty = true;
   h->field_valid = h->guess_uploaded = h->solved_once = false;
   c.bx = c.by = c.bz = c.brpole = c.buind = c.buinp = c.bep = c.bdep = c.bqgrid = nullptr;
+  c.bem = c.bdem = nullptr;
+  c.mscale[0] = c.mscale[1] = 0.0;  // initprm.f:413-416
+  c.mscale[2] = c.mscale[3] = 1.0;
   c.bnelst = c.belst = nullptr;
   c.bmaxelst = 0;
   cudaMemsetAsync(c.d_flags, 0, sizeof(int), c.stream);
@@ -593,6 +609,7 @@ static int clear_system_state(thp_ctx* h) {
   c.sp_off.assign(c.n + 1, 0);
   c.sp_k.clear();
   c.sp_s.clear();
+  c.sp_c.clear();
   return upload_special_pairs(c);  // synchronises the stream
 }
 
@@ -737,6 +754,7 @@ struct SystemImage {
   int* frames = nullptr;   // [3n] z-axis, x-axis, frame type
   int* sp_off = nullptr;   // [n+1]
   int* sp_k = nullptr;     // [m]
+  int* sp_c = nullptr;     // [m]
   double* sp_s = nullptr;  // [3m]
   void* block = nullptr;
 };
@@ -760,15 +778,15 @@ int image_create(const thp_config& cfg, const double* polarity, const double* th
   for (int i = 0; i < n; ++i)
     if (zaxis[i] < 0 || zaxis[i] >= n || xaxis[i] < 0 || xaxis[i] >= n || (axt[i] != 1 && axt[i] != 2))
       return THP_E_INVALID;
-  std::vector<int> so, sk;
+  std::vector<int> so, sk, sc;
   std::vector<double> ss;
-  special_pairs(n, off, idx, scales, so, sk, ss);
+  special_pairs(n, off, idx, scales, so, sk, ss, sc);
   auto* img = new SystemImage();
   img->n = n;
   img->m = (int)sk.size();
   std::memcpy(img->scales, scales, sizeof(img->scales));
   const size_t nd = 3 * (size_t)n + 13 * (size_t)n + 3 * (size_t)img->m;
-  const size_t ni = 3 * (size_t)n + (size_t)n + 1 + (size_t)img->m;
+  const size_t ni = 3 * (size_t)n + (size_t)n + 1 + 2 * (size_t)img->m;
   const size_t bytes = nd * sizeof(double) + ni * sizeof(int);
   if (cudaHostAlloc(&img->block, bytes, cudaHostAllocDefault) == cudaSuccess) {
     img->pinned = true;
@@ -788,6 +806,7 @@ int image_create(const thp_config& cfg, const double* polarity, const double* th
   img->frames = q;
   img->sp_off = q + 3 * (size_t)n;
   img->sp_k = img->sp_off + n + 1;
+  img->sp_c = img->sp_k + img->m;
   std::memcpy(img->par, pdamp, sizeof(double) * n);
   std::memcpy(img->par + n, thole, sizeof(double) * n);
   std::memcpy(img->par + 2 * (size_t)n, polarity, sizeof(double) * n);
@@ -801,6 +820,7 @@ int image_create(const thp_config& cfg, const double* polarity, const double* th
   if (img->m) {
     std::memcpy(img->sp_k, sk.data(), sizeof(int) * img->m);
     std::memcpy(img->sp_s, ss.data(), sizeof(double) * 3 * (size_t)img->m);
+    std::memcpy(img->sp_c, sc.data(), sizeof(int) * img->m);
   }
   *out = img;
   return THP_OK;
@@ -825,6 +845,7 @@ int image_load(thp_ctx* h, const SystemImage* img) {
   c.sp_off.assign(img->sp_off, img->sp_off + n + 1);
   c.sp_k.assign(img->sp_k, img->sp_k + img->m);
   c.sp_s.assign(img->sp_s, img->sp_s + 3 * (size_t)img->m);
+  c.sp_c.assign(img->sp_c, img->sp_c + img->m);
   c.have_conn = true;
   int st = reserve_special_pairs(c);
   if (st) return st;
@@ -832,6 +853,7 @@ int image_load(thp_ctx* h, const SystemImage* img) {
   if (img->m) {
     cudaMemcpyAsync(c.d_sp_k, img->sp_k, sizeof(int) * img->m, cudaMemcpyHostToDevice, c.stream);
     cudaMemcpyAsync(c.d_sp_s, img->sp_s, sizeof(double) * 3 * img->m, cudaMemcpyHostToDevice, c.stream);
+    cudaMemcpyAsync(c.d_sp_c, img->sp_c, sizeof(int) * img->m, cudaMemcpyHostToDevice, c.stream);
   }
   cudaMemcpyAsync(c.d_pole_local, img->pole, sizeof(double) * 13 * n, cudaMemcpyHostToDevice, c.stream);
   cudaMemcpyAsync(c.d_frames, img->frames, sizeof(int) * 3 * n, cudaMemcpyHostToDevice, c.stream);
@@ -955,6 +977,34 @@ int thp_profile(thp_ctx* h, int enable, double* ms_total, int* launches) {
   for (cudaEvent_t e : c.prof_events) cudaEventDestroy(e);
   c.prof_events.clear();
   c.profiling = enable != 0;
+  return THP_OK;
+}
+
+int thp_set_mpole_scales(thp_ctx* h, const double* m) {
+  if (!h || !m) return THP_E_INVALID;
+  for (int j = 0; j < 4; ++j)
+    if (!std::isfinite(m[j])) return THP_E_INVALID;
+  for (int j = 0; j < 4; ++j) h->c.mscale[j] = m[j];
+  return THP_OK;
+}
+
+int thp_empole1(thp_ctx* h, double* em, double* dem) {
+  if (!h || (!em && !dem)) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (!c.have_axes || !c.have_conn) return THP_E_STATE;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st;
+  if ((st = ensure_rpole(h))) return st;
+  if ((st = ensure_list(h, false))) return st;
+  if (!c.d_grad && (st = cuda_status(cudaMalloc((void**)&c.d_grad, sizeof(double) * 3 * c.n), &c, "alloc gradient")))
+    return st;
+  if ((st = launch_empole(c, c.d_grad))) return st;
+  double e = 0.0;
+  cudaMemcpyAsync(&e, c.d_em, sizeof(double), cudaMemcpyDeviceToHost, c.stream);
+  if (dem) cudaMemcpyAsync(dem, c.d_grad, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost, c.stream);
+  if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "empole"))) return st;
+  if (!std::isfinite(e)) return THP_E_NAN;
+  if (em) *em = e;
   return THP_OK;
 }
 
@@ -1481,6 +1531,13 @@ int thp_bind_gradient(thp_ctx* h, double* dep) {
   return THP_OK;
 }
 
+int thp_bind_mpole(thp_ctx* h, double* em, double* dem) {
+  if (!h) return THP_E_INVALID;
+  h->c.bem = em;
+  h->c.bdem = dem;
+  return THP_OK;
+}
+
 static int sync_bound_inputs(thp_ctx* h) {
   Ctx& c = h->c;
   if (!c.bx || !c.by || !c.bz) return THP_E_STATE;
@@ -1559,6 +1616,19 @@ void epolar1_(void) {
     if (!st2 && h->c.buind) st2 = thp_get_dipoles(h, h->c.buind, h->c.buinp);
     if (st2) st = st2;
   }
+  g_last_error = st;
+}
+
+void empole1_(void) {
+  thp_ctx* h = g_current;
+  if (!h) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  int st = sync_bound_inputs(h);
+  double em = 0.0;
+  if (!st) st = thp_empole1(h, &em, h->c.bdem);
+  if (!st && h->c.bem) *h->c.bem = em;
   g_last_error = st;
 }
 

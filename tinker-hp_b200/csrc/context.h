@@ -69,7 +69,9 @@ struct Ctx {
   std::vector<int> sp_off;     // special (scaled) pairs, original indices, CSR
   std::vector<int> sp_k;
   std::vector<double> sp_s;    // (d, p, u) per entry
+  std::vector<int> sp_c;       // 1-2..1-5 class of the entry (0..3; 4: none) for the mpole scales
   double scales[16] = {0};
+  double mscale[4] = {0.0, 0.0, 1.0, 1.0};  // m2scale..m5scale (initprm.f:413-416)
 
   // cell grid of the list build
   int nc[3] = {1, 1, 1};
@@ -105,6 +107,9 @@ struct Ctx {
   int* d_sp_off = nullptr;        // special pairs, ORIGINAL indices, CSR [n+1]
   int* d_sp_k = nullptr;
   double* d_sp_s = nullptr;       // (d, p, u) scale per entry
+  int* d_sp_c = nullptr;          // 1-2..1-5 class per entry (4: none)
+  double* d_empart = nullptr;     // per-block partial sums of the permanent-multipole energy, then
+  double* d_em = nullptr;         // their total (d_empart + blocks), made on first use
   double4* d_pos_built = nullptr; // positions at the last list build
 
   // full neighbor list within ewaldcut+lbuffer (slot-major: nb[s*npad+i])
@@ -189,6 +194,7 @@ struct Ctx {
   int *bnelst = nullptr, *belst = nullptr;
   int bmaxelst = 0;
   double* bdep = nullptr;
+  double *bem = nullptr, *bdem = nullptr;  // energi::em, deriv::dem(3,n), written by empole1_
   double* bqgrid = nullptr;  // pme::qgrid2in_2d(2,n1,n2,n3), read by fphi_uind_site_
 
   // CUDA graph of one CG chunk (captured on first use)

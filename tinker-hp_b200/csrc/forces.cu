@@ -17,6 +17,7 @@
 // add their contributions does not change the sums.
 #include <type_traits>
 
+#include "grad_dev.cuh"
 #include "kernels.h"
 #include "pme_dev.cuh"
 
@@ -25,58 +26,6 @@ namespace thp {
 namespace {
 
 constexpr int kBlock = 128;
-constexpr double kFix = 17179869184.0;  // 2^34
-
-__device__ __forceinline__ void fix_add(unsigned long long* a, double v) {
-  atomicAdd(a, (unsigned long long)(long long)llrint(v * kFix));
-}
-
-// torque.f:6-390, Z-then-X (axt 1) and Bisector (axt 2); site ib, z atom ia,
-// x atom ic; adds d(energy)/d(coordinates) of the torque trq.
-__device__ void torque_dist(const double4* __restrict__ pos, int ib, int ia, int ic, int axt, const double trq[3],
-                            unsigned long long* __restrict__ dep) {
-  const double4 pb = pos[ib], pa = pos[ia], pc = pos[ic];
-  double u[3] = {pa.x - pb.x, pa.y - pb.y, pa.z - pb.z};
-  double v[3] = {pc.x - pb.x, pc.y - pb.y, pc.z - pb.z};
-  const double usiz = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-  const double vsiz = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-  double w[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
-  const double wsiz = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    u[j] /= usiz;
-    v[j] /= vsiz;
-    w[j] /= wsiz;
-  }
-  double uv[3] = {v[1] * u[2] - v[2] * u[1], v[2] * u[0] - v[0] * u[2], v[0] * u[1] - v[1] * u[0]};
-  double uw[3] = {w[1] * u[2] - w[2] * u[1], w[2] * u[0] - w[0] * u[2], w[0] * u[1] - w[1] * u[0]};
-  double vw[3] = {w[1] * v[2] - w[2] * v[1], w[2] * v[0] - w[0] * v[2], w[0] * v[1] - w[1] * v[0]};
-  const double uvsiz = sqrt(uv[0] * uv[0] + uv[1] * uv[1] + uv[2] * uv[2]);
-  const double uwsiz = sqrt(uw[0] * uw[0] + uw[1] * uw[1] + uw[2] * uw[2]);
-  const double vwsiz = sqrt(vw[0] * vw[0] + vw[1] * vw[1] + vw[2] * vw[2]);
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    uv[j] /= uvsiz;
-    uw[j] /= uwsiz;
-    vw[j] /= vwsiz;
-  }
-  const double uvcos = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
-  const double uvsin = sqrt(1.0 - uvcos * uvcos);
-  const double dphidu = -trq[0] * u[0] - trq[1] * u[1] - trq[2] * u[2];
-  const double dphidv = -trq[0] * v[0] - trq[1] * v[1] - trq[2] * v[2];
-  const double dphidw = -trq[0] * w[0] - trq[1] * w[1] - trq[2] * w[2];
-  const double hw = axt == 2 ? 0.5 : 1.0;
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    double du = uv[j] * dphidv / (usiz * uvsin) + hw * uw[j] * dphidw / usiz;
-    double dv = -uv[j] * dphidu / (vsiz * uvsin);
-    if (axt == 2) dv += 0.5 * vw[j] * dphidw / vsiz;
-    fix_add(dep + 3 * ia + j, du);
-    fix_add(dep + 3 * ic + j, dv);
-    fix_add(dep + 3 * ib + j, -du - dv);
-  }
-}
-
 // fphi_uind_site (pmestuff.f:746-1045) in full and the force / torque of
 // eprecip1 (epolar1.f:636-720).  fphirec: [n][20] permanent potential
 // (unscaled), written by the field pass.
@@ -493,32 +442,42 @@ __global__ void __launch_bounds__(kBlock) k_force_real(
   if (axt == 1 || axt == 2) torque_dist(pos, i, iz, ix, axt, tep, dep);
 }
 
-// sorted frame atoms: frs[s] = (iperm[zaxis], iperm[xaxis], axt) of perm[s]
-__global__ void k_frames_sorted(int n, const int* __restrict__ perm, const int* __restrict__ iperm,
-                                const int* __restrict__ frames, int* __restrict__ frs) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const int o = perm[s];
-  frs[3 * s] = iperm[frames[3 * o]];
-  frs[3 * s + 1] = iperm[frames[3 * o + 1]];
-  frs[3 * s + 2] = frames[3 * o + 2];
-}
-
-__global__ void k_dep_out(int n, const int* __restrict__ perm, const unsigned long long* __restrict__ dep,
-                          double* __restrict__ out) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const int o = perm[s];
-#pragma unroll
-  for (int j = 0; j < 3; ++j) out[3 * (size_t)o + j] = (double)(long long)dep[3 * (size_t)s + j] / kFix;
-}
-
 }  // namespace
 
 template <typename P>
 static int alloc_once(Ctx& c, P** p, size_t count, const char* what) {
   if (*p) return THP_OK;
   return cuda_status(cudaMalloc((void**)p, sizeof(P) * count), &c, what);
+}
+
+// fphirec [n][20] (unscaled) of the convolved permanent-multipole grid
+int launch_fphi_mpole20(Ctx& c) {
+  int st = alloc_once(c, &c.d_fphirec, 20 * (size_t)c.n, "alloc fphirec");
+  if (st) return st;
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  PmeGeom g = pme_geom(c);
+  if (c.mixed)
+    k_fphi_mpole20<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftComplex*)c.d_grid, c.d_fphirec);
+  else
+    k_fphi_mpole20<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftDoubleComplex*)c.d_grid,
+                                                        c.d_fphirec);
+  return cuda_status(cudaGetLastError(), &c, "fphi mpole");
+}
+
+// sorted frame atoms of every site into d_frs
+int launch_frames_sorted(Ctx& c) {
+  int st = alloc_once(c, &c.d_frs, 3 * (size_t)c.n, "alloc frames");
+  if (st) return st;
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  k_frames_sorted<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, c.d_iperm, c.d_frames, c.d_frs);
+  return cuda_status(cudaGetLastError(), &c, "frames");
+}
+
+// fixed-point gradient (sorted) -> dE/dx [n][3] in original order
+int launch_gradient_out(Ctx& c, const unsigned long long* dep, double* d_out) {
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  k_dep_out<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, dep, d_out);
+  return cuda_status(cudaGetLastError(), &c, "gradient out");
 }
 
 // Gradient of the polarization energy for the converged dipoles in d_mu
@@ -539,12 +498,7 @@ int launch_forces(Ctx& c, double* d_out) {
   PmeGeom g = pme_geom(c);
   // permanent-multipole potential, 20 derivatives per site
   if ((st = launch_mpole_grid(c))) return st;
-  if (c.mixed)
-    k_fphi_mpole20<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftComplex*)c.d_grid, c.d_fphirec);
-  else
-    k_fphi_mpole20<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftDoubleComplex*)c.d_grid,
-                                                        c.d_fphirec);
-  if ((st = cuda_status(cudaGetLastError(), &c, "fphi mpole"))) return st;
+  if ((st = launch_fphi_mpole20(c))) return st;
   // dipole grid of uind (Re) / uinp (Im), convolved
   if ((st = launch_pme_dipole(c, c.d_mu, nullptr, 0))) return st;
   if (c.mixed)

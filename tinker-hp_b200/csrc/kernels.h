@@ -37,6 +37,12 @@ int launch_gather_dip(Ctx& c, double* d_out, bool check_stop);
 
 // forces.cu
 int launch_forces(Ctx& c, double* d_out);  // dE/dx [n][3], original order, for the dipoles in d_mu
+int launch_fphi_mpole20(Ctx& c);          // fphirec [n][20] of the convolved multipole grid
+int launch_frames_sorted(Ctx& c);         // frame atoms in sorted numbering (d_frs)
+int launch_gradient_out(Ctx& c, const unsigned long long* dep, double* d_out);  // fixed point -> original order
+// permanent-multipole energy into d_em and dE/dx [n][3] (original order) into
+// d_out, for the current sorted positions, multipoles and list
+int launch_empole(Ctx& c, double* d_out);
 
 // sites.cu
 int launch_grid_uind_sites(Ctx& c, int nsites, const int* d_site, const double* d_fuind, const double* d_fuinp,

@@ -1,0 +1,375 @@
+// mpole.cu -- permanent-multipole energy and gradient on the device (empole1c).
+//
+// Restates empole1c (empole1.f:42-340) for the TINFOIL boundary, without
+// charge penetration, charge flux or lambda dynamics (the AMOEBA terms):
+//   * emrecip1 (empole1.f:349-861): the convolved permanent-multipole grid --
+//     the one the polarization solve builds for its direct field -- gathered
+//     to the 20 fractional potential derivatives of every site; energy
+//     1/2 sum fmp.fphi, gradient from the derivative indices deriv1..3 and the
+//     torque from cphi (fphi_to_cphi);
+//   * emreal1c (empole1.f:873-1555, standard branch): Ewald-damped
+//     multipole-multipole pair terms to order 11 with the 1-2..1-5 mscale
+//     factors;
+//   * the Ewald self energy (empole1.f:134-160);
+//   * torque (torque.f:6-390) of each site's summed torque.
+// One thread owns site i over the full neighbor list: each pair is evaluated
+// from both ends, and each end keeps its own force, torque and half of the
+// pair energy (the reference's Newton's-third-law half-list loop gives the
+// same sums).  Gradients are accumulated in 64-bit fixed point, the energy
+// by per-block partials summed in block order, so both are deterministic.
+#include <type_traits>
+
+#include "grad_dev.cuh"
+#include "kernels.h"
+#include "pme_dev.cuh"
+
+namespace thp {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+struct EwM {
+  double a;
+  double f[5];  // (2 a^2)^j / (sqrt(pi) a), j = 1..5 (dampewald order 11)
+};
+
+struct MScale {
+  double v[5];  // m2scale..m5scale, then 1 for pairs outside the 1-2..1-5 lists
+};
+
+// per-block energy partial (warp shuffles, then the warps in order)
+__device__ __forceinline__ void block_partial(double eacc, double* __restrict__ epart) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) eacc += __shfl_down_sync(0xffffffffu, eacc, o);
+  __shared__ double ws[kBlock / 32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = eacc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < kBlock / 32; ++w) t += ws[w];
+    epart[blockIdx.x] = t;
+  }
+}
+
+// emreal1c pair terms (standard branch) seen from site i: adds half the pair
+// energy, the force on i and the torque on i.  m = (q, d, Qxx, Qxy, Qxz,
+// Qyy, Qyz, Qzz) of each site; scalek = 1 - mscale.
+template <typename U>
+__device__ __forceinline__ void mpole_pair(U xr, U yr, U zr, U r2, U scalek, const U* mi, const U* mk, const EwM& ew,
+                                           double& e_acc, double g[3], double t[3]) {
+  const U ci = mi[0], dix = mi[1], diy = mi[2], diz = mi[3];
+  const U qixx = mi[4], qixy = mi[5], qixz = mi[6], qiyy = mi[7], qiyz = mi[8], qizz = mi[9];
+  const U ck = mk[0], dkx = mk[1], dky = mk[2], dkz = mk[3];
+  const U qkxx = mk[4], qkxy = mk[5], qkxz = mk[6], qkyy = mk[7], qkyz = mk[8], qkzz = mk[9];
+  const U f = (U)kElectric;
+  const U r = sqrt(r2);
+  // intermediates involving moments and separation distance
+  const U dir = dix * xr + diy * yr + diz * zr;
+  const U qix = qixx * xr + qixy * yr + qixz * zr, qiy = qixy * xr + qiyy * yr + qiyz * zr,
+          qiz = qixz * xr + qiyz * yr + qizz * zr;
+  const U qir = qix * xr + qiy * yr + qiz * zr;
+  const U dkr = dkx * xr + dky * yr + dkz * zr;
+  const U qkx = qkxx * xr + qkxy * yr + qkxz * zr, qky = qkxy * xr + qkyy * yr + qkyz * zr,
+          qkz = qkxz * xr + qkyz * yr + qkzz * zr;
+  const U qkr = qkx * xr + qky * yr + qkz * zr;
+  const U dik = dix * dkx + diy * dky + diz * dkz;
+  const U qik = qix * qkx + qiy * qky + qiz * qkz;
+  const U diqk = dix * qkx + diy * qky + diz * qkz;
+  const U dkqi = dkx * qix + dky * qiy + dkz * qiz;
+  const U qiqk = U(2) * (qixy * qkxy + qixz * qkxz + qiyz * qkyz) + qixx * qkxx + qiyy * qkyy + qizz * qkzz;
+  // reciprocal distance terms with the Ewald damping to order 11
+  // (damping.f:17-55); the bare terms only for scaled pairs
+  const U ra = (U)ew.a * r;
+  const U ex = exp(-ra * ra);
+  const U b0 = erfc(ra) / r;
+  const U b1 = (b0 + (U)ew.f[0] * ex) / r2;
+  const U b2 = (U(3) * b1 + (U)ew.f[1] * ex) / r2;
+  const U b3 = (U(5) * b2 + (U)ew.f[2] * ex) / r2;
+  const U b4 = (U(7) * b3 + (U)ew.f[3] * ex) / r2;
+  const U b5 = (U(9) * b4 + (U)ew.f[4] * ex) / r2;
+  U rr1 = f * b0, rr3 = f * b1, rr5 = f * b2, rr7 = f * b3, rr9 = f * b4, rr11 = f * b5;
+  if (scalek != U(0)) {
+    const U s1 = f / r;
+    const U s3 = s1 / r2;
+    const U s5 = U(3) * s3 / r2;
+    const U s7 = U(5) * s5 / r2;
+    const U s9 = U(7) * s7 / r2;
+    const U s11 = U(9) * s9 / r2;
+    rr1 -= scalek * s1;
+    rr3 -= scalek * s3;
+    rr5 -= scalek * s5;
+    rr7 -= scalek * s7;
+    rr9 -= scalek * s9;
+    rr11 -= scalek * s11;
+  }
+  const U term1 = ci * ck;
+  const U term2 = ck * dir - ci * dkr + dik;
+  const U term3 = ci * qkr + ck * qir - dir * dkr + U(2) * (dkqi - diqk + qiqk);
+  const U term4 = dir * qkr - dkr * qir - U(4) * qik;
+  const U term5 = qir * qkr;
+  const U e = term1 * rr1 + term2 * rr3 + term3 * rr5 + term4 * rr7 + term5 * rr9;
+  const U de = term1 * rr3 + term2 * rr5 + term3 * rr7 + term4 * rr9 + term5 * rr11;
+  const U t1 = -ck * rr3 + dkr * rr5 - qkr * rr7;
+  const U t2 = ci * rr3 + dir * rr5 + qir * rr7;
+  const U t3 = U(2) * rr5;
+  const U t4 = U(-2) * (ck * rr5 - dkr * rr7 + qkr * rr9);
+  const U t5 = U(-2) * (ci * rr5 + dir * rr7 + qir * rr9);
+  const U t6 = U(4) * rr7;
+  // force on site i (emreal1c's frc; the k end computes its own)
+  const U qixk = qixx * qkx + qixy * qky + qixz * qkz;
+  const U qiyk = qixy * qkx + qiyy * qky + qiyz * qkz;
+  const U qizk = qixz * qkx + qiyz * qky + qizz * qkz;
+  const U qkxi = qkxx * qix + qkxy * qiy + qkxz * qiz;
+  const U qkyi = qkxy * qix + qkyy * qiy + qkyz * qiz;
+  const U qkzi = qkxz * qix + qkyz * qiy + qkzz * qiz;
+  const U diqkx = dix * qkxx + diy * qkxy + diz * qkxz;
+  const U diqky = dix * qkxy + diy * qkyy + diz * qkyz;
+  const U diqkz = dix * qkxz + diy * qkyz + diz * qkzz;
+  const U dkqix = dkx * qixx + dky * qixy + dkz * qixz;
+  const U dkqiy = dkx * qixy + dky * qiyy + dkz * qiyz;
+  const U dkqiz = dkx * qixz + dky * qiyz + dkz * qizz;
+  g[0] += (double)(de * xr + t1 * dix + t2 * dkx + t3 * (diqkx - dkqix) + t4 * qix + t5 * qkx + t6 * (qixk + qkxi));
+  g[1] += (double)(de * yr + t1 * diy + t2 * dky + t3 * (diqky - dkqiy) + t4 * qiy + t5 * qky + t6 * (qiyk + qkyi));
+  g[2] += (double)(de * zr + t1 * diz + t2 * dkz + t3 * (diqkz - dkqiz) + t4 * qiz + t5 * qkz + t6 * (qizk + qkzi));
+  // torque on site i (emreal1c's ttmi)
+  const U dirx = diy * zr - diz * yr, diry = diz * xr - dix * zr, dirz = dix * yr - diy * xr;
+  const U dikx = diy * dkz - diz * dky, diky = diz * dkx - dix * dkz, dikz = dix * dky - diy * dkx;
+  const U qirx = qiz * yr - qiy * zr, qiry = qix * zr - qiz * xr, qirz = qiy * xr - qix * yr;
+  const U qikx = qky * qiz - qkz * qiy, qiky = qkz * qix - qkx * qiz, qikz = qkx * qiy - qky * qix;
+  const U qikrx = qizk * yr - qiyk * zr, qikry = qixk * zr - qizk * xr, qikrz = qiyk * xr - qixk * yr;
+  const U dkqirx = dkqiz * yr - dkqiy * zr, dkqiry = dkqix * zr - dkqiz * xr, dkqirz = dkqiy * xr - dkqix * yr;
+  const U dqikx = diy * qkz - diz * qky + dky * qiz - dkz * qiy -
+                  U(2) * (qixy * qkxz + qiyy * qkyz + qiyz * qkzz - qixz * qkxy - qiyz * qkyy - qizz * qkyz);
+  const U dqiky = diz * qkx - dix * qkz + dkz * qix - dkx * qiz -
+                  U(2) * (qixz * qkxx + qiyz * qkxy + qizz * qkxz - qixx * qkxz - qixy * qkyz - qixz * qkzz);
+  const U dqikz = dix * qky - diy * qkx + dkx * qiy - dky * qix -
+                  U(2) * (qixx * qkxy + qixy * qkyy + qixz * qkyz - qixy * qkxx - qiyy * qkxy - qiyz * qkxz);
+  t[0] += (double)(-rr3 * dikx + t1 * dirx + t3 * (dqikx + dkqirx) - t4 * qirx - t6 * (qikrx + qikx));
+  t[1] += (double)(-rr3 * diky + t1 * diry + t3 * (dqiky + dkqiry) - t4 * qiry - t6 * (qikry + qiky));
+  t[2] += (double)(-rr3 * dikz + t1 * dirz + t3 * (dqikz + dkqirz) - t4 * qirz - t6 * (qikrz + qikz));
+  e_acc += 0.5 * (double)e;
+}
+
+// Pairs outside the 1-2..1-5 lists, in the form's precision over the list:
+// force and torque of site i, half of each pair energy (partials per block).
+template <bool MIXED>
+__global__ void __launch_bounds__(kBlock, MIXED ? 5 : 4) k_empole_pairs(
+    int n, int npad, Box box, double off2, EwM ew, const double4* __restrict__ pos,
+    const typename std::conditional<MIXED, float, double>::type* __restrict__ mrec, const int* __restrict__ perm,
+    const int* __restrict__ sp_off, const int* __restrict__ sp_ks, const int* __restrict__ sp_c,
+    const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb, const int* __restrict__ frs,
+    unsigned long long* __restrict__ dem, double* __restrict__ epart) {
+  using T = typename std::conditional<MIXED, float, double>::type;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double eacc = 0.0;
+  if (i < n) {
+    const double4 pi4 = pos[i];
+    T mi[10];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) mi[q] = mrec[(size_t)i * 12 + 1 + q];
+    const int io = perm[i];
+    const int s0 = sp_off[io], s1 = sp_off[io + 1];
+    double g3[3] = {0.0, 0.0, 0.0}, t3[3] = {0.0, 0.0, 0.0};
+    const int nn = min(nnb[i], maxnb);
+    int knext = nn > 0 ? __ldg(nb + i) : 0;  // list entries fetched one pair ahead
+#pragma unroll 1
+    for (int s = 0; s < nn; ++s) {
+      const int k = knext;
+      if (s + 1 < nn) knext = __ldg(nb + (size_t)(s + 1) * npad + i);
+      const double4 pk4 = pos[k];
+      double xrd = pk4.x - pi4.x, yrd = pk4.y - pi4.y, zrd = pk4.z - pi4.z;
+      image3(box, xrd, yrd, zrd);
+      const double r2d = r2_exact(xrd, yrd, zrd);
+      if (r2d > off2) continue;
+      bool scaled = false;
+      for (int q = s0; q < s1; ++q)
+        if (__ldg(sp_ks + q) == k) {
+          scaled = __ldg(sp_c + q) < 4;
+          break;
+        }
+      if (scaled) continue;
+      T mk[10];
+#pragma unroll
+      for (int q = 0; q < 10; ++q) mk[q] = mrec[(size_t)k * 12 + 1 + q];
+      mpole_pair<T>((T)xrd, (T)yrd, (T)zrd, (T)r2d, T(0), mi, mk, ew, eacc, g3, t3);
+    }
+    fix_add(dem + 3 * i + 0, g3[0]);
+    fix_add(dem + 3 * i + 1, g3[1]);
+    fix_add(dem + 3 * i + 2, g3[2]);
+    const int iz = frs[3 * i], ix = frs[3 * i + 1], axt = frs[3 * i + 2];
+    if (axt == 1 || axt == 2) torque_dist(pos, i, iz, ix, axt, t3, dem);
+  }
+  block_partial(eacc, epart);
+}
+
+// Per site, in FP64: the 1-2..1-5 pairs within the cutoff (all are in the
+// list when it is valid; the damped and bare terms cancel there to a small
+// difference), the emrecip1 terms from fphirec and the self energy.
+__global__ void __launch_bounds__(kBlock) k_empole_site(
+    int n, Box box, double off2, EwM ew, MScale ms, PmeGeom g, const double4* __restrict__ pos,
+    const double* __restrict__ rp, const int* __restrict__ perm, const int* __restrict__ sp_off,
+    const int* __restrict__ sp_ks, const int* __restrict__ sp_c, const double* __restrict__ fphirec,
+    const int* __restrict__ frs, unsigned long long* __restrict__ dem, double* __restrict__ epart) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double eacc = 0.0;
+  if (i < n) {
+    const double4 pi4 = pos[i];
+    const int io = perm[i];
+    const int s0 = sp_off[io], s1 = sp_off[io + 1];
+    double g3[3] = {0.0, 0.0, 0.0}, t3[3] = {0.0, 0.0, 0.0};
+    double mid[10];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) mid[q] = rp[(size_t)i * 10 + q];
+#pragma unroll 1
+    for (int q = s0; q < s1; ++q) {
+      const int cls = __ldg(sp_c + q);
+      if (cls >= 4) continue;
+      const int k = __ldg(sp_ks + q);
+      const double4 pk4 = pos[k];
+      double xrd = pk4.x - pi4.x, yrd = pk4.y - pi4.y, zrd = pk4.z - pi4.z;
+      image3(box, xrd, yrd, zrd);
+      const double r2d = r2_exact(xrd, yrd, zrd);
+      if (r2d > off2) continue;
+      double mkd[10];
+#pragma unroll
+      for (int w = 0; w < 10; ++w) mkd[w] = rp[(size_t)k * 10 + w];
+      mpole_pair<double>(xrd, yrd, zrd, r2d, 1.0 - ms.v[cls], mid, mkd, ew, eacc, g3, t3);
+    }
+    double gx = g3[0], gy = g3[1], gz = g3[2];
+    const double tx = t3[0], ty = t3[1], tz = t3[2];
+    // emrecip1 terms of site i from fphirec (FP64 multipoles)
+    const double fe = kElectric;
+    const double* r = rp + (size_t)i * 10;
+    const double cm[10] = {r[0], r[1], r[2], r[3], r[4], r[7], r[9], 2.0 * r[5], 2.0 * r[6], 2.0 * r[8]};
+    const double fm[10] = {cm[0], g.a[0] * cm[1], g.a[1] * cm[2], g.a[2] * cm[3], g.a[0] * g.a[0] * cm[4],
+                           g.a[1] * g.a[1] * cm[5], g.a[2] * g.a[2] * cm[6], g.a[0] * g.a[1] * cm[7],
+                           g.a[0] * g.a[2] * cm[8], g.a[1] * g.a[2] * cm[9]};
+    double FR[21];
+#pragma unroll
+    for (int q = 0; q < 20; ++q) FR[q + 1] = fe * fphirec[(size_t)i * 20 + q];
+    const int d1[10] = {2, 5, 8, 9, 11, 16, 18, 14, 15, 20};
+    const int d2[10] = {3, 8, 6, 10, 14, 12, 19, 16, 20, 17};
+    const int d3[10] = {4, 9, 10, 7, 15, 17, 13, 20, 18, 19};
+    double erec = 0.0, f1 = 0.0, f2 = 0.0, f3 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+      erec += fm[k] * FR[k + 1];
+      f1 += fm[k] * FR[d1[k]];
+      f2 += fm[k] * FR[d2[k]];
+      f3 += fm[k] * FR[d3[k]];
+    }
+    gx += g.recip[0] * ((double)g.n1 * f1);
+    gy += g.recip[1] * ((double)g.n2 * f2);
+    gz += g.recip[2] * ((double)g.n3 * f3);
+    const double cp[10] = {FR[1],
+                           g.a[0] * FR[2],
+                           g.a[1] * FR[3],
+                           g.a[2] * FR[4],
+                           g.a[0] * g.a[0] * FR[5],
+                           g.a[1] * g.a[1] * FR[6],
+                           g.a[2] * g.a[2] * FR[7],
+                           g.a[0] * g.a[1] * FR[8],
+                           g.a[0] * g.a[2] * FR[9],
+                           g.a[1] * g.a[2] * FR[10]};
+    double trq[3];
+    trq[0] = tx + cm[3] * cp[2] - cm[2] * cp[3] + 2.0 * (cm[6] - cm[5]) * cp[9] + cm[8] * cp[7] + cm[9] * cp[5] -
+             cm[7] * cp[8] - cm[9] * cp[6];
+    trq[1] = ty + cm[1] * cp[3] - cm[3] * cp[1] + 2.0 * (cm[4] - cm[6]) * cp[8] + cm[7] * cp[9] + cm[8] * cp[6] -
+             cm[8] * cp[4] - cm[9] * cp[7];
+    trq[2] = tz + cm[2] * cp[1] - cm[1] * cp[2] + 2.0 * (cm[5] - cm[4]) * cp[7] + cm[7] * cp[4] + cm[9] * cp[8] -
+             cm[7] * cp[5] - cm[8] * cp[9];
+    // Ewald self energy (empole1.f:134-160)
+    const double term = 2.0 * ew.a * ew.a;
+    const double fterm = -fe * ew.a / kSqrtPi;
+    const double dii = cm[1] * cm[1] + cm[2] * cm[2] + cm[3] * cm[3];
+    const double qii = 2.0 * (r[5] * r[5] + r[6] * r[6] + r[8] * r[8]) + r[4] * r[4] + r[7] * r[7] + r[9] * r[9];
+    const double eself = fterm * (cm[0] * cm[0] + term * (dii / 3.0 + 2.0 * term * qii / 5.0));
+    eacc += 0.5 * erec + eself;
+    fix_add(dem + 3 * i + 0, gx);
+    fix_add(dem + 3 * i + 1, gy);
+    fix_add(dem + 3 * i + 2, gz);
+    const int iz = frs[3 * i], ix = frs[3 * i + 1], axt = frs[3 * i + 2];
+    if (axt == 1 || axt == 2) torque_dist(pos, i, iz, ix, axt, trq, dem);
+  }
+  block_partial(eacc, epart);
+}
+
+// one block: the partials in block order, strided per thread, then a tree
+__global__ void __launch_bounds__(256) k_sum_partials(int m, const double* __restrict__ part, double* __restrict__ out) {
+  __shared__ double s[256];
+  double t = 0.0;
+  for (int q = threadIdx.x; q < m; q += 256) t += part[q];
+  s[threadIdx.x] = t;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = s[0];
+}
+
+// buffers made on first use, sized by n (freed when a re-targeted context
+// grows)
+template <typename P>
+int alloc_once(Ctx& c, P** p, size_t count, const char* what) {
+  if (*p) return THP_OK;
+  return cuda_status(cudaMalloc((void**)p, sizeof(P) * count), &c, what);
+}
+
+}  // namespace
+
+// Permanent-multipole energy (into d_em) and gradient (into d_out, original
+// order) for the sorted positions, multipoles and list of the context.
+int launch_empole(Ctx& c, double* d_out) {
+  int st;
+  if (!c.have_axes) return THP_E_STATE;
+  const size_t n = c.n;
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  if ((st = alloc_once(c, &c.d_depfix, 3 * n, "alloc gradient"))) return st;
+  if ((st = alloc_once(c, &c.d_empart, 2 * (size_t)nb + 1, "alloc mpole partials"))) return st;
+  c.d_em = c.d_empart + 2 * nb;
+  unsigned long long* dem = c.d_depfix;
+  if ((st = cuda_status(cudaMemsetAsync(dem, 0, sizeof(unsigned long long) * 3 * n, c.stream), &c, "zero dem")))
+    return st;
+  if ((st = launch_frames_sorted(c))) return st;
+  if ((st = launch_mpole_grid(c))) return st;
+  if ((st = launch_fphi_mpole20(c))) return st;
+  EwM ew;
+  const double a = c.cfg.aewald;
+  ew.a = a;
+  const double aesq2 = 2.0 * a * a;
+  double afac = 1.0 / (kSqrtPi * a);
+  for (int j = 0; j < 5; ++j) {
+    afac *= aesq2;
+    ew.f[j] = afac;
+  }
+  MScale ms;
+  for (int j = 0; j < 4; ++j) ms.v[j] = c.mscale[j];
+  ms.v[4] = 1.0;
+  const double off2 = c.cfg.ewaldcut * c.cfg.ewaldcut;
+  const PmeGeom g = pme_geom(c);
+#define THP_EMPOLE_ARGS                                                                                    \
+  c.n, c.npad, c.box, off2, ew, c.d_pos, MREC, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_c, c.d_nnb, c.d_nb, c.maxnb, \
+      c.d_frs, dem, c.d_empart
+  if (c.mixed) {
+#define MREC c.d_mrecf
+    k_empole_pairs<true><<<nb, kBlock, 0, c.stream>>>(THP_EMPOLE_ARGS);
+#undef MREC
+  } else {
+#define MREC c.d_mrec
+    k_empole_pairs<false><<<nb, kBlock, 0, c.stream>>>(THP_EMPOLE_ARGS);
+#undef MREC
+  }
+#undef THP_EMPOLE_ARGS
+  if ((st = cuda_status(cudaGetLastError(), &c, "empole pairs"))) return st;
+  k_empole_site<<<nb, kBlock, 0, c.stream>>>(c.n, c.box, off2, ew, ms, g, c.d_pos, c.d_rpole, c.d_perm, c.d_sp_off,
+                                             c.d_sp_ks, c.d_sp_c, c.d_fphirec, c.d_frs, dem, c.d_empart + nb);
+  if ((st = cuda_status(cudaGetLastError(), &c, "empole"))) return st;
+  k_sum_partials<<<1, 256, 0, c.stream>>>(2 * nb, c.d_empart, c.d_em);
+  if ((st = cuda_status(cudaGetLastError(), &c, "empole energy"))) return st;
+  return launch_gradient_out(c, dem, d_out);
+}
+
+}  // namespace thp

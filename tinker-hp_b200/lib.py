@@ -128,6 +128,10 @@ def load():
         "thp_bind_state": ([vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_int, _dp], C.c_int),
         "thp_last_error": ([], C.c_int),
         "thp_bind_gradient": ([vp, _dp], C.c_int),
+        "thp_set_mpole_scales": ([vp, _dp], C.c_int),
+        "thp_empole1": ([vp, _dp, _dp], C.c_int),
+        "thp_bind_mpole": ([vp, _dp, _dp], C.c_int),
+        "empole1_": ([], None),
         "thp_bind_grid": ([vp, _dp], C.c_int),
         "grid_uind_sites_": ([_ip, _ip, _dp, _dp, _dp], None),
         "fphi_uind_sites_": ([_ip, _ip, _dp, _dp, _dp, _dp], None),
@@ -258,6 +262,7 @@ class Context:
             offs[q] = _p(off, _ip)
             idxs[q] = _p(idx, _ip)
         self._check(L.thp_set_connectivity(self.h, offs, idxs, _p(scales_array(ws))), "thp_set_connectivity")
+        self._check(L.thp_set_mpole_scales(self.h, _p(_f64(ws.scales["m_scale"]))), "thp_set_mpole_scales")
         self.set_positions(ws.x, ws.y, ws.z)
         if rpole is not None:
             self.set_rpole(rpole)
@@ -331,6 +336,16 @@ class Context:
         ep = C.c_double()
         self._check(load().thp_get_gradient(self.h, _p(dep), C.byref(ep)), "thp_get_gradient")
         return ep.value, dep
+
+    def empole1(self, out=None):
+        """(Em, dEm/dx [n,3] kcal/mol/A): permanent-multipole energy and
+        gradient at the current positions (empole1c); `out` (a C-contiguous
+        float64 [n,3] array, e.g. pinned) receives the gradient."""
+        dem = np.zeros((self.n, 3)) if out is None else out
+        assert dem.shape == (self.n, 3) and dem.dtype == np.float64 and dem.flags["C_CONTIGUOUS"]
+        em = C.c_double()
+        self._check(load().thp_empole1(self.h, C.byref(em), _p(dem)), "thp_empole1")
+        return em.value, dem
 
     def md_verlet(self, nsteps, dt, mass, vel):
         """Velocity-Verlet NVE steps on the device (dt in ps).  Returns
