@@ -8,7 +8,7 @@ magnitudes (the total is their small difference: at 32,400 atoms it is 3e-4
 of them), gradient within 1e-9 of its largest component.  Mixed form (FP32 unscaled pairs and grid; FP64 scaled pairs,
 reciprocal sums and self term): energy within 1e-8 of the sum of the parts'
 magnitudes, force RMS error within 1e-5 of the force RMS (measured: 1e-9 and
-3e-7).
+2e-6).
 """
 import ctypes as C
 

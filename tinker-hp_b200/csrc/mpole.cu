@@ -22,12 +22,18 @@
 #include "grad_dev.cuh"
 #include "kernels.h"
 #include "pme_dev.cuh"
+#include "realspace_dev.cuh"
 
 namespace thp {
 
 namespace {
 
 constexpr int kBlock = 128;
+
+// resident blocks of the mixed pair kernel the register budget is cut for
+#ifndef THP_EMPOLE_MINB
+#define THP_EMPOLE_MINB 6
+#endif
 
 struct EwM {
   double a;
@@ -64,7 +70,14 @@ __device__ __forceinline__ void mpole_pair(U xr, U yr, U zr, U r2, U scalek, con
   const U ck = mk[0], dkx = mk[1], dky = mk[2], dkz = mk[3];
   const U qkxx = mk[4], qkxy = mk[5], qkxz = mk[6], qkyy = mk[7], qkyz = mk[8], qkzz = mk[9];
   const U f = (U)kElectric;
-  const U r = sqrt(r2);
+  // one reciprocal square root, then products (FP32: the approximate rsqrt)
+  U rinv;
+  if constexpr (std::is_same<U, float>::value)
+    rinv = rsqrtf(r2);
+  else
+    rinv = U(1) / sqrt(r2);
+  const U r = r2 * rinv;
+  const U r2inv = rinv * rinv;
   // intermediates involving moments and separation distance
   const U dir = dix * xr + diy * yr + diz * zr;
   const U qix = qixx * xr + qixy * yr + qixz * zr, qiy = qixy * xr + qiyy * yr + qiyz * zr,
@@ -83,20 +96,20 @@ __device__ __forceinline__ void mpole_pair(U xr, U yr, U zr, U r2, U scalek, con
   // (damping.f:17-55); the bare terms only for scaled pairs
   const U ra = (U)ew.a * r;
   const U ex = exp(-ra * ra);
-  const U b0 = erfc(ra) / r;
-  const U b1 = (b0 + (U)ew.f[0] * ex) / r2;
-  const U b2 = (U(3) * b1 + (U)ew.f[1] * ex) / r2;
-  const U b3 = (U(5) * b2 + (U)ew.f[2] * ex) / r2;
-  const U b4 = (U(7) * b3 + (U)ew.f[3] * ex) / r2;
-  const U b5 = (U(9) * b4 + (U)ew.f[4] * ex) / r2;
+  const U b0 = erfc(ra) * rinv;
+  const U b1 = (b0 + (U)ew.f[0] * ex) * r2inv;
+  const U b2 = (U(3) * b1 + (U)ew.f[1] * ex) * r2inv;
+  const U b3 = (U(5) * b2 + (U)ew.f[2] * ex) * r2inv;
+  const U b4 = (U(7) * b3 + (U)ew.f[3] * ex) * r2inv;
+  const U b5 = (U(9) * b4 + (U)ew.f[4] * ex) * r2inv;
   U rr1 = f * b0, rr3 = f * b1, rr5 = f * b2, rr7 = f * b3, rr9 = f * b4, rr11 = f * b5;
   if (scalek != U(0)) {
-    const U s1 = f / r;
-    const U s3 = s1 / r2;
-    const U s5 = U(3) * s3 / r2;
-    const U s7 = U(5) * s5 / r2;
-    const U s9 = U(7) * s7 / r2;
-    const U s11 = U(9) * s9 / r2;
+    const U s1 = f * rinv;
+    const U s3 = s1 * r2inv;
+    const U s5 = U(3) * s3 * r2inv;
+    const U s7 = U(5) * s5 * r2inv;
+    const U s9 = U(7) * s7 * r2inv;
+    const U s11 = U(9) * s9 * r2inv;
     rr1 -= scalek * s1;
     rr3 -= scalek * s3;
     rr5 -= scalek * s5;
@@ -154,21 +167,41 @@ __device__ __forceinline__ void mpole_pair(U xr, U yr, U zr, U r2, U scalek, con
 
 // Pairs outside the 1-2..1-5 lists, in the form's precision over the list:
 // force and torque of site i, half of each pair energy (partials per block).
+// The FP64 form reads the sorted positions and the FP64 multipole records
+// and tests the cutoff in FP64; the mixed form reads one 64-B record per
+// partner (wrapped position and multipoles, FP32) and images and tests in
+// FP32, as its direct-field pass does.
 template <bool MIXED>
-__global__ void __launch_bounds__(kBlock, MIXED ? 5 : 4) k_empole_pairs(
-    int n, int npad, Box box, double off2, EwM ew, const double4* __restrict__ pos,
-    const typename std::conditional<MIXED, float, double>::type* __restrict__ mrec, const int* __restrict__ perm,
-    const int* __restrict__ sp_off, const int* __restrict__ sp_ks, const int* __restrict__ sp_c,
-    const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb, const int* __restrict__ frs,
-    unsigned long long* __restrict__ dem, double* __restrict__ epart) {
+__global__ void __launch_bounds__(kBlock, MIXED ? THP_EMPOLE_MINB : 4) k_empole_pairs(
+    int n, int npad, Box box, double off2, EwM ew, const double4* __restrict__ pos, const double* __restrict__ mrec,
+    const float* __restrict__ erec, const int* __restrict__ perm, const int* __restrict__ sp_off,
+    const int* __restrict__ sp_ks, const int* __restrict__ sp_c, const int* __restrict__ nnb,
+    const int* __restrict__ nb, int maxnb, const int* __restrict__ frs, unsigned long long* __restrict__ dem,
+    double* __restrict__ epart) {
   using T = typename std::conditional<MIXED, float, double>::type;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double eacc = 0.0;
   if (i < n) {
-    const double4 pi4 = pos[i];
     T mi[10];
+    double4 pi4 = make_double4(0.0, 0.0, 0.0, 0.0);
+    float xi = 0.f, yi = 0.f, zi = 0.f;
+    if constexpr (MIXED) {
+      float v[16];
+      ld_rec8(erec + (size_t)i * 16, *reinterpret_cast<float(*)[8]>(&v[0]));
+      ld_rec8(erec + (size_t)i * 16 + 8, *reinterpret_cast<float(*)[8]>(&v[8]));
+      xi = v[0];
+      yi = v[1];
+      zi = v[2];
 #pragma unroll
-    for (int q = 0; q < 10; ++q) mi[q] = mrec[(size_t)i * 12 + 1 + q];
+      for (int q = 0; q < 10; ++q) mi[q] = v[5 + q];
+    } else {
+      pi4 = pos[i];
+#pragma unroll
+      for (int q = 0; q < 10; ++q) mi[q] = mrec[(size_t)i * 12 + 1 + q];
+    }
+    const float bx = (float)box.l[0], by = (float)box.l[1], bz = (float)box.l[2];
+    const float hx = 0.5f * bx, hy = 0.5f * by, hz = 0.5f * bz;
+    const float off2f = (float)off2;
     const int io = perm[i];
     const int s0 = sp_off[io], s1 = sp_off[io + 1];
     double g3[3] = {0.0, 0.0, 0.0}, t3[3] = {0.0, 0.0, 0.0};
@@ -178,11 +211,36 @@ __global__ void __launch_bounds__(kBlock, MIXED ? 5 : 4) k_empole_pairs(
     for (int s = 0; s < nn; ++s) {
       const int k = knext;
       if (s + 1 < nn) knext = __ldg(nb + (size_t)(s + 1) * npad + i);
-      const double4 pk4 = pos[k];
-      double xrd = pk4.x - pi4.x, yrd = pk4.y - pi4.y, zrd = pk4.z - pi4.z;
-      image3(box, xrd, yrd, zrd);
-      const double r2d = r2_exact(xrd, yrd, zrd);
-      if (r2d > off2) continue;
+      T xr, yr, zr, r2;
+      T mk[10];
+      if constexpr (MIXED) {
+        float v[16];
+        ld_rec8(erec + (size_t)k * 16, *reinterpret_cast<float(*)[8]>(&v[0]));
+        ld_rec8(erec + (size_t)k * 16 + 8, *reinterpret_cast<float(*)[8]>(&v[8]));
+        float x = v[0] - xi, y = v[1] - yi, z = v[2] - zi;
+        x = fabsf(x) > hx ? x - copysignf(bx, x) : x;
+        y = fabsf(y) > hy ? y - copysignf(by, y) : y;
+        z = fabsf(z) > hz ? z - copysignf(bz, z) : z;
+        r2 = x * x + y * y + z * z;
+        if (r2 > off2f) continue;
+        xr = x;
+        yr = y;
+        zr = z;
+#pragma unroll
+        for (int q = 0; q < 10; ++q) mk[q] = v[5 + q];
+      } else {
+        const double4 pk4 = pos[k];
+        double xrd = pk4.x - pi4.x, yrd = pk4.y - pi4.y, zrd = pk4.z - pi4.z;
+        image3(box, xrd, yrd, zrd);
+        const double r2d = r2_exact(xrd, yrd, zrd);
+        if (r2d > off2) continue;
+        xr = xrd;
+        yr = yrd;
+        zr = zrd;
+        r2 = r2d;
+#pragma unroll
+        for (int q = 0; q < 10; ++q) mk[q] = mrec[(size_t)k * 12 + 1 + q];
+      }
       bool scaled = false;
       for (int q = s0; q < s1; ++q)
         if (__ldg(sp_ks + q) == k) {
@@ -190,10 +248,7 @@ __global__ void __launch_bounds__(kBlock, MIXED ? 5 : 4) k_empole_pairs(
           break;
         }
       if (scaled) continue;
-      T mk[10];
-#pragma unroll
-      for (int q = 0; q < 10; ++q) mk[q] = mrec[(size_t)k * 12 + 1 + q];
-      mpole_pair<T>((T)xrd, (T)yrd, (T)zrd, (T)r2d, T(0), mi, mk, ew, eacc, g3, t3);
+      mpole_pair<T>(xr, yr, zr, r2, T(0), mi, mk, ew, eacc, g3, t3);
     }
     fix_add(dem + 3 * i + 0, g3[0]);
     fix_add(dem + 3 * i + 1, g3[1]);
@@ -350,18 +405,13 @@ int launch_empole(Ctx& c, double* d_out) {
   ms.v[4] = 1.0;
   const double off2 = c.cfg.ewaldcut * c.cfg.ewaldcut;
   const PmeGeom g = pme_geom(c);
-#define THP_EMPOLE_ARGS                                                                                    \
-  c.n, c.npad, c.box, off2, ew, c.d_pos, MREC, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_c, c.d_nnb, c.d_nb, c.maxnb, \
-      c.d_frs, dem, c.d_empart
-  if (c.mixed) {
-#define MREC c.d_mrecf
+#define THP_EMPOLE_ARGS                                                                                          \
+  c.n, c.npad, c.box, off2, ew, c.d_pos, c.d_mrec, c.d_erec, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_c, c.d_nnb, c.d_nb, \
+      c.maxnb, c.d_frs, dem, c.d_empart
+  if (c.mixed)
     k_empole_pairs<true><<<nb, kBlock, 0, c.stream>>>(THP_EMPOLE_ARGS);
-#undef MREC
-  } else {
-#define MREC c.d_mrec
+  else
     k_empole_pairs<false><<<nb, kBlock, 0, c.stream>>>(THP_EMPOLE_ARGS);
-#undef MREC
-  }
 #undef THP_EMPOLE_ARGS
   if ((st = cuda_status(cudaGetLastError(), &c, "empole pairs"))) return st;
   k_empole_site<<<nb, kBlock, 0, c.stream>>>(c.n, c.box, off2, ew, ms, g, c.d_pos, c.d_rpole, c.d_perm, c.d_sp_off,
