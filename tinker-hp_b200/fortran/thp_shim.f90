@@ -1,14 +1,15 @@
 ! thp_shim.f90 -- ISO_C_BINDING layer between Tinker-HP (v1.2 module state)
 ! and libthp.so.  Replaces the calls newinduce_pme2 (epolar.f:108,
-! epolar1.f:145), mlistcell (nblist.f:109) and epolar1 (gradient.f:165) by
-! thp_newinduce_pme2, thp_mlistcell and thp_epolar1, and offers the batched
-! per-site PME routines.  Not compiled in this repository's image (no Fortran
+! epolar1.f:145), mlistcell (nblist.f:109), epolar1 (gradient.f:165) and
+! empole1 (gradient.f, the permanent-multipole term) by thp_newinduce_pme2,
+! thp_mlistcell, thp_epolar1 and thp_empole1, and offers the batched per-site
+! PME routines.  Not compiled in this repository's image (no Fortran
 ! compiler); it follows the C declarations of include/thp.h.
 module thp_shim
   use iso_c_binding
   implicit none
   private
-  public :: thp_init, thp_newinduce_pme2, thp_mlistcell, thp_epolar, thp_epolar1, thp_finalize
+  public :: thp_init, thp_newinduce_pme2, thp_mlistcell, thp_epolar, thp_epolar1, thp_empole1, thp_finalize
   public :: thp_grid_uind_sites, thp_fphi_uind_sites
 
   type, bind(C) :: thp_config
@@ -64,6 +65,16 @@ module thp_shim
       import :: c_int, c_ptr
       type(c_ptr), value :: h, dep
     end function
+    integer(c_int) function c_set_mpole_scales(h, m) bind(C, name="thp_set_mpole_scales")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, m
+    end function
+    integer(c_int) function c_bind_mpole(h, em, dem) bind(C, name="thp_bind_mpole")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, em, dem
+    end function
+    subroutine c_empole1() bind(C, name="empole1_")
+    end subroutine
     subroutine c_grid_uind_sites(ns, isite, fuind, fuinp, qgrid) bind(C, name="grid_uind_sites_")
       import :: c_int, c_double
       integer(c_int), intent(in) :: ns, isite(*)
@@ -94,9 +105,10 @@ contains
     use polpot, only: politer, poleps, p2scale, p3scale, p4scale, p5scale, p2iscale, p3iscale, &
                       p4iscale, p5iscale, d1scale, d2scale, d3scale, d4scale, u1scale, u2scale, &
                       u3scale, u4scale
+    use mplpot, only: m2scale, m3scale, m4scale, m5scale
     logical, intent(in) :: mixed
     type(thp_config), target :: cfg
-    real(c_double), target :: scales(16)
+    real(c_double), target :: scales(16), mscales(4)
     type(c_ptr), target :: offp(8), idxp(8)
     integer :: st
     cfg%n = n
@@ -119,6 +131,9 @@ contains
     scales = [p2scale, p3scale, p4scale, p5scale, p2iscale, p3iscale, p4iscale, p5iscale, &
               d1scale, d2scale, d3scale, d4scale, u1scale, u2scale, u3scale, u4scale]
     st = c_set_connectivity(ctx, c_loc(offp), c_loc(idxp), c_loc(scales))
+    if (st /= 0) call fatal
+    mscales = [m2scale, m3scale, m4scale, m5scale]
+    st = c_set_mpole_scales(ctx, c_loc(mscales))
     if (st /= 0) call fatal
     call set_frames()
   end subroutine
@@ -234,6 +249,19 @@ contains
     if (st /= 0) call fatal
     call c_epolar1()
     if (c_last_error() /= 0 .and. c_last_error() /= 3) call fatal
+  end subroutine
+
+  ! empole1 (empole1.f:10): energy into em, gradient into deriv::dem
+  ! (overwritten, as empole1c zeroes it)
+  subroutine thp_empole1
+    use deriv, only: dem
+    use energi, only: em
+    integer :: st
+    call bind_all()
+    st = c_bind_mpole(ctx, c_loc(em), c_loc(dem))
+    if (st /= 0) call fatal
+    call c_empole1()
+    if (c_last_error() /= 0) call fatal
   end subroutine
 
   ! grid_uind_site over a whole site list (pmestuff.f:280), one rank
