@@ -39,6 +39,14 @@ class OrSystem(C.Structure):
     ]
 
 
+class OrVdw(C.Structure):
+    _fields_ = [
+        ("nclass", C.c_int), ("cls", _ip), ("radmin", _dp), ("eps", _dp), ("radmin4", _dp), ("eps4", _dp),
+        ("ired", _ip), ("kred", _dp), ("v_scale", C.c_double * 4), ("vdwcut", C.c_double),
+        ("vdwtaper", C.c_double), ("ghal", C.c_double), ("dhal", C.c_double),
+    ]
+
+
 class OrSolveInfo(C.Structure):
     _fields_ = [("niter", C.c_int), ("converged", C.c_int), ("resnrm", C.c_double),
                 ("ene", C.c_double * 2)]
@@ -70,6 +78,7 @@ def lib():
         L.or_epolar.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         L.or_epolar1.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, _dp, _dp]
         L.or_empole1.argtypes = [C.c_void_p, _ip, _ip, _ip, _dp, _dp]
+        L.or_ehal1.argtypes = [C.c_void_p, C.POINTER(OrVdw), _dp, _dp]
         L.or_rotpole.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _dp]
         L.or_grid_uind_sites.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp, _dp]
         L.or_fphi_uind_sites.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp, _dp, _dp]
@@ -235,6 +244,28 @@ class Oracle:
         if st != 0:
             raise RuntimeError(f"oracle empole1 status {st}")
         return parts[0], dem, tuple(parts[1:])
+
+    def ehal1(self, vdw=None):
+        """Buffered 14-7 energy and gradient (ehal1c): (ev, dev [n,3])."""
+        v = self.ws.vdw if vdw is None else vdw
+        keep = [np.ascontiguousarray(v["cls"], np.int32), np.ascontiguousarray(v["radmin"], np.float64),
+                np.ascontiguousarray(v["eps"], np.float64), np.ascontiguousarray(v["radmin4"], np.float64),
+                np.ascontiguousarray(v["eps4"], np.float64), np.ascontiguousarray(v["ired"], np.int32),
+                np.ascontiguousarray(v["kred"], np.float64)]
+        sv = OrVdw()
+        sv.nclass = int(v["nclass"])
+        sv.cls, sv.radmin, sv.eps, sv.radmin4, sv.eps4 = (_p(keep[0], _ip), _p(keep[1]), _p(keep[2]),
+                                                          _p(keep[3]), _p(keep[4]))
+        sv.ired, sv.kred = _p(keep[5], _ip), _p(keep[6])
+        for q in range(4):
+            sv.v_scale[q] = v["v_scale"][q]
+        sv.vdwcut, sv.vdwtaper, sv.ghal, sv.dhal = v["vdwcut"], v["vdwtaper"], v["ghal"], v["dhal"]
+        dev = np.zeros((self.ws.n, 3))
+        ev = C.c_double()
+        st = lib().or_ehal1(self.ctx, C.byref(sv), _p(dev), C.byref(ev))
+        if st != 0:
+            raise RuntimeError(f"oracle ehal1 status {st}")
+        return ev.value, dev
 
     def grid_uind_sites(self, sites, fuind, fuinp, grid):
         """grid_uind_site for 0-based `sites`: adds into a copy of the complex

@@ -2230,4 +2230,121 @@ int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, dou
   return OR_OK;
 }
 
+// ===========================================================================
+// van der Waals: ehal1c (ehal1.f:69-482, standard branch) over the list of
+// vlistcell (nblist.f:1148-1305).  The list is restated as every pair k > i
+// whose reduced minimum-image distance is within vdwcut + lbuffer (the
+// reference finds the same pairs through its cells); the energy loop then
+// applies r <= vdwcut and the taper above vdwtaper.
+int or_ehal1(OrCtx* c, const OrVdw* v, double* dev, double* ev_out) {
+  const OrSystem& s = c->s;
+  const int n = s.n;
+  std::fill(dev, dev + (size_t)n * 3, 0.0);
+  const double vbuf = v->vdwcut + s.lbuffer;
+  if (vbuf > 0.5 * std::min(s.xbox, std::min(s.ybox, s.zbox))) return OR_E_BOX_TOO_SMALL;
+  // reduced coordinates (ehal1.f:193-205)
+  std::vector<double> xr((size_t)n), yr((size_t)n), zr((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    const int iv = v->ired[i];
+    const double rdn = v->kred[i];
+    xr[i] = rdn * (s.x[i] - s.x[iv]) + s.x[iv];
+    yr[i] = rdn * (s.y[i] - s.y[iv]) + s.y[iv];
+    zr[i] = rdn * (s.z[i] - s.z[iv]) + s.z[iv];
+  }
+  // switch.f:80-117 (mode VDW): off = vdwcut, cut = vdwtaper
+  const double off = v->vdwcut, cut = v->vdwtaper;
+  const double off2 = off * off, cut2 = cut * cut;
+  double c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0;
+  if (cut < off) {
+    const double denom = std::pow(off - cut, 5);
+    c0 = off * off2 * (off2 - 5.0 * off * cut + 10.0 * cut2) / denom;
+    c1 = -30.0 * off2 * cut2 / denom;
+    c2 = 30.0 * (off2 * cut + off * cut2) / denom;
+    c3 = -10.0 * (off2 + 4.0 * off * cut + cut2) / denom;
+    c4 = 15.0 * (off + cut) / denom;
+    c5 = -6.0 / denom;
+  }
+  const double ghal = v->ghal, dhal = v->dhal;
+  const int nc = v->nclass;
+  std::vector<double> vscale((size_t)n, 1.0);
+  std::vector<int> iv14((size_t)n, -1);
+  const int slot[4] = {OR_I12, OR_I13, OR_I14, OR_I15};
+  double ev = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const int iv = v->ired[i];
+    const double redi = v->kred[i], rediv = 1.0 - redi;
+    const int it = v->cls[i];
+    for (int b = 0; b < 4; ++b)
+      for_conn(s, slot[b], i, [&](int k) {
+        vscale[k] = v->v_scale[b];
+        if (b == 2) iv14[k] = i;
+      });
+    for (int k = i + 1; k < n; ++k) {
+      double xd = xr[i] - xr[k], yd = yr[i] - yr[k], zd = zr[i] - zr[k];
+      image(c->cell, xd, yd, zd);
+      const double rik2 = xd * xd + yd * yd + zd * zd;
+      if (rik2 > vbuf * vbuf) continue;  // not in the list
+      if (!(rik2 <= off2)) continue;
+      const int kv = v->ired[k];
+      const double redk = v->kred[k], redkv = 1.0 - redk;
+      const int kt = v->cls[k];
+      const double rik = std::sqrt(rik2);
+      double rv = v->radmin[kt * nc + it];
+      double eps = v->eps[kt * nc + it];
+      if (iv14[k] == i) {
+        rv = v->radmin4[kt * nc + it];
+        eps = v->eps4[kt * nc + it];
+      }
+      eps = eps * vscale[k];
+      const double rv7 = std::pow(rv, 7);
+      const double rik6 = rik2 * rik2 * rik2;
+      const double rik7 = rik6 * rik;
+      const double rho = rik7 + ghal * rv7;
+      const double tau = (dhal + 1.0) / (rik + dhal * rv);
+      const double tau7 = std::pow(tau, 7);
+      const double dtau = tau / (dhal + 1.0);
+      const double gtau = eps * tau7 * rik6 * (ghal + 1.0) * (rv7 / rho) * (rv7 / rho);
+      double e = eps * tau7 * rv7 * ((ghal + 1.0) * rv7 / rho - 2.0);
+      double de = -7.0 * (dtau * e + gtau);
+      if (rik2 > cut2) {
+        const double rik3 = rik2 * rik, rik4 = rik2 * rik2, rik5 = rik2 * rik3;
+        const double taper = c5 * rik5 + c4 * rik4 + c3 * rik3 + c2 * rik2 + c1 * rik + c0;
+        const double dtaper = 5.0 * c5 * rik4 + 4.0 * c4 * rik3 + 3.0 * c3 * rik2 + 2.0 * c2 * rik + c1;
+        de = e * dtaper + de * taper;
+        e = e * taper;
+      }
+      ev += e;
+      de = de / rik;
+      const double dedx = de * xd, dedy = de * yd, dedz = de * zd;
+      if (i == iv) {
+        dev[i * 3 + 0] += dedx;
+        dev[i * 3 + 1] += dedy;
+        dev[i * 3 + 2] += dedz;
+      } else {
+        dev[i * 3 + 0] += dedx * redi;
+        dev[i * 3 + 1] += dedy * redi;
+        dev[i * 3 + 2] += dedz * redi;
+        dev[iv * 3 + 0] += dedx * rediv;
+        dev[iv * 3 + 1] += dedy * rediv;
+        dev[iv * 3 + 2] += dedz * rediv;
+      }
+      if (k == kv) {
+        dev[k * 3 + 0] -= dedx;
+        dev[k * 3 + 1] -= dedy;
+        dev[k * 3 + 2] -= dedz;
+      } else {
+        dev[k * 3 + 0] -= dedx * redk;
+        dev[k * 3 + 1] -= dedy * redk;
+        dev[k * 3 + 2] -= dedz * redk;
+        dev[kv * 3 + 0] -= dedx * redkv;
+        dev[kv * 3 + 1] -= dedy * redkv;
+        dev[kv * 3 + 2] -= dedz * redkv;
+      }
+    }
+    for (int b = 0; b < 4; ++b) for_conn(s, slot[b], i, [&](int k) { vscale[k] = 1.0; });
+  }
+  if (ev_out) *ev_out = ev;
+  return OR_OK;
+}
+
 }  // extern "C"

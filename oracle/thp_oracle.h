@@ -102,6 +102,31 @@ int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxi
  * list (or_mlistcell).  parts (may be NULL) [4]: total, real, recip, self. */
 int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, double* dem, double* parts);
 
+/* van der Waals parameters of ehal1c (kvdw.f): per-atom class (0-based),
+ * pair tables [nclass][nclass] of Rmin and epsilon (combined by the
+ * caller's rules) and their 1-4 forms, reduction parent (0-based) and factor,
+ * the 1-2..1-5 scales, cutoff and taper start (absolute, A), buffer
+ * constants. */
+typedef struct OrVdw {
+  int nclass;
+  const int* cls;
+  const double* radmin;
+  const double* eps;
+  const double* radmin4;
+  const double* eps4;
+  const int* ired;
+  const double* kred;
+  double v_scale[4];
+  double vdwcut, vdwtaper;
+  double ghal, dhal;
+} OrVdw;
+
+/* ehal1c (ehal1.f:69-482, standard branch): buffered 14-7 energy and
+ * gradient dev [n][3] over the pairs of the vdW list (vlistcell,
+ * nblist.f:1148-1305: reduced coordinates, half list within vdwcut +
+ * lbuffer), with the 5th-degree taper (switch.f:80-117). */
+int or_ehal1(OrCtx* c, const OrVdw* v, double* dev, double* ev);
+
 /* grid_uind_site (pmestuff.f:280-405) for nsites sites (0-based atom
  * numbers): adds the fractional dipoles fuind/fuinp (3 per site) into the
  * interleaved complex grid [n3][n2][n1] (qgrid2in_2d(2,n1,n2,n3)). */

@@ -185,3 +185,43 @@ def isolated_empole(ws, rpole, electric=332.063714):
             g2 = q[k] * t2 - np.einsum("c,abc->ab", dp[k], t3) + np.einsum("cd,abcd->ab", Q[k], t4)
             e += ms[i, k] * (q[i] * phi + dp[i] @ g1 + np.einsum("ab,ab", Q[i], g2))
     return electric * e
+
+
+def buffered_14_7_energy(ws, vdw):
+    """van der Waals energy by direct summation over all pairs within the
+    cutoff, in the textbook form of the buffered 14-7 potential,
+    E = eps ((1+d)/(rho+d))^7 ((1+g)/(rho^7+g) - 2), rho = r/Rmin, on the
+    reduced (H-shifted) sites, times the smoothstep S(t) = 1 - 10t^3 + 15t^4
+    - 6t^5 between the taper start and the cutoff, with the 1-2..1-5 scales."""
+    n = ws.n
+    pos = ws.positions()
+    par = pos[vdw["ired"]]
+    red = vdw["kred"][:, None] * (pos - par) + par
+    L = np.asarray(ws.box)
+    cls = vdw["cls"]
+    scale = np.ones((n, n))
+    is14 = np.zeros((n, n), dtype=bool)
+    for b, name in enumerate(("i12", "i13", "i14", "i15")):
+        off, idx = ws.conn[name]
+        for i in range(n):
+            for k in idx[off[i]:off[i + 1]]:
+                scale[i, k] = vdw["v_scale"][b]
+                if b == 2:
+                    is14[i, k] = True
+    e = 0.0
+    d, g = vdw["dhal"], vdw["ghal"]
+    cut, off = vdw["vdwtaper"], vdw["vdwcut"]
+    for i in range(n - 1):
+        x = red[i] - red[i + 1:]
+        x -= L * np.round(x / L)
+        r = np.sqrt(np.einsum("ij,ij->i", x, x))
+        k = np.arange(i + 1, n)
+        m = r <= off
+        r, k = r[m], k[m]
+        rv = np.where(is14[i, k], vdw["radmin4"][cls[k], cls[i]], vdw["radmin"][cls[k], cls[i]])
+        ep = np.where(is14[i, k], vdw["eps4"][cls[k], cls[i]], vdw["eps"][cls[k], cls[i]]) * scale[i, k]
+        rho = r / rv
+        ee = ep * ((1 + d) / (rho + d)) ** 7 * ((1 + g) / (rho ** 7 + g) - 2)
+        t = np.clip((r - cut) / (off - cut), 0.0, 1.0)
+        e += np.sum(ee * (1 - 10 * t ** 3 + 15 * t ** 4 - 6 * t ** 5))
+    return e

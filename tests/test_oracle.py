@@ -378,3 +378,39 @@ def test_empole_two_waters_reach_the_isolated_limit(thp):
     fit = np.linalg.solve(np.stack([np.ones(3), Ls ** -3, Ls ** -5], axis=1), np.array([es[L] for L in Ls]))
     assert abs(es[30.0] - eiso) > 1e-3 * abs(eiso), (es, eiso)  # the image term is visible
     assert abs(fit[0] - eiso) < 1e-6 * abs(eiso), (fit, eiso)
+
+
+# ---- van der Waals (ehal1c) -------------------------------------------------
+
+def test_ehal1_energy_matches_textbook_form(thp):
+    # the reference's taper is the smoothstep expanded in powers of r, whose
+    # coefficients reach 1e5 for a 0.9 A window: the two forms differ by
+    # rounding at 1e-11 relative (measured 1.8e-11)
+    ws = thp.water.make_water_box(216, cfg=0, edge=20.0)
+    ev, _ = O.Oracle(ws).ehal1()
+    ref = ewald_ref.buffered_14_7_energy(ws, ws.vdw)
+    assert abs(ev - ref) < 1e-9 * abs(ref), (ev, ref)
+
+
+def test_ehal1_gradient_matches_finite_differences(thp):
+    # the hydrogens' reduced sites move with their oxygens, so the
+    # reduction chain rule is checked too
+    ws = thp.water.make_water_box(216, cfg=0, edge=20.0)
+    _, dev = O.Oracle(ws).ehal1()
+    pos0 = ws.positions()
+    h = 1e-5
+    for atom in (0, 1, 2, 300, 646):
+        for d in range(3):
+            e = []
+            for sgn in (1, -1):
+                p = pos0.copy()
+                p[atom, d] += sgn * h
+                e.append(O.Oracle(ws.with_positions(p)).ehal1()[0])
+            fd = (e[0] - e[1]) / (2 * h)
+            assert abs(fd - dev[atom, d]) < 1e-6 * np.abs(dev).max() + 1e-7, (atom, d, fd, dev[atom, d])
+
+
+def test_ehal1_refuses_a_small_box(thp):
+    ws = thp.water.make_water_box(64, cfg=0, edge=16.0)  # 9 + 0.5 A exceeds half of 16 A
+    with pytest.raises(RuntimeError, match="status 8"):
+        O.Oracle(ws).ehal1()

@@ -48,6 +48,72 @@ SCALES = {
     "m_scale": (0.0, 0.0, 0.4, 0.8),   # mpole-12..15-scale (water03.prm:34-37)
 }
 
+# water03.prm:91-92 (vdw: Rmin as a diameter, epsilon, reduction factor),
+# :23-27 (buffered 14-7, CUBIC-MEAN radii, HHG well depths), :30-33 (scales)
+WATER_VDW = {"O": (3.4050, 0.1100, 0.0), "H": (2.6550, 0.0135, 0.910)}
+VDW_RULES = {"radius": "CUBIC-MEAN", "epsilon": "HHG", "radiustype": "R-MIN", "radiussize": "DIAMETER"}
+VDW_SCALE = (0.0, 0.0, 1.0, 1.0)   # vdw-12..15-scale
+VDW_CUTOFF_DEFAULT = 9.0            # cutoffs.f: vdwcut
+VDW_TAPER = 0.90                    # cutoffs.f: vdwtaper (fraction of the cutoff)
+GHAL, DHAL = 0.12, 0.07             # initprm.f:383-384 (buffered 14-7 constants)
+
+
+def vdw_pair_tables(rad, eps, rad4=None, eps4=None, rules=None):
+    """Pair Rmin and epsilon tables [nc][nc] from per-class values
+    (kvdw.f:318-410 for the SIGMA/DIAMETER conversions and the ARITHMETIC,
+    GEOMETRIC, CUBIC-MEAN radius and ARITHMETIC, GEOMETRIC, HARMONIC, HHG
+    well-depth rules)."""
+    rules = dict(VDW_RULES if rules is None else rules)
+    twosix = 2.0 ** (1.0 / 6.0)
+
+    def conv(r):
+        r = list(r)
+        if rules.get("radiustype", "R-MIN") == "SIGMA":
+            r = [twosix * v for v in r]
+        if rules.get("radiussize", "RADIUS") == "DIAMETER":
+            r = [0.5 * v for v in r]
+        return r
+
+    rad4 = [r4 if r4 else r for r, r4 in zip(rad, rad4 or rad)]
+    eps4 = [e4 if e4 else e for e, e4 in zip(eps, eps4 or eps)]
+    out = []
+    for rr, ee in ((conv(rad), [abs(e) for e in eps]), (conv(rad4), [abs(e) for e in eps4])):
+        nc = len(rr)
+        R = [[0.0] * nc for _ in range(nc)]
+        E = [[0.0] * nc for _ in range(nc)]
+        for i in range(nc):
+            for k in range(i, nc):
+                ri, rk = rr[i], rr[k]
+                if ri == 0.0 and rk == 0.0:
+                    rd = 0.0
+                elif rules["radius"] == "ARITHMETIC":
+                    rd = ri + rk
+                elif rules["radius"] == "GEOMETRIC":
+                    rd = 2.0 * (math.sqrt(ri) * math.sqrt(rk))
+                elif rules["radius"] == "CUBIC-MEAN":
+                    rd = 2.0 * (ri ** 3 + rk ** 3) / (ri ** 2 + rk ** 2)
+                else:
+                    rd = ri + rk
+                ei, ek = ee[i], ee[k]
+                si, sk = math.sqrt(ei), math.sqrt(ek)
+                if ei == 0.0 and ek == 0.0:
+                    ep = 0.0
+                elif rules["epsilon"] == "ARITHMETIC":
+                    ep = 0.5 * (ei + ek)
+                elif rules["epsilon"] == "GEOMETRIC":
+                    ep = si * sk
+                elif rules["epsilon"] == "HARMONIC":
+                    ep = 2.0 * (ei * ek) / (ei + ek)
+                elif rules["epsilon"] == "HHG":
+                    ep = 4.0 * (ei * ek) / (si + sk) ** 2
+                else:
+                    ep = si * sk
+                R[i][k] = R[k][i] = rd
+                E[i][k] = E[k][i] = ep
+        out += [R, E]
+    return out  # radmin, eps, radmin4, eps4
+
+
 # frame codes shared with the C-ABI: 1 = Z-then-X, 2 = Bisector
 AXT_Z_THEN_X = 1
 AXT_BISECTOR = 2

@@ -51,6 +51,7 @@ class WaterSystem:
     nfft: tuple
     bsorder: int = P.BSORDER
     scales: dict = dataclasses.field(default_factory=lambda: dict(P.SCALES))
+    vdw: dict = None       # van der Waals description (water_vdw), or None
 
     def positions(self):
         return np.stack([self.x, self.y, self.z], axis=1)
@@ -176,7 +177,7 @@ def _assemble(nw, edge, xyz, grid_spacing, ewaldcut, lbuffer, aewald):
                        y=np.ascontiguousarray(xyz[:, 1]), z=np.ascontiguousarray(xyz[:, 2]),
                        pole=pole, zaxis=zaxis, xaxis=xaxis, axt=axt, polarity=polarity, thole=thole,
                        pdamp=pdamp, mol=mol, conn=conn, aewald=aewald, ewaldcut=ewaldcut,
-                       lbuffer=lbuffer, nfft=(k, pme_k, k))
+                       lbuffer=lbuffer, nfft=(k, pme_k, k), vdw=water_vdw(n))
 
 
 _EWALD_CACHE = {}
@@ -186,6 +187,24 @@ def _ewaldcof_cached(cut):
     if cut not in _EWALD_CACHE:
         _EWALD_CACHE[cut] = P.ewaldcof(cut)
     return _EWALD_CACHE[cut]
+
+
+def water_vdw(n, vdwcut=P.VDW_CUTOFF_DEFAULT):
+    """van der Waals description of n/3 waters ordered O, H, H: classes
+    (O 0, H 1), pair tables by the water rules, reduction of each H towards
+    its oxygen (kvdw.f:490-503), the vdw-12..15 scales, cutoff and taper."""
+    nw = n // 3
+    rad = [P.WATER_VDW["O"][0], P.WATER_VDW["H"][0]]
+    eps = [P.WATER_VDW["O"][1], P.WATER_VDW["H"][1]]
+    radmin, epsm, radmin4, eps4 = P.vdw_pair_tables(rad, eps)
+    cls = np.tile(np.array([0, 1, 1], np.int32), nw)
+    o = np.repeat(np.arange(nw, dtype=np.int32) * 3, 3)
+    ired = np.where(cls == 0, np.arange(n, dtype=np.int32), o).astype(np.int32)
+    kred = np.where(cls == 0, P.WATER_VDW["O"][2], P.WATER_VDW["H"][2]).astype(np.float64)
+    return {"nclass": 2, "cls": cls, "ired": ired, "kred": kred,
+            "radmin": np.array(radmin), "eps": np.array(epsm), "radmin4": np.array(radmin4),
+            "eps4": np.array(eps4), "v_scale": P.VDW_SCALE, "vdwcut": vdwcut,
+            "vdwtaper": P.VDW_TAPER * vdwcut, "ghal": P.GHAL, "dhal": P.DHAL}
 
 
 def water_connectivity(nw):
