@@ -184,6 +184,25 @@ int thp_set_mpole_scales(thp_ctx* ctx, const double* m);
  * the reciprocal-space sums and the self term in FP64; gradients accumulate
  * in 64-bit fixed point as thp_get_gradient's. */
 int thp_empole1(thp_ctx* ctx, double* em, double* dem);
+/* van der Waals description (kvdw.f): cls [n] vdW class of each atom
+ * (0-based, < nclass); tables [4][nclass][nclass] = pair Rmin (A), pair
+ * epsilon (kcal/mol), and their 1-4 forms, already combined by the force
+ * field's rules (kvdw.f:318-480); ired [n] reduction parent (0-based, the
+ * atom itself when unreduced) and kred [n] reduction factor (kvdw.f:490-503);
+ * vscale [4] v2scale..v5scale; vdwcut and vdwtaper in A (the taper start as
+ * a distance, cutoffs.f:241); ghal, dhal the buffered 14-7 constants
+ * (0.12, 0.07).  THP_E_BOX_TOO_SMALL when vdwcut + lbuffer exceeds half the
+ * box (nblist.f:1183-1193). */
+int thp_set_vdw(thp_ctx* ctx, const int* cls, int nclass, const double* tables, const int* ired,
+                const double* kred, const double* vscale, double vdwcut, double vdwtaper, double ghal,
+                double dhal);
+/* Buffered 14-7 van der Waals energy and gradient, ehal1c (ehal1.f:69-482,
+ * standard branch; no long-range correction) over the pairs vlistcell
+ * (nblist.f:1148) would list: ev (kcal/mol) and dev [n][3] (kcal/mol/A,
+ * original order; either may be NULL), FP64 in both precisions.  The pairs
+ * are found in the context's cell sort (kept or rebuilt as for a solve);
+ * THP_E_INVALID when a reduction moves a site by more than 0.3 A. */
+int thp_ehal1(thp_ctx* ctx, double* ev, double* dev);
 /* Velocity-Verlet NVE dynamics driven by the polarization gradient alone
  * (verlet.f:17-200 with gradient = epolar1): per step a half kick, a drift of
  * the positions on the device, a solve warm-started from the predictor when
@@ -314,6 +333,8 @@ int thp_bind_state(thp_ctx* ctx, double* x, double* y, double* z, double* rpole,
 int thp_last_error(void);
 /* bind deriv::dep(3,n), written by epolar1_ */
 int thp_bind_gradient(thp_ctx* ctx, double* dep);
+/* bind energi::ev and deriv::dev(3,n), written by ehal1_ (may be NULL) */
+int thp_bind_vdw(thp_ctx* ctx, double* ev, double* dev);
 /* bind energi::em and deriv::dem(3,n), written by empole1_ (may be NULL) */
 int thp_bind_mpole(thp_ctx* ctx, double* em, double* dem);
 /* bind pme::qgrid2in_2d(2,n1,n2,n3), read by fphi_uind_site_ */
@@ -361,6 +382,9 @@ void fphi_uind_site_(const int* isite, const int* impi, double* fdip_phi1, doubl
 void mlistcell_(void);
 /* nblist.f:1148 -- same list for the vdW slot name used by the workload */
 void vlistcell_(void);
+/* ehal1.f:17 -- van der Waals energy into the bound ev and its gradient
+ * into the bound dev (overwritten, as ehal1c zeroes it) */
+void ehal1_(void);
 /* empole1.f:10 -- permanent-multipole energy into the bound em and its
  * gradient into the bound dem (overwritten, as empole1c zeroes it) */
 void empole1_(void);

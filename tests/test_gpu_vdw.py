@@ -1,0 +1,87 @@
+"""Buffered 14-7 van der Waals energy and gradient (ehal1c) of the CUDA path
+against the CPU oracle (itself pinned by a textbook-form direct sum and finite
+differences in tests/test_oracle.py).  The pair terms run in FP64 in both
+precisions: energy within 1e-10 relative, gradient within 1e-9 of its largest
+component."""
+import ctypes as C
+import dataclasses
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib(thp):
+    from tinker_hp_b200 import lib as L
+    L.load()
+    return L
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("nw,edge", [(216, 20.0), (648, None)], ids=["216w", "648w"])
+def test_ehal1_matches_oracle(lib, thp, precision, nw, edge):
+    ws = thp.water.make_water_box(nw, cfg=0, edge=edge)
+    ev_ref, dev_ref = O.Oracle(ws).ehal1()
+    ctx = lib.Context(ws, precision=lib.FP64 if precision == "fp64" else lib.MIXED)
+    ev, dev = ctx.ehal1()
+    assert abs(ev - ev_ref) < 1e-10 * abs(ev_ref), (ev, ev_ref)
+    assert rel(dev, dev_ref) < 1e-9, rel(dev, dev_ref)
+
+
+def test_ehal1_large_box_and_moves(lib, thp):
+    # 32,400 atoms: cell reach over many cells; then whole-molecule
+    # displacements below and above the list buffer (the cell sort is kept,
+    # then rebuilt); molecules move rigidly so the reduced sites stay on
+    # their bonds
+    ws = thp.water.make_water_box(10800, cfg=1)
+    ctx = lib.Context(ws)
+    rng = np.random.default_rng(3)
+    for amp in (0.0, 0.1, 0.6):
+        shift = np.repeat(rng.normal(0.0, amp, (ws.nw, 3)), 3, axis=0)
+        w2 = ws.with_positions(ws.positions() + shift) if amp else ws
+        ctx.set_positions(w2.x, w2.y, w2.z)
+        ev, dev = ctx.ehal1()
+        ev_ref, dev_ref = O.Oracle(w2).ehal1()
+        assert abs(ev - ev_ref) < 1e-10 * abs(ev_ref), (amp, ev, ev_ref)
+        assert rel(dev, dev_ref) < 1e-9, (amp, rel(dev, dev_ref))
+
+
+def test_ehal1_fortran_dropin(lib, thp):
+    ws = thp.water.make_water_box(648, cfg=0)
+    ev_ref, dev_ref = O.Oracle(ws).ehal1()
+    L = lib.load()
+    ctx = lib.Context(ws)
+    dp = C.POINTER(C.c_double)
+    x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (ws.x, ws.y, ws.z))
+    rp = np.ascontiguousarray(O.rotpole(ws))
+    u1, u2 = np.zeros((ws.n, 3)), np.zeros((ws.n, 3))
+    assert L.thp_bind_state(ctx.h, x.ctypes.data_as(dp), y.ctypes.data_as(dp), z.ctypes.data_as(dp),
+                            rp.ctypes.data_as(dp), u1.ctypes.data_as(dp), u2.ctypes.data_as(dp), None, None, 0,
+                            None) == 0
+    ev = np.zeros(1)
+    dev = np.full((ws.n, 3), 5.0)  # overwritten, as ehal1c zeroes dev
+    assert L.thp_bind_vdw(ctx.h, ev.ctypes.data_as(dp), dev.ctypes.data_as(dp)) == 0
+    L.ehal1_()
+    assert L.thp_last_error() == 0
+    assert abs(ev[0] - ev_ref) < 1e-10 * abs(ev_ref)
+    assert rel(dev, dev_ref) < 1e-9
+
+
+def test_ehal1_refuses_a_reduction_beyond_the_reach(lib, thp):
+    # H sites reduced to half their bond (0.48 A shift): the pair search's
+    # cell reach assumes at most 0.3 A, so the call reports it
+    ws = thp.water.make_water_box(648, cfg=0)
+    v = dict(ws.vdw)
+    v["kred"] = np.where(v["cls"] == 0, 0.0, 0.5)
+    ctx = lib.Context(dataclasses.replace(ws, vdw=v))
+    with pytest.raises(lib.ThpError) as e:
+        ctx.ehal1()
+    assert e.value.status == lib.THP_E_INVALID

@@ -184,6 +184,10 @@ static int flags_status(Ctx& c) {
       c.last_msg = "non-finite coordinates";
       return THP_E_INVALID;
     }
+    if (f & DEV_VDW_REACH) {
+      c.last_msg = "a vdW reduction shift exceeds the 0.3 A the pair search allows";
+      return THP_E_INVALID;
+    }
     if (f & (DEV_LIST_OVERFLOW | DEV_PAIR_OVERFLOW)) {
       c.last_msg = "neighbor capacity exceeded";
       return THP_E_LIST_OVERFLOW;
@@ -381,7 +385,8 @@ static void pinned_give(Ctx& c) {
 void free_ctx(Ctx& c) {
   void* ptrs[] = {c.slab_cells, c.slab_atoms, c.slab_pairs, c.d_sp_off, c.d_sp_k, c.d_sp_ks, c.d_sp_s, c.d_sp_c,
                   c.d_cg, c.d_flags, c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad, c.d_sgrid, c.d_sscratch,
-                  c.d_alt, c.d_empart};
+                  c.d_alt, c.d_empart, c.d_vcls, c.d_vired, c.d_vkred, c.d_vtab, c.d_vred, c.d_vinfo,
+                  c.d_evpart};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   pme_free(c);
@@ -552,8 +557,10 @@ static int size_buffers(Ctx& c) {
     cudaFree(c.slab_atoms);
     c.slab_atoms = nullptr;
     // buffers made on first use are sized by n as well
-    free_all(&c.d_fphirec, &c.d_depfix, &c.d_trq, &c.d_frs, &c.d_grad, &c.d_empart);
-    c.d_em = nullptr;
+    free_all(&c.d_fphirec, &c.d_depfix, &c.d_trq, &c.d_frs, &c.d_grad, &c.d_empart, &c.d_vcls, &c.d_vired,
+             &c.d_vkred, &c.d_vred, &c.d_vinfo, &c.d_evpart);
+    c.d_em = c.d_ev = nullptr;
+    c.have_vdw = false;
     c.cap_n = 0;
     st = alloc_slab(c, &c.slab_atoms,
                     {item(&c.d_atom_cell, n), item(&c.d_scell, n), item(&c.d_perm, n), item(&c.d_iperm, n),
@@ -598,7 +605,8 @@ static int clear_system_state(thp_ctx* h) {
   h->pos_dirty = h->rpole_dirty = true;
   h->field_valid = h->guess_uploaded = h->solved_once = false;
   c.bx = c.by = c.bz = c.brpole = c.buind = c.buinp = c.bep = c.bdep = c.bqgrid = nullptr;
-  c.bem = c.bdem = nullptr;
+  c.bem = c.bdem = c.bev = c.bdev = nullptr;
+  c.have_vdw = false;
   c.mscale[0] = c.mscale[1] = 0.0;  // initprm.f:413-416
   c.mscale[2] = c.mscale[3] = 1.0;
   c.bnelst = c.belst = nullptr;
@@ -1005,6 +1013,73 @@ int thp_empole1(thp_ctx* h, double* em, double* dem) {
   if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "empole"))) return st;
   if (!std::isfinite(e)) return THP_E_NAN;
   if (em) *em = e;
+  return THP_OK;
+}
+
+int thp_set_vdw(thp_ctx* h, const int* cls, int nclass, const double* tables, const int* ired,
+                const double* kred, const double* vscale, double vdwcut, double vdwtaper, double ghal, double dhal) {
+  if (!h || !cls || !tables || !ired || !kred || !vscale || nclass <= 0 || nclass > 4096) return THP_E_INVALID;
+  Ctx& c = h->c;
+  const int n = c.n;
+  if (!(vdwcut > 0.0) || !(vdwtaper > 0.0) || !std::isfinite(ghal) || !std::isfinite(dhal)) return THP_E_INVALID;
+  for (int i = 0; i < n; ++i)
+    if (cls[i] < 0 || cls[i] >= nclass || ired[i] < 0 || ired[i] >= n || !std::isfinite(kred[i]))
+      return THP_E_INVALID;
+  const size_t nt = 4 * (size_t)nclass * nclass;
+  for (size_t q = 0; q < nt; ++q)
+    if (!std::isfinite(tables[q])) return THP_E_INVALID;
+  for (int j = 0; j < 4; ++j)
+    if (!std::isfinite(vscale[j])) return THP_E_INVALID;
+  if (2.0 * (vdwcut + c.cfg.lbuffer) > std::min(c.cfg.box[0], std::min(c.cfg.box[1], c.cfg.box[2]))) {
+    c.last_msg = "vdW cutoff + list buffer exceeds half the box";
+    return THP_E_BOX_TOO_SMALL;
+  }
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st;
+  auto once = [&](auto** p, size_t count, const char* what) {
+    return *p ? THP_OK : cuda_status(cudaMalloc((void**)p, sizeof(**p) * count), &c, what);
+  };
+  if ((st = once(&c.d_vcls, (size_t)n, "alloc vdw"))) return st;
+  if ((st = once(&c.d_vired, (size_t)n, "alloc vdw"))) return st;
+  if ((st = once(&c.d_vkred, (size_t)n, "alloc vdw"))) return st;
+  if (nt > c.cap_vtab) {
+    cudaFree(c.d_vtab);
+    c.d_vtab = nullptr;
+    c.cap_vtab = 0;
+    if ((st = once(&c.d_vtab, nt, "alloc vdw tables"))) return st;
+    c.cap_vtab = nt;
+  }
+  cudaMemcpyAsync(c.d_vcls, cls, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(c.d_vired, ired, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(c.d_vkred, kred, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(c.d_vtab, tables, sizeof(double) * nt, cudaMemcpyHostToDevice, c.stream);
+  if ((st = cuda_status(cudaStreamSynchronize(c.stream), &c, "upload vdw"))) return st;
+  c.vdw_nclass = nclass;
+  c.vdw_cut = vdwcut;
+  c.vdw_taper = vdwtaper;
+  c.vdw_ghal = ghal;
+  c.vdw_dhal = dhal;
+  for (int j = 0; j < 4; ++j) c.vdw_scale[j] = vscale[j];
+  c.have_vdw = true;
+  return THP_OK;
+}
+
+int thp_ehal1(thp_ctx* h, double* ev, double* dev) {
+  if (!h || (!ev && !dev)) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (!c.have_vdw || !c.have_conn) return THP_E_STATE;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st;
+  if ((st = ensure_list(h, false))) return st;
+  if (!c.d_grad && (st = cuda_status(cudaMalloc((void**)&c.d_grad, sizeof(double) * 3 * c.n), &c, "alloc gradient")))
+    return st;
+  if ((st = launch_ehal(c, c.d_grad))) return st;
+  double e = 0.0;
+  cudaMemcpyAsync(&e, c.d_ev, sizeof(double), cudaMemcpyDeviceToHost, c.stream);
+  if (dev) cudaMemcpyAsync(dev, c.d_grad, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost, c.stream);
+  if ((st = check_flags(h))) return st;  // synchronises the stream
+  if (!std::isfinite(e)) return THP_E_NAN;
+  if (ev) *ev = e;
   return THP_OK;
 }
 
@@ -1531,6 +1606,13 @@ int thp_bind_gradient(thp_ctx* h, double* dep) {
   return THP_OK;
 }
 
+int thp_bind_vdw(thp_ctx* h, double* ev, double* dev) {
+  if (!h) return THP_E_INVALID;
+  h->c.bev = ev;
+  h->c.bdev = dev;
+  return THP_OK;
+}
+
 int thp_bind_mpole(thp_ctx* h, double* em, double* dem) {
   if (!h) return THP_E_INVALID;
   h->c.bem = em;
@@ -1629,6 +1711,19 @@ void empole1_(void) {
   double em = 0.0;
   if (!st) st = thp_empole1(h, &em, h->c.bdem);
   if (!st && h->c.bem) *h->c.bem = em;
+  g_last_error = st;
+}
+
+void ehal1_(void) {
+  thp_ctx* h = g_current;
+  if (!h) {
+    g_last_error = THP_E_STATE;
+    return;
+  }
+  int st = sync_bound_inputs(h);
+  double ev = 0.0;
+  if (!st) st = thp_ehal1(h, &ev, h->c.bdev);
+  if (!st && h->c.bev) *h->c.bev = ev;
   g_last_error = st;
 }
 

@@ -33,7 +33,7 @@ struct CgScalars {
 constexpr int kCgChunk = 4;
 
 // device error flags (bit set)
-enum : int { DEV_LIST_OVERFLOW = 1, DEV_PAIR_OVERFLOW = 2, DEV_NAN = 4, DEV_BAD_INPUT = 8 };
+enum : int { DEV_LIST_OVERFLOW = 1, DEV_PAIR_OVERFLOW = 2, DEV_NAN = 4, DEV_BAD_INPUT = 8, DEV_VDW_REACH = 16 };
 
 // dipole solutions kept for the predictor (MOD_uprior.f: maxualt)
 constexpr int kMaxAlt = 7;
@@ -108,6 +108,22 @@ struct Ctx {
   int* d_sp_k = nullptr;
   double* d_sp_s = nullptr;       // (d, p, u) scale per entry
   int* d_sp_c = nullptr;          // 1-2..1-5 class per entry (4: none)
+  // van der Waals (thp_set_vdw): classes, reduction parents and factors in
+  // original order; pair tables [4][nclass][nclass] (Rmin, eps, 1-4 Rmin,
+  // 1-4 eps); sorted reduced sites and energy partials made on first use
+  bool have_vdw = false;
+  int vdw_nclass = 0;
+  double vdw_cut = 9.0, vdw_taper = 8.1, vdw_ghal = 0.12, vdw_dhal = 0.07;
+  double vdw_scale[4] = {0.0, 0.0, 1.0, 1.0};
+  size_t cap_vtab = 0;
+  int* d_vcls = nullptr;
+  int* d_vired = nullptr;
+  double* d_vkred = nullptr;
+  double* d_vtab = nullptr;
+  double4* d_vred = nullptr;
+  int2* d_vinfo = nullptr;
+  double* d_evpart = nullptr;
+  double* d_ev = nullptr;
   double* d_empart = nullptr;     // per-block partial sums of the permanent-multipole energy, then
   double* d_em = nullptr;         // their total (d_empart + blocks), made on first use
   double4* d_pos_built = nullptr; // positions at the last list build
@@ -195,6 +211,7 @@ struct Ctx {
   int bmaxelst = 0;
   double* bdep = nullptr;
   double *bem = nullptr, *bdem = nullptr;  // energi::em, deriv::dem(3,n), written by empole1_
+  double *bev = nullptr, *bdev = nullptr;  // energi::ev, deriv::dev(3,n), written by ehal1_
   double* bqgrid = nullptr;  // pme::qgrid2in_2d(2,n1,n2,n3), read by fphi_uind_site_
 
   // CUDA graph of one CG chunk (captured on first use)

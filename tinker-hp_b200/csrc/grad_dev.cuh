@@ -79,5 +79,35 @@ __global__ void k_dep_out(int n, const int* __restrict__ perm, const unsigned lo
   for (int j = 0; j < 3; ++j) out[3 * (size_t)o + j] = (double)(long long)dep[3 * (size_t)s + j] / kFix;
 }
 
+// per-block energy partial (warp shuffles, then the warps in order)
+template <int B>
+__device__ __forceinline__ void block_partial(double eacc, double* __restrict__ epart) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) eacc += __shfl_down_sync(0xffffffffu, eacc, o);
+  __shared__ double ws[B / 32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = eacc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < B / 32; ++w) t += ws[w];
+    epart[blockIdx.x] = t;
+  }
+}
+
+// one block: the partials in block order, strided per thread, then a tree
+__global__ void __launch_bounds__(256) k_sum_partials(int m, const double* __restrict__ part, double* __restrict__ out) {
+  __shared__ double s[256];
+  double t = 0.0;
+  for (int q = threadIdx.x; q < m; q += 256) t += part[q];
+  s[threadIdx.x] = t;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = s[0];
+}
+
 }  // namespace
 }  // namespace thp

@@ -43,6 +43,9 @@ int launch_gradient_out(Ctx& c, const unsigned long long* dep, double* d_out);  
 // permanent-multipole energy into d_em and dE/dx [n][3] (original order) into
 // d_out, for the current sorted positions, multipoles and list
 int launch_empole(Ctx& c, double* d_out);
+// buffered 14-7 van der Waals energy into d_ev and dE/dx [n][3] (original
+// order) into d_out, for the current sorted positions and cell sort
+int launch_ehal(Ctx& c, double* d_out);
 
 // sites.cu
 int launch_grid_uind_sites(Ctx& c, int nsites, const int* d_site, const double* d_fuind, const double* d_fuinp,

@@ -44,21 +44,6 @@ struct MScale {
   double v[5];  // m2scale..m5scale, then 1 for pairs outside the 1-2..1-5 lists
 };
 
-// per-block energy partial (warp shuffles, then the warps in order)
-__device__ __forceinline__ void block_partial(double eacc, double* __restrict__ epart) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) eacc += __shfl_down_sync(0xffffffffu, eacc, o);
-  __shared__ double ws[kBlock / 32];
-  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = eacc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-#pragma unroll
-    for (int w = 0; w < kBlock / 32; ++w) t += ws[w];
-    epart[blockIdx.x] = t;
-  }
-}
-
 // emreal1c pair terms (standard branch) seen from site i: adds half the pair
 // energy, the force on i and the torque on i.  m = (q, d, Qxx, Qxy, Qxz,
 // Qyy, Qyz, Qzz) of each site; scalek = 1 - mscale.
@@ -256,7 +241,7 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_EMPOLE_MINB : 4) k_empole_
     const int iz = frs[3 * i], ix = frs[3 * i + 1], axt = frs[3 * i + 2];
     if (axt == 1 || axt == 2) torque_dist(pos, i, iz, ix, axt, t3, dem);
   }
-  block_partial(eacc, epart);
+  block_partial<kBlock>(eacc, epart);
 }
 
 // Per site, in FP64: the 1-2..1-5 pairs within the cutoff (all are in the
@@ -348,21 +333,7 @@ __global__ void __launch_bounds__(kBlock) k_empole_site(
     const int iz = frs[3 * i], ix = frs[3 * i + 1], axt = frs[3 * i + 2];
     if (axt == 1 || axt == 2) torque_dist(pos, i, iz, ix, axt, trq, dem);
   }
-  block_partial(eacc, epart);
-}
-
-// one block: the partials in block order, strided per thread, then a tree
-__global__ void __launch_bounds__(256) k_sum_partials(int m, const double* __restrict__ part, double* __restrict__ out) {
-  __shared__ double s[256];
-  double t = 0.0;
-  for (int q = threadIdx.x; q < m; q += 256) t += part[q];
-  s[threadIdx.x] = t;
-  __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) *out = s[0];
+  block_partial<kBlock>(eacc, epart);
 }
 
 // buffers made on first use, sized by n (freed when a re-targeted context

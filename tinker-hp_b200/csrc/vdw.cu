@@ -1,0 +1,254 @@
+// vdw.cu -- buffered 14-7 van der Waals energy and gradient on the device
+// (ehal1c).
+//
+// Restates ehal1c (ehal1.f:69-482, standard branch: no soft core, groups or
+// short/long split) for the pairs of vlistcell (nblist.f:1148-1305):
+//   * reduced sites: each atom's vdW site moves towards its reduction parent,
+//     x_red = kred (x - x_parent) + x_parent (ehal1.f:193-205);
+//   * e = eps tau^7 Rmin^7 ((1+g) Rmin^7 / (r^7 + g Rmin^7) - 2) with
+//     tau = (1+d) / (r + d Rmin), the 1-2..1-5 vscale factors and the 1-4
+//     Rmin / eps, the 5th-degree taper between vdwtaper and vdwcut
+//     (switch.f:80-117);
+//   * the force on a reduced site split between the atom (kred) and its
+//     parent (1 - kred).
+// The pairs are found without a stored list: each site scans the cells of the
+// context's cell sort within reach of vdwcut (the sort is kept while no atom
+// has moved lbuffer/2, so the reach adds lbuffer and the largest allowed
+// reduction shift on both sides).  One thread per site evaluates each pair
+// from its own end (no atomics for the pair terms); the site's summed force
+// goes to the atom and its parent in 64-bit fixed point, and the energy
+// through per-block partials summed in block order.
+#include "grad_dev.cuh"
+#include "kernels.h"
+
+namespace thp {
+
+namespace {
+
+constexpr int kBlock = 128;
+// largest reduction shift |x_red - x| the cell reach allows (A); a larger one
+// is reported instead of silently missing pairs
+constexpr double kShiftMax = 0.3;
+
+struct VdwConst {
+  double off2, cut2, off, cut;
+  double c0, c1, c2, c3, c4, c5;  // taper coefficients (switch.f:80-117)
+  double ghal, dhal;
+  double vscale[5];               // v2..v5scale, then 1
+  int nclass;
+  int wx, wy, wz;                 // cell reach per axis
+};
+
+// sorted reduced sites: (x, y, z, kred) and (class, parent in sorted order)
+__global__ void k_vdw_sites(int n, const int* __restrict__ perm, const int* __restrict__ iperm,
+                            const double4* __restrict__ pos, const int* __restrict__ cls,
+                            const int* __restrict__ ired, const double* __restrict__ kred, double shift2max,
+                            double4* __restrict__ vred, int2* __restrict__ vinfo, int* __restrict__ flags) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int o = perm[s];
+  const int ps = iperm[ired[o]];
+  const double4 p = pos[s], q = pos[ps];
+  const double r = kred[o];
+  const double dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+  const double x = r * dx + q.x, y = r * dy + q.y, z = r * dz + q.z;
+  const double sx = x - p.x, sy = y - p.y, sz = z - p.z;
+  if (sx * sx + sy * sy + sz * sz > shift2max) atomicOr(flags, DEV_VDW_REACH);
+  vred[s] = make_double4(x, y, z, r);
+  vinfo[s] = make_int2(cls[o], ps);
+}
+
+// cells of one axis within +-w of cell c (all of them when 2w+1 >= nc)
+__device__ __forceinline__ int axis_count(int nc, int w) { return 2 * w + 1 >= nc ? nc : 2 * w + 1; }
+__device__ __forceinline__ int axis_cell(int c, int nc, int w, int q) {
+  return 2 * w + 1 >= nc ? q : ((c + q - w) % nc + nc) % nc;
+}
+
+__global__ void __launch_bounds__(kBlock) k_ehal(int n, Box box, VdwConst vc, const double4* __restrict__ vred,
+                                                 const int2* __restrict__ vinfo, const double* __restrict__ vtab,
+                                                 const int* __restrict__ perm, const int* __restrict__ sp_off,
+                                                 const int* __restrict__ sp_ks, const int* __restrict__ sp_c,
+                                                 const int* __restrict__ scell, const int* __restrict__ cell_start,
+                                                 const int* __restrict__ cell_count, int ncx, int ncy, int ncz,
+                                                 unsigned long long* __restrict__ dev, double* __restrict__ epart) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double eacc = 0.0;
+  if (i < n) {
+    const double4 ri = vred[i];
+    const int2 inf = vinfo[i];
+    const int it = inf.x;
+    const int io = perm[i];
+    const int s0 = sp_off[io], s1 = sp_off[io + 1];
+    const int nc2 = vc.nclass * vc.nclass;
+    const int c = scell[i];
+    const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
+    // x ranges of the window: [a0, a1] and the wrapped [b0, b1]
+    int a0, a1, b0 = 1, b1 = 0;
+    if (2 * vc.wx + 1 >= ncx) {
+      a0 = 0;
+      a1 = ncx - 1;
+    } else {
+      const int lo = cx - vc.wx, hi = cx + vc.wx;
+      if (lo < 0) {
+        a0 = 0;
+        a1 = hi;
+        b0 = lo + ncx;
+        b1 = ncx - 1;
+      } else if (hi >= ncx) {
+        a0 = lo;
+        a1 = ncx - 1;
+        b0 = 0;
+        b1 = hi - ncx;
+      } else {
+        a0 = lo;
+        a1 = hi;
+      }
+    }
+    const int my = axis_count(ncy, vc.wy), mz = axis_count(ncz, vc.wz);
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int qz = 0; qz < mz; ++qz) {
+      const int z = axis_cell(cz, ncz, vc.wz, qz);
+      for (int qy = 0; qy < my; ++qy) {
+        const int y = axis_cell(cy, ncy, vc.wy, qy);
+        const int rowbase = (z * ncy + y) * ncx;
+        for (int part = 0; part < 2; ++part) {
+          const int x0 = part ? b0 : a0, x1 = part ? b1 : a1;
+          if (x0 > x1) continue;
+          const int k0 = cell_start[rowbase + x0];
+          const int k1 = cell_start[rowbase + x1] + cell_count[rowbase + x1];
+#pragma unroll 1
+          for (int k = k0; k < k1; ++k) {
+            if (k == i) continue;
+            const double4 rk = vred[k];
+            double xr = ri.x - rk.x, yr = ri.y - rk.y, zr = ri.z - rk.z;
+            image3(box, xr, yr, zr);
+            const double rik2 = r2_exact(xr, yr, zr);
+            if (rik2 > vc.off2) continue;
+            const int kt = __ldg(&vinfo[k].x);
+            double vs = 1.0;
+            bool is14 = false;
+            for (int q = s0; q < s1; ++q)
+              if (__ldg(sp_ks + q) == k) {
+                const int cls = __ldg(sp_c + q);
+                vs = cls == 0 ? vc.vscale[0] : cls == 1 ? vc.vscale[1] : cls == 2 ? vc.vscale[2]
+                                                                      : cls == 3 ? vc.vscale[3] : 1.0;
+                is14 = cls == 2;
+                break;
+              }
+            const int t = kt * vc.nclass + it;
+            const double rv = __ldg(vtab + (is14 ? 2 * nc2 : 0) + t);
+            const double eps = __ldg(vtab + (is14 ? 3 * nc2 : nc2) + t) * vs;
+            const double rik = sqrt(rik2);
+            const double rv2 = rv * rv, rv7 = rv2 * rv2 * rv2 * rv;
+            const double rik6 = rik2 * rik2 * rik2;
+            const double rik7 = rik6 * rik;
+            const double rho = rik7 + vc.ghal * rv7;
+            const double tau = (vc.dhal + 1.0) / (rik + vc.dhal * rv);
+            const double tau2 = tau * tau, tau7 = tau2 * tau2 * tau2 * tau;
+            const double dtau = tau / (vc.dhal + 1.0);
+            const double q7 = rv7 / rho;
+            const double gtau = eps * tau7 * rik6 * (vc.ghal + 1.0) * q7 * q7;
+            double e = eps * tau7 * rv7 * ((vc.ghal + 1.0) * q7 - 2.0);
+            double de = -7.0 * (dtau * e + gtau);
+            if (rik2 > vc.cut2) {
+              const double rik3 = rik2 * rik, rik4 = rik2 * rik2, rik5 = rik2 * rik3;
+              const double taper = vc.c5 * rik5 + vc.c4 * rik4 + vc.c3 * rik3 + vc.c2 * rik2 + vc.c1 * rik + vc.c0;
+              const double dtaper =
+                  5.0 * vc.c5 * rik4 + 4.0 * vc.c4 * rik3 + 3.0 * vc.c3 * rik2 + 2.0 * vc.c2 * rik + vc.c1;
+              de = e * dtaper + de * taper;
+              e = e * taper;
+            }
+            eacc += 0.5 * e;
+            de = de / rik;
+            gx += de * xr;
+            gy += de * yr;
+            gz += de * zr;
+          }
+        }
+      }
+    }
+    // the site's force: to the atom (kred) and its parent (1 - kred)
+    const int iv = inf.y;
+    if (iv == i) {
+      fix_add(dev + 3 * i + 0, gx);
+      fix_add(dev + 3 * i + 1, gy);
+      fix_add(dev + 3 * i + 2, gz);
+    } else {
+      const double redi = ri.w, rediv = 1.0 - redi;
+      fix_add(dev + 3 * i + 0, gx * redi);
+      fix_add(dev + 3 * i + 1, gy * redi);
+      fix_add(dev + 3 * i + 2, gz * redi);
+      fix_add(dev + 3 * iv + 0, gx * rediv);
+      fix_add(dev + 3 * iv + 1, gy * rediv);
+      fix_add(dev + 3 * iv + 2, gz * rediv);
+    }
+  }
+  block_partial<kBlock>(eacc, epart);
+}
+
+template <typename P>
+int alloc_once(Ctx& c, P** p, size_t count, const char* what) {
+  if (*p) return THP_OK;
+  return cuda_status(cudaMalloc((void**)p, sizeof(P) * count), &c, what);
+}
+
+}  // namespace
+
+// van der Waals energy (into d_ev) and gradient (into d_out, original order)
+// for the sorted positions and the cell sort of the context.
+int launch_ehal(Ctx& c, double* d_out) {
+  int st;
+  if (!c.have_vdw) return THP_E_STATE;
+  const size_t n = c.n;
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  if ((st = alloc_once(c, &c.d_depfix, 3 * n, "alloc gradient"))) return st;
+  if ((st = alloc_once(c, &c.d_vred, n, "alloc vdw sites"))) return st;
+  if ((st = alloc_once(c, &c.d_vinfo, n, "alloc vdw sites"))) return st;
+  if ((st = alloc_once(c, &c.d_evpart, (size_t)nb + 1, "alloc vdw partials"))) return st;
+  c.d_ev = c.d_evpart + nb;
+  unsigned long long* dev = c.d_depfix;
+  if ((st = cuda_status(cudaMemsetAsync(dev, 0, sizeof(unsigned long long) * 3 * n, c.stream), &c, "zero dev")))
+    return st;
+  k_vdw_sites<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, c.d_iperm, c.d_pos, c.d_vcls, c.d_vired, c.d_vkred,
+                                           kShiftMax * kShiftMax, c.d_vred, c.d_vinfo, c.d_flags);
+  if ((st = cuda_status(cudaGetLastError(), &c, "vdw sites"))) return st;
+  VdwConst vc;
+  const double off = c.vdw_cut, cut = c.vdw_taper;
+  vc.off = off;
+  vc.cut = cut;
+  vc.off2 = off * off;
+  vc.cut2 = cut * cut;
+  vc.c0 = vc.c1 = vc.c2 = vc.c3 = vc.c4 = vc.c5 = 0.0;
+  if (cut < off) {  // switch.f:103-111
+    const double off2 = off * off, cut2 = cut * cut;
+    const double denom = pow(off - cut, 5.0);
+    vc.c0 = off * off2 * (off2 - 5.0 * off * cut + 10.0 * cut2) / denom;
+    vc.c1 = -30.0 * off2 * cut2 / denom;
+    vc.c2 = 30.0 * (off2 * cut + off * cut2) / denom;
+    vc.c3 = -10.0 * (off2 + 4.0 * off * cut + cut2) / denom;
+    vc.c4 = 15.0 * (off + cut) / denom;
+    vc.c5 = -6.0 / denom;
+  }
+  vc.ghal = c.vdw_ghal;
+  vc.dhal = c.vdw_dhal;
+  for (int j = 0; j < 4; ++j) vc.vscale[j] = c.vdw_scale[j];
+  vc.vscale[4] = 1.0;
+  vc.nclass = c.vdw_nclass;
+  // cells within reach: vdwcut, the list buffer (atoms move up to half of it
+  // on each side before a re-sort) and the reduction shift on each side
+  const double reach = off + c.cfg.lbuffer + 2.0 * kShiftMax;
+  int w[3];
+  for (int d = 0; d < 3; ++d) w[d] = (int)ceil(reach / (c.cfg.box[d] / c.nc[d]) - 1e-12);
+  vc.wx = w[0];
+  vc.wy = w[1];
+  vc.wz = w[2];
+  k_ehal<<<nb, kBlock, 0, c.stream>>>(c.n, c.box, vc, c.d_vred, c.d_vinfo, c.d_vtab, c.d_perm, c.d_sp_off,
+                                      c.d_sp_ks, c.d_sp_c, c.d_scell, c.d_cell_start, c.d_cell_count, c.nc[0],
+                                      c.nc[1], c.nc[2], dev, c.d_evpart);
+  if ((st = cuda_status(cudaGetLastError(), &c, "ehal"))) return st;
+  k_sum_partials<<<1, 256, 0, c.stream>>>(nb, c.d_evpart, c.d_ev);
+  if ((st = cuda_status(cudaGetLastError(), &c, "ehal energy"))) return st;
+  return launch_gradient_out(c, dev, d_out);
+}
+
+}  // namespace thp

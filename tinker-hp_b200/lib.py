@@ -129,6 +129,11 @@ def load():
         "thp_last_error": ([], C.c_int),
         "thp_bind_gradient": ([vp, _dp], C.c_int),
         "thp_set_mpole_scales": ([vp, _dp], C.c_int),
+        "thp_set_vdw": ([vp, _ip, C.c_int, _dp, _ip, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_double],
+                        C.c_int),
+        "thp_ehal1": ([vp, _dp, _dp], C.c_int),
+        "thp_bind_vdw": ([vp, _dp, _dp], C.c_int),
+        "ehal1_": ([], None),
         "thp_empole1": ([vp, _dp, _dp], C.c_int),
         "thp_bind_mpole": ([vp, _dp, _dp], C.c_int),
         "empole1_": ([], None),
@@ -263,6 +268,8 @@ class Context:
             idxs[q] = _p(idx, _ip)
         self._check(L.thp_set_connectivity(self.h, offs, idxs, _p(scales_array(ws))), "thp_set_connectivity")
         self._check(L.thp_set_mpole_scales(self.h, _p(_f64(ws.scales["m_scale"]))), "thp_set_mpole_scales")
+        if getattr(ws, "vdw", None) is not None and 2.0 * (ws.vdw["vdwcut"] + ws.lbuffer) <= min(ws.box):
+            self.set_vdw(ws.vdw)
         self.set_positions(ws.x, ws.y, ws.z)
         if rpole is not None:
             self.set_rpole(rpole)
@@ -336,6 +343,26 @@ class Context:
         ep = C.c_double()
         self._check(load().thp_get_gradient(self.h, _p(dep), C.byref(ep)), "thp_get_gradient")
         return ep.value, dep
+
+    def set_vdw(self, v):
+        """van der Waals description (water.water_vdw layout)."""
+        nc = int(v["nclass"])
+        tab = np.ascontiguousarray(np.stack([np.asarray(v[k], dtype=np.float64).reshape(nc, nc)
+                                             for k in ("radmin", "eps", "radmin4", "eps4")]))
+        keep = [_i32(v["cls"]), _i32(v["ired"]), _f64(v["kred"]), tab, _f64(v["v_scale"])]
+        self._keep += keep
+        self._check(load().thp_set_vdw(self.h, _p(keep[0], _ip), nc, _p(keep[3]), _p(keep[1], _ip), _p(keep[2]),
+                                       _p(keep[4]), float(v["vdwcut"]), float(v["vdwtaper"]), float(v["ghal"]),
+                                       float(v["dhal"])), "thp_set_vdw")
+
+    def ehal1(self, out=None):
+        """(Ev, dEv/dx [n,3] kcal/mol/A): buffered 14-7 van der Waals energy
+        and gradient at the current positions (ehal1c)."""
+        dev = np.zeros((self.n, 3)) if out is None else out
+        assert dev.shape == (self.n, 3) and dev.dtype == np.float64 and dev.flags["C_CONTIGUOUS"]
+        ev = C.c_double()
+        self._check(load().thp_ehal1(self.h, C.byref(ev), _p(dev)), "thp_ehal1")
+        return ev.value, dev
 
     def empole1(self, out=None):
         """(Em, dEm/dx [n,3] kcal/mol/A): permanent-multipole energy and
