@@ -359,6 +359,24 @@ def empole_run(lib, ws, reps=10):
     return out
 
 
+def ehal_run(lib, ws, reps=10):
+    """Buffered 14-7 van der Waals energy and gradient (ehal1c, FP64) of the
+    box: wall time per call through the C-ABI with the cell sort in place
+    (each call: reduced sites, the cell-window pair search and pair terms,
+    the gradient into a pinned host array)."""
+    import torch
+    ctx = lib.Context(ws, precision=lib.MIXED)
+    buf = torch.empty((ws.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    ctx.ehal1(out=buf)
+    ctx.ehal1(out=buf)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ev, _ = ctx.ehal1(out=buf)
+    dt = (time.perf_counter() - t0) / reps
+    ctx.close()
+    return {"ms_per_call": dt * 1e3, "ev_kcal_mol": ev, "atoms": ws.n, "cutoff_A": ws.vdw["vdwcut"]}
+
+
 def timed_solves(ctx, lib, steps, warmup, rebuild=True, guess=None):
     """Device-resident solves; per-step device time from CUDA events."""
     import torch
@@ -557,6 +575,7 @@ def main():
                                          "fp64_2_systems": served_repeats(lib, [ws, ws2], lib.FP64, count=24)}
         extras["md_config1"] = {"previous": md_run(lib, thp), "aspc": md_run(lib, thp, predictor="ASPC")}
         extras["empole1"] = empole_run(lib, ws)
+        extras["ehal1"] = ehal_run(lib, ws)
         if fp64 is not None:
             best = max(b2["solves_per_s"], b4["solves_per_s"])
             plain64 = world * len(lat64) / (t64 / 1000.0)

@@ -31,6 +31,13 @@ def _same_system(a, b, pos_tol=1e-10):
     for k in b.scales:
         assert tuple(a.scales[k]) == tuple(b.scales[k]), k
     assert a.nfft == b.nfft and a.bsorder == b.bsorder
+    if b.vdw is not None:
+        for k in ("cls", "ired"):
+            np.testing.assert_array_equal(a.vdw[k], b.vdw[k], err_msg=k)
+        for k in ("kred", "radmin", "eps", "radmin4", "eps4"):
+            np.testing.assert_allclose(a.vdw[k], b.vdw[k], rtol=1e-15, atol=0, err_msg=k)
+        for k in ("nclass", "v_scale", "vdwcut", "vdwtaper", "ghal", "dhal"):
+            assert np.allclose(a.vdw[k], b.vdw[k], rtol=1e-15, atol=0), k
     assert a.ewaldcut == b.ewaldcut and a.lbuffer == b.lbuffer and a.aewald == b.aewald
 
 
@@ -69,7 +76,7 @@ def test_box_line_renumbering_and_defaults(tio, thp, tmp_path):
         lines.append(f"{i + 101} {'O' if t == 1 else 'H'} {ws.x[i]:.12f} {ws.y[i]:.12f} {ws.z[i]:.12f} {t} {bonded}")
     (tmp_path / "w.xyz").write_text("\n".join(lines) + "\n")
     back = tio.load_system(str(tmp_path / "w.xyz"))
-    ref = dataclasses.replace(ws, lbuffer=2.0, nfft=(20, 20, 20))  # 1.2 points per A over 16 A -> 20
+    ref = dataclasses.replace(ws, lbuffer=2.0, nfft=(20, 20, 20), vdw=None)  # 1.2 points per A over 16 A -> 20
     _same_system(back, ref)
 
 
@@ -145,3 +152,12 @@ def test_pass_order_beats_entry_order(tio, thp, tmp_path):
     back = tio.load_system(path)
     np.testing.assert_array_equal(back.axt, ws.axt)
     np.testing.assert_allclose(back.pole, ws.pole, rtol=1e-14, atol=1e-16)
+
+
+def test_loaded_box_vdw_matches_the_built_one(tio, thp, tmp_path):
+    ws = thp.water.make_water_box(216, cfg=0, edge=20.0)
+    back = tio.load_system(tio.save_system(str(tmp_path), "v", ws))
+    ea, da = O.Oracle(ws).ehal1()
+    eb, db = O.Oracle(back).ehal1()
+    assert abs(ea - eb) < 1e-10 * abs(ea)
+    np.testing.assert_allclose(db, da, rtol=0, atol=1e-9 * np.abs(da).max())

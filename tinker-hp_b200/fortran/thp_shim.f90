@@ -1,15 +1,16 @@
 ! thp_shim.f90 -- ISO_C_BINDING layer between Tinker-HP (v1.2 module state)
 ! and libthp.so.  Replaces the calls newinduce_pme2 (epolar.f:108,
 ! epolar1.f:145), mlistcell (nblist.f:109), epolar1 (gradient.f:165) and
-! empole1 (gradient.f, the permanent-multipole term) by thp_newinduce_pme2,
-! thp_mlistcell, thp_epolar1 and thp_empole1, and offers the batched per-site
-! PME routines.  Not compiled in this repository's image (no Fortran
+! empole1 and ehal1 (gradient.f, the permanent-multipole and vdW terms) by
+! thp_newinduce_pme2, thp_mlistcell, thp_epolar1, thp_empole1 and thp_ehal1,
+! and offers the batched per-site PME routines.  Not compiled in this repository's image (no Fortran
 ! compiler); it follows the C declarations of include/thp.h.
 module thp_shim
   use iso_c_binding
   implicit none
   private
-  public :: thp_init, thp_newinduce_pme2, thp_mlistcell, thp_epolar, thp_epolar1, thp_empole1, thp_finalize
+  public :: thp_init, thp_newinduce_pme2, thp_mlistcell, thp_epolar, thp_epolar1, thp_empole1, thp_ehal1, &
+            thp_finalize
   public :: thp_grid_uind_sites, thp_fphi_uind_sites
 
   type, bind(C) :: thp_config
@@ -75,6 +76,19 @@ module thp_shim
     end function
     subroutine c_empole1() bind(C, name="empole1_")
     end subroutine
+    integer(c_int) function c_set_vdw(h, cls, nclass, tables, ired, kred, vscale, vdwcut, vdwtaper, &
+        ghal, dhal) bind(C, name="thp_set_vdw")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h, cls, tables, ired, kred, vscale
+      integer(c_int), value :: nclass
+      real(c_double), value :: vdwcut, vdwtaper, ghal, dhal
+    end function
+    integer(c_int) function c_bind_vdw(h, ev, dev) bind(C, name="thp_bind_vdw")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, ev, dev
+    end function
+    subroutine c_ehal1() bind(C, name="ehal1_")
+    end subroutine
     subroutine c_grid_uind_sites(ns, isite, fuind, fuinp, qgrid) bind(C, name="grid_uind_sites_")
       import :: c_int, c_double
       integer(c_int), intent(in) :: ns, isite(*)
@@ -106,6 +120,7 @@ contains
                       p4iscale, p5iscale, d1scale, d2scale, d3scale, d4scale, u1scale, u2scale, &
                       u3scale, u4scale
     use mplpot, only: m2scale, m3scale, m4scale, m5scale
+    use potent, only: use_vdw
     logical, intent(in) :: mixed
     type(thp_config), target :: cfg
     real(c_double), target :: scales(16), mscales(4)
@@ -136,6 +151,36 @@ contains
     st = c_set_mpole_scales(ctx, c_loc(mscales))
     if (st /= 0) call fatal
     call set_frames()
+    if (use_vdw) call set_vdw()
+  end subroutine
+
+  ! vdW description from kvdw (jvdw, radmin, epsilon, radmin4, epsilon4,
+  ! ired, kred), vdwpot (v2scale..v5scale, ghal, dhal) and cutoff (vdwcut,
+  ! vdwtaper, already absolute after cutoffs.f:241)
+  subroutine set_vdw()
+    use atoms, only: n
+    use vdw, only: jvdw, radmin, epsilon, radmin4, epsilon4, ired, kred
+    use vdwpot, only: v2scale, v3scale, v4scale, v5scale, ghal, dhal
+    use cutoff, only: vdwcut, vdwtaper
+    integer(c_int), allocatable, target :: cl(:), ir(:)
+    real(c_double), allocatable, target :: tab(:,:,:), kr(:)
+    real(c_double), target :: vs(4)
+    integer :: i, nc, st
+    nc = size(radmin, 1)
+    allocate(cl(n), ir(n), kr(n), tab(nc, nc, 4))
+    do i = 1, n
+      cl(i) = jvdw(i) - 1
+      ir(i) = ired(i) - 1
+      kr(i) = kred(i)
+    end do
+    tab(:,:,1) = radmin
+    tab(:,:,2) = epsilon
+    tab(:,:,3) = radmin4
+    tab(:,:,4) = epsilon4
+    vs = [v2scale, v3scale, v4scale, v5scale]
+    st = c_set_vdw(ctx, c_loc(cl), int(nc, c_int), c_loc(tab), c_loc(ir), c_loc(kr), c_loc(vs), &
+                   vdwcut, vdwtaper, ghal, dhal)
+    if (st /= 0) call fatal
   end subroutine
 
   ! frame atoms for the torques (and rotpole on the device): mpole::pole,
@@ -261,6 +306,20 @@ contains
     st = c_bind_mpole(ctx, c_loc(em), c_loc(dem))
     if (st /= 0) call fatal
     call c_empole1()
+    if (c_last_error() /= 0) call fatal
+  end subroutine
+
+  ! ehal1 (ehal1.f:17): energy into ev, gradient into deriv::dev; the vdW
+  ! description comes from thp_set_vdw (classes, combined pair tables and
+  ! reduction from the kvdw module), set once after kvdw
+  subroutine thp_ehal1
+    use deriv, only: dev
+    use energi, only: ev
+    integer :: st
+    call bind_all()
+    st = c_bind_vdw(ctx, c_loc(ev), c_loc(dev))
+    if (st /= 0) call fatal
+    call c_ehal1()
     if (c_last_error() /= 0) call fatal
   end subroutine
 

@@ -24,7 +24,10 @@ Each step restates the reference routine that does it at start-up:
     bohr^2/3;
   * kpolar.f:225-300 and polargrp (kpolar.f:598-800) -- polarizability,
     Thole factor, pdamp = polarity^(1/6) and the polarization groups
-    ip11..ip14.
+    ip11..ip14;
+  * readprm.f:199-258 (`atom`, `vdw`, `vdw14`) and kvdw.f:318-503 -- the
+    van der Waals classes, pair tables by the radius/epsilon rules and the
+    reduction parents and factors.
 
 The device path rotates Z-then-X and Bisector frames (the AMOEBA water
 frames); a system with other frame types is refused with a message naming the
@@ -253,6 +256,10 @@ class ParamSet:
         "pi_scale": [0.0, 0.0, 0.5, 1.0], "d_scale": [0.0, 1.0, 1.0, 1.0],
         "u_scale": [1.0, 1.0, 1.0, 1.0]})
     keywords: dict = dataclasses.field(default_factory=dict)        # KEYWORD -> last value text
+    vdw: dict = dataclasses.field(default_factory=dict)             # class -> (Rmin, eps, reduction)
+    vdw14: dict = dataclasses.field(default_factory=dict)           # class -> (Rmin, eps)
+    atom_class: dict = dataclasses.field(default_factory=dict)      # type -> class (`atom` records)
+    v_scale: list = dataclasses.field(default_factory=lambda: [0.0, 0.0, 1.0, 1.0])  # initprm.f:385-388
 
 
 _SCALE_KEYS = {}
@@ -263,6 +270,7 @@ for _b, _s in enumerate(("12", "13", "14", "15")):
 for _b, _s in enumerate(("11", "12", "13", "14")):
     _SCALE_KEYS[f"DIRECT-{_s}-SCALE"] = ("d_scale", _b)
     _SCALE_KEYS[f"MUTUAL-{_s}-SCALE"] = ("u_scale", _b)
+_VDW_SCALE_KEYS = {f"VDW-{s_}-SCALE": b for b, s_ in enumerate(("12", "13", "14", "15"))}
 
 
 def _read_records(path, ps, from_key):
@@ -303,6 +311,31 @@ def _read_records(path, ps, from_key):
                     rest_tok = rest_tok[1:]
             grp = [int(v) for v in rest_tok if int(v) != 0]
             ps.polarize[t] = (pol, thl, thd, grp)
+        elif kw == "VDW":  # readprm.f:233-245
+            tok = rest.split()
+            try:
+                cl = int(tok[0])
+                vals = [float(v) for v in tok[1:4]] + [0.0] * (4 - len(tok[1:4]) - 1)
+            except (ValueError, IndexError) as e:
+                raise TinkerFormatError(f"{where}: bad vdw record {rest!r}") from e
+            ps.vdw[cl] = (vals[0], vals[1], vals[2] if len(vals) > 2 else 0.0)
+        elif kw == "VDW14":  # readprm.f:249-258
+            tok = rest.split()
+            try:
+                ps.vdw14[int(tok[0])] = (float(tok[1]), float(tok[2]))
+            except (ValueError, IndexError) as e:
+                raise TinkerFormatError(f"{where}: bad vdw14 record {rest!r}") from e
+        elif kw == "ATOM":  # readprm.f:199: type, class, symbol, ...
+            tok = rest.split()
+            try:
+                ps.atom_class[int(tok[0])] = int(tok[1])
+            except (ValueError, IndexError) as e:
+                raise TinkerFormatError(f"{where}: bad atom record {rest!r}") from e
+        elif kw in _VDW_SCALE_KEYS:
+            try:
+                ps.v_scale[_VDW_SCALE_KEYS[kw]] = float(rest.split()[0])
+            except (ValueError, IndexError) as e:
+                raise TinkerFormatError(f"{where}: bad value for {kw}") from e
         elif kw in _SCALE_KEYS:
             name, b = _SCALE_KEYS[kw]
             try:
@@ -348,8 +381,17 @@ def write_water_params(path):
     for b, tag in enumerate(("11", "12", "13", "14")):
         lines.append(f"direct-{tag}-scale  {s['d_scale'][b]:.4f}")
         lines.append(f"mutual-{tag}-scale  {s['u_scale'][b]:.4f}")
+    for b, tag in enumerate(("12", "13", "14", "15")):
+        lines.append(f"vdw-{tag}-scale     {P.VDW_SCALE[b]:.4f}")
+    lines += [f"vdwtype           BUFFERED-14-7", f"radiusrule        {P.VDW_RULES['radius']}",
+              f"radiustype        {P.VDW_RULES['radiustype']}", f"radiussize        {P.VDW_RULES['radiussize']}",
+              f"epsilonrule       {P.VDW_RULES['epsilon']}"]
     lines += ["", 'atom          1    1    O     "AMOEBA Water O"    8   15.995    2',
               'atom          2    2    H     "AMOEBA Water H"    1    1.008    1', ""]
+    ro, eo, _ = P.WATER_VDW["O"]
+    rh, eh, fh = P.WATER_VDW["H"]
+    lines += [f"vdw           1               {ro:.4f}     {eo:.4f}",
+              f"vdw           2               {rh:.4f}     {eh:.4f}      {fh:.3f}", ""]
     for t, kind, frame in ((1, "O", "-2   -2"), (2, "H", " 1    2")):
         m = P.WATER_MULTIPOLES[kind]
         d = m["dipole"]
@@ -374,6 +416,8 @@ def write_key(path, ws, prm_name, poleps=None):
              f"c-axis            {ws.box[2]:.12f}",
              "ewald", f"ewald-cutoff      {ws.ewaldcut}", f"ewald-alpha       {ws.aewald!r}",
              f"list-buffer       {ws.lbuffer}",
+             *([f"vdw-cutoff        {ws.vdw['vdwcut']}",
+                f"vdw-taper         {ws.vdw['vdwtaper']}"] if getattr(ws, "vdw", None) else []),
              f"pme-grid          {ws.nfft[0]} {ws.nfft[1]} {ws.nfft[2]}", f"pme-order         {ws.bsorder}",
              "polarization      mutual"]
     if poleps is not None:
@@ -609,6 +653,43 @@ def _kw_float(kw, name, default):
         raise TinkerFormatError(f"bad value for {name}: {kw[name]!r}") from e
 
 
+def _vdw_description(xf, ps, kw):
+    """van der Waals description of the atoms (kvdw.f): classes from the
+    `atom` records, per-class Rmin/eps/reduction, pair tables by the rules
+    keywords, reduction parents (kvdw.f:490-503), vdw-1x-scale, vdw-cutoff
+    and vdw-taper (cutoffs.f:74,143,178,241).  None without vdw records."""
+    if not ps.vdw:
+        return None
+    if kw.get("VDWTYPE", "BUFFERED-14-7").split()[0].upper() != "BUFFERED-14-7":
+        raise TinkerFormatError(f"vdwtype {kw['VDWTYPE']!r}: only BUFFERED-14-7 (AMOEBA) is supported")
+    n = xf.n
+    acls = [ps.atom_class.get(int(t), int(t)) for t in xf.types]
+    used = sorted(set(acls))
+    index = {c: q for q, c in enumerate(used)}
+    for c in used:
+        if c not in ps.vdw:
+            raise TinkerFormatError(f"no vdw parameters for class {c}")
+    rad = [ps.vdw[c][0] for c in used]
+    eps = [ps.vdw[c][1] for c in used]
+    rad4 = [ps.vdw14.get(c, (0.0, 0.0))[0] for c in used]
+    eps4 = [ps.vdw14.get(c, (0.0, 0.0))[1] for c in used]
+    rules = {"radius": kw.get("RADIUSRULE", "ARITHMETIC").split()[0].upper(),
+             "epsilon": kw.get("EPSILONRULE", "GEOMETRIC").split()[0].upper(),
+             "radiustype": kw.get("RADIUSTYPE", "R-MIN").split()[0].upper(),
+             "radiussize": kw.get("RADIUSSIZE", "RADIUS").split()[0].upper()}
+    radmin, epsm, radmin4, eps4t = P.vdw_pair_tables(rad, eps, rad4, eps4, rules)
+    cls = np.array([index[c] for c in acls], np.int32)
+    kred = np.array([ps.vdw[c][2] for c in acls], np.float64)
+    ired = np.array([xf.i12[i][0] if (len(xf.i12[i]) == 1 and kred[i] != 0.0) else i for i in range(n)], np.int32)
+    vdwcut = _kw_float(kw, "VDW-CUTOFF", P.VDW_CUTOFF_DEFAULT)
+    taper = _kw_float(kw, "VDW-TAPER", P.VDW_TAPER)
+    if taper < 1.0:
+        taper = taper * vdwcut
+    return {"nclass": len(used), "cls": cls, "ired": ired, "kred": kred, "radmin": np.array(radmin),
+            "eps": np.array(epsm), "radmin4": np.array(radmin4), "eps4": np.array(eps4t),
+            "v_scale": tuple(ps.v_scale), "vdwcut": vdwcut, "vdwtaper": taper, "ghal": P.GHAL, "dhal": P.DHAL}
+
+
 def load_system(xyz_path, key_path=None, prm_path=None):
     """A system description (water.WaterSystem fields) from Tinker input
     files.  key_path defaults to the .key beside the .xyz; the parameter file
@@ -672,11 +753,12 @@ def load_system(xyz_path, key_path=None, prm_path=None):
             "ip11": _csr(ip11), "ip12": _csr(ip12), "ip13": _csr(ip13), "ip14": _csr(ip14)}
     mol, nmol = _molecules(xf.i12)
     scales = {k: tuple(v) for k, v in ps.scales.items()}
+    vdw = _vdw_description(xf, ps, kw)
     return W.WaterSystem(n=n, nw=nmol, box=tuple(box), x=np.ascontiguousarray(xf.xyz[:, 0]),
                          y=np.ascontiguousarray(xf.xyz[:, 1]), z=np.ascontiguousarray(xf.xyz[:, 2]),
                          pole=pole, zaxis=zaxis.astype(np.int32), xaxis=xaxis.astype(np.int32), axt=axt,
                          polarity=polarity, thole=thole, pdamp=pdamp, mol=mol, conn=conn, aewald=aewald,
-                         ewaldcut=ewaldcut, lbuffer=lbuffer, nfft=nfft, bsorder=bsorder, scales=scales)
+                         ewaldcut=ewaldcut, lbuffer=lbuffer, nfft=nfft, bsorder=bsorder, scales=scales, vdw=vdw)
 
 
 def save_system(directory, name, ws, poleps=None):
