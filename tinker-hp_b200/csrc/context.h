@@ -75,6 +75,7 @@ struct Ctx {
 
   // cell grid of the list build
   int nc[3] = {1, 1, 1};
+  unsigned sort_epoch = 0;  // counts re-sorts of the atoms
   int ncell = 1;
   int* d_cell_count = nullptr;
   int* d_cell_start = nullptr;
@@ -122,6 +123,15 @@ struct Ctx {
   double* d_vtab = nullptr;
   double4* d_vred = nullptr;
   int2* d_vinfo = nullptr;
+  // vdW pair list (vlistcell): full list within vdwcut + lbuffer of the
+  // reduced sites, slot-major [s*npad + i], rebuilt after a re-sort or when an
+  // atom has moved lbuffer/2 since the positions it was built from
+  int maxvnb = 0;
+  int* d_vnb = nullptr;
+  int* d_vnnb = nullptr;
+  double4* d_vpos_built = nullptr;
+  bool have_vlist = false;
+  unsigned vlist_epoch = 0;
   double* d_evpart = nullptr;
   double* d_ev = nullptr;
   double* d_empart = nullptr;     // per-block partial sums of the permanent-multipole energy, then

@@ -13,6 +13,7 @@ int launch_build_list_on(Ctx& c, cudaStream_t s);          // full list within e
 int launch_export_list(Ctx& c, int maxelst, int* d_nelst, int* d_elst);
 int launch_rotpole(Ctx& c);             // local-frame multipoles -> d_rpole_orig
 int launch_max_displacement(Ctx& c, double* h_out);
+int launch_max_displacement_from(Ctx& c, const double4* ref, double* h_out);  // largest move since ref (sorted)
 
 // realspace.cu
 int launch_efld0_coef(Ctx& c, bool with_field);

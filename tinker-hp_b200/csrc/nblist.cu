@@ -415,6 +415,7 @@ __global__ void k_max_disp(int n, const double4* __restrict__ pos, const double4
 
 int launch_sort_atoms(Ctx& c) {
   const int n = c.n;
+  ++c.sort_epoch;  // sorted numbering changes: lists in it are stale
   const int nb = (n + kBlock - 1) / kBlock;
   cudaStream_t s = c.stream;
   // the last dipoles (warm start) follow their atoms into the new order; the
@@ -506,10 +507,12 @@ int launch_rotpole(Ctx& c) {
   return cuda_status(cudaGetLastError(), &c, "rotpole");
 }
 
-int launch_max_displacement(Ctx& c, double* h_out) {
+int launch_max_displacement(Ctx& c, double* h_out) { return launch_max_displacement_from(c, c.d_pos_built, h_out); }
+
+int launch_max_displacement_from(Ctx& c, const double4* ref, double* h_out) {
   unsigned long long* d = reinterpret_cast<unsigned long long*>(c.d_partials);
   cudaMemsetAsync(d, 0, sizeof(unsigned long long), c.stream);
-  k_max_disp<<<(c.n + kBlock - 1) / kBlock, kBlock, 0, c.stream>>>(c.n, c.d_pos, c.d_pos_built, c.box, d);
+  k_max_disp<<<(c.n + kBlock - 1) / kBlock, kBlock, 0, c.stream>>>(c.n, c.d_pos, ref, c.box, d);
   unsigned long long v = 0;
   cudaMemcpyAsync(&v, d, sizeof(v), cudaMemcpyDeviceToHost, c.stream);
   int st = cuda_status(cudaStreamSynchronize(c.stream), &c, "max displacement");

@@ -11,13 +11,17 @@
 //     (switch.f:80-117);
 //   * the force on a reduced site split between the atom (kred) and its
 //     parent (1 - kred).
-// The pairs are found without a stored list: each site scans the cells of the
-// context's cell sort within reach of vdwcut (the sort is kept while no atom
-// has moved lbuffer/2, so the reach adds lbuffer and the largest allowed
-// reduction shift on both sides).  One thread per site evaluates each pair
-// from its own end (no atomics for the pair terms); the site's summed force
-// goes to the atom and its parent in 64-bit fixed point, and the energy
-// through per-block partials summed in block order.
+// The pairs come from a vdW list in the context's sorted numbering (the
+// reference's vlistcell): every site within vdwcut + lbuffer of the reduced
+// site, found by scanning the cells of the cell sort within reach (vdwcut,
+// lbuffer for the atoms' drift since the sort, and the largest allowed
+// reduction shift on both sides).  The list is rebuilt after a re-sort or
+// once an atom has moved lbuffer/2 since the positions it was built from, as
+// the reference's list update does.  One thread per site evaluates each pair
+// from its own end (no atomics for the pair terms): its list is dense in
+// interacting pairs, so the lanes of a warp stay together through the pair
+// arithmetic.  The site's summed force goes to the atom and its parent in
+// 64-bit fixed point, the energy through per-block partials summed in order.
 #include "grad_dev.cuh"
 #include "kernels.h"
 
@@ -29,6 +33,9 @@ constexpr int kBlock = 128;
 // largest reduction shift |x_red - x| the cell reach allows (A); a larger one
 // is reported instead of silently missing pairs
 constexpr double kShiftMax = 0.3;
+// per-site capacity of the vdW list without a max_neighbors setting (a 9.5 A
+// sphere of liquid water holds about 370 sites)
+constexpr int kDefaultMaxVnb = 640;
 
 struct VdwConst {
   double off2, cut2, off, cut;
@@ -36,7 +43,6 @@ struct VdwConst {
   double ghal, dhal;
   double vscale[5];               // v2..v5scale, then 1
   int nclass;
-  int wx, wy, wz;                 // cell reach per axis
 };
 
 // sorted reduced sites: (x, y, z, kred) and (class, parent in sorted order)
@@ -64,13 +70,78 @@ __device__ __forceinline__ int axis_cell(int c, int nc, int w, int q) {
   return 2 * w + 1 >= nc ? q : ((c + q - w) % nc + nc) % nc;
 }
 
-__global__ void __launch_bounds__(kBlock) k_ehal(int n, Box box, VdwConst vc, const double4* __restrict__ vred,
-                                                 const int2* __restrict__ vinfo, const double* __restrict__ vtab,
-                                                 const int* __restrict__ perm, const int* __restrict__ sp_off,
-                                                 const int* __restrict__ sp_ks, const int* __restrict__ sp_c,
-                                                 const int* __restrict__ scell, const int* __restrict__ cell_start,
-                                                 const int* __restrict__ cell_count, int ncx, int ncy, int ncz,
-                                                 unsigned long long* __restrict__ dev, double* __restrict__ epart) {
+// vlistcell (nblist.f:1148-1305) over the cell sort: every other site whose
+// reduced minimum-image distance is within vbuf (both directions)
+__global__ void __launch_bounds__(kBlock) k_vdw_list(int n, int npad, Box box, double vbuf2, int wx, int wy, int wz,
+                                                     const double4* __restrict__ vred, const int* __restrict__ scell,
+                                                     const int* __restrict__ cell_start,
+                                                     const int* __restrict__ cell_count, int ncx, int ncy, int ncz,
+                                                     int maxvnb, int* __restrict__ vnnb, int* __restrict__ vnb,
+                                                     int* __restrict__ flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 ri = vred[i];
+  const int c = scell[i];
+  const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
+  // x ranges of the window: [a0, a1] and the wrapped [b0, b1]
+  int a0, a1, b0 = 1, b1 = 0;
+  if (2 * wx + 1 >= ncx) {
+    a0 = 0;
+    a1 = ncx - 1;
+  } else {
+    const int lo = cx - wx, hi = cx + wx;
+    if (lo < 0) {
+      a0 = 0;
+      a1 = hi;
+      b0 = lo + ncx;
+      b1 = ncx - 1;
+    } else if (hi >= ncx) {
+      a0 = lo;
+      a1 = ncx - 1;
+      b0 = 0;
+      b1 = hi - ncx;
+    } else {
+      a0 = lo;
+      a1 = hi;
+    }
+  }
+  const int my = axis_count(ncy, wy), mz = axis_count(ncz, wz);
+  int cnt = 0;
+  for (int qz = 0; qz < mz; ++qz) {
+    const int z = axis_cell(cz, ncz, wz, qz);
+    for (int qy = 0; qy < my; ++qy) {
+      const int y = axis_cell(cy, ncy, wy, qy);
+      const int rowbase = (z * ncy + y) * ncx;
+      for (int part = 0; part < 2; ++part) {
+        const int x0 = part ? b0 : a0, x1 = part ? b1 : a1;
+        if (x0 > x1) continue;
+        const int k0 = cell_start[rowbase + x0];
+        const int k1 = cell_start[rowbase + x1] + cell_count[rowbase + x1];
+#pragma unroll 4
+        for (int k = k0; k < k1; ++k) {
+          if (k == i) continue;
+          const double4 rk = vred[k];
+          double xr = ri.x - rk.x, yr = ri.y - rk.y, zr = ri.z - rk.z;
+          image3(box, xr, yr, zr);
+          if (r2_exact(xr, yr, zr) <= vbuf2) {
+            if (cnt < maxvnb) vnb[(size_t)cnt * npad + i] = k;
+            ++cnt;
+          }
+        }
+      }
+    }
+  }
+  vnnb[i] = min(cnt, maxvnb);
+  if (cnt > maxvnb) atomicOr(flags, DEV_LIST_OVERFLOW);
+}
+
+__global__ void __launch_bounds__(kBlock) k_ehal(int n, int npad, Box box, VdwConst vc,
+                                                 const double4* __restrict__ vred, const int2* __restrict__ vinfo,
+                                                 const double* __restrict__ vtab, const int* __restrict__ perm,
+                                                 const int* __restrict__ sp_off, const int* __restrict__ sp_ks,
+                                                 const int* __restrict__ sp_c, const int* __restrict__ vnnb,
+                                                 const int* __restrict__ vnb, unsigned long long* __restrict__ dev,
+                                                 double* __restrict__ epart) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double eacc = 0.0;
   if (i < n) {
@@ -80,92 +151,56 @@ __global__ void __launch_bounds__(kBlock) k_ehal(int n, Box box, VdwConst vc, co
     const int io = perm[i];
     const int s0 = sp_off[io], s1 = sp_off[io + 1];
     const int nc2 = vc.nclass * vc.nclass;
-    const int c = scell[i];
-    const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
-    // x ranges of the window: [a0, a1] and the wrapped [b0, b1]
-    int a0, a1, b0 = 1, b1 = 0;
-    if (2 * vc.wx + 1 >= ncx) {
-      a0 = 0;
-      a1 = ncx - 1;
-    } else {
-      const int lo = cx - vc.wx, hi = cx + vc.wx;
-      if (lo < 0) {
-        a0 = 0;
-        a1 = hi;
-        b0 = lo + ncx;
-        b1 = ncx - 1;
-      } else if (hi >= ncx) {
-        a0 = lo;
-        a1 = ncx - 1;
-        b0 = 0;
-        b1 = hi - ncx;
-      } else {
-        a0 = lo;
-        a1 = hi;
-      }
-    }
-    const int my = axis_count(ncy, vc.wy), mz = axis_count(ncz, vc.wz);
     double gx = 0.0, gy = 0.0, gz = 0.0;
-    for (int qz = 0; qz < mz; ++qz) {
-      const int z = axis_cell(cz, ncz, vc.wz, qz);
-      for (int qy = 0; qy < my; ++qy) {
-        const int y = axis_cell(cy, ncy, vc.wy, qy);
-        const int rowbase = (z * ncy + y) * ncx;
-        for (int part = 0; part < 2; ++part) {
-          const int x0 = part ? b0 : a0, x1 = part ? b1 : a1;
-          if (x0 > x1) continue;
-          const int k0 = cell_start[rowbase + x0];
-          const int k1 = cell_start[rowbase + x1] + cell_count[rowbase + x1];
+    const int nn = vnnb[i];
+    int knext = nn > 0 ? __ldg(vnb + i) : 0;  // list entries fetched one pair ahead
 #pragma unroll 1
-          for (int k = k0; k < k1; ++k) {
-            if (k == i) continue;
-            const double4 rk = vred[k];
-            double xr = ri.x - rk.x, yr = ri.y - rk.y, zr = ri.z - rk.z;
-            image3(box, xr, yr, zr);
-            const double rik2 = r2_exact(xr, yr, zr);
-            if (rik2 > vc.off2) continue;
-            const int kt = __ldg(&vinfo[k].x);
-            double vs = 1.0;
-            bool is14 = false;
-            for (int q = s0; q < s1; ++q)
-              if (__ldg(sp_ks + q) == k) {
-                const int cls = __ldg(sp_c + q);
-                vs = cls == 0 ? vc.vscale[0] : cls == 1 ? vc.vscale[1] : cls == 2 ? vc.vscale[2]
-                                                                      : cls == 3 ? vc.vscale[3] : 1.0;
-                is14 = cls == 2;
-                break;
-              }
-            const int t = kt * vc.nclass + it;
-            const double rv = __ldg(vtab + (is14 ? 2 * nc2 : 0) + t);
-            const double eps = __ldg(vtab + (is14 ? 3 * nc2 : nc2) + t) * vs;
-            const double rik = sqrt(rik2);
-            const double rv2 = rv * rv, rv7 = rv2 * rv2 * rv2 * rv;
-            const double rik6 = rik2 * rik2 * rik2;
-            const double rik7 = rik6 * rik;
-            const double rho = rik7 + vc.ghal * rv7;
-            const double tau = (vc.dhal + 1.0) / (rik + vc.dhal * rv);
-            const double tau2 = tau * tau, tau7 = tau2 * tau2 * tau2 * tau;
-            const double dtau = tau / (vc.dhal + 1.0);
-            const double q7 = rv7 / rho;
-            const double gtau = eps * tau7 * rik6 * (vc.ghal + 1.0) * q7 * q7;
-            double e = eps * tau7 * rv7 * ((vc.ghal + 1.0) * q7 - 2.0);
-            double de = -7.0 * (dtau * e + gtau);
-            if (rik2 > vc.cut2) {
-              const double rik3 = rik2 * rik, rik4 = rik2 * rik2, rik5 = rik2 * rik3;
-              const double taper = vc.c5 * rik5 + vc.c4 * rik4 + vc.c3 * rik3 + vc.c2 * rik2 + vc.c1 * rik + vc.c0;
-              const double dtaper =
-                  5.0 * vc.c5 * rik4 + 4.0 * vc.c4 * rik3 + 3.0 * vc.c3 * rik2 + 2.0 * vc.c2 * rik + vc.c1;
-              de = e * dtaper + de * taper;
-              e = e * taper;
-            }
-            eacc += 0.5 * e;
-            de = de / rik;
-            gx += de * xr;
-            gy += de * yr;
-            gz += de * zr;
-          }
+    for (int s = 0; s < nn; ++s) {
+      const int k = knext;
+      if (s + 1 < nn) knext = __ldg(vnb + (size_t)(s + 1) * npad + i);
+      const double4 rk = vred[k];
+      double xr = ri.x - rk.x, yr = ri.y - rk.y, zr = ri.z - rk.z;
+      image3(box, xr, yr, zr);
+      const double rik2 = r2_exact(xr, yr, zr);
+      if (rik2 > vc.off2) continue;
+      const int kt = __ldg(&vinfo[k].x);
+      double vs = 1.0;
+      bool is14 = false;
+      for (int q = s0; q < s1; ++q)
+        if (__ldg(sp_ks + q) == k) {
+          const int cls = __ldg(sp_c + q);
+          vs = cls == 0 ? vc.vscale[0] : cls == 1 ? vc.vscale[1] : cls == 2 ? vc.vscale[2]
+                                                            : cls == 3 ? vc.vscale[3] : 1.0;
+          is14 = cls == 2;
+          break;
         }
+      const int t = kt * vc.nclass + it;
+      const double rv = __ldg(vtab + (is14 ? 2 * nc2 : 0) + t);
+      const double eps = __ldg(vtab + (is14 ? 3 * nc2 : nc2) + t) * vs;
+      const double rik = sqrt(rik2);
+      const double rv2 = rv * rv, rv7 = rv2 * rv2 * rv2 * rv;
+      const double rik6 = rik2 * rik2 * rik2;
+      const double rik7 = rik6 * rik;
+      const double rho = rik7 + vc.ghal * rv7;
+      const double tau = (vc.dhal + 1.0) / (rik + vc.dhal * rv);
+      const double tau2 = tau * tau, tau7 = tau2 * tau2 * tau2 * tau;
+      const double dtau = tau / (vc.dhal + 1.0);
+      const double q7 = rv7 / rho;
+      const double gtau = eps * tau7 * rik6 * (vc.ghal + 1.0) * q7 * q7;
+      double e = eps * tau7 * rv7 * ((vc.ghal + 1.0) * q7 - 2.0);
+      double de = -7.0 * (dtau * e + gtau);
+      if (rik2 > vc.cut2) {
+        const double rik3 = rik2 * rik, rik4 = rik2 * rik2, rik5 = rik2 * rik3;
+        const double taper = vc.c5 * rik5 + vc.c4 * rik4 + vc.c3 * rik3 + vc.c2 * rik2 + vc.c1 * rik + vc.c0;
+        const double dtaper = 5.0 * vc.c5 * rik4 + 4.0 * vc.c4 * rik3 + 3.0 * vc.c3 * rik2 + 2.0 * vc.c2 * rik + vc.c1;
+        de = e * dtaper + de * taper;
+        e = e * taper;
       }
+      eacc += 0.5 * e;
+      de = de / rik;
+      gx += de * xr;
+      gy += de * yr;
+      gz += de * zr;
     }
     // the site's force: to the atom (kred) and its parent (1 - kred)
     const int iv = inf.y;
@@ -234,17 +269,39 @@ int launch_ehal(Ctx& c, double* d_out) {
   for (int j = 0; j < 4; ++j) vc.vscale[j] = c.vdw_scale[j];
   vc.vscale[4] = 1.0;
   vc.nclass = c.vdw_nclass;
-  // cells within reach: vdwcut, the list buffer (atoms move up to half of it
-  // on each side before a re-sort) and the reduction shift on each side
-  const double reach = off + c.cfg.lbuffer + 2.0 * kShiftMax;
-  int w[3];
-  for (int d = 0; d < 3; ++d) w[d] = (int)ceil(reach / (c.cfg.box[d] / c.nc[d]) - 1e-12);
-  vc.wx = w[0];
-  vc.wy = w[1];
-  vc.wz = w[2];
-  k_ehal<<<nb, kBlock, 0, c.stream>>>(c.n, c.box, vc, c.d_vred, c.d_vinfo, c.d_vtab, c.d_perm, c.d_sp_off,
-                                      c.d_sp_ks, c.d_sp_c, c.d_scell, c.d_cell_start, c.d_cell_count, c.nc[0],
-                                      c.nc[1], c.nc[2], dev, c.d_evpart);
+  // the vdW list: built after a re-sort, or once an atom has moved
+  // lbuffer/2 since the positions it was built from (nblist.f:88-109)
+  bool build = !c.have_vlist || c.vlist_epoch != c.sort_epoch;
+  if (!build) {
+    double disp = 0.0;
+    if ((st = launch_max_displacement_from(c, c.d_vpos_built, &disp))) return st;
+    build = disp >= 0.5 * c.cfg.lbuffer;
+  }
+  if (build) {
+    if (!c.d_vnb) {
+      c.maxvnb = c.cfg.max_neighbors > 0 ? 2 * c.cfg.max_neighbors : kDefaultMaxVnb;
+      if ((st = cuda_status(cudaMalloc((void**)&c.d_vnb, sizeof(int) * (size_t)c.maxvnb * c.npad), &c,
+                            "alloc vdw list")))
+        return st;
+    }
+    if ((st = alloc_once(c, &c.d_vnnb, n, "alloc vdw list"))) return st;
+    if ((st = alloc_once(c, &c.d_vpos_built, n, "alloc vdw list"))) return st;
+    // cells within reach: vdwcut + lbuffer, the atoms' drift since the sort
+    // (below lbuffer/2 each) and the reduction shift on each side
+    const double reach = off + 2.0 * c.cfg.lbuffer + 2.0 * kShiftMax;
+    int w[3];
+    for (int d = 0; d < 3; ++d) w[d] = (int)ceil(reach / (c.cfg.box[d] / c.nc[d]) - 1e-12);
+    const double vbuf = off + c.cfg.lbuffer;
+    k_vdw_list<<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vbuf * vbuf, w[0], w[1], w[2], c.d_vred, c.d_scell,
+                                            c.d_cell_start, c.d_cell_count, c.nc[0], c.nc[1], c.nc[2], c.maxvnb,
+                                            c.d_vnnb, c.d_vnb, c.d_flags);
+    if ((st = cuda_status(cudaGetLastError(), &c, "vdw list"))) return st;
+    cudaMemcpyAsync(c.d_vpos_built, c.d_pos, sizeof(double4) * n, cudaMemcpyDeviceToDevice, c.stream);
+    c.have_vlist = true;
+    c.vlist_epoch = c.sort_epoch;
+  }
+  k_ehal<<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vc, c.d_vred, c.d_vinfo, c.d_vtab, c.d_perm, c.d_sp_off,
+                                      c.d_sp_ks, c.d_sp_c, c.d_vnnb, c.d_vnb, dev, c.d_evpart);
   if ((st = cuda_status(cudaGetLastError(), &c, "ehal"))) return st;
   k_sum_partials<<<1, 256, 0, c.stream>>>(nb, c.d_evpart, c.d_ev);
   if ((st = cuda_status(cudaGetLastError(), &c, "ehal energy"))) return st;
