@@ -203,6 +203,10 @@ int thp_set_vdw(thp_ctx* ctx, const int* cls, int nclass, const double* tables, 
  * are found in the context's cell sort (kept or rebuilt as for a solve);
  * THP_E_INVALID when a reduction moves a site by more than 0.3 A. */
 int thp_ehal1(thp_ctx* ctx, double* ev, double* dev);
+/* reference-format vdW half list (vlistcell, nblist.f:1148-1305: reduced
+ * sites within vdwcut + lbuffer, partners k > i, 0-based) copied to the host;
+ * THP_E_LIST_OVERFLOW when a row exceeds maxvlst */
+int thp_get_vlist(thp_ctx* ctx, int maxvlst, int* nvlst, int* vlst);
 /* Velocity-Verlet NVE dynamics driven by the polarization gradient alone
  * (verlet.f:17-200 with gradient = epolar1): per step a half kick, a drift of
  * the positions on the device, a solve warm-started from the predictor when
@@ -333,6 +337,8 @@ int thp_bind_state(thp_ctx* ctx, double* x, double* y, double* z, double* rpole,
 int thp_last_error(void);
 /* bind deriv::dep(3,n), written by epolar1_ */
 int thp_bind_gradient(thp_ctx* ctx, double* dep);
+/* bind neigh::nvlst(n) and vlst(maxvlst,n), filled by vlistcell_ */
+int thp_bind_vlist(thp_ctx* ctx, int* nvlst, int* vlst, int maxvlst);
 /* bind energi::ev and deriv::dev(3,n), written by ehal1_ (may be NULL) */
 int thp_bind_vdw(thp_ctx* ctx, double* ev, double* dev);
 /* bind energi::em and deriv::dem(3,n), written by empole1_ (may be NULL) */
@@ -380,7 +386,9 @@ void fphi_uind_site_(const int* isite, const int* impi, double* fdip_phi1, doubl
                      double* fdip_sum_phi);
 /* nblist.f:117 -- rebuild the polarization list; fills the bound elst/nelst */
 void mlistcell_(void);
-/* nblist.f:1148 -- same list for the vdW slot name used by the workload */
+/* nblist.f:1148 -- the vdW list into the bound nvlst/vlst (1-based) when the
+ * context has a vdW description (thp_set_vdw) and a bound vdW list
+ * (thp_bind_vlist); otherwise the polarization list, as mlistcell_ */
 void vlistcell_(void);
 /* ehal1.f:17 -- van der Waals energy into the bound ev and its gradient
  * into the bound dev (overwritten, as ehal1c zeroes it) */

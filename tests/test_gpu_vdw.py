@@ -85,3 +85,54 @@ def test_ehal1_refuses_a_reduction_beyond_the_reach(lib, thp):
     with pytest.raises(lib.ThpError) as e:
         ctx.ehal1()
     assert e.value.status == lib.THP_E_INVALID
+
+
+def _vdw_pairs_bruteforce(ws):
+    v = ws.vdw
+    pos = ws.positions()
+    par = pos[v["ired"]]
+    red = v["kred"][:, None] * (pos - par) + par
+    L = np.asarray(ws.box)
+    vbuf2 = (v["vdwcut"] + ws.lbuffer) ** 2
+    out = []
+    for i in range(ws.n - 1):
+        x = red[i] - red[i + 1:]
+        x -= L * np.round(x / L)
+        r2 = np.einsum("ij,ij->i", x, x)
+        k = np.nonzero(r2 <= vbuf2)[0] + i + 1
+        out.append(np.stack([np.full(len(k), i), k], axis=1))
+    return np.concatenate(out)
+
+
+def test_vdw_list_is_vlistcell_pair_set(lib, thp):
+    ws = thp.water.make_water_box(648, cfg=0)
+    ctx = lib.Context(ws)
+    got = ctx.vdw_pairs()
+    ref = _vdw_pairs_bruteforce(ws)
+    assert len(got) == len(ref) and np.array_equal(got, ref[np.lexsort((ref[:, 1], ref[:, 0]))])
+
+
+def test_vlistcell_dropin_fills_the_vdw_list(lib, thp):
+    ws = thp.water.make_water_box(648, cfg=0)
+    L = lib.load()
+    ctx = lib.Context(ws)
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (ws.x, ws.y, ws.z))
+    rp = np.ascontiguousarray(O.rotpole(ws))
+    u1, u2 = np.zeros((ws.n, 3)), np.zeros((ws.n, 3))
+    assert L.thp_bind_state(ctx.h, x.ctypes.data_as(dp), y.ctypes.data_as(dp), z.ctypes.data_as(dp),
+                            rp.ctypes.data_as(dp), u1.ctypes.data_as(dp), u2.ctypes.data_as(dp), None, None, 0,
+                            None) == 0
+    maxv = 1200
+    nv = np.zeros(ws.n, np.int32)
+    vl = np.zeros((ws.n, maxv), np.int32)
+    assert L.thp_bind_vlist(ctx.h, nv.ctypes.data_as(ip), vl.ctypes.data_as(ip), maxv) == 0
+    L.vlistcell_()
+    assert L.thp_last_error() == 0
+    rows = np.repeat(np.arange(ws.n), nv)
+    cols = vl[np.arange(maxv)[None, :] < nv[:, None]] - 1  # 1-based in the bound list
+    got = np.stack([rows, cols], axis=1)
+    got = got[np.lexsort((got[:, 1], got[:, 0]))]
+    ref = _vdw_pairs_bruteforce(ws)
+    assert np.array_equal(got, ref[np.lexsort((ref[:, 1], ref[:, 0]))])

@@ -607,6 +607,8 @@ static int clear_system_state(thp_ctx* h) {
   h->field_valid = h->guess_uploaded = h->solved_once = false;
   c.bx = c.by = c.bz = c.brpole = c.buind = c.buinp = c.bep = c.bdep = c.bqgrid = nullptr;
   c.bem = c.bdem = c.bev = c.bdev = nullptr;
+  c.bnvlst = c.bvlst = nullptr;
+  c.bmaxvlst = 0;
   c.have_vdw = false;
   c.mscale[0] = c.mscale[1] = 0.0;  // initprm.f:413-416
   c.mscale[2] = c.mscale[3] = 1.0;
@@ -1490,6 +1492,39 @@ int thp_get_nblist(thp_ctx* h, int maxelst, int* nelst, int* elst) {
   return st;
 }
 
+int thp_get_vlist(thp_ctx* h, int maxvlst, int* nvlst, int* vlst) {
+  if (!h || !nvlst || !vlst || maxvlst <= 0) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (!c.have_vdw) return THP_E_STATE;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st = ensure_list(h, false);
+  if (!st) st = launch_vdw_list(c);
+  if (st) return st;
+  int *dn = nullptr, *de = nullptr;
+  if ((st = dmalloc(c, &dn, c.n, "export"))) return st;
+  if ((st = dmalloc(c, &de, (size_t)c.n * maxvlst, "export"))) {
+    cudaFree(dn);
+    return st;
+  }
+  st = launch_export_pairs(c, c.d_vnnb, c.d_vnb, c.maxvnb, maxvlst, dn, de);
+  if (!st) {
+    cudaMemcpyAsync(nvlst, dn, sizeof(int) * c.n, cudaMemcpyDeviceToHost, c.stream);
+    cudaMemcpyAsync(vlst, de, sizeof(int) * (size_t)c.n * maxvlst, cudaMemcpyDeviceToHost, c.stream);
+    st = check_flags(h);
+  }
+  cudaFree(dn);
+  cudaFree(de);
+  return st;
+}
+
+int thp_bind_vlist(thp_ctx* h, int* nvlst, int* vlst, int maxvlst) {
+  if (!h || maxvlst < 0) return THP_E_INVALID;
+  h->c.bnvlst = nvlst;
+  h->c.bvlst = vlst;
+  h->c.bmaxvlst = maxvlst;
+  return THP_OK;
+}
+
 int thp_tmatxb(thp_ctx* h, int nrhs, int dodiag, const double* mu, double* efi) {
   if (!h || !mu || !efi || nrhs < 1 || nrhs > 2) return THP_E_INVALID;
   Ctx& c = h->c;
@@ -1650,7 +1685,24 @@ void mlistcell_(void) {
   g_last_error = st;
 }
 
-void vlistcell_(void) { mlistcell_(); }
+// nblist.f:1148 -- with a vdW description and a bound vdW list, the vdW list
+// of vlistcell (reduced sites, vdwcut + lbuffer); otherwise the polarization
+// list under this name
+void vlistcell_(void) {
+  thp_ctx* h = g_current;
+  if (!h || !h->c.have_vdw || !h->c.bnvlst || !h->c.bvlst) {
+    mlistcell_();
+    return;
+  }
+  int st = sync_bound_inputs(h);
+  if (!st) st = thp_get_vlist(h, h->c.bmaxvlst, h->c.bnvlst, h->c.bvlst);
+  if (!st) {  // Fortran atom numbers are 1-based
+    const size_t n = h->c.n, m = h->c.bmaxvlst;
+    for (size_t i = 0; i < n; ++i)
+      for (int j = 0; j < h->c.bnvlst[i]; ++j) h->c.bvlst[i * m + j] += 1;
+  }
+  g_last_error = st;
+}
 
 void newinduce_pme2_(void) {
   thp_ctx* h = g_current;

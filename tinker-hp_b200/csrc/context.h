@@ -222,6 +222,8 @@ struct Ctx {
   double* bdep = nullptr;
   double *bem = nullptr, *bdem = nullptr;  // energi::em, deriv::dem(3,n), written by empole1_
   double *bev = nullptr, *bdev = nullptr;  // energi::ev, deriv::dev(3,n), written by ehal1_
+  int *bnvlst = nullptr, *bvlst = nullptr;  // neigh::nvlst(n), vlst(maxvlst,n), filled by vlistcell_
+  int bmaxvlst = 0;
   double* bqgrid = nullptr;  // pme::qgrid2in_2d(2,n1,n2,n3), read by fphi_uind_site_
 
   // CUDA graph of one CG chunk (captured on first use)

@@ -47,6 +47,9 @@ int launch_empole(Ctx& c, double* d_out);
 // buffered 14-7 van der Waals energy into d_ev and dE/dx [n][3] (original
 // order) into d_out, for the current sorted positions and cell sort
 int launch_ehal(Ctx& c, double* d_out);
+int launch_vdw_list(Ctx& c);  // reduced sites, and the vdW list when it is stale
+// reference-format half list (k > i, original numbering) of a slot-major list
+int launch_export_pairs(Ctx& c, const int* nnb, const int* nb, int maxnb, int maxelst, int* d_nelst, int* d_elst);
 
 // sites.cu
 int launch_grid_uind_sites(Ctx& c, int nsites, const int* d_site, const double* d_fuind, const double* d_fuinp,

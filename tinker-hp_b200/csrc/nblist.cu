@@ -494,9 +494,13 @@ int launch_build_list_on(Ctx& c, cudaStream_t s) {
 }
 
 int launch_export_list(Ctx& c, int maxelst, int* d_nelst, int* d_elst) {
+  return launch_export_pairs(c, c.d_nnb, c.d_nb, c.maxnb, maxelst, d_nelst, d_elst);
+}
+
+int launch_export_pairs(Ctx& c, const int* nnb, const int* nb, int maxnb, int maxelst, int* d_nelst, int* d_elst) {
   const int n = c.n;
-  k_export<<<(n + kBlock - 1) / kBlock, kBlock, 0, c.stream>>>(n, c.npad, c.maxnb, c.d_perm, c.d_nnb, c.d_nb,
-                                                               maxelst, d_nelst, d_elst, c.d_flags);
+  k_export<<<(n + kBlock - 1) / kBlock, kBlock, 0, c.stream>>>(n, c.npad, maxnb, c.d_perm, nnb, nb, maxelst, d_nelst,
+                                                               d_elst, c.d_flags);
   return cuda_status(cudaGetLastError(), &c, "export list");
 }
 

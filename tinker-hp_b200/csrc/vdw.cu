@@ -229,6 +229,50 @@ int alloc_once(Ctx& c, P** p, size_t count, const char* what) {
 
 }  // namespace
 
+// Reduced sites for the current positions, and the vdW list when it is stale.
+int launch_vdw_list(Ctx& c) {
+  int st;
+  if (!c.have_vdw) return THP_E_STATE;
+  const size_t n = c.n;
+  const int nb = (c.n + kBlock - 1) / kBlock;
+  if ((st = alloc_once(c, &c.d_vred, n, "alloc vdw sites"))) return st;
+  if ((st = alloc_once(c, &c.d_vinfo, n, "alloc vdw sites"))) return st;
+  k_vdw_sites<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, c.d_iperm, c.d_pos, c.d_vcls, c.d_vired, c.d_vkred,
+                                           kShiftMax * kShiftMax, c.d_vred, c.d_vinfo, c.d_flags);
+  if ((st = cuda_status(cudaGetLastError(), &c, "vdw sites"))) return st;
+  // the vdW list: built after a re-sort, or once an atom has moved
+  // lbuffer/2 since the positions it was built from (nblist.f:88-109)
+  bool build = !c.have_vlist || c.vlist_epoch != c.sort_epoch;
+  if (!build) {
+    double disp = 0.0;
+    if ((st = launch_max_displacement_from(c, c.d_vpos_built, &disp))) return st;
+    build = disp >= 0.5 * c.cfg.lbuffer;
+  }
+  if (!build) return THP_OK;
+  if (!c.d_vnb) {
+    c.maxvnb = c.cfg.max_neighbors > 0 ? 2 * c.cfg.max_neighbors : kDefaultMaxVnb;
+    if ((st = cuda_status(cudaMalloc((void**)&c.d_vnb, sizeof(int) * (size_t)c.maxvnb * c.npad), &c,
+                          "alloc vdw list")))
+      return st;
+  }
+  if ((st = alloc_once(c, &c.d_vnnb, n, "alloc vdw list"))) return st;
+  if ((st = alloc_once(c, &c.d_vpos_built, n, "alloc vdw list"))) return st;
+  // cells within reach: vdwcut + lbuffer, the atoms' drift since the sort
+  // (below lbuffer/2 each) and the reduction shift on each side
+  const double reach = c.vdw_cut + 2.0 * c.cfg.lbuffer + 2.0 * kShiftMax;
+  int w[3];
+  for (int d = 0; d < 3; ++d) w[d] = (int)ceil(reach / (c.cfg.box[d] / c.nc[d]) - 1e-12);
+  const double vbuf = c.vdw_cut + c.cfg.lbuffer;
+  k_vdw_list<<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vbuf * vbuf, w[0], w[1], w[2], c.d_vred, c.d_scell,
+                                          c.d_cell_start, c.d_cell_count, c.nc[0], c.nc[1], c.nc[2], c.maxvnb, c.d_vnnb,
+                                          c.d_vnb, c.d_flags);
+  if ((st = cuda_status(cudaGetLastError(), &c, "vdw list"))) return st;
+  cudaMemcpyAsync(c.d_vpos_built, c.d_pos, sizeof(double4) * n, cudaMemcpyDeviceToDevice, c.stream);
+  c.have_vlist = true;
+  c.vlist_epoch = c.sort_epoch;
+  return THP_OK;
+}
+
 // van der Waals energy (into d_ev) and gradient (into d_out, original order)
 // for the sorted positions and the cell sort of the context.
 int launch_ehal(Ctx& c, double* d_out) {
@@ -237,16 +281,12 @@ int launch_ehal(Ctx& c, double* d_out) {
   const size_t n = c.n;
   const int nb = (c.n + kBlock - 1) / kBlock;
   if ((st = alloc_once(c, &c.d_depfix, 3 * n, "alloc gradient"))) return st;
-  if ((st = alloc_once(c, &c.d_vred, n, "alloc vdw sites"))) return st;
-  if ((st = alloc_once(c, &c.d_vinfo, n, "alloc vdw sites"))) return st;
   if ((st = alloc_once(c, &c.d_evpart, (size_t)nb + 1, "alloc vdw partials"))) return st;
   c.d_ev = c.d_evpart + nb;
   unsigned long long* dev = c.d_depfix;
   if ((st = cuda_status(cudaMemsetAsync(dev, 0, sizeof(unsigned long long) * 3 * n, c.stream), &c, "zero dev")))
     return st;
-  k_vdw_sites<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, c.d_iperm, c.d_pos, c.d_vcls, c.d_vired, c.d_vkred,
-                                           kShiftMax * kShiftMax, c.d_vred, c.d_vinfo, c.d_flags);
-  if ((st = cuda_status(cudaGetLastError(), &c, "vdw sites"))) return st;
+  if ((st = launch_vdw_list(c))) return st;
   VdwConst vc;
   const double off = c.vdw_cut, cut = c.vdw_taper;
   vc.off = off;
@@ -269,37 +309,6 @@ int launch_ehal(Ctx& c, double* d_out) {
   for (int j = 0; j < 4; ++j) vc.vscale[j] = c.vdw_scale[j];
   vc.vscale[4] = 1.0;
   vc.nclass = c.vdw_nclass;
-  // the vdW list: built after a re-sort, or once an atom has moved
-  // lbuffer/2 since the positions it was built from (nblist.f:88-109)
-  bool build = !c.have_vlist || c.vlist_epoch != c.sort_epoch;
-  if (!build) {
-    double disp = 0.0;
-    if ((st = launch_max_displacement_from(c, c.d_vpos_built, &disp))) return st;
-    build = disp >= 0.5 * c.cfg.lbuffer;
-  }
-  if (build) {
-    if (!c.d_vnb) {
-      c.maxvnb = c.cfg.max_neighbors > 0 ? 2 * c.cfg.max_neighbors : kDefaultMaxVnb;
-      if ((st = cuda_status(cudaMalloc((void**)&c.d_vnb, sizeof(int) * (size_t)c.maxvnb * c.npad), &c,
-                            "alloc vdw list")))
-        return st;
-    }
-    if ((st = alloc_once(c, &c.d_vnnb, n, "alloc vdw list"))) return st;
-    if ((st = alloc_once(c, &c.d_vpos_built, n, "alloc vdw list"))) return st;
-    // cells within reach: vdwcut + lbuffer, the atoms' drift since the sort
-    // (below lbuffer/2 each) and the reduction shift on each side
-    const double reach = off + 2.0 * c.cfg.lbuffer + 2.0 * kShiftMax;
-    int w[3];
-    for (int d = 0; d < 3; ++d) w[d] = (int)ceil(reach / (c.cfg.box[d] / c.nc[d]) - 1e-12);
-    const double vbuf = off + c.cfg.lbuffer;
-    k_vdw_list<<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vbuf * vbuf, w[0], w[1], w[2], c.d_vred, c.d_scell,
-                                            c.d_cell_start, c.d_cell_count, c.nc[0], c.nc[1], c.nc[2], c.maxvnb,
-                                            c.d_vnnb, c.d_vnb, c.d_flags);
-    if ((st = cuda_status(cudaGetLastError(), &c, "vdw list"))) return st;
-    cudaMemcpyAsync(c.d_vpos_built, c.d_pos, sizeof(double4) * n, cudaMemcpyDeviceToDevice, c.stream);
-    c.have_vlist = true;
-    c.vlist_epoch = c.sort_epoch;
-  }
   k_ehal<<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vc, c.d_vred, c.d_vinfo, c.d_vtab, c.d_perm, c.d_sp_off,
                                       c.d_sp_ks, c.d_sp_c, c.d_vnnb, c.d_vnb, dev, c.d_evpart);
   if ((st = cuda_status(cudaGetLastError(), &c, "ehal"))) return st;

@@ -132,6 +132,8 @@ def load():
         "thp_set_vdw": ([vp, _ip, C.c_int, _dp, _ip, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_double],
                         C.c_int),
         "thp_ehal1": ([vp, _dp, _dp], C.c_int),
+        "thp_get_vlist": ([vp, C.c_int, _ip, _ip], C.c_int),
+        "thp_bind_vlist": ([vp, _ip, _ip, C.c_int], C.c_int),
         "thp_bind_vdw": ([vp, _dp, _dp], C.c_int),
         "ehal1_": ([], None),
         "thp_empole1": ([vp, _dp, _dp], C.c_int),
@@ -363,6 +365,17 @@ class Context:
         ev = C.c_double()
         self._check(load().thp_ehal1(self.h, C.byref(ev), _p(dev)), "thp_ehal1")
         return ev.value, dev
+
+    def vdw_pairs(self, maxvlst=1200):
+        """Sorted (i, k) pairs of the vdW half list (vlistcell) as [P,2]."""
+        nv = np.zeros(self.n, np.int32)
+        vl = np.zeros(self.n * maxvlst, np.int32)
+        self._check(load().thp_get_vlist(self.h, maxvlst, _p(nv, _ip), _p(vl, _ip)), "thp_get_vlist")
+        vl = vl.reshape(self.n, maxvlst)
+        rows = np.repeat(np.arange(self.n), nv)
+        cols = vl[np.arange(maxvlst)[None, :] < nv[:, None]]
+        p = np.stack([rows, cols], axis=1)
+        return p[np.lexsort((p[:, 1], p[:, 0]))]
 
     def empole1(self, out=None):
         """(Em, dEm/dx [n,3] kcal/mol/A): permanent-multipole energy and
