@@ -122,6 +122,7 @@ struct Ctx {
   double* d_vkred = nullptr;
   double* d_vtab = nullptr;
   double4* d_vred = nullptr;
+  float4* d_vredf = nullptr;      // the same sites wrapped into the box, FP32 (list screen)
   int2* d_vinfo = nullptr;
   // vdW pair list (vlistcell): full list within vdwcut + lbuffer of the
   // reduced sites, slot-major [s*npad + i], rebuilt after a re-sort or when an

@@ -22,6 +22,8 @@
 // interacting pairs, so the lanes of a warp stay together through the pair
 // arithmetic.  The site's summed force goes to the atom and its parent in
 // 64-bit fixed point, the energy through per-block partials summed in order.
+#include <algorithm>
+
 #include "grad_dev.cuh"
 #include "kernels.h"
 
@@ -48,8 +50,9 @@ struct VdwConst {
 // sorted reduced sites: (x, y, z, kred) and (class, parent in sorted order)
 __global__ void k_vdw_sites(int n, const int* __restrict__ perm, const int* __restrict__ iperm,
                             const double4* __restrict__ pos, const int* __restrict__ cls,
-                            const int* __restrict__ ired, const double* __restrict__ kred, double shift2max,
-                            double4* __restrict__ vred, int2* __restrict__ vinfo, int* __restrict__ flags) {
+                            const int* __restrict__ ired, const double* __restrict__ kred, Box box,
+                            double shift2max, double4* __restrict__ vred, float4* __restrict__ vredf,
+                            int2* __restrict__ vinfo, int* __restrict__ flags) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const int o = perm[s];
@@ -61,6 +64,9 @@ __global__ void k_vdw_sites(int n, const int* __restrict__ perm, const int* __re
   const double sx = x - p.x, sy = y - p.y, sz = z - p.z;
   if (sx * sx + sy * sy + sz * sz > shift2max) atomicOr(flags, DEV_VDW_REACH);
   vred[s] = make_double4(x, y, z, r);
+  double wx = x, wy = y, wz = z;  // wrapped into the box for the FP32 screen of the list build
+  image3(box, wx, wy, wz);
+  vredf[s] = make_float4((float)wx, (float)wy, (float)wz, 0.f);
   vinfo[s] = make_int2(cls[o], ps);
 }
 
@@ -72,8 +78,9 @@ __device__ __forceinline__ int axis_cell(int c, int nc, int w, int q) {
 
 // vlistcell (nblist.f:1148-1305) over the cell sort: every other site whose
 // reduced minimum-image distance is within vbuf (both directions)
-__global__ void __launch_bounds__(kBlock) k_vdw_list(int n, int npad, Box box, double vbuf2, int wx, int wy, int wz,
-                                                     const double4* __restrict__ vred, const int* __restrict__ scell,
+__global__ void __launch_bounds__(kBlock) k_vdw_list(int n, int npad, Box box, double vbuf2, int prefilter, float lo,
+                                                     float hi, int wx, int wy, int wz, const double4* __restrict__ vred,
+                                                     const float4* __restrict__ vredf, const int* __restrict__ scell,
                                                      const int* __restrict__ cell_start,
                                                      const int* __restrict__ cell_count, int ncx, int ncy, int ncz,
                                                      int maxvnb, int* __restrict__ vnnb, int* __restrict__ vnb,
@@ -81,6 +88,9 @@ __global__ void __launch_bounds__(kBlock) k_vdw_list(int n, int npad, Box box, d
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 ri = vred[i];
+  const float4 fi = vredf[i];
+  const float bx = (float)box.l[0], by = (float)box.l[1], bz = (float)box.l[2];
+  const float hx = 0.5f * bx, hy = 0.5f * by, hz = 0.5f * bz;
   const int c = scell[i];
   const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
   // x ranges of the window: [a0, a1] and the wrapped [b0, b1]
@@ -120,10 +130,27 @@ __global__ void __launch_bounds__(kBlock) k_vdw_list(int n, int npad, Box box, d
 #pragma unroll 4
         for (int k = k0; k < k1; ++k) {
           if (k == i) continue;
-          const double4 rk = vred[k];
-          double xr = ri.x - rk.x, yr = ri.y - rk.y, zr = ri.z - rk.z;
-          image3(box, xr, yr, zr);
-          if (r2_exact(xr, yr, zr) <= vbuf2) {
+          // FP32 screen: accept below lo, reject above hi, exact FP64 test
+          // between (lo/hi bracket vbuf2 by twice the FP32 error bound)
+          bool take = false, exact = true;
+          if (prefilter) {
+            const float4 fk = vredf[k];
+            float xf = fi.x - fk.x, yf = fi.y - fk.y, zf = fi.z - fk.z;
+            xf = fabsf(xf) > hx ? xf - copysignf(bx, xf) : xf;
+            yf = fabsf(yf) > hy ? yf - copysignf(by, yf) : yf;
+            zf = fabsf(zf) > hz ? zf - copysignf(bz, zf) : zf;
+            const float r2f = xf * xf + yf * yf + zf * zf;
+            if (r2f > hi) continue;
+            take = r2f < lo;
+            exact = !take;
+          }
+          if (exact) {
+            const double4 rk = vred[k];
+            double xr = ri.x - rk.x, yr = ri.y - rk.y, zr = ri.z - rk.z;
+            image3(box, xr, yr, zr);
+            take = r2_exact(xr, yr, zr) <= vbuf2;
+          }
+          if (take) {
             if (cnt < maxvnb) vnb[(size_t)cnt * npad + i] = k;
             ++cnt;
           }
@@ -237,8 +264,9 @@ int launch_vdw_list(Ctx& c) {
   const int nb = (c.n + kBlock - 1) / kBlock;
   if ((st = alloc_once(c, &c.d_vred, n, "alloc vdw sites"))) return st;
   if ((st = alloc_once(c, &c.d_vinfo, n, "alloc vdw sites"))) return st;
-  k_vdw_sites<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, c.d_iperm, c.d_pos, c.d_vcls, c.d_vired, c.d_vkred,
-                                           kShiftMax * kShiftMax, c.d_vred, c.d_vinfo, c.d_flags);
+  if ((st = alloc_once(c, &c.d_vredf, n, "alloc vdw sites"))) return st;
+  k_vdw_sites<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, c.d_iperm, c.d_pos, c.d_vcls, c.d_vired, c.d_vkred, c.box,
+                                           kShiftMax * kShiftMax, c.d_vred, c.d_vredf, c.d_vinfo, c.d_flags);
   if ((st = cuda_status(cudaGetLastError(), &c, "vdw sites"))) return st;
   // the vdW list: built after a re-sort, or once an atom has moved
   // lbuffer/2 since the positions it was built from (nblist.f:88-109)
@@ -263,7 +291,18 @@ int launch_vdw_list(Ctx& c) {
   int w[3];
   for (int d = 0; d < 3; ++d) w[d] = (int)ceil(reach / (c.cfg.box[d] / c.nc[d]) - 1e-12);
   const double vbuf = c.vdw_cut + c.cfg.lbuffer;
-  k_vdw_list<<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vbuf * vbuf, w[0], w[1], w[2], c.d_vred, c.d_scell,
+  const double vbuf2 = vbuf * vbuf;
+  // the FP32 screen, bracketed as the polarization list build's: each
+  // coordinate of a wrapped FP32 difference is off by at most 4 * 2^-24 *
+  // Lmax, r^2 then by 2 vbuf dr + dr^2; pairs must sit well inside half a box
+  const double hmin = std::min(c.box.half[0], std::min(c.box.half[1], c.box.half[2]));
+  const int prefilter = hmin > vbuf + 1.0 ? 1 : 0;
+  const double lmax = std::max(c.box.l[0], std::max(c.box.l[1], c.box.l[2]));
+  const double dr = 1.7320508075688772 * 4.0 * lmax * 5.9604644775390625e-08;
+  const double band = std::max(1e-5, 2.0 * (2.0 * vbuf * dr + dr * dr) / vbuf2);
+  const float lo = (float)(vbuf2 * (1.0 - band)), hi = (float)(vbuf2 * (1.0 + band));
+  k_vdw_list<<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vbuf2, prefilter, lo, hi, w[0], w[1], w[2], c.d_vred,
+                                          c.d_vredf, c.d_scell,
                                           c.d_cell_start, c.d_cell_count, c.nc[0], c.nc[1], c.nc[2], c.maxvnb, c.d_vnnb,
                                           c.d_vnb, c.d_flags);
   if ((st = cuda_status(cudaGetLastError(), &c, "vdw list"))) return st;
