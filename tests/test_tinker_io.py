@@ -161,3 +161,14 @@ def test_loaded_box_vdw_matches_the_built_one(tio, thp, tmp_path):
     eb, db = O.Oracle(back).ehal1()
     assert abs(ea - eb) < 1e-10 * abs(ea)
     np.testing.assert_allclose(db, da, rtol=0, atol=1e-9 * np.abs(da).max())
+
+
+def test_group_lists_of_single_atom_groups(tio):
+    # each atom its own polarization group (no group types): ip12..ip14 are
+    # the atoms one, two and three bonds away along the chain 0-1-2-3-4-5
+    i12 = [[1], [0, 2], [1, 3], [2, 4], [3, 5], [4]]
+    ip11, ip12, ip13, ip14 = tio.polargrp(np.arange(6) + 1, i12, {})
+    assert ip11 == [[i] for i in range(6)]
+    assert ip12 == i12
+    assert ip13 == [[2], [3], [0, 4], [1, 5], [2], [3]]
+    assert ip14 == [[3], [4], [5], [0], [1], [2]]
