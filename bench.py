@@ -360,21 +360,30 @@ def empole_run(lib, ws, reps=10):
 
 
 def ehal_run(lib, ws, reps=10):
-    """Buffered 14-7 van der Waals energy and gradient (ehal1c, FP64) of the
-    box: wall time per call through the C-ABI with the cell sort in place
-    (each call: reduced sites, the cell-window pair search and pair terms,
-    the gradient into a pinned host array)."""
+    """Buffered 14-7 van der Waals energy and gradient (ehal1c) of the box,
+    FP64 and mixed: wall time per call through the C-ABI with the vdW list in
+    place (each call: reduced sites, the displacement check, the pair terms
+    over the list, the gradient into a pinned host array)."""
     import torch
-    ctx = lib.Context(ws, precision=lib.MIXED)
-    buf = torch.empty((ws.n, 3), dtype=torch.float64, pin_memory=True).numpy()
-    ctx.ehal1(out=buf)
-    ctx.ehal1(out=buf)
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        ev, _ = ctx.ehal1(out=buf)
-    dt = (time.perf_counter() - t0) / reps
-    ctx.close()
-    return {"ms_per_call": dt * 1e3, "ev_kcal_mol": ev, "atoms": ws.n, "cutoff_A": ws.vdw["vdwcut"]}
+    out = {"atoms": ws.n, "cutoff_A": ws.vdw["vdwcut"]}
+    res = {}
+    for name, prec in (("fp64", lib.FP64), ("mixed", lib.MIXED)):
+        ctx = lib.Context(ws, precision=prec)
+        buf = torch.empty((ws.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+        ctx.ehal1(out=buf)
+        ctx.ehal1(out=buf)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            ev, dev = ctx.ehal1(out=buf)
+        dt = (time.perf_counter() - t0) / reps
+        res[name] = (ev, dev.copy())
+        out[name] = {"ms_per_call": dt * 1e3, "ev_kcal_mol": ev}
+        ctx.close()
+    (e64, d64), (em, dm) = res["fp64"], res["mixed"]
+    out["mixed_energy_rel_err"] = (em - e64) / e64
+    out["mixed_force_rms_rel_err"] = float(np.sqrt(np.mean(np.sum((dm - d64) ** 2, axis=1)))
+                                           / np.sqrt(np.mean(np.sum(d64 ** 2, axis=1))))
+    return out
 
 
 def timed_solves(ctx, lib, steps, warmup, rebuild=True, guess=None):

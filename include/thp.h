@@ -199,8 +199,10 @@ int thp_set_vdw(thp_ctx* ctx, const int* cls, int nclass, const double* tables, 
 /* Buffered 14-7 van der Waals energy and gradient, ehal1c (ehal1.f:69-482,
  * standard branch; no long-range correction) over the pairs vlistcell
  * (nblist.f:1148) would list: ev (kcal/mol) and dev [n][3] (kcal/mol/A,
- * original order; either may be NULL), FP64 in both precisions.  The pairs
- * are found in the context's cell sort (kept or rebuilt as for a solve);
+ * original order; either may be NULL).  FP64 pair terms in the FP64 form;
+ * the mixed form evaluates them in FP32 from FP32 sites (the taper in its
+ * smoothstep form) and accumulates in FP64.  The pair list is kept in the
+ * context and rebuilt after a re-sort or a move of lbuffer/2;
  * THP_E_INVALID when a reduction moves a site by more than 0.3 A. */
 int thp_ehal1(thp_ctx* ctx, double* ev, double* dev);
 /* reference-format vdW half list (vlistcell, nblist.f:1148-1305: reduced

@@ -1,8 +1,9 @@
 """Buffered 14-7 van der Waals energy and gradient (ehal1c) of the CUDA path
 against the CPU oracle (itself pinned by a textbook-form direct sum and finite
-differences in tests/test_oracle.py).  The pair terms run in FP64 in both
-precisions: energy within 1e-10 relative, gradient within 1e-9 of its largest
-component."""
+differences in tests/test_oracle.py).  FP64 form: energy within 1e-10
+relative, gradient within 1e-9 of its largest component.  Mixed form (FP32
+pair terms from FP32 wrapped sites, FP64 accumulation): energy within 1e-5
+relative, force RMS error within 1e-5 of the force RMS."""
 import ctypes as C
 import dataclasses
 
@@ -32,8 +33,15 @@ def test_ehal1_matches_oracle(lib, thp, precision, nw, edge):
     ev_ref, dev_ref = O.Oracle(ws).ehal1()
     ctx = lib.Context(ws, precision=lib.FP64 if precision == "fp64" else lib.MIXED)
     ev, dev = ctx.ehal1()
-    assert abs(ev - ev_ref) < 1e-10 * abs(ev_ref), (ev, ev_ref)
-    assert rel(dev, dev_ref) < 1e-9, rel(dev, dev_ref)
+    if precision == "fp64":
+        assert abs(ev - ev_ref) < 1e-10 * abs(ev_ref), (ev, ev_ref)
+        assert rel(dev, dev_ref) < 1e-9, rel(dev, dev_ref)
+    else:
+        err = np.sqrt(np.mean(np.sum((dev - dev_ref) ** 2, axis=1)))
+        scale = np.sqrt(np.mean(np.sum(dev_ref ** 2, axis=1)))
+        print(f"mixed ehal: energy error {(ev - ev_ref) / ev_ref:.2e} relative; force RMS error {err / scale:.2e}")
+        assert abs(ev - ev_ref) < 1e-5 * abs(ev_ref), (ev, ev_ref)
+        assert err < 1e-5 * scale, (err, scale)
 
 
 def test_ehal1_large_box_and_moves(lib, thp):

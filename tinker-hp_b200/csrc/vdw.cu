@@ -23,6 +23,7 @@
 // arithmetic.  The site's summed force goes to the atom and its parent in
 // 64-bit fixed point, the energy through per-block partials summed in order.
 #include <algorithm>
+#include <type_traits>
 
 #include "grad_dev.cuh"
 #include "kernels.h"
@@ -162,17 +163,63 @@ __global__ void __launch_bounds__(kBlock) k_vdw_list(int n, int npad, Box box, d
   if (cnt > maxvnb) atomicOr(flags, DEV_LIST_OVERFLOW);
 }
 
+// buffered 14-7 pair terms of one pair at distance r (r2 = r^2): adds
+// e/2 to eacc and returns de/r.  FP64: the reference's arithmetic with the
+// taper in powers of r (switch.f:103-111); FP32: the same polynomial in the
+// smoothstep form 1 - t^3 (10 - 15 t + 6 t^2), t = (r - cut)/(off - cut),
+// since the expanded coefficients (up to 1e5 for a 0.9 A window) cancel far
+// beyond FP32 precision.
+template <typename U>
+__device__ __forceinline__ U hal_pair(U r2, U rv, U eps, const VdwConst& vc, double& eacc) {
+  const U rik = sqrt(r2);
+  const U ghal = (U)vc.ghal, dhal = (U)vc.dhal;
+  const U rv2 = rv * rv, rv7 = rv2 * rv2 * rv2 * rv;
+  const U rik6 = r2 * r2 * r2;
+  const U rik7 = rik6 * rik;
+  const U rho = rik7 + ghal * rv7;
+  const U tau = (dhal + U(1)) / (rik + dhal * rv);
+  const U tau2 = tau * tau, tau7 = tau2 * tau2 * tau2 * tau;
+  const U dtau = tau / (dhal + U(1));
+  const U q7 = rv7 / rho;
+  const U gtau = eps * tau7 * rik6 * (ghal + U(1)) * q7 * q7;
+  U e = eps * tau7 * rv7 * ((ghal + U(1)) * q7 - U(2));
+  U de = U(-7) * (dtau * e + gtau);
+  if (r2 > (U)vc.cut2) {
+    U taper, dtaper;
+    if constexpr (std::is_same<U, double>::value) {
+      const double rik3 = r2 * rik, rik4 = r2 * r2, rik5 = r2 * rik3;
+      taper = vc.c5 * rik5 + vc.c4 * rik4 + vc.c3 * rik3 + vc.c2 * r2 + vc.c1 * rik + vc.c0;
+      dtaper = 5.0 * vc.c5 * rik4 + 4.0 * vc.c4 * rik3 + 3.0 * vc.c3 * r2 + 2.0 * vc.c2 * rik + vc.c1;
+    } else {
+      const U w = (U)(1.0 / (vc.off - vc.cut));
+      const U t = (rik - (U)vc.cut) * w;
+      const U t2 = t * t;
+      taper = U(1) - t2 * t * (U(10) - U(15) * t + U(6) * t2);
+      dtaper = U(-30) * t2 * (U(1) - t) * (U(1) - t) * w;
+    }
+    de = e * dtaper + de * taper;
+    e = e * taper;
+  }
+  eacc += 0.5 * (double)e;
+  return de / rik;
+}
+
+template <bool MIXED>
 __global__ void __launch_bounds__(kBlock) k_ehal(int n, int npad, Box box, VdwConst vc,
-                                                 const double4* __restrict__ vred, const int2* __restrict__ vinfo,
-                                                 const double* __restrict__ vtab, const int* __restrict__ perm,
-                                                 const int* __restrict__ sp_off, const int* __restrict__ sp_ks,
-                                                 const int* __restrict__ sp_c, const int* __restrict__ vnnb,
-                                                 const int* __restrict__ vnb, unsigned long long* __restrict__ dev,
-                                                 double* __restrict__ epart) {
+                                                 const double4* __restrict__ vred, const float4* __restrict__ vredf,
+                                                 const int2* __restrict__ vinfo, const double* __restrict__ vtab,
+                                                 const int* __restrict__ perm, const int* __restrict__ sp_off,
+                                                 const int* __restrict__ sp_ks, const int* __restrict__ sp_c,
+                                                 const int* __restrict__ vnnb, const int* __restrict__ vnb,
+                                                 unsigned long long* __restrict__ dev, double* __restrict__ epart) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double eacc = 0.0;
   if (i < n) {
     const double4 ri = vred[i];
+    const float4 fi = vredf[i];
+    const float bx = (float)box.l[0], by = (float)box.l[1], bz = (float)box.l[2];
+    const float hx = 0.5f * bx, hy = 0.5f * by, hz = 0.5f * bz;
+    const float off2f = (float)vc.off2;
     const int2 inf = vinfo[i];
     const int it = inf.x;
     const int io = perm[i];
@@ -185,11 +232,28 @@ __global__ void __launch_bounds__(kBlock) k_ehal(int n, int npad, Box box, VdwCo
     for (int s = 0; s < nn; ++s) {
       const int k = knext;
       if (s + 1 < nn) knext = __ldg(vnb + (size_t)(s + 1) * npad + i);
-      const double4 rk = vred[k];
-      double xr = ri.x - rk.x, yr = ri.y - rk.y, zr = ri.z - rk.z;
-      image3(box, xr, yr, zr);
-      const double rik2 = r2_exact(xr, yr, zr);
-      if (rik2 > vc.off2) continue;
+      double xr, yr, zr;
+      float xf = 0.f, yf = 0.f, zf = 0.f, r2f = 0.f;
+      double rik2 = 0.0;
+      if constexpr (MIXED) {
+        const float4 fk = vredf[k];
+        xf = fi.x - fk.x;
+        yf = fi.y - fk.y;
+        zf = fi.z - fk.z;
+        xf = fabsf(xf) > hx ? xf - copysignf(bx, xf) : xf;
+        yf = fabsf(yf) > hy ? yf - copysignf(by, yf) : yf;
+        zf = fabsf(zf) > hz ? zf - copysignf(bz, zf) : zf;
+        r2f = xf * xf + yf * yf + zf * zf;
+        if (r2f > off2f) continue;
+      } else {
+        const double4 rk = vred[k];
+        xr = ri.x - rk.x;
+        yr = ri.y - rk.y;
+        zr = ri.z - rk.z;
+        image3(box, xr, yr, zr);
+        rik2 = r2_exact(xr, yr, zr);
+        if (rik2 > vc.off2) continue;
+      }
       const int kt = __ldg(&vinfo[k].x);
       double vs = 1.0;
       bool is14 = false;
@@ -204,30 +268,17 @@ __global__ void __launch_bounds__(kBlock) k_ehal(int n, int npad, Box box, VdwCo
       const int t = kt * vc.nclass + it;
       const double rv = __ldg(vtab + (is14 ? 2 * nc2 : 0) + t);
       const double eps = __ldg(vtab + (is14 ? 3 * nc2 : nc2) + t) * vs;
-      const double rik = sqrt(rik2);
-      const double rv2 = rv * rv, rv7 = rv2 * rv2 * rv2 * rv;
-      const double rik6 = rik2 * rik2 * rik2;
-      const double rik7 = rik6 * rik;
-      const double rho = rik7 + vc.ghal * rv7;
-      const double tau = (vc.dhal + 1.0) / (rik + vc.dhal * rv);
-      const double tau2 = tau * tau, tau7 = tau2 * tau2 * tau2 * tau;
-      const double dtau = tau / (vc.dhal + 1.0);
-      const double q7 = rv7 / rho;
-      const double gtau = eps * tau7 * rik6 * (vc.ghal + 1.0) * q7 * q7;
-      double e = eps * tau7 * rv7 * ((vc.ghal + 1.0) * q7 - 2.0);
-      double de = -7.0 * (dtau * e + gtau);
-      if (rik2 > vc.cut2) {
-        const double rik3 = rik2 * rik, rik4 = rik2 * rik2, rik5 = rik2 * rik3;
-        const double taper = vc.c5 * rik5 + vc.c4 * rik4 + vc.c3 * rik3 + vc.c2 * rik2 + vc.c1 * rik + vc.c0;
-        const double dtaper = 5.0 * vc.c5 * rik4 + 4.0 * vc.c4 * rik3 + 3.0 * vc.c3 * rik2 + 2.0 * vc.c2 * rik + vc.c1;
-        de = e * dtaper + de * taper;
-        e = e * taper;
+      if constexpr (MIXED) {
+        const float de = hal_pair<float>(r2f, (float)rv, (float)eps, vc, eacc);
+        gx += (double)(de * xf);
+        gy += (double)(de * yf);
+        gz += (double)(de * zf);
+      } else {
+        const double de = hal_pair<double>(rik2, rv, eps, vc, eacc);
+        gx += de * xr;
+        gy += de * yr;
+        gz += de * zr;
       }
-      eacc += 0.5 * e;
-      de = de / rik;
-      gx += de * xr;
-      gy += de * yr;
-      gz += de * zr;
     }
     // the site's force: to the atom (kred) and its parent (1 - kred)
     const int iv = inf.y;
@@ -348,8 +399,13 @@ int launch_ehal(Ctx& c, double* d_out) {
   for (int j = 0; j < 4; ++j) vc.vscale[j] = c.vdw_scale[j];
   vc.vscale[4] = 1.0;
   vc.nclass = c.vdw_nclass;
-  k_ehal<<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vc, c.d_vred, c.d_vinfo, c.d_vtab, c.d_perm, c.d_sp_off,
-                                      c.d_sp_ks, c.d_sp_c, c.d_vnnb, c.d_vnb, dev, c.d_evpart);
+  if (c.mixed)
+    k_ehal<true><<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vc, c.d_vred, c.d_vredf, c.d_vinfo, c.d_vtab, c.d_perm,
+                                              c.d_sp_off, c.d_sp_ks, c.d_sp_c, c.d_vnnb, c.d_vnb, dev, c.d_evpart);
+  else
+    k_ehal<false><<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vc, c.d_vred, c.d_vredf, c.d_vinfo, c.d_vtab,
+                                               c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_c, c.d_vnnb, c.d_vnb, dev,
+                                               c.d_evpart);
   if ((st = cuda_status(cudaGetLastError(), &c, "ehal"))) return st;
   k_sum_partials<<<1, 256, 0, c.stream>>>(nb, c.d_evpart, c.d_ev);
   if ((st = cuda_status(cudaGetLastError(), &c, "ehal energy"))) return st;
