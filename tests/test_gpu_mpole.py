@@ -126,3 +126,62 @@ def test_empole1_needs_frames(lib, thp):
     with pytest.raises(lib.ThpError) as e:
         ctx.empole1()
     assert e.value.status == lib.THP_E_STATE
+
+
+def _with_extra_14_15(ws, rng):
+    """The box with artificial 1-4 and 1-5 relations between oxygens of
+    nearby molecules (symmetric), so the m4/m5 scales and the vdW 1-4
+    parameters take part (water itself has only 1-2 and 1-3 pairs)."""
+    import dataclasses
+    pos = ws.positions()
+    L = np.asarray(ws.box)
+    ox = np.arange(0, ws.n, 3)
+    rows14 = [[] for _ in range(ws.n)]
+    rows15 = [[] for _ in range(ws.n)]
+    for a in ox[: len(ox) // 2]:
+        d = pos[ox] - pos[a]
+        d -= L * np.round(d / L)
+        r = np.sqrt(np.einsum("ij,ij->i", d, d))
+        near = [int(b) for b in ox[np.argsort(r)[1:3]]]
+        for rows, b in ((rows14, near[0]), (rows15, near[1])):
+            if b not in rows[a] and b not in rows14[a] and b not in rows15[a]:
+                rows[a].append(b)
+                rows[b].append(a)
+
+    def csr(rows):
+        off = np.zeros(ws.n + 1, np.int32)
+        off[1:] = np.cumsum([len(r) for r in rows])
+        return off, np.array([v for r in rows for v in sorted(r)], dtype=np.int32)
+
+    conn = dict(ws.conn)
+    conn["i14"], conn["i15"] = csr(rows14), csr(rows15)
+    v = dict(ws.vdw)
+    v["radmin4"] = np.asarray(v["radmin"]) * 0.9
+    v["eps4"] = np.asarray(v["eps"]) * 0.5
+    v["v_scale"] = (0.0, 0.0, 0.7, 0.9)
+    sc = dict(ws.scales)
+    sc["m_scale"] = (0.0, 0.0, 0.4, 0.8)
+    return dataclasses.replace(ws, conn=conn, vdw=v, scales=sc)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_scaled_14_15_pairs_match_oracle(lib, thp, precision):
+    ws = _with_extra_14_15(thp.water.make_water_box(648, cfg=0), np.random.default_rng(2))
+    orc = O.Oracle(ws)
+    assert orc.mlistcell()[0] == 0
+    em_ref, dem_ref, parts = orc.empole1()
+    ev_ref, dev_ref = orc.ehal1()
+    ctx = lib.Context(ws, precision=lib.FP64 if precision == "fp64" else lib.MIXED)
+    em, dem = ctx.empole1()
+    ev, dev = ctx.ehal1()
+    if precision == "fp64":
+        assert abs(em - em_ref) < 1e-12 * parts_scale(parts), (em, em_ref)
+        assert rel(dem, dem_ref) < 1e-9
+        assert abs(ev - ev_ref) < 1e-10 * abs(ev_ref), (ev, ev_ref)
+        assert rel(dev, dev_ref) < 1e-9
+    else:
+        assert abs(em - em_ref) < 1e-8 * parts_scale(parts), (em, em_ref)
+        assert abs(ev - ev_ref) < 1e-5 * abs(ev_ref), (ev, ev_ref)
+    # and the scaled pairs matter: the unmodified box gives other energies
+    base = lib.Context(thp.water.make_water_box(648, cfg=0))
+    assert abs(base.empole1()[0] - em_ref) > 1e-3 and abs(base.ehal1()[0] - ev_ref) > 1e-3
