@@ -1081,7 +1081,10 @@ int thp_ehal1(thp_ctx* h, double* ev, double* dev) {
   double e = 0.0;
   cudaMemcpyAsync(&e, c.d_ev, sizeof(double), cudaMemcpyDeviceToHost, c.stream);
   if (dev) cudaMemcpyAsync(dev, c.d_grad, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost, c.stream);
-  if ((st = check_flags(h))) return st;  // synchronises the stream
+  if ((st = check_flags(h))) {  // synchronises the stream
+    c.have_vlist = false;       // a list that overflowed is not kept
+    return st;
+  }
   if (!std::isfinite(e)) return THP_E_NAN;
   if (ev) *ev = e;
   return THP_OK;
@@ -1511,6 +1514,7 @@ int thp_get_vlist(thp_ctx* h, int maxvlst, int* nvlst, int* vlst) {
     cudaMemcpyAsync(nvlst, dn, sizeof(int) * c.n, cudaMemcpyDeviceToHost, c.stream);
     cudaMemcpyAsync(vlst, de, sizeof(int) * (size_t)c.n * maxvlst, cudaMemcpyDeviceToHost, c.stream);
     st = check_flags(h);
+    if (st) c.have_vlist = false;  // the device list may have overflowed too
   }
   cudaFree(dn);
   cudaFree(de);
