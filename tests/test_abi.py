@@ -19,8 +19,9 @@ def declared_functions():
 def test_header_declares_reference_dropins():
     names = declared_functions()
     for f in ("newinduce_pme2_", "inducepcg_pme2_", "tmatxb_pme_", "efld0_direct_", "efld0_recip_",
-              "tmatxbrecip_", "mlistcell_", "vlistcell_", "epolar_", "thp_solve", "thp_ctx_create"):
-        assert f in names
+              "tmatxbrecip_", "mlistcell_", "vlistcell_", "epolar_", "epolar1_", "empole1_", "ehal1_",
+              "thp_solve", "thp_ctx_create", "thp_empole1", "thp_ehal1", "thp_set_vdw", "thp_get_vlist"):
+        assert f in names, f
 
 
 def test_library_exports_every_declared_symbol(thp):
