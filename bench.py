@@ -13,6 +13,7 @@ Contract: one JSON line on rank 0.  N>1 (torchrun): independent replicas, one
 box per GPU (weak scaling), time = max over ranks.
 """
 import argparse
+import math
 import json
 import os
 import subprocess
@@ -359,6 +360,48 @@ def empole_run(lib, ws, reps=10):
     return out
 
 
+def solve_roofline(n, nfft, n_it, ms_mixed, hbm_gbs, ms_fp64=None):
+    """Whole-solve roofline of the polarization path from the per-unit work
+    table of the path (flops and bytes per atom, per list entry, per
+    interacting pair, per grid point):
+      W = a6 + a11 + a4 + a10 + (n_it + 1) (a3 + a5 + CG),
+    roofline time = sum over the terms of max(bytes / HBM, flops / FLOP peak),
+    achieved = roofline time / measured time.  Pair and list counts use the
+    water-box constants P = 71.8 N interacting half-pairs and L = 88.4 N list
+    half-entries (7.0 / 7.5 A); candidates of the list build 712 per atom.
+    The HBM peak is measured; the FP32 / FP64 vector FLOP peaks are nominal
+    (75 / 37 TFLOP/s), as none is measured here.  The mixed form halves the
+    per-atom and grid bytes (not the list)."""
+    K3 = float(nfft[0] * nfft[1] * nfft[2])
+    P, L = 71.8 * n, 88.4 * n
+    log2k3 = math.log2(K3)
+
+    def terms(mixed):
+        h = 0.5 if mixed else 1.0
+        return {
+            "a3_matvec_real": (120.0 * P, h * 136.0 * n + 4.0 * L),
+            "a5_matvec_recip": (3500.0 * n + 10.0 * K3 * log2k3 + 6.0 * K3, h * (128.0 * K3 + 96.0 * n)),
+            "cg_vectors": (60.0 * n, h * 624.0 * n),
+            "a4_efld0_direct": (220.0 * P, h * 184.0 * n + 4.0 * L),
+            "a10_efld0_recip": (3500.0 * n + 10.0 * K3 * log2k3 + 6.0 * K3, h * (128.0 * K3 + 96.0 * n)),
+            "a6_bsplines": (300.0 * n, h * 504.0 * n),
+            "a11_list": (30.0 * 712.0 * n, 24.0 * n + 4.0 * L),
+        }
+
+    out = {"n_it": n_it, "hbm_gbs": hbm_gbs, "flop_peaks_tflops": {"fp32": 75.0, "fp64": 37.0},
+           "flop_peak_kind": "nominal", "hbm_kind": "measured"}
+    for name, mixed, ms in (("mixed", True, ms_mixed), ("fp64", False, ms_fp64)):
+        if ms is None or not hbm_gbs:
+            continue
+        fpk = (75.0 if mixed else 37.0) * 1e12
+        t = 0.0
+        for key, (fl, by) in terms(mixed).items():
+            reps = (n_it + 1) if key in ("a3_matvec_real", "a5_matvec_recip", "cg_vectors") else 1
+            t += reps * max(by / (hbm_gbs * 1e9), fl / fpk)
+        out[name] = {"roofline_ms": t * 1e3, "measured_ms": ms, "achieved": t * 1e3 / ms}
+    return out
+
+
 def ehal_run(lib, ws, reps=10):
     """Buffered 14-7 van der Waals energy and gradient (ehal1c) of the box,
     FP64 and mixed: wall time per call through the C-ABI with the vdW list in
@@ -556,6 +599,9 @@ def main():
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, 96k-atom capture scaled by n",
             "avg_launch_ms": avg_ms, "launches": mv_launches, "alg_bytes_per_launch": alg_bytes}
 
+    solve_roof = solve_roofline(n, ws.nfft, int(np.median(niter)), t_mixed / args.steps, peaks.get("hbm_gbs"),
+                                fp64_line["ms_per_step"] if fp64_line else None)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -612,7 +658,7 @@ def main():
         "speedup_mixed_vs_fp64": (value / fp64_line["value"]) if fp64_line else None,
         "e2e": {"value": world * e2e_steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "host_buffers": "pinned (positions, rpole in; uind, uinp out)"},
-        "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+        "roofline": roof, "solve_roofline": solve_roof, "cpu_baseline": cpu, "clocks": clk,
         "gpu_launches": None,
     }
     # kernels of this library per timed step (cuFFT's not counted): rotpole 1;
