@@ -144,3 +144,34 @@ def test_vlistcell_dropin_fills_the_vdw_list(lib, thp):
     got = got[np.lexsort((got[:, 1], got[:, 0]))]
     ref = _vdw_pairs_bruteforce(ws)
     assert np.array_equal(got, ref[np.lexsort((ref[:, 1], ref[:, 0]))])
+
+
+def test_retargeted_context_and_shared_buffers(lib, thp):
+    # one context re-targeted from a small box to a larger one (the buffers
+    # sized by n are regrown) and then to a mid-size one (they are reused):
+    # the results follow the oracle; the polarization gradient is unchanged
+    # by interleaved empole1/ehal1 calls (they share the gradient buffers)
+    small = thp.water.make_water_box(648, cfg=0)
+    big = thp.water.make_water_box(10800, cfg=1)
+    mid = thp.water.make_water_box(4000, cfg=0)
+    ctx = lib.Context(small)
+    ctx.ehal1()
+    ctx.empole1()
+    for ws in (big, mid):
+        ctx.retarget(ws)
+        orc = O.Oracle(ws)
+        assert orc.mlistcell()[0] == 0
+        ev, dev = ctx.ehal1()
+        ev_ref, dev_ref = orc.ehal1()
+        assert abs(ev - ev_ref) < 1e-10 * abs(ev_ref), (ws.n, ev, ev_ref)
+        assert rel(dev, dev_ref) < 1e-9
+        em, dem = ctx.empole1()
+        em_ref, dem_ref, parts = orc.empole1()
+        assert abs(em - em_ref) < 1e-12 * sum(abs(p) for p in parts), (ws.n, em, em_ref)
+        assert rel(dem, dem_ref) < 1e-9
+    assert ctx.solve()["converged"]
+    ep0, g0 = ctx.gradient()
+    ctx.empole1()
+    ctx.ehal1()
+    ep1, g1 = ctx.gradient()
+    assert ep0 == ep1 and np.array_equal(g0, g1)

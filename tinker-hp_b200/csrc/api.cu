@@ -23,6 +23,7 @@ struct thp_ctx {
   bool field_valid = false;   // d_ef holds E0 for the current positions
   bool guess_uploaded = false;
   bool solved_once = false;
+  bool rpole_current = false;  // rotpole has run for the current positions and frames
 };
 
 namespace thp {
@@ -309,11 +310,12 @@ int ensure_list(thp_ctx* h, bool force_rebuild) {
 
 int ensure_rpole(thp_ctx* h) {
   Ctx& c = h->c;
-  if (c.have_frames) {
+  if (c.have_frames && !h->rpole_current) {  // the same positions rotate to the same multipoles
     int st = launch_rotpole(c);
     if (st) return st;
     c.have_rpole = true;
     h->rpole_dirty = true;
+    h->rpole_current = true;
   }
   return c.have_rpole ? THP_OK : THP_E_STATE;
 }
@@ -604,6 +606,7 @@ static int clear_system_state(thp_ctx* h) {
   c.have_perm = c.have_list = c.have_coef = c.have_dipoles = c.have_ef_prev = false;
   c.pred_mode = c.nualt = c.alt_head = 0;
   h->pos_dirty = h->rpole_dirty = true;
+  h->rpole_current = false;
   h->field_valid = h->guess_uploaded = h->solved_once = false;
   c.bx = c.by = c.bz = c.brpole = c.buind = c.buinp = c.bep = c.bdep = c.bqgrid = nullptr;
   c.bem = c.bdem = c.bev = c.bdev = nullptr;
@@ -727,6 +730,7 @@ int thp_set_params(thp_ctx* h, const double* polarity, const double* thole, cons
   cudaMemcpyAsync(c.d_par_orig + 2 * n, polarity, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
   c.have_params = true;
   h->pos_dirty = true;
+  h->rpole_current = false;
   c.have_coef = false;
   h->field_valid = false;
   return cuda_status(cudaStreamSynchronize(c.stream), &c, "set params");
@@ -869,10 +873,12 @@ int image_load(thp_ctx* h, const SystemImage* img) {
   cudaMemcpyAsync(c.d_pole_local, img->pole, sizeof(double) * 13 * n, cudaMemcpyHostToDevice, c.stream);
   cudaMemcpyAsync(c.d_frames, img->frames, sizeof(int) * 3 * n, cudaMemcpyHostToDevice, c.stream);
   c.have_frames = true;
+  h->rpole_current = false;
   c.have_axes = true;
   c.have_list = false;
   c.have_coef = false;
   h->pos_dirty = true;
+  h->rpole_current = false;
   h->rpole_dirty = true;
   h->field_valid = false;
   return cuda_status(cudaGetLastError(), &c, "load system");
@@ -891,6 +897,7 @@ int upload_positions(thp_ctx* h, const double* x, const double* y, const double*
   cudaMemcpyAsync(c.d_xyz_orig + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream);
   c.have_pos = true;
   h->pos_dirty = true;
+  h->rpole_current = false;
   h->field_valid = false;
   c.have_coef = false;
   if (c.have_frames) h->rpole_dirty = true;
@@ -933,6 +940,7 @@ int thp_set_frames(thp_ctx* h, const double* pole, const int* zaxis, const int* 
   cudaMemcpy(c.d_pole_local, pole, sizeof(double) * 13 * n, cudaMemcpyHostToDevice);
   cudaMemcpy(c.d_frames, fr.data(), sizeof(int) * 3 * n, cudaMemcpyHostToDevice);
   c.have_frames = true;
+  h->rpole_current = false;
   c.have_axes = true;
   h->rpole_dirty = true;
   h->field_valid = false;
@@ -1159,6 +1167,7 @@ static int solve_front_eager(thp_ctx* h, int guess) {
   if (c.have_frames) {
     if ((st = launch_rotpole(c))) return st;
     c.have_rpole = true;
+    h->rpole_current = true;
   }
   if ((st = launch_sort_atoms(c))) return st;
   if ((st = launch_gather_sorted(c))) return st;
@@ -1207,7 +1216,7 @@ static int solve_front_async(thp_ctx* h, int guess) {
     cudaGraphDestroy(g);
   }
   // the host-side state the front leaves behind
-  if (c.have_frames) c.have_rpole = true;
+  if (c.have_frames) c.have_rpole = h->rpole_current = true;
   c.have_perm = c.have_list = true;
   h->pos_dirty = h->rpole_dirty = false;
   h->field_valid = true;
@@ -1420,6 +1429,7 @@ int thp_md_verlet(thp_ctx* h, int nsteps, double dt, const double* mass, double*
     if ((st = launch_kick(c, 0.5 * dt, d_mass, d_grad, d_vel))) break;
     if ((st = launch_drift(c, dt, d_vel))) break;
     h->pos_dirty = true;
+    h->rpole_current = false;
     h->field_valid = false;
     c.have_coef = false;
     if (c.have_frames) h->rpole_dirty = true;
