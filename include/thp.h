@@ -176,7 +176,9 @@ int thp_set_mpole_scales(thp_ctx* ctx, const double* m);
 /* Permanent-multipole energy and gradient, empole1c (empole1.f:42-340):
  * emrecip1 (:349), emreal1c (:873, standard branch, mscale), the Ewald self
  * energy (:134-160) and torque (torque.f:6), TINFOIL boundary, at the current
- * positions and multipoles (rotpole on the device when frames are set).
+ * positions and multipoles (rotpole on the device when frames are set, once per
+ * change of the positions or frames, so a call between a solve and its
+ * gradient leaves the solve valid).  No virial.
  * em (kcal/mol) and dem [n][3] (kcal/mol/A, original order; either may be
  * NULL).  Needs frames (thp_set_frames) and connectivity; THP_E_STATE
  * otherwise.  The list is built or reused as for a solve.  The mixed form
