@@ -2270,16 +2270,19 @@ int or_ehal1(OrCtx* c, const OrVdw* v, double* dev, double* ev_out) {
   std::vector<int> iv14((size_t)n, -1);
   const int slot[4] = {OR_I12, OR_I13, OR_I14, OR_I15};
   double ev = 0.0;
+  auto vdw_site = [&](int a) { return v->radmin[v->cls[a] * nc + v->cls[a]] != 0.0; };  // kvdw.f:592-598
   for (int i = 0; i < n; ++i) {
     const int iv = v->ired[i];
     const double redi = v->kred[i], rediv = 1.0 - redi;
     const int it = v->cls[i];
+    if (!vdw_site(i)) continue;
     for (int b = 0; b < 4; ++b)
       for_conn(s, slot[b], i, [&](int k) {
         vscale[k] = v->v_scale[b];
         if (b == 2) iv14[k] = i;
       });
     for (int k = i + 1; k < n; ++k) {
+      if (!vdw_site(k)) continue;  // vlistcell skips partners without a radius
       double xd = xr[i] - xr[k], yd = yr[i] - yr[k], zd = zr[i] - zr[k];
       image(c->cell, xd, yd, zd);
       const double rik2 = xd * xd + yd * yd + zd * zd;

@@ -175,3 +175,25 @@ def test_retargeted_context_and_shared_buffers(lib, thp):
     ctx.ehal1()
     ep1, g1 = ctx.gradient()
     assert ep0 == ep1 and np.array_equal(g0, g1)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_sites_without_radius_take_no_part(lib, thp, precision):
+    # hydrogens without a vdW radius are not vdW sites (kvdw.f:592-598), even
+    # though the cubic-mean rule gives their pairs with oxygen a nonzero Rmin
+    ws = thp.water.make_water_box(648, cfg=0)
+    P = thp.params
+    rad = [P.WATER_VDW["O"][0], 0.0]
+    eps = [P.WATER_VDW["O"][1], P.WATER_VDW["H"][1]]
+    radmin, epsm, radmin4, eps4 = P.vdw_pair_tables(rad, eps)
+    v = dict(ws.vdw, radmin=np.array(radmin), eps=np.array(epsm), radmin4=np.array(radmin4), eps4=np.array(eps4))
+    assert v["radmin"][0][1] > 0.0
+    w2 = dataclasses.replace(ws, vdw=v)
+    ev_ref, dev_ref = O.Oracle(w2).ehal1()
+    ev_oo, _ = O.Oracle(dataclasses.replace(ws, vdw=dict(v, kred=np.zeros(ws.n)))).ehal1()
+    assert abs(ev_ref - ev_oo) < 1e-9 * abs(ev_oo)  # only O-O pairs remain, whatever the H reduction
+    ctx = lib.Context(w2, precision=lib.FP64 if precision == "fp64" else lib.MIXED)
+    ev, dev = ctx.ehal1()
+    tol = 1e-10 if precision == "fp64" else 1e-5
+    assert abs(ev - ev_ref) < tol * abs(ev_ref), (ev, ev_ref)
+    assert np.abs(dev[1::3]).max() == 0.0 and np.abs(dev[2::3]).max() == 0.0  # no force on the H atoms

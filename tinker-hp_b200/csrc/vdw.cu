@@ -81,13 +81,21 @@ __device__ __forceinline__ int axis_cell(int c, int nc, int w, int q) {
 // reduced minimum-image distance is within vbuf (both directions)
 __global__ void __launch_bounds__(kBlock) k_vdw_list(int n, int npad, Box box, double vbuf2, int prefilter, float lo,
                                                      float hi, int wx, int wy, int wz, const double4* __restrict__ vred,
-                                                     const float4* __restrict__ vredf, const int* __restrict__ scell,
+                                                     const float4* __restrict__ vredf, const int2* __restrict__ vinfo,
+                                                     const double* __restrict__ vtab, int nclass,
+                                                     const int* __restrict__ scell,
                                                      const int* __restrict__ cell_start,
                                                      const int* __restrict__ cell_count, int ncx, int ncy, int ncz,
                                                      int maxvnb, int* __restrict__ vnnb, int* __restrict__ vnb,
                                                      int* __restrict__ flags) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  // sites of a class without a vdW radius take no part (kvdw.f:592-598:
+  // they are not vdW sites; vlistcell skips them as partners)
+  if (__ldg(vtab + (size_t)vinfo[i].x * (nclass + 1)) == 0.0) {
+    vnnb[i] = 0;
+    return;
+  }
   const double4 ri = vred[i];
   const float4 fi = vredf[i];
   const float bx = (float)box.l[0], by = (float)box.l[1], bz = (float)box.l[2];
@@ -151,6 +159,7 @@ __global__ void __launch_bounds__(kBlock) k_vdw_list(int n, int npad, Box box, d
             image3(box, xr, yr, zr);
             take = r2_exact(xr, yr, zr) <= vbuf2;
           }
+          if (take && __ldg(vtab + (size_t)__ldg(&vinfo[k].x) * (nclass + 1)) == 0.0) take = false;
           if (take) {
             if (cnt < maxvnb) vnb[(size_t)cnt * npad + i] = k;
             ++cnt;
@@ -353,7 +362,7 @@ int launch_vdw_list(Ctx& c) {
   const double band = std::max(1e-5, 2.0 * (2.0 * vbuf * dr + dr * dr) / vbuf2);
   const float lo = (float)(vbuf2 * (1.0 - band)), hi = (float)(vbuf2 * (1.0 + band));
   k_vdw_list<<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vbuf2, prefilter, lo, hi, w[0], w[1], w[2], c.d_vred,
-                                          c.d_vredf, c.d_scell,
+                                          c.d_vredf, c.d_vinfo, c.d_vtab, c.vdw_nclass, c.d_scell,
                                           c.d_cell_start, c.d_cell_count, c.nc[0], c.nc[1], c.nc[2], c.maxvnb, c.d_vnnb,
                                           c.d_vnb, c.d_flags);
   if ((st = cuda_status(cudaGetLastError(), &c, "vdw list"))) return st;
