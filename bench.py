@@ -402,6 +402,41 @@ def solve_roofline(n, nfft, n_it, ms_mixed, hbm_gbs, ms_fp64=None):
     return out
 
 
+def nonbonded_run(lib, ws, reps=10, perturb=0.01, seed=5021):
+    """All the AMOEBA non-bonded terms built here, per step as in dynamics:
+    new positions (a 0.01 A RMS displacement of the box), a polarization
+    solve warm-started from the previous dipoles, its gradient, the
+    permanent-multipole and the van der Waals energies and gradients (mixed
+    form; gradients into pinned host arrays).  Wall time per step."""
+    import torch
+    rng = np.random.default_rng(seed)
+    ctx = lib.Context(ws, precision=lib.MIXED, poleps=CG_TOL)
+    pin = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64).pin_memory().numpy()
+    g = torch.empty((ws.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    pos0 = ws.positions()
+    frames = [[pin(p[:, 0]), pin(p[:, 1]), pin(p[:, 2])]
+              for p in (pos0 + rng.normal(0.0, perturb, pos0.shape) for _ in range(reps + 2))]
+    iters = []
+
+    def step(f):
+        ctx.set_positions(*f)
+        r = ctx.solve(lib.GUESS_PREVIOUS)
+        ctx.gradient(out=g)
+        ctx.empole1(out=g)
+        ctx.ehal1(out=g)
+        return r["niter"]
+
+    step(frames[0])
+    step(frames[1])
+    t0 = time.perf_counter()
+    for f in frames[2:]:
+        iters.append(step(f))
+    dt = (time.perf_counter() - t0) / reps
+    ctx.close()
+    return {"ms_per_step": dt * 1e3, "mean_iters": float(np.mean(iters)), "atoms": ws.n,
+            "terms": "polarization solve (warm) + gradient, empole1, ehal1; mixed form"}
+
+
 def ehal_run(lib, ws, reps=10):
     """Buffered 14-7 van der Waals energy and gradient (ehal1c) of the box,
     FP64 and mixed: wall time per call through the C-ABI with the vdW list in
@@ -631,6 +666,7 @@ def main():
         extras["md_config1"] = {"previous": md_run(lib, thp), "aspc": md_run(lib, thp, predictor="ASPC")}
         extras["empole1"] = empole_run(lib, ws)
         extras["ehal1"] = ehal_run(lib, ws)
+        extras["nonbonded_step"] = nonbonded_run(lib, ws)
         if fp64 is not None:
             best = max(b2["solves_per_s"], b4["solves_per_s"])
             plain64 = world * len(lat64) / (t64 / 1000.0)

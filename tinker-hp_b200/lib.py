@@ -339,9 +339,11 @@ class Context:
         self._check(load().thp_get_dipoles(self.h, _p(uind), _p(uinp)), "thp_get_dipoles")
         return uind, uinp
 
-    def gradient(self):
-        """(Epol, dEpol/dx [n,3] kcal/mol/A) for the dipoles of the last solve."""
-        dep = np.zeros((self.n, 3))
+    def gradient(self, out=None):
+        """(Epol, dEpol/dx [n,3] kcal/mol/A) for the dipoles of the last solve;
+        `out` (a C-contiguous float64 [n,3] array, e.g. pinned) receives it."""
+        dep = np.zeros((self.n, 3)) if out is None else out
+        assert dep.shape == (self.n, 3) and dep.dtype == np.float64 and dep.flags["C_CONTIGUOUS"]
         ep = C.c_double()
         self._check(load().thp_get_gradient(self.h, _p(dep), C.byref(ep)), "thp_get_gradient")
         return ep.value, dep
