@@ -388,7 +388,7 @@ void free_ctx(Ctx& c) {
   void* ptrs[] = {c.slab_cells, c.slab_atoms, c.slab_pairs, c.d_sp_off, c.d_sp_k, c.d_sp_ks, c.d_sp_s, c.d_sp_c,
                   c.d_cg, c.d_flags, c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad, c.d_sgrid, c.d_sscratch,
                   c.d_alt, c.d_empart, c.d_vcls, c.d_vired, c.d_vkred, c.d_vtab, c.d_vred, c.d_vinfo,
-                  c.d_evpart, c.d_vnb, c.d_vnnb, c.d_vpos_built, c.d_vredf};
+                  c.d_evpart, c.d_vnb, c.d_vnnb, c.d_vpos_built, c.d_vredf, c.d_muf};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   pme_free(c);
@@ -560,7 +560,8 @@ static int size_buffers(Ctx& c) {
     c.slab_atoms = nullptr;
     // buffers made on first use are sized by n as well
     free_all(&c.d_fphirec, &c.d_depfix, &c.d_trq, &c.d_frs, &c.d_grad, &c.d_empart, &c.d_vcls, &c.d_vired,
-             &c.d_vkred, &c.d_vred, &c.d_vredf, &c.d_vinfo, &c.d_evpart, &c.d_vnb, &c.d_vnnb, &c.d_vpos_built);
+             &c.d_vkred, &c.d_vred, &c.d_vredf, &c.d_vinfo, &c.d_evpart, &c.d_vnb, &c.d_vnnb, &c.d_vpos_built,
+             &c.d_muf);
     c.have_vlist = false;
     c.d_em = c.d_ev = nullptr;
     c.have_vdw = false;

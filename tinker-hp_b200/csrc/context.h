@@ -123,6 +123,7 @@ struct Ctx {
   double* d_vtab = nullptr;
   double4* d_vred = nullptr;
   float4* d_vredf = nullptr;      // the same sites wrapped into the box, FP32 (list screen)
+  float* d_muf = nullptr;         // [n][8] FP32 sorted dipoles for the mixed gradient pass
   int2* d_vinfo = nullptr;
   // vdW pair list (vlistcell): full list within vdwcut + lbuffer of the
   // reduced sites, slot-major [s*npad + i], rebuilt after a re-sort or when an

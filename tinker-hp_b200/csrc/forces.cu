@@ -20,6 +20,7 @@
 #include "grad_dev.cuh"
 #include "kernels.h"
 #include "pme_dev.cuh"
+#include "realspace_dev.cuh"
 
 namespace thp {
 
@@ -196,23 +197,51 @@ __global__ void __launch_bounds__(kBlock) k_fphi_mpole20(int n, PmeGeom g, const
   for (int q = 0; q < 20; ++q) f[q] = (double)S[q];
 }
 
+// sorted dipoles [n][6] FP64 -> [n][8] FP32 (d xyz, p xyz, 2 pad): one
+// 256-bit load per partner in the mixed pair pass
+__global__ void k_mu_f32(int n, const double* __restrict__ mu, float* __restrict__ muf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4* o = reinterpret_cast<float4*>(muf + (size_t)i * 8);
+  const double* m = mu + (size_t)i * 6;
+  o[0] = make_float4((float)m[0], (float)m[1], (float)m[2], (float)m[3]);
+  o[1] = make_float4((float)m[4], (float)m[5], 0.f, 0.f);
+}
+
 struct EwC {
   double a, f1, f2, f3, f4;  // 2 a^2 powers / (sqrt(pi) a) of dampewald order 9
 };
 
 // epreal1c pair terms seen from atom i over its full list, the self torque,
 // and the torque distribution of the summed torque of site i.
+// resident blocks of the mixed gradient pass the register budget is cut for
+#ifndef THP_FORCE_MINB
+#define THP_FORCE_MINB 4
+#endif
+
 template <bool MIXED>
-__global__ void __launch_bounds__(kBlock) k_force_real(
+__global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_real(
     int n, int npad, Box box, double off2, EwC ew, const double4* __restrict__ pos,
     const typename std::conditional<MIXED, float, double>::type* __restrict__ mrec, const double* __restrict__ mu,
-    const int* __restrict__ perm, const int* __restrict__ sp_off, const int* __restrict__ sp_ks,
-    const double* __restrict__ sp_s, const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb,
-    const int* __restrict__ frs, const double* __restrict__ trq_recip, unsigned long long* __restrict__ dep) {
+    const float* __restrict__ erec, const float* __restrict__ muf, const int* __restrict__ perm,
+    const int* __restrict__ sp_off, const int* __restrict__ sp_ks, const double* __restrict__ sp_s,
+    const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb, const int* __restrict__ frs,
+    const double* __restrict__ trq_recip, unsigned long long* __restrict__ dep) {
   using T = typename std::conditional<MIXED, float, double>::type;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 pi4 = pos[i];
+  // mixed form: partners from the 64-B FP32 site record (wrapped position,
+  // 1/pdamp, thole, multipoles) and the FP32 dipole record, imaged in FP32
+  float xi = 0.f, yi = 0.f, zi = 0.f;
+  if constexpr (MIXED) {
+    xi = erec[(size_t)i * 16 + 0];
+    yi = erec[(size_t)i * 16 + 1];
+    zi = erec[(size_t)i * 16 + 2];
+  }
+  const float bxf = (float)box.l[0], byf = (float)box.l[1], bzf = (float)box.l[2];
+  const float hxf = 0.5f * bxf, hyf = 0.5f * byf, hzf = 0.5f * bzf;
+  const float off2f = (float)off2;
   const T* ri = mrec + (size_t)i * 12;
   const T pti = (T)ri[0], ci = (T)ri[1], dix = (T)ri[2], diy = (T)ri[3], diz = (T)ri[4];
   const T qixx = (T)ri[5], qixy = (T)ri[6], qixz = (T)ri[7], qiyy = (T)ri[8], qiyz = (T)ri[9], qizz = (T)ri[10];
@@ -228,11 +257,74 @@ __global__ void __launch_bounds__(kBlock) k_force_real(
 #pragma unroll 1
   for (int s = 0; s < nn; ++s) {
     const int k = __ldg(nb + (size_t)s * npad + i);
-    const double4 pk4 = pos[k];
-    double xrd = pk4.x - pi4.x, yrd = pk4.y - pi4.y, zrd = pk4.z - pi4.z;
-    image3(box, xrd, yrd, zrd);
-    const double r2d = r2_exact(xrd, yrd, zrd);
-    if (r2d > off2) continue;
+    T xr, yr, zr, r2, pdk;
+    T ptk, ck, dkx, dky, dkz, qkxx, qkxy, qkxz, qkyy, qkyz, qkzz;
+    T ukx, uky, ukz, ukxp, ukyp, ukzp;
+    if constexpr (MIXED) {
+      float v[16];
+      ld_rec8(erec + (size_t)k * 16, *reinterpret_cast<float(*)[8]>(&v[0]));
+      float x = v[0] - xi, y = v[1] - yi, z = v[2] - zi;
+      x = fabsf(x) > hxf ? x - copysignf(bxf, x) : x;
+      y = fabsf(y) > hyf ? y - copysignf(byf, y) : y;
+      z = fabsf(z) > hzf ? z - copysignf(bzf, z) : z;
+      const float rf2 = x * x + y * y + z * z;
+      if (rf2 > off2f) continue;
+      ld_rec8(erec + (size_t)k * 16 + 8, *reinterpret_cast<float(*)[8]>(&v[8]));
+      float u[8];
+      ld_rec8(muf + (size_t)k * 8, u);
+      xr = x;
+      yr = y;
+      zr = z;
+      r2 = rf2;
+      pdk = v[3] != 0.f ? 1.f / v[3] : 0.f;
+      ptk = v[4];
+      ck = v[5];
+      dkx = v[6];
+      dky = v[7];
+      dkz = v[8];
+      qkxx = v[9];
+      qkxy = v[10];
+      qkxz = v[11];
+      qkyy = v[12];
+      qkyz = v[13];
+      qkzz = v[14];
+      ukx = u[0];
+      uky = u[1];
+      ukz = u[2];
+      ukxp = u[3];
+      ukyp = u[4];
+      ukzp = u[5];
+    } else {
+      const double4 pk4 = pos[k];
+      double xrd = pk4.x - pi4.x, yrd = pk4.y - pi4.y, zrd = pk4.z - pi4.z;
+      image3(box, xrd, yrd, zrd);
+      const double r2d = r2_exact(xrd, yrd, zrd);
+      if (r2d > off2) continue;
+      xr = (T)xrd;
+      yr = (T)yrd;
+      zr = (T)zrd;
+      r2 = (T)r2d;
+      pdk = (T)pk4.w;
+      const T* rk = mrec + (size_t)k * 12;
+      ptk = (T)rk[0];
+      ck = (T)rk[1];
+      dkx = (T)rk[2];
+      dky = (T)rk[3];
+      dkz = (T)rk[4];
+      qkxx = (T)rk[5];
+      qkxy = (T)rk[6];
+      qkxz = (T)rk[7];
+      qkyy = (T)rk[8];
+      qkyz = (T)rk[9];
+      qkzz = (T)rk[10];
+      const double* mk = mu + (size_t)k * 6;
+      ukx = (T)mk[0];
+      uky = (T)mk[1];
+      ukz = (T)mk[2];
+      ukxp = (T)mk[3];
+      ukyp = (T)mk[4];
+      ukzp = (T)mk[5];
+    }
     T ds = 1, ps = 1, us = 1;
     for (int q = s0; q < s1; ++q)
       if (__ldg(sp_ks + q) == k) {
@@ -241,12 +333,6 @@ __global__ void __launch_bounds__(kBlock) k_force_real(
         us = (T)sp_s[3 * q + 2];
         break;
       }
-    const T* rk = mrec + (size_t)k * 12;
-    const T ptk = (T)rk[0], ck = (T)rk[1], dkx = (T)rk[2], dky = (T)rk[3], dkz = (T)rk[4];
-    const T qkxx = (T)rk[5], qkxy = (T)rk[6], qkxz = (T)rk[7], qkyy = (T)rk[8], qkyz = (T)rk[9], qkzz = (T)rk[10];
-    const double* mk = mu + (size_t)k * 6;
-    const T ukx = (T)mk[0], uky = (T)mk[1], ukz = (T)mk[2], ukxp = (T)mk[3], ukyp = (T)mk[4], ukzp = (T)mk[5];
-    const T xr = (T)xrd, yr = (T)yrd, zr = (T)zrd, r2 = (T)r2d;
     const T r = sqrt(r2);
     const T dir = dix * xr + diy * yr + diz * zr;
     const T qix = qixx * xr + qixy * yr + qixz * zr, qiy = qixy * xr + qiyy * yr + qiyz * zr,
@@ -269,7 +355,7 @@ __global__ void __launch_bounds__(kBlock) k_force_real(
     // Thole factors and their r-derivatives (epolar1.f:1620-1660)
     T sc3 = 1, sc5 = 1, sc7 = 1, rc3[3] = {0, 0, 0}, rc5[3] = {0, 0, 0}, rc7[3] = {0, 0, 0};
     T l3d = 1, l5d = 1, l7d = 1;  // damptholed order 7 for the energy-field (same values)
-    T damp = pdi * (T)pk4.w;
+    T damp = pdi * pdk;
     T pg = min(pti, ptk);
     if (pg == T(0)) pg = max(pti, ptk);
     if (damp != T(0) && pg != T(0)) {
@@ -521,9 +607,14 @@ int launch_forces(Ctx& c, double* d_out) {
   afac *= aesq2;
   ew.f4 = afac;
   const double off2 = c.cfg.ewaldcut * c.cfg.ewaldcut;
-#define THP_FORCE_ARGS                                                                                          \
-  c.n, c.npad, c.box, off2, ew, c.d_pos, MREC, c.d_mu, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_s, c.d_nnb, c.d_nb, \
-      c.maxnb, c.d_frs, c.d_trq, dep
+  if (c.mixed) {
+    if ((st = alloc_once(c, &c.d_muf, 8 * n, "alloc dipoles f32"))) return st;
+    k_mu_f32<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_mu, c.d_muf);
+    if ((st = cuda_status(cudaGetLastError(), &c, "dipoles f32"))) return st;
+  }
+#define THP_FORCE_ARGS                                                                                      \
+  c.n, c.npad, c.box, off2, ew, c.d_pos, MREC, c.d_mu, c.d_erec, c.d_muf, c.d_perm, c.d_sp_off, c.d_sp_ks, \
+      c.d_sp_s, c.d_nnb, c.d_nb, c.maxnb, c.d_frs, c.d_trq, dep
   if (c.mixed) {
 #define MREC c.d_mrecf
     k_force_real<true><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
