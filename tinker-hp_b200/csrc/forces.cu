@@ -333,7 +333,17 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_re
         us = (T)sp_s[3 * q + 2];
         break;
       }
-    const T r = sqrt(r2);
+    // the mixed form: one rsqrt, then products in place of the divisions
+    T r, rinv, r2inv;
+    if constexpr (MIXED) {
+      rinv = rsqrtf(r2);
+      r = r2 * rinv;
+      r2inv = rinv * rinv;
+    } else {
+      r = sqrt(r2);
+      rinv = T(1) / r;
+      r2inv = T(1) / r2;
+    }
     const T dir = dix * xr + diy * yr + diz * zr;
     const T qix = qixx * xr + qixy * yr + qixz * zr, qiy = qixy * xr + qiyy * yr + qiyz * zr,
             qiz = qixz * xr + qiyz * yr + qizz * zr;
@@ -344,13 +354,33 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_re
     const T qkr = qkx * xr + qky * yr + qkz * zr;
     const T uir = uix * xr + uiy * yr + uiz * zr, uirp = uixp * xr + uiyp * yr + uizp * zr;
     const T ukr = ukx * xr + uky * yr + ukz * zr, ukrp = ukxp * xr + ukyp * yr + ukzp * zr;
-    const T rr1 = f / r, rr3 = rr1 / r2, rr5 = T(3) * rr3 / r2, rr7 = T(5) * rr5 / r2, rr9 = T(7) * rr7 / r2;
+    T rr1, rr3, rr5, rr7, rr9, b0, b1, b2, b3, b4;
     // dampewald(9, r, r2, f) (damping.f:17-55)
     const T ra = (T)ew.a * r;
     const T ex = exp(-ra * ra);
-    const T b0 = erfc(ra) / r;
-    const T b1 = (b0 + (T)ew.f1 * ex) / r2, b2 = (T(3) * b1 + (T)ew.f2 * ex) / r2,
-            b3 = (T(5) * b2 + (T)ew.f3 * ex) / r2, b4 = (T(7) * b3 + (T)ew.f4 * ex) / r2;
+    if constexpr (MIXED) {
+      rr1 = f * rinv;
+      rr3 = rr1 * r2inv;
+      rr5 = T(3) * rr3 * r2inv;
+      rr7 = T(5) * rr5 * r2inv;
+      rr9 = T(7) * rr7 * r2inv;
+      b0 = erfc(ra) * rinv;
+      b1 = (b0 + (T)ew.f1 * ex) * r2inv;
+      b2 = (T(3) * b1 + (T)ew.f2 * ex) * r2inv;
+      b3 = (T(5) * b2 + (T)ew.f3 * ex) * r2inv;
+      b4 = (T(7) * b3 + (T)ew.f4 * ex) * r2inv;
+    } else {
+      rr1 = f / r;
+      rr3 = rr1 / r2;
+      rr5 = T(3) * rr3 / r2;
+      rr7 = T(5) * rr5 / r2;
+      rr9 = T(7) * rr7 / r2;
+      b0 = erfc(ra) / r;
+      b1 = (b0 + (T)ew.f1 * ex) / r2;
+      b2 = (T(3) * b1 + (T)ew.f2 * ex) / r2;
+      b3 = (T(5) * b2 + (T)ew.f3 * ex) / r2;
+      b4 = (T(7) * b3 + (T)ew.f4 * ex) / r2;
+    }
     const T e3 = f * b1, e5 = f * b2, e7 = f * b3, e9 = f * b4;
     // Thole factors and their r-derivatives (epolar1.f:1620-1660)
     T sc3 = 1, sc5 = 1, sc7 = 1, rc3[3] = {0, 0, 0}, rc5[3] = {0, 0, 0}, rc7[3] = {0, 0, 0};
@@ -359,14 +389,15 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_re
     T pg = min(pti, ptk);
     if (pg == T(0)) pg = max(pti, ptk);
     if (damp != T(0) && pg != T(0)) {
-      const T t = r / damp;
+      const T t = MIXED ? r * (T(1) / damp) : r / damp;
       damp = pg * (t * t * t);
       if (damp < T(50)) {
         const T ed = exp(-damp);
         sc3 = T(1) - ed;
         sc5 = T(1) - (T(1) + damp) * ed;
         sc7 = T(1) - (T(1) + damp + T(0.6) * damp * damp) * ed;
-        const T temp3 = T(3) * damp * ed / r2, temp5 = damp, temp7 = T(-0.2) + T(0.6) * damp;
+        const T temp3 = MIXED ? T(3) * damp * ed * r2inv : T(3) * damp * ed / r2, temp5 = damp,
+                temp7 = T(-0.2) + T(0.6) * damp;
         rc3[0] = xr * temp3;
         rc3[1] = yr * temp3;
         rc3[2] = zr * temp3;
