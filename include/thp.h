@@ -309,6 +309,16 @@ int thp_server_submit(thp_server* s, unsigned long long key, const double* x, co
 int thp_server_warm(thp_server* s, int count);
 /* Blocks until the request finishes; res receives its outcome. */
 int thp_server_wait(thp_server* s, unsigned long long ticket, thp_result* res);
+/* As thp_server_wait, but gives up after timeout_ms milliseconds of host
+ * time with THP_E_TIMEOUT; the request is not cancelled and its ticket stays
+ * valid for a later wait (its buffers stay the caller's responsibility until
+ * then).  A caller that must not block on a stalled device polls with it. */
+int thp_server_wait_for(thp_server* s, unsigned long long ticket, double timeout_ms, thp_result* res);
+/* paused != 0: the workers take no new request from the queue (requests
+ * already on the GPU finish); submissions still queue.  0 resumes.  For
+ * draining a server for maintenance without refusing requests.  Destroying a
+ * paused server still serves its queue first. */
+int thp_server_pause(thp_server* s, int paused);
 int thp_server_query(thp_server* s, thp_server_stats* out);
 /* Waits for queued work, then frees every context. */
 int thp_server_destroy(thp_server* s);

@@ -5,7 +5,7 @@ energy (tests/test_oracle.py).  Both sides here use the same induced dipoles
 (the GPU's converged ones), so the comparison isolates the gradient kernels:
 FP64 form within 1e-9 of the largest gradient component; mixed form (FP32 pair
 and grid arithmetic, 64-bit fixed-point accumulation) reports its force RMS
-error against the FP64 oracle at the oracle's own dipoles, within 1e-3 of the
+error against the FP64 oracle at the oracle's own dipoles, within 5e-5 of the
 force RMS.
 """
 import ctypes as C
@@ -59,7 +59,9 @@ def test_gradient_mixed_error_vs_fp64(lib, case):
     err = np.sqrt(np.mean(np.sum((dep - dep_ref) ** 2, axis=1)))
     scale = np.sqrt(np.mean(np.sum(dep_ref ** 2, axis=1)))
     print(f"mixed force RMS error {err:.3e} kcal/mol/A of RMS {scale:.3e} ({err / scale:.2e})")
-    assert err < 1e-3 * scale, (err, scale)
+    # 0.8 - 1.4e-5 of the force RMS: the CG tolerance (1e-6 here against the
+    # oracle's 1e-8) and FP32 pair arithmetic
+    assert err < 5e-5 * scale, (err, scale)
 
 
 def test_gradient_matches_finite_difference_of_solved_energy(lib, thp):

@@ -3,7 +3,9 @@
 Tolerances (FP64 form): bit-exact neighbor pair set; operators within 1e-11
 relative of the oracle's; induced dipoles within 1e-6 D RMS and polarization
 energy within 1e-8 relative (the workload's FP64 acceptance).  Mixed form:
-dipole RMS error against the FP64 oracle within 1e-5 D.
+dipole RMS error against the FP64 oracle within 1e-5 D, polarization energy
+within 6e-7 relative (a few times the 5e-8 - 2.4e-7 the FP32 arithmetic
+reaches on these boxes).
 """
 import ctypes as C
 
@@ -102,7 +104,8 @@ def test_solve_mixed_error_vs_fp64(lib, case):
     rms_d = np.sqrt(np.mean(np.sum((uind - ref["uind"]) ** 2, axis=1))) * DEBYE
     assert res["converged"]
     assert rms_d < 1e-5, rms_d
-    assert abs(res["epol"] - e_ref) < 1e-5 * abs(e_ref)
+    # FP32 pair and grid arithmetic moves Epol by 5e-8 - 2.2e-7 relative here
+    assert abs(res["epol"] - e_ref) < 6e-7 * abs(e_ref), (res["epol"], e_ref)
 
 
 def test_run_to_run_reproducible(lib, case):
@@ -304,7 +307,8 @@ def test_solve_large_box_overlapped_rows(lib, large_case, precision):
         assert abs(res["epol"] - e_ref) < 1e-8 * abs(e_ref), (res["epol"], e_ref)
     else:
         assert rms_d < 1e-5 and rms_p < 1e-5, (rms_d, rms_p)
-        assert abs(res["epol"] - e_ref) < 1e-5 * abs(e_ref)
+        # 2.4e-7 relative reached on this box
+        assert abs(res["epol"] - e_ref) < 6e-7 * abs(e_ref), (res["epol"], e_ref)
     # a repeat agrees up to the order of the grid atomics (FP64 / FP32)
     ctx.solve()
     u2, _ = ctx.dipoles()

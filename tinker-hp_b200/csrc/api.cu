@@ -1117,6 +1117,22 @@ static int resolve_predict(Ctx& c, int* guess) {
   return THP_OK;
 }
 
+// After a solve that failed on its inputs or in the CG (non-finite
+// coordinates, parameters or field, list overflow): the dipoles, the last E0,
+// the predictor history and the list may hold values of the failed inputs,
+// so the next solve starts cold and rebuilds the list.
+static void forget_solution(thp_ctx* h) {
+  Ctx& c = h->c;
+  c.have_dipoles = false;
+  c.have_ef_prev = false;
+  c.have_list = false;
+  c.nualt = 0;
+  c.alt_head = 0;
+  h->field_valid = false;
+}
+
+static int solve_one(thp_ctx* h, int guess, thp_solve_info* info);
+
 int thp_solve(thp_ctx* h, int guess, thp_solve_info* info) {
   if (!h) return THP_E_INVALID;
   Ctx& c = h->c;
@@ -1125,6 +1141,13 @@ int thp_solve(thp_ctx* h, int guess, thp_solve_info* info) {
   if (guess < THP_GUESS_DIRECT || guess > THP_GUESS_PREDICT) return THP_E_INVALID;
   if (guess == THP_GUESS_PREVIOUS && !c.have_dipoles) guess = THP_GUESS_DIRECT;
   if (guess == THP_GUESS_HOST && !h->guess_uploaded) return THP_E_STATE;
+  const int st = solve_one(h, guess, info);
+  if (st != THP_OK && st != THP_E_NOT_CONVERGED) forget_solution(h);
+  return st;
+}
+
+static int solve_one(thp_ctx* h, int guess, thp_solve_info* info) {
+  Ctx& c = h->c;
   cudaEventRecord(c.ev0, c.stream);
   // one host sync per solve: the list/pair overflow bits and the CG scalars
   // are read together after Epol (the predictor's least-squares fit and the
@@ -1342,6 +1365,7 @@ int thp_solve_batch(thp_ctx** hs, int count, int guess, thp_solve_info* infos) {
     } else if (infos) {
       infos[i] = thp_solve_info{};
     }
+    if (st[i] && st[i] != THP_E_NOT_CONVERGED) forget_solution(hs[i]);
     if (st[i] && (worst == THP_OK || worst == THP_E_NOT_CONVERGED)) worst = st[i];
   }
   return worst;

@@ -93,6 +93,7 @@ struct thp_server {
   size_t used = 0;
   unsigned long long next_ticket = 1, clock = 0;
   bool stopping = false;
+  bool paused = false;  // workers take no new request (those in flight finish)
   int setups_active = 0;
   std::condition_variable cv_setup;
   long completed = 0, failed = 0, created = 0, reused = 0, evicted = 0;
@@ -201,7 +202,8 @@ void thp_server::worker() {
     // first queued request whose system is not busy with an earlier one
     Req* r = nullptr;
     for (;;) {
-      for (auto it = queue.begin(); it != queue.end(); ++it) {
+      // a paused server still drains its queue once it is being destroyed
+      for (auto it = queue.begin(); (!paused || stopping) && it != queue.end(); ++it) {
         auto res = resident.find((*it)->key);
         if (res == resident.end() || !res->second.busy) {
           r = *it;
@@ -279,7 +281,7 @@ void thp_server::worker() {
       resident.erase(r->key);
     } else {
       slot->busy = false;
-      slot->solved = slot->solved || st == THP_OK;
+      slot->solved = st == THP_OK;  // a failed solve leaves no dipoles to start the next one from
       slot->last_use = ++clock;
     }
     r->res.status = st;
@@ -408,6 +410,29 @@ int thp_server_wait(thp_server* s, unsigned long long ticket, thp_result* res) {
   s->cv_done.wait(lk, [r] { return r->done; });
   if (res) *res = r->res;
   s->reqs.erase(it);
+  return THP_OK;
+}
+
+int thp_server_wait_for(thp_server* s, unsigned long long ticket, double timeout_ms, thp_result* res) {
+  if (!s || !(timeout_ms >= 0.0)) return THP_E_INVALID;
+  std::unique_lock<std::mutex> lk(s->m);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return THP_E_INVALID;
+  Req* r = it->second.get();
+  const auto limit = std::chrono::duration<double, std::milli>(timeout_ms);
+  if (!s->cv_done.wait_for(lk, limit, [r] { return r->done; })) return THP_E_TIMEOUT;  // the ticket stays valid
+  if (res) *res = r->res;
+  s->reqs.erase(it);
+  return THP_OK;
+}
+
+int thp_server_pause(thp_server* s, int paused) {
+  if (!s) return THP_E_INVALID;
+  {
+    std::lock_guard<std::mutex> g(s->m);
+    s->paused = paused != 0;
+  }
+  s->cv_work.notify_all();
   return THP_OK;
 }
 

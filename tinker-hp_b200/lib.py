@@ -149,6 +149,8 @@ def load():
         "thp_server_register": ([vp, C.c_ulonglong, C.POINTER(ThpSystem)], C.c_int),
         "thp_server_submit": ([vp, C.c_ulonglong, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_ulonglong)], C.c_int),
         "thp_server_wait": ([vp, C.c_ulonglong, C.POINTER(ThpResult)], C.c_int),
+        "thp_server_wait_for": ([vp, C.c_ulonglong, C.c_double, C.POINTER(ThpResult)], C.c_int),
+        "thp_server_pause": ([vp, C.c_int], C.c_int),
         "thp_server_warm": ([vp, C.c_int], C.c_int),
         "thp_server_query": ([vp, C.POINTER(ThpServerStats)], C.c_int),
         "thp_server_destroy": ([vp], C.c_int),

@@ -125,13 +125,28 @@ class Server:
         if st:
             raise L.ThpError(st, "thp_server_warm")
 
-    def wait(self, ticket):
+    def wait(self, ticket, timeout_ms=None):
+        """The request's thp_result.  With timeout_ms, raises ThpError with
+        THP_E_TIMEOUT when it has not finished by then; the ticket (and its
+        buffers) stay live for a later wait."""
         r = L.ThpResult()
-        st = L.load().thp_server_wait(self.h, ticket, C.byref(r))
+        if timeout_ms is None:
+            st = L.load().thp_server_wait(self.h, ticket, C.byref(r))
+        else:
+            st = L.load().thp_server_wait_for(self.h, ticket, float(timeout_ms), C.byref(r))
+            if st == L.THP_E_TIMEOUT:
+                raise L.ThpError(st, "thp_server_wait_for")
         self._live.pop(ticket, None)
         if st:
             raise L.ThpError(st, "thp_server_wait")
         return r
+
+    def pause(self, paused=True):
+        """Holds (True) or releases (False) the queue: paused workers take no
+        new request."""
+        st = L.load().thp_server_pause(self.h, 1 if paused else 0)
+        if st:
+            raise L.ThpError(st, "thp_server_pause")
 
     def run(self, requests, realtime=True, warm=0):
         """Serve the stream (submitting each request at its arrival time when
