@@ -166,6 +166,45 @@ def cpu_baseline_oracle(ws_sys, max_seconds, threads, tol=CG_TOL):
     return dt, res, e
 
 
+def cpu_model():
+    """The host CPU's model name (Linux /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_one_core_sample(ws_sys, n_iter, tol=CG_TOL):
+    """One core: the oracle's list build, then two solves stopped after 1 and
+    3 CG iterations; their difference gives the cost of one iteration, from
+    which a full solve of n_iter iterations is assembled (list + front +
+    n_iter iterations).  About 25 s of one core at 288,000 atoms."""
+    from oracle import oracle as O
+    out = {}
+    for politer in (1, 3):
+        orc = O.Oracle(ws_sys, poleps=tol, nthreads=1, politer=politer)
+        t0 = time.perf_counter()
+        st, _, _ = orc.mlistcell()
+        t_list = time.perf_counter() - t0
+        if st != 0:
+            raise RuntimeError(f"oracle list status {st}")
+        t0 = time.perf_counter()
+        orc.solve()
+        out[politer] = (t_list, time.perf_counter() - t0)
+        orc.close()
+    t_list = min(out[1][0], out[3][0])
+    t_iter = max(0.0, (out[3][1] - out[1][1]) / 2.0)
+    t_front = max(0.0, out[1][1] - t_iter)
+    t_solve = t_list + t_front + n_iter * t_iter
+    return {"value": 1.0 / t_solve, "unit": "solves/s", "cores": 1, "kind": "port",
+            "sample": f"one core: list {t_list:.2f} s, front (E0) {t_front:.2f} s, {t_iter:.2f} s per CG "
+                      f"iteration x {n_iter} (from solves stopped after 1 and 3 iterations)"}
+
+
 def run_reference(args, ws_n, rank, world):
     """--impl reference: the CPU restatement of the reference's v1.2 path
     (the Fortran reference cannot be built here), all host threads."""
@@ -196,6 +235,7 @@ def run_reference(args, ws_n, rank, world):
             "config": {"workload": f"{args.workload} ({ws.n} atoms, box {ws.box[0]:.2f} A, grid {ws.nfft[0]}^3)",
                        "cg_tol": CG_TOL, "iterations": res["niter"]},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "cpu_model": cpu_model(),
                              "sample": f"{steps} full FP64 solves of the {ws.n}-atom box (C++ restatement of "
                                        f"v1.2, OpenMP {threads} threads); the Fortran reference needs gfortran+MPI, "
                                        "absent on this image"},
@@ -643,8 +683,13 @@ def main():
             th = os.cpu_count() or 1
             dt, res_c, e_c = cpu_baseline_oracle(ws, 120, th, CG_TOL)
             cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": th, "kind": "port",
+                   "cpu_model": cpu_model(),
                    "sample": f"1 full FP64 solve of the {n}-atom box by the C++ restatement of v1.2 "
                              f"({res_c['niter']} CG iterations, {dt:.1f} s)"}
+            try:
+                cpu["one_core"] = cpu_one_core_sample(ws, res_c["niter"])
+            except Exception as ex:  # the all-core figure stands without it
+                cpu["one_core"] = {"value": None, "sample": f"failed: {ex}"}
         except Exception as ex:  # the GPU number stands without it
             cpu = {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"failed: {ex}"}

@@ -416,6 +416,34 @@ void epolar_(void);
  * the bound dep (overwritten, as epolar1c zeroes it first) */
 void epolar1_(void);
 
+/* The same entry points under names no Tinker-HP object defines, for a
+ * build that keeps the reference's own sources and reaches the library
+ * through the ISO_C_BINDING shim (tinker-hp_b200/fortran/thp_shim.f90): the
+ * reference-named symbols above would collide there with the reference's
+ * newinduce_pme2.f, newinduce_pme.f, pmestuff.f, nblist.f, epolar.f,
+ * epolar1.f, empole1.f and ehal1.f objects.  inducepcg_pme2 runs its device
+ * loop for either tmatxb_pme_ or thp_f_tmatxb_pme as the matvec. */
+void thp_f_newinduce_pme2(void);
+void thp_f_inducepcg_pme2(void (*matvec)(const int* nrhs, const int* dodiag, const double* mu,
+                                         double* efi),
+                          const int* nrhs, const int* precnd, const double* ef, double* mu,
+                          double* murec);
+void thp_f_tmatxb_pme(const int* nrhs, const int* dodiag, const double* mu, double* efi);
+void thp_f_efld0_direct(const int* nrhs, double* ef);
+void thp_f_efld0_recip(double* cphi);
+void thp_f_tmatxbrecip(const double* mu, const double* murec, const int* nrhs, double* dipfield,
+                       double* dipfieldbis);
+void thp_f_grid_uind_sites(const int* nsites, const int* isite, const double* fuind, const double* fuinp,
+                           double* qgrid);
+void thp_f_fphi_uind_sites(const int* nsites, const int* isite, const double* qgrid, double* fdip_phi1,
+                           double* fdip_phi2, double* fdip_sum_phi);
+void thp_f_mlistcell(void);
+void thp_f_vlistcell(void);
+void thp_f_epolar(void);
+void thp_f_epolar1(void);
+void thp_f_empole1(void);
+void thp_f_ehal1(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,3 +48,24 @@ def test_footprint_scales_with_size(thp):
     a = L.footprint(thp.water.make_water_box(216))
     b = L.footprint(thp.water.make_water_box(1000))
     assert 0 < a < b
+
+
+def test_fortran_shim_binds_declared_noncolliding_symbols():
+    # The shim reaches the library only through names that no Tinker-HP
+    # object defines (thp_*), each declared in include/thp.h; the
+    # reference-named drop-ins are for builds that drop those objects.
+    src = open(os.path.join(ROOT, "tinker-hp_b200", "fortran", "thp_shim.f90")).read()
+    names = re.findall(r'bind\(C,\s*name="([^"]+)"\)', src)
+    assert len(names) >= 15
+    declared = set(declared_functions())
+    for n in names:
+        assert n.startswith("thp_"), n
+        assert n in declared, n
+    # module variables (no TARGET attribute in Tinker-HP) never go through c_loc
+    code = "\n".join(l.split("!")[0] for l in src.splitlines())
+    for var in ("x", "y", "z", "rpole", "uind", "uinp", "nelst", "elst", "ep", "em", "ev", "dep", "dem", "dev",
+                "polarity", "thole", "pdamp"):
+        assert not re.search(r"c_loc\(\s*%s\s*\)" % var, code), var
+    # maxelst comes from module sizes, lbuffer from module neigh (v1.2 modules)
+    assert re.search(r"use sizes, only: maxelst", code)
+    assert re.search(r"use neigh, only: lbuffer", code)

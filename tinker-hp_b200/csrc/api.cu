@@ -420,7 +420,7 @@ static void drop_front_graphs(Ctx& c) {
 
 size_t footprint_bytes(const thp_config& cfg, int* ncell_out) {
   const size_t n = cfg.n, npad = (n + 31) / 32 * 32;
-  const size_t maxnb = cfg.max_neighbors > 0 ? cfg.max_neighbors : kDefaultMaxNb;
+  const size_t maxnb = ((cfg.max_neighbors > 0 ? cfg.max_neighbors : kDefaultMaxNb) + 7) / 8 * 8;
   int nc[3];
   cell_grid(cfg, nc);
   const size_t ncell = (size_t)nc[0] * nc[1] * nc[2];
@@ -486,7 +486,7 @@ static void apply_config(Ctx& c, const thp_config& k) {
   c.mixed = k.precision == THP_MIXED;
   c.device = k.device;
   c.maxnb = k.max_neighbors > 0 ? k.max_neighbors : kDefaultMaxNb;
-  c.maxpr = c.maxnb;
+  c.maxpr = (c.maxnb + 7) / 8 * 8;  // the pair stream holds an atom's slots in blocks of 8
   for (int d = 0; d < 3; ++d) {
     c.box.l[d] = k.box[d];
     c.box.half[d] = 0.5 * k.box[d];
@@ -581,15 +581,14 @@ static int size_buffers(Ctx& c) {
                     "per-atom buffers");
     if (!st) c.cap_n = n;
   }
-  const size_t pairs = (size_t)c.maxnb * npad;
+  const size_t pairs = (size_t)c.maxpr * npad;  // list (maxnb <= maxpr slots) and pair stream
   if (!st && pairs > c.cap_pairs) {
     cudaFree(c.slab_pairs);
     c.slab_pairs = nullptr;
     c.cap_pairs = 0;
+    const size_t ps = pairs + kPairTail;  // entries the rows may read past the last group
     st = alloc_slab(c, &c.slab_pairs,
-                    {item(&c.d_nb, pairs), item(&c.d_pk, pairs), SlabItem{&c.d_pc3, esz * pairs},
-                     SlabItem{&c.d_pc5, esz * pairs}},
-                    "pair buffers");
+                    {item(&c.d_nb, pairs), item(&c.d_pk, ps), SlabItem{&c.d_pcc, 2 * esz * ps}}, "pair buffers");
     if (!st) c.cap_pairs = pairs;
   }
   if (!st && !c.d_cg) st = dmalloc(c, &c.d_cg, 1, "cg");
@@ -1974,7 +1973,7 @@ void inducepcg_pme2_(void (*matvec)(const int*, const int*, const double*, doubl
     g_last_error = st;
     return;
   }
-  if (matvec == tmatxb_pme_ && nr == 2 && *precnd) {
+  if ((matvec == tmatxb_pme_ || matvec == thp_f_tmatxb_pme) && nr == 2 && *precnd) {
     // device loop on the caller's E0 and guess
     cudaMemcpyAsync(c.d_tmp6, ef, sizeof(double) * nv, cudaMemcpyHostToDevice, c.stream);
     st = launch_to_sorted6(c, c.d_tmp6, c.d_ef, 2);
@@ -2062,5 +2061,37 @@ void inducepcg_pme2_(void (*matvec)(const int*, const int*, const double*, doubl
   }
   g_last_error = st;
 }
+
+// Fortran-callable aliases of the drop-ins under names no Tinker-HP object
+// defines, for a build that keeps the reference sources and calls the
+// library through the ISO_C_BINDING shim.
+void thp_f_newinduce_pme2(void) { newinduce_pme2_(); }
+void thp_f_inducepcg_pme2(void (*matvec)(const int*, const int*, const double*, double*), const int* nrhs,
+                          const int* precnd, const double* ef, double* mu, double* murec) {
+  inducepcg_pme2_(matvec, nrhs, precnd, ef, mu, murec);
+}
+void thp_f_tmatxb_pme(const int* nrhs, const int* dodiag, const double* mu, double* efi) {
+  tmatxb_pme_(nrhs, dodiag, mu, efi);
+}
+void thp_f_efld0_direct(const int* nrhs, double* ef) { efld0_direct_(nrhs, ef); }
+void thp_f_efld0_recip(double* cphi) { efld0_recip_(cphi); }
+void thp_f_tmatxbrecip(const double* mu, const double* murec, const int* nrhs, double* dipfield,
+                       double* dipfieldbis) {
+  tmatxbrecip_(mu, murec, nrhs, dipfield, dipfieldbis);
+}
+void thp_f_grid_uind_sites(const int* nsites, const int* isite, const double* fuind, const double* fuinp,
+                           double* qgrid) {
+  grid_uind_sites_(nsites, isite, fuind, fuinp, qgrid);
+}
+void thp_f_fphi_uind_sites(const int* nsites, const int* isite, const double* qgrid, double* fdip_phi1,
+                           double* fdip_phi2, double* fdip_sum_phi) {
+  fphi_uind_sites_(nsites, isite, qgrid, fdip_phi1, fdip_phi2, fdip_sum_phi);
+}
+void thp_f_mlistcell(void) { mlistcell_(); }
+void thp_f_vlistcell(void) { vlistcell_(); }
+void thp_f_epolar(void) { epolar_(); }
+void thp_f_epolar1(void) { epolar1_(); }
+void thp_f_empole1(void) { empole1_(); }
+void thp_f_ehal1(void) { ehal1_(); }
 
 }  // extern "C"

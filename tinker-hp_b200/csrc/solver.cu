@@ -52,6 +52,8 @@
 namespace thp {
 
 PairRows pair_rows(const Ctx& c);
+float row_interior(const Ctx& c);
+int group_blocks(int n, int block);
 
 namespace {
 
@@ -115,9 +117,20 @@ __device__ __forceinline__ void store6(float* p, const double (&v)[6]) {
 
 __device__ __forceinline__ double diag_of(double p) { return p == 0.0 ? kTinyPol : p; }
 
+// pairs loaded ahead per lane in the group rows (FP64 / FP32 forms)
+#ifndef THP_GROW_U64
+#define THP_GROW_U64 2
+#endif
+#ifndef THP_GROW_U32
+#define THP_GROW_U32 4
+#endif
+
 // h = T_real x + x/alpha + dipfield(x) - term x  (newinduce_pme2.f:398-405, 469-475)
 // init: also res = ef - h, zr = diag res, pp = zr, ggold = sum res.zr
 // iter: gg = sum pp.h, alpha = ggold / gg
+// A block covers kBlock consecutive atoms: each warp sums the rows of eight
+// groups of four atoms (group_row) into shared memory, then every thread
+// finishes its own atom.
 template <bool MIXED>
 __global__ void __launch_bounds__(kBlock) k_cg_matvec(PairRows pr, Box box, const double4* __restrict__ pos,
                                                       const float4* __restrict__ posf, const double* __restrict__ dipf,
@@ -126,22 +139,35 @@ __global__ void __launch_bounds__(kBlock) k_cg_matvec(PairRows pr, Box box, cons
                                                       double term, int init, double* __restrict__ h,
                                                       double* __restrict__ res, double* __restrict__ zr,
                                                       double* __restrict__ pp, CgScalars* cg,
-                                                      double* __restrict__ partials) {
+                                                      double* __restrict__ partials, float interior) {
+  static_assert(kBlock % 32 == 0, "whole warps");
+  __shared__ double srow[kBlock * 6];
   if (cg->stop) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * kBlock + warp * 32) >> 2;  // first group of this warp
+  for (int gg = 0; gg < 8; ++gg) {
+    const int g = gw + gg;
+    if (4 * g >= pr.n) break;  // the same for every lane of the warp
+    const int t = warp * 32 + gg * 4 + (lane >> 3), j = lane & 7;
+    if (MIXED) {
+      float a32[6];
+      group_row<float, THP_GROW_U32, false>(
+          pr, Partner32{posf, xf}, Image32{(float)box.l[0], (float)box.l[1], (float)box.l[2]}, g, lane, a32,
+          interior);
+      if (j < 6) srow[t * 6 + j] = (double)pick6(a32, j);
+    } else {
+      double a64[6];
+      group_row<double, THP_GROW_U64, false>(pr, Partner64{pos, x}, Image64{box}, g, lane, a64, -1.0);
+      if (j < 6) srow[t * 6 + j] = pick6(a64, j);
+    }
+  }
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double red[2] = {0.0, 0.0};
   if (i < pr.n) {
     double acc[6];
-    if (MIXED) {
-      float a32[6] = {0, 0, 0, 0, 0, 0};
-      tmatxb_row32(pr, (float)box.l[0], (float)box.l[1], (float)box.l[2], i, posf, xf, a32);
 #pragma unroll
-      for (int q = 0; q < 6; ++q) acc[q] = (double)a32[q];
-    } else {
-#pragma unroll
-      for (int q = 0; q < 6; ++q) acc[q] = 0.0;
-      tmatxb_row64(pr, box, i, pos, x, acc);
-    }
+    for (int q = 0; q < 6; ++q) acc[q] = srow[threadIdx.x * 6 + q];
     double dip[6], xi[6];
     load6(dipf + (size_t)i * 6, dip);
     load6(x + (size_t)i * 6, xi);
@@ -228,27 +254,30 @@ __global__ void __launch_bounds__(256) k_pp_rec(int n, int update, const V* __re
   mpz[i] = (float)v[5];
 }
 
-// real-space part of h only: hreal = T_real x (tmatxb_pme without the diagonal)
+// real-space part of h only: hreal = T_real x (tmatxb_pme without the
+// diagonal), one warp per group of four atoms; lane j < 6 of an atom writes
+// component j
 template <bool MIXED, bool NOL1, typename HV>
 __global__ void __launch_bounds__(kBlock, THP_ROW_MINB) k_real_row(PairRows pr, Box box, const double4* __restrict__ pos,
                                                      const float* __restrict__ rec, const double* __restrict__ x,
                                                      const float* __restrict__ mpz, const CgScalars* __restrict__ cg,
-                                                     int check_stop, HV* __restrict__ hreal) {
+                                                     int check_stop, float interior, HV* __restrict__ hreal) {
   if (check_stop && cg->stop) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= pr.n) return;
-  double acc[6];
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (4 * g >= pr.n) return;
+  const int lane = threadIdx.x & 31;
+  const int i = 4 * g + (lane >> 3), j = lane & 7;
   if (MIXED) {
-    float a32[6] = {0, 0, 0, 0, 0, 0};
-    tmatxb_row32_rec<NOL1>(pr, (float)box.l[0], (float)box.l[1], (float)box.l[2], i, rec, mpz, a32);
-#pragma unroll
-    for (int q = 0; q < 6; ++q) acc[q] = (double)a32[q];
+    float a32[6];
+    group_row<float, THP_GROW_U32, NOL1>(pr, PartnerRec{rec, mpz},
+                                         Image32{(float)box.l[0], (float)box.l[1], (float)box.l[2]}, g, lane, a32,
+                                         interior);
+    if (j < 6 && i < pr.n) hreal[(size_t)i * 6 + j] = (HV)pick6(a32, j);
   } else {
-#pragma unroll
-    for (int q = 0; q < 6; ++q) acc[q] = 0.0;
-    tmatxb_row64(pr, box, i, pos, x, acc);
+    double a64[6];
+    group_row<double, THP_GROW_U64, NOL1>(pr, Partner64{pos, x}, Image64{box}, g, lane, a64, -1.0);
+    if (j < 6 && i < pr.n) hreal[(size_t)i * 6 + j] = (HV)pick6(a64, j);
   }
-  store6(hreal + (size_t)i * 6, acc);
 }
 
 // h = hreal + x/alpha + dipfield(x) - term x, then the reductions of
@@ -498,16 +527,18 @@ static int matvec_overlapped(Ctx& c, const XV* x, int init) {
   cudaEventRecord(c.ev_fork, c.stream);
   cudaStreamWaitEvent(c.stream2, c.ev_fork, 0);
   PairRows pr = pair_rows(c);
+  const int nbr = group_blocks(c.n, kBlock);  // one warp per group of four atoms
+  const float interior = row_interior(c);
   prof_mark(c, c.stream2);
   if (c.mixed && c.n >= THP_STREAM_NO_L1_ATOMS)
-    k_real_row<true, true, float><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, nullptr, c.d_mpz, c.d_cg,
-                                                                !init, c.d_hf);
+    k_real_row<true, true, float><<<nbr, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, nullptr, c.d_mpz, c.d_cg,
+                                                                 !init, interior, c.d_hf);
   else if (c.mixed)
-    k_real_row<true, false, float><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, nullptr, c.d_mpz,
-                                                                 c.d_cg, !init, c.d_hf);
+    k_real_row<true, false, float><<<nbr, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, c.d_rec, nullptr, c.d_mpz,
+                                                                  c.d_cg, !init, interior, c.d_hf);
   else if constexpr (std::is_same<XV, double>::value)
-    k_real_row<false, false, double><<<nb, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, nullptr, x, nullptr, c.d_cg,
-                                                                   !init, c.d_h);
+    k_real_row<false, false, double><<<nbr, kBlock, 0, c.stream2>>>(pr, c.box, c.d_pos, nullptr, x, nullptr, c.d_cg,
+                                                                    !init, -1.f, c.d_h);
   prof_mark(c, c.stream2);
   if ((st = cuda_status(cudaGetLastError(), &c, "real row"))) return st;
   cudaEventRecord(c.ev_join, c.stream2);
@@ -542,11 +573,11 @@ static int launch_matvec(Ctx& c, const double* x, int init) {
   if (c.mixed)
     k_cg_matvec<true><<<nb, kBlock, 0, c.stream>>>(pr, c.box, c.d_pos, c.d_posf, c.d_dip, x, c.d_vecf, c.d_pol,
                                                    c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, c.d_cg,
-                                                   c.d_partials);
+                                                   c.d_partials, row_interior(c));
   else
     k_cg_matvec<false><<<nb, kBlock, 0, c.stream>>>(pr, c.box, c.d_pos, c.d_posf, c.d_dip, x, c.d_vecf, c.d_pol,
                                                     c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, c.d_cg,
-                                                    c.d_partials);
+                                                    c.d_partials, -1.f);
   prof_mark(c, c.stream);
   return cuda_status(cudaGetLastError(), &c, "cg matvec");
 }

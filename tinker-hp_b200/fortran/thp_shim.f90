@@ -3,8 +3,26 @@
 ! epolar1.f:145), mlistcell (nblist.f:109), epolar1 (gradient.f:165) and
 ! empole1 and ehal1 (gradient.f, the permanent-multipole and vdW terms) by
 ! thp_newinduce_pme2, thp_mlistcell, thp_epolar1, thp_empole1 and thp_ehal1,
-! and offers the batched per-site PME routines.  Not compiled in this repository's image (no Fortran
-! compiler); it follows the C declarations of include/thp.h.
+! and offers the batched per-site PME routines.
+!
+! Binding rules this file follows:
+!   * It binds to the library's thp_f_* entry points, never to the
+!     reference-named drop-ins (newinduce_pme2_, mlistcell_, ...): those
+!     symbols are also defined by the reference's own objects, so a build
+!     that keeps the reference sources links either a duplicate or the CPU
+!     routine.
+!   * Module arrays go to the C side as assumed-size dummy arguments (the
+!     caller passes their address), not through c_loc, which requires the
+!     TARGET or POINTER attribute that Tinker-HP's module variables do not
+!     carry.  The library keeps the addresses given to c_bind_state,
+!     c_bind_gradient, c_bind_mpole and c_bind_vdw until the next bind: pass
+!     only contiguous allocatable module arrays there (x, y, z, rpole, uind,
+!     uinp, nelst, elst, dep, dem, dev), for which the compiler passes the
+!     array itself and no temporary copy.
+!   * maxelst is a parameter of module sizes (MOD_sizes.f:58) and lbuffer a
+!     variable of module neigh (MOD_neigh.f:58).
+! Not compiled in this repository's image (no Fortran compiler); it follows
+! the C declarations of include/thp.h.
 module thp_shim
   use iso_c_binding
   implicit none
@@ -37,8 +55,9 @@ module thp_shim
       type(c_ptr), value :: h
     end function
     integer(c_int) function c_set_params(h, pol, thl, pdm) bind(C, name="thp_set_params")
-      import :: c_int, c_ptr
-      type(c_ptr), value :: h, pol, thl, pdm
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double), intent(in) :: pol(*), thl(*), pdm(*)
     end function
     integer(c_int) function c_set_connectivity(h, offp, idxp, scales) bind(C, name="thp_set_connectivity")
       import :: c_int, c_ptr
@@ -46,35 +65,39 @@ module thp_shim
     end function
     integer(c_int) function c_bind_state(h, x, y, z, rpole, uind, uinp, nelst, elst, maxelst, ep) &
         bind(C, name="thp_bind_state")
-      import :: c_int, c_ptr
-      type(c_ptr), value :: h, x, y, z, rpole, uind, uinp, nelst, elst, ep
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double) :: x(*), y(*), z(*), rpole(*), uind(*), uinp(*), ep
+      integer(c_int) :: nelst(*), elst(*)
       integer(c_int), value :: maxelst
     end function
-    subroutine c_newinduce_pme2() bind(C, name="newinduce_pme2_")
+    subroutine c_newinduce_pme2() bind(C, name="thp_f_newinduce_pme2")
     end subroutine
-    subroutine c_mlistcell() bind(C, name="mlistcell_")
+    subroutine c_mlistcell() bind(C, name="thp_f_mlistcell")
     end subroutine
-    subroutine c_epolar() bind(C, name="epolar_")
+    subroutine c_epolar() bind(C, name="thp_f_epolar")
     end subroutine
-    subroutine c_epolar1() bind(C, name="epolar1_")
+    subroutine c_epolar1() bind(C, name="thp_f_epolar1")
     end subroutine
     integer(c_int) function c_set_frames(h, pole, zax, xax, axt) bind(C, name="thp_set_frames")
       import :: c_int, c_ptr
       type(c_ptr), value :: h, pole, zax, xax, axt
     end function
     integer(c_int) function c_bind_gradient(h, dep) bind(C, name="thp_bind_gradient")
-      import :: c_int, c_ptr
-      type(c_ptr), value :: h, dep
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double) :: dep(*)
     end function
     integer(c_int) function c_set_mpole_scales(h, m) bind(C, name="thp_set_mpole_scales")
       import :: c_int, c_ptr
       type(c_ptr), value :: h, m
     end function
     integer(c_int) function c_bind_mpole(h, em, dem) bind(C, name="thp_bind_mpole")
-      import :: c_int, c_ptr
-      type(c_ptr), value :: h, em, dem
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double) :: em, dem(*)
     end function
-    subroutine c_empole1() bind(C, name="empole1_")
+    subroutine c_empole1() bind(C, name="thp_f_empole1")
     end subroutine
     integer(c_int) function c_set_vdw(h, cls, nclass, tables, ired, kred, vscale, vdwcut, vdwtaper, &
         ghal, dhal) bind(C, name="thp_set_vdw")
@@ -84,18 +107,19 @@ module thp_shim
       real(c_double), value :: vdwcut, vdwtaper, ghal, dhal
     end function
     integer(c_int) function c_bind_vdw(h, ev, dev) bind(C, name="thp_bind_vdw")
-      import :: c_int, c_ptr
-      type(c_ptr), value :: h, ev, dev
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double) :: ev, dev(*)
     end function
-    subroutine c_ehal1() bind(C, name="ehal1_")
+    subroutine c_ehal1() bind(C, name="thp_f_ehal1")
     end subroutine
-    subroutine c_grid_uind_sites(ns, isite, fuind, fuinp, qgrid) bind(C, name="grid_uind_sites_")
+    subroutine c_grid_uind_sites(ns, isite, fuind, fuinp, qgrid) bind(C, name="thp_f_grid_uind_sites")
       import :: c_int, c_double
       integer(c_int), intent(in) :: ns, isite(*)
       real(c_double), intent(in) :: fuind(3,*), fuinp(3,*)
       real(c_double), intent(inout) :: qgrid(*)
     end subroutine
-    subroutine c_fphi_uind_sites(ns, isite, qgrid, phi1, phi2, sphi) bind(C, name="fphi_uind_sites_")
+    subroutine c_fphi_uind_sites(ns, isite, qgrid, phi1, phi2, sphi) bind(C, name="thp_f_fphi_uind_sites")
       import :: c_int, c_double
       integer(c_int), intent(in) :: ns, isite(*)
       real(c_double), intent(in) :: qgrid(*)
@@ -113,7 +137,8 @@ contains
     use atoms, only: n
     use boxes, only: xbox, ybox, zbox
     use ewald, only: aewald
-    use cutoff, only: ewaldcut, lbuffer
+    use cutoff, only: ewaldcut
+    use neigh, only: lbuffer
     use pme, only: nfft1, nfft2, nfft3, bsorder
     use polar, only: polarity, thole, pdamp
     use polpot, only: politer, poleps, p2scale, p3scale, p4scale, p5scale, p2iscale, p3iscale, &
@@ -140,7 +165,7 @@ contains
     cfg%device = 0
     st = c_ctx_create(cfg, ctx)
     if (st /= 0) call fatal
-    st = c_set_params(ctx, c_loc(polarity), c_loc(thole), c_loc(pdamp))
+    st = c_set_params(ctx, polarity, thole, pdamp)  ! copied before the call returns
     if (st /= 0) call fatal
     call pack_connectivity(offp, idxp)
     scales = [p2scale, p3scale, p4scale, p5scale, p2iscale, p3iscale, p4iscale, p5iscale, &
@@ -259,11 +284,11 @@ contains
     use atoms, only: x, y, z
     use mpole, only: rpole
     use polar, only: uind, uinp
-    use neigh, only: nelst, elst, maxelst
+    use neigh, only: nelst, elst
+    use sizes, only: maxelst
     use energi, only: ep
     integer :: st
-    st = c_bind_state(ctx, c_loc(x), c_loc(y), c_loc(z), c_loc(rpole), c_loc(uind), c_loc(uinp), &
-                      c_loc(nelst), c_loc(elst), int(maxelst, c_int), c_loc(ep))
+    st = c_bind_state(ctx, x, y, z, rpole, uind, uinp, nelst, elst, int(maxelst, c_int), ep)
     if (st /= 0) call fatal
   end subroutine
 
@@ -290,7 +315,7 @@ contains
     use deriv, only: dep
     integer :: st
     call bind_all()
-    st = c_bind_gradient(ctx, c_loc(dep))
+    st = c_bind_gradient(ctx, dep)
     if (st /= 0) call fatal
     call c_epolar1()
     if (c_last_error() /= 0 .and. c_last_error() /= 3) call fatal
@@ -303,7 +328,7 @@ contains
     use energi, only: em
     integer :: st
     call bind_all()
-    st = c_bind_mpole(ctx, c_loc(em), c_loc(dem))
+    st = c_bind_mpole(ctx, em, dem)
     if (st /= 0) call fatal
     call c_empole1()
     if (c_last_error() /= 0) call fatal
@@ -317,7 +342,7 @@ contains
     use energi, only: ev
     integer :: st
     call bind_all()
-    st = c_bind_vdw(ctx, c_loc(ev), c_loc(dev))
+    st = c_bind_vdw(ctx, ev, dev)
     if (st /= 0) call fatal
     call c_ehal1()
     if (c_last_error() /= 0) call fatal
