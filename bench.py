@@ -243,10 +243,12 @@ def run_reference(args, ws_n, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def batched_throughput(lib, systems, copies, steps, warmup=2):
+def batched_throughput(lib, systems, copies, steps, warmup=2, precision=None):
     """Batched form: `copies` resident contexts per system solved together by
-    thp_solve_batch (each on its own stream); host-timed over whole batches."""
-    ctxs = [lib.Context(ws, precision=lib.MIXED, poleps=CG_TOL) for ws in systems for _ in range(copies)]
+    thp_solve_batch (each on its own stream); host-timed over whole batches.
+    Mixed form unless `precision` says otherwise."""
+    prec = lib.MIXED if precision is None else precision
+    ctxs = [lib.Context(ws, precision=prec, poleps=CG_TOL) for ws in systems for _ in range(copies)]
     for _ in range(warmup):
         lib.solve_batch(ctxs)
     t0 = time.perf_counter()
@@ -665,10 +667,13 @@ def main():
     avg_ms = mv_ms / max(mv_launches, 1)
     achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
     # DRAM bytes per launch (read + write) from one ncu capture of this kernel on the 96,000-atom
-    # box (196.9 MB per launch), scaled by the atom count: the traffic is the streamed FP32 pair
-    # coefficients (12 B per directed pair) plus per-atom data, both proportional to n
-    traffic = 196.9e6 * n / 96000.0
+    # box (182.1 MB per launch), scaled by the atom count: the traffic is the streamed pair entries
+    # (index and two FP32 coefficients, 12 B per directed pair) plus per-atom data, both
+    # proportional to n
+    traffic = 182.1e6 * n / 96000.0
     roof = {"bound": "hbm", "kernel": "k_real_row<mixed> (real-space row of the CG matvec)",
+            "limiter": "L1 data pipe (73 % of cycles) and the latency of the dependent stream and partner "
+                       "loads; DRAM at 40 % (ncu, 96k-atom capture)",
             "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
             "frac": achieved / peaks.get("hbm_gbs"), "peak_kind": peak_kind, "traffic": traffic,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, 96k-atom capture scaled by n",
@@ -698,7 +703,8 @@ def main():
     if not args.no_extras:
         b2 = batched_throughput(lib, [ws], 2, max(2, args.steps // 6))
         b4 = batched_throughput(lib, [ws], 4, max(2, args.steps // 10))
-        extras["batched_288k"] = {"copies_2": b2, "copies_4": b4}
+        b2_64 = batched_throughput(lib, [ws], 2, max(2, args.steps // 6), precision=lib.FP64)
+        extras["batched_288k"] = {"copies_2": b2, "copies_4": b4, "fp64_copies_2": b2_64}
         batch64 = thp.water.make_batch(64, seed=4003)
         extras["batch_64_boxes"] = batched_throughput(lib, batch64, 1, 3)
         extras["batch_64_boxes"]["atoms"] = f"{sum(w.n for w in batch64)} over 64 boxes (300-6000 each)"
@@ -742,14 +748,39 @@ def main():
         "roofline": roof, "solve_roofline": solve_roof, "cpu_baseline": cpu, "clocks": clk,
         "gpu_launches": None,
     }
-    # kernels of this library per timed step (cuFFT's not counted): rotpole 1;
-    # re-sort 9 (count/scan/fill/sort, special pairs, dipoles and last E0
-    # carried out of and back into sorted order); sorted gather 1; list,
-    # E_direct, multipole spread, qfac, multipole gather 5; CG start 6 (guess,
-    # records, row, spread, qfac, combine); 7 per iteration (records, row,
-    # spread, qfac, combine, update, loop condition); Epol 1
+    # compact summaries last, so that a truncated record still ends with them
+    if extras and fp64_line:
+        sr = extras["served_288k_repeats"]
+        bt = extras["batched_288k"]
+        line["target_3x"] = {
+            "goal": "mixed batched/served solves/s >= 3x plain FP64 solves/s, 288k box, <= 1e-5 D",
+            "like_for_like": {
+                "cold_mixed_vs_cold_fp64": value / fp64_line["value"],
+                "batched_mixed_vs_batched_fp64": bt["copies_2"]["solves_per_s"] / bt["fp64_copies_2"]["solves_per_s"],
+                "served_mixed_vs_served_fp64": sr["mixed_vs_fp64_served"],
+                "served_2_systems_mixed_vs_fp64": sr["mixed_2_systems_vs_fp64_2_systems"]},
+            "served_mixed_vs_plain_fp64": {
+                "one_system": sr["mixed_vs_fp64_plain"], "two_systems": sr["mixed_2_systems_vs_fp64_plain"],
+                "note": "warm-started served mixed (0.01 A repeats) against cold single FP64 solves"},
+            "batched_mixed_vs_plain_fp64": bt["speedup_vs_fp64_plain"]}
+    if extras:
+        sv = extras["serving"]
+        line["serving"] = {k: sv[k] for k in ("solves_per_s", "p50_ms", "p99_ms", "requests", "rate_req_per_s",
+                                              "mean_setup_ms", "mean_solve_ms", "completed", "failed")}
+    # kernels of this library per timed step (cuFFT's not counted; the
+    # positions do not move, so rotpole does not run):
+    #   re-sort 11: dipoles and last E0 out of sorted order (2), cell count,
+    #     scan (3), fill, sort, special pairs to sorted numbering, dipoles and
+    #     last E0 back (2);
+    #   sorted gather 1; list 1; E_direct + pair stream 1; multipole spread,
+    #     qfac, multipole gather 3;
+    #   CG start 6: direct guess, row records, real row, dipole spread, qfac,
+    #     combine;
+    #   7 per iteration (device-side loop): row records, real row, dipole
+    #     spread, qfac, combine, update, loop condition;
+    #   Epol 1.
     it = int(np.median(niter))
-    per_step = 1 + 9 + 1 + 5 + 6 + 7 * it + 1
+    per_step = 11 + 1 + 1 + 1 + 3 + 6 + 7 * it + 1
     line["gpu_launches"] = per_step * steps
     if rank == 0:
         print(json.dumps(line), flush=True)

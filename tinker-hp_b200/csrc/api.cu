@@ -586,9 +586,9 @@ static int size_buffers(Ctx& c) {
     cudaFree(c.slab_pairs);
     c.slab_pairs = nullptr;
     c.cap_pairs = 0;
-    const size_t ps = pairs + kPairTail;  // entries the rows may read past the last group
     st = alloc_slab(c, &c.slab_pairs,
-                    {item(&c.d_nb, pairs), item(&c.d_pk, ps), SlabItem{&c.d_pcc, 2 * esz * ps}}, "pair buffers");
+                    {item(&c.d_nb, pairs), item(&c.d_pk, pairs), SlabItem{&c.d_pcc, 2 * esz * pairs}},
+                    "pair buffers");
     if (!st) c.cap_pairs = pairs;
   }
   if (!st && !c.d_cg) st = dmalloc(c, &c.d_cg, 1, "cg");

@@ -31,11 +31,6 @@ struct CgScalars {
 
 // CG iterations per host check of the stop flag
 constexpr int kCgChunk = 4;
-// Entries of the pair stream after its last group's capacity that the
-// matvec rows may read and discard: a lane loads whole rounds of U blocks of
-// 32 entries and, with the one-round prefetch, the round after the last:
-// up to 2U - 1 blocks past a group's capacity (U <= 4).
-constexpr int kPairTail = 8 * 32;
 
 // device error flags (bit set)
 enum : int { DEV_LIST_OVERFLOW = 1, DEV_PAIR_OVERFLOW = 2, DEV_NAN = 4, DEV_BAD_INPUT = 8, DEV_VDW_REACH = 16 };

@@ -156,28 +156,33 @@ struct Image32 {
 
 // Stream entries (partner, dmp3, dmp5) of the U blocks of one round for this
 // lane; a slot past the atom's count (8 b < mj fails) gives the lane's own
-// atom with zero coefficients.
+// atom with zero coefficients.  Blocks past the group's last (the same for
+// the whole warp) are not read at all.
 template <typename T, int U, bool NOL1>
 __device__ __forceinline__ void stream_round(const int* pk, const typename Vec2<T>::type* pc, int b, int mj,
-                                             int i_safe, int (&k)[U], T (&c3)[U], T (&c5)[U]) {
+                                             int nblk, int i_safe, int (&k)[U], T (&c3)[U], T (&c5)[U]) {
   using T2 = typename Vec2<T>::type;
 #pragma unroll
   for (int u = 0; u < U; ++u) {
-    const int kr = ld_stream<NOL1>(pk + 32 * u);
-    const T2 cr = ld_stream<NOL1>(pc + 32 * u);
-    const bool ok = 8 * (b + u) < mj;
-    k[u] = ok ? kr : i_safe;
-    c3[u] = ok ? cr.x : T(0);
-    c5[u] = ok ? cr.y : T(0);
+    k[u] = i_safe;
+    c3[u] = T(0);
+    c5[u] = T(0);
+    if (b + u < nblk) {
+      const int kr = ld_stream<NOL1>(pk + 32 * u);
+      const T2 cr = ld_stream<NOL1>(pc + 32 * u);
+      const bool ok = 8 * (b + u) < mj;
+      k[u] = ok ? kr : i_safe;
+      c3[u] = ok ? cr.x : T(0);
+      c5[u] = ok ? cr.y : T(0);
+    }
   }
 }
 
 // One lane's share of the row of atom i (slots j, j+8, j+16, ... of its m
 // partners), U blocks of slots per round.  base = this lane's entry in the
-// group's first block.  Every lane loads every block of a round (the stream
-// holds kPairTail spare entries after its last group, (THP_GROW_PF + 1) U <=
-// kPairTail / 32); a slot past m counts as the lane's own atom with zero
-// coefficients.  WRAP = false skips the periodic wrap: the caller has
+// group's first block.  Every lane of the warp loads every block of a round
+// up to the group's last; a slot past m counts as the lane's own atom with
+// zero coefficients.  WRAP = false skips the periodic wrap: the caller has
 // checked that the group's atoms lie farther than the cutoff from every face
 // of the box, so no pair crosses one.
 template <typename T, int U, bool NOL1, bool WRAP, typename Ld, typename Im>
@@ -189,16 +194,17 @@ __device__ __forceinline__ void group_row_part(const PairRows& pr, const Ld& ld,
   const int mj = m - j;  // slot 8 b + j is a partner while 8 b < mj
   int k[U];
   T c3[U], c5[U];
-  if (THP_GROW_PF) stream_round<T, U, NOL1>(pk, pc, 0, mj, i_safe, k, c3, c5);
+  if (THP_GROW_PF) stream_round<T, U, NOL1>(pk, pc, 0, mj, nblk, i_safe, k, c3, c5);
 #pragma unroll 1
   for (int b = 0; b < nblk; b += U) {
-    if (!THP_GROW_PF) stream_round<T, U, NOL1>(pk + 32 * b, pc + 32 * b, b, mj, i_safe, k, c3, c5);
+    if (!THP_GROW_PF) stream_round<T, U, NOL1>(pk + 32 * b, pc + 32 * b, b, mj, nblk, i_safe, k, c3, c5);
     T p[U][3], w[U][6];
 #pragma unroll
     for (int u = 0; u < U; ++u) ld.load(k[u], p[u], w[u]);
     int kn[U];
     T c3n[U], c5n[U];
-    if (THP_GROW_PF) stream_round<T, U, NOL1>(pk + 32 * (b + U), pc + 32 * (b + U), b + U, mj, i_safe, kn, c3n, c5n);
+    if (THP_GROW_PF)
+      stream_round<T, U, NOL1>(pk + 32 * (b + U), pc + 32 * (b + U), b + U, mj, nblk, i_safe, kn, c3n, c5n);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       T xr = p[u][0] - pi[0], yr = p[u][1] - pi[1], zr = p[u][2] - pi[2];
