@@ -76,7 +76,7 @@ def lib():
         L.or_newinduce_pme2.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.POINTER(OrSolveInfo)]
         L.or_epolar.restype = C.c_double
         L.or_epolar.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
-        L.or_epolar1.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, _dp, _dp]
+        L.or_epolar1.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, _dp, _dp, _dp, _dp]
         L.or_empole1.argtypes = [C.c_void_p, _ip, _ip, _ip, _dp, _dp]
         L.or_ehal1.argtypes = [C.c_void_p, C.POINTER(OrVdw), _dp, _dp]
         L.or_rotpole.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _dp]
@@ -218,18 +218,27 @@ class Oracle:
         return {"uind": uind, "uinp": uinp, "ef": ef, "niter": info.niter,
                 "converged": bool(info.converged), "resnrm": info.resnrm, "ene": tuple(info.ene)}
 
-    def epolar1(self, uind, uinp):
-        """Energy and gradient dE/dx [n,3] (kcal/mol/A), epolar1c."""
+    def epolar1(self, uind, uinp, virial=False):
+        """Energy and gradient dE/dx [n,3] (kcal/mol/A), epolar1c; with
+        virial=True also the internal virial vir(3,3) (kcal/mol) as the
+        reference accumulates it and the frame-atom virial of the
+        reciprocal and self torques it leaves out (their sum is the strain
+        derivative of the energy)."""
         uind = np.ascontiguousarray(uind, dtype=np.float64)
         uinp = np.ascontiguousarray(uinp, dtype=np.float64)
         dep = np.zeros((self.ws.n, 3))
         ep = C.c_double()
         ws = self.ws
+        vir = np.zeros((3, 3)) if virial else None
+        vfr = np.zeros((3, 3)) if virial else None
         st = lib().or_epolar1(self.ctx, _p(uind), _p(uinp), _p(np.ascontiguousarray(ws.zaxis, np.int32), _ip),
                               _p(np.ascontiguousarray(ws.xaxis, np.int32), _ip),
-                              _p(np.ascontiguousarray(ws.axt, np.int32), _ip), _p(dep), C.byref(ep))
+                              _p(np.ascontiguousarray(ws.axt, np.int32), _ip), _p(dep), C.byref(ep), _p(vir),
+                              _p(vfr))
         if st != 0:
             raise RuntimeError(f"oracle epolar1 status {st}")
+        if virial:
+            return ep.value, dep, vir, vfr
         return ep.value, dep
 
     def empole1(self):

@@ -1438,13 +1438,20 @@ void or_rotpole(int n, const double* x, const double* y, const double* z, const 
 // Polarization forces: epolar1c (epolar1.f:57-372) = eprecip1 (:397-1213)
 // + epreal1c (:1215-2540, Thole branch, dpequal false) + self energy and
 // self torque (:181-206), torques distributed by torque (torque.f:6-390).
-// Virial terms are not restated.
+// With vir_out, also the internal virial (TINFOIL boundary, no charge flux):
+// eprecip1's per-site induced terms (:846-908) and scalar sums over the
+// reciprocal lattice ((rpole+uinp) x (rpole+uind) minus the permanent-only
+// sum, :534-541, :932-1091), epreal1c's pairwise terms (:2326-2342) and the
+// torque's frame-atom terms (:2460-2486).  The reference adds no virial for
+// the frame-atom forces of the reciprocal torque (distributed by torque_rec)
+// nor of the self torque; vir_frame (may be NULL) receives those separately:
+// vir + vir_frame is the strain derivative of the energy.
 namespace {
 
 // torque.f:6-390 for Z-then-X and Bisector frames (the water frames);
 // frame atoms 0-based; adds the forces of a torque on site i into de[n][3]
 void torque_site(const double* x, const double* y, const double* z, int ib, int ia, int ic, int axt,
-                 const double trq[3], double* de) {
+                 const double trq[3], double* de, double* fz = nullptr, double* fx = nullptr) {
   double u[3] = {x[ia] - x[ib], y[ia] - y[ib], z[ia] - z[ib]};
   double usiz = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
   double v[3] = {x[ic] - x[ib], y[ic] - y[ib], z[ic] - z[ib]};
@@ -1484,7 +1491,91 @@ void torque_site(const double* x, const double* y, const double* z, int ib, int 
     de[ia * 3 + j] += du;
     de[ic * 3 + j] += dv;
     de[ib * 3 + j] -= du + dv;
+    if (fz) fz[j] = du;  // frcz of torque.f: on the z-axis atom
+    if (fx) fx[j] = dv;  // frcx: on the x-axis atom
   }
+}
+
+// the virial tensor, symmetric, in the accumulation order of the reference
+struct Vir {
+  double xx = 0, xy = 0, xz = 0, yy = 0, yz = 0, zz = 0;
+  void add(double a, double b, double c, double d, double e, double f) {
+    xx += a; xy += b; xz += c; yy += d; yz += e; zz += f;
+  }
+  // the k-space scalar-sum terms: h h vterm - eterm (emrecip1 / eprecip1)
+  void add_k(double h1, double h2, double h3, double vterm, double eterm, double sign) {
+    add(sign * (h1 * h1 * vterm - eterm), sign * h1 * h2 * vterm, sign * h1 * h3 * vterm,
+        sign * (h2 * h2 * vterm - eterm), sign * h2 * h3 * vterm, sign * (h3 * h3 * vterm - eterm));
+  }
+  void out(double* v) const {
+    v[0] = xx; v[1] = xy; v[2] = xz; v[3] = xy; v[4] = yy; v[5] = yz; v[6] = xz; v[7] = yz; v[8] = zz;
+  }
+};
+
+// Sum over the reciprocal lattice (all k but 0, where qfac > 0) of the PME
+// virial terms of a structure factor product struc2(k): eterm =
+// 0.5 f qfac struc2, vterm = (2/h^2)(1 + pterm h^2) eterm (eprecip1,
+// epolar1.f:1041-1091; emrecip1 for the permanent-only sum).
+template <class S2>
+void kspace_virial(const OrCtx* c, double f, double sign, S2&& struc2, Vir& v) {
+  const OrSystem& s = c->s;
+  const double pterm = (kPi / s.aewald) * (kPi / s.aewald);
+  const int nf1 = (s.nfft1 + 1) / 2, nf2 = (s.nfft2 + 1) / 2, nf3 = (s.nfft3 + 1) / 2;
+  for (int k3 = 0; k3 < s.nfft3; ++k3)
+    for (int k2 = 0; k2 < s.nfft2; ++k2)
+      for (int k1 = 0; k1 < s.nfft1; ++k1) {
+        const size_t idx = ((size_t)k3 * s.nfft2 + k2) * s.nfft1 + k1;
+        const double qf = c->qfac[idx];
+        if (qf == 0.0) continue;
+        int m1 = k1, m2 = k2, m3 = k3;
+        if (k1 + 1 > nf1) m1 -= s.nfft1;
+        if (k2 + 1 > nf2) m2 -= s.nfft2;
+        if (k3 + 1 > nf3) m3 -= s.nfft3;
+        const double h1 = c->recip[0][0] * m1 + c->recip[0][1] * m2 + c->recip[0][2] * m3;
+        const double h2 = c->recip[1][0] * m1 + c->recip[1][1] * m2 + c->recip[1][2] * m3;
+        const double h3 = c->recip[2][0] * m1 + c->recip[2][1] * m2 + c->recip[2][2] * m3;
+        const double hsq = h1 * h1 + h2 * h2 + h3 * h3;
+        const double eterm = 0.5 * f * qf * struc2(k1, k2, k3, idx);
+        const double vterm = (2.0 / hsq) * (1.0 + pterm * hsq) * eterm;
+        v.add_k(h1, h2, h3, vterm, eterm, sign);
+      }
+}
+
+// The virial of a torque's frame-atom forces (epolar1.f:2460-2486): fz on
+// the z-axis atom, fx on the x-axis atom (water frames have no y-axis atom).
+void frame_virial(const double* x, const double* y, const double* z, int i, int iz, int ix, const double fz[3],
+                  const double fx[3], Vir& v) {
+  const double xiz = x[iz] - x[i], yiz = y[iz] - y[i], ziz = z[iz] - z[i];
+  const double xix = x[ix] - x[i], yix = y[ix] - y[i], zix = z[ix] - z[i];
+  v.add(xix * fx[0] + xiz * fz[0], 0.5 * (yix * fx[0] + yiz * fz[0] + xix * fx[1] + xiz * fz[1]),
+        0.5 * (zix * fx[0] + ziz * fz[0] + xix * fx[2] + xiz * fz[2]), yix * fx[1] + yiz * fz[1],
+        0.5 * (zix * fx[1] + ziz * fz[1] + yix * fx[2] + yiz * fz[2]), zix * fx[2] + ziz * fz[2]);
+}
+
+// fmp (fractional multipoles) of cmp with the dipole replaced by dip + add3
+void frac_moments(const double ctf[10][10], const double cm[10], const double* add3, double fm[10]) {
+  double c2[10];
+  for (int q = 0; q < 10; ++q) c2[q] = cm[q];
+  if (add3)
+    for (int q = 0; q < 3; ++q) c2[1 + q] += add3[q];
+  fm[0] = ctf[0][0] * c2[0];
+  for (int j = 1; j < 4; ++j) {
+    fm[j] = 0.0;
+    for (int k = 1; k < 4; ++k) fm[j] += ctf[j][k] * c2[k];
+  }
+  for (int j = 4; j < 10; ++j) {
+    fm[j] = 0.0;
+    for (int k = 4; k < 10; ++k) fm[j] += ctf[j][k] * c2[k];
+  }
+}
+
+// grid_mpole_site (pmestuff.f:163-278) terms of one site's fmp
+inline double mpole_stencil(const double* f, const double* t, const double* u, const double* v) {
+  double term0 = f[0] * u[0] * v[0] + f[2] * u[1] * v[0] + f[3] * u[0] * v[1] + f[5] * u[2] * v[0] +
+                 f[6] * u[0] * v[2] + f[9] * u[1] * v[1];
+  double term1 = f[1] * u[0] * v[0] + f[7] * u[1] * v[0] + f[8] * u[0] * v[1];
+  double term2 = f[4] * u[0] * v[0];
+  return term0 * t[0] + term1 * t[1] + term2 * t[2];
 }
 
 }  // namespace
@@ -1602,12 +1693,13 @@ int or_fphi_uind_sites(OrCtx* c, int nsites, const int* isite, const double* gri
 }
 
 int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxis, const int* xaxis,
-               const int* axt, double* dep, double* ep_out) {
+               const int* axt, double* dep, double* ep_out, double* vir_out, double* vir_frame) {
   const OrSystem& s = c->s;
   const int n = s.n, bs = c->bsorder, maxelst = c->maxelst;
   if (!c->have_list) return OR_E_LIST_OVERFLOW;
   std::fill(dep, dep + (size_t)n * 3, 0.0);
   double ep = 0.0;
+  Vir vir, vframe;  // the reference's virial; the frame-atom virial of the reciprocal and self torques
   // permanent-multipole potential fphirec (20 per site) from efld0_recip
   {
     std::vector<double> cphi((size_t)n * 10);
@@ -1718,9 +1810,73 @@ int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxi
                cm[8] * cp[4] - cm[9] * cp[7];
       trq[2] = cm[2] * cp[1] - cm[1] * cp[2] + 2.0 * (cm[5] - cm[4]) * cp[7] + cm[7] * cp[4] + cm[9] * cp[8] -
                cm[7] * cp[5] - cm[8] * cp[9];
-      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], trq, dep);
+      {
+        double fz[3], fx[3];
+        torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], trq, dep, fz, fx);
+        frame_virial(s.x, s.y, s.z, i, zaxis[i], xaxis[i], fz, fx, vframe);
+      }
+      if (vir_out) {
+        // induced dipole contribution to the internal virial (epolar1.f:846-908);
+        // 1-based names: cphim/cphid/cphip(2:4), cphidprec(1:10) = cp, cmp(1:10) = cm
+        double cm_[4] = {0, 0, 0, 0}, cd_[4] = {0, 0, 0, 0}, cq_[4] = {0, 0, 0, 0};
+        for (int j = 1; j <= 3; ++j)
+          for (int k = 1; k <= 3; ++k) {
+            cm_[j] += ftc[j][k] * FR[k + 1];
+            cd_[j] += ftc[j][k] * FD[k + 1];
+            cq_[j] += ftc[j][k] * FP[k + 1];
+          }
+        const double* ui = &uind[i * 3];
+        const double* up = &uinp[i * 3];
+        double vxx = -cp[1] * cm[1] - 0.5 * (cm_[1] * (ui[0] + up[0]) + cd_[1] * up[0] + cq_[1] * ui[0]);
+        double vxy = -0.5 * (cp[1] * cm[2] + cp[2] * cm[1]) -
+                     0.25 * (cm_[1] * (ui[1] + up[1]) + cm_[2] * (ui[0] + up[0]) + cd_[1] * up[1] + cq_[1] * ui[1] +
+                             cd_[2] * up[0] + cq_[2] * ui[0]);
+        double vxz = -0.5 * (cp[1] * cm[3] + cp[3] * cm[1]) -
+                     0.25 * (cm_[1] * (ui[2] + up[2]) + cm_[3] * (ui[0] + up[0]) + cd_[1] * up[2] + cq_[1] * ui[2] +
+                             cd_[3] * up[0] + cq_[3] * ui[0]);
+        double vyy = -cp[2] * cm[2] - 0.5 * (cm_[2] * (ui[1] + up[1]) + cd_[2] * up[1] + cq_[2] * ui[1]);
+        double vyz = -0.5 * (cp[2] * cm[3] + cp[3] * cm[2]) -
+                     0.25 * (cm_[2] * (ui[2] + up[2]) + cm_[3] * (ui[1] + up[1]) + cd_[2] * up[2] + cq_[2] * ui[2] +
+                             cd_[3] * up[1] + cq_[3] * ui[1]);
+        double vzz = -cp[3] * cm[3] - 0.5 * (cm_[3] * (ui[2] + up[2]) + cd_[3] * up[2] + cq_[3] * ui[2]);
+        vxx += -2.0 * cm[4] * cp[4] - cm[7] * cp[7] - cm[8] * cp[8];
+        vxy += -(cm[4] + cm[5]) * cp[7] - 0.5 * (cm[7] * (cp[5] + cp[4]) + cm[8] * cp[9] + cm[9] * cp[8]);
+        vxz += -(cm[4] + cm[6]) * cp[8] - 0.5 * (cm[8] * (cp[4] + cp[6]) + cm[7] * cp[9] + cm[9] * cp[7]);
+        vyy += -2.0 * cm[5] * cp[5] - cm[7] * cp[7] - cm[9] * cp[9];
+        vyz += -(cm[5] + cm[6]) * cp[9] - 0.5 * (cm[9] * (cp[5] + cp[6]) + cm[7] * cp[8] + cm[8] * cp[7]);
+        vzz += -2.0 * cm[6] * cp[6] - cm[8] * cp[8] - cm[9] * cp[9];
+        vir.add(vxx, vxy, vxz, vyy, vyz, vzz);
+      }
     }
     ep += 0.5 * erec;
+    if (vir_out) {
+      const int nthr = nthreads_of(&s);
+      const int n1 = s.nfft1, n2 = s.nfft2, n3 = s.nfft3;
+      // minus the permanent-only scalar sum (the multipole term's own virial,
+      // removed as eprecip1 does with -vmxx..., epolar1.f:534-541)
+      spread_sites(c, [&](int i, const double* t, const double* u, const double* v) {
+        return cd(mpole_stencil(&fmp[(size_t)i * 10], t, u, v), 0.0);
+      });
+      fft3d_impl(c->grid.data(), n1, n2, n3, -1, nthr);
+      kspace_virial(c, f, -1.0, [&](int, int, int, size_t idx) { return std::norm(c->grid[idx]); }, vir);
+      // (rpole + uinp) x (rpole + uind) scalar sum (epolar1.f:932-1091): the two
+      // real grids in the real and imaginary parts of one transform
+      std::vector<double> fa((size_t)n * 10), fb((size_t)n * 10);
+      for (int i = 0; i < n; ++i) {
+        frac_moments(ctf, &cmp[(size_t)i * 10], &uinp[i * 3], &fa[(size_t)i * 10]);
+        frac_moments(ctf, &cmp[(size_t)i * 10], &uind[i * 3], &fb[(size_t)i * 10]);
+      }
+      spread_sites(c, [&](int i, const double* t, const double* u, const double* v) {
+        return cd(mpole_stencil(&fa[(size_t)i * 10], t, u, v), mpole_stencil(&fb[(size_t)i * 10], t, u, v));
+      });
+      fft3d_impl(c->grid.data(), n1, n2, n3, -1, nthr);
+      kspace_virial(c, f, 1.0, [&](int k1, int k2, int k3, size_t idx) {
+        const size_t mi = ((size_t)((n3 - k3) % n3) * n2 + (n2 - k2) % n2) * n1 + (n1 - k1) % n1;
+        const cd g = c->grid[idx], gm = std::conj(c->grid[mi]);
+        const cd fa_k = 0.5 * (g + gm), fb_k = cd(0.0, -0.5) * (g - gm);
+        return fa_k.real() * fb_k.real() + fa_k.imag() * fb_k.imag();
+      }, vir);
+    }
   }
   // ---- epreal1c (Thole branch) -------------------------------------------
   {
@@ -1963,6 +2119,9 @@ int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxi
           dep[i * 3 + j] -= frc[j];
           dep[k * 3 + j] += frc[j];
         }
+        // the virial of the pairwise Cartesian forces (epolar1.f:2326-2342)
+        vir.add(xr * frc[0], 0.5 * (yr * frc[0] + xr * frc[1]), 0.5 * (zr * frc[0] + xr * frc[2]), yr * frc[1],
+                0.5 * (zr * frc[1] + yr * frc[2]), zr * frc[2]);
       }
       reset_dp_scales(s, i, w);
       set_u_scales(s, i, w, true);
@@ -1981,7 +2140,10 @@ int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxi
                (qixx - qizz) * du[3];
       tep[2] = diy * uf[0] - dix * uf[1] + qiyz * du[3] - qixz * du[4] + 2.0 * qixy * (du[0] - du[2]) +
                (qiyy - qixx) * du[1];
-      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], tep, dep);
+      double fz[3], fx[3];
+      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], tep, dep, fz, fx);
+      // the virial of the torque's frame-atom forces (epolar1.f:2460-2486)
+      frame_virial(s.x, s.y, s.z, i, zaxis[i], xaxis[i], fz, fx, vir);
     }
   }
   // ---- self energy and self torque (epolar1.f:181-206) --------------------
@@ -2002,10 +2164,14 @@ int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxi
       double uiy = 0.5 * (uind[i * 3 + 1] + uinp[i * 3 + 1]);
       double uiz = 0.5 * (uind[i * 3 + 2] + uinp[i * 3 + 2]);
       double trq[3] = {term * (diy * uiz - diz * uiy), term * (diz * uix - dix * uiz), term * (dix * uiy - diy * uix)};
-      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], trq, dep);
+      double fz[3], fx[3];
+      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], trq, dep, fz, fx);
+      frame_virial(s.x, s.y, s.z, i, zaxis[i], xaxis[i], fz, fx, vframe);
     }
   }
   if (ep_out) *ep_out = ep;
+  if (vir_out) vir.out(vir_out);
+  if (vir_frame) vframe.out(vir_frame);
   return OR_OK;
 }
 

@@ -93,9 +93,13 @@ double or_epolar(OrCtx* c, const double* uind, double* ereal, double* erecip, do
 
 /* epolar1c (epolar1.f:57-372): polarization energy and its gradient dep
  * [n][3] (kcal/mol/A) from converged uind/uinp; frames (zaxis, xaxis, axt
- * as in or_rotpole) distribute the torques (torque.f:6). */
+ * as in or_rotpole) distribute the torques (torque.f:6).  vir (may be NULL):
+ * the internal virial vir(3,3) (kcal/mol, symmetric, row-major) of the
+ * TINFOIL boundary as the reference accumulates it; vir_frame (may be NULL):
+ * the frame-atom virial of the reciprocal and self torques, which the
+ * reference leaves out (vir + vir_frame is the strain derivative). */
 int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxis, const int* xaxis,
-               const int* axt, double* dep, double* ep);
+               const int* axt, double* dep, double* ep, double* vir, double* vir_frame);
 
 /* empole1c (empole1.f:42-340): permanent-multipole energy and gradient dem
  * [n][3] (kcal/mol/A) at the current positions, TINFOIL boundary; needs the

@@ -233,6 +233,31 @@ def test_epolar1_gradient_matches_finite_differences(box216):
             assert abs(fd - dep[atom, d]) < 1e-5 * np.abs(dep).max() + 1e-6, (atom, d, fd, dep[atom, d])
 
 
+def test_epolar1_virial_matches_strain_derivative(box216):
+    # Scaling every x coordinate and the box edge along x by (1 + eps), the
+    # frames rotating with the atoms and the dipoles solved again: the
+    # central difference of the energy is vir(1,1) + the frame-atom virial
+    # of the reciprocal and self torques (the reference's virial leaves the
+    # latter out); likewise along y and z.  The tensor is symmetric.
+    _, orc, res = _energy(box216)
+    _, _, vir, vfr = orc.epolar1(res["uind"], res["uinp"], virial=True)
+    np.testing.assert_allclose(vir, vir.T, rtol=0, atol=1e-12 * np.abs(vir).max())
+    eps = 1e-5
+    pos0 = box216.positions()
+    for a in range(3):
+        e = []
+        for sgn in (1, -1):
+            p = pos0.copy()
+            p[:, a] *= 1.0 + sgn * eps
+            box = list(box216.box)
+            box[a] *= 1.0 + sgn * eps
+            e.append(_energy(dataclasses.replace(box216.with_positions(p), box=tuple(box)))[0])
+        fd = (e[0] - e[1]) / (2 * eps)
+        assert abs(fd - (vir[a, a] + vfr[a, a])) < 2e-6 * abs(fd), (a, fd, vir[a, a], vfr[a, a])
+        # the terms the reference leaves out are small but not negligible
+        assert abs(vfr[a, a]) < 1e-2 * abs(fd)
+
+
 def test_energy_independent_of_ewald_alpha(thp):
     # Epol is a physical quantity: at a converged real-space cutoff (9 A) and
     # grid (0.45 A spacing) the Ewald split alpha must not change it.  The
