@@ -169,6 +169,21 @@ int thp_get_gradient(thp_ctx* ctx, double* dep, double* ep);
 /* same gradient into device memory d_dep [n][3], enqueued on the context's
  * stream without a host synchronisation */
 int thp_get_gradient_device(thp_ctx* ctx, double* d_dep);
+/* on != 0: every later gradient call also computes the internal virial of
+ * the polarization energy (TINFOIL boundary): eprecip1's induced-dipole
+ * site terms (epolar1.f:846-908) and scalar sums over the reciprocal
+ * lattice ((rpole+uinp) x (rpole+uind) minus the permanent-only sum,
+ * :534-541, :932-1091), epreal1c's pair terms (:2326-2342) and the frame-atom
+ * terms of its torques (:2460-2486).  It costs one more grid spread and
+ * forward transform and two passes over the grid per call. */
+int thp_set_virial(thp_ctx* ctx, int on);
+/* vir [3][3] (kcal/mol, symmetric) of the last gradient call made with the
+ * virial on (THP_E_STATE otherwise).  form 0: as the reference accumulates
+ * it; form 1: plus the frame-atom virial of the reciprocal and self torques,
+ * which the reference does not add (torque_rec / torque carry no virial):
+ * the derivative of the energy with respect to a homogeneous strain of the
+ * box and the coordinates. */
+int thp_get_virial(thp_ctx* ctx, int form, double* vir);
 /* m2scale..m5scale [4] of the permanent-multipole pair terms (mplpot module;
  * defaults initprm.f:413-416: 0, 0, 1, 1; AMOEBA water03.prm:34-37: 0, 0,
  * 0.4, 0.8).  The 1-2..1-5 lists come from thp_set_connectivity. */
@@ -338,7 +353,9 @@ int thp_server_destroy(thp_server* s);
  * THP_NOALLOC_MAX_ATOMS, otherwise THP_E_INVALID.  The first call on a device
  * looks up the scratch's device address and should come before any stream
  * capture.  All calls share the scratch: calls that overlap on the GPU race,
- * so order them on one stream. */
+ * so order them on one stream.  The looked-up address is kept for the life
+ * of the process: calls after a cudaDeviceReset of that device are not
+ * supported. */
 #define THP_NOALLOC_MAX_ATOMS 4194304
 int thp_epolar_noalloc(int n, const double* d_uind, const double* d_ef, double* d_epol, void* stream);
 
@@ -351,6 +368,9 @@ int thp_bind_state(thp_ctx* ctx, double* x, double* y, double* z, double* rpole,
 int thp_last_error(void);
 /* bind deriv::dep(3,n), written by epolar1_ */
 int thp_bind_gradient(thp_ctx* ctx, double* dep);
+/* bind virial::vir(3,3) (may be NULL): epolar1_ adds the polarization virial
+ * into it (form 0 of thp_get_virial), as epolar1c adds into vir */
+int thp_bind_virial(thp_ctx* ctx, double* vir);
 /* bind neigh::nvlst(n) and vlst(maxvlst,n), filled by vlistcell_ */
 int thp_bind_vlist(thp_ctx* ctx, int* nvlst, int* vlst, int maxvlst);
 /* bind energi::ev and deriv::dev(3,n), written by ehal1_ (may be NULL) */

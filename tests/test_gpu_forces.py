@@ -121,3 +121,29 @@ def test_epolar1_dropin(lib, case):
     ep_ref, dep_ref = orc.epolar1(uind, uinp)
     assert abs(ep[0] - ep_ref) < 1e-10 * abs(ep_ref)
     assert rel(dep, dep_ref) < 1e-9
+
+
+def test_mixed_gradient_close_contact(lib, thp):
+    # Two waters at a hydrogen-bond contact much closer than in the boxes
+    # (O...H 1.2 A): the mixed pair terms (FP32 rsqrt and products) against
+    # the FP64 form on the same dipoles, at the two close atoms.
+    ws = thp.water.make_water_box(216, cfg=0)
+    pos = ws.positions().copy()
+    L = ws.box[0]
+    o_a, o_b = 3 * 20, 3 * 120
+    h_b = o_b + 1
+    # move water b rigidly so its first H sits 1.2 A from O of water a
+    d = pos[o_a] + np.array([1.2, 0.0, 0.0]) - pos[h_b]
+    pos[o_b:o_b + 3] += d
+    pos -= L * np.floor(pos / L + 0.5)
+    ws2 = ws.with_positions(pos)
+    f64 = lib.Context(ws2, precision=lib.FP64, poleps=1e-10)
+    assert f64.solve()["converged"]
+    _, g64 = f64.gradient()
+    mx = lib.Context(ws2, precision=lib.MIXED, poleps=1e-10)
+    assert mx.solve()["converged"]
+    _, g32 = mx.gradient()
+    for atom in (o_a, h_b):
+        err = np.linalg.norm(g32[atom] - g64[atom]) / np.linalg.norm(g64[atom])
+        # the close pair's force is large; FP32 pair arithmetic keeps it to ~1e-5
+        assert err < 1e-4, (atom, err, g64[atom], g32[atom])

@@ -388,7 +388,7 @@ void free_ctx(Ctx& c) {
   void* ptrs[] = {c.slab_cells, c.slab_atoms, c.slab_pairs, c.d_sp_off, c.d_sp_k, c.d_sp_ks, c.d_sp_s, c.d_sp_c,
                   c.d_cg, c.d_flags, c.d_fphirec, c.d_depfix, c.d_trq, c.d_frs, c.d_grad, c.d_sgrid, c.d_sscratch,
                   c.d_alt, c.d_empart, c.d_vcls, c.d_vired, c.d_vkred, c.d_vtab, c.d_vred, c.d_vinfo,
-                  c.d_evpart, c.d_vnb, c.d_vnnb, c.d_vpos_built, c.d_vredf, c.d_muf};
+                  c.d_evpart, c.d_vnb, c.d_vnnb, c.d_vpos_built, c.d_vredf, c.d_muf, c.d_virp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   pme_free(c);
@@ -1390,7 +1390,30 @@ int thp_get_gradient_device(thp_ctx* h, double* d_dep) {
   Ctx& c = h->c;
   if (!c.have_axes || !c.have_dipoles || !h->field_valid || !h->solved_once) return THP_E_STATE;
   if (set_current_device(c)) return THP_E_CUDA;
-  return launch_forces(c, d_dep);
+  c.have_virial = false;
+  const int st = launch_forces(c, d_dep);
+  c.have_virial = st == THP_OK && c.want_virial;  // totals land in h_vir when the stream reaches them
+  return st;
+}
+
+int thp_set_virial(thp_ctx* h, int on) {
+  if (!h) return THP_E_INVALID;
+  h->c.want_virial = on != 0;
+  return THP_OK;
+}
+
+int thp_get_virial(thp_ctx* h, int form, double* vir) {
+  if (!h || !vir || form < 0 || form > 1) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (!c.have_virial) return THP_E_STATE;
+  if (set_current_device(c)) return THP_E_CUDA;
+  int st = cuda_status(cudaStreamSynchronize(c.stream), &c, "virial");
+  if (st) return st;
+  double v[6];
+  for (int q = 0; q < 6; ++q) v[q] = c.h_vir[q] + (form == 1 ? c.h_vir[6 + q] : 0.0);
+  const double t[9] = {v[0], v[1], v[2], v[1], v[3], v[4], v[2], v[4], v[5]};
+  std::memcpy(vir, t, sizeof(t));
+  return THP_OK;
 }
 
 int thp_get_gradient(thp_ctx* h, double* dep, double* ep) {
@@ -1675,6 +1698,12 @@ int thp_bind_grid(thp_ctx* h, double* qgrid) {
   return THP_OK;
 }
 
+int thp_bind_virial(thp_ctx* h, double* vir) {
+  if (!h) return THP_E_INVALID;
+  h->c.bvir = vir;
+  return THP_OK;
+}
+
 int thp_bind_gradient(thp_ctx* h, double* dep) {
   if (!h) return THP_E_INVALID;
   h->c.bdep = dep;
@@ -1785,7 +1814,15 @@ void epolar1_(void) {
   if (!st) st = thp_solve(h, THP_GUESS_DIRECT, &info);
   if (!st || st == THP_E_NOT_CONVERGED) {
     int st2 = THP_OK;
-    if (h->c.bdep) st2 = thp_get_gradient(h, h->c.bdep, nullptr);
+    if (h->c.bdep) {
+      h->c.want_virial = h->c.bvir != nullptr;
+      st2 = thp_get_gradient(h, h->c.bdep, nullptr);
+      if (!st2 && h->c.bvir) {  // epolar1c adds into vir (epolar1.f:2334-2342)
+        double v[9];
+        st2 = thp_get_virial(h, 0, v);
+        for (int q = 0; !st2 && q < 9; ++q) h->c.bvir[q] += v[q];
+      }
+    }
     if (!st2 && h->c.bep) *h->c.bep = info.epol;
     if (!st2 && h->c.buind) st2 = thp_get_dipoles(h, h->c.buind, h->c.buinp);
     if (st2) st = st2;

@@ -206,6 +206,13 @@ struct Ctx {
   double* d_fphirec = nullptr;    // [n][20] permanent-multipole potential, fractional
   unsigned long long* d_depfix = nullptr;  // [n][3] 64-bit fixed-point gradient, sorted
   double* d_trq = nullptr;        // [n][3] reciprocal-space torque
+  // virial of the polarization gradient (thp_set_virial): partial sums on
+  // the device, and the last gradient call's totals: the reference's terms
+  // (xx xy xz yy yz zz), then the reciprocal and self torques' frame terms
+  bool want_virial = false, have_virial = false;
+  double* d_virp = nullptr;
+  size_t virp_cap = 0;
+  double h_vir[12] = {};
   int* d_frs = nullptr;           // [n][3] frame atoms (sorted indices), axis type
   double* d_grad = nullptr;       // [n][3] gradient, original order
 
@@ -221,6 +228,7 @@ struct Ctx {
   int *bnelst = nullptr, *belst = nullptr;
   int bmaxelst = 0;
   double* bdep = nullptr;
+  double* bvir = nullptr;  // virial::vir(3,3), added to by epolar1_
   double *bem = nullptr, *bdem = nullptr;  // energi::em, deriv::dem(3,n), written by empole1_
   double *bev = nullptr, *bdev = nullptr;  // energi::ev, deriv::dev(3,n), written by ehal1_
   int *bnvlst = nullptr, *bvlst = nullptr;  // neigh::nvlst(n), vlst(maxvlst,n), filled by vlistcell_

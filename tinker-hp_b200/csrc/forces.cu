@@ -30,15 +30,19 @@ constexpr int kBlock = 128;
 // fphi_uind_site (pmestuff.f:746-1045) in full and the force / torque of
 // eprecip1 (epolar1.f:636-720).  fphirec: [n][20] permanent potential
 // (unscaled), written by the field pass.
-template <typename T>
+// VIR: each block also writes the sum of its sites' induced-dipole virial
+// terms (epolar1.f:846-908) to vpart[block][6].
+template <typename T, bool VIR>
 __global__ void __launch_bounds__(kBlock) k_force_recip(int n, PmeGeom g, const double4* __restrict__ pos,
                                                         const typename Cplx<T>::type* __restrict__ grid,
                                                         const double* __restrict__ fphirec,
                                                         const double* __restrict__ mu, const double* __restrict__ rp,
                                                         double* __restrict__ trq_out,
-                                                        unsigned long long* __restrict__ dep) {
+                                                        unsigned long long* __restrict__ dep,
+                                                        double* __restrict__ vpart) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  double vs[6] = {0, 0, 0, 0, 0, 0};
+  if (i < n) {
   const double4 p = pos[i];
   T tx[kBs][4], ty[kBs][4], tz[kBs][4];
   const int gx = bspline_axis<4, T>(p.x, g.recip[0], g.n1, tx);
@@ -149,6 +153,40 @@ __global__ void __launch_bounds__(kBlock) k_force_recip(int n, PmeGeom g, const 
          cm[8] * cp[4] - cm[9] * cp[7];
   t[2] = cm[2] * cp[1] - cm[1] * cp[2] + 2.0 * (cm[5] - cm[4]) * cp[7] + cm[7] * cp[4] + cm[9] * cp[8] -
          cm[7] * cp[5] - cm[8] * cp[9];
+  if (VIR) {
+    // induced dipole contribution to the internal virial (epolar1.f:846-908):
+    // cphim, cphid, cphip = Cartesian gradients of the permanent, d and p
+    // potentials; 1-based cphidprec(1:10) = cp, cmp(1:10) = cm
+    const double cmx[4] = {0, g.a[0] * FR[2], g.a[1] * FR[3], g.a[2] * FR[4]};
+    const double cdx[4] = {0, g.a[0] * FD[2], g.a[1] * FD[3], g.a[2] * FD[4]};
+    const double cpx[4] = {0, g.a[0] * FP[2], g.a[1] * FP[3], g.a[2] * FP[4]};
+    const double ui[3] = {m[0], m[1], m[2]}, up[3] = {m[3], m[4], m[5]};
+    vs[0] = -cp[1] * cm[1] - 0.5 * (cmx[1] * (ui[0] + up[0]) + cdx[1] * up[0] + cpx[1] * ui[0]);
+    vs[1] = -0.5 * (cp[1] * cm[2] + cp[2] * cm[1]) -
+            0.25 * (cmx[1] * (ui[1] + up[1]) + cmx[2] * (ui[0] + up[0]) + cdx[1] * up[1] + cpx[1] * ui[1] +
+                    cdx[2] * up[0] + cpx[2] * ui[0]);
+    vs[2] = -0.5 * (cp[1] * cm[3] + cp[3] * cm[1]) -
+            0.25 * (cmx[1] * (ui[2] + up[2]) + cmx[3] * (ui[0] + up[0]) + cdx[1] * up[2] + cpx[1] * ui[2] +
+                    cdx[3] * up[0] + cpx[3] * ui[0]);
+    vs[3] = -cp[2] * cm[2] - 0.5 * (cmx[2] * (ui[1] + up[1]) + cdx[2] * up[1] + cpx[2] * ui[1]);
+    vs[4] = -0.5 * (cp[2] * cm[3] + cp[3] * cm[2]) -
+            0.25 * (cmx[2] * (ui[2] + up[2]) + cmx[3] * (ui[1] + up[1]) + cdx[2] * up[2] + cpx[2] * ui[2] +
+                    cdx[3] * up[1] + cpx[3] * ui[1]);
+    vs[5] = -cp[3] * cm[3] - 0.5 * (cmx[3] * (ui[2] + up[2]) + cdx[3] * up[2] + cpx[3] * ui[2]);
+    vs[0] += -2.0 * cm[4] * cp[4] - cm[7] * cp[7] - cm[8] * cp[8];
+    vs[1] += -(cm[4] + cm[5]) * cp[7] - 0.5 * (cm[7] * (cp[5] + cp[4]) + cm[8] * cp[9] + cm[9] * cp[8]);
+    vs[2] += -(cm[4] + cm[6]) * cp[8] - 0.5 * (cm[8] * (cp[4] + cp[6]) + cm[7] * cp[9] + cm[9] * cp[7]);
+    vs[3] += -2.0 * cm[5] * cp[5] - cm[7] * cp[7] - cm[9] * cp[9];
+    vs[4] += -(cm[5] + cm[6]) * cp[9] - 0.5 * (cm[9] * (cp[5] + cp[6]) + cm[7] * cp[8] + cm[8] * cp[7]);
+    vs[5] += -2.0 * cm[6] * cp[6] - cm[8] * cp[8] - cm[9] * cp[9];
+  }
+  }  // i < n
+  if (VIR) {
+    block_reduce<6>(vs);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) vpart[(size_t)blockIdx.x * 6 + q] = vs[q];
+  }
 }
 
 // fphi_mpole_site (pmestuff.f:453-600): the 20 fractional potential
@@ -219,17 +257,23 @@ struct EwC {
 #define THP_FORCE_MINB 4
 #endif
 
-template <bool MIXED>
+// VIR: each block also writes to vpart[block][12] the sum of its sites' pair
+// virials (epolar1.f:2326-2342, half from each end of a pair) and the
+// frame-atom virial of their real-space torques (:2460-2486) in 0..5, and
+// the frame-atom virial of their reciprocal and self torques, which the
+// reference does not add, in 6..11.
+template <bool MIXED, bool VIR>
 __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_real(
     int n, int npad, Box box, double off2, EwC ew, const double4* __restrict__ pos,
     const typename std::conditional<MIXED, float, double>::type* __restrict__ mrec, const double* __restrict__ mu,
     const float* __restrict__ erec, const float* __restrict__ muf, const int* __restrict__ perm,
     const int* __restrict__ sp_off, const int* __restrict__ sp_ks, const double* __restrict__ sp_s,
     const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb, const int* __restrict__ frs,
-    const double* __restrict__ trq_recip, unsigned long long* __restrict__ dep) {
+    const double* __restrict__ trq_recip, unsigned long long* __restrict__ dep, double* __restrict__ vpart) {
   using T = typename std::conditional<MIXED, float, double>::type;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  double vout[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (i < n) {
   const double4 pi4 = pos[i];
   // mixed form: partners from the 64-B FP32 site record (wrapped position,
   // 1/pdamp, thole, multipoles) and the FP32 dipole record, imaged in FP32
@@ -253,6 +297,7 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_re
   const T f = (T)(0.5 * kElectric);
   double gx = 0.0, gy = 0.0, gz = 0.0;
   T uf[3] = {0, 0, 0}, duf[6] = {0, 0, 0, 0, 0, 0};
+  T vp[6] = {0, 0, 0, 0, 0, 0};  // pair virial, half of each pair's
   const int nn = min(nnb[i], maxnb);
 #pragma unroll 1
   for (int s = 0; s < nn; ++s) {
@@ -536,6 +581,15 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_re
     gx -= (double)frc[0];
     gy -= (double)frc[1];
     gz -= (double)frc[2];
+    if (VIR) {
+      const T h = T(0.5);
+      vp[0] += h * (xr * frc[0]);
+      vp[1] += h * (T(0.5) * (yr * frc[0] + xr * frc[1]));
+      vp[2] += h * (T(0.5) * (zr * frc[0] + xr * frc[2]));
+      vp[3] += h * (yr * frc[1]);
+      vp[4] += h * (T(0.5) * (zr * frc[1] + yr * frc[2]));
+      vp[5] += h * (zr * frc[2]);
+    }
   }
   fix_add(dep + 3 * i + 0, gx);
   fix_add(dep + 3 * i + 1, gy);
@@ -552,11 +606,70 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_re
                     (qixx - qizz) * duf[3]);
   tep[2] = (double)(diy * uf[0] - dix * uf[1] + qiyz * duf[3] - qixz * duf[4] + T(2) * qixy * (duf[0] - duf[2]) +
                     (qiyy - qixx) * duf[1]);
-  tep[0] += trq_recip[(size_t)i * 3 + 0] + sterm * (rdy * hz - rdz * hy);
-  tep[1] += trq_recip[(size_t)i * 3 + 1] + sterm * (rdz * hx - rdx * hz);
-  tep[2] += trq_recip[(size_t)i * 3 + 2] + sterm * (rdx * hy - rdy * hx);
   const int iz = frs[3 * i], ix = frs[3 * i + 1], axt = frs[3 * i + 2];
-  if (axt == 1 || axt == 2) torque_dist(pos, i, iz, ix, axt, tep, dep);
+  if (VIR) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) vout[q] = (double)vp[q];
+    if (axt == 1 || axt == 2) {
+      // the real-space torque (in the reference's virial) and the reciprocal +
+      // self torque (not in it), converted apart; the gradient takes both
+      const double tx[3] = {trq_recip[(size_t)i * 3 + 0] + sterm * (rdy * hz - rdz * hy),
+                            trq_recip[(size_t)i * 3 + 1] + sterm * (rdz * hx - rdx * hz),
+                            trq_recip[(size_t)i * 3 + 2] + sterm * (rdx * hy - rdy * hx)};
+      double du[3], dv[3], dux[3], dvx[3];
+      torque_frame(pos, i, iz, ix, axt, tep, du, dv);
+      torque_frame(pos, i, iz, ix, axt, tx, dux, dvx);
+      double vr[6] = {0, 0, 0, 0, 0, 0}, vx[6] = {0, 0, 0, 0, 0, 0};
+      frame_virial(pos, i, iz, ix, du, dv, vr);
+      frame_virial(pos, i, iz, ix, dux, dvx, vx);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        vout[q] += vr[q];
+        vout[6 + q] = vx[q];
+      }
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        fix_add(dep + 3 * iz + j, du[j] + dux[j]);
+        fix_add(dep + 3 * ix + j, dv[j] + dvx[j]);
+        fix_add(dep + 3 * i + j, -(du[j] + dux[j]) - (dv[j] + dvx[j]));
+      }
+    }
+  } else {
+    tep[0] += trq_recip[(size_t)i * 3 + 0] + sterm * (rdy * hz - rdz * hy);
+    tep[1] += trq_recip[(size_t)i * 3 + 1] + sterm * (rdz * hx - rdx * hz);
+    tep[2] += trq_recip[(size_t)i * 3 + 2] + sterm * (rdx * hy - rdy * hx);
+    if (axt == 1 || axt == 2) torque_dist(pos, i, iz, ix, axt, tep, dep);
+  }
+  }  // i < n
+  if (VIR) {
+    block_reduce<12>(vout);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q < 12; ++q) vpart[(size_t)blockIdx.x * 12 + q] = vout[q];
+  }
+}
+
+// The virial of one gradient call from the partial sums, in a fixed order:
+// nk rows of 6 (k-space sums), nr rows of 6 (reciprocal sites), ne rows of
+// 12 (real space: the reference's terms, then the reciprocal and self
+// torques' frame-atom terms).  out: 6 + 6 (xx xy xz yy yz zz twice).
+__global__ void __launch_bounds__(256) k_virial_sum(int nk, const double* __restrict__ kpart, int nr,
+                                                     const double* __restrict__ rpart, int ne,
+                                                     const double* __restrict__ epart, double* __restrict__ out) {
+  double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nk; b += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) v[q] += kpart[(size_t)b * 6 + q];
+  for (int b = threadIdx.x; b < nr; b += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) v[q] += rpart[(size_t)b * 6 + q];
+  for (int b = threadIdx.x; b < ne; b += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < 12; ++q) v[q] += epart[(size_t)b * 12 + q];
+  block_reduce<12>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < 12; ++q) out[q] = v[q];
 }
 
 }  // namespace
@@ -608,23 +721,51 @@ int launch_forces(Ctx& c, double* d_out) {
   if ((st = alloc_once(c, &c.d_depfix, 3 * n, "alloc gradient"))) return st;
   if ((st = alloc_once(c, &c.d_trq, 3 * n, "alloc torque"))) return st;
   if ((st = alloc_once(c, &c.d_frs, 3 * n, "alloc frames"))) return st;
+  const bool vir = c.want_virial;
+  const int nk = 2 * kspace_virial_blocks();
+  double *kpart = nullptr, *rpart = nullptr, *epart = nullptr;
+  if (vir) {
+    // partial sums: nk rows of 6, nb rows of 6, nb rows of 12, then the 12 totals
+    const size_t rows = (size_t)nk * 6 + (size_t)nb * 6 + (size_t)nb * 12 + 12;
+    if (c.virp_cap < rows) {
+      cudaFree(c.d_virp);
+      c.d_virp = nullptr;
+      c.virp_cap = 0;
+      if ((st = cuda_status(cudaMalloc((void**)&c.d_virp, sizeof(double) * rows), &c, "alloc virial"))) return st;
+      c.virp_cap = rows;
+    }
+    kpart = c.d_virp;
+    rpart = kpart + (size_t)nk * 6;
+    epart = rpart + (size_t)nb * 6;
+  }
   unsigned long long* dep = c.d_depfix;
   if ((st = cuda_status(cudaMemsetAsync(dep, 0, sizeof(unsigned long long) * 3 * n, c.stream), &c, "zero gradient")))
     return st;
   k_frames_sorted<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, c.d_iperm, c.d_frames, c.d_frs);
   PmeGeom g = pme_geom(c);
-  // permanent-multipole potential, 20 derivatives per site
-  if ((st = launch_mpole_grid(c))) return st;
+  // permanent-multipole potential, 20 derivatives per site (and the
+  // permanent-only k-space virial, subtracted)
+  if ((st = vir ? launch_mpole_grid_virial(c, kpart) : launch_mpole_grid(c))) return st;
   if ((st = launch_fphi_mpole20(c))) return st;
   // dipole grid of uind (Re) / uinp (Im), convolved
   if ((st = launch_pme_dipole(c, c.d_mu, nullptr, 0))) return st;
-  if (c.mixed)
-    k_force_recip<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftComplex*)c.d_grid, c.d_fphirec,
-                                                      c.d_mu, c.d_rpole, c.d_trq, dep);
+#define THP_RECIP_ARGS c.n, g, c.d_pos, c.d_grid, c.d_fphirec, c.d_mu, c.d_rpole, c.d_trq, dep, rpart
+  if (c.mixed && vir)
+    k_force_recip<float, true><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftComplex*)c.d_grid,
+                                                            c.d_fphirec, c.d_mu, c.d_rpole, c.d_trq, dep, rpart);
+  else if (c.mixed)
+    k_force_recip<float, false><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftComplex*)c.d_grid,
+                                                             c.d_fphirec, c.d_mu, c.d_rpole, c.d_trq, dep, rpart);
+  else if (vir)
+    k_force_recip<double, true><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftDoubleComplex*)c.d_grid,
+                                                             c.d_fphirec, c.d_mu, c.d_rpole, c.d_trq, dep, rpart);
   else
-    k_force_recip<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftDoubleComplex*)c.d_grid,
-                                                       c.d_fphirec, c.d_mu, c.d_rpole, c.d_trq, dep);
+    k_force_recip<double, false><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, (const cufftDoubleComplex*)c.d_grid,
+                                                              c.d_fphirec, c.d_mu, c.d_rpole, c.d_trq, dep, rpart);
+#undef THP_RECIP_ARGS
   if ((st = cuda_status(cudaGetLastError(), &c, "force recip"))) return st;
+  // (rpole + uinp) x (rpole + uind) k-space virial: the grid is free again
+  if (vir && (st = launch_pair_grid_virial(c, kpart + (size_t)kspace_virial_blocks() * 6))) return st;
   EwC ew;
   const double a = c.cfg.aewald;
   double aesq2 = 2.0 * a * a, afac = 1.0 / (kSqrtPi * a);
@@ -645,18 +786,30 @@ int launch_forces(Ctx& c, double* d_out) {
   }
 #define THP_FORCE_ARGS                                                                                      \
   c.n, c.npad, c.box, off2, ew, c.d_pos, MREC, c.d_mu, c.d_erec, c.d_muf, c.d_perm, c.d_sp_off, c.d_sp_ks, \
-      c.d_sp_s, c.d_nnb, c.d_nb, c.maxnb, c.d_frs, c.d_trq, dep
+      c.d_sp_s, c.d_nnb, c.d_nb, c.maxnb, c.d_frs, c.d_trq, dep, epart
   if (c.mixed) {
 #define MREC c.d_mrecf
-    k_force_real<true><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
+    if (vir)
+      k_force_real<true, true><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
+    else
+      k_force_real<true, false><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
 #undef MREC
   } else {
 #define MREC c.d_mrec
-    k_force_real<false><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
+    if (vir)
+      k_force_real<false, true><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
+    else
+      k_force_real<false, false><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
 #undef MREC
   }
 #undef THP_FORCE_ARGS
   if ((st = cuda_status(cudaGetLastError(), &c, "force real"))) return st;
+  if (vir) {
+    double* tot = epart + (size_t)nb * 12;
+    k_virial_sum<<<1, 256, 0, c.stream>>>(nk, kpart, nb, rpart, nb, epart, tot);
+    if ((st = cuda_status(cudaGetLastError(), &c, "virial sum"))) return st;
+    cudaMemcpyAsync(c.h_vir, tot, sizeof(double) * 12, cudaMemcpyDeviceToHost, c.stream);
+  }
   k_dep_out<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, dep, d_out);
   return cuda_status(cudaGetLastError(), &c, "force out");
 }

@@ -14,9 +14,10 @@ __device__ __forceinline__ void fix_add(unsigned long long* a, double v) {
 }
 
 // torque.f:6-390, Z-then-X (axt 1) and Bisector (axt 2); site ib, z atom ia,
-// x atom ic; adds d(energy)/d(coordinates) of the torque trq.
-__device__ void torque_dist(const double4* __restrict__ pos, int ib, int ia, int ic, int axt, const double trq[3],
-                            unsigned long long* __restrict__ dep) {
+// x atom ic: the derivatives du (z atom) and dv (x atom) of the energy of
+// the torque trq; the site itself takes -(du + dv).
+__device__ __forceinline__ void torque_frame(const double4* __restrict__ pos, int ib, int ia, int ic, int axt,
+                                             const double trq[3], double du[3], double dv[3]) {
   const double4 pb = pos[ib], pa = pos[ia], pc = pos[ic];
   double u[3] = {pa.x - pb.x, pa.y - pb.y, pa.z - pb.z};
   double v[3] = {pc.x - pb.x, pc.y - pb.y, pc.z - pb.z};
@@ -50,13 +51,38 @@ __device__ void torque_dist(const double4* __restrict__ pos, int ib, int ia, int
   const double hw = axt == 2 ? 0.5 : 1.0;
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
-    double du = uv[j] * dphidv / (usiz * uvsin) + hw * uw[j] * dphidw / usiz;
-    double dv = -uv[j] * dphidu / (vsiz * uvsin);
-    if (axt == 2) dv += 0.5 * vw[j] * dphidw / vsiz;
-    fix_add(dep + 3 * ia + j, du);
-    fix_add(dep + 3 * ic + j, dv);
-    fix_add(dep + 3 * ib + j, -du - dv);
+    du[j] = uv[j] * dphidv / (usiz * uvsin) + hw * uw[j] * dphidw / usiz;
+    dv[j] = -uv[j] * dphidu / (vsiz * uvsin);
+    if (axt == 2) dv[j] += 0.5 * vw[j] * dphidw / vsiz;
   }
+}
+
+// adds d(energy)/d(coordinates) of the torque trq on site ib
+__device__ void torque_dist(const double4* __restrict__ pos, int ib, int ia, int ic, int axt, const double trq[3],
+                            unsigned long long* __restrict__ dep) {
+  double du[3], dv[3];
+  torque_frame(pos, ib, ia, ic, axt, trq, du, dv);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    fix_add(dep + 3 * ia + j, du[j]);
+    fix_add(dep + 3 * ic + j, dv[j]);
+    fix_add(dep + 3 * ib + j, -du[j] - dv[j]);
+  }
+}
+
+// the virial of a torque's frame-atom derivatives (epolar1.f:2460-2486):
+// du on the z atom ia, dv on the x atom ic of site ib; adds xx xy xz yy yz zz
+__device__ __forceinline__ void frame_virial(const double4* __restrict__ pos, int ib, int ia, int ic,
+                                             const double du[3], const double dv[3], double (&v)[6]) {
+  const double4 pb = pos[ib], pa = pos[ia], pc = pos[ic];
+  const double xiz = pa.x - pb.x, yiz = pa.y - pb.y, ziz = pa.z - pb.z;
+  const double xix = pc.x - pb.x, yix = pc.y - pb.y, zix = pc.z - pb.z;
+  v[0] += xix * dv[0] + xiz * du[0];
+  v[1] += 0.5 * (yix * dv[0] + yiz * du[0] + xix * dv[1] + xiz * du[1]);
+  v[2] += 0.5 * (zix * dv[0] + ziz * du[0] + xix * dv[2] + xiz * du[2]);
+  v[3] += yix * dv[1] + yiz * du[1];
+  v[4] += 0.5 * (zix * dv[1] + ziz * du[1] + yix * dv[2] + yiz * du[2]);
+  v[5] += zix * dv[2] + ziz * du[2];
 }
 
 // sorted frame atoms: frs[s] = (iperm[zaxis], iperm[xaxis], axt) of perm[s]

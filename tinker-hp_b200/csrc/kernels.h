@@ -27,6 +27,9 @@ void pme_free(Ctx& c);
 int launch_efld0_recip(Ctx& c);         // d_cphi and E0 completion
 int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0);
 int launch_mpole_grid(Ctx& c);          // permanent-multipole grid, convolved (grid holds the potential)
+int launch_mpole_grid_virial(Ctx& c, double* d_part);  // the same, with the permanent-only k-space virial
+int launch_pair_grid_virial(Ctx& c, double* d_part);   // (rpole+uinp) x (rpole+uind) k-space virial
+int kspace_virial_blocks();
 int launch_gather_mpole(Ctx& c, double* cphi10, bool with_e0);  // cphi from the convolved grid, E0 completion
 int launch_pme_dipole_f32(Ctx& c, const float* d_vec);  // mode-2 spread of an FP32 vector + convolution
 bool overlap_rows(const Ctx& c);  // the system runs real-space passes on the side stream

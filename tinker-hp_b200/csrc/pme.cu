@@ -109,6 +109,110 @@ __global__ void k_spread_mpole(int n, PmeGeom g, const double4* __restrict__ pos
   }
 }
 
+// grid_mpole_site for the two multipole sets of eprecip1's virial
+// (epolar1.f:932-1040): the permanent moments with uinp added to the dipole
+// into the real part, with uind added into the imaginary part, of one
+// complex grid.  mu sorted [n][6] (uind xyz, uinp xyz).
+template <typename T>
+__global__ void k_spread_mpole2(int n, PmeGeom g, const double4* __restrict__ pos, const double* __restrict__ rp,
+                                const double* __restrict__ mu, typename Cplx<T>::type* __restrict__ grid) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 p = pos[i];
+  T tx[kBs][3], ty[kBs][3], tz[kBs][3];
+  int gx = bspline_axis<3, T>(p.x, g.recip[0], g.n1, tx);
+  int gy = bspline_axis<3, T>(p.y, g.recip[1], g.n2, ty);
+  int gz = bspline_axis<3, T>(p.z, g.recip[2], g.n3, tz);
+  const double* r = rp + (size_t)i * 10;
+  const double* m = mu + (size_t)i * 6;
+  T f[10], fb[3];
+  f[0] = (T)r[0];
+  f[1] = (T)(g.a[0] * (r[1] + m[3]));
+  f[2] = (T)(g.a[1] * (r[2] + m[4]));
+  f[3] = (T)(g.a[2] * (r[3] + m[5]));
+  fb[0] = (T)(g.a[0] * (r[1] + m[0]));
+  fb[1] = (T)(g.a[1] * (r[2] + m[1]));
+  fb[2] = (T)(g.a[2] * (r[3] + m[2]));
+  f[4] = (T)(g.a[0] * g.a[0] * r[4]);
+  f[5] = (T)(g.a[1] * g.a[1] * r[7]);
+  f[6] = (T)(g.a[2] * g.a[2] * r[9]);
+  f[7] = (T)(g.a[0] * g.a[1] * (2.0 * r[5]));
+  f[8] = (T)(g.a[0] * g.a[2] * (2.0 * r[6]));
+  f[9] = (T)(g.a[1] * g.a[2] * (2.0 * r[8]));
+#pragma unroll
+  for (int c = 0; c < kBs; ++c) {
+    size_t kk = (size_t)wrapk(gz + c, g.n3);
+    T v0 = tz[c][0], v1 = tz[c][1], v2 = tz[c][2];
+#pragma unroll
+    for (int b = 0; b < kBs; ++b) {
+      size_t jj = (size_t)wrapk(gy + b, g.n2);
+      T u0 = ty[b][0], u1 = ty[b][1], u2 = ty[b][2];
+      // the terms without a dipole are shared by the two sets
+      T q0 = f[0] * u0 * v0 + f[5] * u2 * v0 + f[6] * u0 * v2 + f[9] * u1 * v1;
+      T term0a = q0 + f[2] * u1 * v0 + f[3] * u0 * v1, term0b = q0 + fb[1] * u1 * v0 + fb[2] * u0 * v1;
+      T q1 = f[7] * u1 * v0 + f[8] * u0 * v1;
+      T term1a = q1 + f[1] * u0 * v0, term1b = q1 + fb[0] * u0 * v0;
+      T term2 = f[4] * u0 * v0;
+      size_t row = (kk * g.n2 + jj) * g.n1;
+#pragma unroll
+      for (int a = 0; a < kBs; ++a) {
+        int ii = wrapk(gx + a, g.n1);
+        grid_add(grid, row + ii, term0a * tx[a][0] + term1a * tx[a][1] + term2 * tx[a][2],
+                 term0b * tx[a][0] + term1b * tx[a][1] + term2 * tx[a][2]);
+      }
+    }
+  }
+}
+
+// Sum over the reciprocal lattice (all k but 0 with qfac > 0) of the PME
+// virial terms h h vterm - eterm (eterm = 0.5 f qfac struc2, vterm =
+// (2/h^2)(1 + pterm h^2) eterm; emrecip1 / eprecip1, epolar1.f:1041-1091)
+// of the forward-transformed grid, times sign.  mode 0: struc2 = |G(k)|^2
+// (one real grid); mode 1: struc2 = Re(A(k) conj B(k)) of the two real grids
+// A (real part) and B (imaginary part) packed in G, separated by
+// A = (G(k) + conj G(-k)) / 2, B = (G(k) - conj G(-k)) / 2i.  Each block
+// writes its 6 sums (xx, xy, xz, yy, yz, zz) to part[block].
+template <typename C, typename Q>
+__global__ void __launch_bounds__(256) k_kspace_virial(int n1, int n2, int n3, const C* __restrict__ grid,
+                                                       const Q* __restrict__ qfac, double r1, double r2, double r3,
+                                                       double pterm, double f, int mode, double sign,
+                                                       double* __restrict__ part) {
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  const long ng = (long)n1 * n2 * n3;
+  const int nf1 = (n1 + 1) / 2, nf2 = (n2 + 1) / 2, nf3 = (n3 + 1) / 2;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < ng; idx += (long)gridDim.x * blockDim.x) {
+    const double qf = (double)qfac[idx];
+    if (qf == 0.0) continue;
+    const int k1 = (int)(idx % n1), k2 = (int)((idx / n1) % n2), k3 = (int)(idx / ((long)n1 * n2));
+    const int m1 = k1 + 1 > nf1 ? k1 - n1 : k1, m2 = k2 + 1 > nf2 ? k2 - n2 : k2, m3 = k3 + 1 > nf3 ? k3 - n3 : k3;
+    const C gk = grid[idx];
+    double struc2;
+    if (mode == 0) {
+      struc2 = (double)gk.x * gk.x + (double)gk.y * gk.y;
+    } else {
+      const long mi = ((long)((n3 - k3) % n3) * n2 + (n2 - k2) % n2) * n1 + (n1 - k1) % n1;
+      const C gm = grid[mi];  // conj G(-k) = (gm.x, -gm.y)
+      const double ax = 0.5 * ((double)gk.x + gm.x), ay = 0.5 * ((double)gk.y - gm.y);
+      const double bx = 0.5 * ((double)gk.y + gm.y), by = -0.5 * ((double)gk.x - gm.x);
+      struc2 = ax * bx + ay * by;
+    }
+    const double h1 = r1 * m1, h2 = r2 * m2, h3 = r3 * m3;
+    const double hsq = h1 * h1 + h2 * h2 + h3 * h3;
+    const double eterm = 0.5 * f * qf * struc2;
+    const double vterm = (2.0 / hsq) * (1.0 + pterm * hsq) * eterm;
+    v[0] += h1 * h1 * vterm - eterm;
+    v[1] += h1 * h2 * vterm;
+    v[2] += h1 * h3 * vterm;
+    v[3] += h2 * h2 * vterm - eterm;
+    v[4] += h2 * h3 * vterm;
+    v[5] += h3 * h3 * vterm - eterm;
+  }
+  block_reduce<6>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) part[(size_t)blockIdx.x * 6 + q] = sign * v[q];
+}
+
 // grid_uind_site (pmestuff.f:280-405); d dipoles in Re, p dipoles in Im.
 // One thread per site (the 125 atomics of neighbouring threads land in
 // different L2 slices; a warp-per-site variant that made them contiguous
@@ -606,6 +710,67 @@ int launch_mpole_grid(Ctx& c) {
     k_spread_mpole<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, c.d_rpole, (cufftDoubleComplex*)c.d_grid);
   if ((st = cuda_status(cudaGetLastError(), &c, "spread mpole"))) return st;
   return convolve(c, 0);
+}
+
+// blocks of the k-space virial sums (each writes 6 partial sums)
+int kspace_virial_blocks() { return 148 * 2; }
+
+static int kspace_virial(Ctx& c, int mode, double sign, double* d_part) {
+  const double pterm = (kPi / c.cfg.aewald) * (kPi / c.cfg.aewald);
+  const PmeGeom g = geom_of(c);
+  if (c.mixed)
+    k_kspace_virial<cufftComplex, float><<<kspace_virial_blocks(), 256, 0, c.stream>>>(
+        g.n1, g.n2, g.n3, (const cufftComplex*)c.d_grid, (const float*)c.d_qfac, g.recip[0], g.recip[1], g.recip[2],
+        pterm, kElectric, mode, sign, d_part);
+  else
+    k_kspace_virial<cufftDoubleComplex, double><<<kspace_virial_blocks(), 256, 0, c.stream>>>(
+        g.n1, g.n2, g.n3, (const cufftDoubleComplex*)c.d_grid, (const double*)c.d_qfac, g.recip[0], g.recip[1],
+        g.recip[2], pterm, kElectric, mode, sign, d_part);
+  return cuda_status(cudaGetLastError(), &c, "k-space virial");
+}
+
+// launch_mpole_grid with, between the forward transform and qfac, the
+// permanent-only scalar-sum virial (emrecip1), subtracted as eprecip1 does
+// (epolar1.f:534-541): kspace_virial_blocks() rows of 6 into d_part.
+int launch_mpole_grid_virial(Ctx& c, double* d_part) {
+  PmeGeom g = geom_of(c);
+  int nb = (c.n + kBlock - 1) / kBlock;
+  int st = zero_grid(c);
+  if (st) return st;
+  if (c.mixed)
+    k_spread_mpole<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, c.d_rpole, (cufftComplex*)c.d_grid);
+  else
+    k_spread_mpole<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, c.d_rpole, (cufftDoubleComplex*)c.d_grid);
+  if ((st = cuda_status(cudaGetLastError(), &c, "spread mpole"))) return st;
+  if ((st = fft(c, CUFFT_FORWARD))) return st;
+  if ((st = kspace_virial(c, 0, -1.0, d_part))) return st;
+  int blocks = 148 * 8;
+  if (c.mixed)
+    k_qfac<cufftComplex, float><<<blocks, 256, 0, c.stream>>>(c.ngrid, (const float*)c.d_qfac,
+                                                             (cufftComplex*)c.d_grid, c.d_cg, 0);
+  else
+    k_qfac<cufftDoubleComplex, double><<<blocks, 256, 0, c.stream>>>(
+        c.ngrid, (const double*)c.d_qfac, (cufftDoubleComplex*)c.d_grid, c.d_cg, 0);
+  if ((st = cuda_status(cudaGetLastError(), &c, "qfac"))) return st;
+  return fft(c, CUFFT_INVERSE);
+}
+
+// The (rpole + uinp) x (rpole + uind) scalar-sum virial of eprecip1
+// (epolar1.f:932-1091) into kspace_virial_blocks() rows of d_part; uses
+// (and leaves transformed) the context's grid.
+int launch_pair_grid_virial(Ctx& c, double* d_part) {
+  PmeGeom g = geom_of(c);
+  int nb = (c.n + kBlock - 1) / kBlock;
+  int st = zero_grid(c);
+  if (st) return st;
+  if (c.mixed)
+    k_spread_mpole2<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, c.d_rpole, c.d_mu, (cufftComplex*)c.d_grid);
+  else
+    k_spread_mpole2<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, c.d_rpole, c.d_mu,
+                                                         (cufftDoubleComplex*)c.d_grid);
+  if ((st = cuda_status(cudaGetLastError(), &c, "spread mpole pair"))) return st;
+  if ((st = fft(c, CUFFT_FORWARD))) return st;
+  return kspace_virial(c, 1, 1.0, d_part);
 }
 
 int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0) {
