@@ -263,6 +263,33 @@ def batched_throughput(lib, systems, copies, steps, warmup=2, precision=None):
             "ms_per_batch": 1000.0 * dt / steps, "median_iters": float(np.median(iters))}
 
 
+def batch_plan_throughput(lib, systems, steps, precision=None):
+    """Batched form through a batch plan (thp_batch_*): the CG iterations of
+    all systems as batched persistent kernels in one graph.  The first solves
+    tune the launch shape (untimed); host-timed over whole batches."""
+    prec = lib.MIXED if precision is None else precision
+    ctxs = [lib.Context(ws, precision=prec, poleps=CG_TOL) for ws in systems]
+    plan = lib.Batch(ctxs)
+    tuning_solves = 0
+    while plan.tuning() is None and tuning_solves < 16:
+        plan.solve()
+        tuning_solves += 1
+    plan.solve()
+    t0 = time.perf_counter()
+    iters = []
+    for _ in range(steps):
+        infos = plan.solve()
+        iters += [f["niter"] for f in infos]
+    dt = time.perf_counter() - t0
+    tuned = plan.tuning()
+    plan.close()
+    for c in ctxs:
+        c.close()
+    return {"solves": len(ctxs) * steps, "seconds": dt, "solves_per_s": len(ctxs) * steps / dt,
+            "ms_per_batch": 1000.0 * dt / steps, "median_iters": float(np.median(iters)),
+            "tuning_solves": tuning_solves, "tuned": tuned}
+
+
 def serving_run(lib, thp, count, workers=8):
     """Serving form: seeded Poisson stream (200 req/s, 1k-60k atoms, 30 %
     repeats perturbed by 0.01 A RMS) through the native request loop with a
@@ -708,6 +735,8 @@ def main():
         batch64 = thp.water.make_batch(64, seed=4003)
         extras["batch_64_boxes"] = batched_throughput(lib, batch64, 1, 3)
         extras["batch_64_boxes"]["atoms"] = f"{sum(w.n for w in batch64)} over 64 boxes (300-6000 each)"
+        extras["batch_64_boxes_plan"] = batch_plan_throughput(lib, batch64, 5)
+        extras["batch_64_boxes_plan_fp64"] = batch_plan_throughput(lib, batch64, 5, precision=lib.FP64)
         extras["serving"] = serving_run(lib, thp, 120)
         ws2 = thp.water.make_water_box(nw, cfg=cfg, seed_lattice=7001, seed_orient=7002)
         extras["served_288k_repeats"] = {"mixed": served_repeats(lib, [ws], lib.MIXED),

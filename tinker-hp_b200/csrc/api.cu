@@ -1212,6 +1212,8 @@ static int solve_front_eager(thp_ctx* h, int guess) {
 // re-sort, captured on first use: a batch of many small systems would
 // otherwise spend its time in the host's launch calls.  The predictor's
 // guess (host-side coefficients) and profiling take the eager path.
+static void front_replayed(thp_ctx* h);
+
 static int solve_front_async(thp_ctx* h, int guess) {
   Ctx& c = h->c;
   const int keep_mu = (c.have_perm && c.have_dipoles) ? 1 : 0;
@@ -1238,20 +1240,29 @@ static int solve_front_async(thp_ctx* h, int guess) {
     }
     cudaGraphDestroy(g);
   }
-  // the host-side state the front leaves behind
+  front_replayed(h);
+  return cuda_status(cudaGraphLaunch(ex, c.stream), &c, "front graph launch");
+}
+
+// The host-side state a replayed front leaves behind (what solve_front_eager
+// records as it enqueues): rotated multipoles, a fresh sort and list, E0, and
+// this solve's E0 kept for the next warm start.
+static void front_replayed(thp_ctx* h) {
+  Ctx& c = h->c;
   if (c.have_frames) c.have_rpole = h->rpole_current = true;
   c.have_perm = c.have_list = true;
+  ++c.sort_epoch;  // the replay re-sorted the atoms: lists in the old numbering are stale
+  c.have_ef_prev = true;
   h->pos_dirty = h->rpole_dirty = false;
   h->field_valid = true;
-  return cuda_status(cudaGraphLaunch(ex, c.stream), &c, "front graph launch");
 }
 
 
 
-int thp_solve_batch(thp_ctx** hs, int count, int guess, thp_solve_info* infos) {
-  if (!hs || count <= 0) return THP_E_INVALID;
-  std::vector<int> st(count, THP_OK), rounds(count, 0);
-  std::vector<char> active(count, 0);
+// The fronts of a batch: every valid system's E0 and CG start enqueued on
+// its own stream (replayed from its front graph); active[i] marks those that
+// started.
+static void batch_fronts(thp_ctx** hs, int count, int guess, std::vector<int>& st, std::vector<char>& active) {
   for (int i = 0; i < count; ++i) {
     thp_ctx* h = hs[i];
     if (!h) {
@@ -1282,47 +1293,11 @@ int thp_solve_batch(thp_ctx** hs, int count, int guess, thp_solve_info* infos) {
     h->guess_uploaded = false;
     active[i] = st[i] == THP_OK;
   }
-  // the whole CG loop of each system as one graph launch where available;
-  // the others take chunk rounds with a host check of the stop flags
-  std::vector<char> looped(count, 0);
-  for (int i = 0; i < count; ++i) {
-    if (!active[i]) continue;
-    Ctx& c = hs[i]->c;
-    set_current_device(c);
-    const int r = pcg_loop_async(c);
-    if (r >= 0) {
-      active[i] = 0;
-      looped[i] = r == 0;
-      if (r > 0) st[i] = r;
-    }
-  }
-  for (int i = 0; i < count; ++i) {
-    if (!looped[i]) continue;
-    Ctx& c = hs[i]->c;
-    set_current_device(c);
-    st[i] = cuda_status(cudaStreamSynchronize(c.stream), &c, "batch sync");
-  }
-  for (bool any = true; any;) {
-    any = false;
-    for (int i = 0; i < count; ++i) {
-      if (!active[i]) continue;
-      Ctx& c = hs[i]->c;
-      set_current_device(c);
-      if ((st[i] = pcg_chunk_async(c))) active[i] = 0;
-    }
-    for (int i = 0; i < count; ++i) {
-      if (!active[i]) continue;
-      Ctx& c = hs[i]->c;
-      set_current_device(c);
-      if ((st[i] = cuda_status(cudaStreamSynchronize(c.stream), &c, "batch sync"))) {
-        active[i] = 0;
-        continue;
-      }
-      rounds[i] += kCgChunk;
-      if (c.h_cg->stop || rounds[i] > c.cfg.politer + kCgChunk) active[i] = 0;
-      any |= active[i] != 0;
-    }
-  }
+}
+
+// The end of a batch once every CG has stopped and its scalars are in h_cg:
+// status, predictor, Epol, flags and the per-system results.
+static int batch_finish(thp_ctx** hs, int count, std::vector<int>& st, thp_solve_info* infos) {
   for (int i = 0; i < count; ++i) {
     if (st[i]) continue;
     Ctx& c = hs[i]->c;
@@ -1368,6 +1343,246 @@ int thp_solve_batch(thp_ctx** hs, int count, int guess, thp_solve_info* infos) {
     if (st[i] && (worst == THP_OK || worst == THP_E_NOT_CONVERGED)) worst = st[i];
   }
   return worst;
+}
+
+int thp_solve_batch(thp_ctx** hs, int count, int guess, thp_solve_info* infos) {
+  if (!hs || count <= 0) return THP_E_INVALID;
+  std::vector<int> st(count, THP_OK), rounds(count, 0);
+  std::vector<char> active(count, 0);
+  batch_fronts(hs, count, guess, st, active);
+  // the whole CG loop of each system as one graph launch where available;
+  // the others take chunk rounds with a host check of the stop flags
+  std::vector<char> looped(count, 0);
+  for (int i = 0; i < count; ++i) {
+    if (!active[i]) continue;
+    Ctx& c = hs[i]->c;
+    set_current_device(c);
+    const int r = pcg_loop_async(c);
+    if (r >= 0) {
+      active[i] = 0;
+      looped[i] = r == 0;
+      if (r > 0) st[i] = r;
+    }
+  }
+  for (int i = 0; i < count; ++i) {
+    if (!looped[i]) continue;
+    Ctx& c = hs[i]->c;
+    set_current_device(c);
+    st[i] = cuda_status(cudaStreamSynchronize(c.stream), &c, "batch sync");
+  }
+  for (bool any = true; any;) {
+    any = false;
+    for (int i = 0; i < count; ++i) {
+      if (!active[i]) continue;
+      Ctx& c = hs[i]->c;
+      set_current_device(c);
+      if ((st[i] = pcg_chunk_async(c))) active[i] = 0;
+    }
+    for (int i = 0; i < count; ++i) {
+      if (!active[i]) continue;
+      Ctx& c = hs[i]->c;
+      set_current_device(c);
+      if ((st[i] = cuda_status(cudaStreamSynchronize(c.stream), &c, "batch sync"))) {
+        active[i] = 0;
+        continue;
+      }
+      rounds[i] += kCgChunk;
+      if (c.h_cg->stop || rounds[i] > c.cfg.politer + kCgChunk) active[i] = 0;
+      any |= active[i] != 0;
+    }
+  }
+  return batch_finish(hs, count, st, infos);
+}
+
+// ---- batch plans: the CG iterations of many systems as batched kernels ----
+
+struct thp_batch {
+  std::vector<thp_ctx*> hs;
+  std::vector<Ctx*> cs;
+  BatchPlan* plan = nullptr;
+  bool no_graph = false;  // the whole-solve graph could not be built: per-system fronts
+};
+
+int thp_batch_create(thp_ctx** hs, int count, thp_batch** out) {
+  if (!hs || !out || count <= 0) return THP_E_INVALID;
+  *out = nullptr;
+  thp_batch* b = new thp_batch();
+  for (int i = 0; i < count; ++i) {
+    if (!hs[i]) {
+      delete b;
+      return THP_E_INVALID;
+    }
+    b->hs.push_back(hs[i]);
+    b->cs.push_back(&hs[i]->c);
+  }
+  if (set_current_device(*b->cs[0])) {
+    delete b;
+    return THP_E_CUDA;
+  }
+  std::string msg;
+  const int st = batch_plan_create(b->cs.data(), count, &b->plan, &msg);
+  if (st) {
+    b->cs[0]->last_msg = msg;
+    delete b;
+    return st;
+  }
+  *out = b;
+  return THP_OK;
+}
+
+// The whole batched solve as one graph launch (every system's front, the
+// batched loop, Epol and the results in mapped host memory), when every
+// system takes the same graphable start: guess DIRECT / PREVIOUS / HOST
+// after resolution, the same dipole carry, no profiling.  Returns -1 when the
+// solve does not qualify (the caller runs the per-system fronts).
+static int batch_solve_graph(thp_batch* b, int guess, thp_solve_info* infos) {
+  BatchPlan& p = *b->plan;
+  const int count = (int)b->hs.size();
+  if (b->no_graph || batch_plan_profiling(p) || guess == THP_GUESS_PREDICT || guess < THP_GUESS_DIRECT ||
+      guess > THP_GUESS_HOST)
+    return -1;
+  int g0 = -1, carry0 = -1;
+  for (int i = 0; i < count; ++i) {
+    thp_ctx* h = b->hs[i];
+    Ctx& c = h->c;
+    if (!THP_FRONT_GRAPH || c.profiling || !c.stream || c.front_failed || c.pred_mode) return -1;
+    if (!c.have_params || !c.have_pos || (!c.have_rpole && !c.have_frames)) return THP_E_STATE;
+    int g = guess;
+    if (g == THP_GUESS_PREVIOUS && !c.have_dipoles) g = THP_GUESS_DIRECT;
+    if (g == THP_GUESS_HOST && !h->guess_uploaded) return THP_E_STATE;
+    const int carry = (c.have_perm && c.have_dipoles) ? 1 : 0;
+    if ((g0 >= 0 && g != g0) || (carry0 >= 0 && carry != carry0)) return -1;
+    g0 = g;
+    carry0 = carry;
+  }
+  const int cand = batch_plan_candidate(p);
+  cudaGraphExec_t ex = batch_plan_solve_exec(p, g0, carry0, cand);
+  if (!ex) {
+    // capture every front (the host state moves as it is enqueued) and build
+    std::vector<cudaGraph_t> fronts;
+    int st = THP_OK;
+    for (int i = 0; i < count && !st; ++i) {
+      Ctx& c = b->hs[i]->c;
+      set_current_device(c);
+      if (cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        st = -1;
+        break;
+      }
+      const int se = solve_front_eager(b->hs[i], g0);
+      cudaGraph_t gr = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(c.stream, &gr);
+      if (se || e != cudaSuccess) {
+        cudaGetLastError();
+        if (gr) cudaGraphDestroy(gr);
+        st = se ? se : -1;
+        break;
+      }
+      fronts.push_back(gr);
+    }
+    if (!st) st = batch_plan_make_solve_exec(p, fronts, g0, carry0, cand) ? -1 : THP_OK;
+    for (cudaGraph_t gr : fronts) cudaGraphDestroy(gr);
+    if (st) {
+      // nothing of the captured fronts ran: run them eagerly on the usual path
+      // (cold: a capture may have moved a context's host state)
+      for (int i = 0; i < count; ++i) forget_solution(b->hs[i]);
+      b->no_graph = true;
+      return -1;
+    }
+    ex = batch_plan_solve_exec(p, g0, carry0, cand);
+  } else {
+    for (int i = 0; i < count; ++i) front_replayed(b->hs[i]);
+  }
+  for (int i = 0; i < count; ++i) b->hs[i]->guess_uploaded = false;
+  std::vector<const CgScalars*> cgs(count);
+  std::vector<const int*> fls(count);
+  float ms = 0.f;
+  const int sr = batch_plan_run_solve(p, ex, cgs.data(), fls.data(), &ms);
+  int worst = THP_OK, maxit = 0;
+  for (int i = 0; i < count; ++i) {
+    thp_ctx* h = b->hs[i];
+    Ctx& c = h->c;
+    int st = sr;
+    if (!st) {
+      *c.h_cg = *cgs[i];
+      *c.h_flags = *fls[i];
+      st = flags_status(c);
+      if (!st) st = pcg_status(c);
+      maxit = std::max(maxit, c.h_cg->niter);
+    }
+    if (!st || st == THP_E_NOT_CONVERGED) {
+      h->solved_once = true;
+      if (infos) {
+        infos[i].niter = c.h_cg->niter;
+        infos[i].converged = c.h_cg->converged;
+        infos[i].resnrm = c.h_cg->resnrm;
+        infos[i].epol = c.h_cg->epol;
+        infos[i].ene[0] = c.h_cg->ene[0] * kElectric;
+        infos[i].ene[1] = c.h_cg->ene[1] * kElectric;
+        infos[i].ms_total = ms;
+      }
+    } else {
+      if (infos) infos[i] = thp_solve_info{};
+      forget_solution(h);
+    }
+    if (st && (worst == THP_OK || worst == THP_E_NOT_CONVERGED)) worst = st;
+  }
+  if (!sr) batch_plan_finish(p, maxit);
+  return worst;
+}
+
+int thp_batch_solve(thp_batch* b, int guess, thp_solve_info* infos) {
+  if (!b) return THP_E_INVALID;
+  const int count = (int)b->hs.size();
+  thp_ctx** hs = b->hs.data();
+  if (int s = batch_plan_check(*b->plan, b->cs.data())) return s;
+  if (set_current_device(*b->cs[0])) return THP_E_CUDA;
+  const int gs = batch_solve_graph(b, guess, infos);
+  if (gs >= 0) return gs;
+  std::vector<int> st(count, THP_OK);
+  std::vector<char> active(count, 0);
+  batch_fronts(hs, count, guess, st, active);
+  for (int i = 0; i < count; ++i) {
+    Ctx& c = *b->cs[i];
+    if (active[i]) continue;
+    // a system whose front did not start takes no part in the loop
+    set_current_device(c);
+    cudaMemsetAsync(c.d_cg, 0, sizeof(CgScalars), c.stream);
+    cudaMemsetAsync(&c.d_cg->stop, 1, sizeof(int), c.stream);
+  }
+  const int sl = batch_plan_loop(*b->plan, b->cs.data());
+  int maxit = 0;
+  for (int i = 0; i < count; ++i) {
+    Ctx& c = *b->cs[i];
+    set_current_device(c);
+    if (sl && !st[i]) st[i] = sl;
+    cudaMemcpyAsync(c.h_cg, c.d_cg, sizeof(CgScalars), cudaMemcpyDeviceToHost, c.stream);
+    const int ss = cuda_status(cudaStreamSynchronize(c.stream), &c, "batch sync");
+    if (ss && !st[i]) st[i] = ss;
+    if (!st[i]) maxit = std::max(maxit, c.h_cg->niter);
+  }
+  if (!sl) batch_plan_finish(*b->plan, maxit);
+  return batch_finish(hs, count, st, infos);
+}
+
+int thp_batch_tuning(thp_batch* b, int* atom_blocks, int* dft_blocks, int* lines, double* ms_per_iteration) {
+  if (!b || !atom_blocks || !dft_blocks || !lines) return THP_E_INVALID;
+  float ms = 0.f;
+  const int st = batch_plan_tuning(*b->plan, atom_blocks, dft_blocks, lines, &ms);
+  if (ms_per_iteration) *ms_per_iteration = ms;
+  return st;
+}
+
+int thp_batch_profile(thp_batch* b, int enable, double* ms, int* iterations) {
+  if (!b) return THP_E_INVALID;
+  return batch_plan_profile(*b->plan, enable, ms, iterations);
+}
+
+int thp_batch_destroy(thp_batch* b) {
+  if (!b) return THP_E_INVALID;
+  batch_plan_destroy(b->plan);
+  delete b;
+  return THP_OK;
 }
 
 int thp_get_dipoles(thp_ctx* h, double* uind, double* uinp) {

@@ -86,4 +86,31 @@ int launch_split_dipoles(Ctx& c, const double* d_sorted, double* d_out);  // uin
 
 int cuda_status(cudaError_t e, Ctx* c, const char* what);
 
+// realspace.cu
+struct PairRows;
+PairRows pair_rows(const Ctx& c);   // the context's pair stream
+float row_interior(const Ctx& c);   // bound of the groups that skip the periodic wrap
+
+// batch.cu: the CG iterations of many small systems as batched persistent
+// kernels in one graph (a plan per set of contexts)
+struct BatchPlan;
+int batch_plan_create(Ctx* const* cs, int count, BatchPlan** out, std::string* msg);
+void batch_plan_destroy(BatchPlan* p);
+int batch_plan_check(const BatchPlan& p, Ctx* const* cs);  // THP_E_STATE if a context was re-targeted
+int batch_plan_loop(BatchPlan& p, Ctx* const* cs);   // after the fronts; the contexts' streams wait for it
+void batch_plan_finish(BatchPlan& p, int max_iterations);  // after the streams synchronised: tuner bookkeeping
+int batch_plan_tuning(const BatchPlan& p, int* atom_blocks, int* dft_blocks, int* lines, float* ms_per_iteration);
+int batch_plan_candidates();
+// enable 1: later solves run the loop eagerly with per-kernel events (0: back
+// to the graph; -1: read only); ms[8] receives the accumulated device time of
+// spread, DFT passes 0-4, matvec and update
+int batch_plan_profile(BatchPlan& p, int enable, double* ms, int* iterations);
+int batch_plan_candidate(const BatchPlan& p);  // the launch shape the next solve uses
+bool batch_plan_profiling(const BatchPlan& p);
+// whole-solve graphs: every system's front, the batched loop and the results
+cudaGraphExec_t batch_plan_solve_exec(const BatchPlan& p, int guess, int carry, int cand);
+int batch_plan_make_solve_exec(BatchPlan& p, const std::vector<cudaGraph_t>& fronts, int guess, int carry, int cand);
+int batch_plan_run_solve(BatchPlan& p, cudaGraphExec_t ex, const CgScalars** cg_out, const int** flags_out,
+                         float* ms);
+
 }  // namespace thp

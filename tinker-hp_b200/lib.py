@@ -125,6 +125,12 @@ def load():
         "thp_efld0_recip": ([vp, _dp], C.c_int),
         "thp_tmatxbrecip": ([vp, C.c_int, _dp, _dp], C.c_int),
         "thp_solve_batch": ([C.POINTER(vp), C.c_int, C.c_int, C.POINTER(ThpSolveInfo)], C.c_int),
+        "thp_batch_create": ([C.POINTER(vp), C.c_int, C.POINTER(vp)], C.c_int),
+        "thp_batch_solve": ([vp, C.c_int, C.POINTER(ThpSolveInfo)], C.c_int),
+        "thp_batch_tuning": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                              C.POINTER(C.c_double)], C.c_int),
+        "thp_batch_profile": ([vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)], C.c_int),
+        "thp_batch_destroy": ([vp], C.c_int),
         "thp_solve_host": ([vp, _dp, _dp, _dp, _dp, _dp, _dp, C.POINTER(ThpSolveInfo)], C.c_int),
         "thp_footprint": ([C.POINTER(ThpConfig)], C.c_size_t),
         "thp_status_string": ([C.c_int], C.c_char_p),
@@ -228,6 +234,72 @@ def solve_batch(contexts, guess=GUESS_DIRECT, allow_unconverged=False):
         raise ThpError(st, "thp_solve_batch")
     return [{"niter": f.niter, "converged": bool(f.converged), "resnrm": f.resnrm, "epol": f.epol,
              "ene": tuple(f.ene), "ms": f.ms_total} for f in infos]
+
+
+def _infos(infos):
+    return [{"niter": f.niter, "converged": bool(f.converged), "resnrm": f.resnrm, "epol": f.epol,
+             "ene": tuple(f.ene), "ms": f.ms_total} for f in infos]
+
+
+class Batch:
+    """A batch plan (thp_batch_*): the CG iterations of a fixed set of small
+    resident systems run as batched persistent kernels in one CUDA graph.  The
+    contexts must stay alive (and not be re-targeted) while the plan is used."""
+
+    def __init__(self, contexts):
+        L = load()
+        self.contexts = list(contexts)
+        n = len(self.contexts)
+        hs = (C.c_void_p * n)(*[c.h for c in self.contexts])
+        h = C.c_void_p()
+        st = L.thp_batch_create(hs, n, C.byref(h))
+        if st != THP_OK:
+            raise ThpError(st, "thp_batch_create")
+        self.h = h
+
+    def solve(self, guess=GUESS_DIRECT, allow_unconverged=False):
+        n = len(self.contexts)
+        infos = (ThpSolveInfo * n)()
+        st = load().thp_batch_solve(self.h, guess, infos)
+        if st != THP_OK and not (allow_unconverged and st == THP_E_NOT_CONVERGED):
+            raise ThpError(st, "thp_batch_solve")
+        return _infos(infos)
+
+    def tuning(self):
+        """The autotuner's kept launch shape, or None while it is still tuning."""
+        a, d, l, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        st = load().thp_batch_tuning(self.h, C.byref(a), C.byref(d), C.byref(l), C.byref(ms))
+        if st == THP_E_STATE:
+            return None
+        if st != THP_OK:
+            raise ThpError(st, "thp_batch_tuning")
+        return {"atom_blocks_per_sm": a.value, "dft_blocks_per_sm": d.value, "dft_lines": l.value,
+                "ms_per_iteration": ms.value}
+
+    KERNELS = ("spread", "dft_x", "dft_y", "dft_z_qfac_z", "dft_y_inv", "dft_x_inv", "matvec", "update")
+
+    def profile(self, enable=None):
+        """enable True/False switches the eager, per-kernel-timed loop on/off
+        (resetting the accumulators); returns the accumulated ms per kernel
+        and the iterations timed so far."""
+        ms = (C.c_double * 8)()
+        it = C.c_int()
+        mode = -1 if enable is None else (1 if enable else 0)
+        st = load().thp_batch_profile(self.h, mode, ms, C.byref(it))
+        if st != THP_OK:
+            raise ThpError(st, "thp_batch_profile")
+        return dict(zip(self.KERNELS, list(ms))), it.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().thp_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def scales_array(ws):
