@@ -23,6 +23,11 @@ import time
 
 import numpy as np
 
+# Independent systems (batches, served requests) run on many streams and as
+# parallel graph branches; the default of 8 hardware work queues would run
+# at most 8 of them at a time.  Read when the CUDA context is created.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)

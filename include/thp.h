@@ -157,30 +157,35 @@ int thp_tmatxbrecip(thp_ctx* ctx, int nrhs, const double* mu, double* dipfield);
 int thp_solve_batch(thp_ctx** ctxs, int count, int guess, thp_solve_info* infos);
 /* Batch plans (the reference has no batched form; the loop each plan runs is
  * inducepcg_pme2, newinduce_pme2.f:285-636).  A plan binds a fixed set of
- * contexts on one device in one precision, each below 20,000 atoms with PME
- * grid lengths of at most 64, and runs the CG iterations of all of them as
- * batched persistent kernels: one launch per kernel per iteration walks a
- * device work list of (system, tile) items, the convolution runs as direct
- * DFTs over all grids, and the loop is one CUDA graph with a conditional
- * WHILE node that runs until every system has stopped.  The fronts (E0,
- * list, CG start) run per system as in thp_solve_batch.  An autotuner times
- * the first solves of a plan, one candidate launch shape each, and keeps the
+ * contexts on one device in one precision, each below 20,000 atoms, and runs
+ * the CG iterations of all of them as batched persistent kernels: one launch
+ * per kernel per iteration walks a device work list of (system, tile) items,
+ * the convolution runs as one batched cuFFT transform per grid shape, and the
+ * loop is a conditional WHILE node that runs until every system has stopped.
+ * A solve whose systems all take the same start (guess DIRECT, PREVIOUS or
+ * HOST after resolution, and the same dipole carry) runs as one graph launch:
+ * every system's front (E0, list, CG start) as a parallel branch, the loop,
+ * and the energies and CG scalars written to mapped host memory; other solves
+ * run the fronts per system as thp_solve_batch does.  An autotuner times the
+ * first solves of a plan, one candidate launch shape each, and keeps the
  * fastest (remembered for later plans of the same size class).
  * thp_batch_create returns THP_E_INVALID for systems outside those limits;
  * thp_batch_solve returns THP_E_STATE if a context was re-targeted
- * (thp_ctx_reset) since the plan was made; results as thp_solve_batch. */
+ * (thp_ctx_reset) since the plan was made; results as thp_solve_batch, with
+ * ms_total the device time of the whole batch. */
 typedef struct thp_batch thp_batch;
 int thp_batch_create(thp_ctx** ctxs, int count, thp_batch** out);
 int thp_batch_solve(thp_batch* b, int guess, thp_solve_info* infos);
-/* the kept launch shape: resident blocks per SM of the atom kernels and of
- * the DFT passes, lines per DFT tile, and its time per CG iteration (ms);
+/* the kept launch shape: resident blocks per SM of the batched kernels, atoms
+ * per matvec tile, and the device time of the solve it was measured on (ms);
  * THP_E_STATE while the plan is still tuning */
-int thp_batch_tuning(thp_batch* b, int* atom_blocks, int* dft_blocks, int* lines, double* ms_per_iteration);
+int thp_batch_tuning(thp_batch* b, int* blocks_per_sm, int* matvec_atoms, double* ms_per_solve);
 /* Per-kernel device time of the batched loop.  enable = 1: later solves run
  * the loop eagerly, one host-checked iteration at a time, with events around
- * each kernel (the accumulators restart); 0: back to the graph; -1: only
- * read.  ms[8] receives the accumulated ms of the spread, the five DFT passes,
- * the matvec and the update; iterations the batched iterations timed. */
+ * each step (the accumulators restart); 0: back to the graph; -1: only read.
+ * ms[6] receives the accumulated ms of the spread, the forward FFTs, the
+ * influence function, the inverse FFTs, the matvec and the update;
+ * iterations the batched iterations timed. */
 int thp_batch_profile(thp_batch* b, int enable, double* ms, int* iterations);
 int thp_batch_destroy(thp_batch* b);
 /* Gradient of the polarization energy, epolar1c (epolar1.f:57-372): eprecip1

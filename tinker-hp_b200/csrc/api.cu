@@ -499,7 +499,7 @@ static void apply_config(Ctx& c, const thp_config& k) {
   c.box.recip[2] = (k.box[0] * (k.box[1] * 1.0) - (k.box[1] * 0.0) * 0.0) / vol;
   cell_grid(k, c.nc);
   c.ncell = c.nc[0] * c.nc[1] * c.nc[2];
-  c.nblk_reduce = (c.n + 127) / 128;
+  c.nblk_reduce = (c.n + 31) / 32;  // partial sums of up to one block per 32 atoms
 }
 
 extern "C++" {
@@ -1498,7 +1498,7 @@ static int batch_solve_graph(thp_batch* b, int guess, thp_solve_info* infos) {
   std::vector<const int*> fls(count);
   float ms = 0.f;
   const int sr = batch_plan_run_solve(p, ex, cgs.data(), fls.data(), &ms);
-  int worst = THP_OK, maxit = 0;
+  int worst = THP_OK;
   for (int i = 0; i < count; ++i) {
     thp_ctx* h = b->hs[i];
     Ctx& c = h->c;
@@ -1508,7 +1508,6 @@ static int batch_solve_graph(thp_batch* b, int guess, thp_solve_info* infos) {
       *c.h_flags = *fls[i];
       st = flags_status(c);
       if (!st) st = pcg_status(c);
-      maxit = std::max(maxit, c.h_cg->niter);
     }
     if (!st || st == THP_E_NOT_CONVERGED) {
       h->solved_once = true;
@@ -1527,7 +1526,7 @@ static int batch_solve_graph(thp_batch* b, int guess, thp_solve_info* infos) {
     }
     if (st && (worst == THP_OK || worst == THP_E_NOT_CONVERGED)) worst = st;
   }
-  if (!sr) batch_plan_finish(p, maxit);
+  if (!sr) batch_plan_finish(p);
   return worst;
 }
 
@@ -1551,7 +1550,6 @@ int thp_batch_solve(thp_batch* b, int guess, thp_solve_info* infos) {
     cudaMemsetAsync(&c.d_cg->stop, 1, sizeof(int), c.stream);
   }
   const int sl = batch_plan_loop(*b->plan, b->cs.data());
-  int maxit = 0;
   for (int i = 0; i < count; ++i) {
     Ctx& c = *b->cs[i];
     set_current_device(c);
@@ -1559,17 +1557,16 @@ int thp_batch_solve(thp_batch* b, int guess, thp_solve_info* infos) {
     cudaMemcpyAsync(c.h_cg, c.d_cg, sizeof(CgScalars), cudaMemcpyDeviceToHost, c.stream);
     const int ss = cuda_status(cudaStreamSynchronize(c.stream), &c, "batch sync");
     if (ss && !st[i]) st[i] = ss;
-    if (!st[i]) maxit = std::max(maxit, c.h_cg->niter);
   }
-  if (!sl) batch_plan_finish(*b->plan, maxit);
+  if (!sl) batch_plan_finish(*b->plan);
   return batch_finish(hs, count, st, infos);
 }
 
-int thp_batch_tuning(thp_batch* b, int* atom_blocks, int* dft_blocks, int* lines, double* ms_per_iteration) {
-  if (!b || !atom_blocks || !dft_blocks || !lines) return THP_E_INVALID;
+int thp_batch_tuning(thp_batch* b, int* blocks_per_sm, int* matvec_atoms, double* ms_per_solve) {
+  if (!b || !blocks_per_sm || !matvec_atoms) return THP_E_INVALID;
   float ms = 0.f;
-  const int st = batch_plan_tuning(*b->plan, atom_blocks, dft_blocks, lines, &ms);
-  if (ms_per_iteration) *ms_per_iteration = ms;
+  const int st = batch_plan_tuning(*b->plan, blocks_per_sm, matvec_atoms, &ms);
+  if (ms_per_solve) *ms_per_solve = ms;
   return st;
 }
 

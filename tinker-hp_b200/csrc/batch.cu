@@ -8,22 +8,24 @@
 // (system, tile) items (the per-system queues laid end to end), each resident
 // block taking items round-robin, and runs the same block-level code as the
 // single-system kernels (cg_dev.cuh) on the item's system.  Per iteration:
-//   1. kb_spread: pp = zr + beta pp (FP32 copy for the mixed rows) and the
-//      dipole spread into grid A (grid_uind_site, pmestuff.f:280-405);
-//   2. kb_dft x5: the convolution as DFTs along x, y, z of the small grids,
-//      each line in two stages of short DFTs (the forward z pass, the
-//      influence function and the inverse z pass fused), A -> B; the first
-//      pass zeroes A behind it for the next spread;
-//   3. kb_matvec: real-space rows, the dipole field gathered from B
+//   1. kb_spread: pp = zr + beta pp (the 32-byte partner records of the mixed
+//      rows beside it) and the dipole spread (grid_uind_site,
+//      pmestuff.f:280-405) into the plan's grids, zeroed just before;
+//   2. the convolution: one batched cuFFT transform per grid-size class (the
+//      classes' grids lie end to end, and the classes run as parallel
+//      branches), kb_qfac over every grid, the batched inverse transforms;
+//   3. kb_matvec: real-space rows, the dipole field gathered from the grid
 //      (fphi_uind_site), h, pp.h and alpha;
 //   4. kb_update: mu, residual, preconditioned residual, beta and the stop
 //      test;
 //   5. kb_cond: keeps the conditional WHILE node looping while a system runs.
 // A system that has converged skips its items.  The whole loop is one CUDA
-// graph.  The item tiles and the resident blocks per SM come from an online
+// graph, and the whole solve (every system's front as a child graph, the
+// loop, Epol and the results written to mapped host memory) another.  The
+// resident blocks per SM and the matvec's tile come from an online
 // autotuner: the first solves of a plan each run one candidate, timed with
-// events per CG iteration, and the fastest is kept (and remembered for plans
-// of the same size class).
+// events, and the fastest is kept (and remembered for plans of the same size
+// class).
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -41,10 +43,10 @@ namespace {
 using namespace cg;
 
 // One system of the batch: its sizes and the device buffers its context owns
-// (grid2, the DFT's output grid, belongs to the plan).
+// (grid, its PME grid in the batched transforms' layout, belongs to the plan).
 struct BatchSys {
-  int n, nblk;  // atoms; blocks of kBlock atoms
-  int nfft[3];
+  int n, nblk;       // atoms; blocks of kBlock atoms
+  int nblk_mv[2];    // blocks of 16 and 32 atoms (the matvec's items)
   int ngrid;
   int politer;
   double poleps, term;
@@ -58,8 +60,7 @@ struct BatchSys {
   const double* ef;
   double *mu, *res, *h, *zr, *pp;
   float *rec, *mpz;  // mixed form: 32-byte partner records of pp (PartnerRec)
-  void* grid;   // A: the spread's target, the context's PME grid
-  void* grid2;  // B: the convolved grid the matvec gathers from
+  void* grid;  // the system's grid in the plan's class-ordered grid array
   const void* qfac;
   CgScalars* cg;
   double* partials;
@@ -72,11 +73,6 @@ struct BatchOut {
   CgScalars cg;
   int flags;
 };
-
-constexpr int kDftThreads = 256;
-constexpr int kDftMaxN = 64;       // grid lengths the batched DFT takes
-constexpr int kMaxLines = 32;      // lines per DFT tile
-constexpr int kDftMaxOut = kMaxLines * kDftMaxN / kDftThreads;  // outputs per thread
 
 // pp = zr + beta pp and the spread of the new pp (the work of k_spread_dip,
 // mode 1); the mixed form also writes the 32-byte partner records its
@@ -109,220 +105,42 @@ __global__ void __launch_bounds__(kBlock) kb_spread(const BatchSys* __restrict__
   }
 }
 
-// Lines of one DFT pass: dimension d of the [n3][n2][n1] grid, line l of
-// the lines_of(d) lines starts at line_base and steps by line_stride.
-__device__ __forceinline__ int lines_of(const BatchSys& s, int d) { return s.ngrid / s.nfft[d]; }
-__device__ __forceinline__ int line_stride(const BatchSys& s, int d) {
-  return d == 0 ? 1 : (d == 1 ? s.nfft[0] : s.nfft[0] * s.nfft[1]);
-}
-__device__ __forceinline__ int line_base(const BatchSys& s, int d, int l) {
-  if (d == 0) return l * s.nfft[0];
-  if (d == 1) return (l / s.nfft[0]) * s.nfft[0] * s.nfft[1] + l % s.nfft[0];
-  return l;
-}
-
-// Transforms of one line as two stages of short DFTs (Cooley-Tukey with
-// N = N1 N2, n = N2 n1 + n2, k = k1 + N1 k2):
-//   Y[k1 N2 + n2] = W^(n2 k1) sum_n1 x[N2 n1 + n2] W^(N2 n1 k1)
-//   X[k1 + N1 k2] = sum_n2 Y[k1 N2 + n2] W^(N1 n2 k2)
-// with W = exp(-2 pi i / N) forward (cuFFT's sign) and its conjugate
-// inverse; N (N1 + N2) products per line instead of N^2.
-template <typename T, typename C>
-__device__ __forceinline__ C cmul(C a, C w, bool forward) {
-  C r;
-  if (forward) {
-    r.x = a.x * w.x + a.y * w.y;
-    r.y = a.y * w.x - a.x * w.y;
-  } else {
-    r.x = a.x * w.x - a.y * w.y;
-    r.y = a.y * w.x + a.x * w.y;
-  }
-  return r;
-}
-template <typename T, typename C>
-__device__ __forceinline__ C dft_stage1(const C* x, const C* tw, int N, int N1, int N2, int o, bool forward) {
-  const int k1 = o / N2, n2 = o - k1 * N2;
-  const int step = (N2 * k1) % N;
-  T re = T(0), im = T(0);
-  int m = 0;
-  for (int n1 = 0; n1 < N1; ++n1) {
-    const C v = cmul<T>(x[N2 * n1 + n2], tw[m], forward);
-    re += v.x;
-    im += v.y;
-    m += step;
-    if (m >= N) m -= N;
-  }
-  C r;
-  r.x = re;
-  r.y = im;
-  return cmul<T>(r, tw[(n2 * k1) % N], forward);
-}
-template <typename T, typename C>
-__device__ __forceinline__ C dft_stage2(const C* y, const C* tw, int N, int N1, int N2, int k, bool forward) {
-  const int k2 = k / N1, k1 = k - k2 * N1;
-  const int step = (N1 * k2) % N;
-  const C* yk = y + k1 * N2;
-  T re = T(0), im = T(0);
-  int m = 0;
-  for (int n2 = 0; n2 < N2; ++n2) {
-    const C v = cmul<T>(yk[n2], tw[m], forward);
-    re += v.x;
-    im += v.y;
-    m += step;
-    if (m >= N) m -= N;
-  }
-  C r;
-  r.x = re;
-  r.y = im;
-  return r;
-}
-
-// the larger factor pair N1 <= N2 of N with N1 as close to sqrt(N) as it gets
-__device__ __forceinline__ int dft_split(int N) {
-  int best = 1;
-  for (int f = 2; f * f <= N; ++f)
-    if (N % f == 0) best = f;
-  return best;
-}
-
-// Position of element e of a tile of lt lines: x lines walk each line, y and
-// z lines walk across lines first (neighbouring lines are neighbouring
-// points of the grid).
-__device__ __forceinline__ void tile_pos(int d, int e, int lt, int N, int& l, int& j) {
-  if (d == 0) {
-    l = e / N;
-    j = e - l * N;
-  } else {
-    j = e / lt;
-    l = e - j * lt;
-  }
-}
-
-// One transform of every line of the tile held in buf (row pitch N + 1): the
-// results end in the threads' out[] (element e = threadIdx.x + q blockDim.x).
-template <typename T, typename C>
-__device__ __forceinline__ void tile_dft(C* buf, const C* tw, int d, int lt, int N, int N1, int N2, bool forward,
-                                         C (&out)[kDftMaxOut]) {
-  const int ne = lt * N;
-#pragma unroll
-  for (int q = 0; q < kDftMaxOut; ++q) {
-    const int e = threadIdx.x + q * kDftThreads;
-    if (e < ne) {
-      int l, o;
-      tile_pos(d, e, lt, N, l, o);
-      out[q] = dft_stage1<T>(buf + l * (N + 1), tw, N, N1, N2, o, forward);
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < kDftMaxOut; ++q) {
-    const int e = threadIdx.x + q * kDftThreads;
-    if (e < ne) {
-      int l, o;
-      tile_pos(d, e, lt, N, l, o);
-      buf[l * (N + 1) + o] = out[q];
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < kDftMaxOut; ++q) {
-    const int e = threadIdx.x + q * kDftThreads;
-    if (e < ne) {
-      int l, k;
-      tile_pos(d, e, lt, N, l, k);
-      out[q] = dft_stage2<T>(buf + l * (N + 1), tw, N, N1, N2, k, forward);
-    }
-  }
-}
-
-// One pass of the convolution over tiles of L lines (pass 0: x forward, A ->
-// B with A zeroed; 1: y forward; 2: z forward, times qfac, z inverse; 3: y
-// inverse; 4: x inverse; passes 1-4 on B).  Unnormalised transforms, as the
-// single-system path's cuFFT C2C / Z2Z (fft_mpi.f90:65,115).
+// The influence function on every running system's transformed grid; items
+// (system, chunk of kQfacChunk points).
+constexpr int kQfacChunk = 2048;
 template <typename T>
-__global__ void __launch_bounds__(kDftThreads) kb_dft(const BatchSys* __restrict__ sys, const int2* __restrict__ items,
-                                                      int nitems, int pass, int L) {
+__global__ void __launch_bounds__(256) kb_qfac(const BatchSys* __restrict__ sys, const int2* __restrict__ items,
+                                               int nitems) {
   using C = typename Cplx<T>::type;
-  extern __shared__ __align__(16) unsigned char dft_smem[];
-  C* tw = reinterpret_cast<C*>(dft_smem);
-  C* buf = tw + kDftMaxN;
-  const int d = pass == 0 || pass == 4 ? 0 : (pass == 1 || pass == 3 ? 1 : 2);
-  const bool forward = pass <= 2;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = items[it];
     const BatchSys& s = sys[w.x];
-    if (s.cg->stop) continue;  // the same for the whole block
-    const int N = s.nfft[d], nl = lines_of(s, d), stride = line_stride(s, d);
-    const int N1 = dft_split(N), N2 = N / N1;
-    const int l0 = w.y * L;
-    const int lt = min(L, nl - l0);
-    const int ne = lt * N;
-    C* src = reinterpret_cast<C*>(pass == 0 ? s.grid : s.grid2);
-    C* dst = reinterpret_cast<C*>(s.grid2);
-    for (int m = threadIdx.x; m < N; m += blockDim.x) {
-      double sn, cs;
-      sincospi(2.0 * m / N, &sn, &cs);
-      tw[m].x = (T)cs;
-      tw[m].y = (T)sn;
+    if (s.cg->stop) continue;
+    C* g = reinterpret_cast<C*>(s.grid);
+    const T* f = reinterpret_cast<const T*>(s.qfac);
+    const int e1 = min(s.ngrid, (w.y + 1) * kQfacChunk);
+    for (int e = w.y * kQfacChunk + threadIdx.x; e < e1; e += blockDim.x) {
+      C v = g[e];
+      const T q = f[e];
+      v.x *= q;
+      v.y *= q;
+      g[e] = v;
     }
-    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-      int l, j;
-      tile_pos(d, e, lt, N, l, j);
-      const size_t gi = (size_t)line_base(s, d, l0 + l) + (size_t)j * stride;
-      buf[l * (N + 1) + j] = src[gi];
-      if (pass == 0) {
-        C zero;
-        zero.x = zero.y = T(0);
-        src[gi] = zero;
-      }
-    }
-    __syncthreads();
-    C out[kDftMaxOut];
-    tile_dft<T>(buf, tw, d, lt, N, N1, N2, forward, out);
-    if (pass == 2) {
-      // influence function on the transformed line, then the inverse z pass
-      const T* qf = reinterpret_cast<const T*>(s.qfac);
-      __syncthreads();
-#pragma unroll
-      for (int q = 0; q < kDftMaxOut; ++q) {
-        const int e = threadIdx.x + q * kDftThreads;
-        if (e < ne) {
-          int l, k;
-          tile_pos(d, e, lt, N, l, k);
-          const T f = qf[(size_t)line_base(s, d, l0 + l) + (size_t)k * stride];
-          C v = out[q];
-          v.x *= f;
-          v.y *= f;
-          buf[l * (N + 1) + k] = v;
-        }
-      }
-      __syncthreads();
-      tile_dft<T>(buf, tw, d, lt, N, N1, N2, false, out);
-    }
-#pragma unroll
-    for (int q = 0; q < kDftMaxOut; ++q) {
-      const int e = threadIdx.x + q * kDftThreads;
-      if (e < ne) {
-        int l, k;
-        tile_pos(d, e, lt, N, l, k);
-        dst[(size_t)line_base(s, d, l0 + l) + (size_t)k * stride] = out[q];
-      }
-    }
-    __syncthreads();  // buf and tw are reused by the block's next item
   }
 }
 
-// real-space rows + dipole field gathered from B + h, pp.h, alpha
-template <bool MIXED>
+// real-space rows + dipole field gathered from the convolved grid + h, pp.h,
+// alpha; items of 16 GPW atoms
+template <bool MIXED, int GPW>
 __global__ void __launch_bounds__(kBlock) kb_matvec(const BatchSys* __restrict__ sys, const int2* __restrict__ items,
                                                     int nitems) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = items[it];
     const BatchSys& s = sys[w.x];
     if (s.cg->stop) continue;
-    cg_matvec_block<MIXED, MIXED ? 1 : 2, MIXED>(w.y, s.nblk, s.pr, s.box, s.pos, s.posf, nullptr, s.g, s.grid2,
-                                                 s.pp, nullptr, s.rec, s.mpz, s.pol, s.ef, s.term, 0, s.h, s.res,
-                                                 s.zr, s.pp, s.cg, s.partials, s.interior);
+    cg_matvec_block<MIXED, MIXED ? 1 : 2, MIXED, GPW>(w.y, s.nblk_mv[GPW - 1], s.pr, s.box, s.pos, s.posf, nullptr,
+                                                      s.g, s.grid, s.pp, nullptr, s.rec, s.mpz, s.pol, s.ef, s.term,
+                                                      0, s.h, s.res, s.zr, s.pp, s.cg, s.partials, s.interior);
   }
 }
 
@@ -388,18 +206,8 @@ __global__ void kb_running(const BatchSys* __restrict__ sys, int count, int* out
   if (threadIdx.x == 0) *out = r;
 }
 
-// A grids of every system to zero (before the first spread of a solve)
-template <typename T>
-__global__ void kb_zero(const BatchSys* __restrict__ sys, int count, unsigned* loops) {
-  using C = typename Cplx<T>::type;
-  if (blockIdx.x == 0 && threadIdx.x == 0) *loops = 0;
-  for (int q = 0; q < count; ++q) {
-    C* g = reinterpret_cast<C*>(sys[q].grid);
-    C zero;
-    zero.x = zero.y = T(0);
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < sys[q].ngrid; e += gridDim.x * blockDim.x) g[e] = zero;
-  }
-}
+// the loop counter of kb_cond, before each solve's loop
+__global__ void kb_reset(unsigned* loops) { *loops = 0; }
 
 int sm_count(int device) {
   int v = 0;
@@ -409,46 +217,61 @@ int sm_count(int device) {
 
 }  // namespace
 
-// Autotuner candidates: resident blocks per SM of the atom kernels (spread,
-// matvec, update) and of the DFT passes, and lines per DFT tile.
+// Autotuner candidates: resident blocks per SM of the batched kernels and
+// groups of four atoms per warp in the matvec (tiles of 16 GPW atoms).
 struct BatchTune {
-  int atom_blocks, dft_blocks, lines;
+  int blocks, gpw;
 };
-static const BatchTune kCandidates[] = {{4, 4, 32}, {8, 8, 32}, {16, 8, 32}, {8, 8, 16}, {16, 16, 16}, {4, 8, 16}};
+static const BatchTune kCandidates[] = {{4, 2}, {8, 2}, {16, 2}, {4, 1}, {8, 1}, {16, 1}};
 constexpr int kNumCandidates = (int)(sizeof(kCandidates) / sizeof(kCandidates[0]));
 
 // size class of a plan: precision, log2 of its atoms and of its systems
-using TuneKey = std::tuple<int, int, int, int>;
+using TuneKey = std::tuple<int, int, int>;
 static std::mutex g_tune_mu;
 static std::map<TuneKey, int> g_tuned;
+
+// The systems of one grid shape: their grids lie end to end in the plan's
+// grid array and one batched cuFFT plan transforms them all, on a stream of
+// its own (a parallel branch of the graph).
+struct FftClass {
+  int n[3] = {0, 0, 0};
+  int count = 0;
+  size_t offset = 0;  // first grid point of the class in the plan's array
+  cufftHandle plan = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+};
 
 struct BatchPlan {
   int device = 0, mixed = 0, count = 0, sms = 1;
   int politer_max = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev_start = nullptr, ev_loop = nullptr, ev_done = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_loop = nullptr, ev_done = nullptr, ev_fork = nullptr;
   BatchSys* d_sys = nullptr;
-  int2* d_atom_items = nullptr;
+  int2* d_atom_items = nullptr;  // (system, block of kBlock atoms)
   int n_atom_items = 0;
-  int2* d_dft_items[2][3] = {};  // [lines 32 / 16][dimension]
-  int n_dft_items[2][3] = {};
-  void* d_grid2 = nullptr;
+  int2* d_mv_items[2] = {};      // (system, block of 16 / 32 atoms)
+  int n_mv_items[2] = {};
+  int2* d_qfac_items = nullptr;  // (system, chunk of grid points)
+  int n_qfac_items = 0;
+  void* d_grid = nullptr;        // every system's grid, class by class
+  size_t grid_bytes = 0;
+  std::vector<FftClass> classes;
   unsigned* d_loops = nullptr;
-  std::vector<int> sys_atoms;
   // the buffers each system's descriptor points at, checked before every
   // solve (a context re-targeted since the plan was made invalidates it)
-  std::vector<std::tuple<int, const void*, const void*, const void*, const void*>> sig;
+  std::vector<std::tuple<int, const void*, const void*, const void*>> sig;
   cudaGraphExec_t exec[kNumCandidates] = {};
-  float best_ms_per_it[kNumCandidates];
-  int tried = 0;          // candidates measured so far (online tuning)
-  int chosen = -1;        // the kept candidate
-  int running = -1;       // candidate of the solve in flight
+  float best_ms[kNumCandidates];
+  int tried = 0;    // candidates measured so far (online tuning)
+  int chosen = -1;  // the kept candidate
+  int running = -1; // candidate of the solve in flight
   TuneKey key;
-  std::string msg;
   // profiling: the loop runs eagerly, one host-checked iteration at a time,
-  // with events around each kernel (spread, five DFT passes, matvec, update)
+  // with events around each step (spread, forward FFTs, qfac, inverse FFTs,
+  // matvec, update)
   bool profiling = false;
-  static constexpr int kKernels = 8;
+  static constexpr int kKernels = 6;
   cudaEvent_t prof_ev[kKernels + 1] = {};
   double prof_ms[kKernels] = {};
   int prof_iterations = 0;
@@ -461,39 +284,64 @@ struct BatchPlan {
   BatchOut* d_out = nullptr;
 };
 
-static int lines_index(int lines) { return lines == 32 ? 0 : 1; }
+// Every class's batched transform in one direction, as parallel branches.
+static int enqueue_ffts(BatchPlan& p, int dir) {
+  cudaEventRecord(p.ev_fork, p.stream);
+  for (FftClass& k : p.classes) {
+    cudaStreamWaitEvent(k.stream, p.ev_fork, 0);
+    cufftResult r;
+    if (p.mixed) {
+      cufftComplex* g = static_cast<cufftComplex*>(p.d_grid) + k.offset;
+      r = cufftExecC2C(k.plan, g, g, dir);
+    } else {
+      cufftDoubleComplex* g = static_cast<cufftDoubleComplex*>(p.d_grid) + k.offset;
+      r = cufftExecZ2Z(k.plan, g, g, dir);
+    }
+    if (r != CUFFT_SUCCESS) return THP_E_CUDA;
+    cudaEventRecord(k.done, k.stream);
+    cudaStreamWaitEvent(p.stream, k.done, 0);
+  }
+  return THP_OK;
+}
 
-// One batched CG iteration; with events (profiling) each kernel is bracketed
+// One batched CG iteration; with events (profiling) each step is bracketed
 // and no condition node is written.
 static int enqueue_body(BatchPlan& p, const BatchTune& t, cudaGraphConditionalHandle handle, bool events = false) {
-  const int ab = std::max(1, std::min(p.n_atom_items, t.atom_blocks * p.sms));
+  const int ab = std::max(1, std::min(p.n_atom_items, t.blocks * p.sms));
   int ke = 0;
   auto mark = [&]() {
     if (events) cudaEventRecord(p.prof_ev[ke++], p.stream);
   };
   mark();
+  cudaMemsetAsync(p.d_grid, 0, p.grid_bytes, p.stream);
   if (p.mixed)
     kb_spread<true><<<ab, kBlock, 0, p.stream>>>(p.d_sys, p.d_atom_items, p.n_atom_items);
   else
     kb_spread<false><<<ab, kBlock, 0, p.stream>>>(p.d_sys, p.d_atom_items, p.n_atom_items);
-  const int li = lines_index(t.lines);
-  const size_t csz = p.mixed ? sizeof(cufftComplex) : sizeof(cufftDoubleComplex);
-  const size_t smem = csz * (kDftMaxN + (size_t)t.lines * (kDftMaxN + 1));
-  for (int pass = 0; pass < 5; ++pass) {
-    const int d = pass == 0 || pass == 4 ? 0 : (pass == 1 || pass == 3 ? 1 : 2);
-    const int ni = p.n_dft_items[li][d];
-    const int db = std::max(1, std::min(ni, t.dft_blocks * p.sms));
-    mark();
-    if (p.mixed)
-      kb_dft<float><<<db, kDftThreads, smem, p.stream>>>(p.d_sys, p.d_dft_items[li][d], ni, pass, t.lines);
-    else
-      kb_dft<double><<<db, kDftThreads, smem, p.stream>>>(p.d_sys, p.d_dft_items[li][d], ni, pass, t.lines);
-  }
   mark();
+  if (enqueue_ffts(p, CUFFT_FORWARD)) return THP_E_CUDA;
+  mark();
+  const int qb = std::max(1, std::min(p.n_qfac_items, 8 * p.sms));
   if (p.mixed)
-    kb_matvec<true><<<ab, kBlock, 0, p.stream>>>(p.d_sys, p.d_atom_items, p.n_atom_items);
+    kb_qfac<float><<<qb, 256, 0, p.stream>>>(p.d_sys, p.d_qfac_items, p.n_qfac_items);
   else
-    kb_matvec<false><<<ab, kBlock, 0, p.stream>>>(p.d_sys, p.d_atom_items, p.n_atom_items);
+    kb_qfac<double><<<qb, 256, 0, p.stream>>>(p.d_sys, p.d_qfac_items, p.n_qfac_items);
+  mark();
+  if (enqueue_ffts(p, CUFFT_INVERSE)) return THP_E_CUDA;
+  mark();
+  const int g = t.gpw - 1;
+  const int mb = std::max(1, std::min(p.n_mv_items[g], t.blocks * p.sms));
+  if (p.mixed) {
+    if (t.gpw == 1)
+      kb_matvec<true, 1><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
+    else
+      kb_matvec<true, 2><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
+  } else {
+    if (t.gpw == 1)
+      kb_matvec<false, 1><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
+    else
+      kb_matvec<false, 2><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
+  }
   mark();
   kb_update<<<ab, kBlock, 0, p.stream>>>(p.d_sys, p.d_atom_items, p.n_atom_items);
   mark();
@@ -532,7 +380,6 @@ static int build_graph(BatchPlan& p, int cand) {
   if (!st && cudaGraphInstantiate(&p.exec[cand], g, 0) != cudaSuccess) st = THP_E_CUDA;
   if (st) {
     p.exec[cand] = nullptr;
-    p.msg = "batch: the loop graph could not be built";
     cudaGetLastError();
   }
   cudaGraphDestroy(g);
@@ -547,20 +394,24 @@ void batch_plan_destroy(BatchPlan* p) {
     if (e) cudaGraphExecDestroy(e);
   for (auto& kv : p->solve_exec)
     if (kv.second) cudaGraphExecDestroy(kv.second);
+  for (FftClass& k : p->classes) {
+    if (k.plan) cufftDestroy(k.plan);
+    if (k.stream) cudaStreamDestroy(k.stream);
+    if (k.done) cudaEventDestroy(k.done);
+  }
   if (p->h_out) cudaFreeHost(p->h_out);
   cudaFree(p->d_sys);
   cudaFree(p->d_atom_items);
-  for (auto& a : p->d_dft_items)
-    for (auto& q : a) cudaFree(q);
-  cudaFree(p->d_grid2);
+  for (auto& m : p->d_mv_items) cudaFree(m);
+  cudaFree(p->d_qfac_items);
+  cudaFree(p->d_grid);
   cudaFree(p->d_loops);
   for (auto& e : p->prof_ev)
     if (e) cudaEventDestroy(e);
   if (p->h_running) cudaFreeHost(p->h_running);
   cudaFree(p->d_running);
-  if (p->ev_start) cudaEventDestroy(p->ev_start);
-  if (p->ev_loop) cudaEventDestroy(p->ev_loop);
-  if (p->ev_done) cudaEventDestroy(p->ev_done);
+  for (cudaEvent_t e : {p->ev_start, p->ev_loop, p->ev_done, p->ev_fork})
+    if (e) cudaEventDestroy(e);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
 }
@@ -587,8 +438,6 @@ int batch_plan_create(Ctx* const* cs, int count, BatchPlan** out, std::string* m
     if (c.device != c0.device || c.mixed != c0.mixed)
       return fail(THP_E_INVALID, "batch: systems on different devices or in different precisions");
     if (overlap_rows(c)) return fail(THP_E_INVALID, "batch: a system too large for the batched kernels");
-    for (int d = 0; d < 3; ++d)
-      if (c.cfg.nfft[d] > kDftMaxN) return fail(THP_E_INVALID, "batch: a PME grid longer than 64 points");
     if (!c.d_grid || !c.d_qfac || !c.d_pp) return fail(THP_E_STATE, "batch: a context without buffers");
   }
   BatchPlan* p = new BatchPlan();
@@ -603,34 +452,57 @@ int batch_plan_create(Ctx* const* cs, int count, BatchPlan** out, std::string* m
     return e == cudaSuccess;
   };
   ok(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
-  ok(cudaEventCreate(&p->ev_start));
-  ok(cudaEventCreate(&p->ev_loop));
-  ok(cudaEventCreate(&p->ev_done));
+  for (cudaEvent_t* e : {&p->ev_start, &p->ev_loop, &p->ev_done}) ok(cudaEventCreate(e));
+  ok(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
   const size_t csz = p->mixed ? sizeof(cufftComplex) : sizeof(cufftDoubleComplex);
-  size_t grid_total = 0;
   long atoms = 0;
+  for (int q = 0; q < count; ++q) atoms += cs[q]->n;
+  // grid-shape classes, in order of first appearance; each system's grid
+  // goes to its class's run of the grid array
+  std::vector<int> cls(count);
   for (int q = 0; q < count; ++q) {
-    grid_total += cs[q]->ngrid;
-    atoms += cs[q]->n;
+    const int* n = cs[q]->cfg.nfft;
+    int k = 0;
+    while (k < (int)p->classes.size() &&
+           !(p->classes[k].n[0] == n[0] && p->classes[k].n[1] == n[1] && p->classes[k].n[2] == n[2]))
+      ++k;
+    if (k == (int)p->classes.size()) {
+      p->classes.emplace_back();
+      for (int d = 0; d < 3; ++d) p->classes[k].n[d] = n[d];
+    }
+    cls[q] = k;
+    ++p->classes[k].count;
   }
-  ok(cudaMalloc(&p->d_grid2, grid_total * csz));
+  size_t off = 0;
+  for (FftClass& k : p->classes) {
+    k.offset = off;
+    off += (size_t)k.count * k.n[0] * k.n[1] * k.n[2];
+  }
+  p->grid_bytes = off * csz;
+  ok(cudaMalloc(&p->d_grid, p->grid_bytes));
+  for (FftClass& k : p->classes) {
+    const int dims[3] = {k.n[2], k.n[1], k.n[0]};
+    const int dist = k.n[0] * k.n[1] * k.n[2];
+    if (cufftPlanMany(&k.plan, 3, const_cast<int*>(dims), nullptr, 1, dist, nullptr, 1, dist,
+                      p->mixed ? CUFFT_C2C : CUFFT_Z2Z, k.count) != CUFFT_SUCCESS && !st)
+      st = THP_E_CUDA;
+    ok(cudaStreamCreateWithFlags(&k.stream, cudaStreamNonBlocking));
+    ok(cudaEventCreateWithFlags(&k.done, cudaEventDisableTiming));
+    if (k.plan) cufftSetStream(k.plan, k.stream);
+  }
   ok(cudaMalloc(&p->d_loops, sizeof(unsigned)));
   if (ok(cudaHostAlloc((void**)&p->h_out, sizeof(BatchOut) * count, cudaHostAllocMapped)))
     ok(cudaHostGetDevicePointer((void**)&p->d_out, p->h_out, 0));
   std::vector<BatchSys> hs(count);
-  std::vector<int2> atom_items;
-  std::vector<int2> dft_items[2][3];
-  size_t goff = 0;
-  // large systems first, so the round-robin ends on small items
-  std::vector<int> order(count);
-  for (int q = 0; q < count; ++q) order[q] = q;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cs[a]->n > cs[b]->n; });
+  std::vector<size_t> next(p->classes.size());
+  for (size_t k = 0; k < p->classes.size(); ++k) next[k] = p->classes[k].offset;
   for (int q = 0; q < count; ++q) {
     Ctx& c = *cs[q];
     BatchSys& s = hs[q];
     s.n = c.n;
     s.nblk = (c.n + kBlock - 1) / kBlock;
-    for (int d = 0; d < 3; ++d) s.nfft[d] = c.cfg.nfft[d];
+    s.nblk_mv[0] = (c.n + 15) / 16;
+    s.nblk_mv[1] = (c.n + 31) / 32;
     s.ngrid = (int)c.ngrid;
     s.politer = c.cfg.politer;
     s.poleps = c.cfg.poleps;
@@ -651,47 +523,48 @@ int batch_plan_create(Ctx* const* cs, int count, BatchPlan** out, std::string* m
     s.pp = c.d_pp;
     s.rec = c.d_rec;
     s.mpz = c.d_mpz;
-    s.grid = c.d_grid;
-    s.grid2 = static_cast<char*>(p->d_grid2) + goff * csz;
-    goff += c.ngrid;
+    s.grid = static_cast<char*>(p->d_grid) + next[cls[q]] * csz;
+    next[cls[q]] += c.ngrid;
     s.qfac = c.d_qfac;
     s.cg = c.d_cg;
     s.partials = c.d_partials;
     s.flags = c.d_flags;
     p->politer_max = std::max(p->politer_max, c.cfg.politer);
-    p->sys_atoms.push_back(c.n);
-    p->sig.emplace_back(c.n, c.d_pp, c.d_grid, c.d_pk, c.d_cg);
+    p->sig.emplace_back(c.n, c.d_pp, c.d_pk, c.d_cg);
   }
+  // work lists, large systems first so the round-robin ends on small items
+  std::vector<int> order(count);
+  for (int q = 0; q < count; ++q) order[q] = q;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cs[a]->n > cs[b]->n; });
+  std::vector<int2> atom_items, mv_items[2], qfac_items;
   for (int q : order) {
+    for (int b = 0; b * kQfacChunk < hs[q].ngrid; ++b) qfac_items.push_back(make_int2(q, b));
     for (int b = 0; b < hs[q].nblk; ++b) atom_items.push_back(make_int2(q, b));
-    for (int li = 0; li < 2; ++li)
-      for (int d = 0; d < 3; ++d) {
-        const int L = li == 0 ? 32 : 16;
-        const int nl = hs[q].ngrid / hs[q].nfft[d];
-        for (int t = 0; t * L < nl; ++t) dft_items[li][d].push_back(make_int2(q, t));
-      }
+    for (int g = 0; g < 2; ++g)
+      for (int b = 0; b < hs[q].nblk_mv[g]; ++b) mv_items[g].push_back(make_int2(q, b));
   }
   ok(cudaMalloc(&p->d_sys, sizeof(BatchSys) * count));
   ok(cudaMemcpy(p->d_sys, hs.data(), sizeof(BatchSys) * count, cudaMemcpyHostToDevice));
   p->n_atom_items = (int)atom_items.size();
   ok(cudaMalloc(&p->d_atom_items, sizeof(int2) * atom_items.size()));
   ok(cudaMemcpy(p->d_atom_items, atom_items.data(), sizeof(int2) * atom_items.size(), cudaMemcpyHostToDevice));
-  for (int li = 0; li < 2; ++li)
-    for (int d = 0; d < 3; ++d) {
-      const auto& v = dft_items[li][d];
-      p->n_dft_items[li][d] = (int)v.size();
-      ok(cudaMalloc(&p->d_dft_items[li][d], sizeof(int2) * std::max<size_t>(1, v.size())));
-      ok(cudaMemcpy(p->d_dft_items[li][d], v.data(), sizeof(int2) * v.size(), cudaMemcpyHostToDevice));
-    }
-  p->key = TuneKey(p->mixed, log2i(atoms), log2i(count), 0);
+  p->n_qfac_items = (int)qfac_items.size();
+  ok(cudaMalloc(&p->d_qfac_items, sizeof(int2) * qfac_items.size()));
+  ok(cudaMemcpy(p->d_qfac_items, qfac_items.data(), sizeof(int2) * qfac_items.size(), cudaMemcpyHostToDevice));
+  for (int g = 0; g < 2; ++g) {
+    p->n_mv_items[g] = (int)mv_items[g].size();
+    ok(cudaMalloc(&p->d_mv_items[g], sizeof(int2) * mv_items[g].size()));
+    ok(cudaMemcpy(p->d_mv_items[g], mv_items[g].data(), sizeof(int2) * mv_items[g].size(), cudaMemcpyHostToDevice));
+  }
+  p->key = TuneKey(p->mixed, log2i(atoms), log2i(count));
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto f = g_tuned.find(p->key);
     if (f != g_tuned.end()) p->chosen = f->second;
   }
-  for (auto& m : p->best_ms_per_it) m = 1e30f;
+  for (auto& m : p->best_ms) m = 1e30f;
   if (st) {
-    if (msg) *msg = "batch: device allocation or copy failed";
+    if (msg) *msg = "batch: device allocation, copy or FFT plan failed";
     batch_plan_destroy(p);
     return st;
   }
@@ -699,21 +572,24 @@ int batch_plan_create(Ctx* const* cs, int count, BatchPlan** out, std::string* m
   return THP_OK;
 }
 
-// Enqueues the batched CG loop on the plan's stream after every system's
-// front (the callers' streams wait for ev_done).  Returns without waiting.
 int batch_plan_check(const BatchPlan& p, Ctx* const* cs) {
   for (int q = 0; q < p.count; ++q) {
     const Ctx& c = *cs[q];
-    if (p.sig[q] != std::make_tuple(c.n, (const void*)c.d_pp, (const void*)c.d_grid, (const void*)c.d_pk,
-                                    (const void*)c.d_cg))
+    if (p.sig[q] != std::make_tuple(c.n, (const void*)c.d_pp, (const void*)c.d_pk, (const void*)c.d_cg))
       return THP_E_STATE;
   }
   return THP_OK;
 }
 
+int batch_plan_candidate(const BatchPlan& p) { return p.chosen >= 0 ? p.chosen : p.tried; }
+
+bool batch_plan_profiling(const BatchPlan& p) { return p.profiling; }
+
+// Enqueues the batched CG loop on the plan's stream after every system's
+// front (the callers' streams wait for ev_done).  Returns without waiting.
 int batch_plan_loop(BatchPlan& p, Ctx* const* cs) {
   cudaSetDevice(p.device);
-  const int cand = p.chosen >= 0 ? p.chosen : p.tried;
+  const int cand = batch_plan_candidate(p);
   if (!p.exec[cand] && !p.profiling) {
     int st = build_graph(p, cand);
     if (st) return st;
@@ -722,10 +598,7 @@ int batch_plan_loop(BatchPlan& p, Ctx* const* cs) {
     cudaEventRecord(cs[q]->ev_fork, cs[q]->stream);
     cudaStreamWaitEvent(p.stream, cs[q]->ev_fork, 0);
   }
-  if (p.mixed)
-    kb_zero<float><<<2 * p.sms, 256, 0, p.stream>>>(p.d_sys, p.count, p.d_loops);
-  else
-    kb_zero<double><<<2 * p.sms, 256, 0, p.stream>>>(p.d_sys, p.count, p.d_loops);
+  kb_reset<<<1, 1, 0, p.stream>>>(p.d_loops);
   cudaEventRecord(p.ev_start, p.stream);
   if (p.profiling) {
     // eager iterations with a host check of the running systems after each
@@ -753,45 +626,63 @@ int batch_plan_loop(BatchPlan& p, Ctx* const* cs) {
   return cudaGetLastError() == cudaSuccess ? THP_OK : THP_E_CUDA;
 }
 
-// After the systems' streams have synchronised: the loop's time per CG
-// iteration (the loop runs as long as the slowest system) feeds the tuner.
-void batch_plan_finish(BatchPlan& p, int max_iterations) {
+// After the solve: its device time (fronts and loop) feeds the tuner, one
+// candidate per solve until all are measured.
+void batch_plan_finish(BatchPlan& p) {
   if (p.chosen >= 0 || p.running < 0 || p.profiling) return;
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, p.ev_start, p.ev_loop) != cudaSuccess) return;
-  const float per_it = ms / (float)std::max(1, max_iterations);
-  float& best = p.best_ms_per_it[p.running];
-  best = std::min(best, per_it);
+  float& best = p.best_ms[p.running];
+  best = std::min(best, ms);
   p.running = -1;
   if (++p.tried < kNumCandidates) return;
   int arg = 0;
   for (int q = 1; q < kNumCandidates; ++q)
-    if (p.best_ms_per_it[q] < p.best_ms_per_it[arg]) arg = q;
+    if (p.best_ms[q] < p.best_ms[arg]) arg = q;
   p.chosen = arg;
   for (int q = 0; q < kNumCandidates; ++q)
     if (q != arg && p.exec[q]) {
       cudaGraphExecDestroy(p.exec[q]);
       p.exec[q] = nullptr;
     }
+  for (auto it = p.solve_exec.begin(); it != p.solve_exec.end();) {
+    if (std::get<2>(it->first) != arg) {
+      cudaGraphExecDestroy(it->second);
+      it = p.solve_exec.erase(it);
+    } else {
+      ++it;
+    }
+  }
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tuned[p.key] = arg;
 }
 
-int batch_plan_tuning(const BatchPlan& p, int* atom_blocks, int* dft_blocks, int* lines, float* ms_per_iteration) {
+int batch_plan_tuning(const BatchPlan& p, int* blocks_per_sm, int* matvec_atoms, float* ms) {
   const int c = p.chosen;
   if (c < 0) return THP_E_STATE;
-  *atom_blocks = kCandidates[c].atom_blocks;
-  *dft_blocks = kCandidates[c].dft_blocks;
-  *lines = kCandidates[c].lines;
-  *ms_per_iteration = p.best_ms_per_it[c] < 1e29f ? p.best_ms_per_it[c] : -1.f;
+  *blocks_per_sm = kCandidates[c].blocks;
+  *matvec_atoms = 16 * kCandidates[c].gpw;
+  *ms = p.best_ms[c] < 1e29f ? p.best_ms[c] : -1.f;
   return THP_OK;
 }
 
-int batch_plan_candidates() { return kNumCandidates; }
-
-int batch_plan_candidate(const BatchPlan& p) { return p.chosen >= 0 ? p.chosen : p.tried; }
-
-bool batch_plan_profiling(const BatchPlan& p) { return p.profiling; }
+int batch_plan_profile(BatchPlan& p, int enable, double* ms, int* iterations) {
+  cudaSetDevice(p.device);
+  if (ms)
+    for (int k = 0; k < BatchPlan::kKernels; ++k) ms[k] = p.prof_ms[k];
+  if (iterations) *iterations = p.prof_iterations;
+  if (enable < 0) return THP_OK;  // read only
+  if (enable && !p.prof_ev[0]) {
+    for (auto& e : p.prof_ev)
+      if (cudaEventCreate(&e) != cudaSuccess) return THP_E_CUDA;
+    if (cudaMallocHost(&p.h_running, sizeof(int)) != cudaSuccess) return THP_E_CUDA;
+    if (cudaMalloc(&p.d_running, sizeof(int)) != cudaSuccess) return THP_E_CUDA;
+  }
+  p.profiling = enable != 0;
+  for (auto& m : p.prof_ms) m = 0.0;
+  p.prof_iterations = 0;
+  return THP_OK;
+}
 
 cudaGraphExec_t batch_plan_solve_exec(const BatchPlan& p, int guess, int carry, int cand) {
   auto f = p.solve_exec.find(std::make_tuple(guess, carry, cand));
@@ -799,8 +690,8 @@ cudaGraphExec_t batch_plan_solve_exec(const BatchPlan& p, int guess, int carry, 
 }
 
 // The whole batched solve as one graph: every system's front (child graphs,
-// in parallel), the zeroing of the A grids, the loop of candidate cand, and
-// kb_finish.  fronts[q] are the captured fronts (copied into the graph).
+// in parallel), the reset of the loop counter, the loop of candidate cand,
+// and kb_finish.  fronts[q] are the captured fronts (copied into the graph).
 int batch_plan_make_solve_exec(BatchPlan& p, const std::vector<cudaGraph_t>& fronts, int guess, int carry, int cand) {
   cudaSetDevice(p.device);
   cudaGraph_t g = nullptr;
@@ -809,17 +700,17 @@ int batch_plan_make_solve_exec(BatchPlan& p, const std::vector<cudaGraph_t>& fro
   std::vector<cudaGraphNode_t> fn(fronts.size());
   for (size_t q = 0; q < fronts.size() && !st; ++q)
     if (cudaGraphAddChildGraphNode(&fn[q], g, nullptr, 0, fronts[q]) != cudaSuccess) st = THP_E_CUDA;
-  cudaGraphNode_t zero = nullptr, loop = nullptr, fin = nullptr;
+  cudaGraphNode_t reset = nullptr, loop = nullptr, fin = nullptr;
   if (!st) {
     cudaKernelNodeParams kp = {};
-    void* args[] = {&p.d_sys, &p.count, &p.d_loops};
-    kp.func = p.mixed ? (void*)kb_zero<float> : (void*)kb_zero<double>;
-    kp.gridDim = dim3(2 * p.sms);
-    kp.blockDim = dim3(256);
+    void* args[] = {&p.d_loops};
+    kp.func = (void*)kb_reset;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(1);
     kp.kernelParams = args;
-    if (cudaGraphAddKernelNode(&zero, g, fn.data(), fn.size(), &kp) != cudaSuccess) st = THP_E_CUDA;
+    if (cudaGraphAddKernelNode(&reset, g, fn.data(), fn.size(), &kp) != cudaSuccess) st = THP_E_CUDA;
   }
-  if (!st) st = add_loop_node(p, g, &zero, 1, cand, &loop);
+  if (!st) st = add_loop_node(p, g, &reset, 1, cand, &loop);
   if (!st) {
     cudaKernelNodeParams kp = {};
     void* args[] = {&p.d_sys, &p.d_atom_items, &p.n_atom_items, &p.d_out};
@@ -841,39 +732,20 @@ int batch_plan_make_solve_exec(BatchPlan& p, const std::vector<cudaGraph_t>& fro
 }
 
 // Launches a whole-solve graph and waits for it; the records of every system
-// are then in out (mapped host memory, count entries).
+// are then in mapped host memory.
 int batch_plan_run_solve(BatchPlan& p, cudaGraphExec_t ex, const CgScalars** cg_out, const int** flags_out,
                          float* ms) {
   cudaSetDevice(p.device);
-  const int cand = batch_plan_candidate(p);
   cudaEventRecord(p.ev_start, p.stream);
   if (cudaGraphLaunch(ex, p.stream) != cudaSuccess) return THP_E_CUDA;
   cudaEventRecord(p.ev_loop, p.stream);
   if (cudaStreamSynchronize(p.stream) != cudaSuccess) return THP_E_CUDA;
-  p.running = cand;
+  p.running = batch_plan_candidate(p);
   cudaEventElapsedTime(ms, p.ev_start, p.ev_loop);
   for (int q = 0; q < p.count; ++q) {
     cg_out[q] = &p.h_out[q].cg;
     flags_out[q] = &p.h_out[q].flags;
   }
-  return THP_OK;
-}
-
-int batch_plan_profile(BatchPlan& p, int enable, double* ms, int* iterations) {
-  cudaSetDevice(p.device);
-  if (ms)
-    for (int k = 0; k < BatchPlan::kKernels; ++k) ms[k] = p.prof_ms[k];
-  if (iterations) *iterations = p.prof_iterations;
-  if (enable < 0) return THP_OK;  // read only
-  if (enable && !p.prof_ev[0]) {
-    for (auto& e : p.prof_ev)
-      if (cudaEventCreate(&e) != cudaSuccess) return THP_E_CUDA;
-    if (cudaMallocHost(&p.h_running, sizeof(int)) != cudaSuccess) return THP_E_CUDA;
-    if (cudaMalloc(&p.d_running, sizeof(int)) != cudaSuccess) return THP_E_CUDA;
-  }
-  p.profiling = enable != 0;
-  for (auto& m : p.prof_ms) m = 0.0;
-  p.prof_iterations = 0;
   return THP_OK;
 }
 

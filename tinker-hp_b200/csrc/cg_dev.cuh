@@ -99,7 +99,11 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double* __restrict_
 // finishes its own atom.
 // REC (mixed form): partners from the 32-byte records rec / mpz (the
 // position and the dipoles of x, PartnerRec) instead of posf and xf.
-template <bool MIXED, int GATHER, bool REC = false>
+// GPW: groups of four atoms per warp; a block of kBlock threads covers
+// 16 GPW atoms (GPW = 8: one atom per thread in the combine step; smaller
+// blocks for small systems, whose few blocks would otherwise each run a long
+// chain of group rows).
+template <bool MIXED, int GATHER, bool REC = false, int GPW = 8>
 __device__ __forceinline__ void cg_matvec_block(int blk, int nblk, const PairRows& pr, const Box& box,
                                                 const double4* __restrict__ pos, const float4* __restrict__ posf,
                                                 const double* __restrict__ dipf, const PmeGeom& pg,
@@ -110,14 +114,15 @@ __device__ __forceinline__ void cg_matvec_block(int blk, int nblk, const PairRow
                                                 double* __restrict__ h, double* __restrict__ res,
                                                 double* __restrict__ zr, double* __restrict__ pp, CgScalars* cg,
                                                 double* __restrict__ partials, float interior) {
-  static_assert(kBlock % 32 == 0, "whole warps");
-  __shared__ double srow[kBlock * 6];
+  static_assert(kBlock == 128 && GPW >= 1 && GPW <= 8, "four warps, up to eight groups each");
+  constexpr int AB = 16 * GPW;  // atoms per block
+  __shared__ double srow[AB * 6];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = (blk * kBlock + warp * 32) >> 2;  // first group of this warp
-  for (int gg = 0; gg < 8; ++gg) {
+  const int gw = blk * 4 * GPW + warp * GPW;  // first group of this warp
+  for (int gg = 0; gg < GPW; ++gg) {
     const int g = gw + gg;
     if (4 * g >= pr.n) break;  // the same for every lane of the warp
-    const int t = warp * 32 + gg * 4 + (lane >> 3), j = lane & 7;
+    const int t = warp * 4 * GPW + gg * 4 + (lane >> 3), j = lane & 7;
     if (MIXED) {
       float a32[6];
       const Image32 im{(float)box.l[0], (float)box.l[1], (float)box.l[2]};
@@ -133,9 +138,9 @@ __device__ __forceinline__ void cg_matvec_block(int blk, int nblk, const PairRow
     }
   }
   __syncthreads();
-  const int i = blk * kBlock + threadIdx.x;
+  const int i = blk * AB + threadIdx.x;
   double red[2] = {0.0, 0.0};
-  if (i < pr.n) {
+  if (threadIdx.x < AB && i < pr.n) {
     double acc[6];
 #pragma unroll
     for (int q = 0; q < 6; ++q) acc[q] = srow[threadIdx.x * 6 + q];

@@ -98,12 +98,11 @@ int batch_plan_create(Ctx* const* cs, int count, BatchPlan** out, std::string* m
 void batch_plan_destroy(BatchPlan* p);
 int batch_plan_check(const BatchPlan& p, Ctx* const* cs);  // THP_E_STATE if a context was re-targeted
 int batch_plan_loop(BatchPlan& p, Ctx* const* cs);   // after the fronts; the contexts' streams wait for it
-void batch_plan_finish(BatchPlan& p, int max_iterations);  // after the streams synchronised: tuner bookkeeping
-int batch_plan_tuning(const BatchPlan& p, int* atom_blocks, int* dft_blocks, int* lines, float* ms_per_iteration);
-int batch_plan_candidates();
+void batch_plan_finish(BatchPlan& p);  // after the solve synchronised: tuner bookkeeping
+int batch_plan_tuning(const BatchPlan& p, int* blocks_per_sm, int* matvec_atoms, float* ms);
 // enable 1: later solves run the loop eagerly with per-kernel events (0: back
-// to the graph; -1: read only); ms[8] receives the accumulated device time of
-// spread, DFT passes 0-4, matvec and update
+// to the graph; -1: read only); ms[6] receives the accumulated device time of
+// spread, forward FFTs, qfac, inverse FFTs, matvec and update
 int batch_plan_profile(BatchPlan& p, int enable, double* ms, int* iterations);
 int batch_plan_candidate(const BatchPlan& p);  // the launch shape the next solve uses
 bool batch_plan_profiling(const BatchPlan& p);

@@ -253,8 +253,40 @@ __device__ __forceinline__ int axis_cells(int c, int nc, int q) {
 #define THP_LIST_MINB 0
 #endif
 
-__global__ void __launch_bounds__(128, THP_LIST_MINB) k_build_list(int n, int npad, Box box, double mbuf2, int prefilter,
-                                                    float lo, float hi, int ncx,
+// systems below this many atoms build their list with one warp per atom
+#ifndef THP_LIST_WARP_ATOMS
+#define THP_LIST_WARP_ATOMS 20000
+#endif
+
+// The list decision for candidate k of atom i: the FP32 screen accepts below
+// lo and rejects above hi; between them (and for every candidate when the
+// screen is off) the exact FP64 r^2 of the reference decides.
+struct ListTest {
+  Box box;
+  double mbuf2;
+  int prefilter;
+  float lo, hi, bx, by, bz, hx, hy, hz;
+  __device__ __forceinline__ bool take(const double4& pi, const float4& fi, int k, const double4* __restrict__ pos,
+                                       const float4* __restrict__ posf) const {
+    if (prefilter) {
+      const float4 fk = posf[k];
+      float xr = fi.x - fk.x, yr = fi.y - fk.y, zr = fi.z - fk.z;
+      xr = fabsf(xr) > hx ? xr - copysignf(bx, xr) : xr;
+      yr = fabsf(yr) > hy ? yr - copysignf(by, yr) : yr;
+      zr = fabsf(zr) > hz ? zr - copysignf(bz, zr) : zr;
+      const float r2f = xr * xr + yr * yr + zr * zr;
+      if (r2f > hi) return false;
+      if (r2f < lo) return true;
+    }
+    const double4 pk = pos[k];
+    // midpointimage (domdecstuff.f:1773): pos = xi - xk, imaged
+    double xr = __dadd_rn(pi.x, -pk.x), yr = __dadd_rn(pi.y, -pk.y), zr = __dadd_rn(pi.z, -pk.z);
+    image3(box, xr, yr, zr);
+    return r2_exact(xr, yr, zr) <= mbuf2;
+  }
+};
+
+__global__ void __launch_bounds__(128, THP_LIST_MINB) k_build_list(int n, int npad, ListTest lt, int ncx,
                                                     int ncy, int ncz, const double4* __restrict__ pos,
                                                     const float4* __restrict__ posf, const int* __restrict__ scell,
                                                     const int* __restrict__ cell_start,
@@ -265,10 +297,6 @@ __global__ void __launch_bounds__(128, THP_LIST_MINB) k_build_list(int n, int np
   if (i >= n) return;
   const double4 pi = pos[i];
   const float4 fi = posf[i];
-  const float bx = (float)box.l[0], by = (float)box.l[1], bz = (float)box.l[2];
-  const float hx = 0.5f * bx, hy = 0.5f * by, hz = 0.5f * bz;
-  // FP32 screen: accept below lo, reject above hi, exact FP64 test between
-  // (lo/hi bracket mbuf2 by twice the FP32 error bound of r^2, set on the host)
   const int c = scell[i];
   const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
   int a0, a1, b0, b1;
@@ -289,27 +317,7 @@ __global__ void __launch_bounds__(128, THP_LIST_MINB) k_build_list(int n, int np
 #pragma unroll 4
         for (int k = k0; k < k1; ++k) {
           if (k == i) continue;
-          bool take;
-          if (prefilter) {
-            const float4 fk = posf[k];
-            float xr = fi.x - fk.x, yr = fi.y - fk.y, zr = fi.z - fk.z;
-            xr = fabsf(xr) > hx ? xr - copysignf(bx, xr) : xr;
-            yr = fabsf(yr) > hy ? yr - copysignf(by, yr) : yr;
-            zr = fabsf(zr) > hz ? zr - copysignf(bz, zr) : zr;
-            const float r2f = xr * xr + yr * yr + zr * zr;
-            if (r2f > hi) continue;
-            take = r2f < lo;
-          } else {
-            take = false;
-          }
-          if (!take) {
-            const double4 pk = pos[k];
-            // midpointimage (domdecstuff.f:1773): pos = xi - xk, imaged
-            double xr = __dadd_rn(pi.x, -pk.x), yr = __dadd_rn(pi.y, -pk.y), zr = __dadd_rn(pi.z, -pk.z);
-            image3(box, xr, yr, zr);
-            take = r2_exact(xr, yr, zr) <= mbuf2;
-          }
-          if (take) {
+          if (lt.take(pi, fi, k, pos, posf)) {
             if (cnt < maxnb) nb[(size_t)cnt * npad + i] = k;
             ++cnt;
           }
@@ -319,6 +327,59 @@ __global__ void __launch_bounds__(128, THP_LIST_MINB) k_build_list(int n, int np
   }
   nnb[i] = cnt;
   if (cnt > maxnb) atomicOr(flags, DEV_LIST_OVERFLOW);
+}
+
+// The same list with one warp per atom: the lanes test 32 consecutive
+// candidates of a cell-row range at a time and the accepted ones are written
+// in candidate order (ballot prefix), so the list is the thread-per-atom
+// kernel's entry for entry.  Small systems, where the +-2 cell window spans
+// most of the box and few atoms leave most of the GPU idle, use it.
+__global__ void __launch_bounds__(128) k_build_list_warp(int n, int npad, ListTest lt, int ncx, int ncy, int ncz,
+                                                        const double4* __restrict__ pos,
+                                                        const float4* __restrict__ posf,
+                                                        const int* __restrict__ scell,
+                                                        const int* __restrict__ cell_start,
+                                                        const int* __restrict__ cell_count, int maxnb,
+                                                        int* __restrict__ nnb, int* __restrict__ nb,
+                                                        int* __restrict__ flags) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= n) return;  // the same for the whole warp
+  const int lane = threadIdx.x & 31;
+  const double4 pi = pos[i];
+  const float4 fi = posf[i];
+  const int c = scell[i];
+  const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
+  int a0, a1, b0, b1;
+  row_ranges(cx, ncx, a0, a1, b0, b1);
+  const int my = min(ncy, 5), mz = min(ncz, 5);
+  int cnt = 0;
+  for (int qz = 0; qz < mz; ++qz) {
+    const int z = axis_cells(cz, ncz, qz);
+    for (int qy = 0; qy < my; ++qy) {
+      const int y = axis_cells(cy, ncy, qy);
+      const int rowbase = (z * ncy + y) * ncx;
+      for (int part = 0; part < 2; ++part) {
+        const int x0 = part ? b0 : a0, x1 = part ? b1 : a1;
+        if (x0 > x1) continue;
+        const int k0 = cell_start[rowbase + x0];
+        const int k1 = cell_start[rowbase + x1] + cell_count[rowbase + x1];
+        for (int kb = k0; kb < k1; kb += 32) {
+          const int k = kb + lane;
+          const bool t = k < k1 && k != i && lt.take(pi, fi, k, pos, posf);
+          const unsigned ball = __ballot_sync(0xffffffffu, t);
+          if (t) {
+            const int slot = cnt + __popc(ball & ((1u << lane) - 1u));
+            if (slot < maxnb) nb[(size_t)slot * npad + i] = k;
+          }
+          cnt += __popc(ball);
+        }
+      }
+    }
+  }
+  if (lane == 0) {
+    nnb[i] = cnt;
+    if (cnt > maxnb) atomicOr(flags, DEV_LIST_OVERFLOW);
+  }
 }
 
 // reference-format half list: row perm[i], partners with larger original index
@@ -485,10 +546,26 @@ int launch_build_list_on(Ctx& c, cudaStream_t s) {
   const double lmax = std::max(c.box.l[0], std::max(c.box.l[1], c.box.l[2]));
   const double dr = 1.7320508075688772 * 4.0 * lmax * 5.9604644775390625e-08;
   const double band = std::max(1e-5, 2.0 * (2.0 * rl * dr + dr * dr) / mbuf2);
-  const float lo = (float)(mbuf2 * (1.0 - band)), hi = (float)(mbuf2 * (1.0 + band));
-  k_build_list<<<(n + 127) / 128, 128, 0, s>>>(
-      n, c.npad, c.box, mbuf2, prefilter, lo, hi, c.nc[0], c.nc[1], c.nc[2], c.d_pos, c.d_posf, c.d_scell, c.d_cell_start,
-      c.d_cell_count, c.maxnb, c.d_nnb, c.d_nb, c.d_flags);
+  ListTest lt;
+  lt.box = c.box;
+  lt.mbuf2 = mbuf2;
+  lt.prefilter = prefilter;
+  lt.lo = (float)(mbuf2 * (1.0 - band));
+  lt.hi = (float)(mbuf2 * (1.0 + band));
+  lt.bx = (float)c.box.l[0];
+  lt.by = (float)c.box.l[1];
+  lt.bz = (float)c.box.l[2];
+  lt.hx = 0.5f * lt.bx;
+  lt.hy = 0.5f * lt.by;
+  lt.hz = 0.5f * lt.bz;
+  if (n < THP_LIST_WARP_ATOMS)
+    k_build_list_warp<<<(n + 3) / 4, 128, 0, s>>>(n, c.npad, lt, c.nc[0], c.nc[1], c.nc[2], c.d_pos, c.d_posf,
+                                                  c.d_scell, c.d_cell_start, c.d_cell_count, c.maxnb, c.d_nnb,
+                                                  c.d_nb, c.d_flags);
+  else
+    k_build_list<<<(n + 127) / 128, 128, 0, s>>>(n, c.npad, lt, c.nc[0], c.nc[1], c.nc[2], c.d_pos, c.d_posf,
+                                                 c.d_scell, c.d_cell_start, c.d_cell_count, c.maxnb, c.d_nnb,
+                                                 c.d_nb, c.d_flags);
   cudaMemcpyAsync(c.d_pos_built, c.d_pos, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s);
   return cuda_status(cudaGetLastError(), &c, "build list");
 }

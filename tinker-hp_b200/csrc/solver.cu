@@ -48,6 +48,11 @@
 #define THP_OVERLAP_MIN_ATOMS 20000
 #endif
 
+// systems below this many atoms run the fused matvec in blocks of 32 atoms
+#ifndef THP_MATVEC_SMALL_ATOMS
+#define THP_MATVEC_SMALL_ATOMS 8000
+#endif
+
 namespace thp {
 
 PairRows pair_rows(const Ctx& c);
@@ -63,7 +68,7 @@ using namespace cg;
 
 // h = T_real x + x/alpha + dipfield(x) - term x and the reductions of one
 // CG step (cg_matvec_block); dipfield comes from k_gather_dip.
-template <bool MIXED>
+template <bool MIXED, int GPW>
 __global__ void __launch_bounds__(kBlock) k_cg_matvec(PairRows pr, Box box, const double4* __restrict__ pos,
                                                       const float4* __restrict__ posf, const double* __restrict__ dipf,
                                                       const double* __restrict__ x, const float* __restrict__ xf,
@@ -73,8 +78,9 @@ __global__ void __launch_bounds__(kBlock) k_cg_matvec(PairRows pr, Box box, cons
                                                       double* __restrict__ pp, CgScalars* cg,
                                                       double* __restrict__ partials, float interior) {
   if (cg->stop) return;
-  cg_matvec_block<MIXED, 0>((int)blockIdx.x, (int)gridDim.x, pr, box, pos, posf, dipf, PmeGeom{}, nullptr, x, xf,
-                            nullptr, nullptr, pol, ef, term, init, h, res, zr, pp, cg, partials, interior);
+  cg_matvec_block<MIXED, 0, false, GPW>((int)blockIdx.x, (int)gridDim.x, pr, box, pos, posf, dipf, PmeGeom{},
+                                        nullptr, x, xf, nullptr, nullptr, pol, ef, term, init, h, res, zr, pp, cg,
+                                        partials, interior);
 }
 
 // pp = zr + beta pp (newinduce_pme2.f:553-559) of the overlapped FP64 rows.
@@ -371,21 +377,32 @@ static int matvec_overlapped(Ctx& c, const XV* x, int init) {
 }
 
 static int launch_matvec(Ctx& c, const double* x, int init) {
-  const int nb = (c.n + kBlock - 1) / kBlock;
   int st = launch_gather_dip(c, c.d_dip, init == 0);
   if (st) return st;
   prof_mark(c, c.stream);
   PairRows pr = pair_rows(c);
   const double a = c.cfg.aewald;
   const double term = (4.0 / 3.0) * a * a * a / kSqrtPi;
-  if (c.mixed)
-    k_cg_matvec<true><<<nb, kBlock, 0, c.stream>>>(pr, c.box, c.d_pos, c.d_posf, c.d_dip, x, c.d_vecf, c.d_pol,
-                                                   c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, c.d_cg,
-                                                   c.d_partials, row_interior(c));
-  else
-    k_cg_matvec<false><<<nb, kBlock, 0, c.stream>>>(pr, c.box, c.d_pos, c.d_posf, c.d_dip, x, c.d_vecf, c.d_pol,
-                                                    c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, c.d_cg,
-                                                    c.d_partials, -1.f);
+  const float interior = c.mixed ? row_interior(c) : -1.f;
+#define THP_MATVEC_ARGS                                                                                          \
+  pr, c.box, c.d_pos, c.d_posf, c.d_dip, x, c.d_vecf, c.d_pol, c.d_ef, term, init, c.d_h, c.d_res, c.d_zr, c.d_pp, \
+      c.d_cg, c.d_partials, interior
+  // small systems: two groups per warp (blocks of 32 atoms), so their few
+  // atoms spread over many blocks instead of long per-warp chains
+  if (c.n < THP_MATVEC_SMALL_ATOMS) {
+    const int nb = (c.n + 31) / 32;
+    if (c.mixed)
+      k_cg_matvec<true, 2><<<nb, kBlock, 0, c.stream>>>(THP_MATVEC_ARGS);
+    else
+      k_cg_matvec<false, 2><<<nb, kBlock, 0, c.stream>>>(THP_MATVEC_ARGS);
+  } else {
+    const int nb = (c.n + kBlock - 1) / kBlock;
+    if (c.mixed)
+      k_cg_matvec<true, 8><<<nb, kBlock, 0, c.stream>>>(THP_MATVEC_ARGS);
+    else
+      k_cg_matvec<false, 8><<<nb, kBlock, 0, c.stream>>>(THP_MATVEC_ARGS);
+  }
+#undef THP_MATVEC_ARGS
   prof_mark(c, c.stream);
   return cuda_status(cudaGetLastError(), &c, "cg matvec");
 }

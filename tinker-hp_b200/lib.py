@@ -127,8 +127,7 @@ def load():
         "thp_solve_batch": ([C.POINTER(vp), C.c_int, C.c_int, C.POINTER(ThpSolveInfo)], C.c_int),
         "thp_batch_create": ([C.POINTER(vp), C.c_int, C.POINTER(vp)], C.c_int),
         "thp_batch_solve": ([vp, C.c_int, C.POINTER(ThpSolveInfo)], C.c_int),
-        "thp_batch_tuning": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
-                              C.POINTER(C.c_double)], C.c_int),
+        "thp_batch_tuning": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
         "thp_batch_profile": ([vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)], C.c_int),
         "thp_batch_destroy": ([vp], C.c_int),
         "thp_solve_host": ([vp, _dp, _dp, _dp, _dp, _dp, _dp, C.POINTER(ThpSolveInfo)], C.c_int),
@@ -267,22 +266,21 @@ class Batch:
 
     def tuning(self):
         """The autotuner's kept launch shape, or None while it is still tuning."""
-        a, d, l, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
-        st = load().thp_batch_tuning(self.h, C.byref(a), C.byref(d), C.byref(l), C.byref(ms))
+        b, a, ms = C.c_int(), C.c_int(), C.c_double()
+        st = load().thp_batch_tuning(self.h, C.byref(b), C.byref(a), C.byref(ms))
         if st == THP_E_STATE:
             return None
         if st != THP_OK:
             raise ThpError(st, "thp_batch_tuning")
-        return {"atom_blocks_per_sm": a.value, "dft_blocks_per_sm": d.value, "dft_lines": l.value,
-                "ms_per_iteration": ms.value}
+        return {"blocks_per_sm": b.value, "matvec_atoms": a.value, "ms_per_solve": ms.value}
 
-    KERNELS = ("spread", "dft_x", "dft_y", "dft_z_qfac_z", "dft_y_inv", "dft_x_inv", "matvec", "update")
+    KERNELS = ("spread", "fft_forward", "qfac", "fft_inverse", "matvec", "update")
 
     def profile(self, enable=None):
         """enable True/False switches the eager, per-kernel-timed loop on/off
         (resetting the accumulators); returns the accumulated ms per kernel
         and the iterations timed so far."""
-        ms = (C.c_double * 8)()
+        ms = (C.c_double * len(self.KERNELS))()
         it = C.c_int()
         mode = -1 if enable is None else (1 if enable else 0)
         st = load().thp_batch_profile(self.h, mode, ms, C.byref(it))
