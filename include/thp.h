@@ -217,6 +217,13 @@ int thp_set_virial(thp_ctx* ctx, int on);
  * the derivative of the energy with respect to a homogeneous strain of the
  * box and the coordinates. */
 int thp_get_virial(thp_ctx* ctx, int form, double* vir);
+/* The virial of the last thp_empole1 call made with thp_set_virial on
+ * (empole1c: emrecip1's site terms and scalar sum, empole1.f:560-598,
+ * 741-761; emreal1c's pair and torque frame terms, :1428-1443, 1466-1497),
+ * form as thp_get_virial (1 adds the frame-atom virial of the reciprocal
+ * torques, which the reference leaves out); THP_E_STATE before such a call.
+ * empole1_ adds form 0 into the bound vir when one is bound. */
+int thp_get_empole_virial(thp_ctx* ctx, int form, double* vir);
 /* m2scale..m5scale [4] of the permanent-multipole pair terms (mplpot module;
  * defaults initprm.f:413-416: 0, 0, 1, 1; AMOEBA water03.prm:34-37: 0, 0,
  * 0.4, 0.8).  The 1-2..1-5 lists come from thp_set_connectivity. */

@@ -77,7 +77,7 @@ def lib():
         L.or_epolar.restype = C.c_double
         L.or_epolar.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         L.or_epolar1.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, _dp, _dp, _dp, _dp]
-        L.or_empole1.argtypes = [C.c_void_p, _ip, _ip, _ip, _dp, _dp]
+        L.or_empole1.argtypes = [C.c_void_p, _ip, _ip, _ip, _dp, _dp, _dp, _dp]
         L.or_ehal1.argtypes = [C.c_void_p, C.POINTER(OrVdw), _dp, _dp]
         L.or_rotpole.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _dp]
         L.or_grid_uind_sites.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp, _dp]
@@ -241,17 +241,25 @@ class Oracle:
             return ep.value, dep, vir, vfr
         return ep.value, dep
 
-    def empole1(self):
+    def empole1(self, virial=False):
         """Permanent-multipole energy and gradient, empole1c: returns
-        (em, dem [n,3], parts) with parts = (real, recip, self) kcal/mol."""
+        (em, dem [n,3], parts) with parts = (real, recip, self) kcal/mol; with
+        virial=True also the internal virial vir(3,3) (kcal/mol) as the
+        reference accumulates it and the frame-atom virial of the reciprocal
+        torques it leaves out (their sum is the strain derivative)."""
         dem = np.zeros((self.ws.n, 3))
         parts = np.zeros(4)
         ws = self.ws
+        vir = np.zeros((3, 3)) if virial else None
+        vfr = np.zeros((3, 3)) if virial else None
         st = lib().or_empole1(self.ctx, _p(np.ascontiguousarray(ws.zaxis, np.int32), _ip),
                               _p(np.ascontiguousarray(ws.xaxis, np.int32), _ip),
-                              _p(np.ascontiguousarray(ws.axt, np.int32), _ip), _p(dem), _p(parts))
+                              _p(np.ascontiguousarray(ws.axt, np.int32), _ip), _p(dem), _p(parts), _p(vir),
+                              _p(vfr))
         if st != 0:
             raise RuntimeError(f"oracle empole1 status {st}")
+        if virial:
+            return parts[0], dem, tuple(parts[1:]), vir, vfr
         return parts[0], dem, tuple(parts[1:])
 
     def ehal1(self, vdw=None):

@@ -2181,13 +2181,15 @@ int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxi
 // emrecip1 (:349-861), emreal1c (:873-1555, standard branch) over the half
 // list, the Ewald self energy (:134-160), torques distributed by torque
 // (torque.f:6-390).  Virial terms are not restated.
-int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, double* dem, double* parts) {
+int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, double* dem, double* parts,
+               double* vir_out, double* vir_frame) {
   const OrSystem& s = c->s;
   const int n = s.n, maxelst = c->maxelst;
   if (!c->have_list) return OR_E_LIST_OVERFLOW;
   std::fill(dem, dem + (size_t)n * 3, 0.0);
   const double f = kElectric;  // electric / dielec, dielec = 1
   double erecip = 0.0, ereal = 0.0, eself = 0.0;
+  Vir vir, vframe;
   // ---- emrecip1 ----------------------------------------------------------
   {
     // the multipole grid, convolved, and fphirec(20) (unscaled)
@@ -2200,7 +2202,7 @@ int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, dou
     cart_to_frac(c, ctf);
     frac_to_cart(c, ftc);
     const int nf[3] = {s.nfft1, s.nfft2, s.nfft3};
-    std::vector<double> demrec((size_t)n * 3, 0.0);
+    std::vector<double> demrec((size_t)n * 3, 0.0), fmp(vir_out ? (size_t)n * 10 : 0);
     for (int i = 0; i < n; ++i) {
       const double* rp = &s.rpole[(size_t)i * 13];
       const double cm[10] = {rp[0], rp[1], rp[2], rp[3], rp[4], rp[8], rp[12], 2.0 * rp[5], 2.0 * rp[6], 2.0 * rp[9]};
@@ -2247,10 +2249,35 @@ int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, dou
                cm[8] * cp[4] - cm[9] * cp[7];
       trq[2] = cm[2] * cp[1] - cm[1] * cp[2] + 2.0 * (cm[5] - cm[4]) * cp[7] + cm[7] * cp[4] + cm[9] * cp[8] -
                cm[7] * cp[5] - cm[8] * cp[9];
-      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], trq, demrec.data());  // torque_rec
+      double fz[3], fx[3];
+      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], trq, demrec.data(), fz, fx);  // torque_rec
+      if (vir_out) {
+        // the frame-atom virial of the reciprocal torque, which the reference
+        // does not add (torque_rec carries no virial)
+        frame_virial(s.x, s.y, s.z, i, zaxis[i], xaxis[i], fz, fx, vframe);
+        for (int q = 0; q < 10; ++q) fmp[(size_t)i * 10 + q] = fm[q];
+        // permanent multipole contribution to the internal virial (empole1.f:741-761)
+        vir.add(-cm[1] * cp[1] - 2.0 * cm[4] * cp[4] - cm[7] * cp[7] - cm[8] * cp[8],
+                -0.5 * (cm[2] * cp[1] + cm[1] * cp[2]) - (cm[4] + cm[5]) * cp[7] - 0.5 * cm[7] * (cp[4] + cp[5]) -
+                    0.5 * (cm[8] * cp[9] + cm[9] * cp[8]),
+                -0.5 * (cm[3] * cp[1] + cm[1] * cp[3]) - (cm[4] + cm[6]) * cp[8] - 0.5 * cm[8] * (cp[4] + cp[6]) -
+                    0.5 * (cm[7] * cp[9] + cm[9] * cp[7]),
+                -cm[2] * cp[2] - 2.0 * cm[5] * cp[5] - cm[7] * cp[7] - cm[9] * cp[9],
+                -0.5 * (cm[3] * cp[2] + cm[2] * cp[3]) - (cm[5] + cm[6]) * cp[9] - 0.5 * cm[9] * (cp[5] + cp[6]) -
+                    0.5 * (cm[7] * cp[8] + cm[8] * cp[7]),
+                -cm[3] * cp[3] - 2.0 * cm[6] * cp[6] - cm[8] * cp[8] - cm[9] * cp[9]);
+      }
     }
     erecip = 0.5 * erecip;
     for (size_t q = 0; q < (size_t)n * 3; ++q) dem[q] += demrec[q];
+    if (vir_out) {
+      // the scalar sum over the reciprocal lattice (empole1.f:560-598)
+      spread_sites(c, [&](int i, const double* t, const double* u, const double* v) {
+        return cd(mpole_stencil(&fmp[(size_t)i * 10], t, u, v), 0.0);
+      });
+      fft3d_impl(c->grid.data(), s.nfft1, s.nfft2, s.nfft3, -1, nthreads_of(&s));
+      kspace_virial(c, f, 1.0, [&](int, int, int, size_t idx) { return std::norm(c->grid[idx]); }, vir);
+    }
   }
   // ---- emreal1c (standard branch) ----------------------------------------
   {
@@ -2367,11 +2394,18 @@ int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, dou
         dem[k * 3 + 0] -= frcx;
         dem[k * 3 + 1] -= frcy;
         dem[k * 3 + 2] -= frcz;
+        // the virial of the pairwise Cartesian forces (empole1.f:1428-1442)
+        vir.add(-xr * frcx, -0.5 * (yr * frcx + xr * frcy), -0.5 * (zr * frcx + xr * frcz), -yr * frcy,
+                -0.5 * (zr * frcy + yr * frcz), -zr * frcz);
       }
       for (int b = 0; b < 4; ++b) for_conn(s, mslot[b], i, [&](int k) { mscale[k] = 1.0; });
     }
-    for (int i = 0; i < n; ++i)
-      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], &tem[(size_t)i * 3], dem);
+    for (int i = 0; i < n; ++i) {
+      double fz[3], fx[3];
+      torque_site(s.x, s.y, s.z, i, zaxis[i], xaxis[i], axt[i], &tem[(size_t)i * 3], dem, fz, fx);
+      // the virial of the torque's frame-atom forces (empole1.f:1466-1497)
+      frame_virial(s.x, s.y, s.z, i, zaxis[i], xaxis[i], fz, fx, vir);
+    }
   }
   // ---- self energy (empole1.f:134-160) -------------------------------------
   {
@@ -2393,6 +2427,8 @@ int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, dou
     parts[2] = erecip;
     parts[3] = eself;
   }
+  if (vir_out) vir.out(vir_out);
+  if (vir_frame) vframe.out(vir_frame);
   return OR_OK;
 }
 

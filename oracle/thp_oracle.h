@@ -103,8 +103,13 @@ int or_epolar1(OrCtx* c, const double* uind, const double* uinp, const int* zaxi
 
 /* empole1c (empole1.f:42-340): permanent-multipole energy and gradient dem
  * [n][3] (kcal/mol/A) at the current positions, TINFOIL boundary; needs the
- * list (or_mlistcell).  parts (may be NULL) [4]: total, real, recip, self. */
-int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, double* dem, double* parts);
+ * list (or_mlistcell).  parts (may be NULL) [4]: total, real, recip, self.
+ * vir (may be NULL): the internal virial vir(3,3) as the reference
+ * accumulates it (emrecip1's site terms and scalar sum, emreal1c's pair and
+ * torque frame terms); vir_frame (may be NULL): the frame-atom virial of the
+ * reciprocal torques, which the reference leaves out. */
+int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, double* dem, double* parts,
+               double* vir, double* vir_frame);
 
 /* van der Waals parameters of ehal1c (kvdw.f): per-atom class (0-based),
  * pair tables [nclass][nclass] of Rmin and epsilon (combined by the

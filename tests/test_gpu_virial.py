@@ -91,3 +91,33 @@ def test_virial_state_and_dropin(lib, case):
     assert L.thp_last_error() == 0
     _, _, vir_ref, _ = orc.epolar1(uind, uinp, virial=True)
     assert np.abs((vir - 2.0) - vir_ref).max() < 1e-9 * np.abs(vir_ref).max()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_empole_virial_matches_oracle(lib, case, precision):
+    # empole1c's virial (emrecip1's site terms and scalar sum, emreal1c's pair
+    # and torque frame terms) and the reciprocal torques' frame-atom terms,
+    # against the oracle's, which the strain derivative of its energy pins
+    # (tests/test_oracle.py::test_empole1_virial_matches_strain_derivative).
+    # Bounds relative to the sum of the energy parts' magnitudes (the virial
+    # is a small difference of real and reciprocal terms of that size):
+    # 1e-10 FP64, 1e-6 mixed (FP32 pair and grid arithmetic).
+    ws, orc = case
+    _, _, parts, vir_ref, vfr_ref = orc.empole1(virial=True)
+    scale = sum(abs(p) for p in parts)
+    prec = lib.FP64 if precision == "fp64" else lib.MIXED
+    ctx = lib.Context(ws, precision=prec)
+    ctx.set_virial(True)
+    _, dem = ctx.empole1()
+    v0, v1 = ctx.empole_virial(0), ctx.empole_virial(1)
+    e0 = np.abs(v0 - vir_ref).max() / scale
+    e1 = np.abs(v1 - (vir_ref + vfr_ref)).max() / scale
+    print(f"\nempole virial {precision}: {e0:.2e} / {e1:.2e} of the parts ({scale:.3e} kcal/mol)")
+    tol = 1e-10 if prec == lib.FP64 else 1e-6
+    assert e0 < tol and e1 < tol, (v0, vir_ref, v1, vir_ref + vfr_ref)
+    np.testing.assert_allclose(v0, v0.T, rtol=0, atol=0)
+    # the energy gradient is the same with the virial off (FP64: to rounding;
+    # mixed: the two kernel variants round their FP32 pair terms differently)
+    ctx.set_virial(False)
+    _, dem2 = ctx.empole1()
+    assert np.abs(dem2 - dem).max() < (1e-12 if prec == lib.FP64 else 1e-6) * np.abs(dem).max()

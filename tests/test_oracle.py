@@ -310,10 +310,10 @@ def test_two_waters_reach_the_isolated_limit(thp):
 
 # ---- permanent-multipole energy and gradient (empole1c) --------------------
 
-def _empole(ws):
+def _empole(ws, virial=False):
     orc = O.Oracle(ws)
     assert orc.mlistcell(maxelst=4000)[0] == 0
-    return orc.empole1()
+    return orc.empole1(virial=virial)
 
 
 def test_empole1_gradient_matches_finite_differences(box216):
@@ -331,6 +331,36 @@ def test_empole1_gradient_matches_finite_differences(box216):
                 e.append(_empole(box216.with_positions(p))[0])
             fd = (e[0] - e[1]) / (2 * h)
             assert abs(fd - dem[atom, d]) < 1e-6 * np.abs(dem).max() + 1e-6, (atom, d, fd, dem[atom, d])
+
+
+def test_empole1_virial_matches_strain_derivative(thp):
+    # Scaling the coordinates and the box edge along x, y or z by (1 + eps),
+    # the frames (and so the multipoles) following the atoms: the central
+    # difference of the energy is vir(a,a) + the frame-atom virial of the
+    # reciprocal torques, which the reference's virial leaves out.  The
+    # real-space energy jumps where a pair crosses the cutoff (a charge pair
+    # there is worth ~1e-7 kcal/mol), so the strain is kept small (1e-7, a
+    # few pairs within reach of the cutoff) and the difference is bounded
+    # against the size of the real and reciprocal parts, which cancel to a
+    # total a hundred times smaller.
+    box = thp.water.make_water_box(216, cfg=0)
+    _, _, _, vir, vfr = _empole(box, virial=True)
+    np.testing.assert_allclose(vir, vir.T, rtol=0, atol=1e-12 * np.abs(vir).max())
+    eps = 1e-7
+    pos0 = box.positions()
+    for a in range(3):
+        e, parts = [], []
+        for sgn in (1, -1):
+            p = pos0.copy()
+            p[:, a] *= 1.0 + sgn * eps
+            edge = list(box.box)
+            edge[a] *= 1.0 + sgn * eps
+            em, _, pt = _empole(dataclasses.replace(box.with_positions(p), box=tuple(edge)))
+            e.append(em)
+            parts.append(pt)
+        fd = (e[0] - e[1]) / (2 * eps)
+        scale = sum(abs(parts[0][q] - parts[1][q]) / (2 * eps) for q in (0, 1))
+        assert abs(fd - (vir[a, a] + vfr[a, a])) < 5e-6 * scale, (a, fd, vir[a, a], vfr[a, a], scale)
 
 
 def test_empole_recip_converges_to_classical_ewald(box216):

@@ -1017,7 +1017,9 @@ int thp_empole1(thp_ctx* h, double* em, double* dem) {
   if ((st = ensure_list(h, false))) return st;
   if (!c.d_grad && (st = cuda_status(cudaMalloc((void**)&c.d_grad, sizeof(double) * 3 * c.n), &c, "alloc gradient")))
     return st;
+  c.have_mvirial = false;
   if ((st = launch_empole(c, c.d_grad))) return st;
+  c.have_mvirial = c.want_virial;  // totals land in h_mvir with the copies below
   double e = 0.0;
   cudaMemcpyAsync(&e, c.d_em, sizeof(double), cudaMemcpyDeviceToHost, c.stream);
   if (dem) cudaMemcpyAsync(dem, c.d_grad, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost, c.stream);
@@ -1608,6 +1610,17 @@ int thp_get_gradient_device(thp_ctx* h, double* d_dep) {
   return st;
 }
 
+int thp_get_empole_virial(thp_ctx* h, int form, double* vir) {
+  if (!h || !vir || form < 0 || form > 1) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (!c.have_mvirial) return THP_E_STATE;
+  double v[6];
+  for (int q = 0; q < 6; ++q) v[q] = c.h_mvir[q] + (form == 1 ? c.h_mvir[6 + q] : 0.0);
+  const double t[9] = {v[0], v[1], v[2], v[1], v[3], v[4], v[2], v[4], v[5]};
+  std::memcpy(vir, t, sizeof(t));
+  return THP_OK;
+}
+
 int thp_set_virial(thp_ctx* h, int on) {
   if (!h) return THP_E_INVALID;
   h->c.want_virial = on != 0;
@@ -2050,8 +2063,14 @@ void empole1_(void) {
   }
   int st = sync_bound_inputs(h);
   double em = 0.0;
+  h->c.want_virial = h->c.bvir != nullptr;
   if (!st) st = thp_empole1(h, &em, h->c.bdem);
   if (!st && h->c.bem) *h->c.bem = em;
+  if (!st && h->c.bvir) {  // empole1c adds into vir (empole1.f:820-828, 1435-1443)
+    double v[9];
+    st = thp_get_empole_virial(h, 0, v);
+    for (int q = 0; !st && q < 9; ++q) h->c.bvir[q] += v[q];
+  }
   g_last_error = st;
 }
 

@@ -14,8 +14,8 @@
 //   2. the convolution: one batched cuFFT transform per grid-size class (the
 //      classes' grids lie end to end, and the classes run as parallel
 //      branches), kb_qfac over every grid, the batched inverse transforms;
-//   3. kb_matvec: real-space rows, the dipole field gathered from the grid
-//      (fphi_uind_site), h, pp.h and alpha;
+//   3. kb_row: real-space rows (tmatxb_pme); kb_combine: the dipole field
+//      gathered from the grid (fphi_uind_site), h, pp.h and alpha;
 //   4. kb_update: mu, residual, preconditioned residual, beta and the stop
 //      test;
 //   5. kb_cond: keeps the conditional WHILE node looping while a system runs.
@@ -46,7 +46,7 @@ using namespace cg;
 // (grid, its PME grid in the batched transforms' layout, belongs to the plan).
 struct BatchSys {
   int n, nblk;       // atoms; blocks of kBlock atoms
-  int nblk_mv[2];    // blocks of 16 and 32 atoms (the matvec's items)
+  int nblk_mv[2];    // blocks of 16 and 32 atoms (the rows' items)
   int ngrid;
   int politer;
   double poleps, term;
@@ -129,18 +129,29 @@ __global__ void __launch_bounds__(256) kb_qfac(const BatchSys* __restrict__ sys,
   }
 }
 
-// real-space rows + dipole field gathered from the convolved grid + h, pp.h,
-// alpha; items of 16 GPW atoms
+// real-space rows T_real pp into h (FP64); items of 16 GPW atoms
 template <bool MIXED, int GPW>
-__global__ void __launch_bounds__(kBlock) kb_matvec(const BatchSys* __restrict__ sys, const int2* __restrict__ items,
-                                                    int nitems) {
+__global__ void __launch_bounds__(kBlock) kb_row(const BatchSys* __restrict__ sys, const int2* __restrict__ items,
+                                                 int nitems) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = items[it];
     const BatchSys& s = sys[w.x];
     if (s.cg->stop) continue;
-    cg_matvec_block<MIXED, MIXED ? 1 : 2, MIXED, GPW>(w.y, s.nblk_mv[GPW - 1], s.pr, s.box, s.pos, s.posf, nullptr,
-                                                      s.g, s.grid, s.pp, nullptr, s.rec, s.mpz, s.pol, s.ef, s.term,
-                                                      0, s.h, s.res, s.zr, s.pp, s.cg, s.partials, s.interior);
+    row_block<MIXED, MIXED, GPW>(w.y, s.pr, s.box, s.pos, s.posf, s.pp, nullptr, s.rec, s.mpz, s.interior, s.h);
+  }
+}
+
+// h = T_real pp + pp/alpha + dipfield(pp) - self term, the dipole field
+// gathered from the convolved grid (fphi_uind_site), pp.h and alpha
+template <bool MIXED>
+__global__ void __launch_bounds__(kBlock) kb_combine(const BatchSys* __restrict__ sys, const int2* __restrict__ items,
+                                                     int nitems) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = items[it];
+    const BatchSys& s = sys[w.x];
+    if (s.cg->stop) continue;
+    cg_combine_block<MIXED ? 1 : 2, double, double>(w.y, s.nblk, s.n, nullptr, s.g, s.pos, s.grid, s.pp, s.pol,
+                                                    s.ef, s.term, 0, s.h, s.res, s.zr, s.pp, s.cg, s.partials);
   }
 }
 
@@ -218,7 +229,8 @@ int sm_count(int device) {
 }  // namespace
 
 // Autotuner candidates: resident blocks per SM of the batched kernels and
-// groups of four atoms per warp in the matvec (tiles of 16 GPW atoms).
+// groups of four atoms per warp in the real-space rows (tiles of 16 GPW
+// atoms).
 struct BatchTune {
   int blocks, gpw;
 };
@@ -250,7 +262,7 @@ struct BatchPlan {
   BatchSys* d_sys = nullptr;
   int2* d_atom_items = nullptr;  // (system, block of kBlock atoms)
   int n_atom_items = 0;
-  int2* d_mv_items[2] = {};      // (system, block of 16 / 32 atoms)
+  int2* d_mv_items[2] = {};      // (system, block of 16 / 32 atoms): the rows' items
   int n_mv_items[2] = {};
   int2* d_qfac_items = nullptr;  // (system, chunk of grid points)
   int n_qfac_items = 0;
@@ -330,17 +342,19 @@ static int enqueue_body(BatchPlan& p, const BatchTune& t, cudaGraphConditionalHa
   if (enqueue_ffts(p, CUFFT_INVERSE)) return THP_E_CUDA;
   mark();
   const int g = t.gpw - 1;
-  const int mb = std::max(1, std::min(p.n_mv_items[g], t.blocks * p.sms));
+  const int mb = std::max(1, std::min(p.n_mv_items[g], 2 * t.blocks * p.sms));
   if (p.mixed) {
     if (t.gpw == 1)
-      kb_matvec<true, 1><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
+      kb_row<true, 1><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
     else
-      kb_matvec<true, 2><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
+      kb_row<true, 2><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
+    kb_combine<true><<<ab, kBlock, 0, p.stream>>>(p.d_sys, p.d_atom_items, p.n_atom_items);
   } else {
     if (t.gpw == 1)
-      kb_matvec<false, 1><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
+      kb_row<false, 1><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
     else
-      kb_matvec<false, 2><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
+      kb_row<false, 2><<<mb, kBlock, 0, p.stream>>>(p.d_sys, p.d_mv_items[g], p.n_mv_items[g]);
+    kb_combine<false><<<ab, kBlock, 0, p.stream>>>(p.d_sys, p.d_atom_items, p.n_atom_items);
   }
   mark();
   kb_update<<<ab, kBlock, 0, p.stream>>>(p.d_sys, p.d_atom_items, p.n_atom_items);

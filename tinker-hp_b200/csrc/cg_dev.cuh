@@ -199,6 +199,107 @@ __device__ __forceinline__ void cg_matvec_block(int blk, int nblk, const PairRow
 }
 
 
+// h = hreal + x/alpha + dipfield(x) - term x, then the reductions of
+// k_cg_matvec (init: residual, zr, pp and ggold; iter: gg and alpha).
+// GATHER 0 reads dipfield from dipf; 1 / 2 gather it here from the
+// convolved FP32 / FP64 grid (the work of k_gather_dip, without the round
+// trip of dipfield through memory).
+template <int GATHER, typename XV, typename V>
+__device__ __forceinline__ void cg_combine_block(int blk, int nblk, int n, const double* __restrict__ dipf,
+                                                 const PmeGeom& g, const double4* __restrict__ pos,
+                                                 const void* __restrict__ grid, const XV* __restrict__ x,
+                                                 const double* __restrict__ pol, const double* __restrict__ ef,
+                                                 double term, int init, V* __restrict__ h, V* __restrict__ res,
+                                                 V* __restrict__ zr, V* __restrict__ pp, CgScalars* cg,
+                                                 double* __restrict__ partials) {
+  const int i = blk * kBlock + threadIdx.x;
+  double red[2] = {0.0, 0.0};
+  if (i < n) {
+    double acc[6], dip[6], xi[6];
+    if constexpr (GATHER == 1)
+      gather_dip<float>(g, pos[i], reinterpret_cast<const cufftComplex*>(grid), dip);
+    else if constexpr (GATHER == 2)
+      gather_dip<double>(g, pos[i], reinterpret_cast<const cufftDoubleComplex*>(grid), dip);
+    else
+      load6(dipf + (size_t)i * 6, dip);
+    load6(h + (size_t)i * 6, acc);
+    load6(x + (size_t)i * 6, xi);
+    const double p = pol[i];
+    const double ip = (p == 0.0) ? 1.0 / kTinyPol : 1.0 / p;
+    double hv[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) hv[q] = ((acc[q] + xi[q] * ip) + dip[q]) - term * xi[q];
+    store6(h + (size_t)i * 6, hv);
+    if (init) {
+      double e6[6], r6[6], z6[6];
+      load6(ef + (size_t)i * 6, e6);
+      const double dg = diag_of(p);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        r6[q] = e6[q] - hv[q];
+        z6[q] = dg * r6[q];
+      }
+      store6(res + (size_t)i * 6, r6);
+      store6(zr + (size_t)i * 6, z6);
+      store6(pp + (size_t)i * 6, z6);
+      red[0] = r6[0] * z6[0] + r6[1] * z6[1] + r6[2] * z6[2];
+      red[1] = r6[3] * z6[3] + r6[4] * z6[4] + r6[5] * z6[5];
+    } else {
+      red[0] = xi[0] * hv[0] + xi[1] * hv[1] + xi[2] * hv[2];
+      red[1] = xi[3] * hv[3] + xi[4] * hv[4] + xi[5] * hv[5];
+    }
+  }
+  double tot[2];
+  if (grid_reduce_of<2>(red, partials, &cg->counter[0], blk, nblk, tot) && threadIdx.x == 0) {
+    if (init) {
+      cg->ggold[0] = tot[0];
+      cg->ggold[1] = tot[1];
+      cg->beta[0] = 0.0;
+      cg->beta[1] = 0.0;
+    } else {
+      cg->gg[0] = tot[0];
+      cg->gg[1] = tot[1];
+      if (tot[0] == 0.0 || tot[1] == 0.0) {
+        cg->stop = 1;  // newinduce_pme2.f:505 returns on gg == 0
+      } else {
+        cg->alpha[0] = cg->ggold[0] / tot[0];
+        cg->alpha[1] = cg->ggold[1] / tot[1];
+      }
+    }
+  }
+}
+
+// The real-space rows T_real x of the atoms of block blk (16 GPW atoms:
+// four warps of GPW groups of four), hreal[i][6] in FP64; lane j < 6 of an
+// atom writes component j.  Partners as in cg_matvec_block.
+template <bool MIXED, bool REC, int GPW>
+__device__ __forceinline__ void row_block(int blk, const PairRows& pr, const Box& box,
+                                          const double4* __restrict__ pos, const float4* __restrict__ posf,
+                                          const double* __restrict__ x, const float* __restrict__ xf,
+                                          const float* __restrict__ rec, const float* __restrict__ mpz,
+                                          float interior, double* __restrict__ hreal) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blk * 4 * GPW + warp * GPW;  // first group of this warp
+  for (int gg = 0; gg < GPW; ++gg) {
+    const int g = gw + gg;
+    if (4 * g >= pr.n) break;  // the same for every lane of the warp
+    const int i = 4 * g + (lane >> 3), j = lane & 7;
+    if (MIXED) {
+      float a32[6];
+      const Image32 im{(float)box.l[0], (float)box.l[1], (float)box.l[2]};
+      if constexpr (REC)
+        group_row<float, THP_GROW_U32, false>(pr, PartnerRec{rec, mpz}, im, g, lane, a32, interior);
+      else
+        group_row<float, THP_GROW_U32, false>(pr, Partner32{posf, xf}, im, g, lane, a32, interior);
+      if (j < 6 && i < pr.n) hreal[(size_t)i * 6 + j] = (double)pick6(a32, j);
+    } else {
+      double a64[6];
+      group_row<double, THP_GROW_U64, false>(pr, Partner64{pos, x}, Image64{box}, g, lane, a64, -1.0);
+      if (j < 6 && i < pr.n) hreal[(size_t)i * 6 + j] = pick6(a64, j);
+    }
+  }
+}
+
 // newinduce_pme2.f:512-572
 template <typename V>
 __device__ __forceinline__ void cg_update_block(int blk, int nblk, int n, const double* __restrict__ pol,

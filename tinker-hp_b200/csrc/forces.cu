@@ -710,6 +710,37 @@ int launch_gradient_out(Ctx& c, const unsigned long long* dep, double* d_out) {
   return cuda_status(cudaGetLastError(), &c, "gradient out");
 }
 
+// Partial-sum rows of one gradient call's virial: 2 kspace_virial_blocks()
+// rows of 6 (k-space sums), nb rows of 6 and nb rows of 12 (per-block site
+// and pair terms), then 12 totals; grown on demand.
+int virial_scratch(Ctx& c, int nb, double** kpart, double** rpart, double** epart) {
+  const int nk = 2 * kspace_virial_blocks();
+  const size_t rows = (size_t)nk * 6 + (size_t)nb * 6 + (size_t)nb * 12 + 12;
+  if (c.virp_cap < rows) {
+    cudaFree(c.d_virp);
+    c.d_virp = nullptr;
+    c.virp_cap = 0;
+    int st = cuda_status(cudaMalloc((void**)&c.d_virp, sizeof(double) * rows), &c, "alloc virial");
+    if (st) return st;
+    c.virp_cap = rows;
+  }
+  *kpart = c.d_virp;
+  *rpart = *kpart + (size_t)nk * 6;
+  *epart = *rpart + (size_t)nb * 6;
+  return THP_OK;
+}
+
+// The 12 totals of the partial sums (in a fixed order; nk k-space rows)
+// copied to h_out when the stream reaches them.
+int virial_total(Ctx& c, int nk, int nb, const double* kpart, const double* rpart, const double* epart,
+                 double* h_out) {
+  double* tot = const_cast<double*>(epart) + (size_t)nb * 12;
+  k_virial_sum<<<1, 256, 0, c.stream>>>(nk, kpart, nb, rpart, nb, epart, tot);
+  const int st = cuda_status(cudaGetLastError(), &c, "virial sum");
+  if (!st) cudaMemcpyAsync(h_out, tot, sizeof(double) * 12, cudaMemcpyDeviceToHost, c.stream);
+  return st;
+}
+
 // Gradient of the polarization energy for the converged dipoles in d_mu
 // (sorted); writes dE/dx [n][3] in ORIGINAL atom order into d_out.
 int launch_forces(Ctx& c, double* d_out) {
@@ -724,20 +755,7 @@ int launch_forces(Ctx& c, double* d_out) {
   const bool vir = c.want_virial;
   const int nk = 2 * kspace_virial_blocks();
   double *kpart = nullptr, *rpart = nullptr, *epart = nullptr;
-  if (vir) {
-    // partial sums: nk rows of 6, nb rows of 6, nb rows of 12, then the 12 totals
-    const size_t rows = (size_t)nk * 6 + (size_t)nb * 6 + (size_t)nb * 12 + 12;
-    if (c.virp_cap < rows) {
-      cudaFree(c.d_virp);
-      c.d_virp = nullptr;
-      c.virp_cap = 0;
-      if ((st = cuda_status(cudaMalloc((void**)&c.d_virp, sizeof(double) * rows), &c, "alloc virial"))) return st;
-      c.virp_cap = rows;
-    }
-    kpart = c.d_virp;
-    rpart = kpart + (size_t)nk * 6;
-    epart = rpart + (size_t)nb * 6;
-  }
+  if (vir && (st = virial_scratch(c, nb, &kpart, &rpart, &epart))) return st;
   unsigned long long* dep = c.d_depfix;
   if ((st = cuda_status(cudaMemsetAsync(dep, 0, sizeof(unsigned long long) * 3 * n, c.stream), &c, "zero gradient")))
     return st;
@@ -745,7 +763,7 @@ int launch_forces(Ctx& c, double* d_out) {
   PmeGeom g = pme_geom(c);
   // permanent-multipole potential, 20 derivatives per site (and the
   // permanent-only k-space virial, subtracted)
-  if ((st = vir ? launch_mpole_grid_virial(c, kpart) : launch_mpole_grid(c))) return st;
+  if ((st = vir ? launch_mpole_grid_virial(c, kpart, -1.0) : launch_mpole_grid(c))) return st;
   if ((st = launch_fphi_mpole20(c))) return st;
   // dipole grid of uind (Re) / uinp (Im), convolved
   if ((st = launch_pme_dipole(c, c.d_mu, nullptr, 0))) return st;
@@ -804,12 +822,7 @@ int launch_forces(Ctx& c, double* d_out) {
   }
 #undef THP_FORCE_ARGS
   if ((st = cuda_status(cudaGetLastError(), &c, "force real"))) return st;
-  if (vir) {
-    double* tot = epart + (size_t)nb * 12;
-    k_virial_sum<<<1, 256, 0, c.stream>>>(nk, kpart, nb, rpart, nb, epart, tot);
-    if ((st = cuda_status(cudaGetLastError(), &c, "virial sum"))) return st;
-    cudaMemcpyAsync(c.h_vir, tot, sizeof(double) * 12, cudaMemcpyDeviceToHost, c.stream);
-  }
+  if (vir && (st = virial_total(c, nk, nb, kpart, rpart, epart, c.h_vir))) return st;
   k_dep_out<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, dep, d_out);
   return cuda_status(cudaGetLastError(), &c, "force out");
 }

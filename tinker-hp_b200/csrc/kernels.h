@@ -27,7 +27,8 @@ void pme_free(Ctx& c);
 int launch_efld0_recip(Ctx& c);         // d_cphi and E0 completion
 int launch_efld0_recip_ex(Ctx& c, double* cphi10, bool with_e0);
 int launch_mpole_grid(Ctx& c);          // permanent-multipole grid, convolved (grid holds the potential)
-int launch_mpole_grid_virial(Ctx& c, double* d_part);  // the same, with the permanent-only k-space virial
+// the same, with the permanent-only k-space virial (times sign) into d_part
+int launch_mpole_grid_virial(Ctx& c, double* d_part, double sign);
 int launch_pair_grid_virial(Ctx& c, double* d_part);   // (rpole+uinp) x (rpole+uind) k-space virial
 int kspace_virial_blocks();
 int launch_gather_mpole(Ctx& c, double* cphi10, bool with_e0);  // cphi from the convolved grid, E0 completion
@@ -41,6 +42,11 @@ int launch_gather_dip(Ctx& c, double* d_out, bool check_stop);
 
 // forces.cu
 int launch_forces(Ctx& c, double* d_out);  // dE/dx [n][3], original order, for the dipoles in d_mu
+// virial partial sums of a gradient call (k-space, per-block rows of 6 and
+// 12) and their 12 totals copied to h_out
+int virial_scratch(Ctx& c, int nb, double** kpart, double** rpart, double** epart);
+int virial_total(Ctx& c, int nk, int nb, const double* kpart, const double* rpart, const double* epart,
+                 double* h_out);
 int launch_fphi_mpole20(Ctx& c);          // fphirec [n][20] of the convolved multipole grid
 int launch_frames_sorted(Ctx& c);         // frame atoms in sorted numbering (d_frs)
 int launch_gradient_out(Ctx& c, const unsigned long long* dep, double* d_out);  // fixed point -> original order

@@ -47,9 +47,11 @@ struct MScale {
 // emreal1c pair terms (standard branch) seen from site i: adds half the pair
 // energy, the force on i and the torque on i.  m = (q, d, Qxx, Qxy, Qxz,
 // Qyy, Qyz, Qzz) of each site; scalek = 1 - mscale.
+// v6 (optional): adds half the pair's virial (empole1.f:1428-1442; the
+// other half comes from the k end) as xx xy xz yy yz zz.
 template <typename U>
 __device__ __forceinline__ void mpole_pair(U xr, U yr, U zr, U r2, U scalek, const U* mi, const U* mk, const EwM& ew,
-                                           double& e_acc, double g[3], double t[3]) {
+                                           double& e_acc, double g[3], double t[3], double* v6 = nullptr) {
   const U ci = mi[0], dix = mi[1], diy = mi[2], diz = mi[3];
   const U qixx = mi[4], qixy = mi[5], qixz = mi[6], qiyy = mi[7], qiyz = mi[8], qizz = mi[9];
   const U ck = mk[0], dkx = mk[1], dky = mk[2], dkz = mk[3];
@@ -128,9 +130,24 @@ __device__ __forceinline__ void mpole_pair(U xr, U yr, U zr, U r2, U scalek, con
   const U dkqix = dkx * qixx + dky * qixy + dkz * qixz;
   const U dkqiy = dkx * qixy + dky * qiyy + dkz * qiyz;
   const U dkqiz = dkx * qixz + dky * qiyz + dkz * qizz;
-  g[0] += (double)(de * xr + t1 * dix + t2 * dkx + t3 * (diqkx - dkqix) + t4 * qix + t5 * qkx + t6 * (qixk + qkxi));
-  g[1] += (double)(de * yr + t1 * diy + t2 * dky + t3 * (diqky - dkqiy) + t4 * qiy + t5 * qky + t6 * (qiyk + qkyi));
-  g[2] += (double)(de * zr + t1 * diz + t2 * dkz + t3 * (diqkz - dkqiz) + t4 * qiz + t5 * qkz + t6 * (qizk + qkzi));
+  const double fx = (double)(de * xr + t1 * dix + t2 * dkx + t3 * (diqkx - dkqix) + t4 * qix + t5 * qkx +
+                             t6 * (qixk + qkxi));
+  const double fy = (double)(de * yr + t1 * diy + t2 * dky + t3 * (diqky - dkqiy) + t4 * qiy + t5 * qky +
+                             t6 * (qiyk + qkyi));
+  const double fz = (double)(de * zr + t1 * diz + t2 * dkz + t3 * (diqkz - dkqiz) + t4 * qiz + t5 * qkz +
+                             t6 * (qizk + qkzi));
+  g[0] += fx;
+  g[1] += fy;
+  g[2] += fz;
+  if (v6) {
+    const double x = xr, y = yr, z = zr;
+    v6[0] -= 0.5 * x * fx;
+    v6[1] -= 0.25 * (y * fx + x * fy);
+    v6[2] -= 0.25 * (z * fx + x * fz);
+    v6[3] -= 0.5 * y * fy;
+    v6[4] -= 0.25 * (z * fy + y * fz);
+    v6[5] -= 0.5 * z * fz;
+  }
   // torque on site i (emreal1c's ttmi)
   const U dirx = diy * zr - diz * yr, diry = diz * xr - dix * zr, dirz = dix * yr - diy * xr;
   const U dikx = diy * dkz - diz * dky, diky = diz * dkx - dix * dkz, dikz = dix * dky - diy * dkx;
@@ -156,16 +173,19 @@ __device__ __forceinline__ void mpole_pair(U xr, U yr, U zr, U r2, U scalek, con
 // and tests the cutoff in FP64; the mixed form reads one 64-B record per
 // partner (wrapped position and multipoles, FP32) and images and tests in
 // FP32, as its direct-field pass does.
-template <bool MIXED>
+// VIR: each block also writes the sum of its sites' pair virial halves and
+// the frame-atom virial of their pair torques (6 values) to vpart.
+template <bool MIXED, bool VIR>
 __global__ void __launch_bounds__(kBlock, MIXED ? THP_EMPOLE_MINB : 4) k_empole_pairs(
     int n, int npad, Box box, double off2, EwM ew, const double4* __restrict__ pos, const double* __restrict__ mrec,
     const float* __restrict__ erec, const int* __restrict__ perm, const int* __restrict__ sp_off,
     const int* __restrict__ sp_ks, const int* __restrict__ sp_c, const int* __restrict__ nnb,
     const int* __restrict__ nb, int maxnb, const int* __restrict__ frs, unsigned long long* __restrict__ dem,
-    double* __restrict__ epart) {
+    double* __restrict__ epart, double* __restrict__ vpart) {
   using T = typename std::conditional<MIXED, float, double>::type;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double eacc = 0.0;
+  double v6[6] = {0, 0, 0, 0, 0, 0};
   if (i < n) {
     T mi[10];
     double4 pi4 = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -233,27 +253,54 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_EMPOLE_MINB : 4) k_empole_
           break;
         }
       if (scaled) continue;
-      mpole_pair<T>(xr, yr, zr, r2, T(0), mi, mk, ew, eacc, g3, t3);
+      mpole_pair<T>(xr, yr, zr, r2, T(0), mi, mk, ew, eacc, g3, t3, VIR ? v6 : nullptr);
     }
     fix_add(dem + 3 * i + 0, g3[0]);
     fix_add(dem + 3 * i + 1, g3[1]);
     fix_add(dem + 3 * i + 2, g3[2]);
     const int iz = frs[3 * i], ix = frs[3 * i + 1], axt = frs[3 * i + 2];
-    if (axt == 1 || axt == 2) torque_dist(pos, i, iz, ix, axt, t3, dem);
+    if (axt == 1 || axt == 2) {
+      if (VIR) {
+        double du[3], dv[3];
+        torque_frame(pos, i, iz, ix, axt, t3, du, dv);
+        frame_virial(pos, i, iz, ix, du, dv, v6);  // empole1.f:1466-1497
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          fix_add(dem + 3 * iz + j, du[j]);
+          fix_add(dem + 3 * ix + j, dv[j]);
+          fix_add(dem + 3 * i + j, -du[j] - dv[j]);
+        }
+      } else {
+        torque_dist(pos, i, iz, ix, axt, t3, dem);
+      }
+    }
   }
   block_partial<kBlock>(eacc, epart);
+  if (VIR) {
+    block_reduce<6>(v6);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) vpart[(size_t)blockIdx.x * 6 + q] = v6[q];
+  }
 }
 
 // Per site, in FP64: the 1-2..1-5 pairs within the cutoff (all are in the
 // list when it is valid; the damped and bare terms cancel there to a small
 // difference), the emrecip1 terms from fphirec and the self energy.
+// VIR: each block also writes 12 virial sums to vpart: the reference's terms
+// (scaled pair halves, the frame-atom virial of their torques and emrecip1's
+// site terms, empole1.f:741-761) and the frame-atom virial of the reciprocal
+// torques, which the reference leaves out.
+template <bool VIR>
 __global__ void __launch_bounds__(kBlock) k_empole_site(
     int n, Box box, double off2, EwM ew, MScale ms, PmeGeom g, const double4* __restrict__ pos,
     const double* __restrict__ rp, const int* __restrict__ perm, const int* __restrict__ sp_off,
     const int* __restrict__ sp_ks, const int* __restrict__ sp_c, const double* __restrict__ fphirec,
-    const int* __restrict__ frs, unsigned long long* __restrict__ dem, double* __restrict__ epart) {
+    const int* __restrict__ frs, unsigned long long* __restrict__ dem, double* __restrict__ epart,
+    double* __restrict__ vpart) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double eacc = 0.0;
+  double v12[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (i < n) {
     const double4 pi4 = pos[i];
     const int io = perm[i];
@@ -275,7 +322,7 @@ __global__ void __launch_bounds__(kBlock) k_empole_site(
       double mkd[10];
 #pragma unroll
       for (int w = 0; w < 10; ++w) mkd[w] = rp[(size_t)k * 10 + w];
-      mpole_pair<double>(xrd, yrd, zrd, r2d, 1.0 - ms.v[cls], mid, mkd, ew, eacc, g3, t3);
+      mpole_pair<double>(xrd, yrd, zrd, r2d, 1.0 - ms.v[cls], mid, mkd, ew, eacc, g3, t3, VIR ? v12 : nullptr);
     }
     double gx = g3[0], gy = g3[1], gz = g3[2];
     const double tx = t3[0], ty = t3[1], tz = t3[2];
@@ -314,12 +361,24 @@ __global__ void __launch_bounds__(kBlock) k_empole_site(
                            g.a[0] * g.a[2] * FR[9],
                            g.a[1] * g.a[2] * FR[10]};
     double trq[3];
-    trq[0] = tx + cm[3] * cp[2] - cm[2] * cp[3] + 2.0 * (cm[6] - cm[5]) * cp[9] + cm[8] * cp[7] + cm[9] * cp[5] -
+    trq[0] = cm[3] * cp[2] - cm[2] * cp[3] + 2.0 * (cm[6] - cm[5]) * cp[9] + cm[8] * cp[7] + cm[9] * cp[5] -
              cm[7] * cp[8] - cm[9] * cp[6];
-    trq[1] = ty + cm[1] * cp[3] - cm[3] * cp[1] + 2.0 * (cm[4] - cm[6]) * cp[8] + cm[7] * cp[9] + cm[8] * cp[6] -
+    trq[1] = cm[1] * cp[3] - cm[3] * cp[1] + 2.0 * (cm[4] - cm[6]) * cp[8] + cm[7] * cp[9] + cm[8] * cp[6] -
              cm[8] * cp[4] - cm[9] * cp[7];
-    trq[2] = tz + cm[2] * cp[1] - cm[1] * cp[2] + 2.0 * (cm[5] - cm[4]) * cp[7] + cm[7] * cp[4] + cm[9] * cp[8] -
+    trq[2] = cm[2] * cp[1] - cm[1] * cp[2] + 2.0 * (cm[5] - cm[4]) * cp[7] + cm[7] * cp[4] + cm[9] * cp[8] -
              cm[7] * cp[5] - cm[8] * cp[9];
+    if (VIR) {
+      // emrecip1's permanent-multipole site terms (empole1.f:741-761)
+      v12[0] -= cm[1] * cp[1] + 2.0 * cm[4] * cp[4] + cm[7] * cp[7] + cm[8] * cp[8];
+      v12[1] -= 0.5 * (cm[2] * cp[1] + cm[1] * cp[2]) + (cm[4] + cm[5]) * cp[7] + 0.5 * cm[7] * (cp[4] + cp[5]) +
+                0.5 * (cm[8] * cp[9] + cm[9] * cp[8]);
+      v12[2] -= 0.5 * (cm[3] * cp[1] + cm[1] * cp[3]) + (cm[4] + cm[6]) * cp[8] + 0.5 * cm[8] * (cp[4] + cp[6]) +
+                0.5 * (cm[7] * cp[9] + cm[9] * cp[7]);
+      v12[3] -= cm[2] * cp[2] + 2.0 * cm[5] * cp[5] + cm[7] * cp[7] + cm[9] * cp[9];
+      v12[4] -= 0.5 * (cm[3] * cp[2] + cm[2] * cp[3]) + (cm[5] + cm[6]) * cp[9] + 0.5 * cm[9] * (cp[5] + cp[6]) +
+                0.5 * (cm[7] * cp[8] + cm[8] * cp[7]);
+      v12[5] -= cm[3] * cp[3] + 2.0 * cm[6] * cp[6] + cm[8] * cp[8] + cm[9] * cp[9];
+    }
     // Ewald self energy (empole1.f:134-160)
     const double term = 2.0 * ew.a * ew.a;
     const double fterm = -fe * ew.a / kSqrtPi;
@@ -331,9 +390,31 @@ __global__ void __launch_bounds__(kBlock) k_empole_site(
     fix_add(dem + 3 * i + 1, gy);
     fix_add(dem + 3 * i + 2, gz);
     const int iz = frs[3 * i], ix = frs[3 * i + 1], axt = frs[3 * i + 2];
-    if (axt == 1 || axt == 2) torque_dist(pos, i, iz, ix, axt, trq, dem);
+    if ((axt == 1 || axt == 2) && VIR) {
+      // the scaled pairs' torque (real space) and the reciprocal torque apart
+      double tr[3] = {tx, ty, tz}, du[3], dv[3], dux[3], dvx[3];
+      torque_frame(pos, i, iz, ix, axt, tr, du, dv);
+      torque_frame(pos, i, iz, ix, axt, trq, dux, dvx);
+      frame_virial(pos, i, iz, ix, du, dv, *reinterpret_cast<double(*)[6]>(&v12[0]));
+      frame_virial(pos, i, iz, ix, dux, dvx, *reinterpret_cast<double(*)[6]>(&v12[6]));
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        fix_add(dem + 3 * iz + j, du[j] + dux[j]);
+        fix_add(dem + 3 * ix + j, dv[j] + dvx[j]);
+        fix_add(dem + 3 * i + j, -(du[j] + dux[j]) - (dv[j] + dvx[j]));
+      }
+    } else if (axt == 1 || axt == 2) {
+      const double tt[3] = {tx + trq[0], ty + trq[1], tz + trq[2]};
+      torque_dist(pos, i, iz, ix, axt, tt, dem);
+    }
   }
   block_partial<kBlock>(eacc, epart);
+  if (VIR) {
+    block_reduce<12>(v12);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q < 12; ++q) vpart[(size_t)blockIdx.x * 12 + q] = v12[q];
+  }
 }
 
 // buffers made on first use, sized by n (freed when a re-targeted context
@@ -360,7 +441,12 @@ int launch_empole(Ctx& c, double* d_out) {
   if ((st = cuda_status(cudaMemsetAsync(dem, 0, sizeof(unsigned long long) * 3 * n, c.stream), &c, "zero dem")))
     return st;
   if ((st = launch_frames_sorted(c))) return st;
-  if ((st = launch_mpole_grid(c))) return st;
+  const bool vir = c.want_virial;
+  double *kpart = nullptr, *rpart = nullptr, *spart = nullptr;
+  if (vir && (st = virial_scratch(c, nb, &kpart, &rpart, &spart))) return st;
+  // the convolved multipole grid (and emrecip1's scalar sum over the
+  // reciprocal lattice, empole1.f:560-598)
+  if ((st = vir ? launch_mpole_grid_virial(c, kpart, 1.0) : launch_mpole_grid(c))) return st;
   if ((st = launch_fphi_mpole20(c))) return st;
   EwM ew;
   const double a = c.cfg.aewald;
@@ -378,18 +464,29 @@ int launch_empole(Ctx& c, double* d_out) {
   const PmeGeom g = pme_geom(c);
 #define THP_EMPOLE_ARGS                                                                                          \
   c.n, c.npad, c.box, off2, ew, c.d_pos, c.d_mrec, c.d_erec, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_c, c.d_nnb, c.d_nb, \
-      c.maxnb, c.d_frs, dem, c.d_empart
-  if (c.mixed)
-    k_empole_pairs<true><<<nb, kBlock, 0, c.stream>>>(THP_EMPOLE_ARGS);
+      c.maxnb, c.d_frs, dem, c.d_empart, rpart
+  if (c.mixed && vir)
+    k_empole_pairs<true, true><<<nb, kBlock, 0, c.stream>>>(THP_EMPOLE_ARGS);
+  else if (c.mixed)
+    k_empole_pairs<true, false><<<nb, kBlock, 0, c.stream>>>(THP_EMPOLE_ARGS);
+  else if (vir)
+    k_empole_pairs<false, true><<<nb, kBlock, 0, c.stream>>>(THP_EMPOLE_ARGS);
   else
-    k_empole_pairs<false><<<nb, kBlock, 0, c.stream>>>(THP_EMPOLE_ARGS);
+    k_empole_pairs<false, false><<<nb, kBlock, 0, c.stream>>>(THP_EMPOLE_ARGS);
 #undef THP_EMPOLE_ARGS
   if ((st = cuda_status(cudaGetLastError(), &c, "empole pairs"))) return st;
-  k_empole_site<<<nb, kBlock, 0, c.stream>>>(c.n, c.box, off2, ew, ms, g, c.d_pos, c.d_rpole, c.d_perm, c.d_sp_off,
-                                             c.d_sp_ks, c.d_sp_c, c.d_fphirec, c.d_frs, dem, c.d_empart + nb);
+#define THP_SITE_ARGS                                                                                              \
+  c.n, c.box, off2, ew, ms, g, c.d_pos, c.d_rpole, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_c, c.d_fphirec, c.d_frs, \
+      dem, c.d_empart + nb, spart
+  if (vir)
+    k_empole_site<true><<<nb, kBlock, 0, c.stream>>>(THP_SITE_ARGS);
+  else
+    k_empole_site<false><<<nb, kBlock, 0, c.stream>>>(THP_SITE_ARGS);
+#undef THP_SITE_ARGS
   if ((st = cuda_status(cudaGetLastError(), &c, "empole"))) return st;
   k_sum_partials<<<1, 256, 0, c.stream>>>(2 * nb, c.d_empart, c.d_em);
   if ((st = cuda_status(cudaGetLastError(), &c, "empole energy"))) return st;
+  if (vir && (st = virial_total(c, kspace_virial_blocks(), nb, kpart, rpart, spart, c.h_mvir))) return st;
   return launch_gradient_out(c, dem, d_out);
 }
 

@@ -641,7 +641,7 @@ static int kspace_virial(Ctx& c, int mode, double sign, double* d_part) {
 // launch_mpole_grid with, between the forward transform and qfac, the
 // permanent-only scalar-sum virial (emrecip1), subtracted as eprecip1 does
 // (epolar1.f:534-541): kspace_virial_blocks() rows of 6 into d_part.
-int launch_mpole_grid_virial(Ctx& c, double* d_part) {
+int launch_mpole_grid_virial(Ctx& c, double* d_part, double sign) {
   PmeGeom g = geom_of(c);
   int nb = (c.n + kBlock - 1) / kBlock;
   int st = zero_grid(c);
@@ -652,7 +652,7 @@ int launch_mpole_grid_virial(Ctx& c, double* d_part) {
     k_spread_mpole<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, c.d_rpole, (cufftDoubleComplex*)c.d_grid);
   if ((st = cuda_status(cudaGetLastError(), &c, "spread mpole"))) return st;
   if ((st = fft(c, CUFFT_FORWARD))) return st;
-  if ((st = kspace_virial(c, 0, -1.0, d_part))) return st;
+  if ((st = kspace_virial(c, 0, sign, d_part))) return st;
   int blocks = 148 * 8;
   if (c.mixed)
     k_qfac<cufftComplex, float><<<blocks, 256, 0, c.stream>>>(c.ngrid, (const float*)c.d_qfac,

@@ -147,11 +147,8 @@ __global__ void __launch_bounds__(kBlock, THP_ROW_MINB) k_real_row(PairRows pr, 
   }
 }
 
-// h = hreal + x/alpha + dipfield(x) - term x, then the reductions of
-// k_cg_matvec (init: residual, zr, pp and ggold; iter: gg and alpha).
-// GATHER 0 reads dipfield from dipf; 1 / 2 gather it here from the
-// convolved FP32 / FP64 grid (the work of k_gather_dip, without the round
-// trip of dipfield through memory).
+// h = hreal + x/alpha + dipfield(x) - term x and the reductions of one CG
+// step (cg_combine_block); hreal comes from k_real_row.
 template <int GATHER, typename XV, typename V>
 __global__ void __launch_bounds__(kBlock) k_cg_combine(int n, const double* __restrict__ dipf, PmeGeom g,
                                                        const double4* __restrict__ pos, const void* __restrict__ grid,
@@ -161,61 +158,8 @@ __global__ void __launch_bounds__(kBlock) k_cg_combine(int n, const double* __re
                                                        V* __restrict__ pp, CgScalars* cg,
                                                        double* __restrict__ partials) {
   if (cg->stop) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double red[2] = {0.0, 0.0};
-  if (i < n) {
-    double acc[6], dip[6], xi[6];
-    if constexpr (GATHER == 1)
-      gather_dip<float>(g, pos[i], reinterpret_cast<const cufftComplex*>(grid), dip);
-    else if constexpr (GATHER == 2)
-      gather_dip<double>(g, pos[i], reinterpret_cast<const cufftDoubleComplex*>(grid), dip);
-    else
-      load6(dipf + (size_t)i * 6, dip);
-    load6(h + (size_t)i * 6, acc);
-    load6(x + (size_t)i * 6, xi);
-    const double p = pol[i];
-    const double ip = (p == 0.0) ? 1.0 / kTinyPol : 1.0 / p;
-    double hv[6];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) hv[q] = ((acc[q] + xi[q] * ip) + dip[q]) - term * xi[q];
-    store6(h + (size_t)i * 6, hv);
-    if (init) {
-      double e6[6], r6[6], z6[6];
-      load6(ef + (size_t)i * 6, e6);
-      const double dg = diag_of(p);
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        r6[q] = e6[q] - hv[q];
-        z6[q] = dg * r6[q];
-      }
-      store6(res + (size_t)i * 6, r6);
-      store6(zr + (size_t)i * 6, z6);
-      store6(pp + (size_t)i * 6, z6);
-      red[0] = r6[0] * z6[0] + r6[1] * z6[1] + r6[2] * z6[2];
-      red[1] = r6[3] * z6[3] + r6[4] * z6[4] + r6[5] * z6[5];
-    } else {
-      red[0] = xi[0] * hv[0] + xi[1] * hv[1] + xi[2] * hv[2];
-      red[1] = xi[3] * hv[3] + xi[4] * hv[4] + xi[5] * hv[5];
-    }
-  }
-  double tot[2];
-  if (grid_reduce<2>(red, partials, &cg->counter[0], tot) && threadIdx.x == 0) {
-    if (init) {
-      cg->ggold[0] = tot[0];
-      cg->ggold[1] = tot[1];
-      cg->beta[0] = 0.0;
-      cg->beta[1] = 0.0;
-    } else {
-      cg->gg[0] = tot[0];
-      cg->gg[1] = tot[1];
-      if (tot[0] == 0.0 || tot[1] == 0.0) {
-        cg->stop = 1;  // newinduce_pme2.f:505 returns on gg == 0
-      } else {
-        cg->alpha[0] = cg->ggold[0] / tot[0];
-        cg->alpha[1] = cg->ggold[1] / tot[1];
-      }
-    }
-  }
+  cg_combine_block<GATHER, XV, V>((int)blockIdx.x, (int)gridDim.x, n, dipf, g, pos, grid, x, pol, ef, term, init, h,
+                                  res, zr, pp, cg, partials);
 }
 
 // mu, residual and preconditioned residual of one CG step (cg_update_block)

@@ -114,6 +114,7 @@ def load():
         "thp_get_gradient_device": ([vp, vp], C.c_int),
         "thp_set_virial": ([vp, C.c_int], C.c_int),
         "thp_get_virial": ([vp, C.c_int, _dp], C.c_int),
+        "thp_get_empole_virial": ([vp, C.c_int, _dp], C.c_int),
         "thp_bind_virial": ([vp, _dp], C.c_int),
         "thp_md_verlet": ([vp, C.c_int, C.c_double, _dp, _dp, _dp, _ip], C.c_int),
         "thp_get_positions": ([vp, _dp, _dp, _dp], C.c_int),
@@ -424,7 +425,7 @@ class Context:
         return ep.value, dep
 
     def set_virial(self, on=True):
-        """Later gradient calls also compute the polarization virial."""
+        """Later gradient and empole1 calls also compute their virials."""
         self._check(load().thp_set_virial(self.h, 1 if on else 0), "thp_set_virial")
 
     def virial(self, form=0):
@@ -432,6 +433,13 @@ class Context:
         on; form 1 adds the reciprocal and self torques' frame-atom terms."""
         v = np.zeros((3, 3))
         self._check(load().thp_get_virial(self.h, int(form), _p(v)), "thp_get_virial")
+        return v
+
+    def empole_virial(self, form=0):
+        """vir [3,3] (kcal/mol) of the last empole1 call made with the virial
+        on; form 1 adds the reciprocal torques' frame-atom terms."""
+        v = np.zeros((3, 3))
+        self._check(load().thp_get_empole_virial(self.h, int(form), _p(v)), "thp_get_empole_virial")
         return v
 
     def set_vdw(self, v):
