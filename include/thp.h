@@ -224,6 +224,11 @@ int thp_get_virial(thp_ctx* ctx, int form, double* vir);
  * torques, which the reference leaves out); THP_E_STATE before such a call.
  * empole1_ adds form 0 into the bound vir when one is bound. */
 int thp_get_empole_virial(thp_ctx* ctx, int form, double* vir);
+/* The virial [3][3] of the last thp_ehal1 call made with thp_set_virial on
+ * (ehal1c's pair terms over the reduced sites, ehal1.f:431-446);
+ * THP_E_STATE before such a call.  ehal1_ adds it into the bound vir when
+ * one is bound. */
+int thp_get_ehal_virial(thp_ctx* ctx, double* vir);
 /* m2scale..m5scale [4] of the permanent-multipole pair terms (mplpot module;
  * defaults initprm.f:413-416: 0, 0, 1, 1; AMOEBA water03.prm:34-37: 0, 0,
  * 0.4, 0.8).  The 1-2..1-5 lists come from thp_set_connectivity. */

@@ -78,7 +78,7 @@ def lib():
         L.or_epolar.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         L.or_epolar1.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, _dp, _dp, _dp, _dp]
         L.or_empole1.argtypes = [C.c_void_p, _ip, _ip, _ip, _dp, _dp, _dp, _dp]
-        L.or_ehal1.argtypes = [C.c_void_p, C.POINTER(OrVdw), _dp, _dp]
+        L.or_ehal1.argtypes = [C.c_void_p, C.POINTER(OrVdw), _dp, _dp, _dp]
         L.or_rotpole.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _dp]
         L.or_grid_uind_sites.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp, _dp]
         L.or_fphi_uind_sites.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp, _dp, _dp]
@@ -262,8 +262,9 @@ class Oracle:
             return parts[0], dem, tuple(parts[1:]), vir, vfr
         return parts[0], dem, tuple(parts[1:])
 
-    def ehal1(self, vdw=None):
-        """Buffered 14-7 energy and gradient (ehal1c): (ev, dev [n,3])."""
+    def ehal1(self, vdw=None, virial=False):
+        """Buffered 14-7 energy and gradient (ehal1c): (ev, dev [n,3]); with
+        virial=True also the pairs' internal virial vir(3,3) (kcal/mol)."""
         v = self.ws.vdw if vdw is None else vdw
         keep = [np.ascontiguousarray(v["cls"], np.int32), np.ascontiguousarray(v["radmin"], np.float64),
                 np.ascontiguousarray(v["eps"], np.float64), np.ascontiguousarray(v["radmin4"], np.float64),
@@ -279,9 +280,12 @@ class Oracle:
         sv.vdwcut, sv.vdwtaper, sv.ghal, sv.dhal = v["vdwcut"], v["vdwtaper"], v["ghal"], v["dhal"]
         dev = np.zeros((self.ws.n, 3))
         ev = C.c_double()
-        st = lib().or_ehal1(self.ctx, C.byref(sv), _p(dev), C.byref(ev))
+        vir = np.zeros((3, 3)) if virial else None
+        st = lib().or_ehal1(self.ctx, C.byref(sv), _p(dev), C.byref(ev), _p(vir))
         if st != 0:
             raise RuntimeError(f"oracle ehal1 status {st}")
+        if virial:
+            return ev.value, dev, vir
         return ev.value, dev
 
     def grid_uind_sites(self, sites, fuind, fuinp, grid):

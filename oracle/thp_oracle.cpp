@@ -2438,10 +2438,11 @@ int or_empole1(OrCtx* c, const int* zaxis, const int* xaxis, const int* axt, dou
 // whose reduced minimum-image distance is within vdwcut + lbuffer (the
 // reference finds the same pairs through its cells); the energy loop then
 // applies r <= vdwcut and the taper above vdwtaper.
-int or_ehal1(OrCtx* c, const OrVdw* v, double* dev, double* ev_out) {
+int or_ehal1(OrCtx* c, const OrVdw* v, double* dev, double* ev_out, double* vir_out) {
   const OrSystem& s = c->s;
   const int n = s.n;
   std::fill(dev, dev + (size_t)n * 3, 0.0);
+  Vir vir;
   const double vbuf = v->vdwcut + s.lbuffer;
   if (vbuf > 0.5 * std::min(s.xbox, std::min(s.ybox, s.zbox))) return OR_E_BOX_TOO_SMALL;
   // reduced coordinates (ehal1.f:193-205)
@@ -2521,6 +2522,8 @@ int or_ehal1(OrCtx* c, const OrVdw* v, double* dev, double* ev_out) {
       ev += e;
       de = de / rik;
       const double dedx = de * xd, dedy = de * yd, dedz = de * zd;
+      // the virial of the pair (ehal1.f:431-446), reduced-site separation
+      vir.add(xd * dedx, yd * dedx, zd * dedx, yd * dedy, zd * dedy, zd * dedz);
       if (i == iv) {
         dev[i * 3 + 0] += dedx;
         dev[i * 3 + 1] += dedy;
@@ -2548,6 +2551,7 @@ int or_ehal1(OrCtx* c, const OrVdw* v, double* dev, double* ev_out) {
     }
     for (int b = 0; b < 4; ++b) for_conn(s, slot[b], i, [&](int k) { vscale[k] = 1.0; });
   }
+  if (vir_out) vir.out(vir_out);
   if (ev_out) *ev_out = ev;
   return OR_OK;
 }

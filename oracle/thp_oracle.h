@@ -133,8 +133,9 @@ typedef struct OrVdw {
 /* ehal1c (ehal1.f:69-482, standard branch): buffered 14-7 energy and
  * gradient dev [n][3] over the pairs of the vdW list (vlistcell,
  * nblist.f:1148-1305: reduced coordinates, half list within vdwcut +
- * lbuffer), with the 5th-degree taper (switch.f:80-117). */
-int or_ehal1(OrCtx* c, const OrVdw* v, double* dev, double* ev);
+ * lbuffer), with the 5th-degree taper (switch.f:80-117).  vir (may be
+ * NULL): the internal virial vir(3,3) of the pairs (ehal1.f:431-446). */
+int or_ehal1(OrCtx* c, const OrVdw* v, double* dev, double* ev, double* vir);
 
 /* grid_uind_site (pmestuff.f:280-405) for nsites sites (0-based atom
  * numbers): adds the fractional dipoles fuind/fuinp (3 per site) into the

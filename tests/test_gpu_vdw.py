@@ -174,7 +174,8 @@ def test_retargeted_context_and_shared_buffers(lib, thp):
     ctx.empole1()
     ctx.ehal1()
     ep1, g1 = ctx.gradient()
-    assert ep0 == ep1 and np.array_equal(g0, g1)
+    # the same up to the order of the PME spread's FP64 atomics (~1e-15)
+    assert ep0 == ep1 and rel(g1, g0) < 1e-12, rel(g1, g0)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -197,3 +198,22 @@ def test_sites_without_radius_take_no_part(lib, thp, precision):
     tol = 1e-10 if precision == "fp64" else 1e-5
     assert abs(ev - ev_ref) < tol * abs(ev_ref), (ev, ev_ref)
     assert np.abs(dev[1::3]).max() == 0.0 and np.abs(dev[2::3]).max() == 0.0  # no force on the H atoms
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ehal1_virial_matches_oracle(lib, thp, precision):
+    # ehal1c's pair virial over the reduced sites (ehal1.f:431-446) against
+    # the oracle's, which the strain derivative of its energy pins
+    # (tests/test_oracle.py::test_ehal1_virial_matches_strain_derivative):
+    # FP64 within 1e-10 of the largest component, mixed (FP32 pair terms)
+    # within 1e-5
+    ws = thp.water.make_water_box(216, cfg=0, edge=20.0)
+    _, _, vir_ref = O.Oracle(ws).ehal1(virial=True)
+    ctx = lib.Context(ws, precision=lib.FP64 if precision == "fp64" else lib.MIXED)
+    ctx.set_virial(True)
+    ctx.ehal1()
+    vir = ctx.ehal_virial()
+    err = np.abs(vir - vir_ref).max() / np.abs(vir_ref).max()
+    print(f"\nehal virial {precision}: {err:.2e} of the largest component")
+    assert err < (1e-10 if precision == "fp64" else 1e-5), (vir, vir_ref)
+    np.testing.assert_allclose(vir, vir.T, rtol=0, atol=0)

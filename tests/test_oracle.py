@@ -465,6 +465,27 @@ def test_ehal1_gradient_matches_finite_differences(thp):
             assert abs(fd - dev[atom, d]) < 1e-6 * np.abs(dev).max() + 1e-7, (atom, d, fd, dev[atom, d])
 
 
+def test_ehal1_virial_matches_strain_derivative(thp):
+    # scaling the coordinates and the box edge along x, y or z: the reduced
+    # sites scale with them, and the taper makes the energy smooth at the
+    # cutoff, so the central difference equals vir(a,a) (ehal1.f:431-446)
+    ws = thp.water.make_water_box(216, cfg=0, edge=20.0)
+    _, _, vir = O.Oracle(ws).ehal1(virial=True)
+    np.testing.assert_allclose(vir, vir.T, rtol=0, atol=1e-12 * np.abs(vir).max())
+    eps = 1e-5
+    pos0 = ws.positions()
+    for a in range(3):
+        e = []
+        for sgn in (1, -1):
+            p = pos0.copy()
+            p[:, a] *= 1.0 + sgn * eps
+            edge = list(ws.box)
+            edge[a] *= 1.0 + sgn * eps
+            e.append(O.Oracle(dataclasses.replace(ws.with_positions(p), box=tuple(edge))).ehal1()[0])
+        fd = (e[0] - e[1]) / (2 * eps)
+        assert abs(fd - vir[a, a]) < 1e-6 * np.abs(vir).max(), (a, fd, vir[a, a])
+
+
 def test_ehal1_refuses_a_small_box(thp):
     ws = thp.water.make_water_box(64, cfg=0, edge=16.0)  # 9 + 0.5 A exceeds half of 16 A
     with pytest.raises(RuntimeError, match="status 8"):

@@ -1087,7 +1087,9 @@ int thp_ehal1(thp_ctx* h, double* ev, double* dev) {
   if ((st = ensure_list(h, false))) return st;
   if (!c.d_grad && (st = cuda_status(cudaMalloc((void**)&c.d_grad, sizeof(double) * 3 * c.n), &c, "alloc gradient")))
     return st;
+  c.have_vvirial = false;
   if ((st = launch_ehal(c, c.d_grad))) return st;
+  c.have_vvirial = c.want_virial;  // totals land in h_vvir with the copies below
   double e = 0.0;
   cudaMemcpyAsync(&e, c.d_ev, sizeof(double), cudaMemcpyDeviceToHost, c.stream);
   if (dev) cudaMemcpyAsync(dev, c.d_grad, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost, c.stream);
@@ -1621,6 +1623,16 @@ int thp_get_empole_virial(thp_ctx* h, int form, double* vir) {
   return THP_OK;
 }
 
+int thp_get_ehal_virial(thp_ctx* h, double* vir) {
+  if (!h || !vir) return THP_E_INVALID;
+  Ctx& c = h->c;
+  if (!c.have_vvirial) return THP_E_STATE;
+  const double* v = c.h_vvir;
+  const double t[9] = {v[0], v[1], v[2], v[1], v[3], v[4], v[2], v[4], v[5]};
+  std::memcpy(vir, t, sizeof(t));
+  return THP_OK;
+}
+
 int thp_set_virial(thp_ctx* h, int on) {
   if (!h) return THP_E_INVALID;
   h->c.want_virial = on != 0;
@@ -2082,8 +2094,14 @@ void ehal1_(void) {
   }
   int st = sync_bound_inputs(h);
   double ev = 0.0;
+  h->c.want_virial = h->c.bvir != nullptr;
   if (!st) st = thp_ehal1(h, &ev, h->c.bdev);
   if (!st && h->c.bev) *h->c.bev = ev;
+  if (!st && h->c.bvir) {  // ehal1c adds into vir (ehal1.f:438-446)
+    double v[9];
+    st = thp_get_ehal_virial(h, v);
+    for (int q = 0; !st && q < 9; ++q) h->c.bvir[q] += v[q];
+  }
   g_last_error = st;
 }
 

@@ -213,9 +213,11 @@ struct Ctx {
   double* d_virp = nullptr;
   size_t virp_cap = 0;
   double h_vir[12] = {};
-  // the same for the last empole1 call (thp_get_empole_virial)
-  bool have_mvirial = false;
+  // the same for the last empole1 call (thp_get_empole_virial) and the
+  // last ehal1 call (thp_get_ehal_virial; 6 values used)
+  bool have_mvirial = false, have_vvirial = false;
   double h_mvir[12] = {};
+  double h_vvir[12] = {};
   int* d_frs = nullptr;           // [n][3] frame atoms (sorted indices), axis type
   double* d_grad = nullptr;       // [n][3] gradient, original order
 

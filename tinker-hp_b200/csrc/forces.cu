@@ -257,12 +257,21 @@ struct EwC {
 #define THP_FORCE_MINB 4
 #endif
 
+// lanes per site of the real-space gradient pass (1 or 8)
+#ifndef THP_FORCE_LPA
+#define THP_FORCE_LPA 8
+#endif
+
 // VIR: each block also writes to vpart[block][12] the sum of its sites' pair
 // virials (epolar1.f:2326-2342, half from each end of a pair) and the
 // frame-atom virial of their real-space torques (:2460-2486) in 0..5, and
 // the frame-atom virial of their reciprocal and self torques, which the
 // reference does not add, in 6..11.
-template <bool MIXED, bool VIR>
+// LPA: lanes per atom.  1: one thread per site over its whole list; 8: a
+// warp takes four consecutive (cell-sorted) sites, eight lanes each, lane j
+// taking list entries j, j+8, ...; the lanes' sums are combined in a fixed
+// shuffle tree and the first lane of the site finishes it.
+template <bool MIXED, bool VIR, int LPA>
 __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_real(
     int n, int npad, Box box, double off2, EwC ew, const double4* __restrict__ pos,
     const typename std::conditional<MIXED, float, double>::type* __restrict__ mrec, const double* __restrict__ mu,
@@ -271,9 +280,14 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_re
     const int* __restrict__ nnb, const int* __restrict__ nb, int maxnb, const int* __restrict__ frs,
     const double* __restrict__ trq_recip, unsigned long long* __restrict__ dep, double* __restrict__ vpart) {
   using T = typename std::conditional<MIXED, float, double>::type;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  static_assert(LPA == 1 || LPA == 8, "one or eight lanes per site");
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i0 = LPA == 1 ? t : t >> 3, jl = LPA == 1 ? 0 : t & 7;
+  const bool live = i0 < n;
+  if (LPA == 1 && !live && !VIR) return;
+  const int i = live ? i0 : n - 1;  // a valid site for the loads of idle lanes
   double vout[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-  if (i < n) {
+  {
   const double4 pi4 = pos[i];
   // mixed form: partners from the 64-B FP32 site record (wrapped position,
   // 1/pdamp, thole, multipoles) and the FP32 dipole record, imaged in FP32
@@ -298,9 +312,9 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_re
   double gx = 0.0, gy = 0.0, gz = 0.0;
   T uf[3] = {0, 0, 0}, duf[6] = {0, 0, 0, 0, 0, 0};
   T vp[6] = {0, 0, 0, 0, 0, 0};  // pair virial, half of each pair's
-  const int nn = min(nnb[i], maxnb);
+  const int nn = live ? min(nnb[i], maxnb) : 0;
 #pragma unroll 1
-  for (int s = 0; s < nn; ++s) {
+  for (int s = jl; s < nn; s += LPA) {
     const int k = __ldg(nb + (size_t)s * npad + i);
     T xr, yr, zr, r2, pdk;
     T ptk, ck, dkx, dky, dkz, qkxx, qkxy, qkxz, qkyy, qkyz, qkzz;
@@ -591,6 +605,22 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_re
       vp[5] += h * (zr * frc[2]);
     }
   }
+  if (LPA == 8) {
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+      gx += __shfl_xor_sync(0xffffffffu, gx, o);
+      gy += __shfl_xor_sync(0xffffffffu, gy, o);
+      gz += __shfl_xor_sync(0xffffffffu, gz, o);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) uf[q] += __shfl_xor_sync(0xffffffffu, uf[q], o);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) duf[q] += __shfl_xor_sync(0xffffffffu, duf[q], o);
+      if (VIR)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) vp[q] += __shfl_xor_sync(0xffffffffu, vp[q], o);
+    }
+  }
+  if (live && jl == 0) {
   fix_add(dep + 3 * i + 0, gx);
   fix_add(dep + 3 * i + 1, gy);
   fix_add(dep + 3 * i + 2, gz);
@@ -640,7 +670,8 @@ __global__ void __launch_bounds__(kBlock, MIXED ? THP_FORCE_MINB : 1) k_force_re
     tep[2] += trq_recip[(size_t)i * 3 + 2] + sterm * (rdx * hy - rdy * hx);
     if (axt == 1 || axt == 2) torque_dist(pos, i, iz, ix, axt, tep, dep);
   }
-  }  // i < n
+  }  // the site's first lane
+  }
   if (VIR) {
     block_reduce<12>(vout);
     if (threadIdx.x == 0)
@@ -713,9 +744,9 @@ int launch_gradient_out(Ctx& c, const unsigned long long* dep, double* d_out) {
 // Partial-sum rows of one gradient call's virial: 2 kspace_virial_blocks()
 // rows of 6 (k-space sums), nb rows of 6 and nb rows of 12 (per-block site
 // and pair terms), then 12 totals; grown on demand.
-int virial_scratch(Ctx& c, int nb, double** kpart, double** rpart, double** epart) {
+int virial_scratch(Ctx& c, int nr, int ne, double** kpart, double** rpart, double** epart) {
   const int nk = 2 * kspace_virial_blocks();
-  const size_t rows = (size_t)nk * 6 + (size_t)nb * 6 + (size_t)nb * 12 + 12;
+  const size_t rows = (size_t)nk * 6 + (size_t)nr * 6 + (size_t)ne * 12 + 12;
   if (c.virp_cap < rows) {
     cudaFree(c.d_virp);
     c.d_virp = nullptr;
@@ -726,16 +757,16 @@ int virial_scratch(Ctx& c, int nb, double** kpart, double** rpart, double** epar
   }
   *kpart = c.d_virp;
   *rpart = *kpart + (size_t)nk * 6;
-  *epart = *rpart + (size_t)nb * 6;
+  *epart = *rpart + (size_t)nr * 6;
   return THP_OK;
 }
 
 // The 12 totals of the partial sums (in a fixed order; nk k-space rows)
 // copied to h_out when the stream reaches them.
-int virial_total(Ctx& c, int nk, int nb, const double* kpart, const double* rpart, const double* epart,
+int virial_total(Ctx& c, int nk, int nr, int ne, const double* kpart, const double* rpart, const double* epart,
                  double* h_out) {
-  double* tot = const_cast<double*>(epart) + (size_t)nb * 12;
-  k_virial_sum<<<1, 256, 0, c.stream>>>(nk, kpart, nb, rpart, nb, epart, tot);
+  double* tot = const_cast<double*>(epart) + (size_t)ne * 12;
+  k_virial_sum<<<1, 256, 0, c.stream>>>(nk, kpart, nr, rpart, ne, epart, tot);
   const int st = cuda_status(cudaGetLastError(), &c, "virial sum");
   if (!st) cudaMemcpyAsync(h_out, tot, sizeof(double) * 12, cudaMemcpyDeviceToHost, c.stream);
   return st;
@@ -755,7 +786,9 @@ int launch_forces(Ctx& c, double* d_out) {
   const bool vir = c.want_virial;
   const int nk = 2 * kspace_virial_blocks();
   double *kpart = nullptr, *rpart = nullptr, *epart = nullptr;
-  if (vir && (st = virial_scratch(c, nb, &kpart, &rpart, &epart))) return st;
+  // the real-space pass: eight lanes per site (blocks of 16 sites)
+  const int nbr = THP_FORCE_LPA == 8 ? (c.n + 15) / 16 : nb;
+  if (vir && (st = virial_scratch(c, nb, nbr, &kpart, &rpart, &epart))) return st;
   unsigned long long* dep = c.d_depfix;
   if ((st = cuda_status(cudaMemsetAsync(dep, 0, sizeof(unsigned long long) * 3 * n, c.stream), &c, "zero gradient")))
     return st;
@@ -805,24 +838,25 @@ int launch_forces(Ctx& c, double* d_out) {
 #define THP_FORCE_ARGS                                                                                      \
   c.n, c.npad, c.box, off2, ew, c.d_pos, MREC, c.d_mu, c.d_erec, c.d_muf, c.d_perm, c.d_sp_off, c.d_sp_ks, \
       c.d_sp_s, c.d_nnb, c.d_nb, c.maxnb, c.d_frs, c.d_trq, dep, epart
+  constexpr int LPA = THP_FORCE_LPA;
   if (c.mixed) {
 #define MREC c.d_mrecf
     if (vir)
-      k_force_real<true, true><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
+      k_force_real<true, true, LPA><<<nbr, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
     else
-      k_force_real<true, false><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
+      k_force_real<true, false, LPA><<<nbr, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
 #undef MREC
   } else {
 #define MREC c.d_mrec
     if (vir)
-      k_force_real<false, true><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
+      k_force_real<false, true, LPA><<<nbr, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
     else
-      k_force_real<false, false><<<nb, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
+      k_force_real<false, false, LPA><<<nbr, kBlock, 0, c.stream>>>(THP_FORCE_ARGS);
 #undef MREC
   }
 #undef THP_FORCE_ARGS
   if ((st = cuda_status(cudaGetLastError(), &c, "force real"))) return st;
-  if (vir && (st = virial_total(c, nk, nb, kpart, rpart, epart, c.h_vir))) return st;
+  if (vir && (st = virial_total(c, nk, nb, nbr, kpart, rpart, epart, c.h_vir))) return st;
   k_dep_out<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_perm, dep, d_out);
   return cuda_status(cudaGetLastError(), &c, "force out");
 }

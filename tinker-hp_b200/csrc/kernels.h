@@ -44,8 +44,8 @@ int launch_gather_dip(Ctx& c, double* d_out, bool check_stop);
 int launch_forces(Ctx& c, double* d_out);  // dE/dx [n][3], original order, for the dipoles in d_mu
 // virial partial sums of a gradient call (k-space, per-block rows of 6 and
 // 12) and their 12 totals copied to h_out
-int virial_scratch(Ctx& c, int nb, double** kpart, double** rpart, double** epart);
-int virial_total(Ctx& c, int nk, int nb, const double* kpart, const double* rpart, const double* epart,
+int virial_scratch(Ctx& c, int nr, int ne, double** kpart, double** rpart, double** epart);
+int virial_total(Ctx& c, int nk, int nr, int ne, const double* kpart, const double* rpart, const double* epart,
                  double* h_out);
 int launch_fphi_mpole20(Ctx& c);          // fphirec [n][20] of the convolved multipole grid
 int launch_frames_sorted(Ctx& c);         // frame atoms in sorted numbering (d_frs)

@@ -443,7 +443,7 @@ int launch_empole(Ctx& c, double* d_out) {
   if ((st = launch_frames_sorted(c))) return st;
   const bool vir = c.want_virial;
   double *kpart = nullptr, *rpart = nullptr, *spart = nullptr;
-  if (vir && (st = virial_scratch(c, nb, &kpart, &rpart, &spart))) return st;
+  if (vir && (st = virial_scratch(c, nb, nb, &kpart, &rpart, &spart))) return st;
   // the convolved multipole grid (and emrecip1's scalar sum over the
   // reciprocal lattice, empole1.f:560-598)
   if ((st = vir ? launch_mpole_grid_virial(c, kpart, 1.0) : launch_mpole_grid(c))) return st;
@@ -486,7 +486,7 @@ int launch_empole(Ctx& c, double* d_out) {
   if ((st = cuda_status(cudaGetLastError(), &c, "empole"))) return st;
   k_sum_partials<<<1, 256, 0, c.stream>>>(2 * nb, c.d_empart, c.d_em);
   if ((st = cuda_status(cudaGetLastError(), &c, "empole energy"))) return st;
-  if (vir && (st = virial_total(c, kspace_virial_blocks(), nb, kpart, rpart, spart, c.h_mvir))) return st;
+  if (vir && (st = virial_total(c, kspace_virial_blocks(), nb, nb, kpart, rpart, spart, c.h_mvir))) return st;
   return launch_gradient_out(c, dem, d_out);
 }
 

@@ -213,16 +213,20 @@ __device__ __forceinline__ U hal_pair(U r2, U rv, U eps, const VdwConst& vc, dou
   return de / rik;
 }
 
-template <bool MIXED>
+// VIR: each block also writes the sum of its sites' pair virials (half of
+// each pair from each end, ehal1.f:431-446) to vpart[block][6].
+template <bool MIXED, bool VIR>
 __global__ void __launch_bounds__(kBlock) k_ehal(int n, int npad, Box box, VdwConst vc,
                                                  const double4* __restrict__ vred, const float4* __restrict__ vredf,
                                                  const int2* __restrict__ vinfo, const double* __restrict__ vtab,
                                                  const int* __restrict__ perm, const int* __restrict__ sp_off,
                                                  const int* __restrict__ sp_ks, const int* __restrict__ sp_c,
                                                  const int* __restrict__ vnnb, const int* __restrict__ vnb,
-                                                 unsigned long long* __restrict__ dev, double* __restrict__ epart) {
+                                                 unsigned long long* __restrict__ dev, double* __restrict__ epart,
+                                                 double* __restrict__ vpart) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double eacc = 0.0;
+  double v6[6] = {0, 0, 0, 0, 0, 0};
   if (i < n) {
     const double4 ri = vred[i];
     const float4 fi = vredf[i];
@@ -277,16 +281,34 @@ __global__ void __launch_bounds__(kBlock) k_ehal(int n, int npad, Box box, VdwCo
       const int t = kt * vc.nclass + it;
       const double rv = __ldg(vtab + (is14 ? 2 * nc2 : 0) + t);
       const double eps = __ldg(vtab + (is14 ? 3 * nc2 : nc2) + t) * vs;
+      double dx, dy, dz, px, py, pz;  // dE/dx of the pair and its separation
       if constexpr (MIXED) {
         const float de = hal_pair<float>(r2f, (float)rv, (float)eps, vc, eacc);
-        gx += (double)(de * xf);
-        gy += (double)(de * yf);
-        gz += (double)(de * zf);
+        dx = (double)(de * xf);
+        dy = (double)(de * yf);
+        dz = (double)(de * zf);
+        px = xf;
+        py = yf;
+        pz = zf;
       } else {
         const double de = hal_pair<double>(rik2, rv, eps, vc, eacc);
-        gx += de * xr;
-        gy += de * yr;
-        gz += de * zr;
+        dx = de * xr;
+        dy = de * yr;
+        dz = de * zr;
+        px = xr;
+        py = yr;
+        pz = zr;
+      }
+      gx += dx;
+      gy += dy;
+      gz += dz;
+      if (VIR) {
+        v6[0] += 0.5 * px * dx;
+        v6[1] += 0.5 * py * dx;
+        v6[2] += 0.5 * pz * dx;
+        v6[3] += 0.5 * py * dy;
+        v6[4] += 0.5 * pz * dy;
+        v6[5] += 0.5 * pz * dz;
       }
     }
     // the site's force: to the atom (kred) and its parent (1 - kred)
@@ -306,6 +328,12 @@ __global__ void __launch_bounds__(kBlock) k_ehal(int n, int npad, Box box, VdwCo
     }
   }
   block_partial<kBlock>(eacc, epart);
+  if (VIR) {
+    block_reduce<6>(v6);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) vpart[(size_t)blockIdx.x * 6 + q] = v6[q];
+  }
 }
 
 template <typename P>
@@ -408,16 +436,25 @@ int launch_ehal(Ctx& c, double* d_out) {
   for (int j = 0; j < 4; ++j) vc.vscale[j] = c.vdw_scale[j];
   vc.vscale[4] = 1.0;
   vc.nclass = c.vdw_nclass;
-  if (c.mixed)
-    k_ehal<true><<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vc, c.d_vred, c.d_vredf, c.d_vinfo, c.d_vtab, c.d_perm,
-                                              c.d_sp_off, c.d_sp_ks, c.d_sp_c, c.d_vnnb, c.d_vnb, dev, c.d_evpart);
+  const bool vir = c.want_virial;
+  double *kpart = nullptr, *vpart = nullptr, *epart = nullptr;
+  if (vir && (st = virial_scratch(c, nb, 0, &kpart, &vpart, &epart))) return st;
+#define THP_EHAL_ARGS                                                                                             \
+  c.n, c.npad, c.box, vc, c.d_vred, c.d_vredf, c.d_vinfo, c.d_vtab, c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_c, \
+      c.d_vnnb, c.d_vnb, dev, c.d_evpart, vpart
+  if (c.mixed && vir)
+    k_ehal<true, true><<<nb, kBlock, 0, c.stream>>>(THP_EHAL_ARGS);
+  else if (c.mixed)
+    k_ehal<true, false><<<nb, kBlock, 0, c.stream>>>(THP_EHAL_ARGS);
+  else if (vir)
+    k_ehal<false, true><<<nb, kBlock, 0, c.stream>>>(THP_EHAL_ARGS);
   else
-    k_ehal<false><<<nb, kBlock, 0, c.stream>>>(c.n, c.npad, c.box, vc, c.d_vred, c.d_vredf, c.d_vinfo, c.d_vtab,
-                                               c.d_perm, c.d_sp_off, c.d_sp_ks, c.d_sp_c, c.d_vnnb, c.d_vnb, dev,
-                                               c.d_evpart);
+    k_ehal<false, false><<<nb, kBlock, 0, c.stream>>>(THP_EHAL_ARGS);
+#undef THP_EHAL_ARGS
   if ((st = cuda_status(cudaGetLastError(), &c, "ehal"))) return st;
   k_sum_partials<<<1, 256, 0, c.stream>>>(nb, c.d_evpart, c.d_ev);
   if ((st = cuda_status(cudaGetLastError(), &c, "ehal energy"))) return st;
+  if (vir && (st = virial_total(c, 0, nb, 0, kpart, vpart, epart, c.h_vvir))) return st;
   return launch_gradient_out(c, dev, d_out);
 }
 

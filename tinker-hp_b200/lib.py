@@ -115,6 +115,7 @@ def load():
         "thp_set_virial": ([vp, C.c_int], C.c_int),
         "thp_get_virial": ([vp, C.c_int, _dp], C.c_int),
         "thp_get_empole_virial": ([vp, C.c_int, _dp], C.c_int),
+        "thp_get_ehal_virial": ([vp, _dp], C.c_int),
         "thp_bind_virial": ([vp, _dp], C.c_int),
         "thp_md_verlet": ([vp, C.c_int, C.c_double, _dp, _dp, _dp, _ip], C.c_int),
         "thp_get_positions": ([vp, _dp, _dp, _dp], C.c_int),
@@ -440,6 +441,12 @@ class Context:
         on; form 1 adds the reciprocal torques' frame-atom terms."""
         v = np.zeros((3, 3))
         self._check(load().thp_get_empole_virial(self.h, int(form), _p(v)), "thp_get_empole_virial")
+        return v
+
+    def ehal_virial(self):
+        """vir [3,3] (kcal/mol) of the last ehal1 call made with the virial on."""
+        v = np.zeros((3, 3))
+        self._check(load().thp_get_ehal_virial(self.h, _p(v)), "thp_get_ehal_virial")
         return v
 
     def set_vdw(self, v):
