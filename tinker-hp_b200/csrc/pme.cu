@@ -174,22 +174,12 @@ __global__ void __launch_bounds__(256) k_kspace_virial(int n1, int n2, int n3, c
     for (int q = 0; q < 6; ++q) part[(size_t)blockIdx.x * 6 + q] = sign * v[q];
 }
 
-// grid_uind_site (pmestuff.f:280-405); d dipoles in Re, p dipoles in Im.
-// One thread per site (the 125 atomics of neighbouring threads land in
-// different L2 slices; a warp-per-site variant that made them contiguous
-// measured 1.6x slower).  mode 1 first forms pp = zr + beta*pp
-// (inducepcg_pme2.f:553-559) and writes it back.
-// V: the stored type of vec (FP32 for the mixed form's overlapped CG, which
-// spreads in mode 2 only)
-template <typename T, typename V = double>
-__global__ void __launch_bounds__(128) k_spread_dip(int n, PmeGeom g, const double4* __restrict__ pos,
-                                                   V* __restrict__ vec, const double* __restrict__ zr,
-                                                   float* __restrict__ vecf, const CgScalars* __restrict__ cg,
-                                                   int mode, typename Cplx<T>::type* __restrict__ grid) {
-  if (mode >= 1 && cg->stop) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double v[6];
+// The vector a site spreads: vec[i] (mode 1: zr + beta vec, written back),
+// with the FP32 copy in vecf when given.
+template <typename V>
+__device__ __forceinline__ void spread_load(int i, V* __restrict__ vec, const double* __restrict__ zr,
+                                            float* __restrict__ vecf, const CgScalars* __restrict__ cg, int mode,
+                                            double (&v)[6]) {
   if constexpr (std::is_same<V, float>::value) {
     const float2* v2 = reinterpret_cast<const float2*>(vec + (size_t)i * 6);
     const float2 a0 = v2[0], a1 = v2[1], a2 = v2[2];
@@ -222,7 +212,44 @@ __global__ void __launch_bounds__(128) k_spread_dip(int n, PmeGeom g, const doub
     o[1] = make_float2((float)v[2], (float)v[3]);
     o[2] = make_float2((float)v[4], (float)v[5]);
   }
-  spread_dip_site<T>(g, pos[i], v, grid);
+}
+
+// grid_uind_site (pmestuff.f:280-405); d dipoles in Re, p dipoles in Im.
+// One thread per site.  TA = 0: each site adds its 125 stencil points to the
+// grid itself (a warp-per-site variant that made them contiguous measured
+// 1.6x slower); TA = 16: the warp sums the stencils of 16 neighbouring sites
+// at a time in a shared-memory tile first (spread_dip_warp), blocks of
+// kSpreadThreads threads with one SpreadWarp<T> per warp in dynamic shared
+// memory.  mode 1 first forms pp = zr + beta*pp (inducepcg_pme2.f:553-559) and
+// writes it back.
+// V: the stored type of vec (FP32 for the mixed form's overlapped CG, which
+// spreads in mode 2 only)
+template <typename T, typename V = double, int TA = 0>
+__global__ void __launch_bounds__(128) k_spread_dip(int n, PmeGeom g, const double4* __restrict__ pos,
+                                                   V* __restrict__ vec, const double* __restrict__ zr,
+                                                   float* __restrict__ vecf, const CgScalars* __restrict__ cg,
+                                                   int mode, typename Cplx<T>::type* __restrict__ grid) {
+  if (mode >= 1 && cg->stop) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  SpreadWarp<T>* sw = nullptr;
+  if constexpr (TA > 0) {
+    extern __shared__ __align__(16) unsigned char spread_smem[];
+    sw = reinterpret_cast<SpreadWarp<T>*>(spread_smem) + (threadIdx.x >> 5);
+    for (int q = threadIdx.x & 31; q < SpreadWarp<T>::kPts; q += 32) sw->tile[q] = {T(0), T(0)};
+  } else if (i >= n) {
+    return;
+  }
+  const bool live = i < n;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  double4 pi = make_double4(0, 0, 0, 0);
+  if (live) {
+    spread_load(i, vec, zr, vecf, cg, mode, v);
+    pi = pos[i];
+  }
+  if constexpr (TA > 0)
+    spread_dip_warp<T>(g, pi, v, live, grid, *sw);
+  else
+    spread_dip_site<T>(g, pi, v, grid);
 }
 
 template <typename C, typename T>
@@ -710,18 +737,45 @@ int launch_efld0_recip(Ctx& c) { return launch_efld0_recip_ex(c, nullptr, true);
 // mode 2: spread as is, no FP32 copy, honours the stop flag.  d_out (if non-null) receives the gathered
 // field gradient [n][6] (tmatxbrecip's dipfield); the CG loop passes null and
 // gathers inside its fused matvec kernel.
+// 1: the dipole spread sums the stencils of 16 neighbouring sites in a
+// shared-memory tile per warp before adding them to the grid (at 288k atoms
+// 105 -> 85 us per FP32 spread, 340 -> 200 us FP64); 0: every site adds its
+// own stencil.
+#ifndef THP_SPREAD_TILE
+#define THP_SPREAD_TILE 1
+#endif
+
+template <typename T, typename V, int TA>
+static void spread_tiled(Ctx& c, const PmeGeom& g, V* vec, float* vf, int mode, typename Cplx<T>::type* grid) {
+  constexpr size_t smem = sizeof(SpreadWarp<T>) * (kSpreadThreads / 32);
+  static const bool attr = [] {
+    cudaFuncSetAttribute(k_spread_dip<T, V, TA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return true;
+  }();
+  (void)attr;
+  const int nb = (c.n + kSpreadThreads - 1) / kSpreadThreads;
+  k_spread_dip<T, V, TA><<<nb, kSpreadThreads, smem, c.stream>>>(c.n, g, c.d_pos, vec, c.d_zr, vf, c.d_cg, mode,
+                                                                  grid);
+}
+
+template <typename T, typename V>
+static void spread_dipoles(Ctx& c, const PmeGeom& g, V* vec, float* vf, int mode, typename Cplx<T>::type* grid) {
+  if (THP_SPREAD_TILE)
+    spread_tiled<T, V, 16>(c, g, vec, vf, mode, grid);
+  else
+    k_spread_dip<T, V, 0><<<(c.n + kBlock - 1) / kBlock, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, vec, c.d_zr, vf,
+                                                                             c.d_cg, mode, grid);
+}
+
 int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode) {
   PmeGeom g = geom_of(c);
-  int nb = (c.n + kBlock - 1) / kBlock;
   int st = zero_grid(c);
   if (st) return st;
   float* vf = (c.mixed && mode != 2) ? c.d_vecf : nullptr;
   if (c.mixed)
-    k_spread_dip<float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<double*>(d_vec), c.d_zr, vf,
-                                                  c.d_cg, mode, (cufftComplex*)c.d_grid);
+    spread_dipoles<float, double>(c, g, const_cast<double*>(d_vec), vf, mode, (cufftComplex*)c.d_grid);
   else
-    k_spread_dip<double><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<double*>(d_vec), c.d_zr, vf,
-                                                   c.d_cg, mode, (cufftDoubleComplex*)c.d_grid);
+    spread_dipoles<double, double>(c, g, const_cast<double*>(d_vec), vf, mode, (cufftDoubleComplex*)c.d_grid);
   if ((st = cuda_status(cudaGetLastError(), &c, "spread dip"))) return st;
   if ((st = convolve(c, mode >= 1))) return st;
   if (d_out) st = launch_gather_dip(c, d_out, false);
@@ -732,11 +786,9 @@ int launch_pme_dipole(Ctx& c, const double* d_vec, double* d_out, int mode) {
 // stop flag honoured, no update, no FP32 copy), then the convolution.
 int launch_pme_dipole_f32(Ctx& c, const float* d_vec) {
   PmeGeom g = geom_of(c);
-  int nb = (c.n + kBlock - 1) / kBlock;
   int st = zero_grid(c);
   if (st) return st;
-  k_spread_dip<float, float><<<nb, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, const_cast<float*>(d_vec), nullptr,
-                                                         nullptr, c.d_cg, 2, (cufftComplex*)c.d_grid);
+  spread_dipoles<float, float>(c, g, const_cast<float*>(d_vec), nullptr, 2, (cufftComplex*)c.d_grid);
   if ((st = cuda_status(cudaGetLastError(), &c, "spread dip"))) return st;
   return convolve(c, true);
 }
