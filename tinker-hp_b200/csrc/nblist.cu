@@ -258,6 +258,12 @@ __device__ __forceinline__ int axis_cells(int c, int nc, int q) {
 #define THP_LIST_WARP_ATOMS 20000
 #endif
 
+// 1: larger systems with at least 7 cells per axis screen their candidates
+// with one periodic shift per candidate row (list_row_shifted)
+#ifndef THP_LIST_SHIFTED
+#define THP_LIST_SHIFTED 1
+#endif
+
 // The list decision for candidate k of atom i: the FP32 screen accepts below
 // lo and rejects above hi; between them (and for every candidate when the
 // screen is off) the exact FP64 r^2 of the reference decides.
@@ -266,35 +272,39 @@ struct ListTest {
   double mbuf2;
   int prefilter;
   float lo, hi, bx, by, bz, hx, hy, hz;
-  __device__ __forceinline__ bool take(const double4& pi, const float4& fi, int k, const double4* __restrict__ pos,
-                                       const float4* __restrict__ posf) const {
-    if (prefilter) {
-      const float4 fk = posf[k];
-      float xr = fi.x - fk.x, yr = fi.y - fk.y, zr = fi.z - fk.z;
-      xr = fabsf(xr) > hx ? xr - copysignf(bx, xr) : xr;
-      yr = fabsf(yr) > hy ? yr - copysignf(by, yr) : yr;
-      zr = fabsf(zr) > hz ? zr - copysignf(bz, zr) : zr;
-      const float r2f = xr * xr + yr * yr + zr * zr;
-      if (r2f > hi) return false;
-      if (r2f < lo) return true;
-    }
+  // the FP32 screen alone: 1 accept, 0 reject, 2 undecided
+  __device__ __forceinline__ int screen(const float4& fi, const float4& fk) const {
+    float xr = fi.x - fk.x, yr = fi.y - fk.y, zr = fi.z - fk.z;
+    xr = fabsf(xr) > hx ? xr - copysignf(bx, xr) : xr;
+    yr = fabsf(yr) > hy ? yr - copysignf(by, yr) : yr;
+    zr = fabsf(zr) > hz ? zr - copysignf(bz, zr) : zr;
+    const float r2f = xr * xr + yr * yr + zr * zr;
+    return r2f > hi ? 0 : (r2f < lo ? 1 : 2);
+  }
+  __device__ __forceinline__ bool exact(const double4& pi, int k, const double4* __restrict__ pos) const {
     const double4 pk = pos[k];
     // midpointimage (domdecstuff.f:1773): pos = xi - xk, imaged
     double xr = __dadd_rn(pi.x, -pk.x), yr = __dadd_rn(pi.y, -pk.y), zr = __dadd_rn(pi.z, -pk.z);
     image3(box, xr, yr, zr);
     return r2_exact(xr, yr, zr) <= mbuf2;
   }
+  __device__ __forceinline__ bool take(const double4& pi, const float4& fi, int k, const double4* __restrict__ pos,
+                                       const float4* __restrict__ posf) const {
+    if (prefilter) {
+      const int d = screen(fi, posf[k]);
+      if (d != 2) return d == 1;
+    }
+    return exact(pi, k, pos);
+  }
 };
 
-__global__ void __launch_bounds__(128, THP_LIST_MINB) k_build_list(int n, int npad, ListTest lt, int ncx,
-                                                    int ncy, int ncz, const double4* __restrict__ pos,
-                                                    const float4* __restrict__ posf, const int* __restrict__ scell,
-                                                    const int* __restrict__ cell_start,
-                                                    const int* __restrict__ cell_count, int maxnb,
-                                                    int* __restrict__ nnb, int* __restrict__ nb,
-                                                    int* __restrict__ flags) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// The list row of atom i, its candidates read from global memory.
+__device__ __forceinline__ void list_row_global(int i, int npad, const ListTest& lt, int ncx, int ncy, int ncz,
+                                                const double4* __restrict__ pos, const float4* __restrict__ posf,
+                                                const int* __restrict__ scell, const int* __restrict__ cell_start,
+                                                const int* __restrict__ cell_count, int maxnb,
+                                                int* __restrict__ nnb, int* __restrict__ nb,
+                                                int* __restrict__ flags) {
   const double4 pi = pos[i];
   const float4 fi = posf[i];
   const int c = scell[i];
@@ -327,6 +337,85 @@ __global__ void __launch_bounds__(128, THP_LIST_MINB) k_build_list(int n, int np
   }
   nnb[i] = cnt;
   if (cnt > maxnb) atomicOr(flags, DEV_LIST_OVERFLOW);
+}
+
+// The same row with one periodic shift per candidate row instead of a wrap
+// per candidate: with at least 7 cells along every axis, every candidate of
+// the +-2 window lies within 3 cells (< half a box) of the atom once the
+// rows past a face are shifted by one box length, so the FP32 screen is
+// fi - shift - fk with no per-candidate image.  The screen's error bound is
+// the same (two roundings per coordinate); the exact FP64 test still images
+// each undecided pair itself.
+__device__ __forceinline__ void list_row_shifted(int i, int npad, const ListTest& lt, int ncx, int ncy, int ncz,
+                                                 const double4* __restrict__ pos, const float4* __restrict__ posf,
+                                                 const int* __restrict__ scell, const int* __restrict__ cell_start,
+                                                 const int* __restrict__ cell_count, int maxnb,
+                                                 int* __restrict__ nnb, int* __restrict__ nb,
+                                                 int* __restrict__ flags) {
+  const double4 pi = pos[i];
+  const float4 fi = posf[i];
+  const int c = scell[i];
+  const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
+  int a0, a1, b0, b1;
+  row_ranges(cx, ncx, a0, a1, b0, b1);
+  // part b lies past the lower face (cx - 2 < 0) or the upper one
+  const float fxb = cx < 2 ? fi.x + lt.bx : fi.x - lt.bx;
+  int cnt = 0;
+  for (int qz = 0; qz < 5; ++qz) {
+    const int zr = cz + qz - 2;
+    const int z = zr < 0 ? zr + ncz : (zr >= ncz ? zr - ncz : zr);
+    const float fz = zr < 0 ? fi.z + lt.bz : (zr >= ncz ? fi.z - lt.bz : fi.z);
+    for (int qy = 0; qy < 5; ++qy) {
+      const int yr = cy + qy - 2;
+      const int y = yr < 0 ? yr + ncy : (yr >= ncy ? yr - ncy : yr);
+      const float fy = yr < 0 ? fi.y + lt.by : (yr >= ncy ? fi.y - lt.by : fi.y);
+      const int rowbase = (z * ncy + y) * ncx;
+#pragma unroll
+      for (int part = 0; part < 2; ++part) {
+        const int x0 = part ? b0 : a0, x1 = part ? b1 : a1;
+        if (x0 > x1) continue;
+        const float fx = part ? fxb : fi.x;
+        const int k0 = cell_start[rowbase + x0];
+        const int k1 = cell_start[rowbase + x1] + cell_count[rowbase + x1];
+#pragma unroll 4
+        for (int k = k0; k < k1; ++k) {
+          const float4 fk = posf[k];
+          const float dx = fx - fk.x, dy = fy - fk.y, dz = fz - fk.z;
+          const float r2f = dx * dx + dy * dy + dz * dz;
+          if (r2f > lt.hi || k == i) continue;
+          if (r2f >= lt.lo && !lt.exact(pi, k, pos)) continue;
+          if (cnt < maxnb) nb[(size_t)cnt * npad + i] = k;
+          ++cnt;
+        }
+      }
+    }
+  }
+  nnb[i] = cnt;
+  if (cnt > maxnb) atomicOr(flags, DEV_LIST_OVERFLOW);
+}
+
+__global__ void __launch_bounds__(128, THP_LIST_MINB) k_build_list_shifted(int n, int npad, ListTest lt, int ncx,
+                                                    int ncy, int ncz, const double4* __restrict__ pos,
+                                                    const float4* __restrict__ posf, const int* __restrict__ scell,
+                                                    const int* __restrict__ cell_start,
+                                                    const int* __restrict__ cell_count, int maxnb,
+                                                    int* __restrict__ nnb, int* __restrict__ nb,
+                                                    int* __restrict__ flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  list_row_shifted(i, npad, lt, ncx, ncy, ncz, pos, posf, scell, cell_start, cell_count, maxnb, nnb, nb, flags);
+}
+
+__global__ void __launch_bounds__(128, THP_LIST_MINB) k_build_list(int n, int npad, ListTest lt, int ncx,
+                                                    int ncy, int ncz, const double4* __restrict__ pos,
+                                                    const float4* __restrict__ posf, const int* __restrict__ scell,
+                                                    const int* __restrict__ cell_start,
+                                                    const int* __restrict__ cell_count, int maxnb,
+                                                    int* __restrict__ nnb, int* __restrict__ nb,
+                                                    int* __restrict__ flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  list_row_global(i, npad, lt, ncx, ncy, ncz, pos, posf, scell, cell_start, cell_count, maxnb, nnb, nb, flags);
 }
 
 // The same list with one warp per atom: the lanes test 32 consecutive
@@ -562,6 +651,10 @@ int launch_build_list_on(Ctx& c, cudaStream_t s) {
     k_build_list_warp<<<(n + 3) / 4, 128, 0, s>>>(n, c.npad, lt, c.nc[0], c.nc[1], c.nc[2], c.d_pos, c.d_posf,
                                                   c.d_scell, c.d_cell_start, c.d_cell_count, c.maxnb, c.d_nnb,
                                                   c.d_nb, c.d_flags);
+  else if (THP_LIST_SHIFTED && prefilter && c.nc[0] >= 7 && c.nc[1] >= 7 && c.nc[2] >= 7)
+    k_build_list_shifted<<<(n + 127) / 128, 128, 0, s>>>(n, c.npad, lt, c.nc[0], c.nc[1], c.nc[2], c.d_pos,
+                                                         c.d_posf, c.d_scell, c.d_cell_start, c.d_cell_count,
+                                                         c.maxnb, c.d_nnb, c.d_nb, c.d_flags);
   else
     k_build_list<<<(n + 127) / 128, 128, 0, s>>>(n, c.npad, lt, c.nc[0], c.nc[1], c.nc[2], c.d_pos, c.d_posf,
                                                  c.d_scell, c.d_cell_start, c.d_cell_count, c.maxnb, c.d_nnb,
