@@ -10,6 +10,8 @@ transforms and reduction tiles round differently), within 1e-6 D of the oracle; 
 oracle.  Mixed form: dipoles within 1e-5 D RMS of the oracle and within
 5e-6 D of the mixed solve alone (its FP32 rounding differs), Epol within 6e-7 relative of the oracle.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -123,3 +125,23 @@ def test_plan_rejects_what_it_cannot_batch(lib, thp, boxes):
     mixed_prec = [lib.Context(boxes[0], precision=lib.MIXED), lib.Context(boxes[1], precision=lib.FP64)]
     with pytest.raises(lib.ThpError):
         lib.Batch(mixed_prec)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_plan_with_an_odd_grid_ahead(lib, boxes, precision):
+    # a system with an odd grid (25^3 points) takes the first grid slots; the
+    # systems after it still start on 16-byte boundaries (paired reductions,
+    # vector gathers) and the batched transforms honour the padded slots
+    prec = lib.FP64 if precision == "fp64" else lib.MIXED
+    odd = dataclasses.replace(boxes[0], nfft=(25, 25, 25))
+    systems = [odd] + list(boxes[1:4])
+    ctxs = [lib.Context(ws, precision=prec, poleps=1e-6) for ws in systems]
+    plan = lib.Batch(ctxs)
+    infos = plan.solve()
+    for q, (ws, ctx, info) in enumerate(zip(systems, ctxs, infos)):
+        assert info["converged"], q
+        uind, uinp = ctx.dipoles()
+        alone, (ua, pa) = solve_alone(lib, ws, prec)
+        d = max(rms(uind, ua), rms(uinp, pa))
+        assert d < (1e-9 if prec == lib.FP64 else 5e-6), (q, d)
+    plan.close()

@@ -532,17 +532,25 @@ int batch_plan_create(Ctx* const* cs, int count, BatchPlan** out, std::string* m
     cls[q] = k;
     ++p->classes[k].count;
   }
+  // each system's grid starts on an even point (16-byte boundary of the FP32
+  // grid, which the paired reductions and vector gathers need)
+  auto slot = [](const FftClass& k) {
+    const size_t pts = (size_t)k.n[0] * k.n[1] * k.n[2];
+    return pts + (pts & 1);
+  };
   size_t off = 0;
   for (FftClass& k : p->classes) {
     k.offset = off;
-    off += (size_t)k.count * k.n[0] * k.n[1] * k.n[2];
+    off += (size_t)k.count * slot(k);
   }
   p->grid_bytes = off * csz;
   ok(cudaMalloc(&p->d_grid, p->grid_bytes));
   for (FftClass& k : p->classes) {
     const int dims[3] = {k.n[2], k.n[1], k.n[0]};
-    const int dist = k.n[0] * k.n[1] * k.n[2];
-    if (cufftPlanMany(&k.plan, 3, const_cast<int*>(dims), nullptr, 1, dist, nullptr, 1, dist,
+    const int dist = (int)slot(k);
+    // the storage dimensions given, so that cuFFT honours the padded distance
+    if (cufftPlanMany(&k.plan, 3, const_cast<int*>(dims), const_cast<int*>(dims), 1, dist,
+                      const_cast<int*>(dims), 1, dist,
                       p->mixed ? CUFFT_C2C : CUFFT_Z2Z, k.count) != CUFFT_SUCCESS && !st)
       st = THP_E_CUDA;
     ok(cudaStreamCreateWithFlags(&k.stream, cudaStreamNonBlocking));
@@ -583,7 +591,7 @@ int batch_plan_create(Ctx* const* cs, int count, BatchPlan** out, std::string* m
     s.rec = c.d_rec;
     s.mpz = c.d_mpz;
     s.grid = static_cast<char*>(p->d_grid) + next[cls[q]] * csz;
-    next[cls[q]] += c.ngrid;
+    next[cls[q]] += slot(p->classes[cls[q]]);
     s.qfac = c.d_qfac;
     s.cg = c.d_cg;
     s.partials = c.d_partials;

@@ -4,6 +4,7 @@
 #include <cufft.h>
 
 #include <climits>
+#include <cstdint>
 #include <type_traits>
 
 #include "common.cuh"
@@ -153,6 +154,8 @@ template <typename T>
 __device__ __forceinline__ void spread_dip_stencil(const PmeGeom& g, int gx, int gy, int gz, const T (&tx)[kBs][2],
                                                    const T (&ty)[kBs][2], const T (&tz)[kBs][2], const T (&fd)[3],
                                                    const T (&fp)[3], typename Cplx<T>::type* __restrict__ grid) {
+  // paired reductions need the grid on a 16-byte boundary
+  const bool aligned = (reinterpret_cast<uintptr_t>(grid) & 15) == 0;
 #pragma unroll
   for (int c = 0; c < kBs; ++c) {
     size_t kk = (size_t)wrapk(gz + c, g.n3);
@@ -166,7 +169,7 @@ __device__ __forceinline__ void spread_dip_stencil(const PmeGeom& g, int gx, int
       T term02 = fp[1] * u1 * v0 + fp[2] * u0 * v1;
       T term12 = fp[0] * u0 * v0;
       size_t row = (kk * g.n2 + jj) * g.n1;
-      if (THP_SPREAD_PAIRS && std::is_same<T, float>::value) {
+      if (THP_SPREAD_PAIRS && std::is_same<T, float>::value && aligned) {
         T re[kBs], im[kBs];
 #pragma unroll
         for (int a = 0; a < kBs; ++a) {
@@ -380,7 +383,7 @@ __device__ __forceinline__ bool spread_tile_pass(const PmeGeom& g, unsigned mk, 
   // points starting on an even grid point (the tile's column -1 or X, outside
   // the tile, reads as zero); otherwise one point per lane.
   constexpr bool kPairs = std::is_same<T, float>::value;
-  const bool pairs = kPairs && (g.n1 & 1) == 0;
+  const bool pairs = kPairs && (g.n1 & 1) == 0 && (reinterpret_cast<uintptr_t>(grid) & 15) == 0;
   const int shift = pairs ? ((x0 & 1) ? -1 : 0) : 0;     // tile column of the lane's first point
   const int cols = pairs ? (X - shift + 1) >> 1 : X;     // pairs or points per line
   const int xw = cols <= 8 ? 8 : (cols <= 16 ? 16 : 32);  // lanes per line
