@@ -1,9 +1,10 @@
 """Allocation-free energy entry point (thp_epolar_noalloc), checked through
 the C-ABI against the energy of the regular solve entry point.
 
-Callers such as a Fortran host whose GPU memory is pooled by OpenACC, or code
-enqueuing work inside a CUDA stream capture, cannot allocate device memory;
-this entry point uses only a fixed scratch array compiled into the library.
+Callers such as a Fortran host whose GPU memory is pooled by OpenACC, or a
+loop that must not stall on the device synchronisation cudaMalloc/cudaFree
+imply, cannot allocate device memory; this entry point uses only a fixed
+scratch array compiled into the library.
 The file sorts last so that a run stopping at the first failure has already
 run every other test.
 """

@@ -3,9 +3,8 @@
 // Some callers cannot allocate device memory when they need the energy: a
 // host program whose GPU memory is reserved up front by another runtime (an
 // OpenACC / CUDA-Fortran code that pools the device, as Tinker-HP's GPU build
-// does), code that enqueues work while a CUDA stream is being captured (where
-// cudaMalloc/cudaFree are not allowed), or a latency-critical loop where the
-// implicit device synchronisation of cudaMalloc/cudaFree is unacceptable.
+// does), or a latency-critical loop where the implicit device synchronisation
+// of cudaMalloc/cudaFree is unacceptable.
 // thp_epolar_noalloc serves them: the caller passes device arrays in and a
 // device scalar out, and the only scratch the reduction needs -- one partial
 // sum per thread block and a completion counter -- lives in a fixed-size
