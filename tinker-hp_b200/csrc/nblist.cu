@@ -258,6 +258,11 @@ __device__ __forceinline__ int axis_cells(int c, int nc, int q) {
 #define THP_LIST_WARP_ATOMS 20000
 #endif
 
+// candidates loaded together by the per-row-shift list build
+#ifndef THP_LIST_BATCH
+#define THP_LIST_BATCH 8
+#endif
+
 // 1: larger systems with at least 7 cells per axis screen their candidates
 // with one periodic shift per candidate row (list_row_shifted)
 #ifndef THP_LIST_SHIFTED
@@ -377,15 +382,23 @@ __device__ __forceinline__ void list_row_shifted(int i, int npad, const ListTest
         const float fx = part ? fxb : fi.x;
         const int k0 = cell_start[rowbase + x0];
         const int k1 = cell_start[rowbase + x1] + cell_count[rowbase + x1];
-#pragma unroll 4
-        for (int k = k0; k < k1; ++k) {
-          const float4 fk = posf[k];
-          const float dx = fx - fk.x, dy = fy - fk.y, dz = fz - fk.z;
-          const float r2f = dx * dx + dy * dy + dz * dz;
-          if (r2f > lt.hi || k == i) continue;
-          if (r2f >= lt.lo && !lt.exact(pi, k, pos)) continue;
-          if (cnt < maxnb) nb[(size_t)cnt * npad + i] = k;
-          ++cnt;
+        // candidates in batches of THP_LIST_BATCH, all loads of a batch
+        // issued before its tests (a slot past the range reads as far away)
+        for (int kb = k0; kb < k1; kb += THP_LIST_BATCH) {
+          float4 fk[THP_LIST_BATCH];
+#pragma unroll
+          for (int u = 0; u < THP_LIST_BATCH; ++u)
+            fk[u] = kb + u < k1 ? __ldg(posf + kb + u) : make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.f);
+#pragma unroll
+          for (int u = 0; u < THP_LIST_BATCH; ++u) {
+            const int k = kb + u;
+            const float dx = fx - fk[u].x, dy = fy - fk[u].y, dz = fz - fk[u].z;
+            const float r2f = dx * dx + dy * dy + dz * dz;
+            if (r2f > lt.hi || k == i) continue;
+            if (r2f >= lt.lo && !lt.exact(pi, k, pos)) continue;
+            if (cnt < maxnb) nb[(size_t)cnt * npad + i] = k;
+            ++cnt;
+          }
         }
       }
     }
