@@ -91,6 +91,10 @@ def test_solve_fp64_matches_oracle(lib, case):
     rms_p = np.sqrt(np.mean(np.sum((uinp - ref["uinp"]) ** 2, axis=1))) * DEBYE
     assert rms_d < 1e-6 and rms_p < 1e-6, (rms_d, rms_p)
     assert abs(res["epol"] - e_ref) < 1e-8 * abs(e_ref), (res["epol"], e_ref)
+    # the CG's energy diagnostic ene (newinduce_pme2.f:560-566) of the last
+    # iteration, d and p sets
+    for k in range(2):
+        assert abs(res["ene"][k] - ref["ene"][k]) < 1e-8 * abs(ref["ene"][k]), (k, res["ene"], ref["ene"])
     np.testing.assert_allclose(ctx.field(), ref["ef"], rtol=0, atol=1e-11 * np.abs(ref["ef"]).max())
 
 
@@ -106,6 +110,8 @@ def test_solve_mixed_error_vs_fp64(lib, case):
     assert rms_d < 1e-5, rms_d
     # FP32 pair and grid arithmetic moves Epol by 5e-8 - 2.2e-7 relative here
     assert abs(res["epol"] - e_ref) < 6e-7 * abs(e_ref), (res["epol"], e_ref)
+    for k in range(2):
+        assert abs(res["ene"][k] - ref["ene"][k]) < 1e-5 * abs(ref["ene"][k]), (k, res["ene"], ref["ene"])
 
 
 def test_run_to_run_reproducible(lib, case):

@@ -206,13 +206,13 @@ __global__ void __launch_bounds__(kBlock) kb_update(const BatchSys* __restrict__
     const int2 w = items[it];
     const BatchSys& s = sys[w.x];
     if (s.cg->stop) continue;
-    cg_update_block<double>(w.y, s.nblk, s.n, s.pol, s.ef, s.h, s.pp, s.mu, s.res, s.zr, s.cg, s.partials, s.poleps,
+    cg_update_block<double>(w.y, s.nblk, s.n, s.pol, s.h, s.pp, s.mu, s.res, s.zr, s.cg, s.partials, s.poleps,
                             s.politer);
   }
 }
 
 // Epol of every system (the identity of k_epol: -1/2 electric sum
-// uind . E_p) and each system's CG scalars and error bits written to mapped
+// uind . E_p), its CG energy ene, and each system's CG scalars and error bits written to mapped
 // host memory by the system's last block, so one host synchronisation after
 // the batch's graph sees every result.
 __global__ void __launch_bounds__(kBlock) kb_finish(const BatchSys* __restrict__ sys, const int2* __restrict__ items,
@@ -221,15 +221,21 @@ __global__ void __launch_bounds__(kBlock) kb_finish(const BatchSys* __restrict__
     const int2 w = items[it];
     const BatchSys& s = sys[w.x];
     const int i = w.y * kBlock + threadIdx.x;
-    double red[1] = {0.0};
+    double red[3] = {0.0, 0.0, 0.0};
     if (i < s.n) {
-      const double* m = s.mu + (size_t)i * 6;
-      const double* e = s.ef + (size_t)i * 6;
+      double m[6], e[6], r[6];
+      load6(s.mu + (size_t)i * 6, m);
+      load6(s.ef + (size_t)i * 6, e);
+      load6(s.res + (size_t)i * 6, r);
       red[0] = m[0] * e[3] + m[1] * e[4] + m[2] * e[5];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) red[q < 3 ? 1 : 2] -= 0.5 * (m[q] * (r[q] + e[q]));
     }
-    double tot[1];
-    if (grid_reduce_of<1>(red, s.partials, &s.cg->counter[2], w.y, s.nblk, tot) && threadIdx.x == 0) {
+    double tot[3];
+    if (grid_reduce_of<3>(red, s.partials, &s.cg->counter[2], w.y, s.nblk, tot) && threadIdx.x == 0) {
       s.cg->epol = -0.5 * kElectric * tot[0];
+      s.cg->ene[0] = tot[1];
+      s.cg->ene[1] = tot[2];
       __threadfence();
       out[w.x].cg = *s.cg;
       out[w.x].flags = *s.flags;

@@ -300,23 +300,25 @@ __device__ __forceinline__ void row_block(int blk, const PairRows& pr, const Box
   }
 }
 
-// newinduce_pme2.f:512-572
+// newinduce_pme2.f:512-572.  The reference's per-iteration energy ene (a
+// diagnostic printed at each step) is formed once, after the loop, from the
+// final mu and residual (k_epol / kb_finish): the same value the last
+// iteration would give, without reading E0 on every iteration.
 template <typename V>
 __device__ __forceinline__ void cg_update_block(int blk, int nblk, int n, const double* __restrict__ pol,
-                                                const double* __restrict__ ef, const V* __restrict__ h,
-                                                const V* __restrict__ pp, double* __restrict__ mu,
-                                                V* __restrict__ res, V* __restrict__ zr, CgScalars* cg,
-                                                double* __restrict__ partials, double poleps, int politer) {
+                                                const V* __restrict__ h, const V* __restrict__ pp,
+                                                double* __restrict__ mu, V* __restrict__ res, V* __restrict__ zr,
+                                                CgScalars* cg, double* __restrict__ partials, double poleps,
+                                                int politer) {
   const int i = blk * kBlock + threadIdx.x;
-  double red[4] = {0, 0, 0, 0};
+  double red[2] = {0, 0};
   if (i < n) {
     const double ad = cg->alpha[0], ap = cg->alpha[1];
-    double m6[6], r6[6], p6[6], h6[6], e6[6], z6[6];
+    double m6[6], r6[6], p6[6], h6[6], z6[6];
     load6(mu + (size_t)i * 6, m6);
     load6(res + (size_t)i * 6, r6);
     load6(pp + (size_t)i * 6, p6);
     load6(h + (size_t)i * 6, h6);
-    load6(ef + (size_t)i * 6, e6);
     const double dg = diag_of(pol[i]);
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
@@ -329,23 +331,18 @@ __device__ __forceinline__ void cg_update_block(int blk, int nblk, int n, const 
     store6(res + (size_t)i * 6, r6);
     store6(zr + (size_t)i * 6, z6);
 #pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      const int k = q < 3 ? 0 : 1;
-      red[k] += r6[q] * z6[q];
-      red[2 + k] -= 0.5 * (m6[q] * (r6[q] + e6[q]));
-    }
+    for (int q = 0; q < 6; ++q) red[q < 3 ? 0 : 1] += r6[q] * z6[q];
   }
-  double tot[4];
-  if (grid_reduce_of<4>(red, partials, &cg->counter[1], blk, nblk, tot) && threadIdx.x == 0) {
+  double tot[2];
+  if (grid_reduce_of<2>(red, partials, &cg->counter[1], blk, nblk, tot) && threadIdx.x == 0) {
     const double nrm = (double)(3 * n);
     double resnrm = 0.0;
     bool bad = false;
     for (int k = 0; k < 2; ++k) {
       cg->ggnew[k] = tot[k];
-      cg->ene[k] = tot[2 + k];
       const double gn = sqrt(tot[k] / nrm);
       resnrm = fmax(resnrm, gn);
-      bad |= !isfinite(tot[k]) || !isfinite(tot[2 + k]);
+      bad |= !isfinite(tot[k]);
       cg->beta[k] = tot[k] / cg->ggold[k];
       cg->ggold[k] = tot[k];
     }

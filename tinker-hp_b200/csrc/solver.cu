@@ -164,13 +164,13 @@ __global__ void __launch_bounds__(kBlock) k_cg_combine(int n, const double* __re
 
 // mu, residual and preconditioned residual of one CG step (cg_update_block)
 template <typename V>
-__global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __restrict__ pol, const double* __restrict__ ef,
+__global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __restrict__ pol,
                                                       const V* __restrict__ h, const V* __restrict__ pp,
                                                       double* __restrict__ mu, V* __restrict__ res,
                                                       V* __restrict__ zr, CgScalars* cg, double* __restrict__ partials,
                                                       double poleps, int politer) {
   if (cg->stop) return;
-  cg_update_block<V>((int)blockIdx.x, (int)gridDim.x, n, pol, ef, h, pp, mu, res, zr, cg, partials, poleps, politer);
+  cg_update_block<V>((int)blockIdx.x, (int)gridDim.x, n, pol, h, pp, mu, res, zr, cg, partials, poleps, politer);
 }
 
 // Last node of the device-side loop body: keep looping while the CG has not
@@ -204,17 +204,30 @@ __global__ void k_guess_delta(int n, const double* __restrict__ pol, const doubl
 
 // epolar0c via the identity Epol = -1/2 electric sum uind . E_p(perm)
 // (epreal0c + eprecip + self of epolar.f:47-520 sum to exactly this form)
+// Epol = -1/2 electric sum uind . E_p, and the CG's ene (newinduce_pme2.f:
+// 560-566: -1/2 sum mu . (res + ef) for the d and p sets, in units of
+// electric) from the final mu and residual; res is stored as V.
+template <typename V>
 __global__ void __launch_bounds__(kBlock) k_epol(int n, const double* __restrict__ mu, const double* __restrict__ ef,
-                                                 CgScalars* cg, double* __restrict__ partials) {
+                                                 const V* __restrict__ res, CgScalars* cg,
+                                                 double* __restrict__ partials) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double red[1] = {0.0};
+  double red[3] = {0.0, 0.0, 0.0};
   if (i < n) {
-    const double* m = mu + (size_t)i * 6;
-    const double* e = ef + (size_t)i * 6;
+    double m[6], e[6], r[6];
+    load6(mu + (size_t)i * 6, m);
+    load6(ef + (size_t)i * 6, e);
+    load6(res + (size_t)i * 6, r);
     red[0] = m[0] * e[3] + m[1] * e[4] + m[2] * e[5];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) red[q < 3 ? 1 : 2] -= 0.5 * (m[q] * (r[q] + e[q]));
   }
-  double tot[1];
-  if (grid_reduce<1>(red, partials, &cg->counter[2], tot) && threadIdx.x == 0) cg->epol = -0.5 * kElectric * tot[0];
+  double tot[3];
+  if (grid_reduce<3>(red, partials, &cg->counter[2], tot) && threadIdx.x == 0) {
+    cg->epol = -0.5 * kElectric * tot[0];
+    cg->ene[0] = tot[1];
+    cg->ene[1] = tot[2];
+  }
 }
 
 // original [n][nrhs][3] <-> sorted [n][6]
@@ -359,7 +372,7 @@ static int enqueue_iteration(Ctx& c) {
                                                              c.d_cg);
     if ((st = cuda_status(cudaGetLastError(), &c, "pp update"))) return st;
     if ((st = matvec_overlapped<float>(c, c.d_ppf, 0))) return st;
-    k_cg_update<float><<<nb, kBlock, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_hf, c.d_ppf, c.d_mu, c.d_resf,
+    k_cg_update<float><<<nb, kBlock, 0, c.stream>>>(c.n, c.d_pol, c.d_hf, c.d_ppf, c.d_mu, c.d_resf,
                                                     c.d_zrf, c.d_cg, c.d_partials, c.cfg.poleps, c.cfg.politer);
     return cuda_status(cudaGetLastError(), &c, "cg update");
   }
@@ -371,7 +384,7 @@ static int enqueue_iteration(Ctx& c) {
     if ((st = launch_pme_dipole(c, c.d_pp, nullptr, 1))) return st;
     if ((st = launch_matvec(c, c.d_pp, 0))) return st;
   }
-  k_cg_update<double><<<nb, kBlock, 0, c.stream>>>(c.n, c.d_pol, c.d_ef, c.d_h, c.d_pp, c.d_mu, c.d_res, c.d_zr,
+  k_cg_update<double><<<nb, kBlock, 0, c.stream>>>(c.n, c.d_pol, c.d_h, c.d_pp, c.d_mu, c.d_res, c.d_zr,
                                                    c.d_cg, c.d_partials, c.cfg.poleps, c.cfg.politer);
   return cuda_status(cudaGetLastError(), &c, "cg update");
 }
@@ -541,7 +554,10 @@ int run_pcg(Ctx& c, int guess) {
 
 int launch_epol(Ctx& c) {
   const int nb = (c.n + kBlock - 1) / kBlock;
-  k_epol<<<nb, kBlock, 0, c.stream>>>(c.n, c.d_mu, c.d_ef, c.d_cg, c.d_partials);
+  if (overlapped(c) && c.mixed)
+    k_epol<float><<<nb, kBlock, 0, c.stream>>>(c.n, c.d_mu, c.d_ef, c.d_resf, c.d_cg, c.d_partials);
+  else
+    k_epol<double><<<nb, kBlock, 0, c.stream>>>(c.n, c.d_mu, c.d_ef, c.d_res, c.d_cg, c.d_partials);
   return cuda_status(cudaGetLastError(), &c, "epol");
 }
 
