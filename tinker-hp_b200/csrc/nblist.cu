@@ -434,8 +434,11 @@ __global__ void __launch_bounds__(128, THP_LIST_MINB) k_build_list(int n, int np
 // The same list with one warp per atom: the lanes test 32 consecutive
 // candidates of a cell-row range at a time and the accepted ones are written
 // in candidate order (ballot prefix), so the list is the thread-per-atom
-// kernel's entry for entry.  Small systems, where the +-2 cell window spans
-// most of the box and few atoms leave most of the GPU idle, use it.
+// kernel's entry for entry.  The ranges of all 25 rows are loaded at once
+// (row q by lane q, passed around by shuffles), and each chunk's positions
+// one chunk ahead of its tests, so a warp waits on far fewer dependent
+// loads.  Small systems, where the +-2 cell window spans most of the box and
+// few atoms leave most of the GPU idle, use it.
 __global__ void __launch_bounds__(128) k_build_list_warp(int n, int npad, ListTest lt, int ncx, int ncy, int ncz,
                                                         const double4* __restrict__ pos,
                                                         const float4* __restrict__ posf,
@@ -453,30 +456,67 @@ __global__ void __launch_bounds__(128) k_build_list_warp(int n, int npad, ListTe
   const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
   int a0, a1, b0, b1;
   row_ranges(cx, ncx, a0, a1, b0, b1);
-  const int my = min(ncy, 5), mz = min(ncz, 5);
-  int cnt = 0;
-  for (int qz = 0; qz < mz; ++qz) {
-    const int z = axis_cells(cz, ncz, qz);
-    for (int qy = 0; qy < my; ++qy) {
-      const int y = axis_cells(cy, ncy, qy);
-      const int rowbase = (z * ncy + y) * ncx;
-      for (int part = 0; part < 2; ++part) {
-        const int x0 = part ? b0 : a0, x1 = part ? b1 : a1;
-        if (x0 > x1) continue;
-        const int k0 = cell_start[rowbase + x0];
-        const int k1 = cell_start[rowbase + x1] + cell_count[rowbase + x1];
-        for (int kb = k0; kb < k1; kb += 32) {
-          const int k = kb + lane;
-          const bool t = k < k1 && k != i && lt.take(pi, fi, k, pos, posf);
-          const unsigned ball = __ballot_sync(0xffffffffu, t);
-          if (t) {
-            const int slot = cnt + __popc(ball & ((1u << lane) - 1u));
-            if (slot < maxnb) nb[(size_t)slot * npad + i] = k;
-          }
-          cnt += __popc(ball);
-        }
+  const int my = min(ncy, 5), mz = min(ncz, 5), nrow = my * mz;
+  // the candidate ranges of all rows at once, row q on lane q: parts a and b
+  int ra0 = 0, ra1 = 0, rb0 = 0, rb1 = 0;
+  if (lane < nrow) {
+    const int qz = lane / my, qy = lane - qz * my;
+    const int rowbase = (axis_cells(cz, ncz, qz) * ncy + axis_cells(cy, ncy, qy)) * ncx;
+    ra0 = cell_start[rowbase + a0];
+    ra1 = cell_start[rowbase + a1] + cell_count[rowbase + a1];
+    if (b0 <= b1) {
+      rb0 = cell_start[rowbase + b0];
+      rb1 = cell_start[rowbase + b1] + cell_count[rowbase + b1];
+    }
+  }
+  // chunks of 32 candidates in the order row, part, position; each chunk's
+  // positions are loaded one chunk ahead of its tests
+  int q = 0, part = 0, kb = __shfl_sync(0xffffffffu, ra0, 0), ke = __shfl_sync(0xffffffffu, ra1, 0);
+  auto advance = [&]() {  // to the next non-empty chunk; q == nrow past the last
+    kb += 32;
+    while (kb >= ke && q < nrow) {
+      if (part == 0 && b0 <= b1) {
+        part = 1;
+        kb = __shfl_sync(0xffffffffu, rb0, q);
+        ke = __shfl_sync(0xffffffffu, rb1, q);
+      } else if (++q < nrow) {
+        part = 0;
+        kb = __shfl_sync(0xffffffffu, ra0, q);
+        ke = __shfl_sync(0xffffffffu, ra1, q);
       }
     }
+  };
+  if (kb >= ke) {
+    kb -= 32;
+    advance();
+  }
+  auto load = [&](int k0, int k1) {
+    const int k = k0 + lane;
+    return (lt.prefilter && k < k1) ? __ldg(posf + k) : make_float4(0.f, 0.f, 0.f, 0.f);
+  };
+  float4 fcur = q < nrow ? load(kb, ke) : make_float4(0.f, 0.f, 0.f, 0.f);
+  int cnt = 0;
+  while (q < nrow) {
+    const int ck = kb, ce = ke;
+    advance();
+    const float4 fnext = q < nrow ? load(kb, ke) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int k = ck + lane;
+    bool t = false;
+    if (k < ce && k != i) {
+      if (lt.prefilter) {
+        const int d = lt.screen(fi, fcur);
+        t = d == 2 ? lt.exact(pi, k, pos) : d == 1;
+      } else {
+        t = lt.exact(pi, k, pos);
+      }
+    }
+    fcur = fnext;
+    const unsigned ball = __ballot_sync(0xffffffffu, t);
+    if (t) {
+      const int slot = cnt + __popc(ball & ((1u << lane) - 1u));
+      if (slot < maxnb) nb[(size_t)slot * npad + i] = k;
+    }
+    cnt += __popc(ball);
   }
   if (lane == 0) {
     nnb[i] = cnt;
