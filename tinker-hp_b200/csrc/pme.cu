@@ -737,12 +737,21 @@ int launch_efld0_recip(Ctx& c) { return launch_efld0_recip_ex(c, nullptr, true);
 // mode 2: spread as is, no FP32 copy, honours the stop flag.  d_out (if non-null) receives the gathered
 // field gradient [n][6] (tmatxbrecip's dipfield); the CG loop passes null and
 // gathers inside its fused matvec kernel.
-// 1: the dipole spread sums the stencils of 16 neighbouring sites in a
-// shared-memory tile per warp before adding them to the grid (at 288k atoms
-// 105 -> 85 us per FP32 spread, 340 -> 200 us FP64); 0: every site adds its
-// own stencil.
+// 1: the dipole spread of systems of at least THP_SPREAD_TILE_ATOMS (FP32
+// grid) / THP_SPREAD_TILE_ATOMS_F64 atoms sums the stencils of 16
+// neighbouring sites in a shared-memory tile per warp before adding them to
+// the grid (at 288k atoms 105 -> 85 us per FP32 spread, 340 -> 200 us FP64);
+// smaller systems, and 0, let every site add its own stencil (measured
+// faster below those sizes: mixed solves of 4.5k-32k atoms against the tile's
+// gain from 96k; FP64 solves of 4.5k-12k atoms against its gain from 32k).
 #ifndef THP_SPREAD_TILE
 #define THP_SPREAD_TILE 1
+#endif
+#ifndef THP_SPREAD_TILE_ATOMS
+#define THP_SPREAD_TILE_ATOMS 50000
+#endif
+#ifndef THP_SPREAD_TILE_ATOMS_F64
+#define THP_SPREAD_TILE_ATOMS_F64 20000
 #endif
 
 template <typename T, typename V, int TA>
@@ -760,7 +769,8 @@ static void spread_tiled(Ctx& c, const PmeGeom& g, V* vec, float* vf, int mode, 
 
 template <typename T, typename V>
 static void spread_dipoles(Ctx& c, const PmeGeom& g, V* vec, float* vf, int mode, typename Cplx<T>::type* grid) {
-  if (THP_SPREAD_TILE)
+  constexpr int kMin = std::is_same<T, float>::value ? THP_SPREAD_TILE_ATOMS : THP_SPREAD_TILE_ATOMS_F64;
+  if (THP_SPREAD_TILE && c.n >= kMin)
     spread_tiled<T, V, 16>(c, g, vec, vf, mode, grid);
   else
     k_spread_dip<T, V, 0><<<(c.n + kBlock - 1) / kBlock, kBlock, 0, c.stream>>>(c.n, g, c.d_pos, vec, c.d_zr, vf,
