@@ -139,11 +139,8 @@ static void launch_kb_spread(cudaStream_t st, const BatchSys* sys, const int2* i
   if (MIXED ? THP_BATCH_SPREAD_TILE_F32 : THP_BATCH_SPREAD_TILE_F64) {
     using T = typename std::conditional<MIXED, float, double>::type;
     constexpr size_t smem = sizeof(SpreadWarp<T>) * (kBlock / 32);
-    static const bool attr = [] {
-      cudaFuncSetAttribute(kb_spread<MIXED, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      return true;
-    }();
-    (void)attr;
+    static std::atomic<unsigned long long> limit_set{0};
+    smem_limit_once(kb_spread<MIXED, true>, smem, limit_set);
     kb_spread<MIXED, true><<<blocks, kBlock, smem, st>>>(sys, items, nitems);
   } else {
     kb_spread<MIXED, false><<<blocks, kBlock, 0, st>>>(sys, items, nitems);

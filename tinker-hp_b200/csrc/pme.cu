@@ -757,11 +757,8 @@ int launch_efld0_recip(Ctx& c) { return launch_efld0_recip_ex(c, nullptr, true);
 template <typename T, typename V, int TA>
 static void spread_tiled(Ctx& c, const PmeGeom& g, V* vec, float* vf, int mode, typename Cplx<T>::type* grid) {
   constexpr size_t smem = sizeof(SpreadWarp<T>) * (kSpreadThreads / 32);
-  static const bool attr = [] {
-    cudaFuncSetAttribute(k_spread_dip<T, V, TA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    return true;
-  }();
-  (void)attr;
+  static std::atomic<unsigned long long> limit_set{0};
+  smem_limit_once(k_spread_dip<T, V, TA>, smem, limit_set);
   const int nb = (c.n + kSpreadThreads - 1) / kSpreadThreads;
   k_spread_dip<T, V, TA><<<nb, kSpreadThreads, smem, c.stream>>>(c.n, g, c.d_pos, vec, c.d_zr, vf, c.d_cg, mode,
                                                                   grid);

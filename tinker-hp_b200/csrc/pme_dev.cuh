@@ -3,6 +3,7 @@
 
 #include <cufft.h>
 
+#include <atomic>
 #include <climits>
 #include <cstdint>
 #include <type_traits>
@@ -234,6 +235,19 @@ __device__ __forceinline__ void spread_dip_site(const PmeGeom& g, double4 p, con
 #ifndef THP_SPREAD_TILE_PTS_F64
 #define THP_SPREAD_TILE_PTS_F64 1024  // FP64 grid: 16 KB of tile per warp
 #endif
+// Raises a kernel's dynamic shared-memory limit on the current device, once
+// per device: the attribute belongs to each device's copy of the kernel, so
+// a process with contexts on several devices sets it on each.
+template <typename K>
+inline void smem_limit_once(K* kernel, size_t bytes, std::atomic<unsigned long long>& done) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  const unsigned long long bit = 1ull << dev;
+  if (done.load(std::memory_order_acquire) & bit) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  done.fetch_or(bit, std::memory_order_acq_rel);
+}
+
 constexpr int kSpreadRec = 36;      // staged weights per site: tx, ty, tz (10 each), fd, fp
 constexpr int kSpreadThreads = 64;  // block of the tiled spread kernels: two warps
 
